@@ -1,0 +1,129 @@
+// Device-side data layout and math of the explicit soft-body substep.
+//
+// Every floating-point expression below is written in the reference's operation order (src/core/math.h vector ops,
+// src/phys/softbody.cpp, src/phys/static_world.cpp, src/phys/world.cpp) and the library is compiled with
+// --fmad=false and IEEE division / square root, so each operation rounds once, as in the reference built without FMA
+// contraction: a node's state after any number of substeps is bitwise the reference's (exp/pow excepted: see
+// bl_expf / bl_powf).
+#pragma once
+
+#include <cstdint>
+
+namespace blg {
+
+constexpr int kMaxCand = 64;               // BL_GPU_MAX_CANDIDATES
+constexpr uint32_t kBeamAsleep = 1u << 31; // Beam meta: the beam's body sleeps (not stepped)
+constexpr float kMaxNodeSpeed = 400.0f;    // softbody.h:153
+constexpr int kSurfCount = 11;
+
+enum : uint32_t { NF_GROUND = 1, NF_FIXED = 2, NF_TYRE = 4, NF_RIM = 8, NF_CONTACTER = 16 };
+enum : uint32_t { BT_NORMAL = 0, BT_ROPE = 1, BT_SUPPORT = 2 };
+enum : uint32_t { BF_BROKEN = 1, BF_NO_DEFORM = 4, BF_NO_BREAK = 8, BF_SHOCK = 64 };
+// body bits kept in each beam's meta word (bits 16-18): the body's allow_deform / allow_break / ductile
+enum : uint32_t { BB_DEFORM = 1u << 16, BB_BREAK = 1u << 17, BB_DUCTILE = 1u << 18 };
+enum : uint32_t { DEVERR_CANDIDATES = 1, DEVERR_NONFINITE = 2 };
+
+// Ground model (GroundModel, static_world.h:18-31): the values of ground_models() (static_world.cpp:85-114)
+struct GroundModel {
+    float va, ms, mc, t2, vs, alpha, strength, soft_depth, fluid_drag, fluid_density;
+};
+
+struct Box {      // StaticBox (static_world.h:121-131): no hull planes
+    float cx, cy, cz, hx, hy, hz;
+    float r[9];   // columns: local axes in world space (to_mat3 of its quaternion, math.h:166-174)
+    float mnx, mny, mnz, mxx, mxy, mxz; // aabb
+    int surface;
+    float max_force;
+};
+
+struct Cyl {      // StaticCylinder (static_world.h:133-137)
+    float bx, by, bz, radius, height;
+    int surface;
+};
+
+// The static world as the kernels see it (by value as a kernel parameter)
+struct Statics {
+    int has_terrain, hnx, hnz, bx, bz;
+    float cell, ox, oz;
+    const float* h;          // nz x nx heights
+    const uint8_t* surf;     // nz x nx surfaces
+    const float* block_max;  // bz x bx maxima over 16 x 16 cells (Heightfield::update_bounds)
+    float kill_y;
+    int nboxes, ncyls;
+    const Box* boxes;
+    const Cyl* cyls;
+    int gx, gz, nbig;        // box grid (StaticWorld::build_grid)
+    float gox, goz, grid_cell;
+    const int* cell_ptr;
+    const int* cell_items;
+    const int* big;
+};
+
+// A body on the device. The first 64 bytes are what the node kernel reads for every node.
+struct alignas(64) Body {
+    // hot: node kernel
+    float fric;              // SoftBody::ground_friction (x rest_friction when resting: rest damping is not supported)
+    float bounce, push_max, slop;
+    float terrain_max;       // this frame's terrain culling height (World::Island::terrain_max)
+    int sleeping;
+    int nbox, ncyl;          // this frame's static candidates (-1: more than kMaxCand)
+    int node0, nnodes, beam0, nbeams;
+    int can_sleep;
+    float sleep_speed;
+    float max_speed, sleep_timer;
+    // frame accumulators (atomics of the node kernel)
+    float acc_mn[3], acc_mx[3];
+    float acc_v2;
+    int acc_contacts;
+    // per frame results
+    float aabb_mn[3], aabb_mx[3];
+    int static_contacts, broken_beams, repaired;
+    int fell_asleep, needs_repair;
+    int box_ids[kMaxCand];
+    int cyl_ids[kMaxCand];
+};
+
+// ------------------------------------------------------------------------------------------ math in the reference's order
+struct v3 {
+    float x, y, z;
+};
+__device__ __forceinline__ v3 V(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ v3 operator+(v3 a, v3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ v3 operator-(v3 a, v3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ v3 operator*(v3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float length(v3 a) { return sqrtf(dot(a, a)); }
+// vec3 / float: times the reciprocal (math.h:56)
+__device__ __forceinline__ v3 divs(v3 a, float s) {
+    const float i = 1.0f / s;
+    return {a.x * i, a.y * i, a.z * i};
+}
+__device__ __forceinline__ v3 normalize(v3 a) {
+    const float l = length(a);
+    return l > 1e-12f ? a * (1.0f / l) : V(0, 0, 0);
+}
+// std::min / std::max as evaluated by the reference
+__device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float smax(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float clampf(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+__device__ __forceinline__ float signf(float v) { return v < 0.0f ? -1.0f : 1.0f; }
+__device__ __forceinline__ v3 vabs(v3 a) { return {fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
+
+// exp and pow of the ground friction's Stribeck curve: evaluated in double precision and rounded once to float, i.e.
+// the correctly rounded float result in all but vanishingly rare cases - the value the reference's libm returns
+__device__ __forceinline__ float bl_expf(float x) { return (float)exp((double)x); }
+__device__ __forceinline__ float bl_powf(float x, float y) { return (float)pow((double)x, (double)y); }
+
+// float atomics through the integer order of IEEE floats (no NaN)
+__device__ __forceinline__ void atomic_min_f(float* a, float v) {
+    if (v >= 0.0f) atomicMin((int*)a, __float_as_int(v));
+    else atomicMax((unsigned int*)a, __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f(float* a, float v) {
+    if (v >= 0.0f) atomicMax((int*)a, __float_as_int(v));
+    else atomicMin((unsigned int*)a, __float_as_uint(v));
+}
+
+__device__ __constant__ GroundModel c_ground[kSurfCount];
+
+} // namespace blg

@@ -1,0 +1,686 @@
+// Kernels of the explicit substep. Per frame (World::step_substeps, world.cpp:368-585):
+//
+//   k_frame_begin   one thread per body: static candidates over the box grown by its travel, terrain height bound
+//   n x { k_beams   one thread per beam: spring-damper, plastic yield, break -> the beam's force (scratch fv)
+//         k_nodes } one thread per node: gravity + its beams' forces in beam order, static contact, integration,
+//                   bounds / top speed / contacts reduced per body
+//   k_frame_finish  one block: each body's bounds, top speed, repair of runaway nodes, sleep
+//   k_sleep_apply   one block per body: a body that fell asleep stops (velocities zero, beams parked)
+//
+// Determinism: k_nodes sums a node's forces in the order the reference's serial loop adds them (gravity, then each
+// beam in index order: f[a] += fv, f[b] -= fv; softbody.cpp:330-470), from a per-node list of incident beams sorted
+// by beam index, so no atomics touch a force.
+#pragma once
+
+#include "bl_device.cuh"
+
+namespace blg {
+
+// ------------------------------------------------------------------------------------------ statics queries
+// Heightfield::sample (static_world.cpp:189-205)
+__device__ __forceinline__ bool hf_sample(const Statics& st, float x, float z, float& out_h, v3& n) {
+    const float lx = (x - st.ox) / st.cell, lz = (z - st.oz) / st.cell;
+    if (!(lx >= 0 && lz >= 0 && lx < st.hnx - 1 && lz < st.hnz - 1)) return false;
+    const int ix = (int)lx, iz = (int)lz;
+    const float fx = lx - ix, fz = lz - iz;
+    const float* row0 = st.h + (size_t)iz * st.hnx;
+    const float* row1 = row0 + st.hnx;
+    const float h00 = row0[ix], h10 = row0[ix + 1], h01 = row1[ix], h11 = row1[ix + 1];
+    if (smin(smin(h00, h10), smin(h01, h11)) < -1e29f) return false;
+    if (fx > fz) {
+        out_h = h00 + (h10 - h00) * fx + (h11 - h10) * fz;
+        n = normalize(V(-(h10 - h00) / st.cell, 1.0f, -(h11 - h10) / st.cell));
+    } else {
+        out_h = h00 + (h11 - h01) * fx + (h01 - h00) * fz;
+        n = normalize(V(-(h11 - h01) / st.cell, 1.0f, -(h01 - h00) / st.cell));
+    }
+    return true;
+}
+
+// Heightfield::surface_at (static_world.cpp:213-218)
+__device__ __forceinline__ int hf_surface_at(const Statics& st, float x, float z) {
+    int ix = (int)lroundf((x - st.ox) / st.cell), iz = (int)lroundf((z - st.oz) / st.cell);
+    ix = max(0, min(st.hnx - 1, ix));
+    iz = max(0, min(st.hnz - 1, iz));
+    return st.surf[(size_t)iz * st.hnx + ix];
+}
+
+// Heightfield::max_height (static_world.cpp:220-231)
+__device__ float hf_max_height(const Statics& st, float x0, float z0, float x1, float z1) {
+    const int kBlock = 16;
+    int bx0 = (int)floorf((x0 - st.ox) / st.cell) / kBlock, bx1 = (int)floorf((x1 - st.ox) / st.cell) / kBlock;
+    int bz0 = (int)floorf((z0 - st.oz) / st.cell) / kBlock, bz1 = (int)floorf((z1 - st.oz) / st.cell) / kBlock;
+    bx0 = max(0, bx0);
+    bz0 = max(0, bz0);
+    bx1 = min(st.bx - 1, bx1);
+    bz1 = min(st.bz - 1, bz1);
+    float m = -1e30f;
+    for (int bz = bz0; bz <= bz1; bz++)
+        for (int bx = bx0; bx <= bx1; bx++) m = smax(m, st.block_max[(size_t)bz * st.bx + bx]);
+    return m;
+}
+
+struct Contact {
+    v3 normal;
+    float depth;
+    int surface;
+    float max_force;
+};
+
+// StaticWorld::collide_point (static_world.cpp:364-474), boxes without hull planes
+__device__ bool collide_point(const Statics& st, v3 p, float r, const int* box_ids, int nbox, const int* cyl_ids, int ncyl, bool test_terrain,
+                              Contact& out) {
+    bool hit = false;
+    out.depth = 0;
+    out.max_force = 0;
+    out.surface = 0;
+    out.normal = V(0, 0, 0);
+    if (test_terrain && st.has_terrain) {
+        float th;
+        v3 n;
+        if (hf_sample(st, p.x, p.z, th, n)) {
+            const float d = (th - p.y) * n.y + r;
+            if (d > 0) {
+                out.depth = d;
+                out.normal = n;
+                out.surface = hf_surface_at(st, p.x, p.z);
+                hit = true;
+            }
+        }
+    }
+    for (int k = 0; k < nbox; k++) {
+        const Box& b = st.boxes[box_ids[k]];
+        if (p.x < b.mnx - r || p.x > b.mxx + r || p.y < b.mny - r || p.y > b.mxy + r || p.z < b.mnz - r || p.z > b.mxz + r) continue;
+        const v3 c0 = V(b.r[0], b.r[1], b.r[2]), c1 = V(b.r[3], b.r[4], b.r[5]), c2 = V(b.r[6], b.r[7], b.r[8]);
+        const v3 rel = p - V(b.cx, b.cy, b.cz);
+        const v3 l = V(dot(rel, c0), dot(rel, c1), dot(rel, c2));
+        const v3 q = V(clampf(l.x, -b.hx, b.hx), clampf(l.y, -b.hy, b.hy), clampf(l.z, -b.hz, b.hz));
+        const v3 d = l - q;
+        const float dist2 = dot(d, d);
+        float depth;
+        v3 nl;
+        if (dist2 > 1e-12f) {
+            if (dist2 >= r * r) continue;
+            const float dist = sqrtf(dist2);
+            depth = r - dist;
+            nl = divs(d, dist);
+        } else {
+            const v3 pen = V(b.hx, b.hy, b.hz) - vabs(l);
+            if (pen.x <= pen.y && pen.x <= pen.z) depth = pen.x, nl = V(signf(l.x), 0, 0);
+            else if (pen.y <= pen.z) depth = pen.y, nl = V(0, signf(l.y), 0);
+            else depth = pen.z, nl = V(0, 0, signf(l.z));
+            depth += r;
+        }
+        if (depth > out.depth) {
+            out.depth = depth;
+            out.normal = c0 * nl.x + c1 * nl.y + c2 * nl.z;
+            out.surface = b.surface;
+            out.max_force = b.max_force;
+            hit = true;
+        }
+    }
+    for (int k = 0; k < ncyl; k++) {
+        const Cyl& c = st.cyls[cyl_ids[k]];
+        const v3 rel = p - V(c.bx, c.by, c.bz);
+        if (rel.y < -r || rel.y > c.height + r) continue;
+        if (fabsf(rel.x) >= c.radius + r || fabsf(rel.z) >= c.radius + r) continue;
+        const float dxz = sqrtf(rel.x * rel.x + rel.z * rel.z);
+        const float side = c.radius + r - dxz;
+        const float top = c.height + r - rel.y;
+        if (side <= 0) continue;
+        float depth;
+        v3 n;
+        if (top < side && rel.y > c.height * 0.5f) depth = top, n = V(0, 1, 0);
+        else depth = side, n = dxz > 1e-6f ? V(rel.x / dxz, 0, rel.z / dxz) : V(1, 0, 0);
+        if (depth > out.depth) {
+            out.depth = depth;
+            out.normal = n;
+            out.surface = c.surface;
+            hit = true;
+        }
+    }
+    return hit;
+}
+
+// primitive_collision (static_world.cpp:8-51)
+__device__ v3 primitive_collision(v3 F, v3 vel, float mass, v3 normal, float dt, const GroundModel& gm, float pen, float friction_coef, float push_max,
+                                  float slop, float restitution) {
+    v3 out = V(0, 0, 0);
+    const float Vn = dot(vel, normal);
+    const float Fn = dot(F, normal);
+    const float sgl = gm.soft_depth;
+    if (sgl > 0 && pen >= 0) {
+        out = out + vel * (-gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f));
+        float Fb = gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f;
+        if (Vn >= 0 && Fn < 0 && Fb > -Fn) Fb = -Fn;
+        out = out + normal * Fb;
+    }
+    if (pen >= sgl) {
+        float R = -Fn;
+        const float take = restitution >= 0 ? 1.0f + smin(restitution, 0.95f) : 0.8f;
+        if (Vn < 0) R -= (take * Vn - smin(0.2f * smax(0.0f, pen - sgl - slop) / dt, push_max)) * mass / dt;
+        if (R > 0) {
+            const v3 slipF = F - normal * Fn;
+            v3 slip = vel - normal * Vn;
+            const float sv = length(slip);
+            if (sv > 1e-9f) slip = divs(slip, sv);
+            else slip = V(0, 0, 0);
+            const float G = R * gm.strength * friction_coef;
+            const float stop = mass * sv / dt;
+            if (sv < gm.va && G > 0 && length(slipF) <= gm.ms * G) {
+                out = out + (normal * R - slip * smin(gm.ms * G * (1.0f - bl_expf(-sv / gm.va)), stop) - slipF);
+            } else {
+                const float g = gm.mc + (gm.ms - gm.mc) * bl_expf(-bl_powf(sv / gm.vs, gm.alpha));
+                out = out + (normal * R - slip * smin((g + smin(gm.t2 * sv, 5.0f)) * G, smax(0.0f, stop + dot(slipF, slip))));
+            }
+        }
+    }
+    return out;
+}
+
+// AABB::overlaps (math.h:307-309) of a box's bounds with (mn, mx)
+__device__ __forceinline__ bool box_overlaps(const Box& b, const float* mn, const float* mx) {
+    return b.mnx <= mx[0] && b.mxx >= mn[0] && b.mny <= mx[1] && b.mxy >= mn[1] && b.mnz <= mx[2] && b.mxz >= mn[2];
+}
+
+// ------------------------------------------------------------------------------------------ per frame
+// The frame's start for each awake body: its static candidates (StaticWorld::query over its box grown by its travel,
+// world.cpp:738-753; static_world.cpp:340-362) and the terrain's height bound there. Sleeping bodies are skipped,
+// as build_islands drops their islands (world.cpp:703-713).
+__global__ void k_frame_begin(Body* __restrict__ bodies, int nbodies, Statics st, float frame_time, int world_sleeping, uint32_t* __restrict__ deverr) {
+    const int bi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bi >= nbodies) return;
+    Body& B = bodies[bi];
+    if (!world_sleeping) B.sleeping = 0;
+    if (B.sleeping) return;
+    const float m = smin(B.max_speed, 200.0f) * frame_time * 2.0f + 0.5f;
+    const float mn[3] = {B.aabb_mn[0] - m, B.aabb_mn[1] - m, B.aabb_mn[2] - m};
+    const float mx[3] = {B.aabb_mx[0] + m, B.aabb_mx[1] + m, B.aabb_mx[2] + m};
+    int n = 0;
+    bool over = false;
+    for (int k = 0; k < st.nbig; k++) {
+        const int i = st.big[k];
+        if (box_overlaps(st.boxes[i], mn, mx)) {
+            if (n < kMaxCand) B.box_ids[n] = i;
+            n++;
+        }
+    }
+    if (st.gx > 0) {
+        int x0 = (int)((mn[0] - st.gox) / st.grid_cell), x1 = (int)((mx[0] - st.gox) / st.grid_cell);
+        int z0 = (int)((mn[2] - st.goz) / st.grid_cell), z1 = (int)((mx[2] - st.goz) / st.grid_cell);
+        x0 = max(0, x0), z0 = max(0, z0), x1 = min(st.gx - 1, x1), z1 = min(st.gz - 1, z1);
+        if (mx[0] >= st.gox && mx[2] >= st.goz)
+            for (int z = z0; z <= z1; z++)
+                for (int x = x0; x <= x1; x++)
+                    for (int q = st.cell_ptr[z * st.gx + x]; q < st.cell_ptr[z * st.gx + x + 1]; q++) {
+                        const int i = st.cell_items[q];
+                        if (!box_overlaps(st.boxes[i], mn, mx)) continue;
+                        bool dup = false;
+                        for (int k = 0; k < min(n, kMaxCand); k++)
+                            if (B.box_ids[k] == i) {
+                                dup = true;
+                                break;
+                            }
+                        if (dup) continue;
+                        if (n < kMaxCand) B.box_ids[n] = i;
+                        n++;
+                    }
+    }
+    if (n > kMaxCand) over = true, n = kMaxCand;
+    B.nbox = n;
+    int nc = 0;
+    for (int i = 0; i < st.ncyls; i++) {
+        const Cyl& c = st.cyls[i];
+        if (mx[0] >= c.bx - c.radius && mn[0] <= c.bx + c.radius && mx[2] >= c.bz - c.radius && mn[2] <= c.bz + c.radius && mx[1] >= c.by &&
+            mn[1] <= c.by + c.height) {
+            if (nc < kMaxCand) B.cyl_ids[nc] = i;
+            nc++;
+        }
+    }
+    if (nc > kMaxCand) over = true, nc = kMaxCand;
+    B.ncyl = nc;
+    if (over) atomicOr(deverr, DEVERR_CANDIDATES);
+    B.terrain_max = st.has_terrain ? hf_max_height(st, mn[0], mn[2], mx[0], mx[2]) + 0.0f : -1e30f;
+    B.acc_v2 = 0.0f;
+    B.acc_contacts = 0;
+}
+
+// ------------------------------------------------------------------------------------------ per substep
+// SoftBody::compute_beam_forces, one beam (softbody.cpp:412-470). fv.w = 1 when the beam pushes on its nodes this
+// substep. Thread j < nbodies also resets body j's bounds accumulator for this substep's k_nodes.
+__global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
+                                               uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
+                                               const int* __restrict__ bbody, float4* __restrict__ fv, const float4* __restrict__ nd,
+                                               Body* __restrict__ bodies, int nbeams, int nbodies) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < nbodies) {
+        Body& B = bodies[j];
+        B.acc_mn[0] = B.acc_mn[1] = B.acc_mn[2] = 1e30f;
+        B.acc_mx[0] = B.acc_mx[1] = B.acc_mx[2] = -1e30f;
+    }
+    if (j >= nbeams) return;
+    uint32_t meta = bmeta[j];
+    if (meta & kBeamAsleep) return;
+    float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const uint32_t type = meta & 0xffu;
+    uint32_t flags = (meta >> 8) & 0xffu;
+    if (!(flags & (BF_BROKEN | BF_SHOCK))) {
+        const int2 e = ab[j];
+        const float4 pa = nd[2 * e.x], va = nd[2 * e.x + 1], pb = nd[2 * e.y], vb = nd[2 * e.y + 1];
+        const v3 dis = V(pa.x - pb.x, pa.y - pb.y, pa.z - pb.z);
+        const float len2 = dot(dis, dis);
+        if (len2 >= 1e-12f) {
+            float4 s = bst[j]; // L, max_pos, max_neg, strength
+            const float2 c = kd[j];
+            const float inv_len = 1.0f / sqrtf(len2);
+            const float len = len2 * inv_len;
+            const float diff = len - s.x;
+            const v3 dv = V(va.x - vb.x, va.y - vb.y, va.z - vb.z);
+            float k = c.x, d = c.y;
+            const bool brk = (meta & BB_BREAK) != 0;
+            bool broke = false, changed = false;
+            if (type == BT_ROPE) {
+                if (diff < 0) k = 0, d *= 0.1f;
+            } else if (type == BT_SUPPORT) {
+                if (diff > 0) {
+                    k = 0;
+                    d *= 0.1f;
+                    if (brk && diff > s.x * bcold[j].z) broke = true;
+                }
+            }
+            if (!broke) {
+                float slen = -k * diff - d * dot(dv, dis) * inv_len;
+                if ((meta & BB_DEFORM) && !(flags & BF_NO_DEFORM) && k != 0) {
+                    if (slen > s.y && diff < 0) {
+                        const float4 cold = bcold[j]; // plastic, L0, support_limit
+                        const float yield_len = s.y / k;
+                        const float def = diff + yield_len * (1.0f - cold.x);
+                        const float Lold = s.x;
+                        s.x = smax(smin(0.1f, 0.3f * cold.y), s.x + def);
+                        slen = slen - (slen - s.y) * 0.5f;
+                        if (s.x < Lold) s.y *= Lold / s.x;
+                        changed = true;
+                    } else if (slen < s.z && diff > 0) {
+                        const float4 cold = bcold[j];
+                        const float yield_len = s.z / k;
+                        const float def = diff + yield_len * (1.0f - cold.x);
+                        const float Lold = s.x;
+                        s.x = s.x + def;
+                        slen = slen - (slen - s.z) * 0.5f;
+                        if (Lold > 0 && s.x > Lold) s.z *= s.x / Lold;
+                        if (!(meta & BB_DUCTILE)) s.w -= def * k;
+                        changed = true;
+                    }
+                }
+                if (changed) bst[j] = s;
+                if (brk && fabsf(slen) > s.w && !(flags & BF_NO_BREAK)) {
+                    broke = true;
+                } else {
+                    stress[j] = slen;
+                    const float sc = slen * inv_len;
+                    out = make_float4(dis.x * sc, dis.y * sc, dis.z * sc, 1.0f);
+                }
+            }
+            if (broke) {
+                flags |= BF_BROKEN;
+                bmeta[j] = (meta & ~(0xffu << 8)) | (flags << 8);
+                atomicAdd(&bodies[bbody[j]].broken_beams, 1);
+            }
+        }
+    }
+    fv[j] = out;
+}
+
+// Gravity + the node's beams in beam order, World::collide_static for the node (world.cpp:781-870), then
+// SoftBody::integrate_nodes (softbody.cpp:769-795). first: the frame's first substep (the top speed starts from the
+// velocities before it, world.cpp:3217-3222).
+__global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const int4* __restrict__ info,
+                                               const int* __restrict__ inc_ptr, const int* __restrict__ inc, const float4* __restrict__ fv,
+                                               Body* __restrict__ bodies, Statics st, float gx, float gy, float gz, float dt, int nnodes, int first) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int body = -1;
+    v3 p = V(0, 0, 0);
+    float v2 = 0.0f, v2start = 0.0f;
+    int contact = 0;
+    bool live = false;
+    if (i < nnodes) {
+        const int4 inf = info[i];
+        body = inf.w;
+        const Body& B = bodies[body];
+        if (!B.sleeping) {
+            live = true;
+            const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
+            if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
+            const float m = Vv.w;
+            v3 f = V(gx * m, gy * m, gz * m); // clear_forces: g * mass (softbody.cpp:376)
+            const int q1 = inc_ptr[i + 1];
+            for (int q = inc_ptr[i]; q < q1; q++) {
+                const int e = inc[q];
+                const float4 b = fv[e & 0x7fffffff];
+                if (b.w != 0.0f) {
+                    if (e < 0) f = V(f.x - b.x, f.y - b.y, f.z - b.z);
+                    else f = V(f.x + b.x, f.y + b.y, f.z + b.z);
+                }
+            }
+            v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
+            float inv_mass = P.w;
+            const uint32_t flags = (uint32_t)inf.x;
+            // ---- static contact (World::collide_static)
+            if ((flags & NF_GROUND) && inv_mass > 0) {
+                if (pos.y < st.kill_y) {
+                    vel = V(0, 0, 0);
+                    inv_mass = 0;
+                } else {
+                    const float r = __int_as_float(inf.z);
+                    const bool near_terrain = st.has_terrain && pos.y - r <= B.terrain_max + 0.05f;
+                    const int nbox = B.nbox, ncyl = B.ncyl;
+                    if (near_terrain || nbox != 0 || ncyl != 0) {
+                        int bids[16], cids[16];
+                        const int* bp = B.box_ids;
+                        const int* cp = B.cyl_ids;
+                        int nb = nbox, nc = ncyl;
+                        bool go = true;
+                        if (nbox <= 16 && ncyl <= 16) {
+                            nb = nc = 0;
+                            const float rr = r + 0.01f;
+                            for (int k = 0; k < nbox; k++) {
+                                const Box& a = st.boxes[B.box_ids[k]];
+                                if (pos.x >= a.mnx - rr && pos.x <= a.mxx + rr && pos.y >= a.mny - rr && pos.y <= a.mxy + rr && pos.z >= a.mnz - rr &&
+                                    pos.z <= a.mxz + rr)
+                                    bids[nb++] = B.box_ids[k];
+                            }
+                            for (int k = 0; k < ncyl; k++) {
+                                const Cyl& cy = st.cyls[B.cyl_ids[k]];
+                                const float cr = cy.radius + rr;
+                                if (fabsf(pos.x - cy.bx) <= cr && fabsf(pos.z - cy.bz) <= cr && pos.y >= cy.by - rr && pos.y <= cy.by + cy.height + rr)
+                                    cids[nc++] = B.cyl_ids[k];
+                            }
+                            bp = bids;
+                            cp = cids;
+                            go = near_terrain || nb != 0 || nc != 0;
+                        }
+                        Contact c;
+                        if (go && collide_point(st, pos, r, bp, nb, cp, nc, near_terrain, c)) {
+                            contact = 1;
+                            const GroundModel& gm = c_ground[c.surface < kSurfCount ? c.surface : 0];
+                            const float fc = __int_as_float(inf.y) * B.fric;
+                            if (c.max_force > 0) {
+                                v3 fcn = primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, -1.0f);
+                                const float fl = length(fcn);
+                                if (fl > c.max_force) fcn = fcn * (c.max_force / fl);
+                                f = f + fcn;
+                            } else {
+                                f = f + primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, B.bounce);
+                            }
+                        }
+                    }
+                }
+            }
+            // ---- integration (SoftBody::integrate_nodes)
+            if (inv_mass > 0) {
+                vel = vel + f * (inv_mass * dt);
+                v2 = dot(vel, vel);
+                if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
+                    vel = vel * (kMaxNodeSpeed / sqrtf(v2));
+                    v2 = kMaxNodeSpeed * kMaxNodeSpeed;
+                } else if (!(v2 >= 0.0f)) {
+                    vel = V(0, 0, 0);
+                    v2 = 0;
+                }
+                pos = pos + vel * dt;
+            }
+            nd[2 * i] = make_float4(pos.x, pos.y, pos.z, inv_mass);
+            nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, m);
+            p = pos;
+            v2 = smax(v2, v2start);
+        }
+    }
+    // ---- per body: bounds, top speed, contacts (a warp of one body reduces first)
+    const int b0 = __shfl_sync(0xffffffffu, body, 0);
+    const bool uniform = __all_sync(0xffffffffu, body == b0 && live);
+    if (uniform) {
+        float mnx = p.x, mny = p.y, mnz = p.z, mxx = p.x, mxy = p.y, mxz = p.z, vv = v2;
+        int cc = contact;
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+            mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+            mnz = fminf(mnz, __shfl_xor_sync(0xffffffffu, mnz, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+            mxz = fmaxf(mxz, __shfl_xor_sync(0xffffffffu, mxz, o));
+            vv = fmaxf(vv, __shfl_xor_sync(0xffffffffu, vv, o));
+            cc += __shfl_xor_sync(0xffffffffu, cc, o);
+        }
+        if (lane == 0) {
+            Body& B = bodies[b0];
+            atomic_min_f(&B.acc_mn[0], mnx), atomic_min_f(&B.acc_mn[1], mny), atomic_min_f(&B.acc_mn[2], mnz);
+            atomic_max_f(&B.acc_mx[0], mxx), atomic_max_f(&B.acc_mx[1], mxy), atomic_max_f(&B.acc_mx[2], mxz);
+            atomic_max_f(&B.acc_v2, vv);
+            if (cc) atomicAdd(&B.acc_contacts, cc);
+        }
+    } else if (live) {
+        Body& B = bodies[body];
+        atomic_min_f(&B.acc_mn[0], p.x), atomic_min_f(&B.acc_mn[1], p.y), atomic_min_f(&B.acc_mn[2], p.z);
+        atomic_max_f(&B.acc_mx[0], p.x), atomic_max_f(&B.acc_mx[1], p.y), atomic_max_f(&B.acc_mx[2], p.z);
+        atomic_max_f(&B.acc_v2, v2);
+        if (contact) atomicAdd(&B.acc_contacts, contact);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ end of frame
+// Block-wide bitonic sort of v[0, P) ascending (P a power of two), in place in global memory.
+__device__ void block_bitonic_sort(float* v, int P) {
+    for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const float a = v[i], b = v[l];
+                    const bool up = (i & k) == 0;
+                    if (up ? (b < a) : (a < b)) v[i] = b, v[l] = a;
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__device__ __forceinline__ bool finite3(float x, float y, float z) { return isfinite(x) && isfinite(y) && isfinite(z); }
+
+// Scratch of k_frame_finish, sized for the largest body (P = its node count rounded up to a power of two).
+struct RepairScratch {
+    float* sort;      // 3 * P
+    int* bad;         // P
+    float4* np;       // P: new positions of the pass
+    float4* nv;       // P: new velocities of the pass
+    int P;
+};
+
+// World::repair_nodes (world.cpp:4022-4111) of one body by the whole block. Returns the nodes reset, -1 when the body
+// cannot be repaired (nothing finite, or most of it bad).
+__device__ int repair_body(Body& B, float4* __restrict__ nd, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
+                           const int2* __restrict__ ab, const uint32_t* __restrict__ bmeta, RepairScratch rs) {
+    __shared__ int s_cnt, s_nbad;
+    __shared__ float s_med[3];
+    const int n = B.nnodes, n0 = B.node0, P = rs.P;
+    // the median of the finite positions, per axis (std::nth_element's element: the sorted one at m / 2)
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        float x = INFINITY, y = INFINITY, z = INFINITY;
+        if (i < n) {
+            const float4 p = nd[2 * (n0 + i)];
+            if (finite3(p.x, p.y, p.z)) x = p.x, y = p.y, z = p.z, atomicAdd(&s_cnt, 1);
+        }
+        rs.sort[i] = x, rs.sort[P + i] = y, rs.sort[2 * P + i] = z;
+    }
+    __syncthreads();
+    const int m = s_cnt;
+    if (m == 0) return -1;
+    for (int a = 0; a < 3; a++) block_bitonic_sort(rs.sort + a * P, P);
+    if (threadIdx.x == 0) s_med[0] = rs.sort[m / 2], s_med[1] = rs.sort[P + m / 2], s_med[2] = rs.sort[2 * P + m / 2], s_nbad = 0;
+    __syncthreads();
+    const v3 med = V(s_med[0], s_med[1], s_med[2]);
+    const float lim = 0.9f * kMaxNodeSpeed;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 p = nd[2 * (n0 + i)], v = nd[2 * (n0 + i) + 1];
+        const bool fin = finite3(p.x, p.y, p.z) && finite3(v.x, v.y, v.z);
+        const v3 vv = V(v.x, v.y, v.z);
+        const bool b = !fin || dot(vv, vv) > lim * lim || length(V(p.x, p.y, p.z) - med) > 300.0f;
+        rs.bad[i] = b;
+        if (b) atomicAdd(&s_nbad, 1);
+    }
+    __syncthreads();
+    const int nbad0 = s_nbad;
+    if (nbad0 == 0) return 0;
+    if (nbad0 * 2 > n) return -1;
+    // up to 8 passes: each bad node takes the mean of its good neighbours over unbroken beams, in beam order
+    for (int pass = 0; pass < 8; pass++) {
+        __syncthreads();
+        if (s_nbad == 0) break;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            rs.nv[i].w = 0.0f;
+            if (!rs.bad[i]) continue;
+            v3 sp = V(0, 0, 0), sv = V(0, 0, 0);
+            int cnt = 0;
+            for (int q = inc_ptr[n0 + i]; q < inc_ptr[n0 + i + 1]; q++) {
+                const int j = inc[q] & 0x7fffffff;
+                if ((bmeta[j] >> 8) & BF_BROKEN) continue;
+                const int2 e = ab[j];
+                const int y = (e.x == n0 + i ? e.y : e.x) - n0;
+                if (rs.bad[y]) continue;
+                const float4 py = nd[2 * (n0 + y)], vy = nd[2 * (n0 + y) + 1];
+                sp = sp + V(py.x, py.y, py.z);
+                sv = sv + V(vy.x, vy.y, vy.z);
+                cnt++;
+            }
+            if (cnt > 0) {
+                const v3 np = divs(sp, (float)cnt), nv = divs(sv, (float)cnt);
+                rs.np[i] = make_float4(np.x, np.y, np.z, 0.0f);
+                rs.nv[i] = make_float4(nv.x, nv.y, nv.z, 1.0f);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            if (rs.nv[i].w != 0.0f) {
+                const float4 p = nd[2 * (n0 + i)], v = nd[2 * (n0 + i) + 1];
+                nd[2 * (n0 + i)] = make_float4(rs.np[i].x, rs.np[i].y, rs.np[i].z, p.w);
+                nd[2 * (n0 + i) + 1] = make_float4(rs.nv[i].x, rs.nv[i].y, rs.nv[i].z, v.w);
+                rs.bad[i] = 0;
+                atomicSub(&s_nbad, 1);
+            }
+        __syncthreads();
+    }
+    // isolated leftovers: at the median, at rest; then the bounds and the top speed afresh
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (rs.bad[i]) {
+            const float4 p = nd[2 * (n0 + i)], v = nd[2 * (n0 + i) + 1];
+            nd[2 * (n0 + i)] = make_float4(med.x, med.y, med.z, p.w);
+            nd[2 * (n0 + i) + 1] = make_float4(0.0f, 0.0f, 0.0f, v.w);
+        }
+    return nbad0;
+}
+
+// Block-wide bounds and top speed of a body (SoftBody::compute_aabb, softbody.cpp:271-275; max of |v|)
+__device__ void body_bounds(Body& B, const float4* __restrict__ nd) {
+    __shared__ float s_mn[3], s_mx[3], s_v;
+    if (threadIdx.x == 0) s_mn[0] = s_mn[1] = s_mn[2] = 1e30f, s_mx[0] = s_mx[1] = s_mx[2] = -1e30f, s_v = 0.0f;
+    __syncthreads();
+    for (int i = threadIdx.x; i < B.nnodes; i += blockDim.x) {
+        const float4 p = nd[2 * (B.node0 + i)], v = nd[2 * (B.node0 + i) + 1];
+        atomic_min_f(&s_mn[0], p.x), atomic_min_f(&s_mn[1], p.y), atomic_min_f(&s_mn[2], p.z);
+        atomic_max_f(&s_mx[0], p.x), atomic_max_f(&s_mx[1], p.y), atomic_max_f(&s_mx[2], p.z);
+        atomic_max_f(&s_v, length(V(v.x, v.y, v.z)));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 3; c++) B.aabb_mn[c] = s_mn[c], B.aabb_mx[c] = s_mx[c];
+        B.max_speed = s_v;
+    }
+    __syncthreads();
+}
+
+// The end of the frame, one block for all bodies: each stepped body's bounds (the last substep's), top speed and
+// static contacts; the repair of the bodies in numerical trouble (world.cpp:3961-3980); World::update_sleep
+// (world.cpp:4113-4157; no sheets, no rest damping).
+__global__ void __launch_bounds__(1024) k_frame_finish(Body* __restrict__ bodies, int nbodies, float4* __restrict__ nd,
+                                                       const int* __restrict__ inc_ptr, const int* __restrict__ inc, const int2* __restrict__ ab,
+                                                       const uint32_t* __restrict__ bmeta, RepairScratch rs, float frame_time, int world_sleeping,
+                                                       float world_sleep_speed, float sleep_time, uint32_t* __restrict__ deverr) {
+    __shared__ int s_any;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    for (int bi = threadIdx.x; bi < nbodies; bi += blockDim.x) {
+        Body& B = bodies[bi];
+        B.needs_repair = 0;
+        if (B.sleeping) continue;
+        for (int c = 0; c < 3; c++) B.aabb_mn[c] = B.acc_mn[c], B.aabb_mx[c] = B.acc_mx[c];
+        B.max_speed = sqrtf(B.acc_v2);
+        B.static_contacts = B.acc_contacts;
+        const float ex = B.aabb_mx[0] - B.aabb_mn[0], ey = B.aabb_mx[1] - B.aabb_mn[1], ez = B.aabb_mx[2] - B.aabb_mn[2];
+        if (!isfinite(B.aabb_mn[0]) || !isfinite(B.aabb_mx[1]) || smax(ex, smax(ey, ez)) > 800.0f || B.max_speed > kMaxNodeSpeed * 0.9f) {
+            B.needs_repair = 1;
+            s_any = 1;
+        }
+    }
+    __syncthreads();
+    if (s_any) {
+        if (threadIdx.x == 0) atomicOr(deverr, DEVERR_NONFINITE);
+        for (int bi = 0; bi < nbodies; bi++) {
+            Body& B = bodies[bi];
+            if (!B.needs_repair) continue;
+            const int fixed = repair_body(B, nd, inc_ptr, inc, ab, bmeta, rs);
+            __syncthreads();
+            if (fixed < 0) {
+                // exploded: frozen where it is (non-finite nodes far below), asleep (world.cpp:3968-3977)
+                for (int i = threadIdx.x; i < B.nnodes; i += blockDim.x) {
+                    const float4 p = nd[2 * (B.node0 + i)], v = nd[2 * (B.node0 + i) + 1];
+                    const bool fin = finite3(p.x, p.y, p.z);
+                    nd[2 * (B.node0 + i)] = make_float4(fin ? p.x : 0.0f, fin ? p.y : -1000.0f, fin ? p.z : 0.0f, 0.0f);
+                    nd[2 * (B.node0 + i) + 1] = make_float4(0.0f, 0.0f, 0.0f, v.w);
+                }
+                const float keep = B.max_speed; // (the frame's top speed stays; the bounds are made afresh)
+                __syncthreads();
+                body_bounds(B, nd);
+                if (threadIdx.x == 0) B.max_speed = keep, B.sleeping = 1, B.fell_asleep = 1, B.needs_repair = 2;
+            } else if (fixed > 0) {
+                __syncthreads();
+                body_bounds(B, nd);
+                if (threadIdx.x == 0) B.repaired += fixed;
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    for (int bi = threadIdx.x; bi < nbodies; bi += blockDim.x) {
+        Body& B = bodies[bi];
+        if (B.sleeping) continue; // (asleep before this frame, or frozen just now)
+        if (!world_sleeping || !B.can_sleep) {
+            B.sleep_timer = 0;
+            continue;
+        }
+        const float rest = smax(world_sleep_speed, B.sleep_speed);
+        if (B.max_speed < rest) {
+            B.sleep_timer += frame_time;
+            if (B.sleep_timer > sleep_time) B.sleeping = 1, B.fell_asleep = 1;
+        } else {
+            B.sleep_timer = 0;
+        }
+    }
+}
+
+// SoftBody::fall_asleep (softbody.h:773-779) for the bodies that just fell asleep: velocities zero; their beams are
+// parked (not stepped while the body sleeps)
+__global__ void k_sleep_apply(Body* __restrict__ bodies, float4* __restrict__ nd, uint32_t* __restrict__ bmeta) {
+    Body& B = bodies[blockIdx.x];
+    if (!B.fell_asleep) return;
+    for (int i = threadIdx.x; i < B.nnodes; i += blockDim.x) {
+        const float4 v = nd[2 * (B.node0 + i) + 1];
+        nd[2 * (B.node0 + i) + 1] = make_float4(0.0f, 0.0f, 0.0f, v.w);
+    }
+    for (int j = threadIdx.x; j < B.nbeams; j += blockDim.x) bmeta[B.beam0 + j] |= kBeamAsleep;
+    __syncthreads();
+    if (threadIdx.x == 0) B.fell_asleep = 0;
+}
+
+} // namespace blg

@@ -1,0 +1,755 @@
+// Host side of the B200 soft-body substep: the context behind include/beamlab_gpu.h.
+//
+// The context keeps a host description of the statics and of the bodies added, and, once committed, the device
+// arrays every kernel reads - all bodies back to back, structure of arrays:
+//   nodes   nd  2 x float4 a node: (p.xyz, inv_mass), (v.xyz, mass) - the byte layout of the reference's Node and of
+//           bl_node, so whole-state transfers are plain copies      info int4 (flags, friction, radius, body)
+//           inc_ptr / inc: each node's incident beams in beam order (beam index, bit 31: the node is the beam's b end)
+//   beams   ab int2 (a, b)   kd float2 (k, d)   bst float4 (L, max_pos, max_neg, strength)   bmeta u32 (type, flags,
+//           the body's deform/break/ductile bits, asleep)   bcold float4 (plastic, L0, support_limit)   stress f32
+//           bbody i32   fv float4: the substep's beam force (scratch between k_beams and k_nodes)
+//   bodies  Body records (bl_device.cuh)
+// A frame (bl_gpu_step_substeps) is captured once per substep count as a CUDA graph and replayed.
+#include "../../include/beamlab_gpu.h"
+#include "bl_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+using namespace blg;
+
+namespace {
+
+struct HostBody {
+    std::vector<bl_node> nodes;
+    std::vector<bl_node_info> info;
+    std::vector<bl_beam> beams;
+    uint32_t beam_bits = 0; // the body's allow_deform / allow_break / ductile as BB_* bits of its beams' meta words
+    Body rec;
+};
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void free_() {
+        if (p) cudaFree(p);
+        p = nullptr, n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        free_();
+        n = count;
+        return cudaMalloc((void**)&p, sizeof(T) * std::max<size_t>(count, 1));
+    }
+};
+
+} // namespace
+
+struct bl_gpu_ctx {
+    bl_gpu_config cfg{};
+    cudaStream_t stream = nullptr;
+    int last_cuda = 0;
+    // host description
+    std::vector<HostBody> bodies;
+    bool bodies_dirty = false; // bodies added since the last commit
+    bool committed = false;
+    // statics (host)
+    int has_terrain = 0, hnx = 0, hnz = 0, hbx = 0, hbz = 0;
+    float cell = 1, ox = 0, oz = 0, kill_y = -200.0f;
+    std::vector<float> heights, block_max;
+    std::vector<uint8_t> surfaces;
+    std::vector<Box> boxes;
+    std::vector<Cyl> cyls;
+    int gx = 0, gz = 0;
+    float gox = 0, goz = 0, grid_cell = 16.0f;
+    std::vector<int> cell_ptr, cell_items, big;
+    bool statics_dirty = true;
+    // device
+    DevBuf<float4> nd, bst, bcold, fv;
+    DevBuf<int4> info;
+    DevBuf<int> inc_ptr, inc, bbody;
+    DevBuf<int2> ab;
+    DevBuf<float2> kd;
+    DevBuf<uint32_t> bmeta;
+    DevBuf<float> stress;
+    DevBuf<Body> dbodies;
+    DevBuf<float> d_heights, d_block_max;
+    DevBuf<uint8_t> d_surf;
+    DevBuf<Box> d_boxes;
+    DevBuf<Cyl> d_cyls;
+    DevBuf<int> d_cell_ptr, d_cell_items, d_big;
+    DevBuf<uint32_t> deverr;
+    DevBuf<float> rs_sort;
+    DevBuf<int> rs_bad;
+    DevBuf<float4> rs_np, rs_nv;
+    int rs_P = 1;
+    int N = 0, M = 0, B = 0;
+    Statics st{};
+    // frames captured as graphs, by substep count
+    std::map<int, cudaGraphExec_t> graphs;
+    struct ProfGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<cudaEvent_t> events;
+    };
+    std::map<int, ProfGraph> pgraphs; // frames with a timing event between kernels (bl_gpu_profile_frame)
+    int64_t launches = 0, total_substeps = 0;
+    int last_substeps = 0;
+};
+
+#define BL_CUDA(ctx, call)                                                                                                                   \
+    do {                                                                                                                                     \
+        cudaError_t e_ = (call);                                                                                                             \
+        if (e_ != cudaSuccess) {                                                                                                             \
+            (ctx)->last_cuda = (int)e_;                                                                                                      \
+            return e_ == cudaErrorMemoryAllocation ? BL_GPU_ENOMEM : BL_GPU_ECUDA;                                                           \
+        }                                                                                                                                    \
+    } while (0)
+
+using ProfGraph = bl_gpu_ctx::ProfGraph;
+
+static void drop_graphs(bl_gpu_ctx* c) {
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+    for (auto& kv : c->pgraphs) {
+        cudaGraphExecDestroy(kv.second.exec);
+        for (cudaEvent_t e : kv.second.events) cudaEventDestroy(e);
+    }
+    c->pgraphs.clear();
+}
+
+static void free_device(bl_gpu_ctx* c) {
+    c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->fv.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
+    c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
+    c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
+}
+
+static void free_statics(bl_gpu_ctx* c) {
+    c->d_heights.free_(), c->d_block_max.free_(), c->d_surf.free_(), c->d_boxes.free_(), c->d_cyls.free_();
+    c->d_cell_ptr.free_(), c->d_cell_items.free_(), c->d_big.free_();
+}
+
+// Ground models (static_world.cpp:85-114): va, ms, mc, t2, vs, alpha, strength, soft_depth, fluid_drag, fluid_density
+static const GroundModel kGroundModels[kSurfCount] = {
+    {3, 0.80f, 0.55f, 0.005f, 7, 2, 1, 0, 0, 0},          {3, 0.80f, 0.58f, 0.006f, 4, 2, 1, 0, 0, 0},
+    {3, 1.20f, 0.75f, 0.010f, 6, 2, 1, 0, 0, 0},          {3, 1.20f, 0.75f, 0.010f, 6, 2, 1, 0, 0, 0},
+    {3, 0.85f, 0.60f, 0.006f, 3, 2, 1, 0, 0, 0},          {2, 0.50f, 0.35f, 0.004f, 3, 2, 1, 0.12f, 60, 1500},
+    {3, 0.70f, 0.55f, 0.0001f, 9, 2, 1, 0.03f, 20, 1600}, {3, 0.95f, 0.70f, 0.007f, 8, 2, 1, 0, 0, 0},
+    {3, 0.90f, 0.60f, 0.005f, 5, 2, 1, 0, 0, 0},          {3, 0.70f, 0.40f, 0.001f, 3, 2, 1, 0, 0, 0},
+    {1, 0.30f, 0.20f, 0.0001f, 3, 2, 1, 0, 0, 0},
+};
+
+// ------------------------------------------------------------------------------------------ statics (host)
+// StaticWorld::build_grid (static_world.cpp:308-338): 16 m cells over the bounds of the boxes and cylinders; a box
+// over more than 64 cells goes to the big list; each cell lists its boxes in box order
+static void build_grid_host(bl_gpu_ctx* c) {
+    c->cell_ptr.clear(), c->cell_items.clear(), c->big.clear();
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    auto add = [&](float x, float y, float z) {
+        const float p[3] = {x, y, z};
+        for (int k = 0; k < 3; k++) mn[k] = (p[k] < mn[k]) ? p[k] : mn[k], mx[k] = (mx[k] < p[k]) ? p[k] : mx[k];
+    };
+    for (const Box& b : c->boxes) add(b.mnx, b.mny, b.mnz), add(b.mxx, b.mxy, b.mxz);
+    for (const Cyl& y : c->cyls) add(y.bx - y.radius, y.by - 0.0f, y.bz - y.radius), add(y.bx + y.radius, y.by + y.height, y.bz + y.radius);
+    if (!(mn[0] <= mx[0])) {
+        c->gx = c->gz = 0;
+        return;
+    }
+    c->gox = mn[0], c->goz = mn[2];
+    c->gx = std::max(1, (int)std::ceil((mx[0] - mn[0]) / c->grid_cell) + 1);
+    c->gz = std::max(1, (int)std::ceil((mx[2] - mn[2]) / c->grid_cell) + 1);
+    std::vector<std::vector<int>> cells((size_t)c->gx * c->gz);
+    for (int i = 0; i < (int)c->boxes.size(); i++) {
+        const Box& a = c->boxes[i];
+        const int x0 = (int)((a.mnx - c->gox) / c->grid_cell), x1 = (int)((a.mxx - c->gox) / c->grid_cell);
+        const int z0 = (int)((a.mnz - c->goz) / c->grid_cell), z1 = (int)((a.mxz - c->goz) / c->grid_cell);
+        if ((x1 - x0 + 1) * (z1 - z0 + 1) > 64) {
+            c->big.push_back(i);
+            continue;
+        }
+        for (int z = z0; z <= z1; z++)
+            for (int x = x0; x <= x1; x++) cells[(size_t)z * c->gx + x].push_back(i);
+    }
+    c->cell_ptr.assign(cells.size() + 1, 0);
+    for (size_t k = 0; k < cells.size(); k++) {
+        c->cell_ptr[k + 1] = c->cell_ptr[k] + (int)cells[k].size();
+        c->cell_items.insert(c->cell_items.end(), cells[k].begin(), cells[k].end());
+    }
+}
+
+template <class T>
+static int upload_vec(bl_gpu_ctx* c, DevBuf<T>& d, const std::vector<T>& h) {
+    BL_CUDA(c, d.alloc(h.size()));
+    if (!h.empty()) BL_CUDA(c, cudaMemcpyAsync(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    return BL_GPU_OK;
+}
+
+static int commit_statics(bl_gpu_ctx* c) {
+    free_statics(c);
+    int rc;
+    if ((rc = upload_vec(c, c->d_heights, c->heights)) || (rc = upload_vec(c, c->d_block_max, c->block_max)) || (rc = upload_vec(c, c->d_surf, c->surfaces)) ||
+        (rc = upload_vec(c, c->d_boxes, c->boxes)) || (rc = upload_vec(c, c->d_cyls, c->cyls)) || (rc = upload_vec(c, c->d_cell_ptr, c->cell_ptr)) ||
+        (rc = upload_vec(c, c->d_cell_items, c->cell_items)) || (rc = upload_vec(c, c->d_big, c->big)))
+        return rc;
+    Statics& s = c->st;
+    s.has_terrain = c->has_terrain, s.hnx = c->hnx, s.hnz = c->hnz, s.bx = c->hbx, s.bz = c->hbz;
+    s.cell = c->cell, s.ox = c->ox, s.oz = c->oz;
+    s.h = c->d_heights.p, s.surf = c->d_surf.p, s.block_max = c->d_block_max.p;
+    s.kill_y = c->kill_y;
+    s.nboxes = (int)c->boxes.size(), s.ncyls = (int)c->cyls.size();
+    s.boxes = c->d_boxes.p, s.cyls = c->d_cyls.p;
+    s.gx = c->gx, s.gz = c->gz, s.nbig = (int)c->big.size();
+    s.gox = c->gox, s.goz = c->goz, s.grid_cell = c->grid_cell;
+    s.cell_ptr = c->d_cell_ptr.p, s.cell_items = c->d_cell_items.p, s.big = c->d_big.p;
+    c->statics_dirty = false;
+    drop_graphs(c);
+    return BL_GPU_OK;
+}
+
+// ------------------------------------------------------------------------------------------ bodies
+// Brings the device's current state of the committed bodies back into the host description (before a re-commit).
+static int pull_state(bl_gpu_ctx* c) {
+    if (!c->committed) return BL_GPU_OK;
+    std::vector<bl_node> nodes(c->N);
+    std::vector<float4> bst(c->M);
+    std::vector<uint32_t> meta(c->M);
+    std::vector<float> stress(c->M);
+    std::vector<Body> recs(c->B);
+    BL_CUDA(c, cudaMemcpyAsync(nodes.data(), c->nd.p, sizeof(bl_node) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    BL_CUDA(c, cudaMemcpyAsync(bst.data(), c->bst.p, sizeof(float4) * c->M, cudaMemcpyDeviceToHost, c->stream));
+    BL_CUDA(c, cudaMemcpyAsync(meta.data(), c->bmeta.p, sizeof(uint32_t) * c->M, cudaMemcpyDeviceToHost, c->stream));
+    BL_CUDA(c, cudaMemcpyAsync(stress.data(), c->stress.p, sizeof(float) * c->M, cudaMemcpyDeviceToHost, c->stream));
+    BL_CUDA(c, cudaMemcpyAsync(recs.data(), c->dbodies.p, sizeof(Body) * c->B, cudaMemcpyDeviceToHost, c->stream));
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int bi = 0; bi < c->B; bi++) {
+        HostBody& hb = c->bodies[bi];
+        const Body& r = recs[bi];
+        for (int i = 0; i < r.nnodes; i++) hb.nodes[i] = nodes[r.node0 + i];
+        for (int j = 0; j < r.nbeams; j++) {
+            bl_beam& b = hb.beams[j];
+            const float4 s = bst[r.beam0 + j];
+            b.L = s.x, b.max_pos = s.y, b.max_neg = s.z, b.strength = s.w;
+            b.flags = (uint8_t)((meta[r.beam0 + j] >> 8) & 0xff);
+            b.stress = stress[r.beam0 + j];
+        }
+        hb.rec = r;
+    }
+    return BL_GPU_OK;
+}
+
+// Lays every body out back to back on the device and builds each node's incident-beam list.
+static int commit_bodies(bl_gpu_ctx* c) {
+    int rc = pull_state(c);
+    if (rc) return rc;
+    int N = 0, M = 0, maxn = 1;
+    for (HostBody& hb : c->bodies) {
+        hb.rec.node0 = N, hb.rec.nnodes = (int)hb.nodes.size(), hb.rec.beam0 = M, hb.rec.nbeams = (int)hb.beams.size();
+        N += hb.rec.nnodes, M += hb.rec.nbeams, maxn = std::max(maxn, hb.rec.nnodes);
+    }
+    const int B = (int)c->bodies.size();
+    std::vector<bl_node> nodes(N);
+    std::vector<float4> bst(M), bcold(M);
+    std::vector<int4> info(N);
+    std::vector<int2> ab(M);
+    std::vector<float2> kd(M);
+    std::vector<uint32_t> meta(M);
+    std::vector<float> stress(M);
+    std::vector<int> bbody(M), inc_ptr(N + 1, 0), inc(2 * (size_t)M);
+    std::vector<Body> recs(B);
+    for (int bi = 0; bi < B; bi++) {
+        const HostBody& hb = c->bodies[bi];
+        const Body& r = hb.rec;
+        recs[bi] = r;
+        for (int i = 0; i < r.nnodes; i++) {
+            const bl_node& n = hb.nodes[i];
+            const bl_node_info& f = hb.info[i];
+            nodes[r.node0 + i] = n;
+            int fr, ra;
+            std::memcpy(&fr, &f.friction, 4), std::memcpy(&ra, &f.radius, 4);
+            info[r.node0 + i] = make_int4((int)f.flags, fr, ra, bi);
+        }
+        for (int j = 0; j < r.nbeams; j++) {
+            const bl_beam& b = hb.beams[j];
+            const int g = r.beam0 + j;
+            ab[g] = make_int2(r.node0 + (int)b.a, r.node0 + (int)b.b);
+            kd[g] = make_float2(b.k, b.d);
+            bst[g] = make_float4(b.L, b.max_pos, b.max_neg, b.strength);
+            bcold[g] = make_float4(b.plastic, b.L0, b.support_limit, 0.0f);
+            stress[g] = b.stress;
+            bbody[g] = bi;
+            inc_ptr[ab[g].x + 1]++, inc_ptr[ab[g].y + 1]++;
+        }
+    }
+    // each beam's meta word: type, flags, the body's deform/break/ductile bits, asleep
+    for (int bi = 0; bi < B; bi++) {
+        const HostBody& hb = c->bodies[bi];
+        const Body& r = hb.rec;
+        const uint32_t bits = hb.beam_bits;
+        for (int j = 0; j < r.nbeams; j++) {
+            const bl_beam& b = hb.beams[j];
+            meta[r.beam0 + j] = (uint32_t)b.type | ((uint32_t)b.flags << 8) | bits | (r.sleeping ? kBeamAsleep : 0u);
+        }
+    }
+    for (int i = 0; i < N; i++) inc_ptr[i + 1] += inc_ptr[i];
+    {
+        std::vector<int> fill(inc_ptr.begin(), inc_ptr.end() - 1);
+        for (int g = 0; g < M; g++) {
+            inc[fill[ab[g].x]++] = g;
+            inc[fill[ab[g].y]++] = (int)((uint32_t)g | 0x80000000u);
+        }
+    }
+    free_device(c);
+    static_assert(sizeof(bl_node) == 2 * sizeof(float4), "bl_node is two float4");
+    BL_CUDA(c, c->nd.alloc(2 * (size_t)N));
+    if (N) BL_CUDA(c, cudaMemcpyAsync(c->nd.p, nodes.data(), sizeof(bl_node) * N, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = upload_vec(c, c->info, info)) || (rc = upload_vec(c, c->inc_ptr, inc_ptr)) ||
+        (rc = upload_vec(c, c->inc, inc)) || (rc = upload_vec(c, c->ab, ab)) || (rc = upload_vec(c, c->kd, kd)) || (rc = upload_vec(c, c->bst, bst)) ||
+        (rc = upload_vec(c, c->bmeta, meta)) || (rc = upload_vec(c, c->bcold, bcold)) || (rc = upload_vec(c, c->stress, stress)) ||
+        (rc = upload_vec(c, c->bbody, bbody)) || (rc = upload_vec(c, c->dbodies, recs)))
+        return rc;
+    BL_CUDA(c, c->fv.alloc(M));
+    int P = 1;
+    while (P < maxn) P <<= 1;
+    c->rs_P = P;
+    BL_CUDA(c, c->rs_sort.alloc(3 * (size_t)P));
+    BL_CUDA(c, c->rs_bad.alloc(P));
+    BL_CUDA(c, c->rs_np.alloc(P));
+    BL_CUDA(c, c->rs_nv.alloc(P));
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->N = N, c->M = M, c->B = B;
+    c->bodies_dirty = false;
+    c->committed = true;
+    drop_graphs(c);
+    return BL_GPU_OK;
+}
+
+static int ensure_committed(bl_gpu_ctx* c) {
+    int rc;
+    if (c->statics_dirty && (rc = commit_statics(c))) return rc;
+    if (c->bodies_dirty && (rc = commit_bodies(c))) return rc;
+    return BL_GPU_OK;
+}
+
+// One frame of n substeps on stream s: 2n + 3 kernels. ev (2n + 4 events, or null): recorded before the first kernel
+// and after each one.
+static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+    int q = 0;
+    auto mark = [&]() {
+        if (ev) cudaEventRecord(ev[q++], s);
+    };
+    mark();
+    const float dt = c->cfg.dt;
+    const float frame_time = (float)n * dt;
+    const int tb = 256;
+    const int gb = (std::max(c->M, c->B) + tb - 1) / tb, gn = (c->N + tb - 1) / tb, gbody = (c->B + tb - 1) / tb;
+    k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
+    mark();
+    for (int k = 0; k < n; k++) {
+        k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fv.p, c->nd.p, c->dbodies.p,
+                                               c->M, c->B);
+        mark();
+        k_nodes<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc.p, c->fv.p, c->dbodies.p, c->st, c->cfg.gravity[0],
+                                               c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0);
+        mark();
+    }
+    RepairScratch rs{c->rs_sort.p, c->rs_bad.p, c->rs_np.p, c->rs_nv.p, c->rs_P};
+    k_frame_finish<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, c->nd.p, c->inc_ptr.p, c->inc.p, c->ab.p, c->bmeta.p, rs, frame_time, c->cfg.sleeping,
+                                      c->cfg.sleep_speed, c->cfg.sleep_time, c->deverr.p);
+    mark();
+    k_sleep_apply<<<std::max(c->B, 1), 256, 0, s>>>(c->dbodies.p, c->nd.p, c->bmeta.p);
+    mark();
+    return BL_GPU_OK;
+}
+
+// ------------------------------------------------------------------------------------------ C ABI
+extern "C" {
+
+void bl_gpu_default_config(bl_gpu_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->gravity[0] = 0, cfg->gravity[1] = -9.81f, cfg->gravity[2] = 0;
+    cfg->dt = 0.0005f;
+    cfg->sleeping = 1;
+    cfg->sleep_speed = 0.06f;
+    cfg->sleep_time = 1.0f;
+    cfg->device = 0;
+    cfg->deterministic = 1;
+}
+
+int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
+
+const char* bl_gpu_error_string(int code) {
+    switch (code) {
+    case BL_GPU_OK: return "ok";
+    case BL_GPU_EINVAL: return "invalid argument";
+    case BL_GPU_ENOMEM: return "out of memory";
+    case BL_GPU_ECUDA: return "CUDA error";
+    case BL_GPU_EUNSUPPORTED: return "unsupported feature";
+    case BL_GPU_ELIMIT: return "capacity exceeded";
+    case BL_GPU_ENODEVICE: return "no sm_100 CUDA device";
+    case BL_GPU_ESTATE: return "invalid state";
+    default: return "unknown error";
+    }
+}
+
+int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
+    if (!out) return BL_GPU_EINVAL;
+    *out = nullptr;
+    bl_gpu_config c0;
+    bl_gpu_default_config(&c0);
+    if (cfg) c0 = *cfg;
+    if (!(c0.dt > 0) || c0.deterministic != 1) return BL_GPU_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, c0.device) != cudaSuccess || prop.major != 10) return BL_GPU_ENODEVICE;
+    bl_gpu_ctx* c = new (std::nothrow) bl_gpu_ctx();
+    if (!c) return BL_GPU_ENOMEM;
+    c->cfg = c0;
+    auto fail = [&](cudaError_t e) {
+        c->last_cuda = (int)e;
+        delete c;
+        return e == cudaErrorMemoryAllocation ? BL_GPU_ENOMEM : BL_GPU_ECUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(c0.device)) != cudaSuccess) return fail(e);
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpyToSymbol(c_ground, kGroundModels, sizeof(kGroundModels))) != cudaSuccess) return fail(e);
+    if ((e = c->deverr.alloc(1)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->deverr.p, 0, sizeof(uint32_t))) != cudaSuccess) return fail(e);
+    *out = c;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_destroy(bl_gpu_ctx* c) {
+    if (!c) return BL_GPU_EINVAL;
+    cudaSetDevice(c->cfg.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    free_device(c);
+    free_statics(c);
+    c->deverr.free_();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_set_terrain(bl_gpu_ctx* c, int32_t nx, int32_t nz, float cell, float origin_x, float origin_z, const float* heights, const uint8_t* surfaces) {
+    if (!c || !heights || nx < 2 || nz < 2 || !(cell > 0)) return BL_GPU_EINVAL;
+    c->hnx = nx, c->hnz = nz, c->cell = cell, c->ox = origin_x, c->oz = origin_z;
+    c->heights.assign(heights, heights + (size_t)nx * nz);
+    if (surfaces) c->surfaces.assign(surfaces, surfaces + (size_t)nx * nz);
+    else c->surfaces.assign((size_t)nx * nz, 0);
+    // Heightfield::update_bounds (static_world.cpp:163-184): maxima over 16 x 16 cells, a vertex in every block it borders
+    const int kBlock = 16;
+    c->hbx = (nx - 1 + kBlock - 1) / kBlock, c->hbz = (nz - 1 + kBlock - 1) / kBlock;
+    c->block_max.assign((size_t)c->hbx * c->hbz, -1e30f);
+    for (int z = 0; z < nz; z++)
+        for (int x = 0; x < nx; x++) {
+            const float v = heights[(size_t)z * nx + x];
+            const int bx0 = std::max(0, (x - 1) / kBlock), bx1 = std::min(c->hbx - 1, x / kBlock);
+            const int bz0 = std::max(0, (z - 1) / kBlock), bz1 = std::min(c->hbz - 1, z / kBlock);
+            for (int bz = bz0; bz <= bz1; bz++)
+                for (int bx = bx0; bx <= bx1; bx++) {
+                    float& m = c->block_max[(size_t)bz * c->hbx + bx];
+                    m = (m < v) ? v : m;
+                }
+        }
+    c->has_terrain = 1;
+    c->statics_dirty = true;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_add_box(bl_gpu_ctx* c, const float center[3], const float half[3], const float q[4], int32_t surface, float max_force) {
+    if (!c || !center || !half || !q || surface < 0 || surface > 255) return BL_GPU_EINVAL;
+    Box b{};
+    b.cx = center[0], b.cy = center[1], b.cz = center[2];
+    b.hx = half[0], b.hy = half[1], b.hz = half[2];
+    // to_mat3 (math.h:166-174)
+    const float x = q[0], y = q[1], z = q[2], w = q[3];
+    const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, xz = x * z, yz = y * z, wx = w * x, wy = w * y, wz = w * z;
+    const float r[9] = {1 - 2 * (yy + zz), 2 * (xy + wz), 2 * (xz - wy), 2 * (xy - wz), 1 - 2 * (xx + zz), 2 * (yz + wx),
+                        2 * (xz + wy),     2 * (yz - wx), 1 - 2 * (xx + yy)};
+    std::memcpy(b.r, r, sizeof(r));
+    // StaticBox::update_aabb (static_world.cpp:242-246): e = |c0| hx + |c1| hy + |c2| hz
+    float e[3];
+    for (int k = 0; k < 3; k++) e[k] = std::fabs(r[k]) * b.hx + std::fabs(r[3 + k]) * b.hy + std::fabs(r[6 + k]) * b.hz;
+    b.mnx = b.cx - e[0], b.mny = b.cy - e[1], b.mnz = b.cz - e[2];
+    b.mxx = b.cx + e[0], b.mxy = b.cy + e[1], b.mxz = b.cz + e[2];
+    b.surface = surface;
+    b.max_force = max_force;
+    c->boxes.push_back(b);
+    c->statics_dirty = true;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_add_cylinder(bl_gpu_ctx* c, const float base[3], float radius, float height, int32_t surface) {
+    if (!c || !base || surface < 0 || surface > 255) return BL_GPU_EINVAL;
+    c->cyls.push_back(Cyl{base[0], base[1], base[2], radius, height, surface});
+    c->statics_dirty = true;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_build_grid(bl_gpu_ctx* c) {
+    if (!c) return BL_GPU_EINVAL;
+    build_grid_host(c);
+    c->statics_dirty = true;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_set_kill_y(bl_gpu_ctx* c, float y) {
+    if (!c) return BL_GPU_EINVAL;
+    c->kill_y = y;
+    c->statics_dirty = true;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
+    if (!c || !d || d->n_nodes < 0 || d->n_beams < 0 || (d->n_nodes > 0 && (!d->nodes || !d->info)) || (d->n_beams > 0 && !d->beams)) return BL_GPU_EINVAL;
+    if ((int64_t)d->n_beams * 2 + 2 * (int64_t)c->M > 0x7fffffffLL) return BL_GPU_ELIMIT;
+    for (int j = 0; j < d->n_beams; j++) {
+        const bl_beam& b = d->beams[j];
+        if (b.a >= (uint32_t)d->n_nodes || b.b >= (uint32_t)d->n_nodes || b.type > BL_BT_SUPPORT) return BL_GPU_EINVAL;
+        if (b.flags & BL_BF_SHOCK) return BL_GPU_EUNSUPPORTED; // shocks have their own force model (softbody.cpp:472-575)
+    }
+    HostBody hb;
+    hb.nodes.assign(d->nodes, d->nodes + d->n_nodes);
+    hb.info.assign(d->info, d->info + d->n_nodes);
+    hb.beams.assign(d->beams, d->beams + d->n_beams);
+    Body& r = hb.rec;
+    std::memset(&r, 0, sizeof(r));
+    r.fric = d->ground_friction;
+    r.bounce = d->bounce, r.push_max = d->contact_push_max, r.slop = d->contact_slop;
+    r.terrain_max = -1e30f;
+    r.sleeping = d->sleeping ? 1 : 0;
+    r.can_sleep = d->can_sleep ? 1 : 0;
+    r.sleep_speed = d->sleep_speed;
+    r.max_speed = d->max_speed;
+    // SoftBody::compute_aabb (softbody.cpp:271-275)
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    for (const bl_node& n : hb.nodes)
+        for (int k = 0; k < 3; k++) mn[k] = (n.p[k] < mn[k]) ? n.p[k] : mn[k], mx[k] = (mx[k] < n.p[k]) ? n.p[k] : mx[k];
+    for (int k = 0; k < 3; k++) r.aabb_mn[k] = mn[k], r.aabb_mx[k] = mx[k];
+    hb.beam_bits = (d->allow_deform ? BB_DEFORM : 0u) | (d->allow_break ? BB_BREAK : 0u) | (d->ductile ? BB_DUCTILE : 0u);
+    c->bodies.push_back(std::move(hb));
+    c->bodies_dirty = true;
+    if (body_id) *body_id = (int32_t)c->bodies.size() - 1;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_step_substeps(bl_gpu_ctx* c, int32_t n, void* stream) {
+    if (!c || n < 0) return BL_GPU_EINVAL;
+    if (n == 0) return BL_GPU_OK;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    int rc = ensure_committed(c);
+    if (rc) return rc;
+    c->last_substeps = n;
+    c->total_substeps += n;
+    if (c->B == 0) return BL_GPU_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    auto it = c->graphs.find(n);
+    if (it == c->graphs.end()) {
+        // capture the frame once on the context's stream, replay it from then on
+        cudaGraph_t g = nullptr;
+        BL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_frame(c, n, c->stream);
+        BL_CUDA(c, cudaStreamEndCapture(c->stream, &g));
+        cudaGraphExec_t ex = nullptr;
+        cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        BL_CUDA(c, e);
+        it = c->graphs.emplace(n, ex).first;
+    }
+    BL_CUDA(c, cudaGraphLaunch(it->second, s));
+    c->launches += 2 * (int64_t)n + 3;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_synchronize(bl_gpu_ctx* c) {
+    if (!c) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    BL_CUDA(c, cudaDeviceSynchronize());
+    return BL_GPU_OK;
+}
+
+static int check_body(bl_gpu_ctx* c, int32_t body) {
+    if (!c || body < 0 || body >= (int32_t)c->bodies.size()) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    return ensure_committed(c);
+}
+
+int bl_gpu_download_nodes(bl_gpu_ctx* c, int32_t body, bl_node* out) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    if (!out) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    const Body& r = c->bodies[body].rec;
+    if (r.nnodes) BL_CUDA(c, cudaMemcpyAsync(out, c->nd.p + 2 * (size_t)r.node0, sizeof(bl_node) * r.nnodes, cudaMemcpyDeviceToHost, c->stream));
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return BL_GPU_OK;
+}
+
+int bl_gpu_upload_nodes(bl_gpu_ctx* c, int32_t body, const bl_node* nodes) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    if (!nodes) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    const Body& r = c->bodies[body].rec;
+    if (r.nnodes) BL_CUDA(c, cudaMemcpyAsync(c->nd.p + 2 * (size_t)r.node0, nodes, sizeof(bl_node) * r.nnodes, cudaMemcpyHostToDevice, c->stream));
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return BL_GPU_OK;
+}
+
+int bl_gpu_download_beams(bl_gpu_ctx* c, int32_t body, bl_beam* out) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    if (!out) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    const HostBody& hb = c->bodies[body];
+    const Body& r = hb.rec;
+    std::vector<float4> bst(r.nbeams);
+    std::vector<uint32_t> meta(r.nbeams);
+    std::vector<float> stress(r.nbeams);
+    if (r.nbeams > 0) {
+        BL_CUDA(c, cudaMemcpyAsync(bst.data(), c->bst.p + r.beam0, sizeof(float4) * r.nbeams, cudaMemcpyDeviceToHost, c->stream));
+        BL_CUDA(c, cudaMemcpyAsync(meta.data(), c->bmeta.p + r.beam0, sizeof(uint32_t) * r.nbeams, cudaMemcpyDeviceToHost, c->stream));
+        BL_CUDA(c, cudaMemcpyAsync(stress.data(), c->stress.p + r.beam0, sizeof(float) * r.nbeams, cudaMemcpyDeviceToHost, c->stream));
+        BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    for (int j = 0; j < r.nbeams; j++) {
+        bl_beam b = hb.beams[j];
+        b.L = bst[j].x, b.max_pos = bst[j].y, b.max_neg = bst[j].z, b.strength = bst[j].w;
+        b.flags = (uint8_t)((meta[j] >> 8) & 0xff);
+        b.stress = stress[j];
+        out[j] = b;
+    }
+    return BL_GPU_OK;
+}
+
+int bl_gpu_body_state(bl_gpu_ctx* c, int32_t body, bl_body_state* out) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    if (!out) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    Body r;
+    BL_CUDA(c, cudaMemcpyAsync(&r, c->dbodies.p + body, sizeof(Body), cudaMemcpyDeviceToHost, c->stream));
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 3; k++) out->aabb_min[k] = r.aabb_mn[k], out->aabb_max[k] = r.aabb_mx[k];
+    out->max_speed = r.max_speed;
+    out->sleeping = r.sleeping;
+    out->static_contacts = r.static_contacts;
+    out->broken_beams = r.broken_beams;
+    out->sleep_timer = r.sleep_timer;
+    out->repaired_nodes = r.repaired;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_stats(bl_gpu_ctx* c, bl_world_stats* out) {
+    if (!c || !out) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    int rc = ensure_committed(c);
+    if (rc) return rc;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    std::memset(out, 0, sizeof(*out));
+    std::vector<Body> recs(c->B);
+    if (c->B) BL_CUDA(c, cudaMemcpy(recs.data(), c->dbodies.p, sizeof(Body) * c->B, cudaMemcpyDeviceToHost));
+    for (const Body& r : recs) {
+        if (r.sleeping) out->sleeping_bodies++;
+        else out->active_bodies++, out->active_nodes += r.nnodes, out->active_beams += r.nbeams;
+    }
+    BL_CUDA(c, cudaMemcpy(&out->device_errors, c->deverr.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    out->substeps = c->last_substeps;
+    out->total_substeps = c->total_substeps;
+    out->kernel_launches = c->launches;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_device_nodes(bl_gpu_ctx* c, void** nodes, int32_t* total) {
+    if (!c) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    int rc = ensure_committed(c);
+    if (rc) return rc;
+    if (nodes) *nodes = c->nd.p;
+    if (total) *total = c->N;
+    return BL_GPU_OK;
+}
+
+static int all_nodes_copy(bl_gpu_ctx* c, bl_node* host, int32_t n, void* stream, bool to_device) {
+    if (!c || !host) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    int rc = ensure_committed(c);
+    if (rc) return rc;
+    if (n != c->N) return BL_GPU_EINVAL;
+    if (n == 0) return BL_GPU_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    if (to_device) BL_CUDA(c, cudaMemcpyAsync(c->nd.p, host, sizeof(bl_node) * (size_t)n, cudaMemcpyHostToDevice, s));
+    else BL_CUDA(c, cudaMemcpyAsync(host, c->nd.p, sizeof(bl_node) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    return BL_GPU_OK;
+}
+
+int bl_gpu_upload_all_nodes(bl_gpu_ctx* c, const bl_node* nodes, int32_t n, void* stream) {
+    return all_nodes_copy(c, const_cast<bl_node*>(nodes), n, stream, true);
+}
+
+int bl_gpu_download_all_nodes(bl_gpu_ctx* c, bl_node* out, int32_t n, void* stream) { return all_nodes_copy(c, out, n, stream, false); }
+
+int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profile* out) {
+    if (!c || !out || n <= 0) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    int rc = ensure_committed(c);
+    if (rc) return rc;
+    std::memset(out, 0, sizeof(*out));
+    out->substeps = n;
+    if (c->B == 0) return BL_GPU_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    auto it = c->pgraphs.find(n);
+    if (it == c->pgraphs.end()) {
+        ProfGraph pg;
+        pg.events.resize(2 * (size_t)n + 4);
+        for (cudaEvent_t& e : pg.events) BL_CUDA(c, cudaEventCreate(&e));
+        cudaGraph_t g = nullptr;
+        BL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_frame(c, n, c->stream, pg.events.data());
+        BL_CUDA(c, cudaStreamEndCapture(c->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&pg.exec, g, 0);
+        cudaGraphDestroy(g);
+        BL_CUDA(c, e);
+        it = c->pgraphs.emplace(n, pg).first;
+    }
+    const ProfGraph& pg = it->second;
+    BL_CUDA(c, cudaGraphLaunch(pg.exec, s));
+    BL_CUDA(c, cudaStreamSynchronize(s));
+    c->launches += 2 * (int64_t)n + 3;
+    c->total_substeps += n;
+    c->last_substeps = n;
+    auto el = [&](int a, int b) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, pg.events[a], pg.events[b]);
+        return ms;
+    };
+    out->begin_ms = el(0, 1);
+    for (int k = 0; k < n; k++) out->beams_ms += el(1 + 2 * k, 2 + 2 * k), out->nodes_ms += el(2 + 2 * k, 3 + 2 * k);
+    out->finish_ms = el(1 + 2 * n, 3 + 2 * n);
+    out->frame_ms = el(0, 3 + 2 * n);
+    return BL_GPU_OK;
+}
+
+int bl_gpu_body_range(bl_gpu_ctx* c, int32_t body, int32_t* first_node, int32_t* n_nodes, int32_t* first_beam, int32_t* n_beams) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    const Body& r = c->bodies[body].rec;
+    if (first_node) *first_node = r.node0;
+    if (n_nodes) *n_nodes = r.nnodes;
+    if (first_beam) *first_beam = r.beam0;
+    if (n_beams) *n_beams = r.nbeams;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_last_cuda_error(bl_gpu_ctx* c) { return c ? c->last_cuda : 0; }
+
+} // extern "C"

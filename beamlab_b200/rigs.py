@@ -1,0 +1,290 @@
+"""Seeded synthetic rigs of the benchmark shapes, as plain numpy arrays.
+
+A rig is a dict ``{"settings": {...}, "statics": {...}, "bodies": [body, ...]}``; a body holds its nodes
+(``pos``, ``vel``, ``mass``, ``node_flags``, ``friction``, ``radius``), its beams (``ab``, ``k``, ``d``, ``strength``,
+``deform``, ``beam_type``, ``beam_flags``) and its knobs (``params``) - the arguments of the reference's builder calls
+``SoftBody::add_node`` / ``add_beam`` (softbody.cpp:8-40) before ``finalize``. The same arrays feed the GPU world
+(beamlab_b200.World) and the CPU oracles, so both step the very same rig.
+
+Random numbers come from a xorshift32 generator seeded like the reference test suite's ``TRng``
+(tests/test_physics.cpp:44-54: state = seed * 2654435761 + 1; uniform = the low 24 bits / 2^24).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+# node flags (softbody.h:29-39) and beam types (softbody.h:60)
+NF_GROUND, NF_FIXED, NF_TYRE, NF_RIM, NF_CONTACTER = 1, 2, 4, 8, 16
+BT_NORMAL, BT_ROPE, BT_SUPPORT = 0, 1, 2
+SURF_GRASS, SURF_CONCRETE = 0, 3
+GRASS_STATIC_FRICTION = 0.80  # ground model "grass", ms (static_world.cpp:97)
+
+
+class TRng:
+    """xorshift32 with the reference test suite's seeding (tests/test_physics.cpp:44-54)."""
+
+    def __init__(self, seed: int):
+        self.s = (seed * 2654435761 + 1) & 0xFFFFFFFF
+
+    def next(self) -> int:
+        s = self.s
+        s ^= (s << 13) & 0xFFFFFFFF
+        s ^= s >> 17
+        s ^= (s << 5) & 0xFFFFFFFF
+        self.s = s
+        return s
+
+    def uni(self) -> np.float32:
+        return np.float32(self.next() & 0xFFFFFF) / np.float32(0x1000000)
+
+    def range(self, a: float, b: float) -> np.float32:
+        a32, b32 = np.float32(a), np.float32(b)
+        return np.float32(a32 + (b32 - a32) * self.uni())
+
+    def gauss(self) -> float:
+        """A standard normal draw (Box-Muller over two uniforms, in double precision)."""
+        u1 = 1.0 - float(self.uni())
+        u2 = float(self.uni())
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+
+def flat_terrain(nx=81, nz=41, cell=1.0, origin=(-40.0, -20.0), height=0.0, surface=SURF_GRASS) -> dict:
+    """A flat heightfield (Heightfield::create, static_world.cpp:147-152) of nz rows of nx samples."""
+    return {"nx": nx, "nz": nz, "cell": cell, "origin": origin,
+            "heights": np.full((nz, nx), height, np.float32),
+            "surfaces": np.full((nz, nx), surface, np.uint8)}
+
+
+def lattice_body(rng: TRng, dims=(20, 4, 5), spacing=0.25, origin=(0.0, 0.0, 0.0), jitter=0.002,
+                 mass_range=(4.0, 6.0), k_median=2e6, k_sigma=0.3, damping=500.0, deform=5e4, strength=1.5e5,
+                 velocity=(0.0, 0.0, 0.0), ground_friction=1.0) -> dict:
+    """A jittered lattice truss: nodes on an nx x ny x nz grid (x fastest-varying last: index = (ix*ny + iy)*nz + iz),
+    beams between every pair of lattice neighbours (|di|,|dj|,|dk| <= 1) whose jittered distance is within
+    sqrt(3) * spacing, stiffness log-normal about k_median."""
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    pos = np.zeros((n, 3), np.float32)
+    mass = np.zeros(n, np.float32)
+    sp = np.float32(spacing)
+    for ix in range(nx):
+        for iy in range(ny):
+            for iz in range(nz):
+                i = (ix * ny + iy) * nz + iz
+                jx, jy, jz = rng.range(-jitter, jitter), rng.range(-jitter, jitter), rng.range(-jitter, jitter)
+                pos[i] = (np.float32(origin[0]) + np.float32(ix) * sp + jx,
+                          np.float32(origin[1]) + np.float32(iy) * sp + jy,
+                          np.float32(origin[2]) + np.float32(iz) * sp + jz)
+                mass[i] = rng.range(*mass_range)
+    thr = np.float32(math.sqrt(3.0) * spacing)
+    offsets = [(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1) if (dx, dy, dz) > (0, 0, 0)]
+    ab, ks = [], []
+    for ix in range(nx):
+        for iy in range(ny):
+            for iz in range(nz):
+                a = (ix * ny + iy) * nz + iz
+                for dx, dy, dz in offsets:
+                    jx, jy, jz = ix + dx, iy + dy, iz + dz
+                    if not (0 <= jx < nx and 0 <= jy < ny and 0 <= jz < nz):
+                        continue
+                    b = (jx * ny + jy) * nz + jz
+                    d = pos[a] - pos[b]
+                    dist = np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1]) + np.float32(d[2] * d[2]))
+                    if dist > thr:
+                        continue
+                    ab.append((a, b))
+                    ks.append(np.float32(k_median * math.exp(k_sigma * rng.gauss())))
+    m = len(ab)
+    vel = np.tile(np.asarray(velocity, np.float32), (n, 1))
+    return {
+        "pos": pos, "vel": vel, "mass": mass,
+        "node_flags": np.full(n, NF_GROUND | NF_CONTACTER, np.uint16),
+        "friction": np.ones(n, np.float32), "radius": np.zeros(n, np.float32),
+        "ab": np.asarray(ab, np.uint32).reshape(m, 2), "k": np.asarray(ks, np.float32),
+        "d": np.full(m, damping, np.float32), "strength": np.full(m, strength, np.float32),
+        "deform": np.full(m, deform, np.float32), "beam_type": np.zeros(m, np.uint8),
+        "beam_flags": np.zeros(m, np.uint8),
+        "params": {"ground_friction": ground_friction, "bounce": -1.0, "contact_push_max": 2.0, "contact_slop": 0.0,
+                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 1, "ductile": 0, "can_sleep": 1,
+                   "sleep_speed": 0.0},
+    }
+
+
+def lattice_body_fast(gen: np.random.Generator, dims=(20, 4, 5), spacing=0.25, origin=(0.0, 0.0, 0.0), jitter=0.002,
+                      mass_range=(4.0, 6.0), k_median=2e6, k_sigma=0.3, damping=500.0, deform=5e4, strength=1.5e5,
+                      velocity=(0.0, 0.0, 0.0), ground_friction=1.0) -> dict:
+    """lattice_body's structure (node order, beam rule and order: node a ascending, then its forward neighbour
+    offsets) with numpy's generator for the random draws, vectorized - for rigs of millions of beams."""
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    sp = np.float32(spacing)
+    jit = gen.uniform(-jitter, jitter, size=(n, 3)).astype(np.float32)
+    pos = np.stack([np.float32(origin[0]) + ix.ravel().astype(np.float32) * sp,
+                    np.float32(origin[1]) + iy.ravel().astype(np.float32) * sp,
+                    np.float32(origin[2]) + iz.ravel().astype(np.float32) * sp], 1).astype(np.float32) + jit
+    mass = gen.uniform(mass_range[0], mass_range[1], size=n).astype(np.float32)
+    thr = np.float32(math.sqrt(3.0) * spacing)
+    offsets = [(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1) if (dx, dy, dz) > (0, 0, 0)]
+    A, Bn, O = [], [], []
+    idx = np.arange(n).reshape(nx, ny, nz)
+    for o, (dx, dy, dz) in enumerate(offsets):
+        sx = slice(max(0, -dx), nx - max(0, dx)); sy = slice(max(0, -dy), ny - max(0, dy)); sz = slice(max(0, -dz), nz - max(0, dz))
+        a = idx[sx, sy, sz].ravel()
+        b = idx[slice(sx.start + dx, sx.stop + dx), slice(sy.start + dy, sy.stop + dy), slice(sz.start + dz, sz.stop + dz)].ravel()
+        d = pos[a] - pos[b]
+        dist = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+        keep = dist <= thr
+        A.append(a[keep]), Bn.append(b[keep]), O.append(np.full(int(keep.sum()), o))
+    A, Bn, O = np.concatenate(A), np.concatenate(Bn), np.concatenate(O)
+    order = np.lexsort((O, A))
+    ab = np.stack([A[order], Bn[order]], 1).astype(np.uint32)
+    m = len(ab)
+    k = (k_median * np.exp(k_sigma * gen.standard_normal(m))).astype(np.float32)
+    return {
+        "pos": pos, "vel": np.tile(np.asarray(velocity, np.float32), (n, 1)), "mass": mass,
+        "node_flags": np.full(n, NF_GROUND | NF_CONTACTER, np.uint16),
+        "friction": np.ones(n, np.float32), "radius": np.zeros(n, np.float32),
+        "ab": ab, "k": k, "d": np.full(m, damping, np.float32), "strength": np.full(m, strength, np.float32),
+        "deform": np.full(m, deform, np.float32), "beam_type": np.zeros(m, np.uint8), "beam_flags": np.zeros(m, np.uint8),
+        "params": {"ground_friction": ground_friction, "bounce": -1.0, "contact_push_max": 2.0, "contact_slop": 0.0,
+                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 1, "ductile": 0, "can_sleep": 1,
+                   "sleep_speed": 0.0},
+    }
+
+
+def truss_car(seed: int = 1, speed: float = 15.0, dims=(20, 4, 5)) -> dict:
+    """The plain explicit mass-spring truss car: a 20 x 4 x 5 node lattice (4.75 m long, 0.75 m high, 1 m wide) at
+    0.25 m with +-2 mm jitter, node mass uniform in [4, 6] kg, beams to every neighbour within sqrt(3) * 0.25 m
+    (about 3,100), k log-normal (median 2e6 N/m, sigma 0.3), d = 500 N s/m, plastic-deform threshold 5e4 N, break
+    threshold 1.5e5 N; gravity 9.81 m/s^2 over flat grass ground at y = 0 (friction 0.8: the grass model's static
+    coefficient, so the body's ground friction factor is 1); driving at `speed` m/s along +x into a rigid concrete
+    wall 2 m ahead; dt = 0.5 ms."""
+    rng = TRng(seed)
+    body = lattice_body(rng, dims=dims, origin=(-6.0, 0.05, -0.5), velocity=(speed, 0.0, 0.0),
+                        ground_friction=0.8 / GRASS_STATIC_FRICTION)
+    front = -6.0 + (dims[0] - 1) * 0.25
+    wall = {"center": (front + 2.0 + 0.25, 1.0, 0.0), "half": (0.25, 1.0, 2.0), "rot": (0.0, 0.0, 0.0, 1.0),
+            "surface": SURF_CONCRETE}
+    return {
+        "settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005},
+        "statics": {"terrain": flat_terrain(), "boxes": [wall], "build_grid": True},
+        "bodies": [body],
+        "name": f"truss_car(seed={seed})",
+    }
+
+
+def rig_counts(rig: dict) -> tuple[int, int]:
+    """(nodes, beams) over the rig's bodies."""
+    return (sum(len(b["mass"]) for b in rig["bodies"]), sum(len(b["k"]) for b in rig["bodies"]))
+
+
+def bumpy_terrain(rng: TRng, nx=129, nz=129, cell=0.5, origin=(-32.0, -32.0), amplitude=0.3, surfaces=(0,)) -> dict:
+    """A seeded heightfield: a sum of a few random sine waves (amplitude in m), each sample's surface drawn from
+    `surfaces`."""
+    xs = np.arange(nx, dtype=np.float64) * cell + origin[0]
+    zs = np.arange(nz, dtype=np.float64) * cell + origin[1]
+    X, Z = np.meshgrid(xs, zs)
+    h = np.zeros_like(X)
+    for _ in range(4):
+        kx, kz = float(rng.range(-0.6, 0.6)), float(rng.range(-0.6, 0.6))
+        ph = float(rng.range(0.0, 6.283))
+        h += np.sin(kx * X + kz * Z + ph)
+    h *= amplitude / 4.0
+    surf = np.zeros((nz, nx), np.uint8)
+    for iz in range(nz):
+        for ix in range(nx):
+            surf[iz, ix] = surfaces[rng.next() % len(surfaces)]
+    return {"nx": nx, "nz": nz, "cell": cell, "origin": origin, "heights": h.astype(np.float32), "surfaces": surf}
+
+
+def stress_rig(seed: int = 7) -> dict:
+    """A small rig that takes every branch of the explicit path: rope and support beams, weak beams that yield and
+    break, a ductile body, anchored nodes, node friction and radii, bumpy ground of grass, mud and sand, a rotated box,
+    a yielding box (max force) and a cylinder in the way."""
+    rng = TRng(seed)
+    bodies = []
+    for bi, (dims, origin, vel, ductile) in enumerate((
+            ((8, 3, 3), (-8.0, 0.4, -0.4), (25.0, -2.0, 0.5), 0),
+            ((6, 3, 2), (-8.0, 0.5, 3.0), (18.0, 0.0, -1.0), 1),
+            ((5, 2, 2), (4.0, 0.6, -4.0), (-3.0, 0.0, 9.0), 0))):
+        b = lattice_body(rng, dims=dims, origin=origin, velocity=vel, strength=2.5e4, deform=8e3,
+                         k_median=6e5, damping=300.0)
+        m = len(b["k"])
+        for j in range(m):
+            r = rng.next() % 10
+            if r == 0:
+                b["beam_type"][j] = BT_ROPE
+            elif r == 1:
+                b["beam_type"][j] = BT_SUPPORT
+            elif r == 2:
+                b["beam_flags"][j] = 4  # BF_NO_DEFORM
+            elif r == 3:
+                b["beam_flags"][j] = 8  # BF_NO_BREAK
+        n = len(b["mass"])
+        b["friction"] = np.asarray([rng.range(0.5, 1.5) for _ in range(n)], np.float32)
+        b["radius"] = np.asarray([rng.range(0.0, 0.03) for _ in range(n)], np.float32)
+        if bi == 2:
+            b["node_flags"][0] |= NF_FIXED  # an anchor (and a zero-mass node, inverse mass 0 too)
+            b["mass"][1] = 0.0
+        b["params"].update({"ductile": ductile, "contact_slop": 0.001 * bi, "contact_push_max": 2.0 - 0.5 * bi,
+                            "bounce": 0.3 if bi == 1 else -1.0})
+        bodies.append(b)
+    half_sin = math.sin(0.3)
+    statics = {
+        "terrain": bumpy_terrain(rng, surfaces=(0, 0, 2, 5, 6)),
+        "boxes": [
+            {"center": (0.0, 0.5, 0.0), "half": (0.3, 0.5, 1.5), "rot": (0.0, half_sin, 0.0, math.cos(0.3)), "surface": 3},
+            {"center": (1.5, 0.4, 3.3), "half": (0.4, 0.4, 0.6), "rot": (0.1, 0.0, 0.0, math.sqrt(1 - 0.01)),
+             "surface": 8, "max_force": 4000.0},
+            {"center": (0.0, -0.5, 0.0), "half": (40.0, 0.2, 40.0), "rot": (0.0, 0.0, 0.0, 1.0), "surface": 4},
+        ],
+        "cylinders": [{"base": (2.0, -0.5, -1.0), "radius": 0.25, "height": 2.0, "surface": 9}],
+        "build_grid": True,
+    }
+    return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005}, "statics": statics, "bodies": bodies,
+            "name": f"stress_rig(seed={seed})"}
+
+
+def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, sigma: float = 0.6,
+          min_nodes: int = 500, max_nodes: int = 20000, terrain_size: float = 1000.0, terrain_samples: int = 2048,
+          amplitude: float = 2.0) -> dict:
+    """A batched fleet of lattice trusses with log-normal node counts (median `median_nodes`, clipped to
+    [min_nodes, max_nodes]), each driving at a speed uniform in [5, 30] m/s with a random yaw over a square heightfield
+    of terrain_samples^2 samples spanning terrain_size metres, `amplitude` m of seeded smooth noise. Vehicles are laid
+    out on a grid 40 m apart so that none touch. Random draws: numpy's PCG64 seeded with `seed`."""
+    gen = np.random.default_rng(seed)
+    cell = terrain_size / (terrain_samples - 1)
+    half = terrain_size / 2
+
+    def octave(m, amp):  # bilinear value noise over an m x m lattice of random heights
+        g = gen.uniform(-1.0, 1.0, size=(m, m))
+        t = np.linspace(0, m - 1, terrain_samples)
+        i0 = np.minimum(np.floor(t).astype(int), m - 2)
+        f = t - i0
+        rows = g[i0] * (1 - f)[:, None] + g[i0 + 1] * f[:, None]
+        return amp * (rows[:, i0] * (1 - f)[None, :] + rows[:, i0 + 1] * f[None, :])
+    h = (octave(33, amplitude) + octave(129, amplitude * 0.25)).astype(np.float32)
+    terrain = {"nx": terrain_samples, "nz": terrain_samples, "cell": cell, "origin": (-half, -half), "heights": h,
+               "surfaces": np.zeros((terrain_samples, terrain_samples), np.uint8)}
+    side = int(math.ceil(math.sqrt(n_vehicles)))
+    bodies = []
+    for v in range(n_vehicles):
+        nn = int(np.clip(median_nodes * math.exp(sigma * gen.standard_normal()), min_nodes, max_nodes))
+        # lattice dims in a car's proportions: length 4, width 1.25, height 1
+        unit = (nn / 5.0) ** (1.0 / 3.0)
+        nx = max(2, int(round(4 * unit / 1.7)))
+        nz = max(2, int(round(1.25 * unit / 1.7 * 1.2)))
+        ny = max(2, int(round(nn / (nx * nz))))
+        gx, gz = v % side, v // side
+        x0, z0 = -half + 60 + gx * 40.0, -half + 60 + gz * 40.0
+        ix, iz = int((x0 + half) / cell), int((z0 + half) / cell)
+        ground = float(h[min(iz, terrain_samples - 1), min(ix, terrain_samples - 1)])
+        speed = float(gen.uniform(5.0, 30.0))
+        yaw = float(gen.uniform(0.0, 2 * math.pi))
+        bodies.append(lattice_body_fast(gen, dims=(nx, ny, nz), origin=(x0, ground + 0.6, z0),
+                                        velocity=(speed * math.cos(yaw), 0.0, speed * math.sin(yaw))))
+    return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005},
+            "statics": {"terrain": terrain, "boxes": [], "build_grid": True}, "bodies": bodies,
+            "name": f"fleet(n={n_vehicles}, seed={seed})"}

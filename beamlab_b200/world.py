@@ -1,0 +1,442 @@
+"""Python host mirror of BeamLab's physics step API over the C ABI (include/beamlab_gpu.h).
+
+Names, argument meaning and defaults follow the reference's ``bl::phys`` classes, so code written against them reads
+the same here:
+
+* ``WorldSettings``   - WorldSettings (src/phys/world.h:24-77), the fields the path reads
+* ``StaticWorld``     - StaticWorld (src/phys/static_world.h:182-201): terrain, add_box, build_grid, kill_y
+* ``SoftBody``        - a SoftBody under construction: add_node / add_beam / finalize (src/phys/softbody.cpp:8-83)
+* ``World``           - World (src/phys/world.h:150-171): add_body, step_substeps, step_frame, stats
+* ``BodyHandle``      - what World.add_body returns (the reference's SoftBody* owned by the World): state read-back
+
+Everything is computed by the CUDA library; this module only describes rigs and moves arrays. Without the built
+library (or without an sm_100 GPU) World() raises - there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+# == bl_node / bl_node_info / bl_beam (include/beamlab_gpu.h) == the reference's Node / NodeInfo / Beam
+NODE_DTYPE = np.dtype([("p", "<f4", 3), ("inv_mass", "<f4"), ("v", "<f4", 3), ("mass", "<f4")])
+NODE_INFO_DTYPE = np.dtype([("flags", "<u2"), ("surface", "u1"), ("pad", "u1"), ("friction", "<f4"), ("radius", "<f4"),
+                            ("frame", "<i4"), ("ror_id", "<i4")])
+BEAM_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("L", "<f4"), ("k", "<f4"), ("d", "<f4"), ("max_pos", "<f4"),
+                       ("max_neg", "<f4"), ("strength", "<f4"), ("plastic", "<f4"), ("stress", "<f4"), ("L0", "<f4"),
+                       ("support_limit", "<f4"), ("type", "u1"), ("flags", "u1"), ("group", "<u2")])
+assert NODE_DTYPE.itemsize == 32 and NODE_INFO_DTYPE.itemsize == 20 and BEAM_DTYPE.itemsize == 52
+
+NF_GROUND, NF_FIXED, NF_CONTACTER = 1, 2, 16
+BF_BROKEN, BF_SHOCK = 1, 64
+
+
+class BeamLabError(RuntimeError):
+    """A C-ABI call returned a negative BL_GPU_E* code."""
+
+
+def _check(rc: int, what: str, ctx=None):
+    if rc != 0:
+        msg = _lib.lib().bl_gpu_error_string(rc).decode()
+        extra = ""
+        if ctx is not None and rc == -3:
+            extra = f" (cuda error {_lib.lib().bl_gpu_last_cuda_error(ctx)})"
+        raise BeamLabError(f"{what}: {msg} [{rc}]{extra}")
+
+
+@dataclass
+class WorldSettings:
+    """WorldSettings (world.h:24-77): the fields of the explicit substep."""
+    gravity: tuple = (0.0, -9.81, 0.0)
+    dt: float = 0.0005
+    sleeping: bool = True
+    sleep_speed: float = 0.06
+    sleep_time: float = 1.0
+
+
+@dataclass
+class StaticWorld:
+    """StaticWorld (static_world.h:182-201): a heightfield, boxes, vertical cylinders. Boxes are candidates for
+    contact only after build_grid(), as in the reference."""
+    terrain: dict | None = None
+    boxes: list = field(default_factory=list)
+    cylinders: list = field(default_factory=list)
+    grid_built: bool = False
+    kill_y: float = -200.0
+
+    def create_terrain(self, nx: int, nz: int, cell: float, origin=(0.0, 0.0), heights=None, surfaces=None):
+        """Heightfield::create (static_world.cpp:147-152) + the heights and surfaces (nz rows of nx, x fastest)."""
+        h = np.zeros((nz, nx), np.float32) if heights is None else np.asarray(heights, np.float32).reshape(nz, nx)
+        s = np.zeros((nz, nx), np.uint8) if surfaces is None else np.asarray(surfaces, np.uint8).reshape(nz, nx)
+        self.terrain = {"nx": nx, "nz": nz, "cell": cell, "origin": tuple(origin), "heights": h, "surfaces": s}
+
+    def add_box(self, center, half, rot=(0.0, 0.0, 0.0, 1.0), surface: int = 3, max_force: float = 0.0):
+        """StaticWorld::add_box (static_world.cpp:298-306); rot is a quaternion (x, y, z, w)."""
+        self.boxes.append({"center": tuple(center), "half": tuple(half), "rot": tuple(rot), "surface": surface,
+                           "max_force": max_force})
+
+    def add_cylinder(self, base, radius: float, height: float, surface: int = 3):
+        self.cylinders.append({"base": tuple(base), "radius": radius, "height": height, "surface": surface})
+
+    def build_grid(self):
+        """StaticWorld::build_grid (static_world.cpp:308-338)."""
+        self.grid_built = True
+
+
+def _dist32(pa: np.ndarray, pb: np.ndarray) -> np.ndarray:
+    """distance(a, b) in float32, in math.h's order: sqrt((dx*dx + dy*dy) + dz*dz)."""
+    d = (pa - pb).astype(np.float32)
+    l2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+    return np.sqrt(l2.astype(np.float32))
+
+
+class SoftBody:
+    """A soft body under construction (SoftBody, softbody.h:595-1119): nodes, beams and the explicit path's knobs."""
+
+    def __init__(self, name: str = ""):
+        self.name = name
+        self._nodes: list = []
+        self._info: list = []
+        self._beams: list = []
+        self.ground_friction = 1.0
+        self.bounce = -1.0
+        self.contact_push_max = 2.0
+        self.contact_slop = 0.0
+        self.collision_radius = 0.05
+        self.allow_deform = True
+        self.allow_break = True
+        self.ductile = False
+        self.can_sleep = True
+        self.sleep_speed = 0.0
+        self.nodes = np.zeros(0, NODE_DTYPE)
+        self.info = np.zeros(0, NODE_INFO_DTYPE)
+        self.beams = np.zeros(0, BEAM_DTYPE)
+
+    def add_node(self, p, mass: float, flags: int = NF_GROUND | NF_CONTACTER, v=(0.0, 0.0, 0.0), friction=1.0,
+                 radius=0.0) -> int:
+        """SoftBody::add_node (softbody.cpp:8-20): an anchored or massless node has inverse mass 0."""
+        m = np.float32(mass)
+        inv = np.float32(0.0) if (flags & NF_FIXED) or m <= 0 else np.float32(1.0) / m
+        self._nodes.append((tuple(np.float32(x) for x in p), inv, tuple(np.float32(x) for x in v), m))
+        self._info.append((flags, 0, 0, np.float32(friction), np.float32(radius), -1, -1))
+        return len(self._nodes) - 1
+
+    def add_beam(self, a: int, b: int, k: float, d: float, strength: float = 1e6, deform: float = 4e5,
+                 type: int = 0, flags: int = 0) -> int:
+        """SoftBody::add_beam (softbody.cpp:22-40)."""
+        self._beams.append((a, b, k, d, strength, deform, type, flags))
+        return len(self._beams) - 1
+
+    @classmethod
+    def from_arrays(cls, body: dict, name: str = "") -> "SoftBody":
+        """A body from the arrays of beamlab_b200.rigs (the builder calls' arguments), finalized."""
+        sb = cls(name)
+        n = len(body["mass"])
+        nodes = np.zeros(n, NODE_DTYPE)
+        nodes["p"] = np.asarray(body["pos"], np.float32)
+        nodes["v"] = np.asarray(body["vel"], np.float32)
+        m = np.asarray(body["mass"], np.float32)
+        nodes["mass"] = m
+        fl = np.asarray(body["node_flags"], np.uint16)
+        with np.errstate(divide="ignore"):
+            inv = np.where(((fl & NF_FIXED) != 0) | (m <= 0), np.float32(0), np.float32(1) / np.where(m > 0, m, 1))
+        nodes["inv_mass"] = inv.astype(np.float32)
+        info = np.zeros(n, NODE_INFO_DTYPE)
+        info["flags"] = fl
+        info["friction"] = np.asarray(body["friction"], np.float32)
+        info["radius"] = np.asarray(body["radius"], np.float32)
+        info["frame"] = -1
+        info["ror_id"] = -1
+        mb = len(body["k"])
+        beams = np.zeros(mb, BEAM_DTYPE)
+        ab = np.asarray(body["ab"], np.uint32).reshape(mb, 2)
+        beams["a"], beams["b"] = ab[:, 0], ab[:, 1]
+        beams["k"] = np.asarray(body["k"], np.float32)
+        beams["d"] = np.asarray(body["d"], np.float32)
+        beams["strength"] = np.asarray(body["strength"], np.float32)
+        dfm = np.asarray(body["deform"], np.float32)
+        beams["max_pos"], beams["max_neg"] = dfm, -dfm
+        beams["support_limit"] = np.float32(4.0)
+        beams["type"] = np.asarray(body["beam_type"], np.uint8)
+        beams["flags"] = np.asarray(body["beam_flags"], np.uint8)
+        sb.nodes, sb.info, sb.beams = nodes, info, beams
+        for k_, v_ in body.get("params", {}).items():
+            setattr(sb, k_, v_)
+        sb._finalize_arrays()
+        return sb
+
+    def finalize(self):
+        """SoftBody::finalize (softbody.cpp:76-83): the node and beam arrays, rest lengths at least 1 mm."""
+        n = len(self._nodes)
+        nodes = np.zeros(n, NODE_DTYPE)
+        info = np.zeros(n, NODE_INFO_DTYPE)
+        for i, (p, inv, v, m) in enumerate(self._nodes):
+            nodes[i] = (p, inv, v, m)
+        for i, t in enumerate(self._info):
+            info[i] = t
+        beams = np.zeros(len(self._beams), BEAM_DTYPE)
+        for j, (a, b, k, d, s, dfm, t, f) in enumerate(self._beams):
+            beams[j]["a"], beams[j]["b"] = a, b
+            beams[j]["k"], beams[j]["d"], beams[j]["strength"] = k, d, s
+            beams[j]["max_pos"], beams[j]["max_neg"] = np.float32(dfm), -np.float32(dfm)
+            beams[j]["support_limit"] = 4.0
+            beams[j]["type"], beams[j]["flags"] = t, f
+        self.nodes, self.info, self.beams = nodes, info, beams
+        self._finalize_arrays()
+
+    def _finalize_arrays(self):
+        if len(self.beams):
+            L = _dist32(self.nodes["p"][self.beams["a"]], self.nodes["p"][self.beams["b"]])
+            L = np.where(np.float32(1e-3) < L, L, np.float32(1e-3)).astype(np.float32)  # std::max(1e-3f, len)
+            self.beams["L"] = L
+            self.beams["L0"] = L
+            self.beams["plastic"] = 0
+            self.beams["stress"] = 0
+
+    def node_count(self) -> int:
+        return len(self.nodes)
+
+
+class _BodyDesc(C.Structure):
+    _fields_ = [("n_nodes", C.c_int32), ("nodes", C.c_void_p), ("info", C.c_void_p), ("n_beams", C.c_int32),
+                ("beams", C.c_void_p), ("ground_friction", C.c_float), ("bounce", C.c_float),
+                ("contact_push_max", C.c_float), ("contact_slop", C.c_float), ("allow_deform", C.c_int32),
+                ("allow_break", C.c_int32), ("ductile", C.c_int32), ("can_sleep", C.c_int32),
+                ("sleep_speed", C.c_float), ("max_speed", C.c_float), ("sleeping", C.c_int32)]
+
+
+class _BodyState(C.Structure):
+    _fields_ = [("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3), ("max_speed", C.c_float),
+                ("sleeping", C.c_int32), ("static_contacts", C.c_int32), ("broken_beams", C.c_int32),
+                ("sleep_timer", C.c_float), ("repaired_nodes", C.c_int32)]
+
+
+class _WorldStats(C.Structure):
+    _fields_ = [("substeps", C.c_int32), ("active_bodies", C.c_int32), ("sleeping_bodies", C.c_int32),
+                ("active_nodes", C.c_int32), ("active_beams", C.c_int32), ("total_substeps", C.c_int64),
+                ("kernel_launches", C.c_int64), ("device_errors", C.c_uint32)]
+
+
+class _FrameProfile(C.Structure):
+    _fields_ = [("substeps", C.c_int32), ("frame_ms", C.c_float), ("begin_ms", C.c_float), ("beams_ms", C.c_float),
+                ("nodes_ms", C.c_float), ("finish_ms", C.c_float)]
+
+
+class _Config(C.Structure):
+    _fields_ = [("gravity", C.c_float * 3), ("dt", C.c_float), ("sleeping", C.c_int32), ("sleep_speed", C.c_float),
+                ("sleep_time", C.c_float), ("device", C.c_int32), ("deterministic", C.c_int32)]
+
+
+class BodyHandle:
+    """A body held by a World (the reference's SoftBody* from World::add_body)."""
+
+    def __init__(self, world: "World", index: int, n_nodes: int, n_beams: int, name: str):
+        self.world, self.index, self.name = world, index, name
+        self.n_nodes, self.n_beams = n_nodes, n_beams
+
+    def nodes(self) -> np.ndarray:
+        out = np.zeros(self.n_nodes, NODE_DTYPE)
+        _check(self.world._L.bl_gpu_download_nodes(self.world._ctx, self.index, out.ctypes.data), "download_nodes",
+               self.world._ctx)
+        return out
+
+    def set_nodes(self, nodes: np.ndarray):
+        nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+        _check(self.world._L.bl_gpu_upload_nodes(self.world._ctx, self.index, nodes.ctypes.data), "upload_nodes",
+               self.world._ctx)
+
+    def beams(self) -> np.ndarray:
+        out = np.zeros(self.n_beams, BEAM_DTYPE)
+        _check(self.world._L.bl_gpu_download_beams(self.world._ctx, self.index, out.ctypes.data), "download_beams",
+               self.world._ctx)
+        return out
+
+    def state(self) -> dict:
+        s = _BodyState()
+        _check(self.world._L.bl_gpu_body_state(self.world._ctx, self.index, C.byref(s)), "body_state",
+               self.world._ctx)
+        return {"aabb_min": np.array(s.aabb_min, np.float32), "aabb_max": np.array(s.aabb_max, np.float32),
+                "max_speed": float(s.max_speed), "sleeping": bool(s.sleeping), "static_contacts": s.static_contacts,
+                "broken_beams": s.broken_beams, "sleep_timer": float(s.sleep_timer),
+                "repaired_nodes": s.repaired_nodes}
+
+
+class World:
+    """World (world.h:150-171) on one B200: the statics, the bodies, frames of 2 kHz substeps."""
+
+    def __init__(self, settings: WorldSettings | None = None, device: int = 0):
+        self.settings = settings or WorldSettings()
+        self.statics = StaticWorld()
+        self._L = _lib.lib()
+        cfg = _Config()
+        self._L.bl_gpu_default_config(C.byref(cfg))
+        cfg.gravity[:] = [float(x) for x in self.settings.gravity]
+        cfg.dt = self.settings.dt
+        cfg.sleeping = int(self.settings.sleeping)
+        cfg.sleep_speed = self.settings.sleep_speed
+        cfg.sleep_time = self.settings.sleep_time
+        cfg.device = device
+        self._ctx = C.c_void_p()
+        _check(self._L.bl_gpu_create(C.byref(cfg), C.byref(self._ctx)), "create")
+        self._bodies: list[BodyHandle] = []
+        self._statics_sent = False
+        self._keep = []
+        self._accum = 0.0
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._L.bl_gpu_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- statics
+    def _send_statics(self):
+        if self._statics_sent:
+            return
+        st, L, ctx = self.statics, self._L, self._ctx
+        if st.terrain is not None:
+            t = st.terrain
+            h = np.ascontiguousarray(t["heights"], np.float32)
+            s = np.ascontiguousarray(t["surfaces"], np.uint8) if t.get("surfaces") is not None else None
+            _check(L.bl_gpu_set_terrain(ctx, int(t["nx"]), int(t["nz"]), float(t["cell"]), float(t["origin"][0]),
+                                        float(t["origin"][1]), h.ctypes.data, s.ctypes.data if s is not None else None),
+                   "set_terrain", ctx)
+        for b in st.boxes:
+            arr = (C.c_float * 3)(*b["center"]), (C.c_float * 3)(*b["half"]), (C.c_float * 4)(*b.get("rot", (0, 0, 0, 1)))
+            _check(L.bl_gpu_add_box(ctx, arr[0], arr[1], arr[2], int(b.get("surface", 3)), float(b.get("max_force", 0.0))),
+                   "add_box", ctx)
+        for c in st.cylinders:
+            _check(L.bl_gpu_add_cylinder(ctx, (C.c_float * 3)(*c["base"]), float(c["radius"]), float(c["height"]),
+                                         int(c.get("surface", 3))), "add_cylinder", ctx)
+        if st.grid_built:
+            _check(L.bl_gpu_build_grid(ctx), "build_grid", ctx)
+        _check(L.bl_gpu_set_kill_y(ctx, float(st.kill_y)), "set_kill_y", ctx)
+        self._statics_sent = True
+
+    # ---- bodies
+    def add_body(self, body: SoftBody) -> BodyHandle:
+        """World::add_body (world.cpp:283-289): the body is copied to the device."""
+        if body.node_count() == 0 and len(body._nodes):
+            body.finalize()
+        nodes = np.ascontiguousarray(body.nodes, NODE_DTYPE)
+        info = np.ascontiguousarray(body.info, NODE_INFO_DTYPE)
+        beams = np.ascontiguousarray(body.beams, BEAM_DTYPE)
+        d = _BodyDesc(len(nodes), nodes.ctypes.data, info.ctypes.data, len(beams), beams.ctypes.data,
+                      body.ground_friction, body.bounce, body.contact_push_max, body.contact_slop,
+                      int(body.allow_deform), int(body.allow_break), int(body.ductile), int(body.can_sleep),
+                      body.sleep_speed, 0.0, 0)
+        idx = C.c_int32()
+        _check(self._L.bl_gpu_add_body(self._ctx, C.byref(d), C.byref(idx)), "add_body", self._ctx)
+        h = BodyHandle(self, idx.value, len(nodes), len(beams), body.name)
+        self._bodies.append(h)
+        return h
+
+    def bodies(self) -> list[BodyHandle]:
+        return list(self._bodies)
+
+    # ---- stepping
+    def step_substeps(self, n: int, stream=None):
+        """World::step_substeps (world.cpp:368-585): one frame of n substeps, enqueued (asynchronous).
+        stream: a torch.cuda.Stream, a raw cudaStream_t (int) or None (the world's own)."""
+        self._send_statics()
+        _check(self._L.bl_gpu_step_substeps(self._ctx, int(n), self._stream(stream)), "step_substeps", self._ctx)
+
+    def step_frame(self, frame_dt: float):
+        """World::step_frame (world.cpp:312-346) without the load-dependent substep limits: the substeps the
+        accumulated time holds, at most 100."""
+        self._accum += frame_dt
+        n = int(self._accum / self.settings.dt)
+        if n > 100:
+            n, self._accum = 100, 0.0
+        else:
+            self._accum -= n * self.settings.dt
+        if n > 0:
+            self.step_substeps(n)
+
+    def synchronize(self):
+        _check(self._L.bl_gpu_synchronize(self._ctx), "synchronize", self._ctx)
+
+    def stats(self) -> dict:
+        s = _WorldStats()
+        self._send_statics()
+        _check(self._L.bl_gpu_stats(self._ctx, C.byref(s)), "stats", self._ctx)
+        return {k: getattr(s, k) for k, _ in _WorldStats._fields_}
+
+    def device_nodes(self):
+        """(pointer, total): the device array of every body's nodes back to back, in NODE_DTYPE records."""
+        self._send_statics()
+        p, n = C.c_void_p(), C.c_int32()
+        _check(self._L.bl_gpu_device_nodes(self._ctx, C.byref(p), C.byref(n)), "device_nodes", self._ctx)
+        return p.value, n.value
+
+    @staticmethod
+    def _stream(stream):
+        s = getattr(stream, "cuda_stream", stream) if stream is not None else None
+        return C.c_void_p(s) if s else None
+
+    def upload_all_nodes(self, nodes: np.ndarray, stream=None):
+        """Every body's nodes (NODE_DTYPE, back to back) to the device, asynchronous on `stream`."""
+        self._send_statics()
+        _check(self._L.bl_gpu_upload_all_nodes(self._ctx, nodes.ctypes.data, len(nodes), self._stream(stream)),
+               "upload_all_nodes", self._ctx)
+
+    def download_all_nodes(self, out: np.ndarray, stream=None):
+        """Every body's nodes from the device into `out` (NODE_DTYPE), asynchronous on `stream`."""
+        self._send_statics()
+        _check(self._L.bl_gpu_download_all_nodes(self._ctx, out.ctypes.data, len(out), self._stream(stream)),
+               "download_all_nodes", self._ctx)
+
+    def profile_frame(self, n: int, stream=None) -> dict:
+        """One frame of n substeps (it advances the world) with the GPU time of each kind of kernel; synchronous."""
+        self._send_statics()
+        p = _FrameProfile()
+        _check(self._L.bl_gpu_profile_frame(self._ctx, int(n), self._stream(stream), C.byref(p)), "profile_frame",
+               self._ctx)
+        return {k: getattr(p, k) for k, _ in _FrameProfile._fields_}
+
+    def body_range(self, body: int):
+        a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        _check(self._L.bl_gpu_body_range(self._ctx, body, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
+               "body_range", self._ctx)
+        return a.value, b.value, c.value, d.value
+
+
+def world_from_rig(rig: dict, device: int = 0, **overrides) -> World:
+    """A World holding a rig of beamlab_b200.rigs: its settings, statics and bodies."""
+    s = dict(rig.get("settings", {}))
+    s.update(overrides)
+    w = World(WorldSettings(**{k: v for k, v in s.items() if k in WorldSettings.__dataclass_fields__}), device)
+    st = rig.get("statics", {})
+    t = st.get("terrain")
+    if t is not None:
+        w.statics.create_terrain(t["nx"], t["nz"], t["cell"], t["origin"], t["heights"], t.get("surfaces"))
+    for b in st.get("boxes", []):
+        w.statics.add_box(b["center"], b["half"], b.get("rot", (0, 0, 0, 1)), b.get("surface", 3),
+                          b.get("max_force", 0.0))
+    for c in st.get("cylinders", []):
+        w.statics.add_cylinder(c["base"], c["radius"], c["height"], c.get("surface", 3))
+    if st.get("build_grid", True):
+        w.statics.build_grid()
+    if "kill_y" in st:
+        w.statics.kill_y = st["kill_y"]
+    for i, b in enumerate(rig["bodies"]):
+        w.add_body(SoftBody.from_arrays(b, name=f"body{i}"))
+    return w
+
+
+__all__ = ["World", "WorldSettings", "StaticWorld", "SoftBody", "BodyHandle", "BeamLabError", "world_from_rig",
+           "NODE_DTYPE", "NODE_INFO_DTYPE", "BEAM_DTYPE"]

@@ -1,0 +1,315 @@
+"""Benchmark of the 2 kHz soft-body substep on B200: node-substeps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload fleet256|truss_car]
+
+A step is one 60 Hz frame of 33 substeps (World::step_substeps(33)) over the whole workload. The default workload is
+the batched fleet: 256 seeded lattice vehicles of log-normal size (500-20,000 nodes, median 3,000; about 0.9 M nodes
+and 8.5 M beams) driving over a 2048^2-sample, 1 km^2 heightfield - the fleet configuration's shape without its wheel
+rings and inter-vehicle contacts (this path has no contacts between bodies yet). Under torchrun each rank steps its
+own fleet (weak scaling, no data-path collective: vehicles that do not touch are independent islands).
+
+Rank 0 prints one JSON line: value = node-substeps/s of all ranks with the state resident in HBM (CUDA events on the
+world's stream, max over ranks); e2e = the same through the C ABI with the node state copied in from pinned host
+memory and back out every frame; roofline = the dominant kernel's algorithmic bytes over its CUDA-event time in a
+profiled frame of the timed region; cpu_baseline = the reference's own CPU step (compiled from its sources, all host
+threads) on a bounded sample of the same workload.
+
+--impl reference times the reference's CPU implementation alone (rank 0; other ranks exit at once).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-substeps/s at 2 kHz, batched+learned vs plain GPU, residual<=1e-6"
+UNIT = "node-substeps/s"
+FRAME = 33
+# algorithmic bytes of one substep (each array touched once): a beam reads its ends (8 B), L, k, d, max_pos, max_neg,
+# strength (24 B), its type and flags (4 B) and writes its force's magnitude (stress, 4 B); a node reads p, v, 1/m
+# (28 B) and writes p, v (24 B)
+BYTES_PER_BEAM = 40
+BYTES_PER_NODE = 52
+
+
+def workload(name: str, rank: int):
+    from beamlab_b200 import rigs
+    if name == "fleet256":
+        rig = rigs.fleet(256, seed=3 + rank)
+        n, m = rigs.rig_counts(rig)
+        desc = (f"fleet256: 256 lattice vehicles ({n:,} nodes, {m:,} beams; log-normal 500-20,000 nodes, median "
+                f"3,000), 2048^2-sample 1 km^2 heightfield, 5-30 m/s random yaw; no wheel rings, no inter-vehicle "
+                f"contacts")
+    elif name == "truss_car":
+        rig = rigs.truss_car(1 + rank)
+        n, m = rigs.rig_counts(rig)
+        desc = f"truss_car: 20x4x5 lattice ({n} nodes, {m} beams) at 15 m/s into a rigid wall"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return rig, n, m, desc
+
+
+class ClockSampler:
+    """nvidia-smi samples of the GPU's clocks and throttle reasons every 200 ms while running."""
+
+    FIELDS = ("clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: str | None):
+        self.gpu, self.lines, self.proc = gpu, [], None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={','.join(self.FIELDS)}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu:
+            cmd += ["-i", self.gpu]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=lambda: self.lines.extend(iter(self.proc.stdout.readline, "")), daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                smax = max(smax, float(p[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_unit():
+    """DRAM bytes per beam / per node of the two substep kernels from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    return json.load(open(path)) if os.path.exists(path) else {}
+
+
+def cpu_reference(rig, n_nodes, frames=2, warm=4):
+    """The reference's own step (compiled from its sources, Release flags) on all host cores: node-substeps/s of a
+    bounded sample (warm-up substeps, then `frames` frames of 33 substeps of the same workload)."""
+    from oracle.oracle import RefWorld, build_world, ref_available, ref_jobs_init, ref_jobs_shutdown
+    if not ref_available("timing"):
+        return None
+    cores = os.cpu_count() or 1
+    threads = ref_jobs_init(max(0, cores - 1), "timing")
+    w = build_world(RefWorld, rig, flavour="timing", multithreaded=True)
+    w.step_substeps(warm)
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        w.step_substeps(FRAME)
+    dt = time.perf_counter() - t0
+    w.close()
+    ref_jobs_shutdown("timing")
+    return {"value": n_nodes * FRAME * frames / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"the same workload, {frames} frames of {FRAME} substeps after {warm} warm-up substeps "
+                      f"({frames * FRAME} substeps, {dt:.2f} s)"}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    rig, n, m, desc = workload(args.workload, 0)
+    from oracle.oracle import RefWorld, build_world, ref_available, ref_jobs_init, ref_jobs_shutdown
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "frame_substeps": FRAME}}
+    if not ref_available("timing"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU build (oracle/_ref) is missing"}),
+              flush=True)
+        return
+    cores = os.cpu_count() or 1
+    threads = ref_jobs_init(max(0, cores - 1), "timing")
+    w = build_world(RefWorld, rig, flavour="timing", multithreaded=True)
+    for _ in range(args.warmup):
+        w.step_substeps(FRAME)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        w.step_substeps(FRAME)
+    dt = time.perf_counter() - t0
+    v = n * FRAME * args.steps / dt
+    w.close()
+    ref_jobs_shutdown("timing")
+    base.update({"value": v, "ms_per_step": dt * 1e3 / args.steps, "scaling": "weak", "vs_baseline": None,
+                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                                  "sample": f"the whole workload, {args.steps} frames of {FRAME} substeps"}})
+    print(json.dumps(base), flush=True)
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from beamlab_b200 import NODE_DTYPE, world_from_rig
+    rig, n, m, desc = workload(args.workload, rank)
+    w = world_from_rig(rig, device=local)
+    stream = torch.cuda.Stream()
+    K, W = args.steps, args.warmup
+
+    # warm-up: every graph used below is captured here (plain frames, the profiled frame)
+    for _ in range(max(W - 1, 0)):
+        w.step_substeps(FRAME, stream)
+    w.profile_frame(FRAME, stream)
+    torch.cuda.synchronize()
+    st0 = w.stats()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.3)
+
+    # ---- resident: K frames, the last one profiled (CUDA events between its kernels)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K - 1):
+        w.step_substeps(FRAME, stream)
+    prof = w.profile_frame(FRAME, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st1 = w.stats()
+
+    # ---- end to end through the C ABI: the node state in from pinned host memory and out again every frame
+    host = torch.empty(n * NODE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+    hbuf = np.frombuffer(host.numpy(), dtype=NODE_DTYPE)
+    w.download_all_nodes(hbuf, stream)
+    stream.synchronize()
+    for _ in range(2):
+        w.upload_all_nodes(hbuf, stream)
+        w.step_substeps(FRAME, stream)
+        w.download_all_nodes(hbuf, stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(K):
+        w.upload_all_nodes(hbuf, stream)
+        w.step_substeps(FRAME, stream)
+        w.download_all_nodes(hbuf, stream)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = f0.elapsed_time(f1)
+    clk = clocks.stop()
+
+    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    units = torch.tensor([float(n)], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(units, op=dist.ReduceOp.SUM)
+        dist.barrier()
+    ms, ms_e2e = float(t[0]), float(t[1])
+    total_nodes = float(units[0])
+    if rank == 0:
+        value = total_nodes * FRAME * K / (ms * 1e-3)
+        e2e = total_nodes * FRAME * K / (ms_e2e * 1e-3)
+        peak, pk_kind = peaks()
+        per_beam = prof["beams_ms"] / FRAME
+        per_node = prof["nodes_ms"] / FRAME
+        kern = {"k_beams": (BYTES_PER_BEAM * m, per_beam, m, "beam"), "k_nodes": (BYTES_PER_NODE * n, per_node, n, "node")}
+        dom = max(kern, key=lambda k: kern[k][1])
+        alg_bytes, kms, units_, unit_name = kern[dom]
+        achieved = alg_bytes / (kms * 1e-3) / 1e9
+        tr = traffic_per_unit().get(dom)
+        traffic = tr[f"dram_bytes_per_{unit_name}"] * units_ if tr else None
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": desc, "frame_substeps": FRAME, "step": f"one frame of {FRAME} substeps",
+                       "l2": "inputs larger than L2 (the fleet's device state is about 0.8 GB)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "kernel_ms_per_substep": {"k_beams": per_beam, "k_nodes": per_node,
+                                                 "frame_begin_finish": (prof["begin_ms"] + prof["finish_ms"]) / FRAME}},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * NODE_DTYPE.itemsize,
+                    "d2h_bytes_per_step": n * NODE_DTYPE.itemsize},
+            "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{pk_kind} hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg_bytes, "traffic": traffic},
+            "clocks": clk,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_reference(rig, n)
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+    w.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="fleet256", choices=["fleet256", "truss_car"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,213 @@
+/* beamlab_gpu.h - the C ABI of the B200-native soft-body substep.
+ *
+ * It replaces, for the bodies it holds, the stepping of BeamLab's `bl::phys::World` (src/phys/world.h:150-171):
+ * gravity, RoR beam spring-dampers with plastic yield and breaking (SoftBody::compute_beam_forces,
+ * src/phys/softbody.cpp:412-470), static contacts against the heightfield, boxes and cylinders
+ * (World::collide_static, src/phys/world.cpp:781-899; StaticWorld::collide_point, src/phys/static_world.cpp:364-474;
+ * primitive_collision, src/phys/static_world.cpp:8-51) and symplectic Euler integration
+ * (SoftBody::integrate_nodes, src/phys/softbody.cpp:769-795), frame by frame as World::step_substeps
+ * (src/phys/world.cpp:368-585) runs them, with the per-frame static candidate query, top speed and sleep.
+ *
+ * Plain C: pointers, sizes and POD records only. The node, node-info and beam records have the byte layout of the
+ * reference's `Node` (softbody.h:43-48), `NodeInfo` (softbody.h:50-58) and `Beam` (softbody.h:71-85), so a host shim
+ * can pass a SoftBody's vectors as they are.
+ *
+ * Threading: one context is used by one host thread at a time (as World is). Calls on a context are ordered on its
+ * CUDA stream; bl_gpu_step_substeps is asynchronous, the download/stat calls synchronise that stream.
+ *
+ * Errors: every call returns BL_GPU_OK (0) or a negative BL_GPU_E* code; bl_gpu_error_string names it. The
+ * reference's step has no return code (its failures show up as counters, src/phys/frame_fem.h:342-344 and
+ * src/phys/world.h:111); those counters are in bl_world_stats. */
+#ifndef BEAMLAB_GPU_H
+#define BEAMLAB_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BL_GPU_ABI_VERSION 1
+
+enum {
+    BL_GPU_OK = 0,
+    BL_GPU_EINVAL = -1,       /* a bad argument (null pointer, index out of range, inconsistent sizes) */
+    BL_GPU_ENOMEM = -2,       /* device or host allocation failed */
+    BL_GPU_ECUDA = -3,        /* a CUDA call failed; bl_gpu_last_cuda_error has its code */
+    BL_GPU_EUNSUPPORTED = -4, /* the body uses a feature this path does not step (shocks, joints, wheels, sheets ...) */
+    BL_GPU_ELIMIT = -5,       /* a fixed capacity was exceeded (see the call's comment) */
+    BL_GPU_ENODEVICE = -6,    /* no CUDA device of compute capability 10.0 */
+    BL_GPU_ESTATE = -7        /* the call is not valid in the context's current state */
+};
+
+/* node flags (NodeFlag, softbody.h:29-39), beam types and flags (BeamType / BeamFlag, softbody.h:60-69) */
+enum {
+    BL_NF_GROUND = 1 << 0, BL_NF_FIXED = 1 << 1, BL_NF_TYRE = 1 << 2, BL_NF_RIM = 1 << 3, BL_NF_CONTACTER = 1 << 4,
+    BL_NF_FRAME = 1 << 5, BL_NF_LOAD = 1 << 6, BL_NF_NO_MOUSE = 1 << 7, BL_NF_SELF_COLL = 1 << 8
+};
+enum { BL_BT_NORMAL = 0, BL_BT_ROPE = 1, BL_BT_SUPPORT = 2 };
+enum {
+    BL_BF_BROKEN = 1 << 0, BL_BF_INVISIBLE = 1 << 1, BL_BF_NO_DEFORM = 1 << 2, BL_BF_NO_BREAK = 1 << 3,
+    BL_BF_WHEEL = 1 << 4, BL_BF_HYDRO = 1 << 5, BL_BF_SHOCK = 1 << 6
+};
+
+/* World settings the path reads (WorldSettings, src/phys/world.h:24-77) plus the device to run on */
+typedef struct {
+    float gravity[3];          /* m/s^2; the reference's default {0, -9.81, 0} */
+    float dt;                  /* substep (s); default 0.0005 (2 kHz) */
+    int32_t sleeping;          /* bodies at rest fall asleep (WorldSettings::sleeping) */
+    float sleep_speed;         /* m/s (WorldSettings::sleep_speed) */
+    float sleep_time;          /* s (WorldSettings::sleep_time) */
+    int32_t device;            /* CUDA device ordinal */
+    int32_t deterministic;     /* 1: every node sums its forces in the reference's order (bitwise equal results);
+                                  the only mode of this version */
+} bl_gpu_config;
+
+/* == bl::phys::Node (softbody.h:43-48): 32 bytes */
+typedef struct {
+    float p[3];
+    float inv_mass;
+    float v[3];
+    float mass;
+} bl_node;
+
+/* == bl::phys::NodeInfo (softbody.h:50-58): 20 bytes */
+typedef struct {
+    uint16_t flags;
+    uint8_t surface;
+    uint8_t pad;
+    float friction;
+    float radius;
+    int32_t frame;
+    int32_t ror_id;
+} bl_node_info;
+
+/* == bl::phys::Beam (softbody.h:71-85): 52 bytes */
+typedef struct {
+    uint32_t a, b;
+    float L, k, d;
+    float max_pos, max_neg, strength, plastic, stress, L0, support_limit;
+    uint8_t type, flags;
+    uint16_t group;
+} bl_beam;
+
+/* One body: a SoftBody after finalize (softbody.cpp:76-83) - its arrays and the knobs of the explicit path
+ * (softbody.h:650-700). Bodies with shocks, joints, wheels, slide nodes, sheets, FEM frames, air drag or grab are
+ * rejected with BL_GPU_EUNSUPPORTED by the caller's shim (this record has no fields for them). */
+typedef struct {
+    int32_t n_nodes;
+    const bl_node* nodes;
+    const bl_node_info* info;
+    int32_t n_beams;
+    const bl_beam* beams;
+    float ground_friction;     /* SoftBody::ground_friction */
+    float bounce;              /* SoftBody::bounce (-1: RoR's 80% of the approach) */
+    float contact_push_max;    /* SoftBody::contact_push_max */
+    float contact_slop;        /* SoftBody::contact_slop */
+    int32_t allow_deform;      /* SoftBody::allow_deform */
+    int32_t allow_break;       /* SoftBody::allow_break */
+    int32_t ductile;           /* SoftBody::ductile */
+    int32_t can_sleep;         /* SoftBody::can_sleep */
+    float sleep_speed;         /* SoftBody::sleep_speed (0: the world's) */
+    float max_speed;           /* SoftBody::max_speed at upload (the first frame's static query margin) */
+    int32_t sleeping;          /* SoftBody::sleeping at upload */
+} bl_body_desc;
+
+/* A body's runtime state (SoftBody::aabb, max_speed, sleeping, static_contacts, stats.broken_beams, sleep_timer) */
+typedef struct {
+    float aabb_min[3];
+    float aabb_max[3];
+    float max_speed;
+    int32_t sleeping;
+    int32_t static_contacts;   /* over the last frame's substeps */
+    int32_t broken_beams;      /* since upload */
+    float sleep_timer;
+    int32_t repaired_nodes;    /* nodes World::repair_nodes reset, since upload */
+} bl_body_state;
+
+/* WorldStats (world.h:79-132), the fields this path fills, and the device's error word */
+typedef struct {
+    int32_t substeps;          /* of the last bl_gpu_step_substeps */
+    int32_t active_bodies, sleeping_bodies, active_nodes, active_beams;
+    int64_t total_substeps;    /* since the context was made */
+    int64_t kernel_launches;   /* kernels this library launched since the context was made */
+    uint32_t device_errors;    /* BL_GPU_DEVERR_* bits raised by the kernels */
+} bl_world_stats;
+
+enum {
+    BL_GPU_DEVERR_CANDIDATES = 1 << 0, /* a body's static candidate list overflowed BL_GPU_MAX_CANDIDATES */
+    BL_GPU_DEVERR_NONFINITE = 1 << 1   /* a body needed the repair of non-finite / runaway nodes */
+};
+#define BL_GPU_MAX_CANDIDATES 64
+
+typedef struct bl_gpu_ctx bl_gpu_ctx;
+
+/* Defaults of the reference's WorldSettings (world.h:25-60) into *cfg. */
+void bl_gpu_default_config(bl_gpu_config* cfg);
+
+/* A world on cfg->device (World::World). The context owns a CUDA stream unless one is given to each call. */
+int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out);
+int bl_gpu_destroy(bl_gpu_ctx* ctx);
+
+/* Statics, before the first step (StaticWorld, static_world.h:182-201). heights/surfaces: nz rows of nx samples,
+ * x fastest (Heightfield::create + h()/surf(), static_world.h:52-70); surfaces may be NULL (grass). */
+int bl_gpu_set_terrain(bl_gpu_ctx* ctx, int32_t nx, int32_t nz, float cell, float origin_x, float origin_z, const float* heights,
+                       const uint8_t* surfaces);
+/* StaticWorld::add_box(center, half, rot = quaternion x,y,z,w, surface); max_force as StaticBox::max_force (0: rigid) */
+int bl_gpu_add_box(bl_gpu_ctx* ctx, const float center[3], const float half[3], const float quat[4], int32_t surface, float max_force);
+/* a vertical cylinder (StaticCylinder, static_world.h:133-137) */
+int bl_gpu_add_cylinder(bl_gpu_ctx* ctx, const float base[3], float radius, float height, int32_t surface);
+/* StaticWorld::build_grid (static_world.cpp:308-338): without it boxes are never candidates, as in the reference */
+int bl_gpu_build_grid(bl_gpu_ctx* ctx);
+/* StaticWorld::kill_y (nodes below are frozen) */
+int bl_gpu_set_kill_y(bl_gpu_ctx* ctx, float y);
+
+/* World::add_body (world.cpp:283-289): copies the body in; *body_id is its index (0, 1, ... in order). */
+int bl_gpu_add_body(bl_gpu_ctx* ctx, const bl_body_desc* desc, int32_t* body_id);
+
+/* World::step_substeps(n) (world.cpp:368-585): one frame of n substeps of every awake body, enqueued on `stream`
+ * (a cudaStream_t; NULL: the context's own). Asynchronous. */
+int bl_gpu_step_substeps(bl_gpu_ctx* ctx, int32_t n, void* stream);
+
+/* Whole-body state transfers (synchronous on the context's stream): nodes in bl_node records, beams in bl_beam. */
+int bl_gpu_download_nodes(bl_gpu_ctx* ctx, int32_t body, bl_node* out);
+int bl_gpu_upload_nodes(bl_gpu_ctx* ctx, int32_t body, const bl_node* nodes);
+int bl_gpu_download_beams(bl_gpu_ctx* ctx, int32_t body, bl_beam* out);
+int bl_gpu_body_state(bl_gpu_ctx* ctx, int32_t body, bl_body_state* out);
+int bl_gpu_stats(bl_gpu_ctx* ctx, bl_world_stats* out);
+/* waits for everything enqueued on the context's stream */
+int bl_gpu_synchronize(bl_gpu_ctx* ctx);
+
+/* The nodes of all bodies back to back, in bl_node records (body after body, as added), asynchronous on `stream`
+ * (NULL: the context's): one copy each way - the caller's buffer should be pinned, and is not to be touched until the
+ * stream has passed the copy. n must be the total node count (bl_gpu_device_nodes). These are what a host shim that
+ * keeps the reference's SoftBody arrays in step moves each frame. */
+int bl_gpu_upload_all_nodes(bl_gpu_ctx* ctx, const bl_node* nodes, int32_t n, void* stream);
+int bl_gpu_download_all_nodes(bl_gpu_ctx* ctx, bl_node* out, int32_t n, void* stream);
+
+/* The device-resident node array (bl_node records of all bodies back to back, 16-byte aligned) and its length, for
+ * callers that keep their own data on the GPU; each body's first node and beam. Valid until the next bl_gpu_add_body. */
+int bl_gpu_device_nodes(bl_gpu_ctx* ctx, void** nodes, int32_t* total_nodes);
+int bl_gpu_body_range(bl_gpu_ctx* ctx, int32_t body, int32_t* first_node, int32_t* n_nodes, int32_t* first_beam, int32_t* n_beams);
+
+/* One frame of n substeps, like bl_gpu_step_substeps, with a timing event between its kernels; waits for it and
+ * returns the GPU time of each kind of kernel (summed over the frame's substeps). */
+typedef struct {
+    int32_t substeps;
+    float frame_ms;            /* the whole frame */
+    float begin_ms;            /* the frame's start (static candidates per body) */
+    float beams_ms;            /* the beams' forces, all substeps */
+    float nodes_ms;            /* the nodes' gather, static contacts and integration, all substeps */
+    float finish_ms;           /* the frame's end (bounds, repair, sleep) */
+} bl_frame_profile;
+int bl_gpu_profile_frame(bl_gpu_ctx* ctx, int32_t n, void* stream, bl_frame_profile* out);
+
+const char* bl_gpu_error_string(int code);
+int bl_gpu_last_cuda_error(bl_gpu_ctx* ctx);
+int bl_gpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,239 @@
+"""Test infrastructure only: ctypes front ends for the two CPU oracles of the explicit soft-body substep.
+
+* ``PortWorld``  - the plain-C restatement (oracle/softbody_oracle.c, built into oracle/_build/liboracle.so);
+* ``RefWorld``   - the reference itself (BeamLab src/phys + src/core, compiled by oracle/Makefile into
+  oracle/_ref/libbeamlab_ref_{parity,timing}.so, driven through oracle/ref_driver.cpp).
+
+Both take the same rig description (a dict of numpy arrays, see beamlab_b200.rigs) and expose the same calls, so a
+test can step one rig through either and compare. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg import this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_LIBS = {
+    "parity": os.path.join(HERE, "_ref", "libbeamlab_ref_parity.so"),
+    "timing": os.path.join(HERE, "_ref", "libbeamlab_ref_timing.so"),
+}
+
+
+class BodyParams(C.Structure):
+    """SoftBody knobs of the explicit path (softbody.h:650-700); the layout of RefBodyParams / OrcBodyParams."""
+    _fields_ = [
+        ("ground_friction", C.c_float), ("bounce", C.c_float), ("contact_push_max", C.c_float),
+        ("contact_slop", C.c_float), ("collision_radius", C.c_float), ("allow_deform", C.c_int32),
+        ("allow_break", C.c_int32), ("ductile", C.c_int32), ("can_sleep", C.c_int32), ("sleep_speed", C.c_float),
+    ]
+
+
+def body_params(body: dict) -> BodyParams:
+    p = body.get("params", {})
+    return BodyParams(
+        float(p.get("ground_friction", 1.0)), float(p.get("bounce", -1.0)), float(p.get("contact_push_max", 2.0)),
+        float(p.get("contact_slop", 0.0)), float(p.get("collision_radius", 0.05)), int(p.get("allow_deform", 1)),
+        int(p.get("allow_break", 1)), int(p.get("ductile", 0)), int(p.get("can_sleep", 1)),
+        float(p.get("sleep_speed", 0.0)),
+    )
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype)) if a is not None else None
+
+
+_loaded: dict[str, C.CDLL] = {}
+
+
+def _load(path: str, prefix: str) -> C.CDLL:
+    if path in _loaded:
+        return _loaded[path]
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library missing: {path} (run `make -C oracle`)")
+    lib = C.CDLL(path)
+    vp, f, i = C.c_void_p, C.c_float, C.c_int
+    fp, u8p, u16p, u32p = C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.POINTER(C.c_uint16), C.POINTER(C.c_uint32)
+    sig = {
+        "world_new": ([], vp),
+        "world_free": ([vp], None),
+        "world_settings": ([vp, f, f, f, f, i, i, i, f, f], None),
+        "set_terrain": ([vp, i, i, f, f, f, fp, u8p], None),
+        "add_box": ([vp, f, f, f, f, f, f, f, f, f, f, i], None),
+        "add_cylinder": ([vp, f, f, f, f, f, i], None),
+        "build_grid": ([vp], None),
+        "set_kill_y": ([vp, f], None),
+        "add_body": ([vp, i, fp, fp, fp, u16p, fp, fp, i, u32p, fp, fp, fp, fp, u8p, u8p, i, u32p, C.POINTER(BodyParams)], i),
+        "step_substeps": ([vp, i], None),
+        "body_nodes": ([vp, i], i),
+        "body_beams": ([vp, i], i),
+        "get_nodes": ([vp, i, fp, fp, fp, fp], None),
+        "set_nodes": ([vp, i, fp, fp], None),
+        "get_beams": ([vp, i, fp, fp, fp, fp, fp, u8p], None),
+        "get_body": ([vp, i, fp], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, f"{prefix}_{name}")
+        fn.argtypes = args
+        fn.restype = res
+    if prefix == "ref":
+        lib.ref_jobs_init.argtypes = [i]
+        lib.ref_jobs_threads.restype = i
+    _loaded[path] = lib
+    return lib
+
+
+class _OracleWorld:
+    """One world of the oracle: statics, bodies, frames of substeps (World::step_substeps)."""
+
+    prefix = ""
+
+    def __init__(self, lib: C.CDLL):
+        self._lib = lib
+        self._fn = lambda name: getattr(lib, f"{self.prefix}_{name}")
+        self._w = self._fn("world_new")()
+        self._keep = []
+
+    def close(self):
+        if self._w:
+            self._fn("world_free")(self._w)
+            self._w = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def settings(self, gravity=(0.0, -9.81, 0.0), dt=0.0005, sleeping=True, multithreaded=True, inter_body=True,
+                 sleep_speed=0.06, sleep_time=1.0):
+        self._fn("world_settings")(self._w, *map(float, gravity), float(dt), int(sleeping), int(multithreaded),
+                                   int(inter_body), float(sleep_speed), float(sleep_time))
+
+    def load_statics(self, statics: dict):
+        t = statics.get("terrain")
+        if t is not None:
+            h = np.ascontiguousarray(t["heights"], dtype=np.float32)
+            s = t.get("surfaces")
+            s = np.ascontiguousarray(s, dtype=np.uint8) if s is not None else None
+            self._keep += [h, s]
+            self._fn("set_terrain")(self._w, int(t["nx"]), int(t["nz"]), float(t["cell"]), float(t["origin"][0]),
+                                    float(t["origin"][1]), _ptr(h, C.c_float), _ptr(s, C.c_uint8))
+        for b in statics.get("boxes", []):
+            q = b.get("rot", (0.0, 0.0, 0.0, 1.0))
+            self._fn("add_box")(self._w, *map(float, b["center"]), *map(float, b["half"]), *map(float, q),
+                                int(b.get("surface", 3)))
+        for c in statics.get("cylinders", []):
+            self._fn("add_cylinder")(self._w, *map(float, c["base"]), float(c["radius"]), float(c["height"]),
+                                     int(c.get("surface", 3)))
+        if statics.get("build_grid", True):
+            self._fn("build_grid")(self._w)
+        if "kill_y" in statics:
+            self._fn("set_kill_y")(self._w, float(statics["kill_y"]))
+
+    def add_body(self, body: dict) -> int:
+        a = {k: np.ascontiguousarray(body[k], dtype=dt) for k, dt in (
+            ("pos", np.float32), ("vel", np.float32), ("mass", np.float32), ("node_flags", np.uint16),
+            ("friction", np.float32), ("radius", np.float32), ("ab", np.uint32), ("k", np.float32),
+            ("d", np.float32), ("strength", np.float32), ("deform", np.float32), ("beam_type", np.uint8),
+            ("beam_flags", np.uint8))}
+        tris = np.ascontiguousarray(body.get("tris", np.zeros((0, 3), np.uint32)), dtype=np.uint32)
+        prm = body_params(body)
+        self._keep += list(a.values()) + [tris, prm]
+        return self._fn("add_body")(
+            self._w, len(a["mass"]), _ptr(a["pos"], C.c_float), _ptr(a["vel"], C.c_float), _ptr(a["mass"], C.c_float),
+            _ptr(a["node_flags"], C.c_uint16), _ptr(a["friction"], C.c_float), _ptr(a["radius"], C.c_float),
+            len(a["k"]), _ptr(a["ab"], C.c_uint32), _ptr(a["k"], C.c_float), _ptr(a["d"], C.c_float),
+            _ptr(a["strength"], C.c_float), _ptr(a["deform"], C.c_float), _ptr(a["beam_type"], C.c_uint8),
+            _ptr(a["beam_flags"], C.c_uint8), len(tris), _ptr(tris, C.c_uint32), C.byref(prm))
+
+    def step_substeps(self, n: int):
+        self._fn("step_substeps")(self._w, int(n))
+
+    def nodes(self, body: int):
+        n = self._fn("body_nodes")(self._w, body)
+        pos = np.zeros((n, 3), np.float32)
+        vel = np.zeros((n, 3), np.float32)
+        im = np.zeros(n, np.float32)
+        m = np.zeros(n, np.float32)
+        self._fn("get_nodes")(self._w, body, _ptr(pos, C.c_float), _ptr(vel, C.c_float), _ptr(im, C.c_float),
+                              _ptr(m, C.c_float))
+        return {"pos": pos, "vel": vel, "inv_mass": im, "mass": m}
+
+    def set_nodes(self, body: int, pos, vel):
+        pos = np.ascontiguousarray(pos, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        self._fn("set_nodes")(self._w, body, _ptr(pos, C.c_float), _ptr(vel, C.c_float))
+
+    def beams(self, body: int):
+        m = self._fn("body_beams")(self._w, body)
+        out = {k: np.zeros(m, np.float32) for k in ("L", "max_pos", "max_neg", "strength", "stress")}
+        fl = np.zeros(m, np.uint8)
+        self._fn("get_beams")(self._w, body, *(_ptr(out[k], C.c_float) for k in ("L", "max_pos", "max_neg",
+                                                                                "strength", "stress")),
+                              _ptr(fl, C.c_uint8))
+        out["flags"] = fl
+        return out
+
+    def body(self, body: int):
+        o = np.zeros(11, np.float32)
+        self._fn("get_body")(self._w, body, _ptr(o, C.c_float))
+        return {"aabb_min": o[0:3].copy(), "aabb_max": o[3:6].copy(), "max_speed": float(o[6]),
+                "sleeping": bool(o[7]), "static_contacts": int(o[8]), "broken_beams": int(o[9]),
+                "sleep_timer": float(o[10])}
+
+
+class PortWorld(_OracleWorld):
+    """The plain-C restatement (single-threaded)."""
+
+    prefix = "orc"
+
+    def __init__(self):
+        super().__init__(_load(PORT_LIB, "orc"))
+
+
+class RefWorld(_OracleWorld):
+    """The reference's own World, compiled from its sources (flavour "parity" or "timing")."""
+
+    prefix = "ref"
+
+    def __init__(self, flavour: str = "parity"):
+        super().__init__(_load(REF_LIBS[flavour], "ref"))
+
+
+def ref_available(flavour: str = "parity") -> bool:
+    return os.path.exists(REF_LIBS[flavour])
+
+
+def port_available() -> bool:
+    return os.path.exists(PORT_LIB)
+
+
+def ref_jobs_init(workers: int, flavour: str = "timing") -> int:
+    """JobSystem::get().init(workers) of the reference library (src/core/jobs.h:22); returns its thread count. The
+    workers are shut down at interpreter exit (a process with them running does not end)."""
+    import atexit
+    lib = _load(REF_LIBS[flavour], "ref")
+    lib.ref_jobs_init(int(workers))
+    atexit.register(lib.ref_jobs_shutdown)
+    return lib.ref_jobs_threads()
+
+
+def ref_jobs_shutdown(flavour: str = "timing"):
+    """JobSystem::get().shutdown() (src/core/jobs.h:23)."""
+    _load(REF_LIBS[flavour], "ref").ref_jobs_shutdown()
+
+
+def build_world(cls, rig: dict, **settings):
+    """A world of `cls` holding the rig's statics and bodies (in order)."""
+    w = cls() if cls is PortWorld else cls(settings.pop("flavour", "parity"))
+    s = dict(rig.get("settings", {}))
+    s.update(settings)
+    w.settings(**s)
+    w.load_statics(rig.get("statics", {}))
+    for b in rig["bodies"]:
+        w.add_body(b)
+    return w

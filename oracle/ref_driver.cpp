@@ -1,0 +1,169 @@
+// Test infrastructure only: a C-ABI driver over the reference's own physics (BeamLab `src/phys`, `src/core`),
+// compiled from the reference's sources where they lie (oracle/Makefile). It lets tests, the golden-fixture script and
+// the CPU-baseline leg of bench.py build the same synthetic rigs through the reference's builder API and step them with
+// the reference's `World::step_substeps`, then read the state back.
+//
+// Nothing of the product links this file. Every call mirrors one reference entry point:
+//   ref_world_new / ref_step_substeps   -> bl::phys::World, World::step_substeps   (src/phys/world.h:150-168)
+//   ref_set_terrain                     -> Heightfield::create + has_terrain + update_bounds (src/phys/static_world.h:52-90)
+//   ref_add_box / ref_build_grid        -> StaticWorld::add_box / build_grid        (src/phys/static_world.h:193-195)
+//   ref_add_body                        -> SoftBody::add_node / add_beam / finalize (src/phys/softbody.h:953-973)
+//   ref_jobs_init                       -> JobSystem::get().init                   (src/core/jobs.h:22)
+#include "core/jobs.h"
+#include "phys/world.h"
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+using namespace bl;
+using namespace bl::phys;
+
+struct RefWorld {
+    World w;
+    std::vector<SoftBody*> bodies;
+};
+
+// per-body knobs of SoftBody that the GPU path supports (softbody.h:650-700)
+struct RefBodyParams {
+    float ground_friction;
+    float bounce;
+    float contact_push_max;
+    float contact_slop;
+    float collision_radius;
+    int32_t allow_deform;
+    int32_t allow_break;
+    int32_t ductile;
+    int32_t can_sleep;
+    float sleep_speed;
+};
+
+extern "C" {
+
+void ref_jobs_init(int workers) { JobSystem::get().init(workers); }
+void ref_jobs_shutdown() { JobSystem::get().shutdown(); }
+int ref_jobs_threads() { return JobSystem::get().num_threads(); }
+
+RefWorld* ref_world_new() { return new RefWorld(); }
+void ref_world_free(RefWorld* r) { delete r; }
+
+void ref_world_settings(RefWorld* r, float gx, float gy, float gz, float dt, int sleeping, int multithreaded, int inter_body, float sleep_speed,
+                        float sleep_time) {
+    WorldSettings& s = r->w.settings;
+    s.gravity = vec3(gx, gy, gz);
+    s.dt = dt;
+    s.sleeping = sleeping != 0;
+    s.multithreaded = multithreaded != 0;
+    s.inter_body_collisions = inter_body != 0;
+    s.sleep_speed = sleep_speed;
+    s.sleep_time = sleep_time;
+}
+
+// heights / surfaces: nz rows of nx samples, x fastest
+void ref_set_terrain(RefWorld* r, int nx, int nz, float cell, float ox, float oz, const float* heights, const uint8_t* surfaces) {
+    StaticWorld& st = r->w.statics;
+    st.terrain.create(nx, nz, cell, vec2(ox, oz));
+    for (int z = 0; z < nz; z++)
+        for (int x = 0; x < nx; x++) {
+            st.terrain.h(x, z) = heights[(size_t)z * nx + x];
+            if (surfaces) st.terrain.surf(x, z) = surfaces[(size_t)z * nx + x];
+        }
+    st.has_terrain = true;
+    st.terrain.update_bounds();
+}
+
+void ref_add_box(RefWorld* r, float cx, float cy, float cz, float hx, float hy, float hz, float qx, float qy, float qz, float qw, int surface) {
+    r->w.statics.add_box(vec3(cx, cy, cz), vec3(hx, hy, hz), quat(qx, qy, qz, qw), (uint8_t)surface);
+}
+
+void ref_add_cylinder(RefWorld* r, float bx, float by, float bz, float radius, float height, int surface) {
+    StaticCylinder c;
+    c.base = vec3(bx, by, bz);
+    c.radius = radius;
+    c.height = height;
+    c.surface = (uint8_t)surface;
+    r->w.statics.cylinders.push_back(c);
+}
+
+void ref_build_grid(RefWorld* r) { r->w.statics.build_grid(); }
+void ref_set_kill_y(RefWorld* r, float y) { r->w.statics.kill_y = y; }
+
+// Builds one body through the reference's builder calls, in this order: add_node (and its velocity, friction, radius),
+// add_beam, add_triangle, finalize; then World::add_body. Returns the body's index in this driver.
+int ref_add_body(RefWorld* r, int n_nodes, const float* pos, const float* vel, const float* mass, const uint16_t* nflags, const float* friction,
+                 const float* radius, int n_beams, const uint32_t* ab, const float* k, const float* d, const float* strength, const float* deform,
+                 const uint8_t* btype, const uint8_t* bflags, int n_tris, const uint32_t* tri, const RefBodyParams* p) {
+    auto b = std::make_unique<SoftBody>();
+    b->name = "body" + std::to_string(r->bodies.size());
+    for (int i = 0; i < n_nodes; i++) {
+        const uint32_t id = b->add_node(vec3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]), mass[i], nflags[i]);
+        b->nodes[id].v = vec3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+        b->info[id].friction = friction[i];
+        b->info[id].radius = radius[i];
+    }
+    for (int j = 0; j < n_beams; j++) b->add_beam(ab[2 * j], ab[2 * j + 1], k[j], d[j], strength[j], deform[j], btype[j], bflags[j]);
+    for (int t = 0; t < n_tris; t++) b->add_triangle(tri[3 * t], tri[3 * t + 1], tri[3 * t + 2]);
+    b->ground_friction = p->ground_friction;
+    b->bounce = p->bounce;
+    b->contact_push_max = p->contact_push_max;
+    b->contact_slop = p->contact_slop;
+    b->collision_radius = p->collision_radius;
+    b->allow_deform = p->allow_deform != 0;
+    b->allow_break = p->allow_break != 0;
+    b->ductile = p->ductile != 0;
+    b->can_sleep = p->can_sleep != 0;
+    b->sleep_speed = p->sleep_speed;
+    b->finalize();
+    r->bodies.push_back(r->w.add_body(std::move(b)));
+    return (int)r->bodies.size() - 1;
+}
+
+void ref_step_substeps(RefWorld* r, int n) { r->w.step_substeps(n); }
+
+int ref_body_nodes(RefWorld* r, int body) { return (int)r->bodies[body]->nodes.size(); }
+int ref_body_beams(RefWorld* r, int body) { return (int)r->bodies[body]->beams.size(); }
+
+// pos, vel: 3 floats a node; inv_mass, mass: 1
+void ref_get_nodes(RefWorld* r, int body, float* pos, float* vel, float* inv_mass, float* mass) {
+    const SoftBody& b = *r->bodies[body];
+    for (size_t i = 0; i < b.nodes.size(); i++) {
+        const Node& x = b.nodes[i];
+        std::memcpy(pos + 3 * i, &x.p, 12);
+        std::memcpy(vel + 3 * i, &x.v, 12);
+        if (inv_mass) inv_mass[i] = x.inv_mass;
+        if (mass) mass[i] = x.mass;
+    }
+}
+
+void ref_set_nodes(RefWorld* r, int body, const float* pos, const float* vel) {
+    SoftBody& b = *r->bodies[body];
+    for (size_t i = 0; i < b.nodes.size(); i++) {
+        std::memcpy(&b.nodes[i].p, pos + 3 * i, 12);
+        std::memcpy(&b.nodes[i].v, vel + 3 * i, 12);
+    }
+}
+
+// the beams' state: rest length, yield limits, strength, last force, flags
+void ref_get_beams(RefWorld* r, int body, float* L, float* max_pos, float* max_neg, float* strength, float* stress, uint8_t* flags) {
+    const SoftBody& b = *r->bodies[body];
+    for (size_t j = 0; j < b.beams.size(); j++) {
+        const Beam& bm = b.beams[j];
+        L[j] = bm.L, max_pos[j] = bm.max_pos, max_neg[j] = bm.max_neg, strength[j] = bm.strength, stress[j] = bm.stress, flags[j] = bm.flags;
+    }
+}
+
+// out[0..5] aabb min/max, out[6] max_speed, out[7] sleeping, out[8] static_contacts (last frame), out[9] broken beams,
+// out[10] sleep_timer
+void ref_get_body(RefWorld* r, int body, float* out) {
+    const SoftBody& b = *r->bodies[body];
+    out[0] = b.aabb.mn.x, out[1] = b.aabb.mn.y, out[2] = b.aabb.mn.z;
+    out[3] = b.aabb.mx.x, out[4] = b.aabb.mx.y, out[5] = b.aabb.mx.z;
+    out[6] = b.max_speed;
+    out[7] = b.sleeping ? 1.0f : 0.0f;
+    out[8] = (float)b.static_contacts;
+    out[9] = (float)b.stats.broken_beams;
+    out[10] = b.sleep_timer;
+}
+
+} // extern "C"

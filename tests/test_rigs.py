@@ -1,0 +1,46 @@
+"""The seeded rig generators (beamlab_b200.rigs): shapes, determinism, the truss car's beam count."""
+import numpy as np
+
+from beamlab_b200 import rigs
+
+
+def test_trng_is_xorshift32():
+    r = rigs.TRng(1)
+    s = (1 * 2654435761 + 1) & 0xFFFFFFFF
+    s ^= (s << 13) & 0xFFFFFFFF
+    s ^= s >> 17
+    s ^= (s << 5) & 0xFFFFFFFF
+    assert r.next() == s
+    u = [float(r.uni()) for _ in range(2000)]
+    assert 0.0 <= min(u) and max(u) < 1.0 and abs(np.mean(u) - 0.5) < 0.03
+
+
+def test_truss_car_shape():
+    rig = rigs.truss_car(1)
+    n, m = rigs.rig_counts(rig)
+    assert n == 400
+    assert 3000 <= m <= 3300  # pairs within sqrt(3) * 0.25 m of the jittered lattice
+    b = rig["bodies"][0]
+    assert b["mass"].min() >= 4.0 and b["mass"].max() <= 6.0
+    k = b["k"].astype(np.float64)
+    assert 1.7e6 < np.median(k) < 2.3e6 and 0.25 < np.std(np.log(k)) < 0.35
+    d = b["pos"][b["ab"][:, 0]] - b["pos"][b["ab"][:, 1]]
+    assert np.sqrt((d.astype(np.float64) ** 2).sum(1)).max() <= np.sqrt(3) * 0.25 + 1e-6
+
+
+def test_rigs_are_deterministic():
+    a, b = rigs.truss_car(5), rigs.truss_car(5)
+    for k in ("pos", "mass", "k", "ab"):
+        assert np.array_equal(a["bodies"][0][k], b["bodies"][0][k])
+    c = rigs.truss_car(6)
+    assert not np.array_equal(a["bodies"][0]["pos"], c["bodies"][0]["pos"])
+
+
+def test_fleet_sizes():
+    rig = rigs.fleet(32, seed=3, terrain_samples=257, terrain_size=400.0)
+    sizes = np.asarray([len(b["mass"]) for b in rig["bodies"]])
+    assert len(sizes) == 32
+    assert sizes.min() >= 200 and sizes.max() <= 26000
+    assert 1000 < np.median(sizes) < 8000
+    t = rig["statics"]["terrain"]
+    assert t["heights"].shape == (257, 257) and np.abs(t["heights"]).max() <= 2.6
