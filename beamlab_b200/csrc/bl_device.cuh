@@ -3,11 +3,13 @@
 // Every floating-point expression below is written in the reference's operation order (src/core/math.h vector ops,
 // src/phys/softbody.cpp, src/phys/static_world.cpp, src/phys/world.cpp) and the library is compiled with
 // --fmad=false and IEEE division / square root, so each operation rounds once, as in the reference built without FMA
-// contraction: a node's state after any number of substeps is bitwise the reference's (exp/pow excepted: see
-// bl_expf / bl_powf).
+// contraction: a node's state after any number of substeps is bitwise the reference's, given the same exp and pow
+// (bl_math.cuh).
 #pragma once
 
 #include <cstdint>
+
+#include "bl_math.cuh"
 
 namespace blg {
 
@@ -108,11 +110,6 @@ __device__ __forceinline__ float smax(float a, float b) { return (a < b) ? b : a
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
 __device__ __forceinline__ float signf(float v) { return v < 0.0f ? -1.0f : 1.0f; }
 __device__ __forceinline__ v3 vabs(v3 a) { return {fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
-
-// exp and pow of the ground friction's Stribeck curve: evaluated in double precision and rounded once to float, i.e.
-// the correctly rounded float result in all but vanishingly rare cases - the value the reference's libm returns
-__device__ __forceinline__ float bl_expf(float x) { return (float)exp((double)x); }
-__device__ __forceinline__ float bl_powf(float x, float y) { return (float)pow((double)x, (double)y); }
 
 // float atomics through the integer order of IEEE floats (no NaN)
 __device__ __forceinline__ void atomic_min_f(float* a, float v) {

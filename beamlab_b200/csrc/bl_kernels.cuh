@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
         const float4 pa = nd[2 * e.x], va = nd[2 * e.x + 1], pb = nd[2 * e.y], vb = nd[2 * e.y + 1];
         const v3 dis = V(pa.x - pb.x, pa.y - pb.y, pa.z - pb.z);
         const float len2 = dot(dis, dis);
-        if (len2 >= 1e-12f) {
+        if (!(len2 < 1e-12f)) { // (a NaN length goes on, as in the reference)
             float4 s = bst[j]; // L, max_pos, max_neg, strength
             const float2 c = kd[j];
             const float inv_len = 1.0f / sqrtf(len2);
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int body = -1;
-    v3 p = V(0, 0, 0);
+    v3 p = V(0, 0, 0), pmx = V(0, 0, 0);
     float v2 = 0.0f, v2start = 0.0f;
     int contact = 0;
     bool live = false;
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
             float inv_mass = P.w;
             const uint32_t flags = (uint32_t)inf.x;
             // ---- static contact (World::collide_static)
-            if ((flags & NF_GROUND) && inv_mass > 0) {
+            if (!(!(flags & NF_GROUND) || inv_mass <= 0)) {
                 if (pos.y < st.kill_y) {
                     vel = V(0, 0, 0);
                     inv_mass = 0;
@@ -432,7 +432,9 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
             }
             nd[2 * i] = make_float4(pos.x, pos.y, pos.z, inv_mass);
             nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, m);
-            p = pos;
+            // the bounds skip a non-finite coordinate as the reference's vmin / vmax do (a NaN never compares less)
+            p = V(pos.x == pos.x ? pos.x : 1e30f, pos.y == pos.y ? pos.y : 1e30f, pos.z == pos.z ? pos.z : 1e30f);
+            pmx = V(pos.x == pos.x ? pos.x : -1e30f, pos.y == pos.y ? pos.y : -1e30f, pos.z == pos.z ? pos.z : -1e30f);
             v2 = smax(v2, v2start);
         }
     }
@@ -440,7 +442,7 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
     const int b0 = __shfl_sync(0xffffffffu, body, 0);
     const bool uniform = __all_sync(0xffffffffu, body == b0 && live);
     if (uniform) {
-        float mnx = p.x, mny = p.y, mnz = p.z, mxx = p.x, mxy = p.y, mxz = p.z, vv = v2;
+        float mnx = p.x, mny = p.y, mnz = p.z, mxx = pmx.x, mxy = pmx.y, mxz = pmx.z, vv = v2;
         int cc = contact;
         for (int o = 16; o > 0; o >>= 1) {
             mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
@@ -462,7 +464,7 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
     } else if (live) {
         Body& B = bodies[body];
         atomic_min_f(&B.acc_mn[0], p.x), atomic_min_f(&B.acc_mn[1], p.y), atomic_min_f(&B.acc_mn[2], p.z);
-        atomic_max_f(&B.acc_mx[0], p.x), atomic_max_f(&B.acc_mx[1], p.y), atomic_max_f(&B.acc_mx[2], p.z);
+        atomic_max_f(&B.acc_mx[0], pmx.x), atomic_max_f(&B.acc_mx[1], pmx.y), atomic_max_f(&B.acc_mx[2], pmx.z);
         atomic_max_f(&B.acc_v2, v2);
         if (contact) atomicAdd(&B.acc_contacts, contact);
     }
@@ -588,9 +590,11 @@ __device__ void body_bounds(Body& B, const float4* __restrict__ nd) {
     __syncthreads();
     for (int i = threadIdx.x; i < B.nnodes; i += blockDim.x) {
         const float4 p = nd[2 * (B.node0 + i)], v = nd[2 * (B.node0 + i) + 1];
-        atomic_min_f(&s_mn[0], p.x), atomic_min_f(&s_mn[1], p.y), atomic_min_f(&s_mn[2], p.z);
-        atomic_max_f(&s_mx[0], p.x), atomic_max_f(&s_mx[1], p.y), atomic_max_f(&s_mx[2], p.z);
-        atomic_max_f(&s_v, length(V(v.x, v.y, v.z)));
+        if (p.x == p.x) atomic_min_f(&s_mn[0], p.x), atomic_max_f(&s_mx[0], p.x);
+        if (p.y == p.y) atomic_min_f(&s_mn[1], p.y), atomic_max_f(&s_mx[1], p.y);
+        if (p.z == p.z) atomic_min_f(&s_mn[2], p.z), atomic_max_f(&s_mx[2], p.z);
+        const float sp = length(V(v.x, v.y, v.z));
+        if (sp == sp) atomic_max_f(&s_v, sp);
     }
     __syncthreads();
     if (threadIdx.x == 0) {

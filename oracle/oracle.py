@@ -19,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIBS = {
     "parity": os.path.join(HERE, "_ref", "libbeamlab_ref_parity.so"),
+    "libm": os.path.join(HERE, "_ref", "libbeamlab_ref_libm.so"),
     "timing": os.path.join(HERE, "_ref", "libbeamlab_ref_timing.so"),
 }
 
@@ -62,7 +63,7 @@ def _load(path: str, prefix: str) -> C.CDLL:
         "world_free": ([vp], None),
         "world_settings": ([vp, f, f, f, f, i, i, i, f, f], None),
         "set_terrain": ([vp, i, i, f, f, f, fp, u8p], None),
-        "add_box": ([vp, f, f, f, f, f, f, f, f, f, f, i], None),
+        "add_box": ([vp, f, f, f, f, f, f, f, f, f, f, i, f], None),
         "add_cylinder": ([vp, f, f, f, f, f, i], None),
         "build_grid": ([vp], None),
         "set_kill_y": ([vp, f], None),
@@ -125,7 +126,7 @@ class _OracleWorld:
         for b in statics.get("boxes", []):
             q = b.get("rot", (0.0, 0.0, 0.0, 1.0))
             self._fn("add_box")(self._w, *map(float, b["center"]), *map(float, b["half"]), *map(float, q),
-                                int(b.get("surface", 3)))
+                                int(b.get("surface", 3)), float(b.get("max_force", 0.0)))
         for c in statics.get("cylinders", []):
             self._fn("add_cylinder")(self._w, *map(float, c["base"]), float(c["radius"]), float(c["height"]),
                                      int(c.get("surface", 3)))

@@ -73,8 +73,10 @@ void ref_set_terrain(RefWorld* r, int nx, int nz, float cell, float ox, float oz
     st.terrain.update_bounds();
 }
 
-void ref_add_box(RefWorld* r, float cx, float cy, float cz, float hx, float hy, float hz, float qx, float qy, float qz, float qw, int surface) {
+void ref_add_box(RefWorld* r, float cx, float cy, float cz, float hx, float hy, float hz, float qx, float qy, float qz, float qw, int surface,
+                 float max_force) {
     r->w.statics.add_box(vec3(cx, cy, cz), vec3(hx, hy, hz), quat(qx, qy, qz, qw), (uint8_t)surface);
+    r->w.statics.boxes.back().max_force = max_force;
 }
 
 void ref_add_cylinder(RefWorld* r, float bx, float by, float bz, float radius, float height, int surface) {

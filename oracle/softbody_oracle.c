@@ -3,6 +3,7 @@
  * Built with -ffp-contract=off: every float operation below happens in the reference's order, one rounding each, as the
  * reference's parity build does. Citations are to files of the reference project (zenkovich/beamlab). */
 #include "softbody_oracle.h"
+#include "orc_math.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -239,15 +240,16 @@ static m3 quat_to_m3(float x, float y, float z, float w) {
     return m;
 }
 
-/* StaticWorld::add_box + StaticBox::update_aabb (static_world.cpp:242-246, 298-306) */
-void orc_add_box(OrcWorld* w, float cx, float cy, float cz, float hx, float hy, float hz, float qx, float qy, float qz, float qw, int surface) {
+/* StaticWorld::add_box + StaticBox::update_aabb (static_world.cpp:242-246, 298-306); max_force: StaticBox::max_force */
+void orc_add_box(OrcWorld* w, float cx, float cy, float cz, float hx, float hy, float hz, float qx, float qy, float qz, float qw, int surface,
+                 float max_force) {
     w->boxes = (box_t*)realloc(w->boxes, sizeof(box_t) * (size_t)(w->nboxes + 1));
     box_t* b = &w->boxes[w->nboxes++];
     b->center = V(cx, cy, cz);
     b->half = V(hx, hy, hz);
     b->rot = quat_to_m3(qx, qy, qz, qw);
     b->surface = (uint8_t)surface;
-    b->max_force = 0;
+    b->max_force = max_force;
     const v3 e = vadd(vadd(vmul(vabs_(b->rot.c[0]), b->half.x), vmul(vabs_(b->rot.c[1]), b->half.y)), vmul(vabs_(b->rot.c[2]), b->half.z));
     b->aabb.mn = vsub(b->center, e);
     b->aabb.mx = vadd(b->center, e);
@@ -449,9 +451,9 @@ static v3 primitive_collision(v3 F, v3 vel, float mass, v3 normal, float dt, con
             const float G = R * gm->strength * friction_coef;
             const float stop = mass * sv / dt;
             if (sv < gm->va && G > 0 && vlen(slipF) <= gm->ms * G) {
-                out = vadd(out, vsub(vsub(vmul(normal, R), vmul(slip, fmin_(gm->ms * G * (1.0f - expf(-sv / gm->va)), stop))), slipF));
+                out = vadd(out, vsub(vsub(vmul(normal, R), vmul(slip, fmin_(gm->ms * G * (1.0f - orc_expf(-sv / gm->va)), stop))), slipF));
             } else {
-                const float g = gm->mc + (gm->ms - gm->mc) * expf(-powf(sv / gm->vs, gm->alpha));
+                const float g = gm->mc + (gm->ms - gm->mc) * orc_expf(-orc_powf(sv / gm->vs, gm->alpha));
                 out = vadd(out, vsub(vmul(normal, R), vmul(slip, fmin_((g + fmin_(gm->t2 * sv, 5.0f)) * G, fmax_(0.0f, stop + vdot(slipF, slip))))));
             }
         }
@@ -814,3 +816,7 @@ void orc_get_body(OrcWorld* w, int body, float* out) {
     out[9] = (float)b->broken_beams;
     out[10] = b->sleep_timer;
 }
+
+/* the portable exp / pow (orc_math.h), for tests of their accuracy against libm */
+float orc_math_exp(float x) { return orc_expf(x); }
+float orc_math_pow(float x, float y) { return orc_powf(x, y); }

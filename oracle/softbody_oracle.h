@@ -36,7 +36,8 @@ void orc_world_free(OrcWorld* w);
 void orc_world_settings(OrcWorld* w, float gx, float gy, float gz, float dt, int sleeping, int multithreaded, int inter_body, float sleep_speed,
                         float sleep_time);
 void orc_set_terrain(OrcWorld* w, int nx, int nz, float cell, float ox, float oz, const float* heights, const uint8_t* surfaces);
-void orc_add_box(OrcWorld* w, float cx, float cy, float cz, float hx, float hy, float hz, float qx, float qy, float qz, float qw, int surface);
+void orc_add_box(OrcWorld* w, float cx, float cy, float cz, float hx, float hy, float hz, float qx, float qy, float qz, float qw, int surface,
+                 float max_force);
 void orc_add_cylinder(OrcWorld* w, float bx, float by, float bz, float radius, float height, int surface);
 void orc_build_grid(OrcWorld* w);
 void orc_set_kill_y(OrcWorld* w, float y);
@@ -54,6 +55,10 @@ void orc_get_body(OrcWorld* w, int body, float* out);
 /* single ground-contact response (static_world.cpp:8-51) for unit tests of the formula */
 void orc_primitive_collision(const float* F, const float* vel, float mass, const float* normal, float dt, int surface, float pen, float friction_coef,
                              float push_max, float slop, float restitution, float* out);
+
+/* the oracle's portable exp and pow (orc_math.h) */
+float orc_math_exp(float x);
+float orc_math_pow(float x, float y);
 
 #ifdef __cplusplus
 }

@@ -106,3 +106,42 @@ def test_port_repair_matches_reference(port_lib, ref_lib):
     a, c = ws[0].nodes(0), ws[1].nodes(0)
     assert np.all(np.isfinite(a["pos"]))
     assert np.array_equal(bits(a["pos"]), bits(c["pos"])) and np.array_equal(bits(a["vel"]), bits(c["vel"]))
+
+
+def test_portable_exp_pow_within_one_ulp_of_libm(port_lib):
+    """The oracle's exp / pow (which the GPU evaluates identically) against libm's expf / powf: at most 1 ulp apart."""
+    import ctypes as C
+    lib = C.CDLL(port_lib)
+    lib.orc_math_exp.argtypes, lib.orc_math_exp.restype = [C.c_float], C.c_float
+    lib.orc_math_pow.argtypes, lib.orc_math_pow.restype = [C.c_float, C.c_float], C.c_float
+    libm = C.CDLL("libm.so.6")
+    libm.expf.argtypes, libm.expf.restype = [C.c_float], C.c_float
+    libm.powf.argtypes, libm.powf.restype = [C.c_float, C.c_float], C.c_float
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([-rng.exponential(3.0, 20000), rng.uniform(-80, 80, 5000), [0.0, -0.0, 1e-30, -87.0, 88.0]])
+    worst = 0
+    for x in xs.astype(np.float32):
+        a, b = np.float32(lib.orc_math_exp(float(x))), np.float32(libm.expf(float(x)))
+        worst = max(worst, abs(int(np.int32(a.view(np.int32))) - int(np.int32(b.view(np.int32)))))
+    assert worst <= 1
+    worst = 0
+    for x, y in zip(rng.uniform(0, 20, 20000).astype(np.float32), rng.choice([2.0, 1.5, 0.5, 3.0], 20000).astype(np.float32)):
+        a, b = np.float32(lib.orc_math_pow(float(x), float(y))), np.float32(libm.powf(float(x), float(y)))
+        worst = max(worst, abs(int(np.int32(a.view(np.int32))) - int(np.int32(b.view(np.int32)))))
+    assert worst <= 1
+    assert lib.orc_math_pow(0.0, 2.0) == 0.0 and lib.orc_math_pow(3.0, 0.0) == 1.0
+
+
+def test_port_within_tolerance_of_reference_with_libm(port_lib):
+    """Against the reference as it runs (libm's exp / pow): the truss car's nodes within 1e-4 m after 2,000 substeps."""
+    from oracle.oracle import PortWorld, RefWorld, build_world, ref_available
+    if not ref_available("libm"):
+        pytest.skip("the compiled reference (oracle/_ref) is not present")
+    rig = rigs.truss_car(1)
+    ref = build_world(RefWorld, rig, flavour="libm", multithreaded=False)
+    port = build_world(PortWorld, rig)
+    for _ in range(100):
+        ref.step_substeps(20)
+        port.step_substeps(20)
+    d = np.abs(ref.nodes(0)["pos"].astype(np.float64) - port.nodes(0)["pos"]).max()
+    assert d <= 1e-4, d
