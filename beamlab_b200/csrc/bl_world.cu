@@ -100,6 +100,9 @@ struct bl_gpu_ctx {
     std::map<int, ProfGraph> pgraphs; // frames with a timing event between kernels (bl_gpu_profile_frame)
     int64_t launches = 0, total_substeps = 0;
     int last_substeps = 0;
+    // the stream of the last enqueued work: work on another stream first waits for it, so calls stay ordered
+    cudaStream_t last_stream = nullptr;
+    cudaEvent_t order_event = nullptr;
 };
 
 #define BL_CUDA(ctx, call)                                                                                                                   \
@@ -328,6 +331,16 @@ static int commit_bodies(bl_gpu_ctx* c) {
     return BL_GPU_OK;
 }
 
+// Orders work about to be enqueued on s after everything the context enqueued before, on whichever stream.
+static int order_on(bl_gpu_ctx* c, cudaStream_t s) {
+    if (c->last_stream != s) {
+        BL_CUDA(c, cudaEventRecord(c->order_event, c->last_stream));
+        BL_CUDA(c, cudaStreamWaitEvent(s, c->order_event, 0));
+        c->last_stream = s;
+    }
+    return BL_GPU_OK;
+}
+
 static int ensure_committed(bl_gpu_ctx* c) {
     int rc;
     if (c->statics_dirty && (rc = commit_statics(c))) return rc;
@@ -340,7 +353,7 @@ static int ensure_committed(bl_gpu_ctx* c) {
 static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev = nullptr) {
     int q = 0;
     auto mark = [&]() {
-        if (ev) cudaEventRecord(ev[q++], s);
+        if (ev) cudaEventRecordWithFlags(ev[q++], s, cudaEventRecordExternal); // (a timing node of the captured graph)
     };
     mark();
     const float dt = c->cfg.dt;
@@ -419,6 +432,8 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     cudaError_t e;
     if ((e = cudaSetDevice(c0.device)) != cudaSuccess) return fail(e);
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&c->order_event, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    c->last_stream = c->stream;
     if ((e = cudaMemcpyToSymbol(c_ground, kGroundModels, sizeof(kGroundModels))) != cudaSuccess) return fail(e);
     if ((e = c->deverr.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(c->deverr.p, 0, sizeof(uint32_t))) != cudaSuccess) return fail(e);
@@ -434,6 +449,7 @@ int bl_gpu_destroy(bl_gpu_ctx* c) {
     free_device(c);
     free_statics(c);
     c->deverr.free_();
+    if (c->order_event) cudaEventDestroy(c->order_event);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return BL_GPU_OK;
@@ -565,6 +581,7 @@ int bl_gpu_step_substeps(bl_gpu_ctx* c, int32_t n, void* stream) {
         BL_CUDA(c, e);
         it = c->graphs.emplace(n, ex).first;
     }
+    if ((rc = order_on(c, s))) return rc;
     BL_CUDA(c, cudaGraphLaunch(it->second, s));
     c->launches += 2 * (int64_t)n + 3;
     return BL_GPU_OK;
@@ -687,6 +704,7 @@ static int all_nodes_copy(bl_gpu_ctx* c, bl_node* host, int32_t n, void* stream,
     if (n != c->N) return BL_GPU_EINVAL;
     if (n == 0) return BL_GPU_OK;
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    if ((rc = order_on(c, s))) return rc;
     if (to_device) BL_CUDA(c, cudaMemcpyAsync(c->nd.p, host, sizeof(bl_node) * (size_t)n, cudaMemcpyHostToDevice, s));
     else BL_CUDA(c, cudaMemcpyAsync(host, c->nd.p, sizeof(bl_node) * (size_t)n, cudaMemcpyDeviceToHost, s));
     return BL_GPU_OK;
@@ -722,20 +740,24 @@ int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profil
         it = c->pgraphs.emplace(n, pg).first;
     }
     const ProfGraph& pg = it->second;
+    if ((rc = order_on(c, s))) return rc;
     BL_CUDA(c, cudaGraphLaunch(pg.exec, s));
     BL_CUDA(c, cudaStreamSynchronize(s));
     c->launches += 2 * (int64_t)n + 3;
     c->total_substeps += n;
     c->last_substeps = n;
+    cudaError_t terr = cudaSuccess;
     auto el = [&](int a, int b) {
         float ms = 0;
-        cudaEventElapsedTime(&ms, pg.events[a], pg.events[b]);
+        const cudaError_t e = cudaEventElapsedTime(&ms, pg.events[a], pg.events[b]);
+        if (e != cudaSuccess) terr = e;
         return ms;
     };
     out->begin_ms = el(0, 1);
     for (int k = 0; k < n; k++) out->beams_ms += el(1 + 2 * k, 2 + 2 * k), out->nodes_ms += el(2 + 2 * k, 3 + 2 * k);
     out->finish_ms = el(1 + 2 * n, 3 + 2 * n);
     out->frame_ms = el(0, 3 + 2 * n);
+    BL_CUDA(c, terr);
     return BL_GPU_OK;
 }
 
