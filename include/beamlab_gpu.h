@@ -203,6 +203,21 @@ typedef struct {
 } bl_frame_profile;
 int bl_gpu_profile_frame(bl_gpu_ctx* ctx, int32_t n, void* stream, bl_frame_profile* out);
 
+/* One substep - gravity, the beams' spring-dampers with yield and breaking, symplectic Euler - of one body whose
+ * device buffers the caller owns, for callers that cannot let the library allocate GPU memory: their memory belongs to
+ * another allocator (an engine's or a framework's pool), or they step where allocation is forbidden (a real-time frame
+ * loop, a CUDA stream capture). No counterpart in the reference: it is the body part of bl_gpu_step_substeps without
+ * a context, without statics and without the frame's bookkeeping, and gives the same node and beam states.
+ * nodes / beams: device arrays of bl_node / bl_beam (in and out); inc_ptr (n_nodes + 1) / inc (2 n_beams): device
+ * arrays listing each node's beams in beam order, a beam's index with bit 31 set where the node is its b end.
+ * Allocates nothing: its per-beam scratch is a fixed device array of BL_GPU_NOALLOC_MAX_BEAMS entries (16 MiB, held by
+ * every GPU that loads the library until exit), so more beams return BL_GPU_ELIMIT. The first call on a device looks
+ * up that array's address and should come before any stream capture. Calls whose kernels overlap on the GPU share the
+ * scratch and race; order them on one stream. Asynchronous on `stream` (NULL: the legacy default stream). */
+#define BL_GPU_NOALLOC_MAX_BEAMS (1 << 20)
+int bl_gpu_substep_noalloc(bl_node* nodes, int32_t n_nodes, bl_beam* beams, int32_t n_beams, const int32_t* inc_ptr, const int32_t* inc,
+                           const float gravity[3], float dt, int32_t allow_deform, int32_t allow_break, int32_t ductile, void* stream);
+
 const char* bl_gpu_error_string(int code);
 int bl_gpu_last_cuda_error(bl_gpu_ctx* ctx);
 int bl_gpu_abi_version(void);
