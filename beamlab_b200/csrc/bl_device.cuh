@@ -81,6 +81,8 @@ struct alignas(64) Body {
     float aabb_mn[3], aabb_mx[3];
     int static_contacts, broken_beams, repaired;
     int fell_asleep, needs_repair;
+    int is_fem;              // the body has a FEM frame: its nodes are integrated after the frame's implicit step
+    int has_ext;             // constant node forces (bl_gpu_set_node_force) are added after gravity
     int box_ids[kMaxCand];
     int cyl_ids[kMaxCand];
 };

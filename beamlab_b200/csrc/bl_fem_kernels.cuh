@@ -1,0 +1,629 @@
+// Kernels of the implicit FEM shell step (FemFrame, src/phys/frame_fem.cpp) for bodies of triangle elements.
+//
+// Per substep, for every frame:
+//   k_fem_begin        frame nodes: double positions re-synced where something else moved a node (frame_fem.cpp:1866-1872)
+//   k_tri_eval         triangles: co-rotated frame, deformation, -K d, K v, membrane tension's geometric stiffness
+//                      (tri_kinematics + eval_tris, frame_fem.cpp:1584-1621, 1661-1831; elastic sections)
+//   (k_nodes)          the frame bodies' node forces, their triangles' forces and torques gathered in the reference's
+//                      order (gather_forces, frame_fem.cpp:2080-2105)
+//   k_fem_assemble     columns: the blocks of (M + (theta h^2 + beta h) K + theta h^2 Kg) and the right side
+//                      h f - (theta_d h^2 + beta h) K v (gather_part, frame_fem.cpp:916-1086)
+//   k_fem_chol_level / k_fem_update_level: the right-looking block Cholesky level by level of the elimination tree:
+//                      the level's columns factored (chol6, right_solve_lt), then their updates T -= P Q^T, one warp
+//                      per target block (frame_fem.cpp:2193-2220, 2887-2919)
+//   k_fem_forward_level / k_fem_backward_level: L y = r and L^T x = y by levels (frame_fem.cpp:2944-2954)
+//   k_fem_velocity     columns: the new velocities to forces m dv / step, spins advanced, safety clamps
+//                      (frame_fem.cpp:2998-3025)
+//   k_fem_integrate    the frame bodies' nodes: SoftBody::integrate_nodes, then FemFrame::sync_positions
+//                      (softbody.cpp:769-795, frame_fem.cpp:3407-3422)
+// The factorization's sums per block are the reference's (same 6 x 6 loops, same order of updates); the element
+// kernels call the GPU's atan2 / sin / cos, which differ from libm's in the last bit, so the step matches the reference
+// within a tolerance, not bitwise.
+#pragma once
+
+#include "bl_device.cuh"
+
+namespace blg {
+
+struct FemSecDev {
+    float E, nu, rho, t, damping, drill;
+};
+
+// All frames of the context, back to back (frame nodes, triangles, columns, blocks in one index space each)
+struct FemDev {
+    int nf, ntri, nblk;
+    const int* fnode;        // frame node -> global body node
+    const int* fbody;        // frame node -> body
+    const int* perm;         // column -> frame node
+    const int* iperm;        // frame node -> column
+    double* xd;              // 3 / frame node
+    float4* q;               // orientation (x y z w)
+    float4* w;               // angular velocity
+    const float* inertia;
+    float4* torque;
+    const int4* tn;          // triangle: frame nodes, section
+    const float* tX;         // 6 / triangle
+    const float4* tr0;       // 3 / triangle
+    const float* tk;         // 162 / triangle
+    const uint8_t* tbroken;
+    float4* tf;              // 3 / triangle: corner forces
+    float4* tt;              // 3 / triangle: corner torques
+    float* ttan;             // 18 / triangle: e1 e2 e3, g[3][3]
+    double* tkv;             // 18 / triangle
+    uint8_t* ton;
+    const FemSecDev* sec;
+    const int* col_ptr;
+    const int* row;
+    const int* gdiag_ptr;
+    const int2* gdiag;       // (triangle, corner)
+    const int* goff_ptr;
+    const int4* goff;        // (triangle, row corner, column corner)
+    double* diag;            // 36 / column
+    double* off;             // 36 / block
+    double* rhs;             // 6 / column
+    double* dinv;            // 6 / column
+    uint8_t* fixed;          // / column
+    const int* grp_tgt;      // per level, per target its columns update: the target (column k: k; block p: nf + p)
+    const int* grp_ptr;      // ... and its updates in gu
+    const int2* gu;          // (pj, pi) of each update, in the order of its source column
+    const int* col_comp;     // column -> component
+    int* comp_fail;
+    const int* rb_ptr;       // / column: the blocks in its row, in the order of their columns
+    const int2* rb;          // (block, column)
+    const int* lvl_col;      // columns grouped by level
+    const double* ch2;       // / column: theta h^2
+    const double* chd;       // / column: theta_d h^2 (numerical dissipation)
+    int* body_failures;      // / body
+    int* body_clamps;        // / body
+    float h, step;
+};
+
+// ------------------------------------------------------------------------------------------ quaternions (math.h:105-215)
+struct q4 {
+    float x, y, z, w;
+};
+__device__ __forceinline__ q4 qmul(q4 a, q4 b) {
+    return {a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x, a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w,
+            a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z};
+}
+__device__ __forceinline__ q4 qconj(q4 q) { return {-q.x, -q.y, -q.z, q.w}; }
+__device__ __forceinline__ q4 qnormalize(q4 q) {
+    const float l = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    if (!(l > 1e-12f)) return {0, 0, 0, 1};
+    const float i = 1.0f / l;
+    return {q.x * i, q.y * i, q.z * i, q.w * i};
+}
+__device__ __forceinline__ q4 qfrom_mat3(v3 c0, v3 c1, v3 c2) {
+    const float m00 = c0.x, m11 = c1.y, m22 = c2.z;
+    const float tr = m00 + m11 + m22;
+    q4 q{0, 0, 0, 1};
+    if (tr > 0) {
+        const float s = sqrtf(tr + 1.0f) * 2;
+        q.w = 0.25f * s, q.x = (c1.z - c2.y) / s, q.y = (c2.x - c0.z) / s, q.z = (c0.y - c1.x) / s;
+    } else if (m00 > m11 && m00 > m22) {
+        const float s = sqrtf(1.0f + m00 - m11 - m22) * 2;
+        q.w = (c1.z - c2.y) / s, q.x = 0.25f * s, q.y = (c1.x + c0.y) / s, q.z = (c2.x + c0.z) / s;
+    } else if (m11 > m22) {
+        const float s = sqrtf(1.0f + m11 - m00 - m22) * 2;
+        q.w = (c2.x - c0.z) / s, q.x = (c1.x + c0.y) / s, q.y = 0.25f * s, q.z = (c2.y + c1.z) / s;
+    } else {
+        const float s = sqrtf(1.0f + m22 - m00 - m11) * 2;
+        q.w = (c0.y - c1.x) / s, q.x = (c2.x + c0.z) / s, q.y = (c2.y + c1.z) / s, q.z = 0.25f * s;
+    }
+    return qnormalize(q);
+}
+__device__ __forceinline__ v3 quat_log(q4 qin) {
+    const q4 q = qin.w < 0 ? q4{qin.x * -1.0f, qin.y * -1.0f, qin.z * -1.0f, qin.w * -1.0f} : qin;
+    const v3 v = V(q.x, q.y, q.z);
+    const float s = length(v);
+    if (s < 1e-8f) return v * 2.0f;
+    const float angle = 2.0f * atan2f(s, q.w);
+    return v * (angle / s);
+}
+__device__ __forceinline__ q4 quat_exp(v3 rv) {
+    const float a = length(rv);
+    if (a < 1e-8f) return qnormalize(q4{rv.x * 0.5f, rv.y * 0.5f, rv.z * 0.5f, 1.0f});
+    const v3 ax = normalize(divs(rv, a));
+    const float hh = a * 0.5f, s = sinf(hh);
+    return {ax.x * s, ax.y * s, ax.z * s, cosf(hh)};
+}
+
+__device__ __forceinline__ double dmax0(double x) { return (0.0 < x) ? x : 0.0; }
+
+// ------------------------------------------------------------------------------------------ per frame node
+__global__ void k_fem_begin(FemDev F, const float4* __restrict__ nd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.nf) return;
+    const float4 p = nd[2 * F.fnode[i]];
+    double* x = F.xd + 3 * (size_t)i;
+    if ((float)x[0] != p.x || (float)x[1] != p.y || (float)x[2] != p.z) x[0] = p.x, x[1] = p.y, x[2] = p.z;
+}
+
+// ------------------------------------------------------------------------------------------ per triangle
+__global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __restrict__ nd) {
+    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= F.ntri) return;
+    F.ton[ti] = 0;
+    if (F.tbroken[ti]) return;
+    const int4 tn = F.tn[ti];
+    const int fnv[3] = {tn.x, tn.y, tn.z};
+    const FemSecDev s = F.sec[tn.w];
+    float X[3][2];
+    for (int i = 0; i < 3; i++) X[i][0] = F.tX[6 * ti + 2 * i], X[i][1] = F.tX[6 * ti + 2 * i + 1];
+    // ---- tri_kinematics (frame_fem.cpp:1584-1621)
+    double x[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) x[i][j] = F.xd[3 * (size_t)fnv[i] + j];
+    const double a[3] = {x[1][0] - x[0][0], x[1][1] - x[0][1], x[1][2] - x[0][2]}, c[3] = {x[2][0] - x[0][0], x[2][1] - x[0][1], x[2][2] - x[0][2]};
+    double n[3] = {a[1] * c[2] - a[2] * c[1], a[2] * c[0] - a[0] * c[2], a[0] * c[1] - a[1] * c[0]};
+    const double nl = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]), al = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    if (!(nl > 1e-12) || !(al > 1e-9) || !isfinite(nl)) return;
+    for (int j = 0; j < 3; j++) n[j] /= nl;
+    const double t1[3] = {a[0] / al, a[1] / al, a[2] / al};
+    const double t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
+    double cen[3];
+    for (int j = 0; j < 3; j++) cen[j] = (x[0][j] + x[1][j] + x[2][j]) / 3.0;
+    double p[3][2];
+    for (int i = 0; i < 3; i++) {
+        const double r[3] = {x[i][0] - cen[0], x[i][1] - cen[1], x[i][2] - cen[2]};
+        p[i][0] = r[0] * t1[0] + r[1] * t1[1] + r[2] * t1[2];
+        p[i][1] = r[0] * t2[0] + r[1] * t2[1] + r[2] * t2[2];
+    }
+    double sn = 0, cs = 0;
+    for (int i = 0; i < 3; i++) sn += X[i][0] * p[i][1] - X[i][1] * p[i][0], cs += X[i][0] * p[i][0] + X[i][1] * p[i][1];
+    const double phi = atan2(sn, cs), cp = cos(phi), sp = sin(phi);
+    double e1d[3], e2d[3];
+    for (int j = 0; j < 3; j++) e1d[j] = cp * t1[j] + sp * t2[j], e2d[j] = -sp * t1[j] + cp * t2[j];
+    const v3 e1 = V((float)e1d[0], (float)e1d[1], (float)e1d[2]), e2 = V((float)e2d[0], (float)e2d[1], (float)e2d[2]);
+    const v3 e3 = V((float)n[0], (float)n[1], (float)n[2]);
+    const q4 Ec = qconj(qfrom_mat3(e1, e2, e3));
+    double d[18];
+    for (int i = 0; i < 3; i++) {
+        d[6 * i] = cp * p[i][0] + sp * p[i][1] - X[i][0];
+        d[6 * i + 1] = -sp * p[i][0] + cp * p[i][1] - X[i][1];
+        d[6 * i + 2] = 0;
+        const float4 qf = F.q[fnv[i]], rf = F.tr0[3 * ti + i];
+        const v3 th = quat_log(qmul(Ec, qnormalize(qmul(q4{qf.x, qf.y, qf.z, qf.w}, q4{rf.x, rf.y, rf.z, rf.w}))));
+        d[6 * i + 3] = th.x, d[6 * i + 4] = th.y, d[6 * i + 5] = th.z;
+    }
+    // ---- eval_tris (frame_fem.cpp:1661-1831), an elastic section
+    double b3[3], c3[3];
+    for (int i = 0; i < 3; i++) {
+        const int j = (i + 1) % 3, k = (i + 2) % 3;
+        b3[i] = (double)X[j][1] - X[k][1];
+        c3[i] = (double)X[k][0] - X[j][0];
+    }
+    const double A2 = ((double)X[1][0] - X[0][0]) * ((double)X[2][1] - X[0][1]) - ((double)X[2][0] - X[0][0]) * ((double)X[1][1] - X[0][1]);
+    if (!(A2 > 0)) return;
+    const double nu = s.nu, Dm = (double)s.E / (1 - nu * nu);
+    double eps[3] = {0, 0, 0}, sig[3];
+    for (int i = 0; i < 3; i++) {
+        eps[0] += b3[i] * d[6 * i] / A2;
+        eps[1] += c3[i] * d[6 * i + 1] / A2;
+        eps[2] += (c3[i] * d[6 * i] + b3[i] * d[6 * i + 1]) / A2;
+    }
+    sig[0] = Dm * (eps[0] + nu * eps[1]), sig[1] = Dm * (nu * eps[0] + eps[1]), sig[2] = Dm * 0.5 * (1 - nu) * eps[2];
+    const float* Km = F.tk + 162 * (size_t)ti;
+    const float* Kp = Km + 81;
+    double vl[18];
+    {
+        const double E[3][3] = {{e1.x, e2.x, e3.x}, {e1.y, e2.y, e3.y}, {e1.z, e2.z, e3.z}};
+        for (int i = 0; i < 3; i++) {
+            const float4 vv = nd[2 * F.fnode[fnv[i]] + 1], om = F.w[fnv[i]];
+            for (int a2 = 0; a2 < 3; a2++) {
+                vl[6 * i + a2] = E[0][a2] * vv.x + E[1][a2] * vv.y + E[2][a2] * vv.z;
+                vl[6 * i + 3 + a2] = E[0][a2] * om.x + E[1][a2] * om.y + E[2][a2] * om.z;
+            }
+        }
+    }
+    const int kMem[3] = {0, 1, 5}, kPlate[3] = {2, 3, 4};
+    double f[18], fl[18];
+    {
+        double dm[9], dp[9], vm[9], vp[9];
+        for (int a = 0; a < 9; a++) {
+            const int ci = 6 * (a / 3);
+            dm[a] = d[ci + kMem[a % 3]], dp[a] = d[ci + kPlate[a % 3]];
+            vm[a] = vl[ci + kMem[a % 3]], vp[a] = vl[ci + kPlate[a % 3]];
+        }
+        double fm[9] = {}, fp[9] = {}, um[9] = {}, up[9] = {};
+        for (int cc = 0; cc < 9; cc++)
+            for (int a = 0; a < 9; a++) {
+                const double km = (double)Km[cc * 9 + a], kp = (double)Kp[cc * 9 + a];
+                fm[a] += km * dm[cc], um[a] += km * vm[cc];
+                fp[a] += kp * dp[cc], up[a] += kp * vp[cc];
+            }
+        for (int a = 0; a < 9; a++) {
+            const int ci = 6 * (a / 3);
+            f[ci + kMem[a % 3]] = fm[a], fl[ci + kMem[a % 3]] = um[a];
+            f[ci + kPlate[a % 3]] = fp[a], fl[ci + kPlate[a % 3]] = up[a];
+        }
+    }
+    for (int i = 0; i < 3; i++) {
+        const v3 fo = e1 * (float)f[6 * i] + e2 * (float)f[6 * i + 1] + e3 * (float)f[6 * i + 2];
+        const v3 to = e1 * (float)f[6 * i + 3] + e2 * (float)f[6 * i + 4] + e3 * (float)f[6 * i + 5];
+        F.tf[3 * ti + i] = make_float4(-fo.x, -fo.y, -fo.z, 0.0f);
+        F.tt[3 * ti + i] = make_float4(-to.x, -to.y, -to.z, 0.0f);
+    }
+    float* tg = F.ttan + 18 * (size_t)ti;
+    tg[0] = e1.x, tg[1] = e1.y, tg[2] = e1.z, tg[3] = e2.x, tg[4] = e2.y, tg[5] = e2.z, tg[6] = e3.x, tg[7] = e3.y, tg[8] = e3.z;
+    {
+        const double sx = sig[0] * s.t, sy = sig[1] * s.t, sxy = sig[2] * s.t;
+        const double tr = 0.5 * (sx + sy), df = sqrt(0.25 * (sx - sy) * (sx - sy) + sxy * sxy);
+        const double l1 = dmax0(tr + df), l2 = dmax0(tr - df);
+        double vx = sxy, vy = l1 - sx;
+        if (fabs(vx) + fabs(vy) < 1e-12 * (fabs(sx) + fabs(sy) + 1)) vx = sx >= sy ? 1 : 0, vy = sx >= sy ? 0 : 1;
+        const double vln = sqrt(vx * vx + vy * vy);
+        vx /= vln, vy /= vln;
+        const double S00 = l1 * vx * vx + l2 * vy * vy, S01 = (l1 - l2) * vx * vy, S11 = l1 * vy * vy + l2 * vx * vx;
+        const double A = 0.5 * A2;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                const double gi0 = b3[i] / A2, gi1 = c3[i] / A2, gj0 = b3[j] / A2, gj1 = c3[j] / A2;
+                tg[9 + 3 * i + j] = (float)(A * (gi0 * (S00 * gj0 + S01 * gj1) + gi1 * (S01 * gj0 + S11 * gj1)));
+            }
+    }
+    {
+        const double E[3][3] = {{e1.x, e2.x, e3.x}, {e1.y, e2.y, e3.y}, {e1.z, e2.z, e3.z}};
+        double* kv = F.tkv + 18 * (size_t)ti;
+        for (int i = 0; i < 3; i++)
+            for (int pp = 0; pp < 3; pp++) {
+                kv[6 * i + pp] = E[pp][0] * fl[6 * i] + E[pp][1] * fl[6 * i + 1] + E[pp][2] * fl[6 * i + 2];
+                kv[6 * i + 3 + pp] = E[pp][0] * fl[6 * i + 3] + E[pp][1] * fl[6 * i + 4] + E[pp][2] * fl[6 * i + 5];
+            }
+    }
+    F.ton[ti] = 1;
+}
+
+// ------------------------------------------------------------------------------------------ assembly
+// A triangle's block of corners (i, j) in the world's axes times c, with its tension's geometric stiffness
+// (gather_part's tri_block, frame_fem.cpp:961-1003)
+__device__ void tri_block_add(const FemDev& F, int t, int i, int j, double h2, double* D) {
+    const FemSecDev s = F.sec[F.tn[t].w];
+    const double c = h2 + (double)s.damping * F.h;
+    const float* tg = F.ttan + 18 * (size_t)t;
+    const double E[3][3] = {{tg[0], tg[3], tg[6]}, {tg[1], tg[4], tg[7]}, {tg[2], tg[5], tg[8]}};
+    const float* Km = F.tk + 162 * (size_t)t;
+    const float* Kp = Km + 81;
+#define BL_M(s2, t2) ((double)Km[(3 * i + (s2)) * 9 + 3 * j + (t2)])
+#define BL_P(s2, t2) ((double)Kp[(3 * i + (s2)) * 9 + 3 * j + (t2)])
+    for (int ra = 0; ra < 2; ra++)
+        for (int cb = 0; cb < 2; cb++) {
+            double T[3][3];
+            for (int pp = 0; pp < 3; pp++) {
+                const double E0 = E[pp][0], E1 = E[pp][1], E2 = E[pp][2];
+                if (ra == 0 && cb == 0) {
+                    T[pp][0] = E0 * BL_M(0, 0) + E1 * BL_M(1, 0);
+                    T[pp][1] = E0 * BL_M(0, 1) + E1 * BL_M(1, 1);
+                    T[pp][2] = E2 * BL_P(0, 0);
+                } else if (ra == 0) {
+                    T[pp][0] = E2 * BL_P(0, 1);
+                    T[pp][1] = E2 * BL_P(0, 2);
+                    T[pp][2] = E0 * BL_M(0, 2) + E1 * BL_M(1, 2);
+                } else if (cb == 0) {
+                    T[pp][0] = E2 * BL_M(2, 0);
+                    T[pp][1] = E2 * BL_M(2, 1);
+                    T[pp][2] = E0 * BL_P(1, 0) + E1 * BL_P(2, 0);
+                } else {
+                    T[pp][0] = E0 * BL_P(1, 1) + E1 * BL_P(2, 1);
+                    T[pp][1] = E0 * BL_P(1, 2) + E1 * BL_P(2, 2);
+                    T[pp][2] = E2 * BL_M(2, 2);
+                }
+            }
+            for (int pp = 0; pp < 3; pp++)
+                for (int qq = 0; qq < 3; qq++) D[(3 * ra + pp) * 6 + 3 * cb + qq] += c * (T[pp][0] * E[qq][0] + T[pp][1] * E[qq][1] + T[pp][2] * E[qq][2]);
+        }
+#undef BL_M
+#undef BL_P
+    const double gg = h2 * tg[9 + 3 * i + j];
+    if (gg != 0)
+        for (int pp = 0; pp < 3; pp++) D[pp * 7] += gg;
+}
+
+// One column's diagonal block, right side and off-diagonal blocks; nforce: the nodes' forces of the substep
+__global__ void k_fem_assemble(FemDev F, const float4* __restrict__ nd, const float4* __restrict__ nforce) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= F.nf) return;
+    const int i = F.perm[k];
+    const int bn = F.fnode[i];
+    const float4 P = nd[2 * bn], Vv = nd[2 * bn + 1];
+    const double h2 = F.ch2[k], hd = F.chd[k];
+    double D[36];
+    double* R = F.rhs + 6 * (size_t)k;
+    for (int x = 0; x < 36; x++) D[x] = 0.0;
+    if (k == 0 || F.col_comp[k] != F.col_comp[k - 1]) F.comp_fail[F.col_comp[k]] = 0;
+    const bool fixed = P.w <= 0;
+    F.fixed[k] = fixed;
+    if (fixed) {
+        for (int j = 0; j < 6; j++) D[j * 7] = 1.0, R[j] = 0.0;
+    } else {
+        D[0] = D[7] = D[14] = Vv.w;
+        D[21] = D[28] = D[35] = F.inertia[i];
+        double rd[6] = {0, 0, 0, 0, 0, 0};
+        for (int qq = F.gdiag_ptr[k]; qq < F.gdiag_ptr[k + 1]; qq++) {
+            const int2 g = F.gdiag[qq];
+            if (!F.ton[g.x]) continue;
+            tri_block_add(F, g.x, g.y, g.y, h2, D);
+            const double cr = hd + (double)F.sec[F.tn[g.x].w].damping * F.h;
+            if (cr != 0) {
+                const double* kv = F.tkv + 18 * (size_t)g.x + 6 * g.y;
+                for (int j = 0; j < 6; j++) rd[j] -= cr * kv[j];
+            }
+        }
+        const float4 f = nforce[bn], m = F.torque[i];
+        const double h = F.h;
+        R[0] = h * (double)f.x, R[1] = h * (double)f.y, R[2] = h * (double)f.z;
+        R[3] = h * (double)m.x, R[4] = h * (double)m.y, R[5] = h * (double)m.z;
+        for (int j = 0; j < 6; j++) R[j] += rd[j];
+    }
+    double* Dg = F.diag + 36 * (size_t)k;
+    for (int x = 0; x < 36; x++) Dg[x] = D[x];
+    for (int pb = F.col_ptr[k]; pb < F.col_ptr[k + 1]; pb++) {
+        double O[36];
+        for (int x = 0; x < 36; x++) O[x] = 0.0;
+        const int rnode = F.fnode[F.perm[F.row[pb]]];
+        if (!fixed && F.goff_ptr[pb] != F.goff_ptr[pb + 1] && !(nd[2 * rnode].w <= 0))
+            for (int qq = F.goff_ptr[pb]; qq < F.goff_ptr[pb + 1]; qq++) {
+                const int4 g = F.goff[qq];
+                if (F.ton[g.x]) tri_block_add(F, g.x, g.y, g.z, h2, O);
+            }
+        double* Og = F.off + 36 * (size_t)pb;
+        for (int x = 0; x < 36; x++) Og[x] = O[x];
+    }
+}
+
+// ------------------------------------------------------------------------------------------ factorization
+// chol6 (frame_fem.cpp:2193-2209) by one thread
+__device__ bool chol6_dev(double* A, double* dinv) {
+    for (int j = 0; j < 6; j++) {
+        double s = A[j * 6 + j];
+        for (int k = 0; k < j; k++) s -= A[j * 6 + k] * A[j * 6 + k];
+        if (!(s > 0)) return false;
+        const double d = sqrt(s), id = 1.0 / d;
+        A[j * 6 + j] = d;
+        dinv[j] = id;
+        for (int i = j + 1; i < 6; i++) {
+            double t = A[i * 6 + j];
+            for (int k = 0; k < j; k++) t -= A[i * 6 + k] * A[j * 6 + k];
+            A[i * 6 + j] = t * id;
+        }
+        for (int i = 0; i < j; i++) A[i * 6 + j] = 0;
+    }
+    return true;
+}
+
+// The level's columns, one warp each: chol6 of the diagonal block (lane 0), then every row of the column's
+// off-diagonal blocks against it, X := X L^-T (right_solve_lt, frame_fem.cpp:2211-2220), rows over the lanes
+__global__ void __launch_bounds__(128) k_fem_chol_level(FemDev F, int c0, int c1) {
+    const int lane = threadIdx.x & 31;
+    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (ci >= c1) return;
+    const int k = F.lvl_col[ci];
+    double* Lkk = F.diag + 36 * (size_t)k;
+    double* dk = F.dinv + 6 * (size_t)k;
+    int ok = 1;
+    if (lane == 0) ok = chol6_dev(Lkk, dk);
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (!ok) {
+        if (lane == 0) atomicExch(&F.comp_fail[F.col_comp[k]], 1);
+        return;
+    }
+    __syncwarp();
+    double L[21], di[6];
+    for (int j = 0, x = 0; j < 6; j++) {
+        di[j] = dk[j];
+        for (int m = 0; m <= j; m++) L[x++] = Lkk[j * 6 + m];
+    }
+    const int nrows = 6 * (F.col_ptr[k + 1] - F.col_ptr[k]);
+    for (int rr = lane; rr < nrows; rr += 32) {
+        double* xrow = F.off + 36 * (size_t)(F.col_ptr[k] + rr / 6) + 6 * (rr % 6);
+        double x[6];
+        for (int j = 0; j < 6; j++) x[j] = xrow[j];
+        for (int j = 0, b = 0; j < 6; j++) {
+            double s = x[j];
+            for (int m = 0; m < j; m++) s -= L[b + m] * x[m];
+            x[j] = s * di[j];
+            b += j + 1;
+        }
+        for (int j = 0; j < 6; j++) xrow[j] = x[j];
+    }
+}
+
+// The level's columns' updates (the right-looking step of frame_fem.cpp:2910-2914), one warp per target block: the
+// updates this level's columns make to it, in the order of those columns, T -= P Q^T each (sub_abt's sums,
+// frame_fem.cpp:2276-2288). A target meets every level's updates in the order of the levels.
+__global__ void __launch_bounds__(128) k_fem_update_level(FemDev F, int g0, int g1) {
+    __shared__ double sPQ[4][72];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gi = g0 + blockIdx.x * 4 + wib;
+    if (gi >= g1) return;
+    const int tgt = F.grp_tgt[gi];
+    double* T = tgt < F.nf ? F.diag + 36 * (size_t)tgt : F.off + 36 * (size_t)(tgt - F.nf);
+    double* pq = sPQ[wib];
+    const int e0 = lane, e1 = lane + 32; // (lane e, and e + 32 for e < 4, own entry e = 6 r + c)
+    double acc0 = T[e0], acc1 = lane < 4 ? T[e1] : 0.0;
+    for (int u = F.grp_ptr[gi]; u < F.grp_ptr[gi + 1]; u++) {
+        const int2 pp = F.gu[u];
+        const double* Pm = F.off + 36 * (size_t)pp.x; // P = L(pj)
+        const double* Qm = F.off + 36 * (size_t)pp.y; // Q = L(pi)
+        __syncwarp();
+        for (int x = lane; x < 72; x += 32) pq[x] = x < 36 ? Pm[x] : Qm[x - 36];
+        __syncwarp();
+        {
+            const int r = e0 / 6, cc = e0 % 6;
+            double s = 0;
+            for (int m = 0; m < 6; m++) s += pq[r * 6 + m] * pq[36 + cc * 6 + m];
+            acc0 -= s;
+        }
+        if (lane < 4) {
+            const int r = e1 / 6, cc = e1 % 6;
+            double s = 0;
+            for (int m = 0; m < 6; m++) s += pq[r * 6 + m] * pq[36 + cc * 6 + m];
+            acc1 -= s;
+        }
+    }
+    T[e0] = acc0;
+    if (lane < 4) T[e1] = acc1;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// L y = r for the level's columns, one warp a column: the blocks in its row (from the columns before it) spread over
+// the lanes and summed, then forward6 (frame_fem.cpp:2304-2310, 2944-2948)
+__global__ void __launch_bounds__(128) k_fem_forward_level(FemDev F, int c0, int c1) {
+    const int lane = threadIdx.x & 31;
+    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (ci >= c1) return;
+    const int k = F.lvl_col[ci];
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = F.rb_ptr[k] + lane; q < F.rb_ptr[k + 1]; q += 32) {
+        const int2 bc = F.rb[q];
+        const double* L = F.off + 36 * (size_t)bc.x;
+        const double* yk = F.rhs + 6 * (size_t)bc.y;
+        for (int ii = 0; ii < 6; ii++) {
+            double t = 0;
+            for (int j = 0; j < 6; j++) t += L[ii * 6 + j] * yk[j];
+            s[ii] += t;
+        }
+    }
+    for (int j = 0; j < 6; j++) s[j] = warp_sum(s[j]);
+    if (lane != 0) return;
+    double y[6];
+    for (int j = 0; j < 6; j++) y[j] = F.rhs[6 * (size_t)k + j] - s[j];
+    const double* Lkk = F.diag + 36 * (size_t)k;
+    const double* dk = F.dinv + 6 * (size_t)k;
+    for (int j = 0; j < 6; j++) {
+        double t = y[j];
+        for (int m = 0; m < j; m++) t -= Lkk[j * 6 + m] * y[m];
+        y[j] = t * dk[j];
+    }
+    for (int j = 0; j < 6; j++) F.rhs[6 * (size_t)k + j] = y[j];
+}
+
+// L^T x = y for the level's columns (the levels from the top down), one warp a column: its blocks' L^T x_row over
+// the lanes, summed, then backward6 (frame_fem.cpp:2296-2303, 2311-2317, 2949-2954)
+__global__ void __launch_bounds__(128) k_fem_backward_level(FemDev F, int c0, int c1) {
+    const int lane = threadIdx.x & 31;
+    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (ci >= c1) return;
+    const int k = F.lvl_col[ci];
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int pb = F.col_ptr[k] + lane; pb < F.col_ptr[k + 1]; pb += 32) {
+        const double* L = F.off + 36 * (size_t)pb;
+        const double* xr = F.rhs + 6 * (size_t)F.row[pb];
+        for (int j = 0; j < 6; j++) {
+            double t = 0;
+            for (int ii = 0; ii < 6; ii++) t += L[ii * 6 + j] * xr[ii];
+            s[j] += t;
+        }
+    }
+    for (int j = 0; j < 6; j++) s[j] = warp_sum(s[j]);
+    if (lane != 0) return;
+    double x[6];
+    for (int j = 0; j < 6; j++) x[j] = F.rhs[6 * (size_t)k + j] - s[j];
+    const double* Lkk = F.diag + 36 * (size_t)k;
+    const double* dk = F.dinv + 6 * (size_t)k;
+    for (int j = 5; j >= 0; j--) {
+        double t = x[j];
+        for (int m = j + 1; m < 6; m++) t -= Lkk[m * 6 + j] * x[m];
+        x[j] = t * dk[j];
+    }
+    for (int j = 0; j < 6; j++) F.rhs[6 * (size_t)k + j] = x[j];
+}
+
+// ------------------------------------------------------------------------------------------ after the solve
+__global__ void k_fem_velocity(FemDev F, const float4* __restrict__ nd, float4* __restrict__ nforce) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= F.nf) return;
+    const int i = F.perm[k];
+    F.torque[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); // (used by this step: torques from outside add up until the next)
+    if (F.comp_fail[F.col_comp[k]]) {
+        if (k == 0 || F.col_comp[k] != F.col_comp[k - 1]) atomicAdd(&F.body_failures[F.fbody[i]], 1);
+        return; // (a failed factorization: the elements' forces stay in the node forces, an explicit step this once)
+    }
+    if (F.fixed[k]) {
+        F.w[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    const double* x = F.rhs + 6 * (size_t)k;
+    const int bn = F.fnode[i];
+    const float mass = nd[2 * bn + 1].w;
+    v3 dv = V((float)x[0], (float)x[1], (float)x[2]);
+    const v3 dw = V((float)x[3], (float)x[4], (float)x[5]);
+    if (!isfinite(dv.x + dv.y + dv.z + dw.x + dw.y + dw.z)) {
+        atomicAdd(&F.body_failures[F.fbody[i]], 1);
+        return;
+    }
+    const float kMaxDv = 40.0f, kMaxW = 3000.0f;
+    {
+        const float l = length(dv);
+        if (l > kMaxDv) dv = dv * (kMaxDv / l), atomicAdd(&F.body_clamps[F.fbody[i]], 1);
+    }
+    const v3 fv = dv * (mass / F.step);
+    nforce[bn] = make_float4(fv.x, fv.y, fv.z, 0.0f);
+    const float4 w0 = F.w[i];
+    v3 wn = V(w0.x, w0.y, w0.z) + dw;
+    {
+        const float l = length(wn);
+        if (l > kMaxW) wn = wn * (kMaxW / l), atomicAdd(&F.body_clamps[F.fbody[i]], 1);
+    }
+    F.w[i] = make_float4(wn.x, wn.y, wn.z, 0.0f);
+}
+
+// The frame bodies' nodes: SoftBody::integrate_nodes with the forces the solve left (softbody.cpp:769-795), the body's
+// bounds and top speed; then a frame node's FemFrame::sync_positions (frame_fem.cpp:3407-3422): its double position
+// advanced by h v, its orientation turned by w h, its float position taken from the double one unless something moved
+// it. fem_nodes: the frame bodies' nodes (global node indices), fslot: a node's frame node (-1: none).
+__global__ void __launch_bounds__(256) k_fem_integrate(FemDev F, float4* __restrict__ nd, const float4* __restrict__ nforce,
+                                                       const int* __restrict__ fem_nodes, int n_fem_nodes, const int* __restrict__ fslot,
+                                                       const int4* __restrict__ info, Body* __restrict__ bodies, float dt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_fem_nodes) return;
+    const int i = fem_nodes[t];
+    Body& B = bodies[info[i].w];
+    if (B.sleeping) return;
+    float4 P = nd[2 * i], Vv = nd[2 * i + 1];
+    v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
+    float v2 = 0.0f;
+    if (P.w > 0) {
+        const float4 f4 = nforce[i];
+        vel = vel + V(f4.x, f4.y, f4.z) * (P.w * dt);
+        v2 = dot(vel, vel);
+        if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
+            vel = vel * (kMaxNodeSpeed / sqrtf(v2));
+            v2 = kMaxNodeSpeed * kMaxNodeSpeed;
+        } else if (!(v2 >= 0.0f)) {
+            vel = V(0, 0, 0);
+            v2 = 0;
+        }
+        pos = pos + vel * dt;
+    }
+    const int fs = fslot[i];
+    if (fs >= 0) {
+        double* x = F.xd + 3 * (size_t)fs;
+        const double h = F.h;
+        x[0] += h * vel.x, x[1] += h * vel.y, x[2] += h * vel.z;
+        const float4 w4 = F.w[fs];
+        const v3 w = V(w4.x, w4.y, w4.z);
+        if (dot(w, w) > 0) {
+            const float4 q0 = F.q[fs];
+            const q4 qn = qnormalize(qmul(quat_exp(w * F.h), q4{q0.x, q0.y, q0.z, q0.w}));
+            F.q[fs] = make_float4(qn.x, qn.y, qn.z, qn.w);
+        }
+        const double tol = 1e-4 * (1.0 + fabs((double)pos.x) + fabs((double)pos.y) + fabs((double)pos.z));
+        if (P.w > 0 && fabs(x[0] - pos.x) <= tol && fabs(x[1] - pos.y) <= tol && fabs(x[2] - pos.z) <= tol)
+            pos = V((float)x[0], (float)x[1], (float)x[2]);
+        else
+            x[0] = pos.x, x[1] = pos.y, x[2] = pos.z;
+    }
+    nd[2 * i] = make_float4(pos.x, pos.y, pos.z, P.w);
+    nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, Vv.w);
+    if (pos.x == pos.x) atomic_min_f(&B.acc_mn[0], pos.x), atomic_max_f(&B.acc_mx[0], pos.x);
+    if (pos.y == pos.y) atomic_min_f(&B.acc_mn[1], pos.y), atomic_max_f(&B.acc_mx[1], pos.y);
+    if (pos.z == pos.z) atomic_min_f(&B.acc_mn[2], pos.z), atomic_max_f(&B.acc_mx[2], pos.z);
+    atomic_max_f(&B.acc_v2, v2);
+}
+
+} // namespace blg

@@ -331,16 +331,33 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
     fv[j] = out;
 }
 
-// Gravity + the node's beams in beam order, World::collide_static for the node (world.cpp:781-870), then
-// SoftBody::integrate_nodes (softbody.cpp:769-795). first: the frame's first substep (the top speed starts from the
-// velocities before it, world.cpp:3217-3222).
+// Gravity (and any constant node force) + the node's beams in beam order, World::collide_static for the node
+// (world.cpp:781-870), then SoftBody::integrate_nodes (softbody.cpp:769-795). first: the frame's first substep (the top
+// speed starts from the velocities before it, world.cpp:3217-3222).
+// Frame bodies (Body::is_fem) stop after their forces: the triangles' forces and torques are gathered onto the frame
+// nodes in the reference's order (gather_forces, frame_fem.cpp:2080-2105) and the node's force is kept in nforce for
+// the frame's implicit step (their nodes do not touch the static world).
+struct NodeFem {
+    const int* fslot;        // node -> frame node (-1: none)
+    const int* iperm;        // frame node -> column
+    const int* gdiag_ptr;    // column -> its triangles' corners
+    const int2* gdiag;
+    const uint8_t* ton;
+    const float4* tf;
+    const float4* tt;
+    float4* torque;
+    float4* nforce;
+    const float4* ext;       // constant node forces (bl_gpu_set_node_force)
+};
+
 __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const int4* __restrict__ info,
                                                const int* __restrict__ inc_ptr, const int* __restrict__ inc, const float4* __restrict__ fv,
-                                               Body* __restrict__ bodies, Statics st, float gx, float gy, float gz, float dt, int nnodes, int first) {
+                                               Body* __restrict__ bodies, Statics st, float gx, float gy, float gz, float dt, int nnodes, int first,
+                                               NodeFem nf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int body = -1;
-    v3 p = V(0, 0, 0), pmx = V(0, 0, 0);
+    v3 p = V(1e30f, 1e30f, 1e30f), pmx = V(-1e30f, -1e30f, -1e30f);
     float v2 = 0.0f, v2start = 0.0f;
     int contact = 0;
     bool live = false;
@@ -354,6 +371,10 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
             if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
             const float m = Vv.w;
             v3 f = V(gx * m, gy * m, gz * m); // clear_forces: g * mass (softbody.cpp:376)
+            if (B.has_ext) {                  // (a controller's push, world.cpp:3261)
+                const float4 e = nf.ext[i];
+                f = V(f.x + e.x, f.y + e.y, f.z + e.z);
+            }
             const int q1 = inc_ptr[i + 1];
             for (int q = inc_ptr[i]; q < q1; q++) {
                 const int e = inc[q];
@@ -363,79 +384,97 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
                     else f = V(f.x + b.x, f.y + b.y, f.z + b.z);
                 }
             }
-            v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
-            float inv_mass = P.w;
-            const uint32_t flags = (uint32_t)inf.x;
-            // ---- static contact (World::collide_static)
-            if (!(!(flags & NF_GROUND) || inv_mass <= 0)) {
-                if (pos.y < st.kill_y) {
-                    vel = V(0, 0, 0);
-                    inv_mass = 0;
-                } else {
-                    const float r = __int_as_float(inf.z);
-                    const bool near_terrain = st.has_terrain && pos.y - r <= B.terrain_max + 0.05f;
-                    const int nbox = B.nbox, ncyl = B.ncyl;
-                    if (near_terrain || nbox != 0 || ncyl != 0) {
-                        int bids[16], cids[16];
-                        const int* bp = B.box_ids;
-                        const int* cp = B.cyl_ids;
-                        int nb = nbox, nc = ncyl;
-                        bool go = true;
-                        if (nbox <= 16 && ncyl <= 16) {
-                            nb = nc = 0;
-                            const float rr = r + 0.01f;
-                            for (int k = 0; k < nbox; k++) {
-                                const Box& a = st.boxes[B.box_ids[k]];
-                                if (pos.x >= a.mnx - rr && pos.x <= a.mxx + rr && pos.y >= a.mny - rr && pos.y <= a.mxy + rr && pos.z >= a.mnz - rr &&
-                                    pos.z <= a.mxz + rr)
-                                    bids[nb++] = B.box_ids[k];
+            if (B.is_fem) {
+                const int fs = nf.fslot[i];
+                if (fs >= 0) {
+                    const int k = nf.iperm[fs];
+                    v3 tq = V(0, 0, 0);
+                    for (int g = nf.gdiag_ptr[k]; g < nf.gdiag_ptr[k + 1]; g++) {
+                        const int2 e = nf.gdiag[g];
+                        if (!nf.ton[e.x]) continue;
+                        const float4 tf = nf.tf[3 * e.x + e.y], tt = nf.tt[3 * e.x + e.y];
+                        f = V(f.x + tf.x, f.y + tf.y, f.z + tf.z);
+                        tq = V(tq.x + tt.x, tq.y + tt.y, tq.z + tt.z);
+                    }
+                    nf.torque[fs] = make_float4(tq.x, tq.y, tq.z, 0.0f);
+                }
+                nf.nforce[i] = make_float4(f.x, f.y, f.z, 0.0f);
+                v2 = v2start; // (its bounds and speeds after the frame's step: k_fem_integrate)
+            } else {
+                v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
+                float inv_mass = P.w;
+                const uint32_t flags = (uint32_t)inf.x;
+                // ---- static contact (World::collide_static)
+                if (!(!(flags & NF_GROUND) || inv_mass <= 0)) {
+                    if (pos.y < st.kill_y) {
+                        vel = V(0, 0, 0);
+                        inv_mass = 0;
+                    } else {
+                        const float r = __int_as_float(inf.z);
+                        const bool near_terrain = st.has_terrain && pos.y - r <= B.terrain_max + 0.05f;
+                        const int nbox = B.nbox, ncyl = B.ncyl;
+                        if (near_terrain || nbox != 0 || ncyl != 0) {
+                            int bids[16], cids[16];
+                            const int* bp = B.box_ids;
+                            const int* cp = B.cyl_ids;
+                            int nb = nbox, nc = ncyl;
+                            bool go = true;
+                            if (nbox <= 16 && ncyl <= 16) {
+                                nb = nc = 0;
+                                const float rr = r + 0.01f;
+                                for (int k = 0; k < nbox; k++) {
+                                    const Box& a = st.boxes[B.box_ids[k]];
+                                    if (pos.x >= a.mnx - rr && pos.x <= a.mxx + rr && pos.y >= a.mny - rr && pos.y <= a.mxy + rr && pos.z >= a.mnz - rr &&
+                                        pos.z <= a.mxz + rr)
+                                        bids[nb++] = B.box_ids[k];
+                                }
+                                for (int k = 0; k < ncyl; k++) {
+                                    const Cyl& cy = st.cyls[B.cyl_ids[k]];
+                                    const float cr = cy.radius + rr;
+                                    if (fabsf(pos.x - cy.bx) <= cr && fabsf(pos.z - cy.bz) <= cr && pos.y >= cy.by - rr && pos.y <= cy.by + cy.height + rr)
+                                        cids[nc++] = B.cyl_ids[k];
+                                }
+                                bp = bids;
+                                cp = cids;
+                                go = near_terrain || nb != 0 || nc != 0;
                             }
-                            for (int k = 0; k < ncyl; k++) {
-                                const Cyl& cy = st.cyls[B.cyl_ids[k]];
-                                const float cr = cy.radius + rr;
-                                if (fabsf(pos.x - cy.bx) <= cr && fabsf(pos.z - cy.bz) <= cr && pos.y >= cy.by - rr && pos.y <= cy.by + cy.height + rr)
-                                    cids[nc++] = B.cyl_ids[k];
-                            }
-                            bp = bids;
-                            cp = cids;
-                            go = near_terrain || nb != 0 || nc != 0;
-                        }
-                        Contact c;
-                        if (go && collide_point(st, pos, r, bp, nb, cp, nc, near_terrain, c)) {
-                            contact = 1;
-                            const GroundModel& gm = c_ground[c.surface < kSurfCount ? c.surface : 0];
-                            const float fc = __int_as_float(inf.y) * B.fric;
-                            if (c.max_force > 0) {
-                                v3 fcn = primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, -1.0f);
-                                const float fl = length(fcn);
-                                if (fl > c.max_force) fcn = fcn * (c.max_force / fl);
-                                f = f + fcn;
-                            } else {
-                                f = f + primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, B.bounce);
+                            Contact c;
+                            if (go && collide_point(st, pos, r, bp, nb, cp, nc, near_terrain, c)) {
+                                contact = 1;
+                                const GroundModel& gm = c_ground[c.surface < kSurfCount ? c.surface : 0];
+                                const float fc = __int_as_float(inf.y) * B.fric;
+                                if (c.max_force > 0) {
+                                    v3 fcn = primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, -1.0f);
+                                    const float fl = length(fcn);
+                                    if (fl > c.max_force) fcn = fcn * (c.max_force / fl);
+                                    f = f + fcn;
+                                } else {
+                                    f = f + primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, B.bounce);
+                                }
                             }
                         }
                     }
                 }
-            }
-            // ---- integration (SoftBody::integrate_nodes)
-            if (inv_mass > 0) {
-                vel = vel + f * (inv_mass * dt);
-                v2 = dot(vel, vel);
-                if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
-                    vel = vel * (kMaxNodeSpeed / sqrtf(v2));
-                    v2 = kMaxNodeSpeed * kMaxNodeSpeed;
-                } else if (!(v2 >= 0.0f)) {
-                    vel = V(0, 0, 0);
-                    v2 = 0;
+                // ---- integration (SoftBody::integrate_nodes)
+                if (inv_mass > 0) {
+                    vel = vel + f * (inv_mass * dt);
+                    v2 = dot(vel, vel);
+                    if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
+                        vel = vel * (kMaxNodeSpeed / sqrtf(v2));
+                        v2 = kMaxNodeSpeed * kMaxNodeSpeed;
+                    } else if (!(v2 >= 0.0f)) {
+                        vel = V(0, 0, 0);
+                        v2 = 0;
+                    }
+                    pos = pos + vel * dt;
                 }
-                pos = pos + vel * dt;
+                nd[2 * i] = make_float4(pos.x, pos.y, pos.z, inv_mass);
+                nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, m);
+                // the bounds skip a non-finite coordinate as the reference's vmin / vmax do (a NaN never compares less)
+                p = V(pos.x == pos.x ? pos.x : 1e30f, pos.y == pos.y ? pos.y : 1e30f, pos.z == pos.z ? pos.z : 1e30f);
+                pmx = V(pos.x == pos.x ? pos.x : -1e30f, pos.y == pos.y ? pos.y : -1e30f, pos.z == pos.z ? pos.z : -1e30f);
+                v2 = smax(v2, v2start);
             }
-            nd[2 * i] = make_float4(pos.x, pos.y, pos.z, inv_mass);
-            nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, m);
-            // the bounds skip a non-finite coordinate as the reference's vmin / vmax do (a NaN never compares less)
-            p = V(pos.x == pos.x ? pos.x : 1e30f, pos.y == pos.y ? pos.y : 1e30f, pos.z == pos.z ? pos.z : 1e30f);
-            pmx = V(pos.x == pos.x ? pos.x : -1e30f, pos.y == pos.y ? pos.y : -1e30f, pos.z == pos.z ? pos.z : -1e30f);
-            v2 = smax(v2, v2start);
         }
     }
     // ---- per body: bounds, top speed, contacts (a warp of one body reduces first)

@@ -11,6 +11,8 @@
 //   bodies  Body records (bl_device.cuh)
 // A frame (bl_gpu_step_substeps) is captured once per substep count as a CUDA graph and replayed.
 #include "../../include/beamlab_gpu.h"
+#include "bl_fem_host.cuh"
+#include "bl_fem_kernels.cuh"
 #include "bl_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -19,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <new>
 #include <vector>
 
@@ -32,6 +35,12 @@ struct HostBody {
     std::vector<bl_beam> beams;
     uint32_t beam_bits = 0; // the body's allow_deform / allow_break / ductile as BB_* bits of its beams' meta words
     Body rec;
+    std::vector<float4> ext;               // constant node forces (empty: none)
+    std::shared_ptr<FemModel> fem;         // its FEM frame (null: none), with its dynamic state q / w between commits
+    std::vector<FemSection> sections;
+    std::vector<float> fq, fw;             // frame nodes' orientation (4) and angular velocity (3)
+    float theta = 0.5f, diss = 0.02f;
+    int fem_failures = 0, fem_clamps = 0;
 };
 
 template <class T>
@@ -91,6 +100,21 @@ struct bl_gpu_ctx {
     int rs_P = 1;
     int N = 0, M = 0, B = 0;
     Statics st{};
+    // FEM frames of all bodies back to back (see bl_fem_kernels.cuh)
+    int NF = 0, NT = 0, NB = 0, n_fem_nodes = 0;
+    bool any_ext = false;
+    std::vector<int> lvl_grp_ptr, lvl_col_ptr; // per level: its update groups / columns
+    int64_t fem_launches = 0;                  // kernels of one substep's frame step
+    DevBuf<float4> ext, nforce, fq, fw, ftorque, tr0, tf, tt;
+    DevBuf<int> fnode, fbody, fperm, fiperm, grp_tgt, grp_ptr, col_comp, comp_fail, rb_ptr, lvl_col, fem_nodes, fslot;
+    DevBuf<int> fcol_ptr, frow, gdiag_ptr, goff_ptr, fem_fail, fem_clamp;
+    DevBuf<int2> gdiag, gu, rb;
+    DevBuf<int4> goff, tn;
+    DevBuf<double> xd, diag, off, rhs, dinv, tkv, ch2, chd;
+    DevBuf<float> finertia, tX, tk, ttan;
+    DevBuf<uint8_t> tbroken, ton, ffixed;
+    DevBuf<FemSecDev> fsec;
+    FemDev fd{};
     // frames captured as graphs, by substep count
     std::map<int, cudaGraphExec_t> graphs;
     struct ProfGraph {
@@ -126,7 +150,18 @@ static void drop_graphs(bl_gpu_ctx* c) {
     c->pgraphs.clear();
 }
 
+static void free_fem(bl_gpu_ctx* c) {
+    c->ext.free_(), c->nforce.free_(), c->fq.free_(), c->fw.free_(), c->ftorque.free_(), c->tr0.free_(), c->tf.free_(), c->tt.free_();
+    c->fnode.free_(), c->fbody.free_(), c->fperm.free_(), c->fiperm.free_(), c->grp_tgt.free_(), c->grp_ptr.free_();
+    c->col_comp.free_(), c->comp_fail.free_(), c->rb_ptr.free_(), c->lvl_col.free_(), c->fem_nodes.free_(), c->fslot.free_();
+    c->fcol_ptr.free_(), c->frow.free_(), c->gdiag_ptr.free_(), c->goff_ptr.free_(), c->fem_fail.free_(), c->fem_clamp.free_();
+    c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
+    c->xd.free_(), c->diag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
+    c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
+}
+
 static void free_device(bl_gpu_ctx* c) {
+    free_fem(c);
     c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->fv.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
@@ -242,6 +277,204 @@ static int pull_state(bl_gpu_ctx* c) {
         }
         hb.rec = r;
     }
+    // the frames' dynamic state (their positions in double, orientations, spins) and counters
+    if (c->NF > 0) {
+        std::vector<double> xd(3 * (size_t)c->NF);
+        std::vector<float4> q(c->NF), w(c->NF);
+        std::vector<int> ff(c->B), fc(c->B);
+        BL_CUDA(c, cudaMemcpy(xd.data(), c->xd.p, sizeof(double) * xd.size(), cudaMemcpyDeviceToHost));
+        BL_CUDA(c, cudaMemcpy(q.data(), c->fq.p, sizeof(float4) * c->NF, cudaMemcpyDeviceToHost));
+        BL_CUDA(c, cudaMemcpy(w.data(), c->fw.p, sizeof(float4) * c->NF, cudaMemcpyDeviceToHost));
+        BL_CUDA(c, cudaMemcpy(ff.data(), c->fem_fail.p, sizeof(int) * c->B, cudaMemcpyDeviceToHost));
+        BL_CUDA(c, cudaMemcpy(fc.data(), c->fem_clamp.p, sizeof(int) * c->B, cudaMemcpyDeviceToHost));
+        int fo = 0;
+        for (int bi = 0; bi < c->B; bi++) {
+            HostBody& hb = c->bodies[bi];
+            hb.fem_failures = ff[bi], hb.fem_clamps = fc[bi];
+            if (!hb.fem) continue;
+            const int nf = (int)hb.fem->node.size();
+            for (int i = 0; i < nf; i++) {
+                for (int j = 0; j < 3; j++) hb.fem->xd[3 * i + j] = xd[3 * (size_t)(fo + i) + j];
+                hb.fq[4 * i] = q[fo + i].x, hb.fq[4 * i + 1] = q[fo + i].y, hb.fq[4 * i + 2] = q[fo + i].z, hb.fq[4 * i + 3] = q[fo + i].w;
+                hb.fw[3 * i] = w[fo + i].x, hb.fw[3 * i + 1] = w[fo + i].y, hb.fw[3 * i + 2] = w[fo + i].z;
+            }
+            fo += nf;
+        }
+    }
+    return BL_GPU_OK;
+}
+
+// The FEM frames of all bodies on the device, back to back, and the factorization's schedule: the columns by
+// elimination-tree level (a column's level is one more than its deepest child's), each level's target blocks (a
+// column's diagonal block then its off-diagonal ones) with each target's updates in the order of their source columns,
+// each row's blocks in the order of their columns for the forward substitution.
+static int commit_fem(bl_gpu_ctx* c) {
+    int NF = 0, NT = 0, NB = 0, NC = 0, NS = 0, nfem_nodes = 0;
+    for (const HostBody& hb : c->bodies)
+        if (hb.fem) NF += (int)hb.fem->node.size(), NT += (int)hb.fem->tn.size(), NB += (int)hb.fem->row.size(), NC += hb.fem->ncomp,
+                    NS += (int)hb.sections.size(), nfem_nodes += hb.rec.nnodes;
+    c->NF = NF, c->NT = NT, c->NB = NB, c->n_fem_nodes = nfem_nodes;
+    c->lvl_grp_ptr.clear(), c->lvl_col_ptr.clear();
+    std::vector<float4> ext(c->any_ext ? c->N : 0, make_float4(0, 0, 0, 0));
+    for (const HostBody& hb : c->bodies)
+        if (!hb.ext.empty())
+            for (int i = 0; i < hb.rec.nnodes; i++) ext[hb.rec.node0 + i] = hb.ext[i];
+    int rc;
+    if ((rc = upload_vec(c, c->ext, ext))) return rc;
+    if (NF == 0) {
+        c->fd = FemDev{};
+        return BL_GPU_OK;
+    }
+    std::vector<int> fnode(NF), fbody(NF), perm(NF), iperm(NF), col_ptr(NF + 1, 0), row(NB), col_comp(NF), gdiag_ptr(NF + 1, 0), goff_ptr(NB + 1, 0);
+    std::vector<int> fem_nodes, fslot(c->N, -1), level(NF, 0);
+    std::vector<double> xd(3 * (size_t)NF), ch2(NF), chd(NF);
+    std::vector<float4> q(NF), w(NF), tr0(3 * (size_t)NT);
+    std::vector<float> inertia(NF), tX(6 * (size_t)NT), tk(162 * (size_t)NT);
+    std::vector<int4> tn(NT), goff;
+    std::vector<int2> gdiag;
+    std::vector<uint8_t> tbroken(NT);
+    std::vector<FemSecDev> sec;
+    std::vector<std::array<int, 3>> gupd; // every update (global): target, pj, pi - in the reference's order
+    std::vector<int> upd_col;             // ... and its source column
+    int fo = 0, to = 0, bo = 0, co = 0, so = 0;
+    for (int bi = 0; bi < c->B; bi++) {
+        const HostBody& hb = c->bodies[bi];
+        if (!hb.fem) continue;
+        const FemModel& M = *hb.fem;
+        const int nf = (int)M.node.size(), nt = (int)M.tn.size(), nb = (int)M.row.size();
+        for (int i = 0; i < hb.rec.nnodes; i++) fem_nodes.push_back(hb.rec.node0 + i);
+        const float dt = c->cfg.dt;
+        const double h2 = (double)hb.theta * dt * dt, hd = (double)hb.diss * dt * dt;
+        for (int i = 0; i < nf; i++) {
+            fnode[fo + i] = hb.rec.node0 + (int)M.node[i];
+            fslot[hb.rec.node0 + M.node[i]] = fo + i;
+            fbody[fo + i] = bi;
+            perm[fo + i] = fo + M.perm[i];
+            iperm[fo + i] = fo + M.iperm[i];
+            for (int j = 0; j < 3; j++) xd[3 * (size_t)(fo + i) + j] = M.xd[3 * i + j];
+            q[fo + i] = make_float4(hb.fq[4 * i], hb.fq[4 * i + 1], hb.fq[4 * i + 2], hb.fq[4 * i + 3]);
+            w[fo + i] = make_float4(hb.fw[3 * i], hb.fw[3 * i + 1], hb.fw[3 * i + 2], 0.0f);
+            inertia[fo + i] = M.inertia[i];
+            ch2[fo + i] = h2, chd[fo + i] = hd;
+        }
+        for (int k = 0; k < nf; k++) {
+            col_ptr[fo + k + 1] = bo + M.col_ptr[k + 1];
+            gdiag_ptr[fo + k + 1] = (int)gdiag.size() + (M.gdiag_ptr[k + 1] - M.gdiag_ptr[0]);
+        }
+        for (const auto& g : M.gdiag) gdiag.push_back(make_int2(to + g[0], g[1]));
+        for (int pb = 0; pb < nb; pb++) {
+            row[bo + pb] = fo + M.row[pb];
+            goff_ptr[bo + pb + 1] = (int)goff.size() + (M.goff_ptr[pb + 1] - M.goff_ptr[0]);
+        }
+        for (const auto& g : M.goff) goff.push_back(make_int4(to + g[0], g[1], g[2], 0));
+        for (int cc = 0; cc < M.ncomp; cc++)
+            for (int k = M.comp_first[cc]; k < M.comp_first[cc + 1]; k++) col_comp[fo + k] = co + cc;
+        for (int t = 0; t < nt; t++) {
+            tn[to + t] = make_int4(fo + M.tn[t][0], fo + M.tn[t][1], fo + M.tn[t][2], so + M.tsec[t]);
+            for (int x = 0; x < 6; x++) tX[6 * (size_t)(to + t) + x] = M.tX[6 * t + x];
+            for (int i = 0; i < 3; i++) tr0[3 * (size_t)(to + t) + i] = make_float4(M.tr0[12 * t + 4 * i], M.tr0[12 * t + 4 * i + 1], M.tr0[12 * t + 4 * i + 2], M.tr0[12 * t + 4 * i + 3]);
+            for (int x = 0; x < 162; x++) tk[162 * (size_t)(to + t) + x] = M.tk[162 * t + x];
+            tbroken[to + t] = M.tbroken[t];
+        }
+        for (const FemSection& fs : hb.sections) sec.push_back(FemSecDev{fs.E, fs.nu, fs.rho, fs.t, fs.damping, fs.drill});
+        for (int k = 0; k < nf; k++)
+            for (int u = M.upd_ptr[k]; u < M.upd_ptr[k + 1]; u++) {
+                const auto& up = M.upd[u];
+                gupd.push_back({up[2] >= 0 ? NF + bo + up[2] : fo + (-up[2] - 1), bo + up[1], bo + up[0]});
+                upd_col.push_back(fo + k);
+            }
+        // levels: a column's level one more than its deepest child's (its parent: the first row below its diagonal)
+        for (int k = 0; k < nf; k++) {
+            if (M.col_ptr[k + 1] == M.col_ptr[k]) continue;
+            int par = M.row[M.col_ptr[k]];
+            for (int pb = M.col_ptr[k]; pb < M.col_ptr[k + 1]; pb++) par = std::min(par, M.row[pb]);
+            level[fo + par] = std::max(level[fo + par], level[fo + k] + 1);
+        }
+        fo += nf, to += nt, bo += nb, co += M.ncomp, so += (int)hb.sections.size();
+    }
+    int nlev = 0;
+    for (int k = 0; k < NF; k++) nlev = std::max(nlev, level[k] + 1);
+    // per level: its columns, and the updates they make grouped by target (each group in the order of its columns)
+    std::vector<int> lvl_col, grp_tgt, grp_ptr(1, 0);
+    std::vector<int2> gu, rbv;
+    std::vector<int> rb_ptr(NF + 1, 0);
+    std::vector<std::vector<int>> bylev(nlev);
+    for (int k = 0; k < NF; k++) bylev[level[k]].push_back(k);
+    std::vector<std::vector<int>> col_upds(NF);
+    for (size_t u = 0; u < gupd.size(); u++) col_upds[upd_col[u]].push_back((int)u);
+    c->lvl_grp_ptr.assign(1, 0), c->lvl_col_ptr.assign(1, 0);
+    std::vector<int> slot_of(NF + NB, -1);
+    for (int L = 0; L < nlev; L++) {
+        std::vector<int> tg;                     // the level's targets, in order of first appearance
+        std::vector<std::vector<int2>> lists;
+        for (int k : bylev[L]) {
+            lvl_col.push_back(k);
+            for (int u : col_upds[k]) {
+                const int t = gupd[u][0];
+                if (slot_of[t] < 0) slot_of[t] = (int)tg.size(), tg.push_back(t), lists.emplace_back();
+                lists[slot_of[t]].push_back(make_int2(gupd[u][1], gupd[u][2]));
+            }
+        }
+        for (size_t x = 0; x < tg.size(); x++) {
+            grp_tgt.push_back(tg[x]);
+            gu.insert(gu.end(), lists[x].begin(), lists[x].end());
+            grp_ptr.push_back((int)gu.size());
+            slot_of[tg[x]] = -1;
+        }
+        c->lvl_grp_ptr.push_back((int)grp_tgt.size());
+        c->lvl_col_ptr.push_back((int)lvl_col.size());
+    }
+    // begin, triangles, assembly, per level a factor (and an update) kernel and two substitutions, velocities, integration
+    c->fem_launches = 5 + 3 * (int64_t)nlev;
+    for (int L = 0; L < nlev; L++) c->fem_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
+    {   // each row's blocks in the order of their columns
+        std::vector<std::vector<int2>> rows(NF);
+        for (int k = 0; k < NF; k++)
+            for (int pb = col_ptr[k]; pb < col_ptr[k + 1]; pb++) rows[row[pb]].push_back(make_int2(pb, k));
+        for (int r = 0; r < NF; r++) {
+            rb_ptr[r + 1] = rb_ptr[r] + (int)rows[r].size();
+            rbv.insert(rbv.end(), rows[r].begin(), rows[r].end());
+        }
+    }
+    std::vector<int> zeros_nf(NF, 0), zeros_b(c->B, 0), zeros_c(NC, 0);
+    for (int bi = 0; bi < c->B; bi++) zeros_b[bi] = c->bodies[bi].fem_failures;
+    std::vector<int> clamps_b(c->B);
+    for (int bi = 0; bi < c->B; bi++) clamps_b[bi] = c->bodies[bi].fem_clamps;
+    std::vector<float4> zero4(NF, make_float4(0, 0, 0, 0));
+    if ((rc = upload_vec(c, c->fnode, fnode)) || (rc = upload_vec(c, c->fbody, fbody)) || (rc = upload_vec(c, c->fperm, perm)) ||
+        (rc = upload_vec(c, c->fiperm, iperm)) || (rc = upload_vec(c, c->xd, xd)) || (rc = upload_vec(c, c->fq, q)) || (rc = upload_vec(c, c->fw, w)) ||
+        (rc = upload_vec(c, c->finertia, inertia)) || (rc = upload_vec(c, c->ftorque, zero4)) || (rc = upload_vec(c, c->tn, tn)) ||
+        (rc = upload_vec(c, c->tX, tX)) || (rc = upload_vec(c, c->tr0, tr0)) || (rc = upload_vec(c, c->tk, tk)) || (rc = upload_vec(c, c->tbroken, tbroken)) ||
+        (rc = upload_vec(c, c->fsec, sec)) || (rc = upload_vec(c, c->fcol_ptr, col_ptr)) || (rc = upload_vec(c, c->frow, row)) ||
+        (rc = upload_vec(c, c->gdiag_ptr, gdiag_ptr)) || (rc = upload_vec(c, c->gdiag, gdiag)) || (rc = upload_vec(c, c->goff_ptr, goff_ptr)) ||
+        (rc = upload_vec(c, c->goff, goff)) || (rc = upload_vec(c, c->grp_tgt, grp_tgt)) || (rc = upload_vec(c, c->grp_ptr, grp_ptr)) ||
+        (rc = upload_vec(c, c->gu, gu)) || (rc = upload_vec(c, c->col_comp, col_comp)) || (rc = upload_vec(c, c->comp_fail, zeros_c)) || (rc = upload_vec(c, c->rb_ptr, rb_ptr)) ||
+        (rc = upload_vec(c, c->rb, rbv)) || (rc = upload_vec(c, c->lvl_col, lvl_col)) || (rc = upload_vec(c, c->ch2, ch2)) ||
+        (rc = upload_vec(c, c->chd, chd)) || (rc = upload_vec(c, c->fem_fail, zeros_b)) || (rc = upload_vec(c, c->fem_clamp, clamps_b)) ||
+        (rc = upload_vec(c, c->fem_nodes, fem_nodes)) || (rc = upload_vec(c, c->fslot, fslot)))
+        return rc;
+    BL_CUDA(c, c->nforce.alloc(c->N));
+    BL_CUDA(c, c->tf.alloc(3 * (size_t)NT));
+    BL_CUDA(c, c->tt.alloc(3 * (size_t)NT));
+    BL_CUDA(c, c->ttan.alloc(18 * (size_t)NT));
+    BL_CUDA(c, c->tkv.alloc(18 * (size_t)NT));
+    BL_CUDA(c, c->ton.alloc(NT));
+    BL_CUDA(c, c->diag.alloc(36 * (size_t)NF));
+    BL_CUDA(c, c->off.alloc(36 * (size_t)std::max(NB, 1)));
+    BL_CUDA(c, c->rhs.alloc(6 * (size_t)NF));
+    BL_CUDA(c, c->dinv.alloc(6 * (size_t)NF));
+    BL_CUDA(c, c->ffixed.alloc(NF));
+    BL_CUDA(c, cudaMemsetAsync(c->ton.p, 0, NT, c->stream));
+    FemDev& F = c->fd;
+    F.nf = NF, F.ntri = NT, F.nblk = NB;
+    F.fnode = c->fnode.p, F.fbody = c->fbody.p, F.perm = c->fperm.p, F.iperm = c->fiperm.p, F.xd = c->xd.p, F.q = c->fq.p, F.w = c->fw.p;
+    F.inertia = c->finertia.p, F.torque = c->ftorque.p, F.tn = c->tn.p, F.tX = c->tX.p, F.tr0 = c->tr0.p, F.tk = c->tk.p, F.tbroken = c->tbroken.p;
+    F.tf = c->tf.p, F.tt = c->tt.p, F.ttan = c->ttan.p, F.tkv = c->tkv.p, F.ton = c->ton.p, F.sec = c->fsec.p, F.col_ptr = c->fcol_ptr.p, F.row = c->frow.p;
+    F.gdiag_ptr = c->gdiag_ptr.p, F.gdiag = c->gdiag.p, F.goff_ptr = c->goff_ptr.p, F.goff = c->goff.p, F.diag = c->diag.p, F.off = c->off.p;
+    F.rhs = c->rhs.p, F.dinv = c->dinv.p, F.fixed = c->ffixed.p, F.grp_tgt = c->grp_tgt.p, F.grp_ptr = c->grp_ptr.p, F.gu = c->gu.p;
+    F.col_comp = c->col_comp.p, F.comp_fail = c->comp_fail.p, F.rb_ptr = c->rb_ptr.p;
+    F.rb = c->rb.p, F.lvl_col = c->lvl_col.p, F.ch2 = c->ch2.p, F.chd = c->chd.p, F.body_failures = c->fem_fail.p, F.body_clamps = c->fem_clamp.p;
+    F.h = c->cfg.dt, F.step = c->cfg.dt;
     return BL_GPU_OK;
 }
 
@@ -298,6 +531,12 @@ static int commit_bodies(bl_gpu_ctx* c) {
             meta[r.beam0 + j] = (uint32_t)b.type | ((uint32_t)b.flags << 8) | bits | (r.sleeping ? kBeamAsleep : 0u);
         }
     }
+    c->any_ext = false;
+    for (int bi = 0; bi < B; bi++) {
+        recs[bi].is_fem = c->bodies[bi].fem ? 1 : 0;
+        recs[bi].has_ext = c->bodies[bi].ext.empty() ? 0 : 1;
+        c->any_ext |= recs[bi].has_ext != 0;
+    }
     for (int i = 0; i < N; i++) inc_ptr[i + 1] += inc_ptr[i];
     {
         std::vector<int> fill(inc_ptr.begin(), inc_ptr.end() - 1);
@@ -323,8 +562,9 @@ static int commit_bodies(bl_gpu_ctx* c) {
     BL_CUDA(c, c->rs_bad.alloc(P));
     BL_CUDA(c, c->rs_np.alloc(P));
     BL_CUDA(c, c->rs_nv.alloc(P));
-    BL_CUDA(c, cudaStreamSynchronize(c->stream));
     c->N = N, c->M = M, c->B = B;
+    if ((rc = commit_fem(c))) return rc;
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
     c->bodies_dirty = false;
     c->committed = true;
     drop_graphs(c);
@@ -348,8 +588,15 @@ static int ensure_committed(bl_gpu_ctx* c) {
     return BL_GPU_OK;
 }
 
-// One frame of n substeps on stream s: 2n + 3 kernels. ev (2n + 4 events, or null): recorded before the first kernel
-// and after each one.
+// One frame of n substeps on stream s: without FEM frames 2n + 3 kernels. ev (2n + 4 events, or null): recorded
+// before the first kernel, after the frame's start, after each substep's beams (and triangles) and after the rest of
+// each substep, after the frame's end kernels.
+static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
+    int64_t per = 2;
+    if (c->NF > 0) per += c->fem_launches;
+    return per * n + 3;
+}
+
 static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev = nullptr) {
     int q = 0;
     auto mark = [&]() {
@@ -362,12 +609,37 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     const int gb = (std::max(c->M, c->B) + tb - 1) / tb, gn = (c->N + tb - 1) / tb, gbody = (c->B + tb - 1) / tb;
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
     mark();
+    NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p};
+    const FemDev& F = c->fd;
     for (int k = 0; k < n; k++) {
+        if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
         k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fv.p, c->nd.p, c->dbodies.p,
                                                c->M, c->B);
+        if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
         k_nodes<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc.p, c->fv.p, c->dbodies.p, c->st, c->cfg.gravity[0],
-                                               c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0);
+                                               c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0, nfm);
+        if (c->NF > 0) {
+            // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
+            k_fem_assemble<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
+            const int nlev = (int)c->lvl_col_ptr.size() - 1;
+            for (int L = 0; L < nlev; L++) {
+                const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1], g0 = c->lvl_grp_ptr[L], g1 = c->lvl_grp_ptr[L + 1];
+                k_fem_chol_level<<<(c1 - c0 + 3) / 4, 128, 0, s>>>(F, c0, c1);
+                if (g1 > g0) k_fem_update_level<<<(g1 - g0 + 3) / 4, 128, 0, s>>>(F, g0, g1);
+            }
+            for (int L = 0; L < nlev; L++) {
+                const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
+                k_fem_forward_level<<<(c1 - c0 + 3) / 4, 128, 0, s>>>(F, c0, c1);
+            }
+            for (int L = nlev - 1; L >= 0; L--) {
+                const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
+                k_fem_backward_level<<<(c1 - c0 + 3) / 4, 128, 0, s>>>(F, c0, c1);
+            }
+            k_fem_velocity<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
+            k_fem_integrate<<<(c->n_fem_nodes + 255) / 256, 256, 0, s>>>(F, c->nd.p, c->nforce.p, c->fem_nodes.p, c->n_fem_nodes, c->fslot.p, c->info.p,
+                                                                       c->dbodies.p, dt);
+        }
         mark();
     }
     RepairScratch rs{c->rs_sort.p, c->rs_bad.p, c->rs_np.p, c->rs_nv.p, c->rs_P};
@@ -376,6 +648,53 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     mark();
     k_sleep_apply<<<std::max(c->B, 1), 256, 0, s>>>(c->dbodies.p, c->nd.p, c->bmeta.p);
     mark();
+    return BL_GPU_OK;
+}
+
+// A body's FEM frame of triangle elements made ready (bl_fem_host.cuh): frame nodes in the order FemFrame::add_tri
+// makes them, FemFrame::finalize's rest shapes and inertias, analyse's pattern, the elements' stiffnesses.
+static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32_t n_nodes, const bl_fem_desc& fd, std::vector<FemSection>& sections,
+                           std::shared_ptr<FemModel>& out) {
+    if (!fd.tris || !fd.sections || fd.n_sections <= 0 || !nodes || !info) return BL_GPU_EINVAL;
+    sections.clear();
+    for (int k = 0; k < fd.n_sections; k++) {
+        const bl_shell_section& ss = fd.sections[k];
+        if (ss.yield > 0) return BL_GPU_EUNSUPPORTED; // (plastic flow, folds and tears: not on this path)
+        if (!(ss.t > 0) || !(ss.E > 0)) return BL_GPU_EINVAL;
+        sections.push_back(FemSection{ss.E, ss.nu, ss.rho, ss.t, ss.yield, ss.damping, ss.drill});
+    }
+    auto M = std::make_shared<FemModel>();
+    std::vector<int> slot(n_nodes, -1);
+    auto add_node = [&](uint32_t bn) {
+        if (slot[bn] < 0) slot[bn] = (int)M->node.size(), M->node.push_back(bn);
+        return slot[bn];
+    };
+    for (int t = 0; t < fd.n_tris; t++) {
+        const bl_fem_tri& tr = fd.tris[t];
+        if (tr.a >= (uint32_t)n_nodes || tr.b >= (uint32_t)n_nodes || tr.c >= (uint32_t)n_nodes || tr.section >= fd.n_sections) return BL_GPU_EINVAL;
+        const int a = add_node(tr.a), b = add_node(tr.b), cc = add_node(tr.c);
+        M->tn.push_back({a, b, cc});
+        M->tsec.push_back(tr.section);
+        M->tmass.push_back(tr.mass);
+    }
+    for (uint32_t bn : M->node)
+        if (info[bn].flags & BL_NF_GROUND) return BL_GPU_EUNSUPPORTED; // (a frame's static contacts: not on this path)
+    std::vector<float> px(n_nodes), py(n_nodes), pz(n_nodes), ms(n_nodes);
+    for (int i = 0; i < n_nodes; i++) px[i] = nodes[i].p[0], py[i] = nodes[i].p[1], pz[i] = nodes[i].p[2], ms[i] = nodes[i].mass;
+    fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data());
+    bool again = false;
+    for (size_t t = 0; t < M->tn.size(); t++) // (the caller's mass, else its section's over its area: tri_mass, frame_fem.h:373)
+        if (!(M->tmass[t] > 0)) M->tmass[t] = sections[M->tsec[t]].rho * sections[M->tsec[t]].t * M->tarea0[t], again = true;
+    if (again) fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data()); // (the inertias from those masses)
+    fem_analyse(*M);
+    M->tk.assign(162 * M->tn.size(), 0.0f);
+    for (size_t t = 0; t < M->tn.size(); t++) {
+        if (M->tbroken[t]) continue;
+        float X[3][2];
+        for (int i = 0; i < 3; i++) X[i][0] = M->tX[6 * t + 2 * i], X[i][1] = M->tX[6 * t + 2 * i + 1];
+        tri_stiffness_host(X, sections[M->tsec[t]], &M->tk[162 * t]);
+    }
+    out = M;
     return BL_GPU_OK;
 }
 
@@ -552,6 +871,18 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
         for (int k = 0; k < 3; k++) mn[k] = (n.p[k] < mn[k]) ? n.p[k] : mn[k], mx[k] = (mx[k] < n.p[k]) ? n.p[k] : mx[k];
     for (int k = 0; k < 3; k++) r.aabb_mn[k] = mn[k], r.aabb_mx[k] = mx[k];
     hb.beam_bits = (d->allow_deform ? BB_DEFORM : 0u) | (d->allow_break ? BB_BREAK : 0u) | (d->ductile ? BB_DUCTILE : 0u);
+    if (d->fem && d->fem->n_tris > 0) {
+        std::shared_ptr<FemModel> M;
+        const int rc = build_fem_model(d->nodes, d->info, d->n_nodes, *d->fem, hb.sections, M);
+        if (rc) return rc;
+        hb.fq.assign(4 * M->node.size(), 0.0f);
+        for (size_t i = 0; i < M->node.size(); i++) hb.fq[4 * i + 3] = 1.0f;
+        hb.fw.assign(3 * M->node.size(), 0.0f);
+        // (solve_begin's clamps, frame_fem.cpp:2525-2526)
+        hb.diss = std::min(std::max(d->fem->dissipation, 0.0f), 1.0f);
+        hb.theta = std::min(std::max(d->fem->theta, 0.25f + 0.5f * hb.diss), 1.0f);
+        hb.fem = M;
+    }
     c->bodies.push_back(std::move(hb));
     c->bodies_dirty = true;
     if (body_id) *body_id = (int32_t)c->bodies.size() - 1;
@@ -583,7 +914,7 @@ int bl_gpu_step_substeps(bl_gpu_ctx* c, int32_t n, void* stream) {
     }
     if ((rc = order_on(c, s))) return rc;
     BL_CUDA(c, cudaGraphLaunch(it->second, s));
-    c->launches += 2 * (int64_t)n + 3;
+    c->launches += frame_launches(c, n);
     return BL_GPU_OK;
 }
 
@@ -663,6 +994,11 @@ int bl_gpu_body_state(bl_gpu_ctx* c, int32_t body, bl_body_state* out) {
     out->broken_beams = r.broken_beams;
     out->sleep_timer = r.sleep_timer;
     out->repaired_nodes = r.repaired;
+    out->fem_failures = out->fem_clamps = 0;
+    if (c->NF > 0) {
+        BL_CUDA(c, cudaMemcpy(&out->fem_failures, c->fem_fail.p + body, sizeof(int), cudaMemcpyDeviceToHost));
+        BL_CUDA(c, cudaMemcpy(&out->fem_clamps, c->fem_clamp.p + body, sizeof(int), cudaMemcpyDeviceToHost));
+    }
     return BL_GPU_OK;
 }
 
@@ -743,7 +1079,7 @@ int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profil
     if ((rc = order_on(c, s))) return rc;
     BL_CUDA(c, cudaGraphLaunch(pg.exec, s));
     BL_CUDA(c, cudaStreamSynchronize(s));
-    c->launches += 2 * (int64_t)n + 3;
+    c->launches += frame_launches(c, n);
     c->total_substeps += n;
     c->last_substeps = n;
     cudaError_t terr = cudaSuccess;
@@ -761,6 +1097,54 @@ int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profil
     return BL_GPU_OK;
 }
 
+int bl_gpu_set_node_force(bl_gpu_ctx* c, int32_t body, int32_t node, const float force[3]) {
+    if (!c || body < 0 || body >= (int32_t)c->bodies.size() || !force) return BL_GPU_EINVAL;
+    HostBody& hb = c->bodies[body];
+    if (node < 0 || node >= (int32_t)hb.nodes.size()) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    const bool had = !hb.ext.empty();
+    if (!had) hb.ext.assign(hb.nodes.size(), make_float4(0, 0, 0, 0));
+    hb.ext[node] = make_float4(force[0], force[1], force[2], 0.0f);
+    if (!had || !c->committed) { // (the body's first: its flag and the array are laid out again)
+        int rc = pull_state(c);
+        if (rc) return rc;
+        c->bodies_dirty = true;
+        return BL_GPU_OK;
+    }
+    if (c->bodies_dirty) return BL_GPU_OK;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    BL_CUDA(c, cudaMemcpy(c->ext.p + hb.rec.node0 + node, &hb.ext[node], sizeof(float4), cudaMemcpyHostToDevice));
+    return BL_GPU_OK;
+}
+
+int bl_gpu_download_fem(bl_gpu_ctx* c, int32_t body, int32_t* n, int32_t* node, double* xd, float* q, float* w) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    const HostBody& hb = c->bodies[body];
+    if (n) *n = hb.fem ? (int32_t)hb.fem->node.size() : 0;
+    if (!hb.fem) return BL_GPU_OK;
+    int fo = 0;
+    for (int bi = 0; bi < body; bi++)
+        if (c->bodies[bi].fem) fo += (int)c->bodies[bi].fem->node.size();
+    const int nf = (int)hb.fem->node.size();
+    if (node)
+        for (int i = 0; i < nf; i++) node[i] = (int32_t)hb.fem->node[i];
+    if (xd) BL_CUDA(c, cudaMemcpy(xd, c->xd.p + 3 * (size_t)fo, sizeof(double) * 3 * nf, cudaMemcpyDeviceToHost));
+    if (q || w) {
+        std::vector<float4> tmp(nf);
+        if (q) {
+            BL_CUDA(c, cudaMemcpy(tmp.data(), c->fq.p + fo, sizeof(float4) * nf, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < nf; i++) q[4 * i] = tmp[i].x, q[4 * i + 1] = tmp[i].y, q[4 * i + 2] = tmp[i].z, q[4 * i + 3] = tmp[i].w;
+        }
+        if (w) {
+            BL_CUDA(c, cudaMemcpy(tmp.data(), c->fw.p + fo, sizeof(float4) * nf, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < nf; i++) w[3 * i] = tmp[i].x, w[3 * i + 1] = tmp[i].y, w[3 * i + 2] = tmp[i].z;
+        }
+    }
+    return BL_GPU_OK;
+}
+
 int bl_gpu_body_range(bl_gpu_ctx* c, int32_t body, int32_t* first_node, int32_t* n_nodes, int32_t* first_beam, int32_t* n_beams) {
     int rc = check_body(c, body);
     if (rc) return rc;
@@ -769,6 +1153,25 @@ int bl_gpu_body_range(bl_gpu_ctx* c, int32_t body, int32_t* first_node, int32_t*
     if (n_nodes) *n_nodes = r.nnodes;
     if (first_beam) *first_beam = r.beam0;
     if (n_beams) *n_beams = r.nbeams;
+    return BL_GPU_OK;
+}
+
+int bl_fem_pattern(const bl_node* nodes, const bl_node_info* info, int32_t n_nodes, const bl_fem_desc* fem, int32_t sizes[4], int32_t* perm,
+                   int32_t* col_ptr, int32_t* row, int32_t* upd, float* rest, float* inertia) {
+    if (!fem || !sizes || n_nodes < 0) return BL_GPU_EINVAL;
+    std::vector<FemSection> secs;
+    std::shared_ptr<FemModel> M;
+    const int rc = build_fem_model(nodes, info, n_nodes, *fem, secs, M);
+    if (rc) return rc;
+    const int nf = (int)M->node.size();
+    sizes[0] = nf, sizes[1] = (int32_t)M->row.size(), sizes[2] = (int32_t)M->upd.size(), sizes[3] = M->ncomp;
+    if (perm) std::copy(M->perm.begin(), M->perm.end(), perm);
+    if (col_ptr) std::copy(M->col_ptr.begin(), M->col_ptr.end(), col_ptr);
+    if (row) std::copy(M->row.begin(), M->row.end(), row);
+    if (upd)
+        for (size_t u = 0; u < M->upd.size(); u++) upd[3 * u] = M->upd[u][0], upd[3 * u + 1] = M->upd[u][1], upd[3 * u + 2] = M->upd[u][2];
+    if (rest) std::copy(M->tX.begin(), M->tX.end(), rest);
+    if (inertia) std::copy(M->inertia.begin(), M->inertia.end(), inertia);
     return BL_GPU_OK;
 }
 

@@ -288,3 +288,72 @@ def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, si
     return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005},
             "statics": {"terrain": terrain, "boxes": [], "build_grid": True}, "bodies": bodies,
             "name": f"fleet(n={n_vehicles}, seed={seed})"}
+
+
+def shell_plate(n: int = 63, size: float = 1.0, origin=(0.0, 1.0, 0.0), thickness: float = 0.0015, E: float = 210e9,
+                nu: float = 0.3, rho: float = 7850.0, damping: float = 3e-4, drill: float = 0.05, clamp_edge: bool = True,
+                load: float = 500.0, seed: int = 1, node_flags: int = 0) -> dict:
+    """The co-rotational FEM shell plate: (n + 1)^2 nodes on a size x size square in the horizontal plane at `origin`,
+    2 n^2 CST/DKT triangles (two a cell, diagonals alternating: ShellMesher::grid, fem_shell.cpp:34-50), an elastic
+    steel section (E, nu, rho, thickness), each triangle's mass a third on each corner; the edge z = origin.z clamped
+    (anchored nodes); a seeded random point load of `load` N on a uniformly drawn free node; gravity. The default is
+    the 64 x 64-node, 7,938-triangle plate of 1.5 mm steel."""
+    ox, oy, oz = (np.float32(v) for v in origin)
+    du = np.float32(size / n)
+    pos = np.zeros(((n + 1) * (n + 1), 3), np.float32)
+    for j in range(n + 1):
+        for i in range(n + 1):
+            k = j * (n + 1) + i
+            # origin + du * i + dv * j, in float (du along x, dv along z)
+            x = np.float32(ox + np.float32(du * np.float32(i))) + np.float32(0.0)
+            z = np.float32(oz + np.float32(0.0)) + np.float32(du * np.float32(j))
+            pos[k] = (x, np.float32(np.float32(oy + np.float32(0.0)) + np.float32(0.0)), z)
+    nn = len(pos)
+    mass = np.zeros(nn, np.float32)
+    tris = []
+    tmass = []
+    mpm2 = np.float32(np.float32(rho) * np.float32(thickness))
+
+    def tri(a, b, c):
+        pa, pb, pc = pos[a], pos[b], pos[c]
+        e1, e2 = pb - pa, pc - pa
+        cr = np.array([e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]], np.float32)
+        area = np.float32(0.5) * np.sqrt(np.float32(cr[0] * cr[0] + cr[1] * cr[1]) + np.float32(cr[2] * cr[2]))
+        m = np.float32(mpm2 * area)
+        for v in (a, b, c):
+            mass[v] = np.float32(mass[v] + np.float32(m / np.float32(3.0)))
+        tris.append((a, b, c))
+        tmass.append(m)
+
+    for j in range(n):
+        for i in range(n):
+            n00, n10 = j * (n + 1) + i, j * (n + 1) + i + 1
+            n01, n11 = (j + 1) * (n + 1) + i, (j + 1) * (n + 1) + i + 1
+            if (i + j) & 1:
+                tri(n00, n10, n11), tri(n00, n11, n01)
+            else:
+                tri(n00, n10, n01), tri(n10, n11, n01)
+    flags = np.full(nn, node_flags, np.uint16)
+    if clamp_edge:
+        flags[: n + 1] |= NF_FIXED
+    rng = np.random.default_rng(seed)
+    free = np.nonzero((flags & NF_FIXED) == 0)[0]
+    node = int(free[rng.integers(len(free))])
+    d = rng.normal(size=3)
+    f = (load * d / np.linalg.norm(d)).astype(np.float32)
+    body = {
+        "pos": pos, "vel": np.zeros((nn, 3), np.float32), "mass": mass, "node_flags": flags,
+        "friction": np.ones(nn, np.float32), "radius": np.zeros(nn, np.float32),
+        "ab": np.zeros((0, 2), np.uint32), "k": np.zeros(0, np.float32), "d": np.zeros(0, np.float32),
+        "strength": np.zeros(0, np.float32), "deform": np.zeros(0, np.float32), "beam_type": np.zeros(0, np.uint8),
+        "beam_flags": np.zeros(0, np.uint8),
+        "params": {"ground_friction": 1.0, "bounce": -1.0, "contact_push_max": 2.0, "contact_slop": 0.0,
+                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 1, "ductile": 0, "can_sleep": 0,
+                   "sleep_speed": 0.0},
+        "fem_sections": [{"E": E, "nu": nu, "rho": rho, "t": thickness, "yield": 0.0, "damping": damping, "drill": drill}],
+        "fem_tris": np.asarray(tris, np.uint32), "fem_tri_mass": np.asarray(tmass, np.float32),
+        "loads": [(node, tuple(float(x) for x in f))],
+        "plate": {"n": n, "size": size, "origin": tuple(float(v) for v in origin)},
+    }
+    return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005}, "statics": {}, "bodies": [body],
+            "name": f"shell_plate(n={n}, seed={seed})"}

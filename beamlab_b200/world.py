@@ -114,6 +114,11 @@ class SoftBody:
         self.nodes = np.zeros(0, NODE_DTYPE)
         self.info = np.zeros(0, NODE_INFO_DTYPE)
         self.beams = np.zeros(0, BEAM_DTYPE)
+        # FEM frame of triangle elements (FemFrame: add_shell_section / add_tri)
+        self.fem_sections: list[dict] = []
+        self.fem_tris = np.zeros(0, FEM_TRI_DTYPE)
+        self.fem_theta = 0.5
+        self.fem_dissipation = 0.02
 
     def add_node(self, p, mass: float, flags: int = NF_GROUND | NF_CONTACTER, v=(0.0, 0.0, 0.0), friction=1.0,
                  radius=0.0) -> int:
@@ -165,6 +170,14 @@ class SoftBody:
         sb.nodes, sb.info, sb.beams = nodes, info, beams
         for k_, v_ in body.get("params", {}).items():
             setattr(sb, k_, v_)
+        if "fem_tris" in body:
+            sb.fem_sections = list(body["fem_sections"])
+            ft = np.zeros(len(body["fem_tris"]), FEM_TRI_DTYPE)
+            tri = np.asarray(body["fem_tris"], np.uint32).reshape(-1, 3)
+            ft["a"], ft["b"], ft["c"] = tri[:, 0], tri[:, 1], tri[:, 2]
+            ft["section"] = np.asarray(body.get("fem_tri_section", np.zeros(len(tri))), np.uint16)
+            ft["mass"] = np.asarray(body["fem_tri_mass"], np.float32)
+            sb.fem_tris = ft
         sb._finalize_arrays()
         return sb
 
@@ -200,18 +213,33 @@ class SoftBody:
         return len(self.nodes)
 
 
+class _ShellSection(C.Structure):
+    _fields_ = [("E", C.c_float), ("nu", C.c_float), ("rho", C.c_float), ("t", C.c_float), ("yield_", C.c_float),
+                ("damping", C.c_float), ("drill", C.c_float)]
+
+
+FEM_TRI_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("c", "<u4"), ("section", "<u2"), ("pad", "<u2"), ("mass", "<f4")])
+
+
+class _FemDesc(C.Structure):
+    _fields_ = [("n_sections", C.c_int32), ("sections", C.c_void_p), ("n_tris", C.c_int32), ("tris", C.c_void_p),
+                ("theta", C.c_float), ("dissipation", C.c_float)]
+
+
 class _BodyDesc(C.Structure):
     _fields_ = [("n_nodes", C.c_int32), ("nodes", C.c_void_p), ("info", C.c_void_p), ("n_beams", C.c_int32),
                 ("beams", C.c_void_p), ("ground_friction", C.c_float), ("bounce", C.c_float),
                 ("contact_push_max", C.c_float), ("contact_slop", C.c_float), ("allow_deform", C.c_int32),
                 ("allow_break", C.c_int32), ("ductile", C.c_int32), ("can_sleep", C.c_int32),
-                ("sleep_speed", C.c_float), ("max_speed", C.c_float), ("sleeping", C.c_int32)]
+                ("sleep_speed", C.c_float), ("max_speed", C.c_float), ("sleeping", C.c_int32),
+                ("fem", C.POINTER(_FemDesc))]
 
 
 class _BodyState(C.Structure):
     _fields_ = [("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3), ("max_speed", C.c_float),
                 ("sleeping", C.c_int32), ("static_contacts", C.c_int32), ("broken_beams", C.c_int32),
-                ("sleep_timer", C.c_float), ("repaired_nodes", C.c_int32)]
+                ("sleep_timer", C.c_float), ("repaired_nodes", C.c_int32), ("fem_failures", C.c_int32),
+                ("fem_clamps", C.c_int32)]
 
 
 class _WorldStats(C.Structure):
@@ -261,7 +289,28 @@ class BodyHandle:
         return {"aabb_min": np.array(s.aabb_min, np.float32), "aabb_max": np.array(s.aabb_max, np.float32),
                 "max_speed": float(s.max_speed), "sleeping": bool(s.sleeping), "static_contacts": s.static_contacts,
                 "broken_beams": s.broken_beams, "sleep_timer": float(s.sleep_timer),
-                "repaired_nodes": s.repaired_nodes}
+                "repaired_nodes": s.repaired_nodes, "fem_failures": s.fem_failures, "fem_clamps": s.fem_clamps}
+
+    def fem(self) -> dict | None:
+        """The FEM frame's nodes: body node, double positions, orientations (x y z w), angular velocities."""
+        L, ctx = self.world._L, self.world._ctx
+        n = C.c_int32()
+        _check(L.bl_gpu_download_fem(ctx, self.index, C.byref(n), None, None, None, None), "download_fem", ctx)
+        if n.value == 0:
+            return None
+        node = np.zeros(n.value, np.int32)
+        xd = np.zeros((n.value, 3), np.float64)
+        q = np.zeros((n.value, 4), np.float32)
+        w = np.zeros((n.value, 3), np.float32)
+        _check(L.bl_gpu_download_fem(ctx, self.index, C.byref(n), node.ctypes.data, xd.ctypes.data, q.ctypes.data,
+                                     w.ctypes.data), "download_fem", ctx)
+        return {"node": node, "xd": xd, "q": q, "w": w}
+
+    def set_node_force(self, node: int, force):
+        """A constant force on one node, every substep after gravity (a SoftBody::pre_substep push)."""
+        f = (C.c_float * 3)(*[float(x) for x in force])
+        _check(self.world._L.bl_gpu_set_node_force(self.world._ctx, self.index, int(node), f), "set_node_force",
+               self.world._ctx)
 
 
 class World:
@@ -335,10 +384,20 @@ class World:
         nodes = np.ascontiguousarray(body.nodes, NODE_DTYPE)
         info = np.ascontiguousarray(body.info, NODE_INFO_DTYPE)
         beams = np.ascontiguousarray(body.beams, BEAM_DTYPE)
+        fem_ptr = None
+        if len(body.fem_tris):
+            secs = (_ShellSection * len(body.fem_sections))(*[
+                _ShellSection(float(x["E"]), float(x["nu"]), float(x["rho"]), float(x["t"]), float(x.get("yield", 0.0)),
+                              float(x.get("damping", 3e-4)), float(x.get("drill", 0.05))) for x in body.fem_sections])
+            tris = np.ascontiguousarray(body.fem_tris, FEM_TRI_DTYPE)
+            fd = _FemDesc(len(body.fem_sections), C.cast(secs, C.c_void_p), len(tris), tris.ctypes.data,
+                          float(body.fem_theta), float(body.fem_dissipation))
+            self._keep += [secs, tris, fd]
+            fem_ptr = C.pointer(fd)
         d = _BodyDesc(len(nodes), nodes.ctypes.data, info.ctypes.data, len(beams), beams.ctypes.data,
                       body.ground_friction, body.bounce, body.contact_push_max, body.contact_slop,
                       int(body.allow_deform), int(body.allow_break), int(body.ductile), int(body.can_sleep),
-                      body.sleep_speed, 0.0, 0)
+                      body.sleep_speed, 0.0, 0, fem_ptr)
         idx = C.c_int32()
         _check(self._L.bl_gpu_add_body(self._ctx, C.byref(d), C.byref(idx)), "add_body", self._ctx)
         h = BodyHandle(self, idx.value, len(nodes), len(beams), body.name)
@@ -434,7 +493,9 @@ def world_from_rig(rig: dict, device: int = 0, **overrides) -> World:
     if "kill_y" in st:
         w.statics.kill_y = st["kill_y"]
     for i, b in enumerate(rig["bodies"]):
-        w.add_body(SoftBody.from_arrays(b, name=f"body{i}"))
+        h = w.add_body(SoftBody.from_arrays(b, name=f"body{i}"))
+        for node, f in b.get("loads", []):
+            h.set_node_force(node, f)
     return w
 
 

@@ -50,6 +50,12 @@ def workload(name: str, rank: int):
         desc = (f"fleet256: 256 lattice vehicles ({n:,} nodes, {m:,} beams; log-normal 500-20,000 nodes, median "
                 f"3,000), 2048^2-sample 1 km^2 heightfield, 5-30 m/s random yaw; no wheel rings, no inter-vehicle "
                 f"contacts")
+    elif name == "plate64":
+        rig = rigs.shell_plate(63, seed=1 + rank)
+        n, m = rigs.rig_counts(rig)
+        desc = ("plate64: co-rotational FEM shell plate, 64 x 64 nodes (4,096), 7,938 CST/DKT triangles, 1 m x 1 m, "
+                "1.5 mm steel (E 210 GPa, nu 0.3, 7,850 kg/m^3), one edge clamped, a seeded 500 N point load, gravity; "
+                "implicit step every substep: 64,411 off-diagonal 6x6 blocks, 1,359,082 block updates")
     elif name == "truss_car":
         rig = rigs.truss_car(1 + rank)
         n, m = rigs.rig_counts(rig)
@@ -300,7 +306,7 @@ def main():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fleet256", choices=["fleet256", "truss_car"])
+    ap.add_argument("--workload", default="fleet256", choices=["fleet256", "plate64", "truss_car"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -92,9 +92,39 @@ typedef struct {
     uint16_t group;
 } bl_beam;
 
+/* == the fields of bl::phys::ShellSection (frame_fem.h:114-150) the elastic shell step reads */
+typedef struct {
+    float E, nu, rho, t;       /* Young's modulus (Pa), Poisson's ratio, density (kg/m3), thickness (m) */
+    float yield;               /* yield stress (Pa): 0 only (elastic); a yielding section is BL_GPU_EUNSUPPORTED */
+    float damping;             /* stiffness-proportional damping (s) */
+    float drill;               /* the corners' drilling spring, a share of G t A */
+} bl_shell_section;
+
+/* A triangle element between three body nodes, as FemFrame::add_tri makes it (frame_fem.cpp:201-209), and the mass
+ * it put on its corners (ShellMesher::tri, fem_shell.cpp:17-31; <= 0: its section's areal mass) */
+typedef struct {
+    uint32_t a, b, c;
+    uint16_t section;
+    uint16_t pad;
+    float mass;
+} bl_fem_tri;
+
+/* A body's FEM frame of triangle elements (FemFrame, frame_fem.h:330-815: its add_tri calls; no members or mounts).
+ * The library does what the reference's FemFrame::finalize and analyse do (rest shapes, inertias, the minimum-degree
+ * ordering and the factor's pattern) and steps it implicitly every substep (FemFrame::solve, frame_fem.cpp:2512-3027). */
+typedef struct {
+    int32_t n_sections;
+    const bl_shell_section* sections;
+    int32_t n_tris;
+    const bl_fem_tri* tris;
+    float theta;               /* WorldSettings::frame_theta (0.5) */
+    float dissipation;         /* SoftBody::fem_dissipation, else WorldSettings::frame_dissipation (0.02) */
+} bl_fem_desc;
+
 /* One body: a SoftBody after finalize (softbody.cpp:76-83) - its arrays and the knobs of the explicit path
- * (softbody.h:650-700). Bodies with shocks, joints, wheels, slide nodes, sheets, FEM frames, air drag or grab are
- * rejected with BL_GPU_EUNSUPPORTED by the caller's shim (this record has no fields for them). */
+ * (softbody.h:650-700), and optionally its FEM frame of triangle elements. Bodies with shocks, joints, wheels, slide
+ * nodes, sheets, FEM members or mounts, air drag or grab are rejected with BL_GPU_EUNSUPPORTED by the caller's shim
+ * (this record has no fields for them); so is a FEM frame whose nodes collide with the static world (NF_GROUND). */
 typedef struct {
     int32_t n_nodes;
     const bl_node* nodes;
@@ -112,6 +142,7 @@ typedef struct {
     float sleep_speed;         /* SoftBody::sleep_speed (0: the world's) */
     float max_speed;           /* SoftBody::max_speed at upload (the first frame's static query margin) */
     int32_t sleeping;          /* SoftBody::sleeping at upload */
+    const bl_fem_desc* fem;    /* NULL: no FEM frame */
 } bl_body_desc;
 
 /* A body's runtime state (SoftBody::aabb, max_speed, sleeping, static_contacts, stats.broken_beams, sleep_timer) */
@@ -124,6 +155,8 @@ typedef struct {
     int32_t broken_beams;      /* since upload */
     float sleep_timer;
     int32_t repaired_nodes;    /* nodes World::repair_nodes reset, since upload */
+    int32_t fem_failures;      /* FemFrame::solve_failures: failed factorizations and non-finite velocity changes */
+    int32_t fem_clamps;        /* FemFrame::clamps: velocity changes cut to the safety limits */
 } bl_body_state;
 
 /* WorldStats (world.h:79-132), the fields this path fills, and the device's error word */
@@ -166,6 +199,14 @@ int bl_gpu_set_kill_y(bl_gpu_ctx* ctx, float y);
 /* World::add_body (world.cpp:283-289): copies the body in; *body_id is its index (0, 1, ... in order). */
 int bl_gpu_add_body(bl_gpu_ctx* ctx, const bl_body_desc* desc, int32_t* body_id);
 
+/* A constant force (N) on one node of a body, added every substep right after gravity - what a SoftBody::pre_substep
+ * controller that pushes a node does (world.cpp:3261). Zero removes it. */
+int bl_gpu_set_node_force(bl_gpu_ctx* ctx, int32_t body, int32_t node, const float force[3]);
+
+/* A body's FEM frame nodes (FemFrame::node / xd / q / w, frame_fem.h:331-350): body node, double position (3),
+ * orientation (x y z w), angular velocity (3); n the frame node count (0: none). Any pointer may be NULL. */
+int bl_gpu_download_fem(bl_gpu_ctx* ctx, int32_t body, int32_t* n, int32_t* node, double* xd, float* q, float* w);
+
 /* World::step_substeps(n) (world.cpp:368-585): one frame of n substeps of every awake body, enqueued on `stream`
  * (a cudaStream_t; NULL: the context's own). Asynchronous. */
 int bl_gpu_step_substeps(bl_gpu_ctx* ctx, int32_t n, void* stream);
@@ -202,6 +243,15 @@ typedef struct {
     float finish_ms;           /* the frame's end (bounds, repair, sleep) */
 } bl_frame_profile;
 int bl_gpu_profile_frame(bl_gpu_ctx* ctx, int32_t n, void* stream, bl_frame_profile* out);
+
+/* The symbolic phase of a FEM frame, on the host, no GPU needed: what bl_gpu_add_body computes for the frame of `fem`
+ * over the body's nodes - FemFrame::analyse's exact minimum-degree order and factor pattern (frame_fem.cpp:544-860)
+ * and FemFrame::finalize's rest shapes and inertias (frame_fem.cpp:224-260, 3075-3086). sizes[0..3] receive the frame
+ * nodes, off-diagonal blocks, block updates and components; any array may be NULL (call once with NULLs for sizes):
+ * perm (frame nodes), col_ptr (frame nodes + 1), row (blocks), upd (3 per update: pi, pj, target as the reference
+ * stores them), rest (6 per triangle: its corners in its plane), inertia (frame nodes). */
+int bl_fem_pattern(const bl_node* nodes, const bl_node_info* info, int32_t n_nodes, const bl_fem_desc* fem, int32_t sizes[4], int32_t* perm,
+                   int32_t* col_ptr, int32_t* row, int32_t* upd, float* rest, float* inertia);
 
 /* One substep - gravity, the beams' spring-dampers with yield and breaking, symplectic Euler - of one body whose
  * device buffers the caller owns, for callers that cannot let the library allocate GPU memory: their memory belongs to

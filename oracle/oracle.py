@@ -83,6 +83,13 @@ def _load(path: str, prefix: str) -> C.CDLL:
     if prefix == "ref":
         lib.ref_jobs_init.argtypes = [i]
         lib.ref_jobs_threads.restype = i
+        lib.ref_add_plate.argtypes = [vp, i] + [f] * 9 + [f] * 7 + [i, i]
+        lib.ref_add_plate.restype = i
+        lib.ref_set_point_load.argtypes = [vp, i, i, f, f, f]
+        lib.ref_fem_info.argtypes = [vp, i, C.POINTER(C.c_longlong)]
+        lib.ref_fem_pattern.argtypes = [vp, i, vp, vp, vp, vp]
+        lib.ref_fem_nodes.argtypes = [vp, i, vp, vp, vp, vp]
+        lib.ref_fem_tris.argtypes = [vp, i, vp, vp, vp, vp, vp]
     _loaded[path] = lib
     return lib
 
@@ -187,6 +194,50 @@ class _OracleWorld:
                 "sleep_timer": float(o[10])}
 
 
+class _FemMixin:
+    """The reference's FEM frames (RefWorld only): shell plates built by its own ShellMesher, their pattern and state."""
+
+    def add_plate(self, body: dict) -> int:
+        pl = body["plate"]
+        sec = body["fem_sections"][0]
+        n, size = int(pl["n"]), float(pl["size"])
+        o = pl["origin"]
+        du = float(np.float32(size / n))
+        b = self._lib.ref_add_plate(self._w, n, *map(float, o), du, 0.0, 0.0, 0.0, 0.0, du, float(sec["E"]), float(sec["nu"]),
+                                    float(sec["rho"]), float(sec["t"]), float(sec.get("yield", 0.0)), float(sec.get("damping", 3e-4)),
+                                    float(sec.get("drill", 0.05)), 1 if (body["node_flags"][0] & 2) else 0, int(body["node_flags"][-1]))
+        for node, fv in body.get("loads", []):
+            self._lib.ref_set_point_load(self._w, b, int(node), *map(float, fv))
+        return b
+
+    def fem_info(self, body: int) -> dict:
+        o = (C.c_longlong * 7)()
+        self._lib.ref_fem_info(self._w, body, o)
+        return dict(zip(("frame_nodes", "tris", "components", "blocks", "updates", "solve_failures", "clamps"), list(o)))
+
+    def fem_pattern(self, body: int) -> dict:
+        info = self.fem_info(body)
+        n, nb, nu = info["frame_nodes"], info["blocks"], info["updates"]
+        out = {"perm": np.zeros(n, np.int32), "col_ptr": np.zeros(n + 1, np.int32), "row": np.zeros(nb, np.int32),
+               "upd": np.zeros(3 * nu, np.int32)}
+        self._lib.ref_fem_pattern(self._w, body, *(out[k].ctypes.data for k in ("perm", "col_ptr", "row", "upd")))
+        return out
+
+    def fem_nodes(self, body: int) -> dict:
+        n = self.fem_info(body)["frame_nodes"]
+        out = {"node": np.zeros(n, np.int32), "xd": np.zeros((n, 3), np.float64), "q": np.zeros((n, 4), np.float32),
+               "w": np.zeros((n, 3), np.float32)}
+        self._lib.ref_fem_nodes(self._w, body, *(out[k].ctypes.data for k in ("node", "xd", "q", "w")))
+        return out
+
+    def fem_tris(self, body: int) -> dict:
+        t = self.fem_info(body)["tris"]
+        out = {"n": np.zeros((t, 3), np.int32), "X": np.zeros((t, 6), np.float32), "r0": np.zeros((t, 12), np.float32),
+               "mass": np.zeros(t, np.float32), "area0": np.zeros(t, np.float32)}
+        self._lib.ref_fem_tris(self._w, body, *(out[k].ctypes.data for k in ("n", "X", "r0", "mass", "area0")))
+        return out
+
+
 class PortWorld(_OracleWorld):
     """The plain-C restatement (single-threaded)."""
 
@@ -196,8 +247,8 @@ class PortWorld(_OracleWorld):
         super().__init__(_load(PORT_LIB, "orc"))
 
 
-class RefWorld(_OracleWorld):
-    """The reference's own World, compiled from its sources (flavour "parity" or "timing")."""
+class RefWorld(_FemMixin, _OracleWorld):
+    """The reference's own World, compiled from its sources (flavour "parity", "libm" or "timing")."""
 
     prefix = "ref"
 
@@ -236,5 +287,10 @@ def build_world(cls, rig: dict, **settings):
     w.settings(**s)
     w.load_statics(rig.get("statics", {}))
     for b in rig["bodies"]:
-        w.add_body(b)
+        if "plate" in b:
+            if not hasattr(w, "add_plate"):
+                raise ValueError("FEM plates step in the reference only (RefWorld)")
+            w.add_plate(b)
+        else:
+            w.add_body(b)
     return w

@@ -9,13 +9,28 @@
 //   ref_add_box / ref_build_grid        -> StaticWorld::add_box / build_grid        (src/phys/static_world.h:193-195)
 //   ref_add_body                        -> SoftBody::add_node / add_beam / finalize (src/phys/softbody.h:953-973)
 //   ref_jobs_init                       -> JobSystem::get().init                   (src/core/jobs.h:22)
-#include "core/jobs.h"
-#include "phys/world.h"
-
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <functional>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <tuple>
 #include <vector>
+
+#include "core/jobs.h"
+// (the FEM frame's solver pattern - ordering, blocks, updates - is private to FemFrame; the checker reads it)
+#define private public
+#include "phys/fem_shell.h"
+#include "phys/world.h"
+#undef private
 
 using namespace bl;
 using namespace bl::phys;
@@ -122,6 +137,84 @@ int ref_add_body(RefWorld* r, int n_nodes, const float* pos, const float* vel, c
 }
 
 void ref_step_substeps(RefWorld* r, int n) { r->w.step_substeps(n); }
+
+// ---- FEM shell plates (ShellMesher::grid, fem_shell.cpp:34-50) ----
+// A plate body of n x n cells: origin + du * i + dv * j, triangle elements of one shell section (E, nu, rho, t,
+// yield, damping, drill as given), the nodes of row j = 0 anchored (NF_FIXED) when clamp_edge, gravity on. Its nodes
+// carry node_flags. Returns the body index.
+int ref_add_plate(RefWorld* r, int n, float ox, float oy, float oz, float dux, float duy, float duz, float dvx, float dvy, float dvz, float E, float nu,
+                  float rho, float t, float yield, float damping, float drill, int clamp_edge, int node_flags) {
+    auto b = std::make_unique<SoftBody>();
+    b->name = "plate" + std::to_string(r->bodies.size());
+    b->can_sleep = false;
+    ShellSection s = make_shell_section("Steel", t);
+    s.E = E, s.nu = nu, s.rho = rho, s.t = t, s.yield = yield, s.damping = damping, s.drill = drill;
+    s.pattern = ShellPattern::None;
+    s.max_level = 0;
+    const uint16_t sec = b->fem.add_shell_section(s);
+    ShellMesher m(*b, (uint16_t)node_flags);
+    const std::vector<uint32_t> ids = m.grid(vec3(ox, oy, oz), vec3(dux, duy, duz), vec3(dvx, dvy, dvz), n, n, sec, false);
+    if (clamp_edge)
+        for (int i = 0; i <= n; i++) b->info[ids[i]].flags |= NF_FIXED;
+    m.finish();
+    b->finalize();
+    SoftBody* bp = r->w.add_body(std::move(b));
+    bp->fem.finalize(*bp); // (what its first step would do: FemFrame::begin_forces, frame_fem.cpp:1860)
+    r->bodies.push_back(bp);
+    return (int)r->bodies.size() - 1;
+}
+
+// A constant force on one node of a body, applied every substep right after gravity (the SoftBody::pre_substep hook,
+// world.cpp:3261)
+void ref_set_point_load(RefWorld* r, int body, int node, float fx, float fy, float fz) {
+    SoftBody* b = r->bodies[body];
+    const vec3 f(fx, fy, fz);
+    const uint32_t nd = (uint32_t)node;
+    b->pre_substep = [nd, f](SoftBody& sb, float) {
+        if (nd < sb.force.size()) sb.force[nd] += f;
+    };
+}
+
+// the frame's pattern sizes: [frame nodes, tris, components, off-diagonal blocks, block updates, solve failures, clamps]
+void ref_fem_info(RefWorld* r, int body, long long* out) {
+    const FemFrame& f = r->bodies[body]->fem;
+    out[0] = (long long)f.node.size(), out[1] = (long long)f.tris.size(), out[2] = f.components(), out[3] = (long long)f.row_.size();
+    out[4] = (long long)f.upd_.size(), out[5] = f.solve_failures, out[6] = f.clamps;
+}
+
+// the pattern itself: perm (n), col_ptr (n + 1), row (blocks), upd as (pi, pj, target) triples
+void ref_fem_pattern(RefWorld* r, int body, int* perm, int* col_ptr, int* row, int* upd) {
+    const FemFrame& f = r->bodies[body]->fem;
+    std::copy(f.perm_.begin(), f.perm_.end(), perm);
+    std::copy(f.col_ptr_.begin(), f.col_ptr_.end(), col_ptr);
+    std::copy(f.row_.begin(), f.row_.end(), row);
+    for (size_t u = 0; u < f.upd_.size(); u++) upd[3 * u] = f.upd_[u].pi, upd[3 * u + 1] = f.upd_[u].pj, upd[3 * u + 2] = f.upd_[u].target;
+}
+
+// the frame nodes' state: body node, double positions (3), orientation (x y z w), angular velocity (3)
+void ref_fem_nodes(RefWorld* r, int body, int* node, double* xd, float* q, float* w) {
+    const FemFrame& f = r->bodies[body]->fem;
+    for (size_t i = 0; i < f.node.size(); i++) {
+        node[i] = (int)f.node[i];
+        xd[3 * i] = f.xd[3 * i], xd[3 * i + 1] = f.xd[3 * i + 1], xd[3 * i + 2] = f.xd[3 * i + 2];
+        q[4 * i] = f.q[i].x, q[4 * i + 1] = f.q[i].y, q[4 * i + 2] = f.q[i].z, q[4 * i + 3] = f.q[i].w;
+        w[3 * i] = f.w[i].x, w[3 * i + 1] = f.w[i].y, w[3 * i + 2] = f.w[i].z;
+    }
+}
+
+// the triangles: nodes (frame nodes, 3), rest shape X (6), rest frames r0 (12), mass, area0
+void ref_fem_tris(RefWorld* r, int body, int* n, float* X, float* r0, float* mass, float* area0) {
+    const FemFrame& f = r->bodies[body]->fem;
+    for (size_t t = 0; t < f.tris.size(); t++) {
+        const FrameTri& tr = f.tris[t];
+        for (int i = 0; i < 3; i++) {
+            n[3 * t + i] = (int)tr.n[i];
+            X[6 * t + 2 * i] = tr.X[i][0], X[6 * t + 2 * i + 1] = tr.X[i][1];
+            r0[12 * t + 4 * i] = tr.r0[i].x, r0[12 * t + 4 * i + 1] = tr.r0[i].y, r0[12 * t + 4 * i + 2] = tr.r0[i].z, r0[12 * t + 4 * i + 3] = tr.r0[i].w;
+        }
+        mass[t] = tr.mass, area0[t] = tr.area0;
+    }
+}
 
 int ref_body_nodes(RefWorld* r, int body) { return (int)r->bodies[body]->nodes.size(); }
 int ref_body_beams(RefWorld* r, int body) { return (int)r->bodies[body]->beams.size(); }
