@@ -56,6 +56,12 @@ def workload(name: str, rank: int):
         desc = ("plate64: co-rotational FEM shell plate, 64 x 64 nodes (4,096), 7,938 CST/DKT triangles, 1 m x 1 m, "
                 "1.5 mm steel (E 210 GPa, nu 0.3, 7,850 kg/m^3), one edge clamped, a seeded 500 N point load, gravity; "
                 "implicit step every substep: 64,411 off-diagonal 6x6 blocks, 1,359,082 block updates")
+    elif name == "plate64":
+        rig = rigs.shell_plate(63, seed=1 + rank)
+        n, m = rigs.rig_counts(rig)
+        desc = ("plate64: co-rotational FEM shell plate, 64 x 64 nodes (4,096), 7,938 CST/DKT triangles, 1 m x 1 m, "
+                "1.5 mm steel (E 210 GPa, nu 0.3, 7,850 kg/m^3), one edge clamped, a seeded 500 N point load, gravity; "
+                "implicit step every substep: 64,411 off-diagonal 6x6 blocks, 1,359,082 block updates")
     elif name == "truss_car":
         rig = rigs.truss_car(1 + rank)
         n, m = rigs.rig_counts(rig)
