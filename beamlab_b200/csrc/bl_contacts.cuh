@@ -1,0 +1,1025 @@
+// Contacts between bodies: islands, the candidate pairs of nodes and collision triangles, their narrow phase and the
+// contact response in the reference's pair order.
+//
+// Reference: World::build_islands (world.cpp:636-762), World::rebuild_pairs (world.cpp:1851-2308: node-triangle
+// pairs only - no capsules, plate mid points or self collision), World::fast_pairs (world.cpp:2314-2520),
+// World::near_pairs (world.cpp:2525-2598), World::pair_detect (world.cpp:2807-2858), World::collide_pairs
+// (world.cpp:2964-3023) with contact_force<1,3> and hull_push_out<3> (world.cpp:59-120), the wake requests of sleeping
+// bodies (world.cpp:2983-2995, 3333-3337).
+//
+// Layout. Collision triangles of all bodies back to back: int4 (a, b, c as global node indices; flags: bit 0 two-sided,
+// bit 1 torn, bits 8.. the body) and their longest rest edge squared. Each frame k_islands labels every body with the
+// first body of its island (the reference numbers islands in that order and keeps each island's bodies in body
+// order). An island with two or more bodies has contact pairs: its bodies' nodes are "split" - k_nodes phase 0 stores
+// their gravity + beam forces in `fsplit`, the contacts add to those, and k_nodes phase 1 finishes them (static
+// contact, integration) - while every other body keeps the fused node kernel.
+//
+// The pair search runs on the substeps the reference rebuilds on (the frame's first and every rebuild interval after):
+// one CTA per island (k_rebuild) makes the island's margins and cell size, the partners, the spatial hash of the slow
+// bodies' contacter nodes (cell_hash & mask buckets, each bucket in node order), the triangles' queries, the fast
+// bodies' dense grids and their partners' queries, and keeps the pairs near_pairs keeps - in the reference's order: a
+// count pass, one global range for the island, a write pass. Every substep k_detect finds the contacts of all pairs
+// in parallel and k_collide applies them one island per thread, pair after pair: contact_force cancels the force
+// accumulated so far on both sides, so the order within an island is the reference's.
+#pragma once
+
+#include "bl_kernels.cuh"
+
+namespace blg {
+
+constexpr int kIslMaxBodies = 256;     // bodies of one island with contact pairs (more: DEVERR_ISLAND)
+constexpr int kGridCells = 48 * 48 * 48;
+constexpr int kGridItemsPerNode = 4;   // fast grid entries per node (a node in the cells of its travel)
+constexpr float kFastSpeed = 8.0f;     // world.cpp:1881
+constexpr float kTornStretch2 = 2.5f * 2.5f; // softbody.h:154
+enum : uint32_t { TF_TWO_SIDED = 1, TF_TORN = 2 };
+enum : uint32_t { DEVERR_PAIRS = 4, DEVERR_ISLAND = 8, DEVERR_GRID = 16, DEVERR_CONTACT_UNSUPPORTED = 32 };
+
+struct Contacts {
+    int4* tri;                 // a, b, c, flags | body << 8
+    const float* tri_rest2;
+    int* parent;               // per body: union-find
+    float* ibox;               // per body: island box (6)
+    int* isl_live;             // per root body: the island has an awake body
+    int* isl_cnt;              // per root body: its bodies
+    int* isl_nodes;            // per root body: its nodes
+    int* isl_idx;              // per root body: its rank among the islands with pairs
+    int* isl_noff;             // per root body: first node of its scratch
+    int* isl_poff;             // per root body: its pairs in `pairs`
+    int* isl_pcnt;
+    int* isl_contacts;         // per root body: this frame's contacts (stats)
+    int* pair_total;           // pairs of all islands (reset before each rebuild)
+    int2* pairs;               // (node, triangle), global indices
+    float4* hit_a;             // per pair: bary.xyz, pen
+    float4* hit_b;             // per pair: normal.xyz, w = 1 when the pair is in contact
+    int max_pairs;
+    // rebuild scratch
+    int* pt_node;              // hashed nodes of an island, in order
+    int* pt_body;
+    int4* pt_cell;
+    int* bk_start;             // buckets (4 n + 65 per island)
+    int* bk_fill;
+    int* bk_items;             // hashed nodes by bucket
+    int* run_end;
+    int* g_start;              // fast grids (kGridCells + 1 per island)
+    int* g_fill;
+    int* g_items;              // kGridItemsPerNode per node
+    float4* fsplit;            // per node: the force before the contacts (bodies of islands with pairs)
+    int* counters;             // [0] pair searches [1] contacts [2] pairs of the searches
+    int interval;              // rebuild interval in substeps (world.cpp:1887)
+    float dt;
+    float wake_speed;          // WorldSettings::sleep_speed
+};
+
+// ------------------------------------------------------------------------------------------ geometry (reference order)
+__device__ __forceinline__ v3 cross(v3 a, v3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+__device__ __forceinline__ float length2(v3 a) { return dot(a, a); }
+__device__ __forceinline__ v3 vmin3(v3 a, v3 b) { return {smin(a.x, b.x), smin(a.y, b.y), smin(a.z, b.z)}; }
+__device__ __forceinline__ v3 vmax3(v3 a, v3 b) { return {smax(a.x, b.x), smax(a.y, b.y), smax(a.z, b.z)}; }
+__device__ __forceinline__ v3 neg(v3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ v3 nd_p(const float4* nd, int i) {
+    const float4 p = nd[2 * i];
+    return V(p.x, p.y, p.z);
+}
+__device__ __forceinline__ v3 nd_v(const float4* nd, int i) {
+    const float4 v = nd[2 * i + 1];
+    return V(v.x, v.y, v.z);
+}
+__device__ __forceinline__ float max_edge2(v3 a, v3 b, v3 c) { return smax(length2(b - a), smax(length2(c - b), length2(a - c))); }
+
+// world.cpp:23-25 (the int products wrap, as the reference's do)
+__device__ __forceinline__ uint32_t cell_hash(int x, int y, int z) {
+    return ((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349663u) ^ ((uint32_t)z * 83492791u);
+}
+
+// closest_on_triangle (softbody.h:158-190, Ericson 5.1.5)
+__device__ v3 closest_on_triangle(v3 p, v3 a, v3 b, v3 c, v3& bary) {
+    const v3 ab = b - a, ac = c - a, ap = p - a;
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0 && d2 <= 0) {
+        bary = V(1, 0, 0);
+        return a;
+    }
+    const v3 bp = p - b;
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0 && d4 <= d3) {
+        bary = V(0, 1, 0);
+        return b;
+    }
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+        const float v = d1 / (d1 - d3);
+        bary = V(1 - v, v, 0);
+        return a + ab * v;
+    }
+    const v3 cp = p - c;
+    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0 && d5 <= d6) {
+        bary = V(0, 0, 1);
+        return c;
+    }
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+        const float w = d2 / (d2 - d6);
+        bary = V(1 - w, 0, w);
+        return a + ac * w;
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+        const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        bary = V(0, 1 - w, w);
+        return b + (c - b) * w;
+    }
+    const float denom = 1.0f / (va + vb + vc);
+    const float v = vb * denom, w = vc * denom;
+    bary = V(1 - v - w, v, w);
+    return a + ab * v + ac * w;
+}
+
+// near_triangle (world.cpp:1135-1142)
+__device__ __forceinline__ bool near_triangle(v3 p, v3 a, v3 b, v3 c, v3 tu, float r, bool two_sided, float depth) {
+    const float s = dot(p - a, tu);
+    v3 bary;
+    if (two_sided) return fabsf(s) <= r && length2(closest_on_triangle(p, a, b, c, bary) - p) <= r * r;
+    if (s > r || s < -r - depth) return false;
+    const v3 q = p - tu * s;
+    return length2(closest_on_triangle(q, a, b, c, bary) - q) <= r * r;
+}
+
+__device__ __forceinline__ bool outside(v3 p, v3 mn, v3 mx) { return p.x < mn.x || p.y < mn.y || p.z < mn.z || p.x > mx.x || p.y > mx.y || p.z > mx.z; }
+
+// ------------------------------------------------------------------------------------------ block helpers
+// exclusive scan of one int per thread of the block; *total: the block's sum. Every thread of the block calls it.
+__device__ int block_scan_excl(int v, int& total, int* s_warp) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = lane < nw ? s_warp[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < nw) s_warp[lane] = t;
+    }
+    __syncthreads();
+    const int before = (w > 0 ? s_warp[w - 1] : 0) + x - v;
+    total = s_warp[nw - 1];
+    __syncthreads();
+    return before;
+}
+
+// ------------------------------------------------------------------------------------------ islands (once a frame)
+__device__ __forceinline__ int uf_find(volatile int* parent, int x) {
+    while (true) {
+        const int p = parent[x];
+        if (p == x) return x;
+        x = p;
+    }
+}
+__device__ void uf_union(int* parent, int a, int b) {
+    while (true) {
+        a = uf_find(parent, a), b = uf_find(parent, b);
+        if (a == b) return;
+        if (a > b) {
+            const int t = a;
+            a = b, b = t;
+        }
+        if (atomicCAS(&parent[b], b, a) == b) return; // (the larger root under the smaller: a component's root is its first body)
+    }
+}
+
+// World::build_islands (world.cpp:636-720) for bodies that can touch: node-triangle contacts only (no capsules or
+// collision volumes). One block. Bodies with FEM frames take no contacts here: one that would is flagged
+// (DEVERR_CONTACT_UNSUPPORTED) and stays in an island of its own.
+__global__ void __launch_bounds__(1024) k_islands(Body* __restrict__ bodies, int nb, float frame_time, int world_sleeping, Contacts C,
+                                                  uint32_t* __restrict__ deverr) {
+    __shared__ int s_warp[32];
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        Body& B = bodies[i];
+        if (!world_sleeping) B.sleeping = 0;
+        C.parent[i] = i;
+        C.isl_live[i] = 0, C.isl_cnt[i] = 0, C.isl_nodes[i] = 0, C.isl_pcnt[i] = 0, C.isl_contacts[i] = 0;
+        const float m = (B.sleeping ? 0.05f : smin(B.max_speed, 200.0f) * frame_time * 2.0f + 0.3f) + (B.hull ? B.hull_depth : 0.0f);
+        float* bx = C.ibox + 6 * i;
+        bx[0] = B.aabb_mn[0] - m, bx[1] = B.aabb_mn[1] - m, bx[2] = B.aabb_mn[2] - m;
+        bx[3] = B.aabb_mx[0] + m, bx[4] = B.aabb_mx[1] + m, bx[5] = B.aabb_mx[2] + m;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        const Body& Bi = bodies[i];
+        const float* a = C.ibox + 6 * i;
+        for (int j = i + 1; j < nb; j++) {
+            const float* b = C.ibox + 6 * j;
+            if (!(a[0] <= b[3] && a[3] >= b[0] && a[1] <= b[4] && a[4] >= b[1] && a[2] <= b[5] && a[5] >= b[2])) continue;
+            const Body& Bj = bodies[j];
+            if (Bi.sleeping && Bj.sleeping) continue;
+            if (Bi.group != 0 && Bi.group == Bj.group) continue;
+            const bool can = (Bi.contacters && Bj.ntris > 0) || (Bj.contacters && Bi.ntris > 0);
+            if (!can) continue;
+            if (Bi.is_fem || Bj.is_fem) {
+                atomicOr(deverr, DEVERR_CONTACT_UNSUPPORTED);
+                continue;
+            }
+            uf_union(C.parent, i, j);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        const int r = uf_find(C.parent, i);
+        C.parent[i] = r;
+        atomicAdd(&C.isl_cnt[r], 1);
+        atomicAdd(&C.isl_nodes[r], bodies[i].nnodes);
+        if (!bodies[i].sleeping) atomicOr(&C.isl_live[r], 1);
+    }
+    __syncthreads();
+    // the islands with pairs: their rank and their first node of scratch (in body order)
+    int carry_n = 0, carry_i = 0;
+    for (int base = 0; base < nb; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        bool pr = false;
+        if (i < nb) {
+            Body& B = bodies[i];
+            const int r = C.parent[i];
+            const bool live = C.isl_live[r] != 0;
+            B.island = live ? r : -1;
+            B.pairs = live && C.isl_cnt[r] > 1 ? 1 : 0;
+            B.body_contacts = 0;
+            pr = r == i && B.pairs;
+        }
+        int tn, ti;
+        const int on = block_scan_excl(pr ? C.isl_nodes[i] : 0, tn, s_warp);
+        const int oi = block_scan_excl(pr ? 1 : 0, ti, s_warp);
+        if (pr) C.isl_noff[i] = carry_n + on, C.isl_idx[i] = carry_i + oi;
+        carry_n += tn, carry_i += ti;
+    }
+}
+
+// ------------------------------------------------------------------------------------------ wake requests (each substep)
+// simulate_island's substep start (world.cpp:3333-3337): a sleeping body a moving partner touched wakes; its beams step
+// again (SoftBody::wake, softbody.h:996).
+__global__ void k_wake(Body* __restrict__ bodies, uint32_t* __restrict__ bmeta) {
+    Body& B = bodies[blockIdx.x];
+    if (!B.wake_request || B.island < 0) return;
+    for (int j = threadIdx.x; j < B.nbeams; j += blockDim.x) bmeta[B.beam0 + j] &= ~kBeamAsleep;
+    __syncthreads();
+    if (threadIdx.x == 0) B.wake_request = 0, B.sleeping = 0, B.sleep_timer = 0.0f;
+}
+
+// ------------------------------------------------------------------------------------------ the pair search
+struct IslBody {
+    int id;               // global body index
+    float sp;             // max_speed now (the frame's running maximum)
+    float extra;          // extra pair margin of a fast body
+    float bulk;           // bulk speed of a fast body
+    float mn[3], mx[3];   // its bounds now
+    float bmn[3], bmx[3]; // its box grown by the reach (Island::boxes)
+};
+
+struct RebuildShared {
+    IslBody b[kIslMaxBodies];
+    uint32_t partner[kIslMaxBodies][kIslMaxBodies / 32];
+    double term0[1024];
+    double term1[1024];
+    int warp[32];
+    int nb;
+    float rmax, margin, inv_cell, slow_speed, slow_reach, travel;
+    int npts, mask;
+    int count;
+    // the fast grid of the current fast body
+    float g_org[3], g_inv;
+    int g_dim[3];
+};
+
+__device__ __forceinline__ bool same_group(const Body& a, const Body& b) { return a.group != 0 && a.group == b.group; }
+
+__device__ __forceinline__ bool box_hits(const float* mn, const float* mx, v3 qmn, v3 qmx) {
+    return qmn.x <= mx[0] && qmx.x >= mn[0] && qmn.y <= mx[1] && qmx.y >= mn[1] && qmn.z <= mx[2] && qmx.z >= mn[2];
+}
+// near_partner (world.cpp:1955-1962)
+__device__ bool near_partner(const RebuildShared& S, int k, v3 mn, v3 mx) {
+    for (int w = 0; w < kIslMaxBodies / 32; w++) {
+        uint32_t bits = S.partner[k][w];
+        while (bits) {
+            const int o = w * 32 + __ffs(bits) - 1;
+            bits &= bits - 1;
+            if (box_hits(S.b[o].bmn, S.b[o].bmx, mn, mx)) return true;
+        }
+    }
+    return false;
+}
+__device__ __forceinline__ bool has_partner(const RebuildShared& S, int k) {
+    for (int w = 0; w < kIslMaxBodies / 32; w++)
+        if (S.partner[k][w]) return true;
+    return false;
+}
+
+// near_pairs' test of one candidate (world.cpp:2536-2583); T: the reach's time
+__device__ bool near_keep(const float4* __restrict__ nd, const Body& bn, const Body& bt, int node, int4 t, float T) {
+    if (t.w & TF_TORN) return false;
+    const bool two_sided = (t.w & TF_TWO_SIDED) != 0;
+    const v3 xp = nd_p(nd, node), xv = nd_v(nd, node);
+    const v3 ap = nd_p(nd, t.x), bp = nd_p(nd, t.y), cp = nd_p(nd, t.z);
+    const v3 av = nd_v(nd, t.x), bv = nd_v(nd, t.y), cv = nd_v(nd, t.z);
+    v3 bary;
+    const v3 q = closest_on_triangle(xp, ap, bp, cp, bary);
+    const float r0 = bn.crad + (two_sided ? 0.0f : bt.hull_depth);
+    const v3 da = xv - av, db = xv - bv, dc = xv - cv;
+    const float vrel = sqrtf(smax(length2(da), smax(length2(db), length2(dc))));
+    const float reach = r0 + 1.25f * vrel * T + 0.02f;
+    if (length2(xp - q) >= reach * reach) return false;
+    const v3 nn = cross(bp - ap, cp - ap);
+    const float nl = length(nn);
+    if (nl > 1e-12f) {
+        const v3 n0 = divs(nn, nl);
+        const float s0 = dot(n0, xp - ap);
+        if (two_sided || s0 > bn.crad) {
+            const float sg = s0 >= 0 ? 1.0f : -1.0f;
+            const float close = smax(0.0f, smax(-sg * dot(n0, da), smax(-sg * dot(n0, db), -sg * dot(n0, dc))));
+            if (fabsf(s0) - 1.25f * close * T - 0.02f >= bn.crad) return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ int cell_of(float v, float inv_cell) { return (int)floorf(v * inv_cell); }
+
+// One triangle of body bt (island slot kt) against the slow bodies' hash (world.cpp:2037-2083), near_pairs' filter
+// applied: counts the pairs, and writes them from `out` when it is given.
+__device__ int slow_query(const RebuildShared& S, const Contacts& C, const Body* __restrict__ bodies, const float4* __restrict__ nd, int kt, int tg,
+                          int bk0, int pt0, float T, int2* out) {
+    const Body& o = bodies[S.b[kt].id];
+    const int4 tr = C.tri[tg];
+    if (tr.w & TF_TORN) return 0;
+    const bool two_sided = (tr.w & TF_TWO_SIDED) != 0;
+    const float depth = two_sided ? 0.0f : o.hull_depth;
+    const float rq = S.rmax + S.margin + S.b[kt].extra + depth;
+    const v3 a = nd_p(nd, tr.x), bb = nd_p(nd, tr.y), c = nd_p(nd, tr.z);
+    const v3 tmn = vmin3(a, vmin3(bb, c)), tmx = vmax3(a, vmax3(bb, c));
+    const v3 vr = V(rq, rq, rq);
+    if (!near_partner(S, kt, tmn - vr, tmx + vr)) return 0;
+    const v3 tn = cross(bb - a, c - a);
+    const float tn2 = dot(tn, tn);
+    const v3 tu = tn2 > 1e-20f ? tn * (1.0f / sqrtf(tn2)) : V(0, 0, 0);
+    const float ic = S.inv_cell;
+    const int x0 = cell_of(tmn.x - rq, ic), x1 = cell_of(tmx.x + rq, ic);
+    const int y0 = cell_of(tmn.y - rq, ic), y1 = cell_of(tmx.y + rq, ic);
+    const int z0 = cell_of(tmn.z - rq, ic), z1 = cell_of(tmx.z + rq, ic);
+    if ((long long)(x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1) > 512) return 0; // degenerate/exploded
+    const int bt = S.b[kt].id;
+    int n = 0;
+    for (int z = z0; z <= z1; z++)
+        for (int y = y0; y <= y1; y++)
+            for (int x = x0; x <= x1; x++) {
+                const int bk = (int)(cell_hash(x, y, z) & (uint32_t)S.mask);
+                const int k1 = C.bk_start[bk0 + bk + 1];
+                for (int k = C.bk_start[bk0 + bk]; k < k1; k++) {
+                    const int pi = C.bk_items[pt0 + k];
+                    const int pb = C.pt_body[pt0 + pi];
+                    if (pb == bt) { // own nodes: skip the whole run
+                        k = C.run_end[pt0 + k] - 1;
+                        continue;
+                    }
+                    const int4 pc = C.pt_cell[pt0 + pi];
+                    if (pc.x != x || pc.y != y || pc.z != z) continue; // hash collision
+                    const int node = C.pt_node[pt0 + pi];
+                    const v3 p = nd_p(nd, node);
+                    if (p.x < tmn.x - rq || p.y < tmn.y - rq || p.z < tmn.z - rq || p.x > tmx.x + rq || p.y > tmx.y + rq || p.z > tmx.z + rq) continue;
+                    const Body& b = bodies[pb];
+                    if (same_group(b, o)) continue;
+                    if (b.sleeping && o.sleeping) continue;
+                    const float r = b.crad + S.margin + S.b[kt].extra;
+                    const float rb = r + depth;
+                    if (p.x < tmn.x - rb || p.y < tmn.y - rb || p.z < tmn.z - rb || p.x > tmx.x + rb || p.y > tmx.y + rb || p.z > tmx.z + rb) continue;
+                    if (!near_triangle(p, a, bb, c, tu, r, two_sided, depth)) continue;
+                    if (!near_keep(nd, b, o, node, tr, T)) continue;
+                    if (out) out[n] = make_int2(node, tg);
+                    n++;
+                }
+            }
+    return n;
+}
+
+// The fast body's grid cell of p (World::fast_pairs' cell_index, world.cpp:2341-2346), per axis
+__device__ __forceinline__ int3 grid_cell(const RebuildShared& S, v3 p) {
+    const int x = min(max((int)((p.x - S.g_org[0]) * S.g_inv), 0), S.g_dim[0] - 1);
+    const int y = min(max((int)((p.y - S.g_org[1]) * S.g_inv), 0), S.g_dim[1] - 1);
+    const int z = min(max((int)((p.z - S.g_org[2]) * S.g_inv), 0), S.g_dim[2] - 1);
+    return make_int3(x, y, z);
+}
+// the cells a node of the fast body is listed in: those within its own travel (world.cpp:2350-2362), as a box of cells
+__device__ __forceinline__ void node_cells(const RebuildShared& S, const float4* __restrict__ nd, int node, int3& lo, int3& hi) {
+    const v3 p = nd_p(nd, node);
+    const float m = length(nd_v(nd, node)) * S.travel;
+    const v3 vm = V(m, m, m);
+    lo = grid_cell(S, p - vm);
+    hi = grid_cell(S, p + vm);
+}
+
+// One triangle of partner body `ko` against fast body `kf`'s grid (world.cpp:2394-2475), near_pairs' filter applied;
+// the pairs come out in node order (the reference sorts and deduplicates the cells' lists; here a node listed in
+// several cells of the scan is taken in the first of them, and the triangle's pairs are sorted after).
+__device__ int fast_query(const RebuildShared& S, const Contacts& C, const Body* __restrict__ bodies, const float4* __restrict__ nd, int kf, int ko,
+                          int tg, int gs0, int gi0, float fast_extra_o, float T, int2* out) {
+    const Body& F = bodies[S.b[kf].id];
+    const Body& o = bodies[S.b[ko].id];
+    const int4 tr = C.tri[tg];
+    if (tr.w & TF_TORN) return 0;
+    const bool o_fast = S.b[ko].extra > 0;
+    const float r = F.crad + S.slow_reach + S.travel * (S.b[kf].sp + (o_fast ? S.b[ko].sp : 0.0f)) + fast_extra_o;
+    const v3 fmn = V(S.b[kf].mn[0] - r, S.b[kf].mn[1] - r, S.b[kf].mn[2] - r), fmx = V(S.b[kf].mx[0] + r, S.b[kf].mx[1] + r, S.b[kf].mx[2] + r);
+    const v3 a = nd_p(nd, tr.x), bb = nd_p(nd, tr.y), c = nd_p(nd, tr.z);
+    const v3 tmn = vmin3(a, vmin3(bb, c)), tmx = vmax3(a, vmax3(bb, c));
+    if (tmx.x < fmn.x || tmx.y < fmn.y || tmx.z < fmn.z || tmn.x > fmx.x || tmn.y > fmx.y || tmn.z > fmx.z) return 0;
+    const float r00 = F.crad + (o_fast ? 0.01f : S.slow_reach);
+    const float rt = o_fast ? r00 + S.travel * sqrtf(smax(length2(nd_v(nd, tr.x)), smax(length2(nd_v(nd, tr.y)), length2(nd_v(nd, tr.z))))) : r00;
+    const bool two_sided = (tr.w & TF_TWO_SIDED) != 0;
+    const float depth = two_sided ? 0.0f : o.hull_depth;
+    const v3 tn = cross(bb - a, c - a);
+    const float tn2 = dot(tn, tn);
+    const v3 tu = tn2 > 1e-20f ? tn * (1.0f / sqrtf(tn2)) : V(0, 0, 0);
+    const float rr = rt + depth;
+    const v3 mn = tmn - V(rr, rr, rr), mx = tmx + V(rr, rr, rr);
+    const int x0 = max(0, (int)floorf((mn.x - S.g_org[0]) * S.g_inv)), x1 = min(S.g_dim[0] - 1, (int)((mx.x - S.g_org[0]) * S.g_inv));
+    const int y0 = max(0, (int)floorf((mn.y - S.g_org[1]) * S.g_inv)), y1 = min(S.g_dim[1] - 1, (int)((mx.y - S.g_org[1]) * S.g_inv));
+    const int z0 = max(0, (int)floorf((mn.z - S.g_org[2]) * S.g_inv)), z1 = min(S.g_dim[2] - 1, (int)((mx.z - S.g_org[2]) * S.g_inv));
+    if (x0 > x1 || y0 > y1 || z0 > z1) return 0;
+    int n = 0;
+    for (int z = z0; z <= z1; z++)
+        for (int y = y0; y <= y1; y++)
+            for (int x = x0; x <= x1; x++) {
+                const int cell = (z * S.g_dim[1] + y) * S.g_dim[0] + x;
+                const int k0 = C.g_start[gs0 + cell], k1 = C.g_start[gs0 + cell + 1];
+                for (int k = k0; k < k1; k++) {
+                    const int ni = C.g_items[gi0 + k];
+                    // taken once: in the first cell (z, y, x order) of its own cells' box within the scan's box
+                    int3 lo, hi;
+                    node_cells(S, nd, ni, lo, hi);
+                    if (max(lo.x, x0) != x || max(lo.y, y0) != y || max(lo.z, z0) != z) continue;
+                    const v3 p = nd_p(nd, ni);
+                    const float rn = rt + length(nd_v(nd, ni)) * S.travel, rb = rn + depth;
+                    if (p.x < tmn.x - rb || p.y < tmn.y - rb || p.z < tmn.z - rb || p.x > tmx.x + rb || p.y > tmx.y + rb || p.z > tmx.z + rb) continue;
+                    if (!near_triangle(p, a, bb, c, tu, rn, two_sided, depth)) continue;
+                    if (!near_keep(nd, F, o, ni, tr, T)) continue;
+                    if (out) out[n] = make_int2(ni, tg);
+                    n++;
+                }
+            }
+    if (out)
+        for (int i = 1; i < n; i++) { // (by node: the order of the reference's sorted scan)
+            const int2 v = out[i];
+            int j = i - 1;
+            while (j >= 0 && out[j].x > v.x) out[j + 1] = out[j], j--;
+            out[j + 1] = v;
+        }
+    return n;
+}
+
+// acc += s_t[0] + s_t[1] + ... one after another, as the reference's loop adds them
+__device__ __forceinline__ void serial_add(double& acc, const double* s_t, int n) {
+    for (int i = 0; i < n; i++) acc += s_t[i];
+}
+
+// World::rebuild_pairs + near_pairs for one island with pairs (its first body = blockIdx.x); s0: the frame's first
+// substep (the bodies' bounds are the frame's, their top speeds are measured now: world.cpp:3216-3222).
+__global__ void __launch_bounds__(1024) k_rebuild(Body* __restrict__ bodies, int nbodies, const float4* __restrict__ nd, const int4* __restrict__ info,
+                                                  Contacts C, int s0, uint32_t* __restrict__ deverr) {
+    const int root = blockIdx.x;
+    if (root >= nbodies) return;
+    {
+        const Body& R = bodies[root];
+        if (!R.pairs || R.island != root) return;
+    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RebuildShared& S = *reinterpret_cast<RebuildShared*>(smem_raw);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) S.nb = 0;
+    for (int w = tid; w < kIslMaxBodies * (kIslMaxBodies / 32); w += nt) (&S.partner[0][0])[w] = 0u;
+    __syncthreads();
+    // ---- the island's bodies in body order
+    if (tid == 0) {
+        int n = 0;
+        for (int i = root; i < nbodies; i++)
+            if (C.parent[i] == root) {
+                if (n < kIslMaxBodies) S.b[n].id = i;
+                n++;
+            }
+        if (n > kIslMaxBodies) atomicOr(deverr, DEVERR_ISLAND), n = 0;
+        S.nb = n;
+    }
+    __syncthreads();
+    const int nb = S.nb;
+    if (nb == 0) return;
+    // ---- top speeds (measured over the nodes on the frame's first substep, world.cpp:3217-3222), bounds now
+    if (s0)
+        for (int k = 0; k < nb; k++) {
+            Body& B = bodies[S.b[k].id];
+            if (B.sleeping) continue;
+            float m2 = 0.0f;
+            for (int i = tid; i < B.nnodes; i += nt) m2 = smax(m2, length2(nd_v(nd, B.node0 + i)));
+            for (int o = 16; o > 0; o >>= 1) m2 = fmaxf(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+            if ((tid & 31) == 0 && m2 > 0.0f) atomic_max_f(&B.acc_v2, m2);
+        }
+    __syncthreads();
+    for (int k = tid; k < nb; k += nt) {
+        const Body& B = bodies[S.b[k].id];
+        S.b[k].sp = sqrtf(B.acc_v2);
+        const bool acc = !s0 && B.acc_mn[0] <= B.acc_mx[0]; // (stepped in the last substep: its bounds then)
+        for (int c = 0; c < 3; c++) S.b[k].mn[c] = acc ? B.acc_mn[c] : B.aabb_mn[c], S.b[k].mx[c] = acc ? B.acc_mx[c] : B.aabb_mx[c];
+        S.b[k].extra = 0.0f, S.b[k].bulk = 0.0f;
+    }
+    // ---- torn triangles (world.cpp:1870-1878)
+    for (int k = 0; k < nb; k++) {
+        const Body& B = bodies[S.b[k].id];
+        if (B.sleeping) continue;
+        for (int t = tid; t < B.ntris; t += nt) {
+            const int tg = B.tri0 + t;
+            int4 tr = C.tri[tg];
+            const float r2 = C.tri_rest2[tg];
+            if (!(tr.w & TF_TORN) && r2 > 0 && max_edge2(nd_p(nd, tr.x), nd_p(nd, tr.y), nd_p(nd, tr.z)) > kTornStretch2 * r2) {
+                tr.w |= TF_TORN;
+                C.tri[tg] = tr;
+            }
+        }
+    }
+    __syncthreads();
+    const float dt = C.dt;
+    const int interval = C.interval;
+    if (tid == 0) {
+        float rmax = 0.0f, slow = 0.0f;
+        for (int k = 0; k < nb; k++) {
+            const Body& B = bodies[S.b[k].id];
+            rmax = smax(rmax, B.crad);
+            if (S.b[k].sp <= kFastSpeed) slow = smax(slow, S.b[k].sp);
+        }
+        const float speed = slow + 0.5f;
+        S.rmax = rmax;
+        S.slow_speed = speed;
+        S.margin = 2.0f * speed * (float)interval * dt + 0.02f;
+        S.slow_reach = 2.0f * speed * (float)interval * dt + 0.01f;
+        S.travel = 1.25f * (float)interval * dt;
+    }
+    __syncthreads();
+    // ---- bulk speeds of the fast bodies: mass-weighted RMS in node order, in double (world.cpp:1891-1902)
+    for (int k = 0; k < nb; k++) {
+        const Body& B = bodies[S.b[k].id];
+        if (B.sleeping || !(S.b[k].sp > kFastSpeed)) continue;
+        double mv2 = 0.0, m = 0.0;
+        for (int c0 = 0; c0 < B.nnodes; c0 += nt) {
+            const int i = c0 + tid;
+            if (i < B.nnodes) {
+                const float4 v = nd[2 * (B.node0 + i) + 1];
+                S.term0[tid] = (double)v.w * length2(V(v.x, v.y, v.z));
+                S.term1[tid] = (double)v.w;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                const int n = min(nt, B.nnodes - c0);
+                serial_add(mv2, S.term0, n);
+                serial_add(m, S.term1, n);
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            const float bulk = clampf(m > 0 ? 1.25f * (float)sqrt(mv2 / m) : S.b[k].sp, kFastSpeed, 400.0f);
+            S.b[k].bulk = bulk;
+            S.b[k].extra = bulk * (float)interval * dt;
+        }
+        __syncthreads();
+    }
+    // ---- cell size: the mean longest edge of every 7th triangle, in double (world.cpp:1914-1926)
+    {
+        double tri_size = 0.0;
+        int samples = 0;
+        for (int k = 0; k < nb; k++) {
+            const Body& B = bodies[S.b[k].id];
+            const int ns = (B.ntris + 6) / 7;
+            for (int c0 = 0; c0 < ns; c0 += nt) {
+                const int q = c0 + tid;
+                if (q < ns) {
+                    const int4 tr = C.tri[B.tri0 + 7 * q];
+                    S.term0[tid] = (double)sqrtf(max_edge2(nd_p(nd, tr.x), nd_p(nd, tr.y), nd_p(nd, tr.z)));
+                }
+                __syncthreads();
+                if (tid == 0) serial_add(tri_size, S.term0, min(nt, ns - c0));
+                __syncthreads();
+            }
+            samples += ns;
+        }
+        if (tid == 0) {
+            const float mean = samples ? (float)(tri_size / samples) : 1.0f;
+            S.inv_cell = 1.0f / clampf(mean + 2.0f * (S.rmax + S.margin), 0.25f, 1.0f);
+        }
+    }
+    __syncthreads();
+    // ---- partners: bodies whose boxes, grown by the reach, overlap (world.cpp:1933-1954)
+    const float reach = S.rmax + S.margin;
+    for (int k = tid; k < nb; k += nt) {
+        const Body& B = bodies[S.b[k].id];
+        const float g = reach + S.b[k].extra + (B.hull ? B.hull_depth : 0.0f);
+        for (int c = 0; c < 3; c++) S.b[k].bmn[c] = S.b[k].mn[c] - g, S.b[k].bmx[c] = S.b[k].mx[c] + g;
+    }
+    __syncthreads();
+    for (int q = tid; q < nb * nb; q += nt) {
+        const int a = q / nb, b = q % nb;
+        if (b <= a) continue;
+        const Body& A = bodies[S.b[a].id];
+        const Body& Bb = bodies[S.b[b].id];
+        if (same_group(A, Bb) || (A.sleeping && Bb.sleeping)) continue;
+        if (!(S.b[a].bmn[0] <= S.b[b].bmx[0] && S.b[a].bmx[0] >= S.b[b].bmn[0] && S.b[a].bmn[1] <= S.b[b].bmx[1] && S.b[a].bmx[1] >= S.b[b].bmn[1] &&
+              S.b[a].bmn[2] <= S.b[b].bmx[2] && S.b[a].bmx[2] >= S.b[b].bmn[2]))
+            continue;
+        atomicOr(&S.partner[a][b >> 5], 1u << (b & 31));
+        atomicOr(&S.partner[b][a >> 5], 1u << (a & 31));
+    }
+    __syncthreads();
+    // ---- 1) the spatial hash of the slow bodies' contacter nodes (world.cpp:1966-1978), in body and node order
+    const int pt0 = C.isl_noff[root];
+    const int bk0 = 4 * pt0 + 65 * C.isl_idx[root];
+    {
+        int base = 0;
+        for (int k = 0; k < nb; k++) {
+            const Body& B = bodies[S.b[k].id];
+            if (!has_partner(S, k) || S.b[k].extra > 0) continue;
+            for (int c0 = 0; c0 < B.nnodes; c0 += nt) {
+                const int i = c0 + tid;
+                bool take = false;
+                int4 cell = make_int4(0, 0, 0, 0);
+                if (i < B.nnodes && ((uint32_t)info[B.node0 + i].x & NF_CONTACTER)) {
+                    const v3 p = nd_p(nd, B.node0 + i);
+                    if (near_partner(S, k, p, p)) {
+                        take = true;
+                        cell = make_int4(cell_of(p.x, S.inv_cell), cell_of(p.y, S.inv_cell), cell_of(p.z, S.inv_cell), 0);
+                    }
+                }
+                int tot;
+                const int at = block_scan_excl(take ? 1 : 0, tot, S.warp);
+                if (take) {
+                    C.pt_node[pt0 + base + at] = B.node0 + i;
+                    C.pt_body[pt0 + base + at] = S.b[k].id;
+                    C.pt_cell[pt0 + base + at] = cell;
+                }
+                base += tot;
+            }
+        }
+        if (tid == 0) {
+            int nbk = 64;
+            while (nbk < 2 * base) nbk <<= 1;
+            S.npts = base, S.mask = nbk - 1;
+        }
+        __syncthreads();
+    }
+    const int npts = S.npts, nbk = S.mask + 1;
+    int any_tris = 0;
+    for (int k = 0; k < nb; k++) any_tris |= bodies[S.b[k].id].ntris > 0;
+    if (npts > 0 && any_tris) {
+        // buckets: counts, starts, items (each bucket in node order), runs of one body's nodes
+        for (int q = tid; q <= nbk; q += nt) C.bk_start[bk0 + q] = 0;
+        __syncthreads();
+        for (int q = tid; q < npts; q += nt) {
+            const int4 c = C.pt_cell[pt0 + q];
+            atomicAdd(&C.bk_start[bk0 + (int)(cell_hash(c.x, c.y, c.z) & (uint32_t)S.mask) + 1], 1);
+        }
+        __syncthreads();
+        {
+            int carry = 0;
+            for (int c0 = 0; c0 <= nbk; c0 += nt) {
+                const int q = c0 + tid;
+                const int v = q <= nbk ? C.bk_start[bk0 + q] : 0;
+                int tot;
+                const int ex = block_scan_excl(v, tot, S.warp);
+                if (q <= nbk) C.bk_start[bk0 + q] = carry + ex + v;
+                carry += tot;
+            }
+        }
+        __syncthreads();
+        for (int q = tid; q < nbk; q += nt) C.bk_fill[bk0 + q] = C.bk_start[bk0 + q];
+        __syncthreads();
+        for (int q = tid; q < npts; q += nt) {
+            const int4 c = C.pt_cell[pt0 + q];
+            const int at = atomicAdd(&C.bk_fill[bk0 + (int)(cell_hash(c.x, c.y, c.z) & (uint32_t)S.mask)], 1);
+            C.bk_items[pt0 + at] = q;
+        }
+        __syncthreads();
+        for (int q = tid; q < nbk; q += nt) {
+            const int k0 = C.bk_start[bk0 + q], k1 = C.bk_start[bk0 + q + 1];
+            for (int i = k0 + 1; i < k1; i++) {
+                const int v = C.bk_items[pt0 + i];
+                int j = i - 1;
+                while (j >= k0 && C.bk_items[pt0 + j] > v) C.bk_items[pt0 + j + 1] = C.bk_items[pt0 + j], j--;
+                C.bk_items[pt0 + j + 1] = v;
+            }
+            for (int i = k1; i-- > k0;) {
+                const bool same = i + 1 < k1 && C.pt_body[pt0 + C.bk_items[pt0 + i + 1]] == C.pt_body[pt0 + C.bk_items[pt0 + i]];
+                C.run_end[pt0 + i] = same ? C.run_end[pt0 + i + 1] : i + 1;
+            }
+        }
+        __syncthreads();
+    }
+    const float T = (float)max(interval, 1) * dt;
+    const int gs0 = C.isl_idx[root] * (kGridCells + 1);
+    const int gi0 = kGridItemsPerNode * pt0;
+    // ---- 2) count, then 3) write: the slow queries (bodies with partners, triangles in order), then the fast pairs
+    int total = 0;
+    for (int pass = 0; pass < 2; pass++) {
+        int2* dst = nullptr;
+        int at = 0;
+        if (pass == 1) {
+            if (tid == 0) {
+                int off = atomicAdd(C.pair_total, total);
+                if (off + total > C.max_pairs) {
+                    atomicOr(deverr, DEVERR_PAIRS);
+                    off = -1;
+                }
+                S.count = off;
+                C.isl_poff[root] = off < 0 ? 0 : off;
+                C.isl_pcnt[root] = off < 0 ? 0 : total;
+                if (off >= 0) atomicAdd(&C.counters[2], total);
+            }
+            __syncthreads();
+            if (S.count < 0) return;
+            dst = C.pairs + S.count;
+        }
+        if (npts > 0 && any_tris) {
+            for (int kt = 0; kt < nb; kt++) {
+                const Body& o = bodies[S.b[kt].id];
+                if (!has_partner(S, kt)) continue;
+                for (int c0 = 0; c0 < o.ntris; c0 += nt) {
+                    const int t = c0 + tid;
+                    const int n = t < o.ntris ? slow_query(S, C, bodies, nd, kt, o.tri0 + t, bk0, pt0, T, nullptr) : 0;
+                    int tot;
+                    const int ex = block_scan_excl(n, tot, S.warp);
+                    if (pass == 1 && n > 0) slow_query(S, C, bodies, nd, kt, o.tri0 + t, bk0, pt0, T, dst + at + ex);
+                    at += tot;
+                }
+            }
+        }
+        // fast bodies' nodes against their partners' triangles (world.cpp:2314-2475)
+        for (int kf = 0; kf < nb; kf++) {
+            if (!(S.b[kf].extra > 0) || !has_partner(S, kf)) continue; // (without partners it has no pairs)
+            const Body& F = bodies[S.b[kf].id];
+            if (tid == 0) {
+                float rmx = 0.0f;
+                for (int ko = 0; ko < nb; ko++)
+                    if (S.partner[kf][ko >> 5] & (1u << (ko & 31))) {
+                        const float fe = S.b[ko].extra > 0 ? S.b[ko].bulk * (float)interval * dt : 0.0f;
+                        rmx = smax(rmx, F.crad + S.slow_reach + fe);
+                    }
+                const float ex = S.b[kf].mx[0] - S.b[kf].mn[0] + 2e-3f, ey = S.b[kf].mx[1] - S.b[kf].mn[1] + 2e-3f;
+                const float ez = S.b[kf].mx[2] - S.b[kf].mn[2] + 2e-3f;
+                float cellsz = clampf(2.0f * rmx, 0.15f, 2.0f);
+                cellsz = smax(cellsz, smax(ex, smax(ey, ez)) / 48.0f);
+                S.g_inv = 1.0f / cellsz;
+                S.g_org[0] = S.b[kf].mn[0] - 1e-3f, S.g_org[1] = S.b[kf].mn[1] - 1e-3f, S.g_org[2] = S.b[kf].mn[2] - 1e-3f;
+                S.g_dim[0] = max(1, min(48, (int)(ex * S.g_inv) + 1));
+                S.g_dim[1] = max(1, min(48, (int)(ey * S.g_inv) + 1));
+                S.g_dim[2] = max(1, min(48, (int)(ez * S.g_inv) + 1));
+            }
+            __syncthreads();
+            const int ncell = S.g_dim[0] * S.g_dim[1] * S.g_dim[2];
+            for (int q = tid; q <= ncell; q += nt) C.g_start[gs0 + q] = 0;
+            __syncthreads();
+            // every contacter node in the cells of its travel: counts, starts, items ascending within a cell
+            for (int i = tid; i < F.nnodes; i += nt) {
+                if (!((uint32_t)info[F.node0 + i].x & NF_CONTACTER)) continue;
+                int3 lo, hi;
+                node_cells(S, nd, F.node0 + i, lo, hi);
+                for (int z = lo.z; z <= hi.z; z++)
+                    for (int y = lo.y; y <= hi.y; y++)
+                        for (int x = lo.x; x <= hi.x; x++) atomicAdd(&C.g_start[gs0 + (z * S.g_dim[1] + y) * S.g_dim[0] + x + 1], 1);
+            }
+            __syncthreads();
+            {
+                int carry = 0;
+                for (int c0 = 0; c0 <= ncell; c0 += nt) {
+                    const int q = c0 + tid;
+                    const int v = q <= ncell ? C.g_start[gs0 + q] : 0;
+                    int tot;
+                    const int ex = block_scan_excl(v, tot, S.warp);
+                    if (q <= ncell) C.g_start[gs0 + q] = carry + ex + v;
+                    carry += tot;
+                }
+            }
+            __syncthreads();
+            const int nitems = C.g_start[gs0 + ncell];
+            if (nitems > kGridItemsPerNode * C.isl_nodes[root]) {
+                if (tid == 0) atomicOr(deverr, DEVERR_GRID);
+                continue; // (uniform: every thread read the same count)
+            }
+            for (int q = tid; q < ncell; q += nt) C.g_fill[gs0 + q] = C.g_start[gs0 + q];
+            __syncthreads();
+            for (int i = tid; i < F.nnodes; i += nt) {
+                if (!((uint32_t)info[F.node0 + i].x & NF_CONTACTER)) continue;
+                int3 lo, hi;
+                node_cells(S, nd, F.node0 + i, lo, hi);
+                for (int z = lo.z; z <= hi.z; z++)
+                    for (int y = lo.y; y <= hi.y; y++)
+                        for (int x = lo.x; x <= hi.x; x++) {
+                            const int at2 = atomicAdd(&C.g_fill[gs0 + (z * S.g_dim[1] + y) * S.g_dim[0] + x], 1);
+                            C.g_items[gi0 + at2] = F.node0 + i;
+                        }
+            }
+            __syncthreads();
+            for (int q = tid; q < ncell; q += nt) {
+                const int k0 = C.g_start[gs0 + q], k1 = C.g_start[gs0 + q + 1];
+                for (int i = k0 + 1; i < k1; i++) {
+                    const int v = C.g_items[gi0 + i];
+                    int j = i - 1;
+                    while (j >= k0 && C.g_items[gi0 + j] > v) C.g_items[gi0 + j + 1] = C.g_items[gi0 + j], j--;
+                    C.g_items[gi0 + j + 1] = v;
+                }
+            }
+            __syncthreads();
+            for (int ko = 0; ko < nb; ko++) {
+                if (!(S.partner[kf][ko >> 5] & (1u << (ko & 31)))) continue;
+                const Body& o = bodies[S.b[ko].id];
+                const float fe = S.b[ko].extra > 0 ? S.b[ko].bulk * (float)interval * dt : 0.0f;
+                for (int c0 = 0; c0 < o.ntris; c0 += nt) {
+                    const int t = c0 + tid;
+                    const int n = t < o.ntris ? fast_query(S, C, bodies, nd, kf, ko, o.tri0 + t, gs0, gi0, fe, T, nullptr) : 0;
+                    int tot;
+                    const int ex = block_scan_excl(n, tot, S.warp);
+                    if (pass == 1 && n > 0) fast_query(S, C, bodies, nd, kf, ko, o.tri0 + t, gs0, gi0, fe, T, dst + at + ex);
+                    at += tot;
+                }
+            }
+            __syncthreads();
+        }
+        if (pass == 0) total = at;
+    }
+    if (tid == 0) atomicAdd(&C.counters[0], 1);
+}
+
+// ------------------------------------------------------------------------------------------ narrow phase (each substep)
+// World::pair_detect for node-triangle pairs (world.cpp:2819-2858): hit_a = (bary, pen), hit_b = (normal, 1) when
+// the pair is in contact, hit_b.w = 0 when not
+__global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, const int4* __restrict__ info, const Body* __restrict__ bodies, Contacts C) {
+    const int total = min(*C.pair_total, C.max_pairs);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int2 pr = C.pairs[i];
+        const int4 tr = C.tri[pr.y];
+        const Body& bn = bodies[info[pr.x].w];
+        const Body& bt = bodies[tr.w >> 8];
+        float4 ha = make_float4(0, 0, 0, 0), hb = make_float4(0, 0, 0, 0);
+        bool hit = false;
+        do {
+            if (bn.sleeping && bt.sleeping) break;
+            if (tr.w & TF_TORN) break; // (torn since the pairs were found)
+            const bool two_sided = (tr.w & TF_TWO_SIDED) != 0;
+            const v3 np = nd_p(nd, pr.x);
+            const v3 a = nd_p(nd, tr.x), b = nd_p(nd, tr.y), cc = nd_p(nd, tr.z);
+            v3 bary;
+            const float r = bt.faces_only && !two_sided ? bt.face_skin : bn.crad;
+            if (!two_sided) {
+                // a hull triangle: over its face pushed out along the face's normal, from as deep as the hull's depth
+                const v3 fn = normalize(cross(b - a, cc - a));
+                const float s = dot(np - a, fn);
+                if (s >= r || s < -bt.hull_depth) break;
+                const v3 q = np - fn * s;
+                const v3 cq = closest_on_triangle(q, a, b, cc, bary);
+                if (length2(cq - q) <= 1e-6f) {
+                    ha = make_float4(bary.x, bary.y, bary.z, r - s), hb = make_float4(fn.x, fn.y, fn.z, 0.0f);
+                    hit = true;
+                    break;
+                }
+                if (s < 0 || bt.faces_only) break;
+            } else {
+                const v3 lo = vmin3(a, vmin3(b, cc)) - V(r, r, r), hi = vmax3(a, vmax3(b, cc)) + V(r, r, r);
+                if (outside(np, lo, hi)) break;
+            }
+            const v3 cp = closest_on_triangle(np, a, b, cc, bary);
+            const v3 d = np - cp;
+            const float dist2 = dot(d, d);
+            if (dist2 >= r * r) break;
+            const float dist = sqrtf(dist2);
+            v3 nrm;
+            if (dist > 1e-5f) {
+                nrm = divs(d, dist);
+            } else {
+                nrm = normalize(cross(b - a, cc - a));
+                const v3 vt = nd_v(nd, tr.x) * bary.x + nd_v(nd, tr.y) * bary.y + nd_v(nd, tr.z) * bary.z;
+                if (dot(nd_v(nd, pr.x) - vt, nrm) > 0) nrm = neg(nrm);
+            }
+            ha = make_float4(bary.x, bary.y, bary.z, r - dist), hb = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+            hit = true;
+        } while (false);
+        hb.w = hit ? 1.0f : 0.0f;
+        C.hit_a[i] = ha;
+        C.hit_b[i] = hb;
+    }
+}
+
+// ------------------------------------------------------------------------------------------ response (each substep)
+// World::collide_pairs for node-triangle pairs (world.cpp:2975-3023): one thread an island, its pairs in order;
+// contact_force<1, 3> and hull_push_out<3> (world.cpp:59-120) on the forces in fsplit; the concrete ground model.
+__global__ void k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, int nbodies, Contacts C) {
+    const int root = blockIdx.x * blockDim.x + threadIdx.x;
+    if (root >= nbodies) return;
+    const int cnt = C.isl_pcnt[root];
+    if (cnt <= 0 || bodies[root].island != root || !bodies[root].pairs) return;
+    const int off = C.isl_poff[root];
+    const float dt = C.dt;
+    const GroundModel& gm = c_ground[3]; // SURF_CONCRETE
+    float4* Fs = C.fsplit;
+    int contacts = 0;
+    for (int i = off; i < off + cnt; i++) {
+        const float4 hb4 = C.hit_b[i];
+        if (hb4.w == 0.0f) continue;
+        const float4 ha = C.hit_a[i];
+        const int2 pr = C.pairs[i];
+        const int4 tr = C.tri[pr.y];
+        Body& bn = bodies[info[pr.x].w];
+        Body& bt = bodies[tr.w >> 8];
+        // movable (world.cpp:2983-2993): a sleeping side is immovable and asks to wake when the other moves
+        bool ma = true, mb = true;
+        if (bn.sleeping) {
+            if (sqrtf(bt.acc_v2) > smax(C.wake_speed, bt.sleep_speed) * 1.0f) bn.wake_request = 1;
+            ma = false;
+        }
+        if (bt.sleeping) {
+            if (sqrtf(bn.acc_v2) > smax(C.wake_speed, bn.sleep_speed) * 1.0f) bt.wake_request = 1;
+            mb = false;
+        }
+        const int ia = pr.x, ib[3] = {tr.x, tr.y, tr.z};
+        const float wb[3] = {ha.x, ha.y, ha.z};
+        const v3 n = V(hb4.x, hb4.y, hb4.z);
+        const float pen = ha.w;
+        const float4 pa = nd[2 * ia], va4 = nd[2 * ia + 1];
+        const v3 Av = V(va4.x, va4.y, va4.z);
+        const float Aim = pa.w;
+        v3 Bv[3];
+        float Bim[3];
+        for (int q = 0; q < 3; q++) {
+            const float4 p = nd[2 * ib[q]], v = nd[2 * ib[q] + 1];
+            Bv[q] = V(v.x, v.y, v.z), Bim[q] = p.w;
+        }
+        const float4 fa4 = Fs[ia];
+        v3 FA = V(fa4.x, fa4.y, fa4.z);
+        v3 FB[3];
+        for (int q = 0; q < 3; q++) {
+            const float4 f = Fs[ib[q]];
+            FB[q] = V(f.x, f.y, f.z);
+        }
+        if (!(tr.w & TF_TWO_SIDED) && pen > bn.crad) {
+            // hull_push_out<3> (world.cpp:97-118): behind a hull's face
+            float W = ma ? Aim : 0.0f;
+            if (mb)
+                for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
+            if (W <= 1e-12f) continue;
+            v3 vb = V(0, 0, 0), acc = V(0, 0, 0);
+            if (ma) acc = acc + FA * Aim;
+            for (int q = 0; q < 3; q++) {
+                vb = vb + Bv[q] * wb[q];
+                if (mb) acc = acc - FB[q] * (wb[q] * Bim[q]);
+            }
+            const float m = 1.0f / W, vr = dot(Av - vb, n), target = smin(0.2f * pen / dt, 2.0f);
+            const float fn = (target - vr) * m / dt - dot(acc, n) * m;
+            if (fn > 0) {
+                const v3 f = n * fn;
+                if (ma) FA = FA + f;
+                if (mb)
+                    for (int q = 0; q < 3; q++) FB[q] = FB[q] - f * wb[q];
+            }
+        } else {
+            // contact_force<1, 3> (world.cpp:59-92), the node's weight 1
+            const float fric = 0.8f * smin(bn.cfric, bt.cfric);
+            float W = 0;
+            if (ma) W += 1.0f * 1.0f * Aim;
+            if (mb)
+                for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
+            if (W <= 1e-12f) continue;
+            const float m = 1.0f / W;
+            v3 va = V(0, 0, 0), vb = V(0, 0, 0), acc = V(0, 0, 0);
+            va = va + Av * 1.0f;
+            if (ma) acc = acc + FA * (1.0f * Aim);
+            for (int q = 0; q < 3; q++) {
+                vb = vb + Bv[q] * wb[q];
+                if (mb) acc = acc - FB[q] * (wb[q] * Bim[q]);
+            }
+            const v3 f_rel = acc * m;
+            if (!ma) {
+                const v3 f = primitive_collision(neg(f_rel), vb - va, m, neg(n), dt, gm, pen, fric, 2.0f, 0.0f, -1.0f);
+                for (int q = 0; q < 3; q++) FB[q] = FB[q] + f * wb[q];
+            } else {
+                const v3 f = primitive_collision(f_rel, va - vb, m, n, dt, gm, pen, fric, 2.0f, 0.0f, -1.0f);
+                FA = FA + f * 1.0f;
+                if (mb)
+                    for (int q = 0; q < 3; q++) FB[q] = FB[q] - f * wb[q];
+            }
+        }
+        Fs[ia] = make_float4(FA.x, FA.y, FA.z, 0.0f);
+        for (int q = 0; q < 3; q++) Fs[ib[q]] = make_float4(FB[q].x, FB[q].y, FB[q].z, 0.0f);
+        contacts++;
+        bn.body_contacts++;
+        bt.body_contacts++;
+    }
+    C.isl_contacts[root] += contacts;
+    if (contacts) atomicAdd(&C.counters[1], contacts);
+}
+
+} // namespace blg

@@ -85,6 +85,20 @@ struct alignas(64) Body {
     int has_ext;             // constant node forces (bl_gpu_set_node_force) are added after gravity
     int box_ids[kMaxCand];
     int cyl_ids[kMaxCand];
+    // contacts with other bodies (bl_contacts.cuh)
+    int tri0, ntris;         // its collision triangles
+    float crad;              // SoftBody::collision_radius
+    float cfric;             // SoftBody::contact_friction
+    float hull_depth;        // SoftBody::hull_depth
+    float face_skin;         // SoftBody::face_skin
+    int faces_only;          // SoftBody::faces_only
+    int hull;                // it has hull (one-sided) triangles: SoftBody::hull_reach() = hull_depth
+    int group;               // SoftBody::collision_group
+    int contacters;          // it has NF_CONTACTER nodes
+    int island;              // this frame: the first body of its island (-1: its island sleeps)
+    int pairs;               // this frame: its island has contact pairs (its nodes finish after the contacts)
+    int wake_request;        // SoftBody::wake_request
+    int body_contacts;       // SoftBody::body_contacts (this frame)
 };
 
 // ------------------------------------------------------------------------------------------ math in the reference's order

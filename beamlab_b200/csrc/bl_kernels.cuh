@@ -192,7 +192,8 @@ __global__ void k_frame_begin(Body* __restrict__ bodies, int nbodies, Statics st
     if (bi >= nbodies) return;
     Body& B = bodies[bi];
     if (!world_sleeping) B.sleeping = 0;
-    if (B.sleeping) return;
+    if (B.sleeping && B.island < 0) return; // (an island asleep as a whole is not stepped; a sleeping body beside a
+                                            // moving one is, and may be woken by it)
     const float m = smin(B.max_speed, 200.0f) * frame_time * 2.0f + 0.5f;
     const float mn[3] = {B.aabb_mn[0] - m, B.aabb_mn[1] - m, B.aabb_mn[2] - m};
     const float mx[3] = {B.aabb_mx[0] + m, B.aabb_mx[1] + m, B.aabb_mx[2] + m};
@@ -243,6 +244,7 @@ __global__ void k_frame_begin(Body* __restrict__ bodies, int nbodies, Statics st
     B.terrain_max = st.has_terrain ? hf_max_height(st, mn[0], mn[2], mx[0], mx[2]) + 0.0f : -1e30f;
     B.acc_v2 = 0.0f;
     B.acc_contacts = 0;
+    if (B.sleeping) B.max_speed = 0.0f; // (simulate_island's top speed of a sleeping body, world.cpp:3217-3222)
 }
 
 // ------------------------------------------------------------------------------------------ per substep
@@ -350,10 +352,12 @@ struct NodeFem {
     const float4* ext;       // constant node forces (bl_gpu_set_node_force)
 };
 
+// phase 0: every body; the bodies of islands with contact pairs (Body::pairs) only keep their force in fsplit.
+// phase 1: those bodies alone, after the contacts added to fsplit: static contact and integration.
 __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const int4* __restrict__ info,
                                                const int* __restrict__ inc_ptr, const int* __restrict__ inc, const float4* __restrict__ fv,
                                                Body* __restrict__ bodies, Statics st, float gx, float gy, float gz, float dt, int nnodes, int first,
-                                               NodeFem nf) {
+                                               NodeFem nf, int phase, float4* __restrict__ fsplit) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int body = -1;
@@ -365,26 +369,35 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
         const int4 inf = info[i];
         body = inf.w;
         const Body& B = bodies[body];
-        if (!B.sleeping) {
-            live = true;
+        const bool split = B.pairs != 0;
+        if (!B.sleeping && (phase == 0 || split)) {
             const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
-            if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
             const float m = Vv.w;
-            v3 f = V(gx * m, gy * m, gz * m); // clear_forces: g * mass (softbody.cpp:376)
-            if (B.has_ext) {                  // (a controller's push, world.cpp:3261)
-                const float4 e = nf.ext[i];
-                f = V(f.x + e.x, f.y + e.y, f.z + e.z);
-            }
-            const int q1 = inc_ptr[i + 1];
-            for (int q = inc_ptr[i]; q < q1; q++) {
-                const int e = inc[q];
-                const float4 b = fv[e & 0x7fffffff];
-                if (b.w != 0.0f) {
-                    if (e < 0) f = V(f.x - b.x, f.y - b.y, f.z - b.z);
-                    else f = V(f.x + b.x, f.y + b.y, f.z + b.z);
+            v3 f;
+            if (phase == 1) {
+                const float4 fs = fsplit[i];
+                f = V(fs.x, fs.y, fs.z);
+            } else {
+                f = V(gx * m, gy * m, gz * m); // clear_forces: g * mass (softbody.cpp:376)
+                if (B.has_ext) {               // (a controller's push, world.cpp:3261)
+                    const float4 e = nf.ext[i];
+                    f = V(f.x + e.x, f.y + e.y, f.z + e.z);
+                }
+                const int q1 = inc_ptr[i + 1];
+                for (int q = inc_ptr[i]; q < q1; q++) {
+                    const int e = inc[q];
+                    const float4 b = fv[e & 0x7fffffff];
+                    if (b.w != 0.0f) {
+                        if (e < 0) f = V(f.x - b.x, f.y - b.y, f.z - b.z);
+                        else f = V(f.x + b.x, f.y + b.y, f.z + b.z);
+                    }
                 }
             }
-            if (B.is_fem) {
+            live = !(phase == 0 && split);
+            if (!live) {
+                fsplit[i] = make_float4(f.x, f.y, f.z, 0.0f); // (the contacts between bodies come next: World::collide_pairs)
+            } else if (B.is_fem) {
+                if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
                 const int fs = nf.fslot[i];
                 if (fs >= 0) {
                     const int k = nf.iperm[fs];
@@ -401,6 +414,7 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
                 nf.nforce[i] = make_float4(f.x, f.y, f.z, 0.0f);
                 v2 = v2start; // (its bounds and speeds after the frame's step: k_fem_integrate)
             } else {
+                if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
                 v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
                 float inv_mass = P.w;
                 const uint32_t flags = (uint32_t)inf.x;

@@ -11,6 +11,7 @@
 //   bodies  Body records (bl_device.cuh)
 // A frame (bl_gpu_step_substeps) is captured once per substep count as a CUDA graph and replayed.
 #include "../../include/beamlab_gpu.h"
+#include "bl_contacts.cuh"
 #include "bl_fem_host.cuh"
 #include "bl_fem_kernels.cuh"
 #include "bl_kernels.cuh"
@@ -33,6 +34,7 @@ struct HostBody {
     std::vector<bl_node> nodes;
     std::vector<bl_node_info> info;
     std::vector<bl_beam> beams;
+    std::vector<bl_tri> tris;              // collision triangles (their torn flags come back from the device)
     uint32_t beam_bits = 0; // the body's allow_deform / allow_break / ductile as BB_* bits of its beams' meta words
     Body rec;
     std::vector<float4> ext;               // constant node forces (empty: none)
@@ -115,6 +117,16 @@ struct bl_gpu_ctx {
     DevBuf<uint8_t> tbroken, ton, ffixed;
     DevBuf<FemSecDev> fsec;
     FemDev fd{};
+    // contacts between bodies (bl_contacts.cuh): on when some body has collision triangles
+    bool contacts_on = false;
+    int interval = 1, NTRI = 0, max_isl = 0;
+    DevBuf<int4> dtri, pt_cell;
+    DevBuf<float> tri_rest2, ibox;
+    DevBuf<int> parent, isl_live, isl_cnt, isl_nodes, isl_idx, isl_noff, isl_poff, isl_pcnt, isl_contacts, pair_total;
+    DevBuf<int> pt_node, pt_body, bk_start, bk_fill, bk_items, run_end, g_start, g_fill, g_items, counters;
+    DevBuf<int2> pairs;
+    DevBuf<float4> hit_a, hit_b, fsplit;
+    Contacts ct{};
     // frames captured as graphs, by substep count
     std::map<int, cudaGraphExec_t> graphs;
     struct ProfGraph {
@@ -160,8 +172,18 @@ static void free_fem(bl_gpu_ctx* c) {
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
 }
 
+static void free_contacts(bl_gpu_ctx* c) {
+    c->dtri.free_(), c->pt_cell.free_(), c->tri_rest2.free_(), c->ibox.free_(), c->parent.free_(), c->isl_live.free_();
+    c->isl_cnt.free_(), c->isl_nodes.free_(), c->isl_idx.free_(), c->isl_noff.free_(), c->isl_poff.free_(), c->isl_pcnt.free_();
+    c->isl_contacts.free_(), c->pair_total.free_(), c->pt_node.free_(), c->pt_body.free_(), c->bk_start.free_(), c->bk_fill.free_();
+    c->bk_items.free_(), c->run_end.free_(), c->g_start.free_(), c->g_fill.free_(), c->g_items.free_(), c->counters.free_();
+    c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_(), c->fsplit.free_();
+    c->contacts_on = false;
+}
+
 static void free_device(bl_gpu_ctx* c) {
     free_fem(c);
+    free_contacts(c);
     c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->fv.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
@@ -276,6 +298,14 @@ static int pull_state(bl_gpu_ctx* c) {
             b.stress = stress[r.beam0 + j];
         }
         hb.rec = r;
+    }
+    if (c->contacts_on && c->NTRI > 0) {
+        std::vector<int4> tri(c->NTRI);
+        BL_CUDA(c, cudaMemcpy(tri.data(), c->dtri.p, sizeof(int4) * c->NTRI, cudaMemcpyDeviceToHost));
+        for (int bi = 0; bi < c->B; bi++) {
+            HostBody& hb = c->bodies[bi];
+            for (int t = 0; t < hb.rec.ntris; t++) hb.tris[t].torn = (tri[hb.rec.tri0 + t].w & TF_TORN) ? 1 : 0;
+        }
     }
     // the frames' dynamic state (their positions in double, orientations, spins) and counters
     if (c->NF > 0) {
@@ -479,6 +509,69 @@ static int commit_fem(bl_gpu_ctx* c) {
 }
 
 // Lays every body out back to back on the device and builds each node's incident-beam list.
+// The collision triangles of all bodies back to back and the contacts' scratch (bl_contacts.cuh), when some body has
+// triangles and the world collides bodies.
+static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
+    free_contacts(c);
+    int T = 0;
+    for (int bi = 0; bi < c->B; bi++) recs[bi].tri0 = T, recs[bi].ntris = (int)c->bodies[bi].tris.size(), T += recs[bi].ntris;
+    c->NTRI = T;
+    c->contacts_on = T > 0 && c->cfg.inter_body_collisions != 0;
+    if (!c->contacts_on) {
+        for (Body& r : recs) r.island = -1, r.pairs = 0;
+        return BL_GPU_OK;
+    }
+    std::vector<int4> tri(T);
+    std::vector<float> rest2(T);
+    for (int bi = 0; bi < c->B; bi++) {
+        const HostBody& hb = c->bodies[bi];
+        const int n0 = recs[bi].node0;
+        for (int t = 0; t < recs[bi].ntris; t++) {
+            const bl_tri& x = hb.tris[t];
+            const int fl = (x.two_sided ? (int)TF_TWO_SIDED : 0) | (x.torn ? (int)TF_TORN : 0) | (bi << 8);
+            tri[recs[bi].tri0 + t] = make_int4(n0 + (int)x.a, n0 + (int)x.b, n0 + (int)x.c, fl);
+            rest2[recs[bi].tri0 + t] = x.rest_edge2;
+        }
+    }
+    const int N = c->N, B = c->B;
+    c->max_isl = B / 2 + 1; // (an island with pairs holds two bodies or more)
+    int rc;
+    if ((rc = upload_vec(c, c->dtri, tri)) || (rc = upload_vec(c, c->tri_rest2, rest2))) return rc;
+    BL_CUDA(c, c->ibox.alloc(6 * (size_t)B));
+    for (DevBuf<int>* d : {&c->parent, &c->isl_live, &c->isl_cnt, &c->isl_nodes, &c->isl_idx, &c->isl_noff, &c->isl_poff, &c->isl_pcnt, &c->isl_contacts})
+        BL_CUDA(c, d->alloc(B));
+    BL_CUDA(c, c->pair_total.alloc(1));
+    BL_CUDA(c, c->counters.alloc(4));
+    BL_CUDA(c, c->pairs.alloc(c->cfg.max_pairs));
+    BL_CUDA(c, c->hit_a.alloc(c->cfg.max_pairs));
+    BL_CUDA(c, c->hit_b.alloc(c->cfg.max_pairs));
+    for (DevBuf<int>* d : {&c->pt_node, &c->pt_body, &c->bk_items, &c->run_end}) BL_CUDA(c, d->alloc(N));
+    BL_CUDA(c, c->pt_cell.alloc(N));
+    BL_CUDA(c, c->bk_start.alloc(4 * (size_t)N + 65 * (size_t)B + 1));
+    BL_CUDA(c, c->bk_fill.alloc(4 * (size_t)N + 65 * (size_t)B + 1));
+    BL_CUDA(c, c->g_start.alloc((size_t)c->max_isl * (kGridCells + 1)));
+    BL_CUDA(c, c->g_fill.alloc((size_t)c->max_isl * (kGridCells + 1)));
+    BL_CUDA(c, c->g_items.alloc((size_t)kGridItemsPerNode * N));
+    BL_CUDA(c, c->fsplit.alloc(N));
+    // (the pair list starts as valid indices: k_detect reads up to the last search's total)
+    BL_CUDA(c, cudaMemsetAsync(c->pairs.p, 0, sizeof(int2) * c->cfg.max_pairs, c->stream));
+    BL_CUDA(c, cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), c->stream));
+    BL_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 4 * sizeof(int), c->stream));
+    BL_CUDA(c, cudaMemsetAsync(c->isl_pcnt.p, 0, sizeof(int) * B, c->stream));
+    BL_CUDA(c, cudaMemsetAsync(c->isl_contacts.p, 0, sizeof(int) * B, c->stream));
+    const double hz = std::max(1.0f, c->cfg.collision_hz);
+    c->interval = std::max(1, (int)std::ceil(1.0 / (hz * (double)c->cfg.dt) - 1e-6)); // (world.cpp:1887)
+    Contacts& C = c->ct;
+    C.tri = c->dtri.p, C.tri_rest2 = c->tri_rest2.p, C.parent = c->parent.p, C.ibox = c->ibox.p;
+    C.isl_live = c->isl_live.p, C.isl_cnt = c->isl_cnt.p, C.isl_nodes = c->isl_nodes.p, C.isl_idx = c->isl_idx.p;
+    C.isl_noff = c->isl_noff.p, C.isl_poff = c->isl_poff.p, C.isl_pcnt = c->isl_pcnt.p, C.isl_contacts = c->isl_contacts.p;
+    C.pair_total = c->pair_total.p, C.pairs = c->pairs.p, C.hit_a = c->hit_a.p, C.hit_b = c->hit_b.p, C.max_pairs = c->cfg.max_pairs;
+    C.pt_node = c->pt_node.p, C.pt_body = c->pt_body.p, C.pt_cell = c->pt_cell.p, C.bk_start = c->bk_start.p, C.bk_fill = c->bk_fill.p;
+    C.bk_items = c->bk_items.p, C.run_end = c->run_end.p, C.g_start = c->g_start.p, C.g_fill = c->g_fill.p, C.g_items = c->g_items.p;
+    C.fsplit = c->fsplit.p, C.counters = c->counters.p, C.interval = c->interval, C.dt = c->cfg.dt, C.wake_speed = c->cfg.sleep_speed;
+    return BL_GPU_OK;
+}
+
 static int commit_bodies(bl_gpu_ctx* c) {
     int rc = pull_state(c);
     if (rc) return rc;
@@ -537,6 +630,9 @@ static int commit_bodies(bl_gpu_ctx* c) {
         recs[bi].has_ext = c->bodies[bi].ext.empty() ? 0 : 1;
         c->any_ext |= recs[bi].has_ext != 0;
     }
+    free_device(c);
+    c->N = N, c->M = M, c->B = B;
+    if ((rc = commit_contacts(c, recs))) return rc;
     for (int i = 0; i < N; i++) inc_ptr[i + 1] += inc_ptr[i];
     {
         std::vector<int> fill(inc_ptr.begin(), inc_ptr.end() - 1);
@@ -545,7 +641,6 @@ static int commit_bodies(bl_gpu_ctx* c) {
             inc[fill[ab[g].y]++] = (int)((uint32_t)g | 0x80000000u);
         }
     }
-    free_device(c);
     static_assert(sizeof(bl_node) == 2 * sizeof(float4), "bl_node is two float4");
     BL_CUDA(c, c->nd.alloc(2 * (size_t)N));
     if (N) BL_CUDA(c, cudaMemcpyAsync(c->nd.p, nodes.data(), sizeof(bl_node) * N, cudaMemcpyHostToDevice, c->stream));
@@ -591,10 +686,17 @@ static int ensure_committed(bl_gpu_ctx* c) {
 // One frame of n substeps on stream s: without FEM frames 2n + 3 kernels. ev (2n + 4 events, or null): recorded
 // before the first kernel, after the frame's start, after each substep's beams (and triangles) and after the rest of
 // each substep, after the frame's end kernels.
+static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0; } // (s == 0 || s >= next_rebuild)
+
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
     int64_t per = 2;
     if (c->NF > 0) per += c->fem_launches;
-    return per * n + 3;
+    int64_t total = per * n + 3;
+    if (c->contacts_on) {
+        total += 1 + 4 * (int64_t)n; // k_islands; k_wake, k_detect, k_collide, k_nodes phase 1 a substep
+        for (int k = 0; k < n; k++) total += rebuild_at(c, k) ? 1 : 0;
+    }
+    return total;
 }
 
 static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev = nullptr) {
@@ -607,18 +709,35 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     const float frame_time = (float)n * dt;
     const int tb = 256;
     const int gb = (std::max(c->M, c->B) + tb - 1) / tb, gn = (c->N + tb - 1) / tb, gbody = (c->B + tb - 1) / tb;
+    const Contacts& CT = c->ct;
+    if (c->contacts_on) k_islands<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, frame_time, c->cfg.sleeping, CT, c->deverr.p);
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
     mark();
     NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p};
     const FemDev& F = c->fd;
     for (int k = 0; k < n; k++) {
+        if (c->contacts_on) {
+            // wake requests, then the pair search on its substeps (on the positions and velocities the substep starts from)
+            k_wake<<<c->B, 256, 0, s>>>(c->dbodies.p, c->bmeta.p);
+            if (rebuild_at(c, k)) {
+                cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), s);
+                k_rebuild<<<c->B, 1024, sizeof(RebuildShared), s>>>(c->dbodies.p, c->B, c->nd.p, c->info.p, CT, k == 0 ? 1 : 0, c->deverr.p);
+            }
+        }
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
         k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fv.p, c->nd.p, c->dbodies.p,
                                                c->M, c->B);
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
         k_nodes<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc.p, c->fv.p, c->dbodies.p, c->st, c->cfg.gravity[0],
-                                               c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0, nfm);
+                                               c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0, nfm, 0, c->fsplit.p);
+        if (c->contacts_on) {
+            // contacts between bodies on the forces so far, then the nodes of their islands finish
+            k_detect<<<148 * 4, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, CT);
+            k_collide<<<(c->B + 127) / 128, 128, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT);
+            k_nodes<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc.p, c->fv.p, c->dbodies.p, c->st, c->cfg.gravity[0],
+                                                   c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0, nfm, 1, c->fsplit.p);
+        }
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
             k_fem_assemble<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
@@ -711,6 +830,9 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->sleep_time = 1.0f;
     cfg->device = 0;
     cfg->deterministic = 1;
+    cfg->collision_hz = 120.0f;
+    cfg->inter_body_collisions = 1;
+    cfg->max_pairs = 1 << 21;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -735,7 +857,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_config c0;
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
-    if (!(c0.dt > 0) || c0.deterministic != 1) return BL_GPU_EINVAL;
+    if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1) return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
     cudaDeviceProp prop;
@@ -852,12 +974,23 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
         if (b.a >= (uint32_t)d->n_nodes || b.b >= (uint32_t)d->n_nodes || b.type > BL_BT_SUPPORT) return BL_GPU_EINVAL;
         if (b.flags & BL_BF_SHOCK) return BL_GPU_EUNSUPPORTED; // shocks have their own force model (softbody.cpp:472-575)
     }
+    if (d->n_tris < 0 || (d->n_tris > 0 && !d->tris)) return BL_GPU_EINVAL;
+    for (int t = 0; t < d->n_tris; t++)
+        if (d->tris[t].a >= (uint32_t)d->n_nodes || d->tris[t].b >= (uint32_t)d->n_nodes || d->tris[t].c >= (uint32_t)d->n_nodes) return BL_GPU_EINVAL;
+    if (d->self_collision) return BL_GPU_EUNSUPPORTED;                               // (a body's nodes against its own triangles)
+    if (d->n_tris > 0 && d->fem && d->fem->n_tris > 0) return BL_GPU_EUNSUPPORTED; // (contacts of frame nodes)
+    if (c->bodies.size() >= (size_t)(1 << 23)) return BL_GPU_ELIMIT;               // (a triangle keeps its body in 23 bits)
     HostBody hb;
     hb.nodes.assign(d->nodes, d->nodes + d->n_nodes);
     hb.info.assign(d->info, d->info + d->n_nodes);
     hb.beams.assign(d->beams, d->beams + d->n_beams);
+    if (d->n_tris > 0) hb.tris.assign(d->tris, d->tris + d->n_tris);
     Body& r = hb.rec;
     std::memset(&r, 0, sizeof(r));
+    r.crad = d->collision_radius, r.cfric = d->contact_friction, r.hull_depth = d->hull_depth, r.face_skin = d->face_skin;
+    r.faces_only = d->faces_only ? 1 : 0, r.group = d->collision_group, r.island = -1;
+    for (const bl_tri& t : hb.tris) r.hull |= t.two_sided ? 0 : 1;
+    for (int i = 0; i < d->n_nodes; i++) r.contacters |= (d->info[i].flags & BL_NF_CONTACTER) ? 1 : 0;
     r.fric = d->ground_friction;
     r.bounce = d->bounce, r.push_max = d->contact_push_max, r.slop = d->contact_slop;
     r.terrain_max = -1e30f;
@@ -994,6 +1127,8 @@ int bl_gpu_body_state(bl_gpu_ctx* c, int32_t body, bl_body_state* out) {
     out->broken_beams = r.broken_beams;
     out->sleep_timer = r.sleep_timer;
     out->repaired_nodes = r.repaired;
+    out->body_contacts = r.body_contacts;
+    out->wake_request = r.wake_request;
     out->fem_failures = out->fem_clamps = 0;
     if (c->NF > 0) {
         BL_CUDA(c, cudaMemcpy(&out->fem_failures, c->fem_fail.p + body, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1019,6 +1154,48 @@ int bl_gpu_stats(bl_gpu_ctx* c, bl_world_stats* out) {
     out->substeps = c->last_substeps;
     out->total_substeps = c->total_substeps;
     out->kernel_launches = c->launches;
+    if (c->contacts_on) {
+        int cnt[4];
+        BL_CUDA(c, cudaMemcpy(cnt, c->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost));
+        int total = 0;
+        BL_CUDA(c, cudaMemcpy(&total, c->pair_total.p, sizeof(int), cudaMemcpyDeviceToHost));
+        out->pair_searches = cnt[0], out->contacts = cnt[1], out->pairs = total;
+        for (int i = 0; i < (int)recs.size(); i++) out->islands += (recs[i].pairs && recs[i].island == i) ? 1 : 0;
+    }
+    return BL_GPU_OK;
+}
+
+int bl_gpu_download_pairs(bl_gpu_ctx* c, int32_t* pairs, int32_t capacity, int32_t* n_pairs) {
+    if (!c || !n_pairs || capacity < 0 || (capacity > 0 && !pairs)) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    int rc = ensure_committed(c);
+    if (rc) return rc;
+    *n_pairs = 0;
+    if (!c->contacts_on) return BL_GPU_OK;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    std::vector<int> poff(c->B), pcnt(c->B);
+    std::vector<Body> recs(c->B);
+    BL_CUDA(c, cudaMemcpy(poff.data(), c->isl_poff.p, sizeof(int) * c->B, cudaMemcpyDeviceToHost));
+    BL_CUDA(c, cudaMemcpy(pcnt.data(), c->isl_pcnt.p, sizeof(int) * c->B, cudaMemcpyDeviceToHost));
+    BL_CUDA(c, cudaMemcpy(recs.data(), c->dbodies.p, sizeof(Body) * c->B, cudaMemcpyDeviceToHost));
+    std::vector<int4> tri(c->NTRI), nodeinfo(c->N);
+    BL_CUDA(c, cudaMemcpy(tri.data(), c->dtri.p, sizeof(int4) * c->NTRI, cudaMemcpyDeviceToHost));
+    BL_CUDA(c, cudaMemcpy(nodeinfo.data(), c->info.p, sizeof(int4) * c->N, cudaMemcpyDeviceToHost));
+    std::vector<int2> pr;
+    int w = 0;
+    for (int r = 0; r < c->B; r++) { // (islands in the order of their first body)
+        if (pcnt[r] <= 0) continue;
+        pr.resize(pcnt[r]);
+        BL_CUDA(c, cudaMemcpy(pr.data(), c->pairs.p + poff[r], sizeof(int2) * pcnt[r], cudaMemcpyDeviceToHost));
+        for (const int2& p : pr) {
+            if (w < capacity) {
+                const int bn = nodeinfo[p.x].w, bt = tri[p.y].w >> 8;
+                pairs[4 * w] = bn, pairs[4 * w + 1] = p.x - recs[bn].node0, pairs[4 * w + 2] = bt, pairs[4 * w + 3] = p.y - recs[bt].tri0;
+            }
+            w++;
+        }
+    }
+    *n_pairs = w;
     return BL_GPU_OK;
 }
 

@@ -28,7 +28,11 @@ NODE_INFO_DTYPE = np.dtype([("flags", "<u2"), ("surface", "u1"), ("pad", "u1"), 
 BEAM_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("L", "<f4"), ("k", "<f4"), ("d", "<f4"), ("max_pos", "<f4"),
                        ("max_neg", "<f4"), ("strength", "<f4"), ("plastic", "<f4"), ("stress", "<f4"), ("L0", "<f4"),
                        ("support_limit", "<f4"), ("type", "u1"), ("flags", "u1"), ("group", "<u2")])
+# == bl_tri == the reference's Triangle (softbody.h:138-147)
+TRI_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("c", "<u4"), ("surface", "u1"), ("two_sided", "u1"), ("torn", "u1"),
+                      ("pad", "u1"), ("rest_edge2", "<f4")])
 assert NODE_DTYPE.itemsize == 32 and NODE_INFO_DTYPE.itemsize == 20 and BEAM_DTYPE.itemsize == 52
+assert TRI_DTYPE.itemsize == 20
 
 NF_GROUND, NF_FIXED, NF_CONTACTER = 1, 2, 16
 BF_BROKEN, BF_SHOCK = 1, 64
@@ -55,6 +59,8 @@ class WorldSettings:
     sleeping: bool = True
     sleep_speed: float = 0.06
     sleep_time: float = 1.0
+    collision_hz: float = 120.0
+    inter_body_collisions: bool = True
 
 
 @dataclass
@@ -111,6 +117,15 @@ class SoftBody:
         self.ductile = False
         self.can_sleep = True
         self.sleep_speed = 0.0
+        # contacts with other bodies (softbody.h:614-721)
+        self.contact_friction = 1.0
+        self.hull_depth = 0.3
+        self.face_skin = 0.002
+        self.faces_only = False
+        self.collision_group = 0
+        self.self_collision = False
+        self._tris: list = []
+        self.tris = np.zeros(0, TRI_DTYPE)
         self.nodes = np.zeros(0, NODE_DTYPE)
         self.info = np.zeros(0, NODE_INFO_DTYPE)
         self.beams = np.zeros(0, BEAM_DTYPE)
@@ -134,6 +149,11 @@ class SoftBody:
         """SoftBody::add_beam (softbody.cpp:22-40)."""
         self._beams.append((a, b, k, d, strength, deform, type, flags))
         return len(self._beams) - 1
+
+    def add_triangle(self, a: int, b: int, c: int, two_sided: bool = True) -> int:
+        """SoftBody::add_triangle (softbody.h:958): a collision triangle; two_sided False makes a hull triangle."""
+        self._tris.append((a, b, c, bool(two_sided)))
+        return len(self._tris) - 1
 
     @classmethod
     def from_arrays(cls, body: dict, name: str = "") -> "SoftBody":
@@ -178,6 +198,12 @@ class SoftBody:
             ft["section"] = np.asarray(body.get("fem_tri_section", np.zeros(len(tri))), np.uint16)
             ft["mass"] = np.asarray(body["fem_tri_mass"], np.float32)
             sb.fem_tris = ft
+        if "tris" in body and len(body["tris"]):
+            tri = np.asarray(body["tris"], np.uint32).reshape(-1, 3)
+            tr = np.zeros(len(tri), TRI_DTYPE)
+            tr["a"], tr["b"], tr["c"] = tri[:, 0], tri[:, 1], tri[:, 2]
+            tr["two_sided"] = np.asarray(body.get("tri_two_sided", np.ones(len(tri))), np.uint8)
+            sb.tris = tr
         sb._finalize_arrays()
         return sb
 
@@ -198,6 +224,10 @@ class SoftBody:
             beams[j]["support_limit"] = 4.0
             beams[j]["type"], beams[j]["flags"] = t, f
         self.nodes, self.info, self.beams = nodes, info, beams
+        tr = np.zeros(len(self._tris), TRI_DTYPE)
+        for t, (a, b, c, two) in enumerate(self._tris):
+            tr[t]["a"], tr[t]["b"], tr[t]["c"], tr[t]["two_sided"] = a, b, c, int(two)
+        self.tris = tr
         self._finalize_arrays()
 
     def _finalize_arrays(self):
@@ -208,6 +238,16 @@ class SoftBody:
             self.beams["L0"] = L
             self.beams["plastic"] = 0
             self.beams["stress"] = 0
+        if len(self.tris):  # rest_edge2: max_edge2 of the triangle at finalize (softbody.cpp:80, softbody.h:155)
+            p = self.nodes["p"]
+            a, b, c = p[self.tris["a"]], p[self.tris["b"]], p[self.tris["c"]]
+
+            def l2(d):
+                d = d.astype(np.float32)
+                return ((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]).astype(np.float32)
+            e0, e1, e2 = l2(b - a), l2(c - b), l2(a - c)
+            m12 = np.where(e1 < e2, e2, e1)  # std::max(e1, e2)
+            self.tris["rest_edge2"] = np.where(e0 < m12, m12, e0)
 
     def node_count(self) -> int:
         return len(self.nodes)
@@ -232,20 +272,24 @@ class _BodyDesc(C.Structure):
                 ("contact_push_max", C.c_float), ("contact_slop", C.c_float), ("allow_deform", C.c_int32),
                 ("allow_break", C.c_int32), ("ductile", C.c_int32), ("can_sleep", C.c_int32),
                 ("sleep_speed", C.c_float), ("max_speed", C.c_float), ("sleeping", C.c_int32),
-                ("fem", C.POINTER(_FemDesc))]
+                ("fem", C.POINTER(_FemDesc)), ("n_tris", C.c_int32), ("tris", C.c_void_p),
+                ("collision_radius", C.c_float), ("contact_friction", C.c_float), ("hull_depth", C.c_float),
+                ("face_skin", C.c_float), ("faces_only", C.c_int32), ("collision_group", C.c_int32),
+                ("self_collision", C.c_int32)]
 
 
 class _BodyState(C.Structure):
     _fields_ = [("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3), ("max_speed", C.c_float),
                 ("sleeping", C.c_int32), ("static_contacts", C.c_int32), ("broken_beams", C.c_int32),
                 ("sleep_timer", C.c_float), ("repaired_nodes", C.c_int32), ("fem_failures", C.c_int32),
-                ("fem_clamps", C.c_int32)]
+                ("fem_clamps", C.c_int32), ("body_contacts", C.c_int32), ("wake_request", C.c_int32)]
 
 
 class _WorldStats(C.Structure):
     _fields_ = [("substeps", C.c_int32), ("active_bodies", C.c_int32), ("sleeping_bodies", C.c_int32),
                 ("active_nodes", C.c_int32), ("active_beams", C.c_int32), ("total_substeps", C.c_int64),
-                ("kernel_launches", C.c_int64), ("device_errors", C.c_uint32)]
+                ("kernel_launches", C.c_int64), ("device_errors", C.c_uint32), ("contacts", C.c_int64),
+                ("pair_searches", C.c_int64), ("pairs", C.c_int32), ("islands", C.c_int32)]
 
 
 class _FrameProfile(C.Structure):
@@ -255,7 +299,8 @@ class _FrameProfile(C.Structure):
 
 class _Config(C.Structure):
     _fields_ = [("gravity", C.c_float * 3), ("dt", C.c_float), ("sleeping", C.c_int32), ("sleep_speed", C.c_float),
-                ("sleep_time", C.c_float), ("device", C.c_int32), ("deterministic", C.c_int32)]
+                ("sleep_time", C.c_float), ("device", C.c_int32), ("deterministic", C.c_int32),
+                ("collision_hz", C.c_float), ("inter_body_collisions", C.c_int32), ("max_pairs", C.c_int32)]
 
 
 class BodyHandle:
@@ -289,7 +334,8 @@ class BodyHandle:
         return {"aabb_min": np.array(s.aabb_min, np.float32), "aabb_max": np.array(s.aabb_max, np.float32),
                 "max_speed": float(s.max_speed), "sleeping": bool(s.sleeping), "static_contacts": s.static_contacts,
                 "broken_beams": s.broken_beams, "sleep_timer": float(s.sleep_timer),
-                "repaired_nodes": s.repaired_nodes, "fem_failures": s.fem_failures, "fem_clamps": s.fem_clamps}
+                "repaired_nodes": s.repaired_nodes, "fem_failures": s.fem_failures, "fem_clamps": s.fem_clamps,
+                "body_contacts": s.body_contacts, "wake_request": bool(s.wake_request)}
 
     def fem(self) -> dict | None:
         """The FEM frame's nodes: body node, double positions, orientations (x y z w), angular velocities."""
@@ -328,6 +374,8 @@ class World:
         cfg.sleep_speed = self.settings.sleep_speed
         cfg.sleep_time = self.settings.sleep_time
         cfg.device = device
+        cfg.collision_hz = self.settings.collision_hz
+        cfg.inter_body_collisions = int(self.settings.inter_body_collisions)
         self._ctx = C.c_void_p()
         _check(self._L.bl_gpu_create(C.byref(cfg), C.byref(self._ctx)), "create")
         self._bodies: list[BodyHandle] = []
@@ -398,6 +446,12 @@ class World:
                       body.ground_friction, body.bounce, body.contact_push_max, body.contact_slop,
                       int(body.allow_deform), int(body.allow_break), int(body.ductile), int(body.can_sleep),
                       body.sleep_speed, 0.0, 0, fem_ptr)
+        tris = np.ascontiguousarray(body.tris, TRI_DTYPE)
+        self._keep.append(tris)
+        d.n_tris, d.tris = len(tris), (tris.ctypes.data if len(tris) else None)
+        d.collision_radius, d.contact_friction = float(body.collision_radius), float(body.contact_friction)
+        d.hull_depth, d.face_skin, d.faces_only = float(body.hull_depth), float(body.face_skin), int(body.faces_only)
+        d.collision_group, d.self_collision = int(body.collision_group), int(body.self_collision)
         idx = C.c_int32()
         _check(self._L.bl_gpu_add_body(self._ctx, C.byref(d), C.byref(idx)), "add_body", self._ctx)
         h = BodyHandle(self, idx.value, len(nodes), len(beams), body.name)
@@ -466,6 +520,18 @@ class World:
         _check(self._L.bl_gpu_profile_frame(self._ctx, int(n), self._stream(stream), C.byref(p)), "profile_frame",
                self._ctx)
         return {k: getattr(p, k) for k, _ in _FrameProfile._fields_}
+
+    def pairs(self) -> np.ndarray:
+        """The contact pairs of the last pair search, island after island, each in the reference's order: rows of
+        (node's body, node, triangle's body, triangle)."""
+        self._send_statics()
+        n = C.c_int32()
+        _check(self._L.bl_gpu_download_pairs(self._ctx, None, 0, C.byref(n)), "download_pairs", self._ctx)
+        out = np.zeros((n.value, 4), np.int32)
+        if n.value:
+            _check(self._L.bl_gpu_download_pairs(self._ctx, out.ctypes.data, n.value, C.byref(n)), "download_pairs",
+                   self._ctx)
+        return out
 
     def body_range(self, body: int):
         a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()

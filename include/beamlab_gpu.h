@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define BL_GPU_ABI_VERSION 1
+#define BL_GPU_ABI_VERSION 2
 
 enum {
     BL_GPU_OK = 0,
@@ -62,6 +62,11 @@ typedef struct {
     int32_t device;            /* CUDA device ordinal */
     int32_t deterministic;     /* 1: every node sums its forces in the reference's order (bitwise equal results);
                                   the only mode of this version */
+    float collision_hz;        /* WorldSettings::collision_hz (120): the contact pairs are searched again every
+                                  ceil(1 / (collision_hz dt)) substeps and at each frame's start */
+    int32_t inter_body_collisions; /* WorldSettings::inter_body_collisions (1) */
+    int32_t max_pairs;         /* capacity of the contact pair list of all islands (default 2^21); more pairs in one
+                                  search raise BL_GPU_DEVERR_PAIRS and that island's contacts are skipped */
 } bl_gpu_config;
 
 /* == bl::phys::Node (softbody.h:43-48): 32 bytes */
@@ -99,6 +104,17 @@ typedef struct {
     float damping;             /* stiffness-proportional damping (s) */
     float drill;               /* the corners' drilling spring, a share of G t A */
 } bl_shell_section;
+
+/* == bl::phys::Triangle (softbody.h:138-147): 20 bytes. A collision triangle between three of the body's nodes
+ * (SoftBody::add_triangle, softbody.h:958; rest_edge2 as SoftBody::finalize sets it, softbody.cpp:80). */
+typedef struct {
+    uint32_t a, b, c;
+    uint8_t surface;
+    uint8_t two_sided;         /* 0: a hull triangle - one-sided, its winding faces out */
+    uint8_t torn;              /* stretched past 2.5x its longest rest edge: no collision */
+    uint8_t pad;
+    float rest_edge2;          /* longest rest edge, squared */
+} bl_tri;
 
 /* A triangle element between three body nodes, as FemFrame::add_tri makes it (frame_fem.cpp:201-209), and the mass
  * it put on its corners (ShellMesher::tri, fem_shell.cpp:17-31; <= 0: its section's areal mass) */
@@ -143,6 +159,16 @@ typedef struct {
     float max_speed;           /* SoftBody::max_speed at upload (the first frame's static query margin) */
     int32_t sleeping;          /* SoftBody::sleeping at upload */
     const bl_fem_desc* fem;    /* NULL: no FEM frame */
+    /* contacts with other bodies' nodes (World::rebuild_pairs / collide_pairs): node-triangle pairs */
+    int32_t n_tris;            /* SoftBody::tris (none on a body with a FEM frame) */
+    const bl_tri* tris;
+    float collision_radius;    /* SoftBody::collision_radius (0.05) */
+    float contact_friction;    /* SoftBody::contact_friction (1) */
+    float hull_depth;          /* SoftBody::hull_depth (0.3) */
+    float face_skin;           /* SoftBody::face_skin (0.002) */
+    int32_t faces_only;        /* SoftBody::faces_only */
+    int32_t collision_group;   /* SoftBody::collision_group (0: none) */
+    int32_t self_collision;    /* SoftBody::self_collision: not supported (BL_GPU_EUNSUPPORTED when set) */
 } bl_body_desc;
 
 /* A body's runtime state (SoftBody::aabb, max_speed, sleeping, static_contacts, stats.broken_beams, sleep_timer) */
@@ -157,6 +183,8 @@ typedef struct {
     int32_t repaired_nodes;    /* nodes World::repair_nodes reset, since upload */
     int32_t fem_failures;      /* FemFrame::solve_failures: failed factorizations and non-finite velocity changes */
     int32_t fem_clamps;        /* FemFrame::clamps: velocity changes cut to the safety limits */
+    int32_t body_contacts;     /* SoftBody::body_contacts: contacts with other bodies over the last frame */
+    int32_t wake_request;      /* SoftBody::wake_request: a moving body touched it while it slept */
 } bl_body_state;
 
 /* WorldStats (world.h:79-132), the fields this path fills, and the device's error word */
@@ -166,12 +194,21 @@ typedef struct {
     int64_t total_substeps;    /* since the context was made */
     int64_t kernel_launches;   /* kernels this library launched since the context was made */
     uint32_t device_errors;    /* BL_GPU_DEVERR_* bits raised by the kernels */
+    int64_t contacts;          /* contacts between bodies applied since the context was made */
+    int64_t pair_searches;     /* an island's pair search (World::rebuild_pairs + near_pairs) counts one */
+    int32_t pairs;             /* candidate pairs of all islands after the last search */
+    int32_t islands;           /* islands of the last frame with contact pairs */
 } bl_world_stats;
 
 enum {
     BL_GPU_DEVERR_CANDIDATES = 1 << 0, /* a body's static candidate list overflowed BL_GPU_MAX_CANDIDATES */
-    BL_GPU_DEVERR_NONFINITE = 1 << 1   /* a body needed the repair of non-finite / runaway nodes */
+    BL_GPU_DEVERR_NONFINITE = 1 << 1,  /* a body needed the repair of non-finite / runaway nodes */
+    BL_GPU_DEVERR_PAIRS = 1 << 2,      /* the contact pair list overflowed bl_gpu_config.max_pairs */
+    BL_GPU_DEVERR_ISLAND = 1 << 3,     /* an island with contact pairs held more than BL_GPU_MAX_ISLAND_BODIES bodies */
+    BL_GPU_DEVERR_GRID = 1 << 4,       /* a fast body's contact grid overflowed (nodes listed in more than 4 cells each) */
+    BL_GPU_DEVERR_CONTACT_UNSUPPORTED = 1 << 5 /* a body with a FEM frame met another body's triangles (not stepped) */
 };
+#define BL_GPU_MAX_ISLAND_BODIES 256
 #define BL_GPU_MAX_CANDIDATES 64
 
 typedef struct bl_gpu_ctx bl_gpu_ctx;
@@ -231,6 +268,12 @@ int bl_gpu_download_all_nodes(bl_gpu_ctx* ctx, bl_node* out, int32_t n, void* st
  * callers that keep their own data on the GPU; each body's first node and beam. Valid until the next bl_gpu_add_body. */
 int bl_gpu_device_nodes(bl_gpu_ctx* ctx, void** nodes, int32_t* total_nodes);
 int bl_gpu_body_range(bl_gpu_ctx* ctx, int32_t body, int32_t* first_node, int32_t* n_nodes, int32_t* first_beam, int32_t* n_beams);
+
+/* The contact pairs (node, triangle) of the last pair search, island after island (islands in the order of their
+ * first body, each island's pairs in the reference's order: World::Island::nt after rebuild_pairs + near_pairs,
+ * world.cpp:1851-2598): 4 int32 a pair - the node's body, the node, the triangle's body, the triangle. Writes at most
+ * `capacity` pairs; *n_pairs = all of them. Waits for the device. */
+int bl_gpu_download_pairs(bl_gpu_ctx* ctx, int32_t* pairs, int32_t capacity, int32_t* n_pairs);
 
 /* One frame of n substeps, like bl_gpu_step_substeps, with a timing event between its kernels; waits for it and
  * returns the GPU time of each kind of kernel (summed over the frame's substeps). */
