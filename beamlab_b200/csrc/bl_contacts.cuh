@@ -29,11 +29,10 @@ namespace blg {
 
 constexpr int kIslMaxBodies = 256;     // bodies of one island with contact pairs (more: DEVERR_ISLAND)
 constexpr int kGridCells = 48 * 48 * 48;
-constexpr int kGridItemsPerNode = 4;   // fast grid entries per node (a node in the cells of its travel)
 constexpr float kFastSpeed = 8.0f;     // world.cpp:1881
 constexpr float kTornStretch2 = 2.5f * 2.5f; // softbody.h:154
 enum : uint32_t { TF_TWO_SIDED = 1, TF_TORN = 2 };
-enum : uint32_t { DEVERR_PAIRS = 4, DEVERR_ISLAND = 8, DEVERR_GRID = 16, DEVERR_CONTACT_UNSUPPORTED = 32 };
+enum : uint32_t { DEVERR_PAIRS = 4, DEVERR_ISLAND = 8, DEVERR_CONTACT_UNSUPPORTED = 32 };
 
 struct Contacts {
     int4* tri;                 // a, b, c, flags | body << 8
@@ -63,7 +62,7 @@ struct Contacts {
     int* run_end;
     int* g_start;              // fast grids (kGridCells + 1 per island)
     int* g_fill;
-    int* g_items;              // kGridItemsPerNode per node
+    int* g_items;              // fast grids' nodes, each listed once, in the lowest cell of its travel
     float4* fsplit;            // per node: the force before the contacts (bodies of islands with pairs)
     int* counters;             // [0] pair searches [1] contacts [2] pairs of the searches
     int interval;              // rebuild interval in substeps (world.cpp:1887)
@@ -294,6 +293,7 @@ struct RebuildShared {
     // the fast grid of the current fast body
     float g_org[3], g_inv;
     int g_dim[3];
+    int g_span[3];        // the most cells a node's travel spans along each axis, less one
 };
 
 __device__ __forceinline__ bool same_group(const Body& a, const Body& b) { return a.group != 0 && a.group == b.group; }
@@ -449,18 +449,21 @@ __device__ int fast_query(const RebuildShared& S, const Contacts& C, const Body*
     const int y0 = max(0, (int)floorf((mn.y - S.g_org[1]) * S.g_inv)), y1 = min(S.g_dim[1] - 1, (int)((mx.y - S.g_org[1]) * S.g_inv));
     const int z0 = max(0, (int)floorf((mn.z - S.g_org[2]) * S.g_inv)), z1 = min(S.g_dim[2] - 1, (int)((mx.z - S.g_org[2]) * S.g_inv));
     if (x0 > x1 || y0 > y1 || z0 > z1) return 0;
+    // The reference lists a node in every cell of its travel and scans the cells of the box: a node is found when its
+    // cells' box meets the scan's box. Here each node is listed once, in its lowest cell: the scan starts g_span
+    // cells lower and keeps the nodes whose box reaches the scan's box - each found once, as after the reference's
+    // sort and deduplication.
     int n = 0;
-    for (int z = z0; z <= z1; z++)
-        for (int y = y0; y <= y1; y++)
-            for (int x = x0; x <= x1; x++) {
+    for (int z = max(0, z0 - S.g_span[2]); z <= z1; z++)
+        for (int y = max(0, y0 - S.g_span[1]); y <= y1; y++)
+            for (int x = max(0, x0 - S.g_span[0]); x <= x1; x++) {
                 const int cell = (z * S.g_dim[1] + y) * S.g_dim[0] + x;
                 const int k0 = C.g_start[gs0 + cell], k1 = C.g_start[gs0 + cell + 1];
                 for (int k = k0; k < k1; k++) {
                     const int ni = C.g_items[gi0 + k];
-                    // taken once: in the first cell (z, y, x order) of its own cells' box within the scan's box
                     int3 lo, hi;
                     node_cells(S, nd, ni, lo, hi);
-                    if (max(lo.x, x0) != x || max(lo.y, y0) != y || max(lo.z, z0) != z) continue;
+                    if (hi.x < x0 || hi.y < y0 || hi.z < z0) continue;
                     const v3 p = nd_p(nd, ni);
                     const float rn = rt + length(nd_v(nd, ni)) * S.travel, rb = rn + depth;
                     if (p.x < tmn.x - rb || p.y < tmn.y - rb || p.z < tmn.z - rb || p.x > tmx.x + rb || p.y > tmx.y + rb || p.z > tmx.z + rb) continue;
@@ -723,7 +726,7 @@ __global__ void __launch_bounds__(1024) k_rebuild(Body* __restrict__ bodies, int
     }
     const float T = (float)max(interval, 1) * dt;
     const int gs0 = C.isl_idx[root] * (kGridCells + 1);
-    const int gi0 = kGridItemsPerNode * pt0;
+    const int gi0 = pt0;
     // ---- 2) count, then 3) write: the slow queries (bodies with partners, triangles in order), then the fast pairs
     int total = 0;
     for (int pass = 0; pass < 2; pass++) {
@@ -779,19 +782,21 @@ __global__ void __launch_bounds__(1024) k_rebuild(Body* __restrict__ bodies, int
                 S.g_dim[0] = max(1, min(48, (int)(ex * S.g_inv) + 1));
                 S.g_dim[1] = max(1, min(48, (int)(ey * S.g_inv) + 1));
                 S.g_dim[2] = max(1, min(48, (int)(ez * S.g_inv) + 1));
+                S.g_span[0] = S.g_span[1] = S.g_span[2] = 0;
             }
             __syncthreads();
             const int ncell = S.g_dim[0] * S.g_dim[1] * S.g_dim[2];
             for (int q = tid; q <= ncell; q += nt) C.g_start[gs0 + q] = 0;
             __syncthreads();
-            // every contacter node in the cells of its travel: counts, starts, items ascending within a cell
+            // every contacter node in the lowest cell of its travel: counts, starts, items ascending within a cell
             for (int i = tid; i < F.nnodes; i += nt) {
                 if (!((uint32_t)info[F.node0 + i].x & NF_CONTACTER)) continue;
                 int3 lo, hi;
                 node_cells(S, nd, F.node0 + i, lo, hi);
-                for (int z = lo.z; z <= hi.z; z++)
-                    for (int y = lo.y; y <= hi.y; y++)
-                        for (int x = lo.x; x <= hi.x; x++) atomicAdd(&C.g_start[gs0 + (z * S.g_dim[1] + y) * S.g_dim[0] + x + 1], 1);
+                atomicAdd(&C.g_start[gs0 + (lo.z * S.g_dim[1] + lo.y) * S.g_dim[0] + lo.x + 1], 1);
+                if (hi.x - lo.x > S.g_span[0]) atomicMax(&S.g_span[0], hi.x - lo.x);
+                if (hi.y - lo.y > S.g_span[1]) atomicMax(&S.g_span[1], hi.y - lo.y);
+                if (hi.z - lo.z > S.g_span[2]) atomicMax(&S.g_span[2], hi.z - lo.z);
             }
             __syncthreads();
             {
@@ -806,23 +811,14 @@ __global__ void __launch_bounds__(1024) k_rebuild(Body* __restrict__ bodies, int
                 }
             }
             __syncthreads();
-            const int nitems = C.g_start[gs0 + ncell];
-            if (nitems > kGridItemsPerNode * C.isl_nodes[root]) {
-                if (tid == 0) atomicOr(deverr, DEVERR_GRID);
-                continue; // (uniform: every thread read the same count)
-            }
             for (int q = tid; q < ncell; q += nt) C.g_fill[gs0 + q] = C.g_start[gs0 + q];
             __syncthreads();
             for (int i = tid; i < F.nnodes; i += nt) {
                 if (!((uint32_t)info[F.node0 + i].x & NF_CONTACTER)) continue;
                 int3 lo, hi;
                 node_cells(S, nd, F.node0 + i, lo, hi);
-                for (int z = lo.z; z <= hi.z; z++)
-                    for (int y = lo.y; y <= hi.y; y++)
-                        for (int x = lo.x; x <= hi.x; x++) {
-                            const int at2 = atomicAdd(&C.g_fill[gs0 + (z * S.g_dim[1] + y) * S.g_dim[0] + x], 1);
-                            C.g_items[gi0 + at2] = F.node0 + i;
-                        }
+                const int at2 = atomicAdd(&C.g_fill[gs0 + (lo.z * S.g_dim[1] + lo.y) * S.g_dim[0] + lo.x], 1);
+                C.g_items[gi0 + at2] = F.node0 + i;
             }
             __syncthreads();
             for (int q = tid; q < ncell; q += nt) {

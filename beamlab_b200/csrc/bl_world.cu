@@ -551,7 +551,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     BL_CUDA(c, c->bk_fill.alloc(4 * (size_t)N + 65 * (size_t)B + 1));
     BL_CUDA(c, c->g_start.alloc((size_t)c->max_isl * (kGridCells + 1)));
     BL_CUDA(c, c->g_fill.alloc((size_t)c->max_isl * (kGridCells + 1)));
-    BL_CUDA(c, c->g_items.alloc((size_t)kGridItemsPerNode * N));
+    BL_CUDA(c, c->g_items.alloc(N));
     BL_CUDA(c, c->fsplit.alloc(N));
     // (the pair list starts as valid indices: k_detect reads up to the last search's total)
     BL_CUDA(c, cudaMemsetAsync(c->pairs.p, 0, sizeof(int2) * c->cfg.max_pairs, c->stream));

@@ -154,6 +154,70 @@ def lattice_body_fast(gen: np.random.Generator, dims=(20, 4, 5), spacing=0.25, o
     }
 
 
+def lattice_tris(dims) -> np.ndarray:
+    """Collision triangles over the outer faces of an nx x ny x nz lattice (node index (ix*ny + iy)*nz + iz): each face
+    quad as two triangles wound so that cross(b - a, c - a) points out of the body - the SoftBody::add_triangle calls
+    (softbody.h:958) that give a lattice truss a skin other bodies' nodes collide with (hull triangles when one-sided)."""
+    nx, ny, nz = dims
+    idx = lambda ix, iy, iz: (ix * ny + iy) * nz + iz
+    tris = []
+
+    def face(corner, nu, nv, outward):
+        # corner(i, j) -> node; (u, v) spans the face; outward: cross(u, v) points out of the body
+        for i in range(nu - 1):
+            for j in range(nv - 1):
+                p00, p10, p01, p11 = corner(i, j), corner(i + 1, j), corner(i, j + 1), corner(i + 1, j + 1)
+                if outward:
+                    tris.append((p00, p10, p11)), tris.append((p00, p11, p01))
+                else:
+                    tris.append((p00, p11, p10)), tris.append((p00, p01, p11))
+    face(lambda i, j: idx(0, i, j), ny, nz, False)            # -x: cross(y, z) = +x points in
+    face(lambda i, j: idx(nx - 1, i, j), ny, nz, True)        # +x
+    face(lambda i, j: idx(i, 0, j), nx, nz, True)             # -y: cross(x, z) = -y points out
+    face(lambda i, j: idx(i, ny - 1, j), nx, nz, False)       # +y
+    face(lambda i, j: idx(i, j, 0), nx, ny, False)            # -z: cross(x, y) = +z points in
+    face(lambda i, j: idx(i, j, nz - 1), nx, ny, True)        # +z
+    return np.asarray(tris, np.uint32).reshape(-1, 3)
+
+
+def crash_pair(seed: int = 1, speed_a: float = 12.0, speed_b: float = 12.0, gap: float = 0.3, hull: bool = False,
+               dims=(12, 4, 5), sleeping: bool = False) -> dict:
+    """Two lattice trusses with collision skins (lattice_tris) head on along x over flat ground: body 0 at speed_a
+    towards +x, body 1 at speed_b towards -x, their fronts `gap` apart; hull: one-sided (hull) skins."""
+    rng = TRng(seed)
+    length = (dims[0] - 1) * 0.25
+    a = lattice_body(rng, dims=dims, origin=(-gap / 2 - length, 0.05, -0.5), velocity=(speed_a, 0.0, 0.0),
+                     ground_friction=0.8 / GRASS_STATIC_FRICTION)
+    b = lattice_body(rng, dims=dims, origin=(gap / 2, 0.05, -0.45), velocity=(-speed_b, 0.0, 0.0),
+                     ground_friction=0.8 / GRASS_STATIC_FRICTION)
+    for body in (a, b):
+        body["tris"] = lattice_tris(dims)
+        body["tri_two_sided"] = np.full(len(body["tris"]), 0 if hull else 1, np.uint8)
+    return {
+        "settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005, "sleeping": sleeping},
+        "statics": {"terrain": flat_terrain(), "boxes": [], "build_grid": True},
+        "bodies": [a, b],
+        "name": f"crash_pair(seed={seed}, {speed_a}, {speed_b}, hull={hull})",
+    }
+
+
+def drop_pair(seed: int = 1, height: float = 7.0, dims=(8, 3, 4), hull: bool = False) -> dict:
+    """A lattice truss at rest on flat ground and another dropped onto it from `height` m above (both with collision
+    skins; sleeping on): the one below falls asleep before the other lands, and is woken by it."""
+    rng = TRng(seed)
+    b = lattice_body(rng, dims=dims, origin=(-1.0, 0.02, -0.4), ground_friction=0.8 / GRASS_STATIC_FRICTION)
+    a = lattice_body(rng, dims=dims, origin=(-0.9, 0.02 + height, -0.35), ground_friction=0.8 / GRASS_STATIC_FRICTION)
+    for body in (b, a):
+        body["tris"] = lattice_tris(dims)
+        body["tri_two_sided"] = np.full(len(body["tris"]), 0 if hull else 1, np.uint8)
+    return {
+        "settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005, "sleeping": True},
+        "statics": {"terrain": flat_terrain(), "boxes": [], "build_grid": True},
+        "bodies": [b, a],
+        "name": f"drop_pair(seed={seed}, height={height}, hull={hull})",
+    }
+
+
 def truss_car(seed: int = 1, speed: float = 15.0, dims=(20, 4, 5)) -> dict:
     """The plain explicit mass-spring truss car: a 20 x 4 x 5 node lattice (4.75 m long, 0.75 m high, 1 m wide) at
     0.25 m with +-2 mm jitter, node mass uniform in [4, 6] kg, beams to every neighbour within sqrt(3) * 0.25 m
@@ -249,11 +313,12 @@ def stress_rig(seed: int = 7) -> dict:
 
 def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, sigma: float = 0.6,
           min_nodes: int = 500, max_nodes: int = 20000, terrain_size: float = 1000.0, terrain_samples: int = 2048,
-          amplitude: float = 2.0) -> dict:
+          amplitude: float = 2.0, skins: bool = True) -> dict:
     """A batched fleet of lattice trusses with log-normal node counts (median `median_nodes`, clipped to
     [min_nodes, max_nodes]), each driving at a speed uniform in [5, 30] m/s with a random yaw over a square heightfield
-    of terrain_samples^2 samples spanning terrain_size metres, `amplitude` m of seeded smooth noise. Vehicles are laid
-    out on a grid 40 m apart so that none touch. Random draws: numpy's PCG64 seeded with `seed`."""
+    of terrain_samples^2 samples spanning terrain_size metres, `amplitude` m of seeded smooth noise. Vehicles start on
+    a grid 40 m apart; with skins (lattice_tris) those that meet collide. Random draws: numpy's PCG64 seeded with
+    `seed` (the skins draw none)."""
     gen = np.random.default_rng(seed)
     cell = terrain_size / (terrain_samples - 1)
     half = terrain_size / 2
@@ -283,8 +348,11 @@ def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, si
         ground = float(h[min(iz, terrain_samples - 1), min(ix, terrain_samples - 1)])
         speed = float(gen.uniform(5.0, 30.0))
         yaw = float(gen.uniform(0.0, 2 * math.pi))
-        bodies.append(lattice_body_fast(gen, dims=(nx, ny, nz), origin=(x0, ground + 0.6, z0),
-                                        velocity=(speed * math.cos(yaw), 0.0, speed * math.sin(yaw))))
+        body = lattice_body_fast(gen, dims=(nx, ny, nz), origin=(x0, ground + 0.6, z0),
+                                 velocity=(speed * math.cos(yaw), 0.0, speed * math.sin(yaw)))
+        if skins:
+            body["tris"] = lattice_tris((nx, ny, nz))
+        bodies.append(body)
     return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005},
             "statics": {"terrain": terrain, "boxes": [], "build_grid": True}, "bodies": bodies,
             "name": f"fleet(n={n_vehicles}, seed={seed})"}

@@ -205,7 +205,6 @@ enum {
     BL_GPU_DEVERR_NONFINITE = 1 << 1,  /* a body needed the repair of non-finite / runaway nodes */
     BL_GPU_DEVERR_PAIRS = 1 << 2,      /* the contact pair list overflowed bl_gpu_config.max_pairs */
     BL_GPU_DEVERR_ISLAND = 1 << 3,     /* an island with contact pairs held more than BL_GPU_MAX_ISLAND_BODIES bodies */
-    BL_GPU_DEVERR_GRID = 1 << 4,       /* a fast body's contact grid overflowed (nodes listed in more than 4 cells each) */
     BL_GPU_DEVERR_CONTACT_UNSUPPORTED = 1 << 5 /* a body with a FEM frame met another body's triangles (not stepped) */
 };
 #define BL_GPU_MAX_ISLAND_BODIES 256

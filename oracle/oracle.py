@@ -30,6 +30,9 @@ class BodyParams(C.Structure):
         ("ground_friction", C.c_float), ("bounce", C.c_float), ("contact_push_max", C.c_float),
         ("contact_slop", C.c_float), ("collision_radius", C.c_float), ("allow_deform", C.c_int32),
         ("allow_break", C.c_int32), ("ductile", C.c_int32), ("can_sleep", C.c_int32), ("sleep_speed", C.c_float),
+        # contacts with other bodies (RefBodyParams only; the restatement reads the fields above)
+        ("contact_friction", C.c_float), ("hull_depth", C.c_float), ("face_skin", C.c_float), ("faces_only", C.c_int32),
+        ("collision_group", C.c_int32),
     ]
 
 
@@ -39,7 +42,8 @@ def body_params(body: dict) -> BodyParams:
         float(p.get("ground_friction", 1.0)), float(p.get("bounce", -1.0)), float(p.get("contact_push_max", 2.0)),
         float(p.get("contact_slop", 0.0)), float(p.get("collision_radius", 0.05)), int(p.get("allow_deform", 1)),
         int(p.get("allow_break", 1)), int(p.get("ductile", 0)), int(p.get("can_sleep", 1)),
-        float(p.get("sleep_speed", 0.0)),
+        float(p.get("sleep_speed", 0.0)), float(p.get("contact_friction", 1.0)), float(p.get("hull_depth", 0.3)),
+        float(p.get("face_skin", 0.002)), int(p.get("faces_only", 0)), int(p.get("collision_group", 0)),
     )
 
 
@@ -90,6 +94,9 @@ def _load(path: str, prefix: str) -> C.CDLL:
         lib.ref_fem_pattern.argtypes = [vp, i, vp, vp, vp, vp]
         lib.ref_fem_nodes.argtypes = [vp, i, vp, vp, vp, vp]
         lib.ref_fem_tris.argtypes = [vp, i, vp, vp, vp, vp, vp]
+        lib.ref_set_tri_sides.argtypes = [vp, i, vp]
+        lib.ref_get_pairs.argtypes = [vp, vp, i]
+        lib.ref_get_pairs.restype = i
     _loaded[path] = lib
     return lib
 
@@ -151,12 +158,17 @@ class _OracleWorld:
         tris = np.ascontiguousarray(body.get("tris", np.zeros((0, 3), np.uint32)), dtype=np.uint32)
         prm = body_params(body)
         self._keep += list(a.values()) + [tris, prm]
-        return self._fn("add_body")(
+        idx = self._fn("add_body")(
             self._w, len(a["mass"]), _ptr(a["pos"], C.c_float), _ptr(a["vel"], C.c_float), _ptr(a["mass"], C.c_float),
             _ptr(a["node_flags"], C.c_uint16), _ptr(a["friction"], C.c_float), _ptr(a["radius"], C.c_float),
             len(a["k"]), _ptr(a["ab"], C.c_uint32), _ptr(a["k"], C.c_float), _ptr(a["d"], C.c_float),
             _ptr(a["strength"], C.c_float), _ptr(a["deform"], C.c_float), _ptr(a["beam_type"], C.c_uint8),
             _ptr(a["beam_flags"], C.c_uint8), len(tris), _ptr(tris, C.c_uint32), C.byref(prm))
+        if self.prefix == "ref" and len(tris) and "tri_two_sided" in body:
+            sides = np.ascontiguousarray(body["tri_two_sided"], dtype=np.uint8)
+            self._keep.append(sides)
+            self._lib.ref_set_tri_sides(self._w, idx, sides.ctypes.data)
+        return idx
 
     def step_substeps(self, n: int):
         self._fn("step_substeps")(self._w, int(n))
@@ -254,6 +266,15 @@ class RefWorld(_FemMixin, _OracleWorld):
 
     def __init__(self, flavour: str = "parity"):
         super().__init__(_load(REF_LIBS[flavour], "ref"))
+
+    def pairs(self) -> np.ndarray:
+        """Island::nt of the islands that searched for pairs in the last frame (world.cpp:3466-3475): rows of
+        (node's body, node, triangle's body, triangle)."""
+        n = self._lib.ref_get_pairs(self._w, None, 0)
+        out = np.zeros((n, 4), np.int32)
+        if n:
+            self._lib.ref_get_pairs(self._w, out.ctypes.data, n)
+        return out
 
 
 def ref_available(flavour: str = "parity") -> bool:

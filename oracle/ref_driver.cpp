@@ -52,6 +52,12 @@ struct RefBodyParams {
     int32_t ductile;
     int32_t can_sleep;
     float sleep_speed;
+    // contacts with other bodies (softbody.h:614-721)
+    float contact_friction;
+    float hull_depth;
+    float face_skin;
+    int32_t faces_only;
+    int32_t collision_group;
 };
 
 extern "C" {
@@ -131,12 +137,28 @@ int ref_add_body(RefWorld* r, int n_nodes, const float* pos, const float* vel, c
     b->ductile = p->ductile != 0;
     b->can_sleep = p->can_sleep != 0;
     b->sleep_speed = p->sleep_speed;
+    b->contact_friction = p->contact_friction;
+    b->hull_depth = p->hull_depth;
+    b->face_skin = p->face_skin;
+    b->faces_only = p->faces_only != 0;
+    b->collision_group = p->collision_group;
     b->finalize();
     r->bodies.push_back(r->w.add_body(std::move(b)));
     return (int)r->bodies.size() - 1;
 }
 
 void ref_step_substeps(RefWorld* r, int n) { r->w.step_substeps(n); }
+
+// Triangle::two_sided of a body's collision triangles (0: a hull triangle), set before its first step
+void ref_set_tri_sides(RefWorld* r, int body, const uint8_t* two_sided) {
+    SoftBody& b = *r->bodies[body];
+    for (size_t t = 0; t < b.tris.size(); t++) b.tris[t].two_sided = two_sided[t] != 0;
+    b.hull_count = -1;
+}
+
+// the islands' contact pairs of the last pair search (ref_world_tu.cpp)
+int ref_world_pairs(void* world, int32_t* out, int cap);
+int ref_get_pairs(RefWorld* r, int32_t* out, int cap) { return ref_world_pairs(&r->w, out, cap); }
 
 // ---- FEM shell plates (ShellMesher::grid, fem_shell.cpp:34-50) ----
 // A plate body of n x n cells: origin + du * i + dv * j, triangle elements of one shell section (E, nu, rho, t,

@@ -36,7 +36,7 @@ def test_gpu_matches_golden(name):
 
 @pytest.mark.parametrize("make", [lambda: rigs.truss_car(2, speed=30.0), lambda: rigs.stress_rig(11),
                                   lambda: rigs.fleet(12, seed=5, median_nodes=800, min_nodes=60, max_nodes=4000,
-                                                     terrain_size=300.0, terrain_samples=257)])
+                                                     terrain_size=300.0, terrain_samples=257, skins=False)])
 def test_gpu_matches_oracle_live(port_lib, make):
     from oracle.oracle import PortWorld, build_world
     rig = make()
