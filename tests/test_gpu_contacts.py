@@ -1,0 +1,81 @@
+"""Contacts between bodies on the GPU against the reference (World::rebuild_pairs / near_pairs / pair_detect /
+collide_pairs, world.cpp:1851-3023).
+
+The pair lists (every island's node-triangle pairs after each search, in the reference's order) must equal the
+reference's element for element, and the node states bit for bit: the pair search is integer and comparison work,
+and the contact response runs each island's pairs in the reference's order with its float operations in its order.
+Fixtures: tests/golden/make_golden_contacts.py (the reference, parity build)."""
+import numpy as np
+import pytest
+
+from beamlab_b200 import rigs, world_from_rig
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "crash_slow_s1": lambda: rigs.crash_pair(1, speed_a=3.0, speed_b=0.0, gap=0.1),
+    "crash_fast_s2": lambda: rigs.crash_pair(2, speed_a=12.0, speed_b=12.0, gap=0.5),
+    "crash_mixed_s3": lambda: rigs.crash_pair(3, speed_a=25.0, speed_b=3.0, gap=0.6),
+    "crash_hull_s4": lambda: rigs.crash_pair(4, speed_a=10.0, speed_b=4.0, gap=0.2, hull=True),
+}
+
+
+def bits(a):
+    a = np.ascontiguousarray(a, np.float32).copy()
+    a[np.isnan(a)] = np.nan  # (one NaN for all payloads)
+    return a.view(np.uint32)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_pairs_and_states_equal_reference_fixture(name):
+    g = golden(name)
+    w = world_from_rig(CASES[name]())
+    snaps = set(int(x) for x in g["snap_frames"])
+    total_pairs = 0
+    for f, n in enumerate(g["frames"]):
+        w.step_substeps(int(n))
+        got, want = w.pairs(), g[f"pairs_f{f}"]
+        assert got.shape == want.shape, f"frame {f}: {len(got)} pairs, the reference {len(want)}"
+        assert np.array_equal(got, want), f"frame {f}: pair lists differ"
+        total_pairs += len(want)
+        if f in snaps:
+            for b in range(2):
+                nd = w.bodies()[b].nodes()
+                assert np.array_equal(bits(nd["p"]), bits(g[f"pos{b}_f{f}"])), f"frame {f} body {b}: positions differ"
+                assert np.array_equal(bits(nd["v"]), bits(g[f"vel{b}_f{f}"])), f"frame {f} body {b}: velocities differ"
+    st = w.stats()
+    assert total_pairs > 0 and st["contacts"] > 0 and st["pair_searches"] > 0
+    assert st["device_errors"] == 0
+    w.close()
+
+
+@pytest.mark.parametrize("name", ["crash_mixed_s3", "crash_hull_s4"])
+def test_2000_substeps_equal_live_reference(ref_lib, name):
+    """2,013 substeps (61 frames of 33) of a crash: every node state bitwise the reference's (the tolerance the
+    contract allows is 1e-4 m; the path reaches equality)."""
+    from oracle.oracle import RefWorld, build_world
+    rig = CASES[name]()
+    w = world_from_rig(rig)
+    r = build_world(RefWorld, rig, multithreaded=False)
+    for _ in range(61):
+        w.step_substeps(33)
+        r.step_substeps(33)
+    for b in range(2):
+        nd, rn = w.bodies()[b].nodes(), r.nodes(b)
+        assert np.max(np.abs(nd["p"].astype(np.float64) - rn["pos"])) <= 1e-4
+        assert np.array_equal(bits(nd["p"]), bits(rn["pos"])) and np.array_equal(bits(nd["v"]), bits(rn["vel"]))
+        s, t = w.bodies()[b].state(), r.body(b)
+        assert np.array_equal(s["aabb_min"], t["aabb_min"]) and s["max_speed"] == t["max_speed"]  # (values: -0 == +0)
+    w.close()
+    r.close()
+
+
+def test_contacts_off_keeps_bodies_apart_from_pairs():
+    """WorldSettings::inter_body_collisions off: no islands, no pairs, the bodies pass through each other."""
+    rig = rigs.crash_pair(1, speed_a=3.0, speed_b=0.0, gap=0.1)
+    w = world_from_rig(rig, inter_body_collisions=False)
+    w.step_substeps(33)
+    st = w.stats()
+    assert len(w.pairs()) == 0 and st["contacts"] == 0 and st["pair_searches"] == 0
+    w.close()

@@ -148,3 +148,26 @@ def test_port_within_tolerance_of_reference_with_libm(port_lib):
         port.step_substeps(20)
     d = np.abs(ref.nodes(0)["pos"].astype(np.float64) - port.nodes(0)["pos"]).max()
     assert d <= 1e-4, d
+
+
+@pytest.mark.parametrize("name", ["crash_slow_s1", "crash_hull_s4"])
+def test_reference_contact_fixture_reproduces(ref_lib, name):
+    """The contact fixtures come from the reference: it gives them again (pairs each frame, node states), and the
+    pairs are valid (node, triangle) indices of the two bodies."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location("mgc", os.path.join(os.path.dirname(__file__), "golden", "make_golden_contacts.py"))
+    mgc = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mgc)
+    d = mgc.generate(name)
+    g = golden(name)
+    assert set(d) == set(g)
+    for k in g:
+        assert np.array_equal(d[k], g[k]), k
+    rig = mgc.CASES[name]()
+    for f in range(len(g["frames"])):
+        p = g[f"pairs_f{f}"]
+        if len(p):
+            assert set(np.unique(p[:, 0])) <= {0, 1} and np.all(p[:, 0] != p[:, 2])
+            for row in p:
+                assert row[1] < len(rig["bodies"][row[0]]["mass"]) and row[3] < len(rig["bodies"][row[2]]["tris"])

@@ -44,3 +44,17 @@ def test_fleet_sizes():
     assert 1000 < np.median(sizes) < 8000
     t = rig["statics"]["terrain"]
     assert t["heights"].shape == (257, 257) and np.abs(t["heights"]).max() <= 2.6
+
+
+def test_lattice_skin_faces_outward():
+    """lattice_tris: 2 triangles per face quad, every normal pointing away from the lattice's centre."""
+    dims = (5, 3, 4)
+    tris = rigs.lattice_tris(dims)
+    nx, ny, nz = dims
+    assert len(tris) == 4 * ((nx - 1) * (ny - 1) + (nx - 1) * (nz - 1) + (ny - 1) * (nz - 1))
+    rig = rigs.crash_pair(1, dims=dims)
+    p = rig["bodies"][0]["pos"].astype(np.float64)
+    c = p.mean(0)
+    a, b, d = p[tris[:, 0]], p[tris[:, 1]], p[tris[:, 2]]
+    n = np.cross(b - a, d - a)
+    assert np.all(np.einsum("ij,ij->i", n, (a + b + d) / 3 - c) > 0)
