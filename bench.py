@@ -4,8 +4,8 @@
 
 A step is one 60 Hz frame of 33 substeps (World::step_substeps(33)) over the whole workload. The default workload is
 the batched fleet: 256 seeded lattice vehicles of log-normal size (500-20,000 nodes, median 3,000; about 0.9 M nodes
-and 8.5 M beams) driving over a 2048^2-sample, 1 km^2 heightfield - the fleet configuration's shape without its wheel
-rings and inter-vehicle contacts (this path has no contacts between bodies yet). Under torchrun each rank steps its
+and 8.5 M beams) with collision skins, driving over a 2048^2-sample, 1 km^2 heightfield with contacts between the
+vehicles that meet - the fleet configuration's shape without its wheel rings. Under torchrun each rank steps its
 own fleet (weak scaling, no data-path collective: vehicles that do not touch are independent islands).
 
 Rank 0 prints one JSON line: value = node-substeps/s of all ranks with the state resident in HBM (CUDA events on the
@@ -47,9 +47,10 @@ def workload(name: str, rank: int):
     if name == "fleet256":
         rig = rigs.fleet(256, seed=3 + rank)
         n, m = rigs.rig_counts(rig)
-        desc = (f"fleet256: 256 lattice vehicles ({n:,} nodes, {m:,} beams; log-normal 500-20,000 nodes, median "
-                f"3,000), 2048^2-sample 1 km^2 heightfield, 5-30 m/s random yaw; no wheel rings, no inter-vehicle "
-                f"contacts")
+        nt = sum(len(b.get("tris", ())) for b in rig["bodies"])
+        desc = (f"fleet256: 256 lattice vehicles ({n:,} nodes, {m:,} beams, {nt:,} collision triangles; log-normal "
+                f"500-20,000 nodes, median 3,000), 2048^2-sample 1 km^2 heightfield, 5-30 m/s random yaw, "
+                f"inter-vehicle node-triangle contacts (islands, pair search every 17 substeps); no wheel rings")
     elif name == "plate64":
         rig = rigs.shell_plate(63, seed=1 + rank)
         n, m = rigs.rig_counts(rig)
@@ -134,9 +135,10 @@ def traffic_per_unit():
     return json.load(open(path)) if os.path.exists(path) else {}
 
 
-def cpu_reference(rig, n_nodes, frames=2, warm=4):
+def cpu_reference(rig, n_nodes, budget_s=10.0, max_frames=100, warm=4):
     """The reference's own step (compiled from its sources, Release flags) on all host cores: node-substeps/s of a
-    bounded sample (warm-up substeps, then `frames` frames of 33 substeps of the same workload)."""
+    bounded sample (warm-up substeps, then frames of 33 substeps of the same workload until about budget_s seconds
+    have passed, at least 2 and at most max_frames)."""
     from oracle.oracle import RefWorld, build_world, ref_available, ref_jobs_init, ref_jobs_shutdown
     if not ref_available("timing"):
         return None
@@ -145,8 +147,10 @@ def cpu_reference(rig, n_nodes, frames=2, warm=4):
     w = build_world(RefWorld, rig, flavour="timing", multithreaded=True)
     w.step_substeps(warm)
     t0 = time.perf_counter()
-    for _ in range(frames):
+    frames = 0
+    while frames < 2 or (frames < max_frames and time.perf_counter() - t0 < budget_s):
         w.step_substeps(FRAME)
+        frames += 1
     dt = time.perf_counter() - t0
     w.close()
     ref_jobs_shutdown("timing")
@@ -293,6 +297,8 @@ def run_gpu(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * NODE_DTYPE.itemsize,
                     "d2h_bytes_per_step": n * NODE_DTYPE.itemsize},
             "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
+            "contacts": {"applied": int(st1["contacts"] - st0["contacts"]), "pair_searches": int(st1["pair_searches"] - st0["pair_searches"]),
+                         "device_errors": int(st1["device_errors"])},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{pk_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": alg_bytes, "traffic": traffic},
