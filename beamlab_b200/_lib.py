@@ -42,6 +42,7 @@ _SIGNATURES = {
     "bl_gpu_set_node_force": ([_vp, _i32, _i32, _vp], C.c_int),
     "bl_gpu_download_fem": ([_vp, _i32, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "bl_gpu_download_pairs": ([_vp, _vp, _i32, _vp], C.c_int),
+    "bl_gpu_fem_stats": ([_vp, _vp], C.c_int),
     "bl_fem_pattern": ([_vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "bl_gpu_error_string": ([C.c_int], C.c_char_p),
     "bl_gpu_last_cuda_error": ([_vp], C.c_int),

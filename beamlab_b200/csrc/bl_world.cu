@@ -14,6 +14,7 @@
 #include "bl_contacts.cuh"
 #include "bl_fem_host.cuh"
 #include "bl_fem_kernels.cuh"
+#include "bl_fem_pcg.cuh"
 #include "bl_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -106,7 +107,15 @@ struct bl_gpu_ctx {
     int NF = 0, NT = 0, NB = 0, n_fem_nodes = 0;
     bool any_ext = false;
     std::vector<int> lvl_grp_ptr, lvl_col_ptr; // per level: its update groups / columns
-    int64_t fem_launches = 0;                  // kernels of one substep's frame step
+    int64_t fem_launches = 0;                  // kernels of one substep's frame step (with the Cholesky)
+    int64_t chol_launches = 0;                 // of those, the factorization's and substitutions'
+    // the frames' solve by PCG (bl_fem_pcg.cuh) and the residual check
+    DevBuf<double> px, pr, pz, pp, ppf, ppdi, pred, a0d, a0o, b0, res, plast;
+    DevBuf<int> pstat;
+    DevBuf<long long> piters;
+    DevBuf<float> guess, gscale;               // the learned per-frame-node dv guess (3) and preconditioner scale (9)
+    int pcg_grid = 1;
+    cudaStream_t aux = nullptr;                // (captures the bodies of conditional graph nodes)
     DevBuf<float4> ext, nforce, fq, fw, ftorque, tr0, tf, tt;
     DevBuf<int> fnode, fbody, fperm, fiperm, grp_tgt, grp_ptr, col_comp, comp_fail, rb_ptr, lvl_col, fem_nodes, fslot;
     DevBuf<int> fcol_ptr, frow, gdiag_ptr, goff_ptr, fem_fail, fem_clamp;
@@ -167,6 +176,8 @@ static void free_fem(bl_gpu_ctx* c) {
     c->fnode.free_(), c->fbody.free_(), c->fperm.free_(), c->fiperm.free_(), c->grp_tgt.free_(), c->grp_ptr.free_();
     c->col_comp.free_(), c->comp_fail.free_(), c->rb_ptr.free_(), c->lvl_col.free_(), c->fem_nodes.free_(), c->fslot.free_();
     c->fcol_ptr.free_(), c->frow.free_(), c->gdiag_ptr.free_(), c->goff_ptr.free_(), c->fem_fail.free_(), c->fem_clamp.free_();
+    c->px.free_(), c->pr.free_(), c->pz.free_(), c->pp.free_(), c->ppf.free_(), c->ppdi.free_(), c->pred.free_(), c->a0d.free_();
+    c->a0o.free_(), c->b0.free_(), c->res.free_(), c->plast.free_(), c->pstat.free_(), c->piters.free_(), c->guess.free_(), c->gscale.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
     c->xd.free_(), c->diag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
@@ -455,8 +466,9 @@ static int commit_fem(bl_gpu_ctx* c) {
         c->lvl_col_ptr.push_back((int)lvl_col.size());
     }
     // begin, triangles, assembly, per level a factor (and an update) kernel and two substitutions, velocities, integration
-    c->fem_launches = 5 + 3 * (int64_t)nlev;
-    for (int L = 0; L < nlev; L++) c->fem_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
+    c->chol_launches = 3 * (int64_t)nlev;
+    for (int L = 0; L < nlev; L++) c->chol_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
+    c->fem_launches = 5 + c->chol_launches;
     {   // each row's blocks in the order of their columns
         std::vector<std::vector<int2>> rows(NF);
         for (int k = 0; k < NF; k++)
@@ -505,6 +517,36 @@ static int commit_fem(bl_gpu_ctx* c) {
     F.col_comp = c->col_comp.p, F.comp_fail = c->comp_fail.p, F.rb_ptr = c->rb_ptr.p;
     F.rb = c->rb.p, F.lvl_col = c->lvl_col.p, F.ch2 = c->ch2.p, F.chd = c->chd.p, F.body_failures = c->fem_fail.p, F.body_clamps = c->fem_clamp.p;
     F.h = c->cfg.dt, F.step = c->cfg.dt;
+    // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
+    for (DevBuf<double>* d : {&c->px, &c->pr, &c->pz, &c->pp, &c->ppdi}) BL_CUDA(c, d->alloc(6 * (size_t)NF));
+    BL_CUDA(c, c->ppf.alloc(36 * (size_t)NF));
+    int per_sm = 0, nsm = 0, dev = c->cfg.device;
+    BL_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fem_pcg, 256, 0));
+    BL_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    c->pcg_grid = std::max(1, std::min(per_sm * nsm, (NF + 7) / 8));
+    BL_CUDA(c, c->pred.alloc(8 * (size_t)c->pcg_grid * 8));
+    BL_CUDA(c, c->pstat.alloc(4));
+    BL_CUDA(c, c->piters.alloc(1));
+    BL_CUDA(c, c->plast.alloc(1));
+    BL_CUDA(c, c->res.alloc(4));
+    BL_CUDA(c, cudaMemsetAsync(c->pstat.p, 0, 4 * sizeof(int), c->stream));
+    BL_CUDA(c, cudaMemsetAsync(c->piters.p, 0, sizeof(long long), c->stream));
+    BL_CUDA(c, cudaMemsetAsync(c->plast.p, 0, sizeof(double), c->stream));
+    BL_CUDA(c, cudaMemsetAsync(c->res.p, 0, 4 * sizeof(double), c->stream));
+    if (c->cfg.fem_check_residual) {
+        BL_CUDA(c, c->a0d.alloc(36 * (size_t)NF));
+        BL_CUDA(c, c->a0o.alloc(36 * (size_t)std::max(NB, 1)));
+        BL_CUDA(c, c->b0.alloc(6 * (size_t)NF));
+    }
+    BL_CUDA(c, c->guess.alloc(3 * (size_t)NF));
+    BL_CUDA(c, c->gscale.alloc(9 * (size_t)NF));
+    BL_CUDA(c, cudaMemsetAsync(c->guess.p, 0, sizeof(float) * 3 * NF, c->stream));
+    {
+        std::vector<float> eye(9 * (size_t)NF, 0.0f);
+        for (int i = 0; i < NF; i++) eye[9 * i] = eye[9 * i + 4] = eye[9 * i + 8] = 1.0f;
+        BL_CUDA(c, cudaMemcpyAsync(c->gscale.p, eye.data(), sizeof(float) * eye.size(), cudaMemcpyHostToDevice, c->stream));
+        BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
     return BL_GPU_OK;
 }
 
@@ -690,13 +732,74 @@ static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0
 
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
     int64_t per = 2;
-    if (c->NF > 0) per += c->fem_launches;
+    if (c->NF > 0) {
+        per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
+        if (c->cfg.fem_solver != BL_GPU_FEM_CHOLESKY) per += 1 - c->chol_launches; // (the Cholesky runs on a fallback only)
+    }
     int64_t total = per * n + 3;
     if (c->contacts_on) {
         total += 1 + 4 * (int64_t)n; // k_islands; k_wake, k_detect, k_collide, k_nodes phase 1 a substep
         for (int k = 0; k < n; k++) total += rebuild_at(c, k) ? 1 : 0;
     }
     return total;
+}
+
+// A condition of the graph being captured on s (its default 1 at every launch of the graph); false when s is not
+// capturing.
+static bool make_condition(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle* h) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr) != cudaSuccess || st != cudaStreamCaptureStatusActive) return false;
+    return cudaGraphConditionalHandleCreate(h, g, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+}
+
+// body(stream) under an IF node of the graph being captured on s, after everything captured so far (the body is
+// captured on the context's aux stream into the node's body graph); without capture, body(s) runs as it is.
+template <class Fn>
+static void enqueue_if(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle h, bool have, Fn body) {
+    if (!have) {
+        body(s);
+        return;
+    }
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd);
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (cudaGraphAddNode(&node, g, deps, nd, &p) != cudaSuccess) {
+        body(s); // (recorded as an error by the capture's end if the graph is unusable)
+        return;
+    }
+    cudaGraph_t bg = p.conditional.phGraph_out[0];
+    cudaStreamBeginCaptureToGraph(c->aux, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    body(c->aux);
+    cudaGraph_t out = nullptr;
+    cudaStreamEndCapture(c->aux, &out);
+    cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+// The frames' PCG solve: one cooperative launch of k_fem_pcg (bl_fem_pcg.cuh)
+static void launch_pcg(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle h, bool have, bool learned) {
+    PcgArgs P{};
+    P.x = c->px.p, P.r = c->pr.p, P.z = c->pz.p, P.p = c->pp.p, P.pf = c->ppf.p, P.pdi = c->ppdi.p;
+    P.guess = learned ? c->guess.p : nullptr;
+    P.scale = learned ? c->gscale.p : nullptr;
+    P.red = c->pred.p, P.stat = c->pstat.p, P.iters_total = c->piters.p, P.last_res = c->plast.p;
+    P.cond = h, P.has_cond = have ? 1 : 0;
+    P.max_iters = c->cfg.pcg_max_iters, P.tol = (double)c->cfg.pcg_tol;
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(c->pcg_grid), lc.blockDim = dim3(256), lc.dynamicSmemBytes = 0, lc.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at, lc.numAttrs = 1;
+    cudaLaunchKernelEx(&lc, k_fem_pcg, c->fd, P);
 }
 
 static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev = nullptr) {
@@ -741,19 +844,39 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
             k_fem_assemble<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
-            const int nlev = (int)c->lvl_col_ptr.size() - 1;
-            for (int L = 0; L < nlev; L++) {
-                const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1], g0 = c->lvl_grp_ptr[L], g1 = c->lvl_grp_ptr[L + 1];
-                k_fem_chol_level<<<(c1 - c0 + 3) / 4, 128, 0, s>>>(F, c0, c1);
-                if (g1 > g0) k_fem_update_level<<<(g1 - g0 + 3) / 4, 128, 0, s>>>(F, g0, g1);
+            if (c->cfg.fem_check_residual) {
+                cudaMemcpyAsync(c->a0d.p, c->diag.p, sizeof(double) * 36 * c->NF, cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(c->a0o.p, c->off.p, sizeof(double) * 36 * std::max(c->NB, 1), cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(c->b0.p, c->rhs.p, sizeof(double) * 6 * c->NF, cudaMemcpyDeviceToDevice, s);
             }
-            for (int L = 0; L < nlev; L++) {
-                const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
-                k_fem_forward_level<<<(c1 - c0 + 3) / 4, 128, 0, s>>>(F, c0, c1);
+            auto cholesky = [c, &F](cudaStream_t cs) {
+                const int nlev = (int)c->lvl_col_ptr.size() - 1;
+                for (int L = 0; L < nlev; L++) {
+                    const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1], g0 = c->lvl_grp_ptr[L], g1 = c->lvl_grp_ptr[L + 1];
+                    k_fem_chol_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
+                    if (g1 > g0) k_fem_update_level<<<(g1 - g0 + 3) / 4, 128, 0, cs>>>(F, g0, g1);
+                }
+                for (int L = 0; L < nlev; L++) {
+                    const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
+                    k_fem_forward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
+                }
+                for (int L = nlev - 1; L >= 0; L--) {
+                    const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
+                    k_fem_backward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
+                }
+            };
+            if (c->cfg.fem_solver == BL_GPU_FEM_CHOLESKY) {
+                cholesky(s);
+            } else {
+                // PCG first; the Cholesky under a conditional node that the PCG kernel sets when it missed the tolerance
+                cudaGraphConditionalHandle h{};
+                const bool have = make_condition(c, s, &h);
+                launch_pcg(c, s, h, have, c->cfg.fem_solver == BL_GPU_FEM_PCG_LEARNED);
+                enqueue_if(c, s, h, have, cholesky);
             }
-            for (int L = nlev - 1; L >= 0; L--) {
-                const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
-                k_fem_backward_level<<<(c1 - c0 + 3) / 4, 128, 0, s>>>(F, c0, c1);
+            if (c->cfg.fem_check_residual) {
+                k_fem_residual<<<(c->NF + 3) / 4, 128, 0, s>>>(F, c->a0d.p, c->a0o.p, c->b0.p, c->res.p);
+                k_fem_residual_done<<<1, 1, 0, s>>>(c->res.p);
             }
             k_fem_velocity<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
             k_fem_integrate<<<(c->n_fem_nodes + 255) / 256, 256, 0, s>>>(F, c->nd.p, c->nforce.p, c->fem_nodes.p, c->n_fem_nodes, c->fslot.p, c->info.p,
@@ -833,6 +956,10 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->collision_hz = 120.0f;
     cfg->inter_body_collisions = 1;
     cfg->max_pairs = 1 << 21;
+    cfg->fem_solver = BL_GPU_FEM_CHOLESKY;
+    cfg->pcg_max_iters = 200;
+    cfg->pcg_tol = 1e-6f;
+    cfg->fem_check_residual = 0;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -857,7 +984,9 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_config c0;
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
-    if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1) return BL_GPU_EINVAL;
+    if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 2 || c0.pcg_max_iters < 0 ||
+        !(c0.pcg_tol > 0))
+        return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
     cudaDeviceProp prop;
@@ -873,6 +1002,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     cudaError_t e;
     if ((e = cudaSetDevice(c0.device)) != cudaSuccess) return fail(e);
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    if ((e = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
     if ((e = cudaEventCreateWithFlags(&c->order_event, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     c->last_stream = c->stream;
     if ((e = cudaMemcpyToSymbol(c_ground, kGroundModels, sizeof(kGroundModels))) != cudaSuccess) return fail(e);
@@ -892,6 +1022,7 @@ int bl_gpu_destroy(bl_gpu_ctx* c) {
     c->deverr.free_();
     if (c->order_event) cudaEventDestroy(c->order_event);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->aux) cudaStreamDestroy(c->aux);
     delete c;
     return BL_GPU_OK;
 }
@@ -1154,6 +1285,11 @@ int bl_gpu_stats(bl_gpu_ctx* c, bl_world_stats* out) {
     out->substeps = c->last_substeps;
     out->total_substeps = c->total_substeps;
     out->kernel_launches = c->launches;
+    if (c->NF > 0 && c->cfg.fem_solver != BL_GPU_FEM_CHOLESKY) { // (the factorization's kernels ran on the fallbacks)
+        int st[4];
+        BL_CUDA(c, cudaMemcpy(st, c->pstat.p, sizeof(st), cudaMemcpyDeviceToHost));
+        out->kernel_launches += (int64_t)st[1] * c->chol_launches;
+    }
     if (c->contacts_on) {
         int cnt[4];
         BL_CUDA(c, cudaMemcpy(cnt, c->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost));
@@ -1162,6 +1298,26 @@ int bl_gpu_stats(bl_gpu_ctx* c, bl_world_stats* out) {
         out->pair_searches = cnt[0], out->contacts = cnt[1], out->pairs = total;
         for (int i = 0; i < (int)recs.size(); i++) out->islands += (recs[i].pairs && recs[i].island == i) ? 1 : 0;
     }
+    return BL_GPU_OK;
+}
+
+int bl_gpu_fem_stats(bl_gpu_ctx* c, bl_fem_stats* out) {
+    if (!c || !out) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    int rc = ensure_committed(c);
+    if (rc) return rc;
+    std::memset(out, 0, sizeof(*out));
+    if (c->NF == 0) return BL_GPU_OK;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    int st[4];
+    long long it = 0;
+    double res[4], last = 0;
+    BL_CUDA(c, cudaMemcpy(st, c->pstat.p, sizeof(st), cudaMemcpyDeviceToHost));
+    BL_CUDA(c, cudaMemcpy(&it, c->piters.p, sizeof(it), cudaMemcpyDeviceToHost));
+    BL_CUDA(c, cudaMemcpy(res, c->res.p, sizeof(res), cudaMemcpyDeviceToHost));
+    BL_CUDA(c, cudaMemcpy(&last, c->plast.p, sizeof(last), cudaMemcpyDeviceToHost));
+    out->pcg_solves = st[0], out->pcg_fallbacks = st[1], out->last_iterations = st[2], out->pcg_iterations = it;
+    out->last_pcg_residual = last, out->max_residual = res[0], out->last_residual = res[3];
     return BL_GPU_OK;
 }
 

@@ -61,6 +61,12 @@ class WorldSettings:
     sleep_time: float = 1.0
     collision_hz: float = 120.0
     inter_body_collisions: bool = True
+    # the FEM frames' implicit step (no counterpart in the reference, which always factors): "cholesky", "pcg",
+    # "pcg_learned"; a PCG solve that misses pcg_tol within pcg_max_iters falls back to the Cholesky
+    fem_solver: str = "cholesky"
+    pcg_max_iters: int = 200
+    pcg_tol: float = 1e-6
+    fem_check_residual: bool = False
 
 
 @dataclass
@@ -300,7 +306,18 @@ class _FrameProfile(C.Structure):
 class _Config(C.Structure):
     _fields_ = [("gravity", C.c_float * 3), ("dt", C.c_float), ("sleeping", C.c_int32), ("sleep_speed", C.c_float),
                 ("sleep_time", C.c_float), ("device", C.c_int32), ("deterministic", C.c_int32),
-                ("collision_hz", C.c_float), ("inter_body_collisions", C.c_int32), ("max_pairs", C.c_int32)]
+                ("collision_hz", C.c_float), ("inter_body_collisions", C.c_int32), ("max_pairs", C.c_int32),
+                ("fem_solver", C.c_int32), ("pcg_max_iters", C.c_int32), ("pcg_tol", C.c_float),
+                ("fem_check_residual", C.c_int32)]
+
+
+class _FemStats(C.Structure):
+    _fields_ = [("pcg_solves", C.c_int64), ("pcg_fallbacks", C.c_int64), ("pcg_iterations", C.c_int64),
+                ("last_iterations", C.c_int32), ("pad", C.c_int32), ("last_pcg_residual", C.c_double),
+                ("max_residual", C.c_double), ("last_residual", C.c_double)]
+
+
+FEM_SOLVERS = {"cholesky": 0, "pcg": 1, "pcg_learned": 2}
 
 
 class BodyHandle:
@@ -376,6 +393,10 @@ class World:
         cfg.device = device
         cfg.collision_hz = self.settings.collision_hz
         cfg.inter_body_collisions = int(self.settings.inter_body_collisions)
+        cfg.fem_solver = FEM_SOLVERS[self.settings.fem_solver]
+        cfg.pcg_max_iters = int(self.settings.pcg_max_iters)
+        cfg.pcg_tol = float(self.settings.pcg_tol)
+        cfg.fem_check_residual = int(self.settings.fem_check_residual)
         self._ctx = C.c_void_p()
         _check(self._L.bl_gpu_create(C.byref(cfg), C.byref(self._ctx)), "create")
         self._bodies: list[BodyHandle] = []
@@ -520,6 +541,13 @@ class World:
         _check(self._L.bl_gpu_profile_frame(self._ctx, int(n), self._stream(stream), C.byref(p)), "profile_frame",
                self._ctx)
         return {k: getattr(p, k) for k, _ in _FrameProfile._fields_}
+
+    def fem_stats(self) -> dict:
+        """The implicit FEM step's solver counters: PCG solves, fallbacks, iterations, residuals."""
+        self._send_statics()
+        s = _FemStats()
+        _check(self._L.bl_gpu_fem_stats(self._ctx, C.byref(s)), "fem_stats", self._ctx)
+        return {k: getattr(s, k) for k, _ in _FemStats._fields_ if k != "pad"}
 
     def pairs(self) -> np.ndarray:
         """The contact pairs of the last pair search, island after island, each in the reference's order: rows of

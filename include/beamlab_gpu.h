@@ -67,7 +67,18 @@ typedef struct {
     int32_t inter_body_collisions; /* WorldSettings::inter_body_collisions (1) */
     int32_t max_pairs;         /* capacity of the contact pair list of all islands (default 2^21); more pairs in one
                                   search raise BL_GPU_DEVERR_PAIRS and that island's contacts are skipped */
+    /* the FEM frames' implicit step (no counterpart in the reference, which always factors): */
+    int32_t fem_solver;        /* BL_GPU_FEM_CHOLESKY (default: the reference's block Cholesky), BL_GPU_FEM_PCG (conjugate
+                                  gradients, block-Jacobi, from zero), BL_GPU_FEM_PCG_LEARNED (from the learned per-node
+                                  guess, the preconditioner scaled by the learned 3x3 blocks); a PCG solve that misses
+                                  pcg_tol within pcg_max_iters falls back to the Cholesky for that substep */
+    int32_t pcg_max_iters;     /* default 200 */
+    float pcg_tol;             /* relative residual |A dv - rhs| / |rhs| to reach; default 1e-6 */
+    int32_t fem_check_residual; /* 1: keep a copy of each assembled system and measure the residual of the solution the
+                                   step took (bl_gpu_fem_stats); costs a copy of the system a substep */
 } bl_gpu_config;
+
+enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2 };
 
 /* == bl::phys::Node (softbody.h:43-48): 32 bytes */
 typedef struct {
@@ -267,6 +278,19 @@ int bl_gpu_download_all_nodes(bl_gpu_ctx* ctx, bl_node* out, int32_t n, void* st
  * callers that keep their own data on the GPU; each body's first node and beam. Valid until the next bl_gpu_add_body. */
 int bl_gpu_device_nodes(bl_gpu_ctx* ctx, void** nodes, int32_t* total_nodes);
 int bl_gpu_body_range(bl_gpu_ctx* ctx, int32_t body, int32_t* first_node, int32_t* n_nodes, int32_t* first_beam, int32_t* n_beams);
+
+/* The implicit FEM step's solver counters (all frames of the context as one system) */
+typedef struct {
+    int64_t pcg_solves;        /* PCG solves run (fem_solver >= 1) */
+    int64_t pcg_fallbacks;     /* of those, the ones that missed pcg_tol and were factored instead */
+    int64_t pcg_iterations;    /* CG iterations over all solves */
+    int32_t last_iterations;   /* of the last solve */
+    int32_t pad;
+    double last_pcg_residual;  /* relative residual the last PCG solve reached */
+    double max_residual;       /* fem_check_residual: the largest relative residual of a solution the step took */
+    double last_residual;      /* fem_check_residual: that of the last substep */
+} bl_fem_stats;
+int bl_gpu_fem_stats(bl_gpu_ctx* ctx, bl_fem_stats* out);
 
 /* The contact pairs (node, triangle) of the last pair search, island after island (islands in the order of their
  * first body, each island's pairs in the reference's order: World::Island::nt after rebuild_pairs + near_pairs,
