@@ -43,6 +43,14 @@ _SIGNATURES = {
     "bl_gpu_download_fem": ([_vp, _i32, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "bl_gpu_download_pairs": ([_vp, _vp, _i32, _vp], C.c_int),
     "bl_gpu_fem_stats": ([_vp, _vp], C.c_int),
+    "bl_gpu_mlp_init": ([_vp, C.c_uint64], C.c_int),
+    "bl_gpu_mlp_set_weights": ([_vp, _vp, _i32], C.c_int),
+    "bl_gpu_mlp_get_weights": ([_vp, _vp, _i32], C.c_int),
+    "bl_gpu_mlp_record": ([_vp, _i32], C.c_int),
+    "bl_gpu_mlp_samples": ([_vp, _vp], C.c_int),
+    "bl_gpu_mlp_train": ([_vp, _i32, _i32, _f, C.c_uint64, _vp], C.c_int),
+    "bl_gpu_mlp_forward": ([_vp, _vp, _i32, _vp], C.c_int),
+    "bl_gpu_mlp_gradient": ([_vp, _vp, _vp, _vp, _i32, _vp, _vp], C.c_int),
     "bl_fem_pattern": ([_vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "bl_gpu_error_string": ([C.c_int], C.c_char_p),
     "bl_gpu_last_cuda_error": ([_vp], C.c_int),

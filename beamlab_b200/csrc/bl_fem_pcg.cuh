@@ -5,7 +5,10 @@
 // block Cholesky (frame_fem.cpp:2887-2954), which this library runs as the default and as the judge. k_fem_pcg solves
 // the same system by CG with a block-Jacobi preconditioner (each column's 6 x 6 diagonal block, its translational 3 x 3
 // part optionally scaled by a learned S: z = T D^-1 T^T r with T = diag(S, I), symmetric positive definite for any
-// invertible S) from an initial guess (zero, or a learned per-node dv). One cooperative launch per solve: a warp per
+// invertible S) from an initial guess: zero, or the best combination (in the energy norm: the Galerkin projection onto
+// their span) of the last substep's solution and, with the learned warm start, the network's per-node dv. The
+// projection makes a guess safe: its error in the A-norm is never larger than that of a zero start, however rough the
+// network's prediction. One cooperative launch per solve: a warp per
 // column for A p (the column's lower blocks transposed plus its row's blocks, fill blocks skipped), grid-wide sums in
 // a fixed order (the result does not depend on timing), until |r| <= tol |rhs| or the iteration budget is spent. On
 // success it writes dv where the Cholesky would have left it and clears the graph's condition, so the factorization
@@ -27,9 +30,11 @@ struct PcgArgs {
     double* p;
     double* pf;              // 36 / column: Cholesky factor of the column's diagonal block
     double* pdi;             // 6 / column: its inverse diagonal
-    const float* guess;      // 3 / frame node: initial translational dv (null: zero)
+    const float* guess;      // 3 / frame node: the network's translational dv (null: none)
+    double* xprev;           // 6 / column: the last substep's solution (kept here after every solve)
+    int use_prev;            // the last solution joins the initial guess
     const float* scale;      // 9 / frame node: the preconditioner's translational scale S (null: identity)
-    double* red;             // 2 x 4 / warp of the grid: partial sums (two buffers used in turn: a block may still read
+    double* red;             // 2 x 8 / warp of the grid: partial sums (two buffers used in turn: a block may still read
                              // one reduction's partials while another block writes the next's)
     int* stat;               // [0] solves [1] fallbacks [2] iterations of the last solve [3] solves with a failed block factor
     long long* iters_total;
@@ -106,14 +111,14 @@ __device__ __forceinline__ void precond(const PcgArgs& P, const FemDev& F, int k
     for (int j = 0; j < 6; j++) z[j] = u[j];
 }
 
-// the grid's partial sums (buffer `buf`, 4 a warp) added in a fixed order by warp 0 of each block into s_tot: every
+// the grid's partial sums (buffer `buf`, 8 a warp) added in a fixed order by warp 0 of each block into s_tot: every
 // block gets the same totals, so every block takes the same branches and meets the same grid syncs
 __device__ __forceinline__ void grid_totals(const PcgArgs& P, int buf, int nw, int nv, double* s_tot) {
-    const double* red = P.red + (size_t)buf * 4 * nw;
+    const double* red = P.red + (size_t)buf * 8 * nw;
     if (threadIdx.x < 32) {
-        double t[4] = {0, 0, 0, 0};
+        double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int w = threadIdx.x; w < nw; w += 32)
-            for (int c = 0; c < nv; c++) t[c] += red[4 * (size_t)w + c];
+            for (int c = 0; c < nv; c++) t[c] += red[8 * (size_t)w + c];
         for (int c = 0; c < nv; c++) t[c] = warp_sum(t[c]);
         if (threadIdx.x == 0)
             for (int c = 0; c < nv; c++) s_tot[c] = t[c];
@@ -123,13 +128,14 @@ __device__ __forceinline__ void grid_totals(const PcgArgs& P, int buf, int nw, i
 
 __global__ void __launch_bounds__(256) k_fem_pcg(FemDev F, PcgArgs P) {
     cgr::grid_group grid = cgr::this_grid();
-    __shared__ double s_tot[4];
+    __shared__ double s_tot[8];
     const int lane = threadIdx.x & 31;
     const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
     const int nf = F.nf;
-    double* red0 = P.red;                 // (the loop's first reduction)
-    double* red1 = P.red + 4 * (size_t)nw; // (the set-up's and the loop's second)
-    // ---- the preconditioner's factors, the initial guess
+    double* red0 = P.red;                  // (the loop's first reduction)
+    double* red1 = P.red + 8 * (size_t)nw; // (the set-up's and the loop's second)
+    const bool guess = P.guess || P.use_prev;
+    // ---- the preconditioner's factors; the guess's basis: u1 = the network's dv (in x), u2 = the last solution (in p)
     double nbad = 0;
     for (int k = gw; k < nf; k += nw) {
         if (lane != 0) continue;
@@ -137,21 +143,63 @@ __global__ void __launch_bounds__(256) k_fem_pcg(FemDev F, PcgArgs P) {
         const double* D = F.diag + 36 * (size_t)k;
         for (int x = 0; x < 36; x++) L[x] = D[x];
         if (!chol6_dev(L, P.pdi + 6 * (size_t)k)) nbad += 1;
-        double* xk = P.x + 6 * (size_t)k;
         const int i = F.perm[k];
-        const bool g = P.guess && !F.fixed[k];
-        for (int j = 0; j < 6; j++) xk[j] = (g && j < 3) ? (double)P.guess[3 * i + j] : 0.0;
+        const bool fx = F.fixed[k] != 0;
+        for (int j = 0; j < 6; j++) {
+            P.x[6 * (size_t)k + j] = (P.guess && !fx && j < 3) ? (double)P.guess[3 * i + j] : 0.0;
+            P.p[6 * (size_t)k + j] = (P.use_prev && !fx) ? P.xprev[6 * (size_t)k + j] : 0.0;
+        }
+    }
+    double a1 = 0, a2 = 0;
+    if (guess) {
+        // Galerkin: x0 = a1 u1 + a2 u2 with [u.A u][a] = [u.b]; A u1 into z, A u2 into r
+        grid.sync();
+        double pr[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = gw; k < nf; k += nw) {
+            double au1[6], au2[6];
+            spmv_col(F, F.diag, F.off, k, P.x, lane, au1);
+            spmv_col(F, F.diag, F.off, k, P.p, lane, au2);
+            if (lane != 0) continue;
+            const double* b = F.rhs + 6 * (size_t)k;
+            const double* u1 = P.x + 6 * (size_t)k;
+            const double* u2 = P.p + 6 * (size_t)k;
+            for (int j = 0; j < 6; j++) {
+                P.z[6 * (size_t)k + j] = au1[j], P.r[6 * (size_t)k + j] = au2[j];
+                pr[0] += u1[j] * au1[j], pr[1] += u1[j] * au2[j], pr[2] += u2[j] * au2[j], pr[3] += u1[j] * b[j], pr[4] += u2[j] * b[j];
+            }
+        }
+        if (lane == 0)
+            for (int c = 0; c < 5; c++) red0[8 * (size_t)gw + c] = pr[c];
+        grid.sync();
+        grid_totals(P, 0, nw, 5, s_tot);
+        const double g11 = s_tot[0], g12 = s_tot[1], g22 = s_tot[2], c1 = s_tot[3], c2 = s_tot[4];
+        const double det = g11 * g22 - g12 * g12;
+        if (g11 > 0 && g22 > 0 && det > 1e-12 * g11 * g22) {
+            a1 = (c1 * g22 - c2 * g12) / det, a2 = (g11 * c2 - g12 * c1) / det;
+        } else if (g11 > 0 && (!(g22 > 0) || c1 * c1 / g11 >= c2 * c2 / g22)) {
+            a1 = c1 / g11;
+        } else if (g22 > 0) {
+            a2 = c2 / g22;
+        }
+        if (!(a1 == a1) || !(a2 == a2)) a1 = a2 = 0; // (NaN: from zero)
     }
     grid.sync();
-    // ---- r = b - A x0, z = P r, p = z
+    // ---- x0, r = b - A x0, z = P r, p = z
     double pr[4] = {0, 0, 0, 0}; // (lane 0: b.b, r.z, r.r)
     for (int k = gw; k < nf; k += nw) {
-        double ax[6];
-        spmv_col(F, F.diag, F.off, k, P.x, lane, ax);
         if (lane != 0) continue;
         const double* b = F.rhs + 6 * (size_t)k;
         double r[6], z[6];
-        for (int j = 0; j < 6; j++) r[j] = b[j] - ax[j];
+        for (int j = 0; j < 6; j++) {
+            const size_t q = 6 * (size_t)k + j;
+            if (guess) {
+                r[j] = b[j] - a1 * P.z[q] - a2 * P.r[q];
+                P.x[q] = a1 * P.x[q] + a2 * P.p[q];
+            } else {
+                r[j] = b[j];
+                P.x[q] = 0.0;
+            }
+        }
         precond(P, F, k, r, z);
         for (int j = 0; j < 6; j++) {
             P.r[6 * (size_t)k + j] = r[j], P.z[6 * (size_t)k + j] = z[j], P.p[6 * (size_t)k + j] = z[j];
@@ -159,8 +207,8 @@ __global__ void __launch_bounds__(256) k_fem_pcg(FemDev F, PcgArgs P) {
         }
     }
     if (lane == 0) {
-        for (int c = 0; c < 3; c++) red1[4 * (size_t)gw + c] = pr[c];
-        red1[4 * (size_t)gw + 3] = nbad;
+        for (int c = 0; c < 3; c++) red1[8 * (size_t)gw + c] = pr[c];
+        red1[8 * (size_t)gw + 3] = nbad;
     }
     grid.sync();
     grid_totals(P, 1, nw, 4, s_tot);
@@ -181,7 +229,7 @@ __global__ void __launch_bounds__(256) k_fem_pcg(FemDev F, PcgArgs P) {
             const double* pk = P.p + 6 * (size_t)k;
             for (int j = 0; j < 6; j++) P.z[6 * (size_t)k + j] = q[j], pq += pk[j] * q[j];
         }
-        if (lane == 0) red0[4 * (size_t)gw] = pq;
+        if (lane == 0) red0[8 * (size_t)gw] = pq;
         grid.sync();
         grid_totals(P, 0, nw, 1, s_tot);
         const double alpha = rz / s_tot[0];
@@ -197,7 +245,7 @@ __global__ void __launch_bounds__(256) k_fem_pcg(FemDev F, PcgArgs P) {
             precond(P, F, k, r, z);
             for (int j = 0; j < 6; j++) zk[j] = z[j], rzn += r[j] * z[j], rrn += r[j] * r[j];
         }
-        if (lane == 0) red1[4 * (size_t)gw] = rzn, red1[4 * (size_t)gw + 1] = rrn;
+        if (lane == 0) red1[8 * (size_t)gw] = rzn, red1[8 * (size_t)gw + 1] = rrn;
         grid.sync();
         grid_totals(P, 1, nw, 2, s_tot);
         rr = s_tot[1];

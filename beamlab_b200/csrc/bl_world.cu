@@ -15,6 +15,7 @@
 #include "bl_fem_host.cuh"
 #include "bl_fem_kernels.cuh"
 #include "bl_fem_pcg.cuh"
+#include "bl_mlp.cuh"
 #include "bl_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -110,12 +111,19 @@ struct bl_gpu_ctx {
     int64_t fem_launches = 0;                  // kernels of one substep's frame step (with the Cholesky)
     int64_t chol_launches = 0;                 // of those, the factorization's and substitutions'
     // the frames' solve by PCG (bl_fem_pcg.cuh) and the residual check
-    DevBuf<double> px, pr, pz, pp, ppf, ppdi, pred, a0d, a0o, b0, res, plast;
+    DevBuf<double> px, pr, pz, pp, ppf, ppdi, pred, a0d, a0o, b0, res, plast, pxprev;
     DevBuf<int> pstat;
     DevBuf<long long> piters;
     DevBuf<float> guess, gscale;               // the learned per-frame-node dv guess (3) and preconditioner scale (9)
     int pcg_grid = 1;
     cudaStream_t aux = nullptr;                // (captures the bodies of conditional graph nodes)
+    // the learned warm start (bl_mlp.cuh): parameters, the step's features, recorded samples, training scratch
+    DevBuf<float> mlp_w, mlp_m, mlp_v, feat, prev_dv, smp_x, smp_t, smp_w, gpart, lpart, gsum;
+    DevBuf<__nv_bfloat16> mlp_wb;
+    DevBuf<int> adj_ptr, adj, scount, sidx;
+    int rec_cap = 0;                           // the samples' capacity
+    bool rec_on = false;                       // the step records samples
+    int adam_t = 0;
     DevBuf<float4> ext, nforce, fq, fw, ftorque, tr0, tf, tt;
     DevBuf<int> fnode, fbody, fperm, fiperm, grp_tgt, grp_ptr, col_comp, comp_fail, rb_ptr, lvl_col, fem_nodes, fslot;
     DevBuf<int> fcol_ptr, frow, gdiag_ptr, goff_ptr, fem_fail, fem_clamp;
@@ -176,8 +184,9 @@ static void free_fem(bl_gpu_ctx* c) {
     c->fnode.free_(), c->fbody.free_(), c->fperm.free_(), c->fiperm.free_(), c->grp_tgt.free_(), c->grp_ptr.free_();
     c->col_comp.free_(), c->comp_fail.free_(), c->rb_ptr.free_(), c->lvl_col.free_(), c->fem_nodes.free_(), c->fslot.free_();
     c->fcol_ptr.free_(), c->frow.free_(), c->gdiag_ptr.free_(), c->goff_ptr.free_(), c->fem_fail.free_(), c->fem_clamp.free_();
-    c->px.free_(), c->pr.free_(), c->pz.free_(), c->pp.free_(), c->ppf.free_(), c->ppdi.free_(), c->pred.free_(), c->a0d.free_();
+    c->px.free_(), c->pr.free_(), c->pz.free_(), c->pp.free_(), c->ppf.free_(), c->ppdi.free_(), c->pred.free_(), c->a0d.free_(), c->pxprev.free_();
     c->a0o.free_(), c->b0.free_(), c->res.free_(), c->plast.free_(), c->pstat.free_(), c->piters.free_(), c->guess.free_(), c->gscale.free_();
+    c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
     c->xd.free_(), c->diag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
@@ -524,7 +533,9 @@ static int commit_fem(bl_gpu_ctx* c) {
     BL_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fem_pcg, 256, 0));
     BL_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     c->pcg_grid = std::max(1, std::min(per_sm * nsm, (NF + 7) / 8));
-    BL_CUDA(c, c->pred.alloc(8 * (size_t)c->pcg_grid * 8));
+    BL_CUDA(c, c->pred.alloc(2 * 8 * (size_t)c->pcg_grid * 8)); // (two buffers, 8 sums a warp, 8 warps a block)
+    BL_CUDA(c, c->pxprev.alloc(6 * (size_t)NF));
+    BL_CUDA(c, cudaMemsetAsync(c->pxprev.p, 0, sizeof(double) * 6 * NF, c->stream));
     BL_CUDA(c, c->pstat.alloc(4));
     BL_CUDA(c, c->piters.alloc(1));
     BL_CUDA(c, c->plast.alloc(1));
@@ -540,6 +551,26 @@ static int commit_fem(bl_gpu_ctx* c) {
     }
     BL_CUDA(c, c->guess.alloc(3 * (size_t)NF));
     BL_CUDA(c, c->gscale.alloc(9 * (size_t)NF));
+    {   // each frame node's 1-ring (the frame nodes it shares a triangle with), ascending: the network's neighbourhood
+        std::vector<std::vector<int>> nb(NF);
+        for (const int4& t : tn) {
+            const int v[3] = {t.x, t.y, t.z};
+            for (int a = 0; a < 3; a++)
+                for (int b2 = 0; b2 < 3; b2++)
+                    if (a != b2) nb[v[a]].push_back(v[b2]);
+        }
+        std::vector<int> aptr(NF + 1, 0), av;
+        for (int i = 0; i < NF; i++) {
+            std::sort(nb[i].begin(), nb[i].end());
+            nb[i].erase(std::unique(nb[i].begin(), nb[i].end()), nb[i].end());
+            av.insert(av.end(), nb[i].begin(), nb[i].end());
+            aptr[i + 1] = (int)av.size();
+        }
+        if ((rc = upload_vec(c, c->adj_ptr, aptr)) || (rc = upload_vec(c, c->adj, av))) return rc;
+    }
+    BL_CUDA(c, c->feat.alloc((size_t)kIn * NF));
+    BL_CUDA(c, c->prev_dv.alloc(3 * (size_t)NF));
+    BL_CUDA(c, cudaMemsetAsync(c->prev_dv.p, 0, sizeof(float) * 3 * NF, c->stream));
     BL_CUDA(c, cudaMemsetAsync(c->guess.p, 0, sizeof(float) * 3 * NF, c->stream));
     {
         std::vector<float> eye(9 * (size_t)NF, 0.0f);
@@ -735,6 +766,8 @@ static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
     if (c->NF > 0) {
         per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
         if (c->cfg.fem_solver != BL_GPU_FEM_CHOLESKY) per += 1 - c->chol_launches; // (the Cholesky runs on a fallback only)
+        const bool learned = c->cfg.fem_solver == BL_GPU_FEM_PCG_LEARNED, rec = c->rec_on;
+        per += (learned || rec ? 2 : 0) + (learned ? 1 : 0) + (rec ? 3 : 0);
     }
     int64_t total = per * n + 3;
     if (c->contacts_on) {
@@ -742,6 +775,14 @@ static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
         for (int k = 0; k < n; k++) total += rebuild_at(c, k) ? 1 : 0;
     }
     return total;
+}
+
+static MlpDev mlp_dev(const bl_gpu_ctx* c) {
+    MlpDev M{};
+    M.wb = c->mlp_wb.p, M.w = c->mlp_w.p, M.m = c->mlp_m.p, M.v = c->mlp_v.p;
+    M.adj_ptr = c->adj_ptr.p, M.adj = c->adj.p, M.prev_dv = c->prev_dv.p, M.feat = c->feat.p;
+    M.sx = c->smp_x.p, M.st = c->smp_t.p, M.sw = c->smp_w.p, M.scount = c->scount.p, M.cap = std::max(c->rec_cap, 1);
+    return M;
 }
 
 // A condition of the graph being captured on s (its default 1 at every launch of the graph); false when s is not
@@ -785,11 +826,14 @@ static void enqueue_if(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle
 }
 
 // The frames' PCG solve: one cooperative launch of k_fem_pcg (bl_fem_pcg.cuh)
-static void launch_pcg(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle h, bool have, bool learned) {
+static void launch_pcg(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle h, bool have, int solver) {
+    const bool learned = solver == BL_GPU_FEM_PCG_LEARNED;
     PcgArgs P{};
     P.x = c->px.p, P.r = c->pr.p, P.z = c->pz.p, P.p = c->pp.p, P.pf = c->ppf.p, P.pdi = c->ppdi.p;
     P.guess = learned ? c->guess.p : nullptr;
-    P.scale = learned ? c->gscale.p : nullptr;
+    P.scale = learned && c->cfg.pcg_learned_scale ? c->gscale.p : nullptr;
+    P.xprev = c->pxprev.p;
+    P.use_prev = (learned || solver == BL_GPU_FEM_PCG_PREVIOUS) ? 1 : 0;
     P.red = c->pred.p, P.stat = c->pstat.p, P.iters_total = c->piters.p, P.last_res = c->plast.p;
     P.cond = h, P.has_cond = have ? 1 : 0;
     P.max_iters = c->cfg.pcg_max_iters, P.tol = (double)c->cfg.pcg_tol;
@@ -849,6 +893,11 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                 cudaMemcpyAsync(c->a0o.p, c->off.p, sizeof(double) * 36 * std::max(c->NB, 1), cudaMemcpyDeviceToDevice, s);
                 cudaMemcpyAsync(c->b0.p, c->rhs.p, sizeof(double) * 6 * c->NF, cudaMemcpyDeviceToDevice, s);
             }
+            const bool learned = c->cfg.fem_solver == BL_GPU_FEM_PCG_LEARNED, rec = c->rec_on;
+            const MlpDev MD = mlp_dev(c);
+            if (learned || rec) k_mlp_features<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD, c->nd.p, c->nforce.p);
+            if (rec) k_mlp_record_pre<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
+            if (learned) k_mlp_infer<<<(c->NF + kLanes - 1) / kLanes, kLanes, 0, s>>>(F, MD, c->guess.p, c->gscale.p);
             auto cholesky = [c, &F](cudaStream_t cs) {
                 const int nlev = (int)c->lvl_col_ptr.size() - 1;
                 for (int L = 0; L < nlev; L++) {
@@ -871,13 +920,20 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                 // PCG first; the Cholesky under a conditional node that the PCG kernel sets when it missed the tolerance
                 cudaGraphConditionalHandle h{};
                 const bool have = make_condition(c, s, &h);
-                launch_pcg(c, s, h, have, c->cfg.fem_solver == BL_GPU_FEM_PCG_LEARNED);
+                launch_pcg(c, s, h, have, c->cfg.fem_solver);
                 enqueue_if(c, s, h, have, cholesky);
+                // (the solution, PCG's or the fallback's, is the next solve's guess)
+                cudaMemcpyAsync(c->pxprev.p, c->rhs.p, sizeof(double) * 6 * c->NF, cudaMemcpyDeviceToDevice, s);
             }
             if (c->cfg.fem_check_residual) {
                 k_fem_residual<<<(c->NF + 3) / 4, 128, 0, s>>>(F, c->a0d.p, c->a0o.p, c->b0.p, c->res.p);
                 k_fem_residual_done<<<1, 1, 0, s>>>(c->res.p);
             }
+            if (rec) {
+                k_mlp_record_post<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
+                k_mlp_record_done<<<1, 1, 0, s>>>(MD, c->NF);
+            }
+            if (learned || rec) k_mlp_store_dv<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
             k_fem_velocity<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
             k_fem_integrate<<<(c->n_fem_nodes + 255) / 256, 256, 0, s>>>(F, c->nd.p, c->nforce.p, c->fem_nodes.p, c->n_fem_nodes, c->fslot.p, c->info.p,
                                                                        c->dbodies.p, dt);
@@ -960,6 +1016,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->pcg_max_iters = 200;
     cfg->pcg_tol = 1e-6f;
     cfg->fem_check_residual = 0;
+    cfg->pcg_learned_scale = 1;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -984,7 +1041,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_config c0;
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
-    if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 2 || c0.pcg_max_iters < 0 ||
+    if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 3 || c0.pcg_max_iters < 0 ||
         !(c0.pcg_tol > 0))
         return BL_GPU_EINVAL;
     int ndev = 0;
@@ -1007,6 +1064,16 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     c->last_stream = c->stream;
     if ((e = cudaMemcpyToSymbol(c_ground, kGroundModels, sizeof(kGroundModels))) != cudaSuccess) return fail(e);
     if ((e = c->deverr.alloc(1)) != cudaSuccess) return fail(e);
+    for (DevBuf<float>* d : {&c->mlp_w, &c->mlp_m, &c->mlp_v, &c->gsum})
+        if ((e = d->alloc(kParams)) != cudaSuccess) return fail(e);
+    if ((e = c->mlp_wb.alloc(kParams)) != cudaSuccess) return fail(e);
+    if ((e = c->scount.alloc(1)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->scount.p, 0, sizeof(int))) != cudaSuccess) return fail(e);
+    if (bl_gpu_mlp_init(c, 1) != BL_GPU_OK) {
+        const int rc0 = c->last_cuda;
+        delete c;
+        return rc0 == cudaErrorMemoryAllocation ? BL_GPU_ENOMEM : BL_GPU_ECUDA;
+    }
     if ((e = cudaMemset(c->deverr.p, 0, sizeof(uint32_t))) != cudaSuccess) return fail(e);
     *out = c;
     return BL_GPU_OK;
@@ -1299,6 +1366,168 @@ int bl_gpu_stats(bl_gpu_ctx* c, bl_world_stats* out) {
         for (int i = 0; i < (int)recs.size(); i++) out->islands += (recs[i].pairs && recs[i].island == i) ? 1 : 0;
     }
     return BL_GPU_OK;
+}
+
+// ---- the learned warm start's network (bl_mlp.cuh)
+static int mlp_upload(bl_gpu_ctx* c, const float* w) {
+    BL_CUDA(c, cudaMemcpy(c->mlp_w.p, w, sizeof(float) * kParams, cudaMemcpyHostToDevice));
+    BL_CUDA(c, cudaMemset(c->mlp_m.p, 0, sizeof(float) * kParams));
+    BL_CUDA(c, cudaMemset(c->mlp_v.p, 0, sizeof(float) * kParams));
+    k_mlp_sync_bf16<<<(kParams + 255) / 256, 256, 0, c->stream>>>(mlp_dev(c));
+    BL_CUDA(c, cudaGetLastError());
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->adam_t = 0;
+    return BL_GPU_OK;
+}
+
+int bl_gpu_mlp_init(bl_gpu_ctx* c, uint64_t seed) {
+    if (!c) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    // uniform in +-sqrt(6 / fan_in) (He), biases zero; the last layer 10x smaller (the guess starts near sl(dv) = 0)
+    std::vector<float> w(kParams, 0.0f);
+    uint64_t x = seed * 0x9E3779B97F4A7C15ull + 1;
+    auto uni = [&]() {
+        x ^= x << 13, x ^= x >> 7, x ^= x << 17;
+        return (float)((x >> 11) * (1.0 / 9007199254740992.0));
+    };
+    auto fill = [&](int off, int nout, int nin, float gain) {
+        const float a = gain * std::sqrt(6.0f / (float)nin);
+        for (int q = 0; q < nout * nin; q++) w[off + q] = (2.0f * uni() - 1.0f) * a;
+    };
+    fill(kOffW1, kHid, kIn, 1.0f), fill(kOffW2, kHid, kHid, 1.0f), fill(kOffW3, kHid, kHid, 1.0f), fill(kOffW4, kOut, kHid, 0.1f);
+    return mlp_upload(c, w.data());
+}
+
+int bl_gpu_mlp_set_weights(bl_gpu_ctx* c, const float* w, int32_t n) {
+    if (!c || !w || n != kParams) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    return mlp_upload(c, w);
+}
+
+int bl_gpu_mlp_get_weights(bl_gpu_ctx* c, float* w, int32_t n) {
+    if (!c || !w || n != kParams) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    BL_CUDA(c, cudaDeviceSynchronize());
+    BL_CUDA(c, cudaMemcpy(w, c->mlp_w.p, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
+    return BL_GPU_OK;
+}
+
+int bl_gpu_mlp_record(bl_gpu_ctx* c, int32_t capacity) {
+    if (!c || capacity < 0) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    BL_CUDA(c, cudaDeviceSynchronize());
+    if (capacity == 0) {
+        c->rec_on = false;
+    } else {
+        BL_CUDA(c, c->smp_x.alloc((size_t)kIn * capacity));
+        BL_CUDA(c, c->smp_t.alloc((size_t)kOut * capacity));
+        BL_CUDA(c, c->smp_w.alloc((size_t)kOut * capacity));
+        BL_CUDA(c, cudaMemset(c->scount.p, 0, sizeof(int)));
+        c->rec_cap = capacity, c->rec_on = true;
+    }
+    drop_graphs(c); // (the frames are captured again with or without the recording kernels)
+    return BL_GPU_OK;
+}
+
+int bl_gpu_mlp_samples(bl_gpu_ctx* c, int32_t* n) {
+    if (!c || !n) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    BL_CUDA(c, cudaDeviceSynchronize());
+    int k = 0;
+    BL_CUDA(c, cudaMemcpy(&k, c->scount.p, sizeof(int), cudaMemcpyDeviceToHost));
+    *n = std::min(k, c->rec_cap);
+    return BL_GPU_OK;
+}
+
+// one pass of k_mlp_grad over n samples (x, t, w on the device; idx: the samples, or null) and, with lr > 0, Adam
+static int mlp_batch(bl_gpu_ctx* c, const float* x, const float* t, const float* w, const int* idx, int n, float lr, float* gsum, double* acc) {
+    const int nblk = (n + kLanes - 1) / kLanes;
+    if (c->gpart.n < (size_t)nblk * kParams) BL_CUDA(c, c->gpart.alloc((size_t)nblk * kParams));
+    if (c->lpart.n < (size_t)nblk) BL_CUDA(c, c->lpart.alloc(nblk));
+    const MlpDev M = mlp_dev(c);
+    k_mlp_grad<<<nblk, kLanes, 0, c->stream>>>(M, x, t, w, idx, n, c->gpart.p, c->lpart.p);
+    if (lr > 0) c->adam_t++;
+    k_mlp_adam<<<(kParams + 255) / 256, 256, 0, c->stream>>>(M, c->gpart.p, nblk, gsum, lr, 0.9f, 0.999f, 1e-8f, std::max(c->adam_t, 1));
+    if (acc) k_loss_acc<<<1, 32, 0, c->stream>>>(c->lpart.p, nblk, acc);
+    BL_CUDA(c, cudaGetLastError());
+    return BL_GPU_OK;
+}
+
+int bl_gpu_mlp_train(bl_gpu_ctx* c, int32_t epochs, int32_t batch, float lr, uint64_t seed, float* loss) {
+    if (!c || epochs < 0 || batch < 1 || !(lr > 0)) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    BL_CUDA(c, cudaDeviceSynchronize());
+    int n = 0;
+    int rc = bl_gpu_mlp_samples(c, &n);
+    if (rc) return rc;
+    if (n == 0) return BL_GPU_ESTATE;
+    BL_CUDA(c, c->sidx.alloc(n));
+    DevBuf<double> acc;
+    BL_CUDA(c, acc.alloc(1));
+    std::vector<int> order(n);
+    uint64_t x = seed * 0x9E3779B97F4A7C15ull + 7;
+    auto next = [&]() {
+        x ^= x << 13, x ^= x >> 7, x ^= x << 17;
+        return x;
+    };
+    for (int e = 0; e < epochs; e++) {
+        for (int i = 0; i < n; i++) order[i] = i;
+        for (int i = n - 1; i > 0; i--) std::swap(order[i], order[(int)(next() % (uint64_t)(i + 1))]);
+        BL_CUDA(c, cudaMemcpyAsync(c->sidx.p, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+        BL_CUDA(c, cudaMemsetAsync(acc.p, 0, sizeof(double), c->stream));
+        for (int b0 = 0; b0 < n; b0 += batch)
+            if ((rc = mlp_batch(c, c->smp_x.p, c->smp_t.p, c->smp_w.p, c->sidx.p + b0, std::min(batch, n - b0), lr, nullptr, acc.p))) {
+                acc.free_();
+                return rc;
+            }
+        BL_CUDA(c, cudaStreamSynchronize(c->stream)); // (the next epoch's order overwrites sidx)
+    }
+    double a = 0;
+    BL_CUDA(c, cudaMemcpy(&a, acc.p, sizeof(double), cudaMemcpyDeviceToHost));
+    acc.free_();
+    if (loss) *loss = (float)(a / n);
+    return BL_GPU_OK;
+}
+
+int bl_gpu_mlp_forward(bl_gpu_ctx* c, const float* x, int32_t n, float* y) {
+    if (!c || n < 0 || (n > 0 && (!x || !y))) return BL_GPU_EINVAL;
+    if (n == 0) return BL_GPU_OK;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    DevBuf<float> dx, dy;
+    BL_CUDA(c, dx.alloc((size_t)kIn * n));
+    BL_CUDA(c, dy.alloc((size_t)kOut * n));
+    BL_CUDA(c, cudaMemcpy(dx.p, x, sizeof(float) * kIn * n, cudaMemcpyHostToDevice));
+    k_mlp_forward_batch<<<(n + kLanes - 1) / kLanes, kLanes, 0, c->stream>>>(mlp_dev(c), dx.p, n, dy.p);
+    BL_CUDA(c, cudaGetLastError());
+    BL_CUDA(c, cudaStreamSynchronize(c->stream));
+    BL_CUDA(c, cudaMemcpy(y, dy.p, sizeof(float) * kOut * n, cudaMemcpyDeviceToHost));
+    dx.free_(), dy.free_();
+    return BL_GPU_OK;
+}
+
+int bl_gpu_mlp_gradient(bl_gpu_ctx* c, const float* x, const float* t, const float* w, int32_t n, float* grad, float* loss) {
+    if (!c || n < 1 || !x || !t || !w || !grad) return BL_GPU_EINVAL;
+    BL_CUDA(c, cudaSetDevice(c->cfg.device));
+    DevBuf<float> dx, dt, dw;
+    DevBuf<double> acc;
+    BL_CUDA(c, dx.alloc((size_t)kIn * n));
+    BL_CUDA(c, dt.alloc((size_t)kOut * n));
+    BL_CUDA(c, dw.alloc((size_t)kOut * n));
+    BL_CUDA(c, acc.alloc(1));
+    BL_CUDA(c, cudaMemcpy(dx.p, x, sizeof(float) * kIn * n, cudaMemcpyHostToDevice));
+    BL_CUDA(c, cudaMemcpy(dt.p, t, sizeof(float) * kOut * n, cudaMemcpyHostToDevice));
+    BL_CUDA(c, cudaMemcpy(dw.p, w, sizeof(float) * kOut * n, cudaMemcpyHostToDevice));
+    BL_CUDA(c, cudaMemset(acc.p, 0, sizeof(double)));
+    int rc = mlp_batch(c, dx.p, dt.p, dw.p, nullptr, n, 0.0f, c->gsum.p, acc.p);
+    if (!rc) {
+        BL_CUDA(c, cudaStreamSynchronize(c->stream));
+        BL_CUDA(c, cudaMemcpy(grad, c->gsum.p, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
+        double a = 0;
+        BL_CUDA(c, cudaMemcpy(&a, acc.p, sizeof(double), cudaMemcpyDeviceToHost));
+        if (loss) *loss = (float)(a / n);
+    }
+    dx.free_(), dt.free_(), dw.free_(), acc.free_();
+    return rc;
 }
 
 int bl_gpu_fem_stats(bl_gpu_ctx* c, bl_fem_stats* out) {

@@ -62,11 +62,12 @@ class WorldSettings:
     collision_hz: float = 120.0
     inter_body_collisions: bool = True
     # the FEM frames' implicit step (no counterpart in the reference, which always factors): "cholesky", "pcg",
-    # "pcg_learned"; a PCG solve that misses pcg_tol within pcg_max_iters falls back to the Cholesky
+    # "pcg_learned", "pcg_previous"; a PCG solve that misses pcg_tol within pcg_max_iters falls back to the Cholesky
     fem_solver: str = "cholesky"
     pcg_max_iters: int = 200
     pcg_tol: float = 1e-6
     fem_check_residual: bool = False
+    pcg_learned_scale: bool = True
 
 
 @dataclass
@@ -308,7 +309,7 @@ class _Config(C.Structure):
                 ("sleep_time", C.c_float), ("device", C.c_int32), ("deterministic", C.c_int32),
                 ("collision_hz", C.c_float), ("inter_body_collisions", C.c_int32), ("max_pairs", C.c_int32),
                 ("fem_solver", C.c_int32), ("pcg_max_iters", C.c_int32), ("pcg_tol", C.c_float),
-                ("fem_check_residual", C.c_int32)]
+                ("fem_check_residual", C.c_int32), ("pcg_learned_scale", C.c_int32)]
 
 
 class _FemStats(C.Structure):
@@ -317,7 +318,7 @@ class _FemStats(C.Structure):
                 ("max_residual", C.c_double), ("last_residual", C.c_double)]
 
 
-FEM_SOLVERS = {"cholesky": 0, "pcg": 1, "pcg_learned": 2}
+FEM_SOLVERS = {"cholesky": 0, "pcg": 1, "pcg_learned": 2, "pcg_previous": 3}
 
 
 class BodyHandle:
@@ -397,6 +398,7 @@ class World:
         cfg.pcg_max_iters = int(self.settings.pcg_max_iters)
         cfg.pcg_tol = float(self.settings.pcg_tol)
         cfg.fem_check_residual = int(self.settings.fem_check_residual)
+        cfg.pcg_learned_scale = int(self.settings.pcg_learned_scale)
         self._ctx = C.c_void_p()
         _check(self._L.bl_gpu_create(C.byref(cfg), C.byref(self._ctx)), "create")
         self._bodies: list[BodyHandle] = []
@@ -548,6 +550,54 @@ class World:
         s = _FemStats()
         _check(self._L.bl_gpu_fem_stats(self._ctx, C.byref(s)), "fem_stats", self._ctx)
         return {k: getattr(s, k) for k, _ in _FemStats._fields_ if k != "pad"}
+
+    # ---- the learned warm start's network (include/beamlab_gpu.h: bl_gpu_mlp_*)
+    MLP_PARAMS, MLP_INPUTS, MLP_OUTPUTS = 11468, 36, 12
+
+    def mlp_init(self, seed: int = 1):
+        _check(self._L.bl_gpu_mlp_init(self._ctx, int(seed)), "mlp_init", self._ctx)
+
+    def mlp_weights(self) -> np.ndarray:
+        w = np.zeros(self.MLP_PARAMS, np.float32)
+        _check(self._L.bl_gpu_mlp_get_weights(self._ctx, w.ctypes.data, len(w)), "mlp_get_weights", self._ctx)
+        return w
+
+    def set_mlp_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32)
+        _check(self._L.bl_gpu_mlp_set_weights(self._ctx, w.ctypes.data, len(w)), "mlp_set_weights", self._ctx)
+
+    def mlp_record(self, capacity: int):
+        """Record one training sample per frame node and substep into a ring of `capacity` (0: stop recording)."""
+        self._send_statics()
+        _check(self._L.bl_gpu_mlp_record(self._ctx, int(capacity)), "mlp_record", self._ctx)
+
+    def mlp_samples(self) -> int:
+        n = C.c_int32()
+        _check(self._L.bl_gpu_mlp_samples(self._ctx, C.byref(n)), "mlp_samples", self._ctx)
+        return n.value
+
+    def mlp_train(self, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 1) -> float:
+        loss = C.c_float()
+        _check(self._L.bl_gpu_mlp_train(self._ctx, int(epochs), int(batch), float(lr), int(seed), C.byref(loss)),
+               "mlp_train", self._ctx)
+        return loss.value
+
+    def mlp_forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.MLP_INPUTS)
+        y = np.zeros((len(x), self.MLP_OUTPUTS), np.float32)
+        _check(self._L.bl_gpu_mlp_forward(self._ctx, x.ctypes.data, len(x), y.ctypes.data), "mlp_forward", self._ctx)
+        return y
+
+    def mlp_gradient(self, x: np.ndarray, t: np.ndarray, w: np.ndarray):
+        """(gradient, loss) of sum_s sum_o w (y - t)^2 / (2 n) over the n samples."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.MLP_INPUTS)
+        t = np.ascontiguousarray(t, np.float32).reshape(-1, self.MLP_OUTPUTS)
+        w = np.ascontiguousarray(w, np.float32).reshape(-1, self.MLP_OUTPUTS)
+        g = np.zeros(self.MLP_PARAMS, np.float32)
+        loss = C.c_float()
+        _check(self._L.bl_gpu_mlp_gradient(self._ctx, x.ctypes.data, t.ctypes.data, w.ctypes.data, len(x), g.ctypes.data,
+                                           C.byref(loss)), "mlp_gradient", self._ctx)
+        return g, loss.value
 
     def pairs(self) -> np.ndarray:
         """The contact pairs of the last pair search, island after island, each in the reference's order: rows of

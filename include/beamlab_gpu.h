@@ -69,16 +69,19 @@ typedef struct {
                                   search raise BL_GPU_DEVERR_PAIRS and that island's contacts are skipped */
     /* the FEM frames' implicit step (no counterpart in the reference, which always factors): */
     int32_t fem_solver;        /* BL_GPU_FEM_CHOLESKY (default: the reference's block Cholesky), BL_GPU_FEM_PCG (conjugate
-                                  gradients, block-Jacobi, from zero), BL_GPU_FEM_PCG_LEARNED (from the learned per-node
-                                  guess, the preconditioner scaled by the learned 3x3 blocks); a PCG solve that misses
-                                  pcg_tol within pcg_max_iters falls back to the Cholesky for that substep */
+                                  gradients, block-Jacobi, from zero), BL_GPU_FEM_PCG_LEARNED (from the energy-norm best
+                                  combination of the learned per-node guess and the last solution, the preconditioner
+                                  scaled by the learned 3x3 blocks), BL_GPU_FEM_PCG_PREVIOUS (from the last solution,
+                                  scaled alike: the warm start without the network); a PCG solve that misses pcg_tol
+                                  within pcg_max_iters falls back to the Cholesky for that substep */
     int32_t pcg_max_iters;     /* default 200 */
     float pcg_tol;             /* relative residual |A dv - rhs| / |rhs| to reach; default 1e-6 */
     int32_t fem_check_residual; /* 1: keep a copy of each assembled system and measure the residual of the solution the
                                    step took (bl_gpu_fem_stats); costs a copy of the system a substep */
+    int32_t pcg_learned_scale; /* BL_GPU_FEM_PCG_LEARNED: 1 (default) the learned 3x3 scale of the preconditioner, 0 none */
 } bl_gpu_config;
 
-enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2 };
+enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };
 
 /* == bl::phys::Node (softbody.h:43-48): 32 bytes */
 typedef struct {
@@ -291,6 +294,31 @@ typedef struct {
     double last_residual;      /* fem_check_residual: that of the last substep */
 } bl_fem_stats;
 int bl_gpu_fem_stats(bl_gpu_ctx* ctx, bl_fem_stats* out);
+
+/* The learned warm start (BL_GPU_FEM_PCG_LEARNED; no counterpart in the reference): a per-frame-node MLP
+ * 36 -> 64 -> 64 -> 64 -> 12 (ReLU), BF16 weights with FP32 accumulation, whose outputs are the PCG's initial dv guess
+ * (3) and a 3 x 3 scale of its block preconditioner's translational part (9). Its features and targets are described
+ * in beamlab_b200/csrc/bl_mlp.cuh. Parameters: one float vector of BL_GPU_MLP_PARAMS - W1 (64 x 36, row = output), b1,
+ * W2 (64 x 64), b2, W3 (64 x 64), b3, W4 (12 x 64), b4. Every context starts with the weights of seed 1. */
+#define BL_GPU_MLP_PARAMS 11468
+#define BL_GPU_MLP_INPUTS 36
+#define BL_GPU_MLP_OUTPUTS 12
+int bl_gpu_mlp_init(bl_gpu_ctx* ctx, uint64_t seed);                    /* He-uniform weights, zero biases */
+int bl_gpu_mlp_set_weights(bl_gpu_ctx* ctx, const float* w, int32_t n); /* n == BL_GPU_MLP_PARAMS; resets Adam */
+int bl_gpu_mlp_get_weights(bl_gpu_ctx* ctx, float* w, int32_t n);
+/* capacity > 0: from the next frame on, every substep's solve records one training sample per frame node (features,
+ * targets from the solution the step took) into a ring of `capacity` samples (older ones are overwritten);
+ * capacity 0: stop recording (the samples stay for bl_gpu_mlp_train). The frames' graphs are captured again. */
+int bl_gpu_mlp_record(bl_gpu_ctx* ctx, int32_t capacity);
+int bl_gpu_mlp_samples(bl_gpu_ctx* ctx, int32_t* n);
+/* Adam (beta 0.9 / 0.999) on the recorded samples, shuffled each epoch (seeded), minibatches of `batch`; *loss: the
+ * mean sample loss over the last epoch. Synchronous. */
+int bl_gpu_mlp_train(bl_gpu_ctx* ctx, int32_t epochs, int32_t batch, float lr, uint64_t seed, float* loss);
+/* The network on n samples (x: n x 36, y: n x 12; host memory), and the gradient of the loss
+ * sum_s sum_o w_so (y_so - t_so)^2 / (2 n) over n samples with respect to the parameters (the BF16 values the
+ * forward uses), and that loss. Synchronous; for checks against a CPU restatement. */
+int bl_gpu_mlp_forward(bl_gpu_ctx* ctx, const float* x, int32_t n, float* y);
+int bl_gpu_mlp_gradient(bl_gpu_ctx* ctx, const float* x, const float* t, const float* w, int32_t n, float* grad, float* loss);
 
 /* The contact pairs (node, triangle) of the last pair search, island after island (islands in the order of their
  * first body, each island's pairs in the reference's order: World::Island::nt after rebuild_pairs + near_pairs,
