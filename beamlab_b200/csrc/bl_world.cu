@@ -1016,7 +1016,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->pcg_max_iters = 200;
     cfg->pcg_tol = 1e-6f;
     cfg->fem_check_residual = 0;
-    cfg->pcg_learned_scale = 1;
+    cfg->pcg_learned_scale = 0;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }

@@ -67,7 +67,7 @@ class WorldSettings:
     pcg_max_iters: int = 200
     pcg_tol: float = 1e-6
     fem_check_residual: bool = False
-    pcg_learned_scale: bool = True
+    pcg_learned_scale: bool = False
 
 
 @dataclass

@@ -78,7 +78,8 @@ typedef struct {
     float pcg_tol;             /* relative residual |A dv - rhs| / |rhs| to reach; default 1e-6 */
     int32_t fem_check_residual; /* 1: keep a copy of each assembled system and measure the residual of the solution the
                                    step took (bl_gpu_fem_stats); costs a copy of the system a substep */
-    int32_t pcg_learned_scale; /* BL_GPU_FEM_PCG_LEARNED: 1 (default) the learned 3x3 scale of the preconditioner, 0 none */
+    int32_t pcg_learned_scale; /* BL_GPU_FEM_PCG_LEARNED: 1 the learned 3x3 scale of the block preconditioner, 0 (default)
+                                  none - measured on the plates, the scale as trained costs iterations */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };
