@@ -159,6 +159,42 @@ def cpu_reference(rig, n_nodes, budget_s=10.0, max_frames=100, warm=4):
                       f"({frames * FRAME} substeps, {dt:.2f} s)"}
 
 
+def fem_solvers(device: int, frames: int = 2):
+    """The plate's implicit step by each solver (include/beamlab_gpu.h: fem_solver), on a load the network was not
+    trained on: ms a substep (CUDA events of a profiled frame), CG iterations a solve, fallbacks, the largest relative
+    residual of a solution the step took. The network is trained first on 200 substeps of the Cholesky's solves of
+    another load (seed 1; 12 epochs of Adam)."""
+    from beamlab_b200 import rigs, world_from_rig
+    rec = world_from_rig(rigs.shell_plate(63, seed=1), device=device)
+    rec.mlp_record(200 * 4096)
+    for _ in range(10):
+        rec.step_substeps(20)
+    rec.mlp_record(0)
+    t0 = time.perf_counter()
+    rec.mlp_train(1, batch=4096, lr=2e-3, seed=0)
+    loss = rec.mlp_train(12, batch=4096, lr=1e-3, seed=1)
+    train_s = time.perf_counter() - t0
+    weights = rec.mlp_weights()
+    rec.close()
+    out = {"load": "shell_plate(63, seed=2)", "training": {"samples": 200 * 4096, "epochs": 13, "loss": loss,
+                                                           "seconds": train_s}}
+    for solver in ("cholesky", "pcg", "pcg_previous", "pcg_learned"):
+        w = world_from_rig(rigs.shell_plate(63, seed=2), device=device, fem_solver=solver, pcg_max_iters=3000,
+                           fem_check_residual=True)
+        if solver == "pcg_learned":
+            w.set_mlp_weights(weights)
+        w.step_substeps(FRAME)  # (warm-up: the graph is captured)
+        ms = 0.0
+        for _ in range(frames):
+            ms += w.profile_frame(FRAME)["frame_ms"]
+        st = w.fem_stats()
+        out[solver] = {"ms_per_substep": ms / (frames * FRAME), "max_residual": st["max_residual"],
+                       "cg_iterations_per_solve": st["pcg_iterations"] / st["pcg_solves"] if st["pcg_solves"] else None,
+                       "fallbacks": st["pcg_fallbacks"]}
+        w.close()
+    return out
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -304,6 +340,8 @@ def run_gpu(args):
                          "algorithmic_bytes_per_launch": alg_bytes, "traffic": traffic},
             "clocks": clk,
         }
+        if ws == 1 and args.workload == "plate64":
+            out["fem_solvers"] = fem_solvers(local)
         if ws == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_reference(rig, n)
         print(json.dumps(out), flush=True)
