@@ -10,9 +10,8 @@
 // Layout. Collision triangles of all bodies back to back: int4 (a, b, c as global node indices; flags: bit 0 two-sided,
 // bit 1 torn, bits 8.. the body) and their longest rest edge squared. Each frame k_islands labels every body with the
 // first body of its island (the reference numbers islands in that order and keeps each island's bodies in body
-// order). An island with two or more bodies has contact pairs: its bodies' nodes are "split" - k_nodes phase 0 stores
-// their gravity + beam forces in `fsplit`, the contacts add to those, and k_nodes phase 1 finishes them (static
-// contact, integration) - while every other body keeps the fused node kernel.
+// order). An island with two or more bodies has contact pairs: the contacts add to its nodes' forces (fnode: gravity
+// and beams, k_force) before k_integrate takes the static contacts and integrates.
 //
 // The pair search runs on the substeps the reference rebuilds on (the frame's first and every rebuild interval after):
 // one CTA per island (k_rebuild) makes the island's margins and cell size, the partners, the spatial hash of the slow
@@ -63,7 +62,6 @@ struct Contacts {
     int* g_start;              // fast grids (kGridCells + 1 per island)
     int* g_fill;
     int* g_items;              // fast grids' nodes, each listed once, in the lowest cell of its travel
-    float4* fsplit;            // per node: the force before the contacts (bodies of islands with pairs)
     int* counters;             // [0] pair searches [1] contacts [2] pairs of the searches
     int interval;              // rebuild interval in substeps (world.cpp:1887)
     float dt;
@@ -912,8 +910,10 @@ __global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, c
 
 // ------------------------------------------------------------------------------------------ response (each substep)
 // World::collide_pairs for node-triangle pairs (world.cpp:2975-3023): one thread an island, its pairs in order;
-// contact_force<1, 3> and hull_push_out<3> (world.cpp:59-120) on the forces in fsplit; the concrete ground model.
-__global__ void k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, int nbodies, Contacts C) {
+// contact_force<1, 3> and hull_push_out<3> (world.cpp:59-120) on the nodes' forces so far (Fs); the concrete ground
+// model.
+__global__ void k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, int nbodies, Contacts C,
+                          float4* __restrict__ Fs) {
     const int root = blockIdx.x * blockDim.x + threadIdx.x;
     if (root >= nbodies) return;
     const int cnt = C.isl_pcnt[root];
@@ -921,7 +921,6 @@ __global__ void k_collide(const float4* __restrict__ nd, const int4* __restrict_
     const int off = C.isl_poff[root];
     const float dt = C.dt;
     const GroundModel& gm = c_ground[3]; // SURF_CONCRETE
-    float4* Fs = C.fsplit;
     int contacts = 0;
     for (int i = off; i < off + cnt; i++) {
         const float4 hb4 = C.hit_b[i];

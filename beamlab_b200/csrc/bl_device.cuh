@@ -16,6 +16,8 @@ namespace blg {
 constexpr int kMaxCand = 64;               // BL_GPU_MAX_CANDIDATES
 constexpr uint32_t kBeamAsleep = 1u << 31; // Beam meta: the beam's body sleeps (not stepped)
 constexpr float kMaxNodeSpeed = 400.0f;    // softbody.h:153
+// a beam's force scalar when it does not push this substep (a NaN no arithmetic makes: the GPU's NaNs are 0x7fffffff)
+#define kNoPush __uint_as_float(0x7fc0beefu)
 constexpr int kSurfCount = 11;
 
 enum : uint32_t { NF_GROUND = 1, NF_FIXED = 2, NF_TYRE = 4, NF_RIM = 8, NF_CONTACTER = 16 };

@@ -4,7 +4,7 @@
 //   k_fem_begin        frame nodes: double positions re-synced where something else moved a node (frame_fem.cpp:1866-1872)
 //   k_tri_eval         triangles: co-rotated frame, deformation, -K d, K v, membrane tension's geometric stiffness
 //                      (tri_kinematics + eval_tris, frame_fem.cpp:1584-1621, 1661-1831; elastic sections)
-//   (k_nodes)          the frame bodies' node forces, their triangles' forces and torques gathered in the reference's
+//   (k_force)          the frame bodies' node forces, their triangles' forces and torques gathered in the reference's
 //                      order (gather_forces, frame_fem.cpp:2080-2105)
 //   k_fem_assemble     columns: the blocks of (M + (theta h^2 + beta h) K + theta h^2 Kg) and the right side
 //                      h f - (theta_d h^2 + beta h) K v (gather_part, frame_fem.cpp:916-1086)

@@ -1,15 +1,17 @@
 // Kernels of the explicit substep. Per frame (World::step_substeps, world.cpp:368-585):
 //
-//   k_frame_begin   one thread per body: static candidates over the box grown by its travel, terrain height bound
-//   n x { k_beams   one thread per beam: spring-damper, plastic yield, break -> the beam's force (scratch fv)
-//         k_nodes } one thread per node: gravity + its beams' forces in beam order, static contact, integration,
-//                   bounds / top speed / contacts reduced per body
-//   k_frame_finish  one block: each body's bounds, top speed, repair of runaway nodes, sleep
-//   k_sleep_apply   one block per body: a body that fell asleep stops (velocities zero, beams parked)
+//   k_frame_begin     one thread per body: static candidates over the box grown by its travel, terrain height bound
+//   n x { k_beams     one thread per beam: spring-damper, plastic yield, break -> the beam's force scalar (fsc)
+//         k_force     one thread per node: gravity + its beams' forces in beam order (each made again from the scalar
+//                     and the two positions) -> the node's force
+//         (contacts between bodies add to the force: bl_contacts.cuh)
+//         k_integrate } one thread per node: static contact, integration, bounds / top speed / contacts per body
+//   k_frame_finish    one block: each body's bounds, top speed, repair of runaway nodes, sleep
+//   k_sleep_apply     one block per body: a body that fell asleep stops (velocities zero, beams parked)
 //
-// Determinism: k_nodes sums a node's forces in the order the reference's serial loop adds them (gravity, then each
+// Determinism: k_force sums a node's forces in the order the reference's serial loop adds them (gravity, then each
 // beam in index order: f[a] += fv, f[b] -= fv; softbody.cpp:330-470), from a per-node list of incident beams sorted
-// by beam index, so no atomics touch a force.
+// by beam index, so no atomics touch a force; fv = (p_a - p_b) * scalar rounds exactly as the reference's product.
 #pragma once
 
 #include "bl_device.cuh"
@@ -248,11 +250,12 @@ __global__ void k_frame_begin(Body* __restrict__ bodies, int nbodies, Statics st
 }
 
 // ------------------------------------------------------------------------------------------ per substep
-// SoftBody::compute_beam_forces, one beam (softbody.cpp:412-470). fv.w = 1 when the beam pushes on its nodes this
-// substep. Thread j < nbodies also resets body j's bounds accumulator for this substep's k_nodes.
+// SoftBody::compute_beam_forces, one beam (softbody.cpp:412-470). The beam's force on its end a is dis * fsc[j]
+// (dis = p_a - p_b), on b its negative; fsc[j] = kNoPush when the beam does not push this substep. Thread j < nbodies
+// also resets body j's bounds accumulator for this substep's k_integrate.
 __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
                                                uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
-                                               const int* __restrict__ bbody, float4* __restrict__ fv, const float4* __restrict__ nd,
+                                               const int* __restrict__ bbody, float* __restrict__ fsc, const float4* __restrict__ nd,
                                                Body* __restrict__ bodies, int nbeams, int nbodies) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < nbodies) {
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
     if (j >= nbeams) return;
     uint32_t meta = bmeta[j];
     if (meta & kBeamAsleep) return;
-    float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float out = kNoPush;
     const uint32_t type = meta & 0xffu;
     uint32_t flags = (meta >> 8) & 0xffu;
     if (!(flags & (BF_BROKEN | BF_SHOCK))) {
@@ -319,8 +322,7 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
                     broke = true;
                 } else {
                     stress[j] = slen;
-                    const float sc = slen * inv_len;
-                    out = make_float4(dis.x * sc, dis.y * sc, dis.z * sc, 1.0f);
+                    out = slen * inv_len; // (the force on a is dis * out: k_force makes dis again from the same positions)
                 }
             }
             if (broke) {
@@ -330,15 +332,10 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
             }
         }
     }
-    fv[j] = out;
+    fsc[j] = out;
 }
 
-// Gravity (and any constant node force) + the node's beams in beam order, World::collide_static for the node
-// (world.cpp:781-870), then SoftBody::integrate_nodes (softbody.cpp:769-795). first: the frame's first substep (the top
-// speed starts from the velocities before it, world.cpp:3217-3222).
-// Frame bodies (Body::is_fem) stop after their forces: the triangles' forces and torques are gathered onto the frame
-// nodes in the reference's order (gather_forces, frame_fem.cpp:2080-2105) and the node's force is kept in nforce for
-// the frame's implicit step (their nodes do not touch the static world).
+// The frame bodies' gather (NodeFem): their nodes' forces go to the frame's implicit step
 struct NodeFem {
     const int* fslot;        // node -> frame node (-1: none)
     const int* iperm;        // frame node -> column
@@ -352,146 +349,10 @@ struct NodeFem {
     const float4* ext;       // constant node forces (bl_gpu_set_node_force)
 };
 
-// phase 0: every body; the bodies of islands with contact pairs (Body::pairs) only keep their force in fsplit.
-// phase 1: those bodies alone, after the contacts added to fsplit: static contact and integration.
-__global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const int4* __restrict__ info,
-                                               const int* __restrict__ inc_ptr, const int* __restrict__ inc, const float4* __restrict__ fv,
-                                               Body* __restrict__ bodies, Statics st, float gx, float gy, float gz, float dt, int nnodes, int first,
-                                               NodeFem nf, int phase, float4* __restrict__ fsplit) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// the bounds, top speed and static contacts of a warp's nodes into their bodies' accumulators (a warp of one body
+// reduces first)
+__device__ __forceinline__ void accumulate_bounds(Body* __restrict__ bodies, int body, bool live, v3 p, v3 pmx, float v2, int contact) {
     const int lane = threadIdx.x & 31;
-    int body = -1;
-    v3 p = V(1e30f, 1e30f, 1e30f), pmx = V(-1e30f, -1e30f, -1e30f);
-    float v2 = 0.0f, v2start = 0.0f;
-    int contact = 0;
-    bool live = false;
-    if (i < nnodes) {
-        const int4 inf = info[i];
-        body = inf.w;
-        const Body& B = bodies[body];
-        const bool split = B.pairs != 0;
-        if (!B.sleeping && (phase == 0 || split)) {
-            const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
-            const float m = Vv.w;
-            v3 f;
-            if (phase == 1) {
-                const float4 fs = fsplit[i];
-                f = V(fs.x, fs.y, fs.z);
-            } else {
-                f = V(gx * m, gy * m, gz * m); // clear_forces: g * mass (softbody.cpp:376)
-                if (B.has_ext) {               // (a controller's push, world.cpp:3261)
-                    const float4 e = nf.ext[i];
-                    f = V(f.x + e.x, f.y + e.y, f.z + e.z);
-                }
-                const int q1 = inc_ptr[i + 1];
-                for (int q = inc_ptr[i]; q < q1; q++) {
-                    const int e = inc[q];
-                    const float4 b = fv[e & 0x7fffffff];
-                    if (b.w != 0.0f) {
-                        if (e < 0) f = V(f.x - b.x, f.y - b.y, f.z - b.z);
-                        else f = V(f.x + b.x, f.y + b.y, f.z + b.z);
-                    }
-                }
-            }
-            live = !(phase == 0 && split);
-            if (!live) {
-                fsplit[i] = make_float4(f.x, f.y, f.z, 0.0f); // (the contacts between bodies come next: World::collide_pairs)
-            } else if (B.is_fem) {
-                if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
-                const int fs = nf.fslot[i];
-                if (fs >= 0) {
-                    const int k = nf.iperm[fs];
-                    v3 tq = V(0, 0, 0);
-                    for (int g = nf.gdiag_ptr[k]; g < nf.gdiag_ptr[k + 1]; g++) {
-                        const int2 e = nf.gdiag[g];
-                        if (!nf.ton[e.x]) continue;
-                        const float4 tf = nf.tf[3 * e.x + e.y], tt = nf.tt[3 * e.x + e.y];
-                        f = V(f.x + tf.x, f.y + tf.y, f.z + tf.z);
-                        tq = V(tq.x + tt.x, tq.y + tt.y, tq.z + tt.z);
-                    }
-                    nf.torque[fs] = make_float4(tq.x, tq.y, tq.z, 0.0f);
-                }
-                nf.nforce[i] = make_float4(f.x, f.y, f.z, 0.0f);
-                v2 = v2start; // (its bounds and speeds after the frame's step: k_fem_integrate)
-            } else {
-                if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
-                v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
-                float inv_mass = P.w;
-                const uint32_t flags = (uint32_t)inf.x;
-                // ---- static contact (World::collide_static)
-                if (!(!(flags & NF_GROUND) || inv_mass <= 0)) {
-                    if (pos.y < st.kill_y) {
-                        vel = V(0, 0, 0);
-                        inv_mass = 0;
-                    } else {
-                        const float r = __int_as_float(inf.z);
-                        const bool near_terrain = st.has_terrain && pos.y - r <= B.terrain_max + 0.05f;
-                        const int nbox = B.nbox, ncyl = B.ncyl;
-                        if (near_terrain || nbox != 0 || ncyl != 0) {
-                            int bids[16], cids[16];
-                            const int* bp = B.box_ids;
-                            const int* cp = B.cyl_ids;
-                            int nb = nbox, nc = ncyl;
-                            bool go = true;
-                            if (nbox <= 16 && ncyl <= 16) {
-                                nb = nc = 0;
-                                const float rr = r + 0.01f;
-                                for (int k = 0; k < nbox; k++) {
-                                    const Box& a = st.boxes[B.box_ids[k]];
-                                    if (pos.x >= a.mnx - rr && pos.x <= a.mxx + rr && pos.y >= a.mny - rr && pos.y <= a.mxy + rr && pos.z >= a.mnz - rr &&
-                                        pos.z <= a.mxz + rr)
-                                        bids[nb++] = B.box_ids[k];
-                                }
-                                for (int k = 0; k < ncyl; k++) {
-                                    const Cyl& cy = st.cyls[B.cyl_ids[k]];
-                                    const float cr = cy.radius + rr;
-                                    if (fabsf(pos.x - cy.bx) <= cr && fabsf(pos.z - cy.bz) <= cr && pos.y >= cy.by - rr && pos.y <= cy.by + cy.height + rr)
-                                        cids[nc++] = B.cyl_ids[k];
-                                }
-                                bp = bids;
-                                cp = cids;
-                                go = near_terrain || nb != 0 || nc != 0;
-                            }
-                            Contact c;
-                            if (go && collide_point(st, pos, r, bp, nb, cp, nc, near_terrain, c)) {
-                                contact = 1;
-                                const GroundModel& gm = c_ground[c.surface < kSurfCount ? c.surface : 0];
-                                const float fc = __int_as_float(inf.y) * B.fric;
-                                if (c.max_force > 0) {
-                                    v3 fcn = primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, -1.0f);
-                                    const float fl = length(fcn);
-                                    if (fl > c.max_force) fcn = fcn * (c.max_force / fl);
-                                    f = f + fcn;
-                                } else {
-                                    f = f + primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, B.bounce);
-                                }
-                            }
-                        }
-                    }
-                }
-                // ---- integration (SoftBody::integrate_nodes)
-                if (inv_mass > 0) {
-                    vel = vel + f * (inv_mass * dt);
-                    v2 = dot(vel, vel);
-                    if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
-                        vel = vel * (kMaxNodeSpeed / sqrtf(v2));
-                        v2 = kMaxNodeSpeed * kMaxNodeSpeed;
-                    } else if (!(v2 >= 0.0f)) {
-                        vel = V(0, 0, 0);
-                        v2 = 0;
-                    }
-                    pos = pos + vel * dt;
-                }
-                nd[2 * i] = make_float4(pos.x, pos.y, pos.z, inv_mass);
-                nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, m);
-                // the bounds skip a non-finite coordinate as the reference's vmin / vmax do (a NaN never compares less)
-                p = V(pos.x == pos.x ? pos.x : 1e30f, pos.y == pos.y ? pos.y : 1e30f, pos.z == pos.z ? pos.z : 1e30f);
-                pmx = V(pos.x == pos.x ? pos.x : -1e30f, pos.y == pos.y ? pos.y : -1e30f, pos.z == pos.z ? pos.z : -1e30f);
-                v2 = smax(v2, v2start);
-            }
-        }
-    }
-    // ---- per body: bounds, top speed, contacts (a warp of one body reduces first)
     const int b0 = __shfl_sync(0xffffffffu, body, 0);
     const bool uniform = __all_sync(0xffffffffu, body == b0 && live);
     if (uniform) {
@@ -521,6 +382,169 @@ __global__ void __launch_bounds__(256) k_nodes(float4* __restrict__ nd, const in
         atomic_max_f(&B.acc_v2, v2);
         if (contact) atomicAdd(&B.acc_contacts, contact);
     }
+}
+
+// A node's force: clear_forces' gravity (and any constant node force), then its beams in beam order
+// (softbody.cpp:376, 466-467); each beam's force made again from the beam's scalar and the two positions, as k_beams
+// made it. inc2: the node's incidences (beam | bit 31 when the node is the beam's b end, the other end). Into fnode
+// for World::collide_static and the integration (k_integrate) - the contacts between bodies add to it first.
+// Frame bodies (Body::is_fem): the triangles' forces and torques are gathered onto the frame nodes in the reference's
+// order (gather_forces, frame_fem.cpp:2080-2105) and the force is kept in nforce for the frame's implicit step.
+__global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ inc_ptr,
+                                               const int2* __restrict__ inc2, const float* __restrict__ fsc, Body* __restrict__ bodies, float gx,
+                                               float gy, float gz, int nnodes, int first, NodeFem nf, float4* __restrict__ fnode) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int body = -1;
+    float v2 = 0.0f;
+    bool live = false;
+    if (i < nnodes) {
+        body = info[i].w;
+        const Body& B = bodies[body];
+        if (!B.sleeping) {
+            const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
+            const float m = Vv.w;
+            v3 f = V(gx * m, gy * m, gz * m);
+            if (B.has_ext) {
+                const float4 e = nf.ext[i];
+                f = V(f.x + e.x, f.y + e.y, f.z + e.z);
+            }
+            const int q1 = inc_ptr[i + 1];
+            for (int q = inc_ptr[i]; q < q1; q++) {
+                const int2 e = inc2[q];
+                const float sc = fsc[e.x & 0x7fffffff];
+                if (__float_as_uint(sc) == __float_as_uint(kNoPush)) continue;
+                const float4 Po = nd[2 * e.y];
+                if (e.x < 0) { // (this node is the beam's b: dis = p_a - p_b, the force subtracted)
+                    const v3 dis = V(Po.x - P.x, Po.y - P.y, Po.z - P.z);
+                    f = V(f.x - dis.x * sc, f.y - dis.y * sc, f.z - dis.z * sc);
+                } else {
+                    const v3 dis = V(P.x - Po.x, P.y - Po.y, P.z - Po.z);
+                    f = V(f.x + dis.x * sc, f.y + dis.y * sc, f.z + dis.z * sc);
+                }
+            }
+            if (B.is_fem) {
+                live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)
+                if (first) v2 = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
+                const int fs = nf.fslot[i];
+                if (fs >= 0) {
+                    const int k = nf.iperm[fs];
+                    v3 tq = V(0, 0, 0);
+                    for (int g = nf.gdiag_ptr[k]; g < nf.gdiag_ptr[k + 1]; g++) {
+                        const int2 e = nf.gdiag[g];
+                        if (!nf.ton[e.x]) continue;
+                        const float4 tf = nf.tf[3 * e.x + e.y], tt = nf.tt[3 * e.x + e.y];
+                        f = V(f.x + tf.x, f.y + tf.y, f.z + tf.z);
+                        tq = V(tq.x + tt.x, tq.y + tt.y, tq.z + tt.z);
+                    }
+                    nf.torque[fs] = make_float4(tq.x, tq.y, tq.z, 0.0f);
+                }
+                nf.nforce[i] = make_float4(f.x, f.y, f.z, 0.0f);
+            } else {
+                fnode[i] = make_float4(f.x, f.y, f.z, 0.0f);
+            }
+        }
+    }
+    accumulate_bounds(bodies, body, live, V(1e30f, 1e30f, 1e30f), V(-1e30f, -1e30f, -1e30f), v2, 0);
+}
+
+// World::collide_static for the node (world.cpp:781-870), then SoftBody::integrate_nodes (softbody.cpp:769-795), on
+// the force in fnode (gravity, beams, contacts with other bodies). first: the frame's first substep (the top speed
+// starts from the velocities before it, world.cpp:3217-3222). Frame bodies' nodes are integrated after their solve.
+__global__ void __launch_bounds__(256) k_integrate(float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Statics st,
+                                                   float dt, int nnodes, int first, const float4* __restrict__ fnode) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int body = -1;
+    v3 p = V(1e30f, 1e30f, 1e30f), pmx = V(-1e30f, -1e30f, -1e30f);
+    float v2 = 0.0f, v2start = 0.0f;
+    int contact = 0;
+    bool live = false;
+    if (i < nnodes) {
+        const int4 inf = info[i];
+        body = inf.w;
+        const Body& B = bodies[body];
+        if (!B.sleeping && !B.is_fem) {
+            live = true;
+            const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
+            const float m = Vv.w;
+            const float4 f4 = fnode[i];
+            v3 f = V(f4.x, f4.y, f4.z);
+            if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
+            v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
+            float inv_mass = P.w;
+            const uint32_t flags = (uint32_t)inf.x;
+            // ---- static contact (World::collide_static)
+            if (!(!(flags & NF_GROUND) || inv_mass <= 0)) {
+                if (pos.y < st.kill_y) {
+                    vel = V(0, 0, 0);
+                    inv_mass = 0;
+                } else {
+                    const float r = __int_as_float(inf.z);
+                    const bool near_terrain = st.has_terrain && pos.y - r <= B.terrain_max + 0.05f;
+                    const int nbox = B.nbox, ncyl = B.ncyl;
+                    if (near_terrain || nbox != 0 || ncyl != 0) {
+                        int bids[16], cids[16];
+                        const int* bp = B.box_ids;
+                        const int* cp = B.cyl_ids;
+                        int nb = nbox, nc = ncyl;
+                        bool go = true;
+                        if (nbox <= 16 && ncyl <= 16) {
+                            nb = nc = 0;
+                            const float rr = r + 0.01f;
+                            for (int k = 0; k < nbox; k++) {
+                                const Box& a = st.boxes[B.box_ids[k]];
+                                if (pos.x >= a.mnx - rr && pos.x <= a.mxx + rr && pos.y >= a.mny - rr && pos.y <= a.mxy + rr && pos.z >= a.mnz - rr &&
+                                    pos.z <= a.mxz + rr)
+                                    bids[nb++] = B.box_ids[k];
+                            }
+                            for (int k = 0; k < ncyl; k++) {
+                                const Cyl& cy = st.cyls[B.cyl_ids[k]];
+                                const float cr = cy.radius + rr;
+                                if (fabsf(pos.x - cy.bx) <= cr && fabsf(pos.z - cy.bz) <= cr && pos.y >= cy.by - rr && pos.y <= cy.by + cy.height + rr)
+                                    cids[nc++] = B.cyl_ids[k];
+                            }
+                            bp = bids;
+                            cp = cids;
+                            go = near_terrain || nb != 0 || nc != 0;
+                        }
+                        Contact c;
+                        if (go && collide_point(st, pos, r, bp, nb, cp, nc, near_terrain, c)) {
+                            contact = 1;
+                            const GroundModel& gm = c_ground[c.surface < kSurfCount ? c.surface : 0];
+                            const float fc = __int_as_float(inf.y) * B.fric;
+                            if (c.max_force > 0) {
+                                v3 fcn = primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, -1.0f);
+                                const float fl = length(fcn);
+                                if (fl > c.max_force) fcn = fcn * (c.max_force / fl);
+                                f = f + fcn;
+                            } else {
+                                f = f + primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, B.bounce);
+                            }
+                        }
+                    }
+                }
+            }
+            // ---- integration (SoftBody::integrate_nodes)
+            if (inv_mass > 0) {
+                vel = vel + f * (inv_mass * dt);
+                v2 = dot(vel, vel);
+                if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
+                    vel = vel * (kMaxNodeSpeed / sqrtf(v2));
+                    v2 = kMaxNodeSpeed * kMaxNodeSpeed;
+                } else if (!(v2 >= 0.0f)) {
+                    vel = V(0, 0, 0);
+                    v2 = 0;
+                }
+                pos = pos + vel * dt;
+            }
+            nd[2 * i] = make_float4(pos.x, pos.y, pos.z, inv_mass);
+            nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, m);
+            // the bounds skip a non-finite coordinate as the reference's vmin / vmax do (a NaN never compares less)
+            p = V(pos.x == pos.x ? pos.x : 1e30f, pos.y == pos.y ? pos.y : 1e30f, pos.z == pos.z ? pos.z : 1e30f);
+            pmx = V(pos.x == pos.x ? pos.x : -1e30f, pos.y == pos.y ? pos.y : -1e30f, pos.z == pos.z ? pos.z : -1e30f);
+            v2 = smax(v2, v2start);
+        }
+    }
+    accumulate_bounds(bodies, body, live, p, pmx, v2, contact);
 }
 
 // ------------------------------------------------------------------------------------------ end of frame

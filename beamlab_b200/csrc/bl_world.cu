@@ -7,7 +7,9 @@
 //           inc_ptr / inc: each node's incident beams in beam order (beam index, bit 31: the node is the beam's b end)
 //   beams   ab int2 (a, b)   kd float2 (k, d)   bst float4 (L, max_pos, max_neg, strength)   bmeta u32 (type, flags,
 //           the body's deform/break/ductile bits, asleep)   bcold float4 (plastic, L0, support_limit)   stress f32
-//           bbody i32   fv float4: the substep's beam force (scratch between k_beams and k_nodes)
+//           bbody i32   fsc f32: the substep's beam force scalar (scratch between k_beams and k_force)
+//   per node: inc2 - the incidences with the other end (k_force), nodef float4 - the substep's force (k_force, the
+//           contacts between bodies, k_integrate)
 //   bodies  Body records (bl_device.cuh)
 // A frame (bl_gpu_step_substeps) is captured once per substep count as a CUDA graph and replayed.
 #include "../../include/beamlab_gpu.h"
@@ -84,7 +86,9 @@ struct bl_gpu_ctx {
     std::vector<int> cell_ptr, cell_items, big;
     bool statics_dirty = true;
     // device
-    DevBuf<float4> nd, bst, bcold, fv;
+    DevBuf<float4> nd, bst, bcold, nodef;
+    DevBuf<float> fsc;
+    DevBuf<int2> inc2;
     DevBuf<int4> info;
     DevBuf<int> inc_ptr, inc, bbody;
     DevBuf<int2> ab;
@@ -142,7 +146,7 @@ struct bl_gpu_ctx {
     DevBuf<int> parent, isl_live, isl_cnt, isl_nodes, isl_idx, isl_noff, isl_poff, isl_pcnt, isl_contacts, pair_total;
     DevBuf<int> pt_node, pt_body, bk_start, bk_fill, bk_items, run_end, g_start, g_fill, g_items, counters;
     DevBuf<int2> pairs;
-    DevBuf<float4> hit_a, hit_b, fsplit;
+    DevBuf<float4> hit_a, hit_b;
     Contacts ct{};
     // frames captured as graphs, by substep count
     std::map<int, cudaGraphExec_t> graphs;
@@ -197,14 +201,14 @@ static void free_contacts(bl_gpu_ctx* c) {
     c->isl_cnt.free_(), c->isl_nodes.free_(), c->isl_idx.free_(), c->isl_noff.free_(), c->isl_poff.free_(), c->isl_pcnt.free_();
     c->isl_contacts.free_(), c->pair_total.free_(), c->pt_node.free_(), c->pt_body.free_(), c->bk_start.free_(), c->bk_fill.free_();
     c->bk_items.free_(), c->run_end.free_(), c->g_start.free_(), c->g_fill.free_(), c->g_items.free_(), c->counters.free_();
-    c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_(), c->fsplit.free_();
+    c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_();
     c->contacts_on = false;
 }
 
 static void free_device(bl_gpu_ctx* c) {
     free_fem(c);
     free_contacts(c);
-    c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->fv.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
+    c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
 }
@@ -625,7 +629,6 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     BL_CUDA(c, c->g_start.alloc((size_t)c->max_isl * (kGridCells + 1)));
     BL_CUDA(c, c->g_fill.alloc((size_t)c->max_isl * (kGridCells + 1)));
     BL_CUDA(c, c->g_items.alloc(N));
-    BL_CUDA(c, c->fsplit.alloc(N));
     // (the pair list starts as valid indices: k_detect reads up to the last search's total)
     BL_CUDA(c, cudaMemsetAsync(c->pairs.p, 0, sizeof(int2) * c->cfg.max_pairs, c->stream));
     BL_CUDA(c, cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), c->stream));
@@ -641,7 +644,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     C.pair_total = c->pair_total.p, C.pairs = c->pairs.p, C.hit_a = c->hit_a.p, C.hit_b = c->hit_b.p, C.max_pairs = c->cfg.max_pairs;
     C.pt_node = c->pt_node.p, C.pt_body = c->pt_body.p, C.pt_cell = c->pt_cell.p, C.bk_start = c->bk_start.p, C.bk_fill = c->bk_fill.p;
     C.bk_items = c->bk_items.p, C.run_end = c->run_end.p, C.g_start = c->g_start.p, C.g_fill = c->g_fill.p, C.g_items = c->g_items.p;
-    C.fsplit = c->fsplit.p, C.counters = c->counters.p, C.interval = c->interval, C.dt = c->cfg.dt, C.wake_speed = c->cfg.sleep_speed;
+    C.counters = c->counters.p, C.interval = c->interval, C.dt = c->cfg.dt, C.wake_speed = c->cfg.sleep_speed;
     return BL_GPU_OK;
 }
 
@@ -722,7 +725,18 @@ static int commit_bodies(bl_gpu_ctx* c) {
         (rc = upload_vec(c, c->bmeta, meta)) || (rc = upload_vec(c, c->bcold, bcold)) || (rc = upload_vec(c, c->stress, stress)) ||
         (rc = upload_vec(c, c->bbody, bbody)) || (rc = upload_vec(c, c->dbodies, recs)))
         return rc;
-    BL_CUDA(c, c->fv.alloc(M));
+    BL_CUDA(c, c->fsc.alloc(M));
+    BL_CUDA(c, c->nodef.alloc(N));
+    {
+        std::vector<int2> inc2(inc.size());
+        for (int i = 0; i < N; i++)
+            for (int q = inc_ptr[i]; q < inc_ptr[i + 1]; q++) {
+                const int e = inc[q];
+                const int2 e2 = ab[e & 0x7fffffff];
+                inc2[q] = make_int2(e, e < 0 ? e2.x : e2.y); // (the other end)
+            }
+        if ((rc = upload_vec(c, c->inc2, inc2))) return rc;
+    }
     int P = 1;
     while (P < maxn) P <<= 1;
     c->rs_P = P;
@@ -762,7 +776,7 @@ static int ensure_committed(bl_gpu_ctx* c) {
 static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0; } // (s == 0 || s >= next_rebuild)
 
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
-    int64_t per = 2;
+    int64_t per = 3;
     if (c->NF > 0) {
         per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
         if (c->cfg.fem_solver != BL_GPU_FEM_CHOLESKY) per += 1 - c->chol_launches; // (the Cholesky runs on a fallback only)
@@ -771,7 +785,7 @@ static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
     }
     int64_t total = per * n + 3;
     if (c->contacts_on) {
-        total += 1 + 4 * (int64_t)n; // k_islands; k_wake, k_detect, k_collide, k_nodes phase 1 a substep
+        total += 1 + 3 * (int64_t)n; // k_islands; k_wake, k_detect, k_collide a substep
         for (int k = 0; k < n; k++) total += rebuild_at(c, k) ? 1 : 0;
     }
     return total;
@@ -872,19 +886,18 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             }
         }
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
-        k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fv.p, c->nd.p, c->dbodies.p,
+        k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p,
                                                c->M, c->B);
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
-        k_nodes<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc.p, c->fv.p, c->dbodies.p, c->st, c->cfg.gravity[0],
-                                               c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0, nfm, 0, c->fsplit.p);
+        k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0], c->cfg.gravity[1],
+                                               c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
         if (c->contacts_on) {
-            // contacts between bodies on the forces so far, then the nodes of their islands finish
+            // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
             k_detect<<<148 * 4, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, CT);
-            k_collide<<<(c->B + 127) / 128, 128, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT);
-            k_nodes<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc.p, c->fv.p, c->dbodies.p, c->st, c->cfg.gravity[0],
-                                                   c->cfg.gravity[1], c->cfg.gravity[2], dt, c->N, k == 0 ? 1 : 0, nfm, 1, c->fsplit.p);
+            k_collide<<<(c->B + 127) / 128, 128, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
         }
+        k_integrate<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p);
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
             k_fem_assemble<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);

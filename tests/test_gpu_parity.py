@@ -85,4 +85,4 @@ def test_gpu_frames_and_streams(port_lib):
         ow.step_substeps(n)
     assert_same(gw, ow, 3, "mixed frames")
     st = gw.w.stats()
-    assert st["total_substeps"] == 125 and st["kernel_launches"] == 2 * 125 + 3 * 8 and st["device_errors"] == 0
+    assert st["total_substeps"] == 125 and st["kernel_launches"] == 3 * 125 + 3 * 8 and st["device_errors"] == 0
