@@ -250,33 +250,21 @@ __global__ void k_frame_begin(Body* __restrict__ bodies, int nbodies, Statics st
 }
 
 // ------------------------------------------------------------------------------------------ per substep
-// SoftBody::compute_beam_forces, one beam (softbody.cpp:412-470). The beam's force on its end a is dis * fsc[j]
-// (dis = p_a - p_b), on b its negative; fsc[j] = kNoPush when the beam does not push this substep. Thread j < nbodies
-// also resets body j's bounds accumulator for this substep's k_integrate.
-__global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
-                                               uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
-                                               const int* __restrict__ bbody, float* __restrict__ fsc, const float4* __restrict__ nd,
-                                               Body* __restrict__ bodies, int nbeams, int nbodies) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < nbodies) {
-        Body& B = bodies[j];
-        B.acc_mn[0] = B.acc_mn[1] = B.acc_mn[2] = 1e30f;
-        B.acc_mx[0] = B.acc_mx[1] = B.acc_mx[2] = -1e30f;
-    }
-    if (j >= nbeams) return;
-    uint32_t meta = bmeta[j];
+// SoftBody::compute_beam_forces, one beam (softbody.cpp:412-470), from its loaded state: meta, s0 = (L, max_pos,
+// max_neg, strength), c = (k, d), its ends' states. The beam's force on its end a is dis * fsc[j] (dis = p_a - p_b), on
+// b its negative; fsc[j] = kNoPush when the beam does not push this substep.
+__device__ __forceinline__ void beam_step(int j, uint32_t meta, float4 s0, float2 c, float4 pa, float4 va, float4 pb, float4 vb, float4* __restrict__ bst,
+                                          uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
+                                          const int* __restrict__ bbody, float* __restrict__ fsc, Body* __restrict__ bodies) {
     if (meta & kBeamAsleep) return;
     float out = kNoPush;
     const uint32_t type = meta & 0xffu;
     uint32_t flags = (meta >> 8) & 0xffu;
     if (!(flags & (BF_BROKEN | BF_SHOCK))) {
-        const int2 e = ab[j];
-        const float4 pa = nd[2 * e.x], va = nd[2 * e.x + 1], pb = nd[2 * e.y], vb = nd[2 * e.y + 1];
         const v3 dis = V(pa.x - pb.x, pa.y - pb.y, pa.z - pb.z);
         const float len2 = dot(dis, dis);
         if (!(len2 < 1e-12f)) { // (a NaN length goes on, as in the reference)
-            float4 s = bst[j]; // L, max_pos, max_neg, strength
-            const float2 c = kd[j];
+            float4 s = s0; // L, max_pos, max_neg, strength
             const float inv_len = 1.0f / sqrtf(len2);
             const float len = len2 * inv_len;
             const float diff = len - s.x;
@@ -333,6 +321,31 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
         }
     }
     fsc[j] = out;
+}
+
+// Two beams a thread (j and j + blockDim.x of the block's pair of tiles): both beams' loads are issued before either
+// computes. Thread t < nbodies of the grid also resets body t's bounds accumulator for this substep's k_integrate.
+__global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
+                                               uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
+                                               const int* __restrict__ bbody, float* __restrict__ fsc, const float4* __restrict__ nd,
+                                               Body* __restrict__ bodies, int nbeams, int nbodies) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nbodies) {
+        Body& B = bodies[t];
+        B.acc_mn[0] = B.acc_mn[1] = B.acc_mn[2] = 1e30f;
+        B.acc_mx[0] = B.acc_mx[1] = B.acc_mx[2] = -1e30f;
+    }
+    const int j0 = 2 * blockIdx.x * blockDim.x + threadIdx.x, j1 = j0 + blockDim.x;
+    const bool h0 = j0 < nbeams, h1 = j1 < nbeams;
+    const uint32_t m0 = h0 ? bmeta[j0] : kBeamAsleep, m1 = h1 ? bmeta[j1] : kBeamAsleep;
+    const int2 e0 = h0 ? ab[j0] : make_int2(0, 0), e1 = h1 ? ab[j1] : make_int2(0, 0);
+    const float4 s0 = h0 ? bst[j0] : make_float4(0, 0, 0, 0), s1 = h1 ? bst[j1] : make_float4(0, 0, 0, 0);
+    const float2 c0 = h0 ? kd[j0] : make_float2(0, 0), c1 = h1 ? kd[j1] : make_float2(0, 0);
+    float4 pa0 = make_float4(0, 0, 0, 0), va0 = pa0, pb0 = pa0, vb0 = pa0, pa1 = pa0, va1 = pa0, pb1 = pa0, vb1 = pa0;
+    if (h0) pa0 = nd[2 * e0.x], va0 = nd[2 * e0.x + 1], pb0 = nd[2 * e0.y], vb0 = nd[2 * e0.y + 1];
+    if (h1) pa1 = nd[2 * e1.x], va1 = nd[2 * e1.x + 1], pb1 = nd[2 * e1.y], vb1 = nd[2 * e1.y + 1];
+    if (h0) beam_step(j0, m0, s0, c0, pa0, va0, pb0, vb0, bst, bmeta, bcold, stress, bbody, fsc, bodies);
+    if (h1) beam_step(j1, m1, s1, c1, pa1, va1, pb1, vb1, bst, bmeta, bcold, stress, bbody, fsc, bodies);
 }
 
 // The frame bodies' gather (NodeFem): their nodes' forces go to the frame's implicit step
@@ -408,12 +421,9 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, co
                 const float4 e = nf.ext[i];
                 f = V(f.x + e.x, f.y + e.y, f.z + e.z);
             }
-            const int q1 = inc_ptr[i + 1];
-            for (int q = inc_ptr[i]; q < q1; q++) {
-                const int2 e = inc2[q];
-                const float sc = fsc[e.x & 0x7fffffff];
-                if (__float_as_uint(sc) == __float_as_uint(kNoPush)) continue;
-                const float4 Po = nd[2 * e.y];
+            // (eight incidences' loads issued together, then added in order: the gathers overlap)
+            auto add = [&](int2 e, float sc, float4 Po) {
+                if (__float_as_uint(sc) == __float_as_uint(kNoPush)) return;
                 if (e.x < 0) { // (this node is the beam's b: dis = p_a - p_b, the force subtracted)
                     const v3 dis = V(Po.x - P.x, Po.y - P.y, Po.z - P.z);
                     f = V(f.x - dis.x * sc, f.y - dis.y * sc, f.z - dis.z * sc);
@@ -421,6 +431,23 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, co
                     const v3 dis = V(P.x - Po.x, P.y - Po.y, P.z - Po.z);
                     f = V(f.x + dis.x * sc, f.y + dis.y * sc, f.z + dis.z * sc);
                 }
+            };
+            const int q1 = inc_ptr[i + 1];
+            int q = inc_ptr[i];
+            for (; q + 8 <= q1; q += 8) {
+                int2 e[8];
+                float sc[8];
+                float4 Po[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) e[u] = inc2[q + u];
+#pragma unroll
+                for (int u = 0; u < 8; u++) sc[u] = fsc[e[u].x & 0x7fffffff], Po[u] = nd[2 * e[u].y];
+#pragma unroll
+                for (int u = 0; u < 8; u++) add(e[u], sc[u], Po[u]);
+            }
+            for (; q < q1; q++) {
+                const int2 e = inc2[q];
+                add(e, fsc[e.x & 0x7fffffff], nd[2 * e.y]);
             }
             if (B.is_fem) {
                 live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)

@@ -869,7 +869,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     const float dt = c->cfg.dt;
     const float frame_time = (float)n * dt;
     const int tb = 256;
-    const int gb = (std::max(c->M, c->B) + tb - 1) / tb, gn = (c->N + tb - 1) / tb, gbody = (c->B + tb - 1) / tb;
+    const int gb = std::max((c->M + 2 * tb - 1) / (2 * tb), (c->B + tb - 1) / tb), gn = (c->N + tb - 1) / tb, gbody = (c->B + tb - 1) / tb;
     const Contacts& CT = c->ct;
     if (c->contacts_on) k_islands<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, frame_time, c->cfg.sleeping, CT, c->deverr.p);
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
