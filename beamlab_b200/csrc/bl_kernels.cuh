@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, co
                 const float4 e = nf.ext[i];
                 f = V(f.x + e.x, f.y + e.y, f.z + e.z);
             }
-            // (eight incidences' loads issued together, then added in order: the gathers overlap)
+            // (four incidences' loads issued together, then added in order: the gathers overlap)
             auto add = [&](int2 e, float sc, float4 Po) {
                 if (__float_as_uint(sc) == __float_as_uint(kNoPush)) return;
                 if (e.x < 0) { // (this node is the beam's b: dis = p_a - p_b, the force subtracted)
@@ -434,16 +434,16 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, co
             };
             const int q1 = inc_ptr[i + 1];
             int q = inc_ptr[i];
-            for (; q + 8 <= q1; q += 8) {
-                int2 e[8];
-                float sc[8];
-                float4 Po[8];
+            for (; q + 4 <= q1; q += 4) {
+                int2 e[4];
+                float sc[4];
+                float4 Po[4];
 #pragma unroll
-                for (int u = 0; u < 8; u++) e[u] = inc2[q + u];
+                for (int u = 0; u < 4; u++) e[u] = inc2[q + u];
 #pragma unroll
-                for (int u = 0; u < 8; u++) sc[u] = fsc[e[u].x & 0x7fffffff], Po[u] = nd[2 * e[u].y];
+                for (int u = 0; u < 4; u++) sc[u] = fsc[e[u].x & 0x7fffffff], Po[u] = nd[2 * e[u].y];
 #pragma unroll
-                for (int u = 0; u < 8; u++) add(e[u], sc[u], Po[u]);
+                for (int u = 0; u < 4; u++) add(e[u], sc[u], Po[u]);
             }
             for (; q < q1; q++) {
                 const int2 e = inc2[q];

@@ -773,9 +773,9 @@ static int ensure_committed(bl_gpu_ctx* c) {
     return BL_GPU_OK;
 }
 
-// One frame of n substeps on stream s: without FEM frames 2n + 3 kernels. ev (2n + 4 events, or null): recorded
-// before the first kernel, after the frame's start, after each substep's beams (and triangles) and after the rest of
-// each substep, after the frame's end kernels.
+// One frame of n substeps on stream s. ev (5n + 4 events, or null): recorded before the first kernel, after the
+// frame's start, in each substep after the beams (and triangles), the nodes' forces, the contacts between bodies, the
+// integration and the FEM frames' step, and after the frame's end kernels.
 static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0; } // (s == 0 || s >= next_rebuild)
 
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
@@ -907,6 +907,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         mark();
         k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0], c->cfg.gravity[1],
                                                c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
+        mark();
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
             enqueue_if(c, s, cs.h[cond ? 2 * k + 1 : 0], cond, [&](cudaStream_t cs2) {
@@ -914,7 +915,9 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                 k_collide<<<(c->B + 127) / 128, 128, 0, cs2>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
             });
         }
+        mark();
         k_integrate<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p);
+        mark();
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
             k_fem_assemble<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
@@ -1659,7 +1662,7 @@ int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profil
     auto it = c->pgraphs.find(n);
     if (it == c->pgraphs.end()) {
         ProfGraph pg;
-        pg.events.resize(2 * (size_t)n + 4);
+        pg.events.resize(5 * (size_t)n + 4);
         for (cudaEvent_t& e : pg.events) BL_CUDA(c, cudaEventCreate(&e));
         cudaGraph_t g = nullptr;
         BL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1685,9 +1688,14 @@ int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profil
         return ms;
     };
     out->begin_ms = el(0, 1);
-    for (int k = 0; k < n; k++) out->beams_ms += el(1 + 2 * k, 2 + 2 * k), out->nodes_ms += el(2 + 2 * k, 3 + 2 * k);
-    out->finish_ms = el(1 + 2 * n, 3 + 2 * n);
-    out->frame_ms = el(0, 3 + 2 * n);
+    for (int k = 0; k < n; k++) {
+        const int b = 1 + 5 * k;
+        out->beams_ms += el(b, b + 1), out->force_ms += el(b + 1, b + 2), out->contacts_ms += el(b + 2, b + 3);
+        out->integrate_ms += el(b + 3, b + 4), out->fem_ms += el(b + 4, b + 5);
+    }
+    out->nodes_ms = out->force_ms + out->contacts_ms + out->integrate_ms + out->fem_ms;
+    out->finish_ms = el(1 + 5 * n, 3 + 5 * n);
+    out->frame_ms = el(0, 3 + 5 * n);
     BL_CUDA(c, terr);
     return BL_GPU_OK;
 }
