@@ -324,14 +324,11 @@ __device__ __forceinline__ void beam_step(int j, uint32_t meta, float4 s0, float
 }
 
 // Two beams a thread (j and j + blockDim.x of the block's pair of tiles): both beams' loads are issued before either
-// computes. The nodes the block's beams reach (range[block] = [lo, hi), hi < 0: too many) are first copied into shared
-// memory with coalesced loads, and the beams read their ends there. Thread t < nbodies of the grid also resets body t's
-// bounds accumulator for this substep's k_integrate.
+// computes. Thread t < nbodies of the grid also resets body t's bounds accumulator for this substep's k_integrate.
 __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
                                                uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
                                                const int* __restrict__ bbody, float* __restrict__ fsc, const float4* __restrict__ nd,
-                                               Body* __restrict__ bodies, int nbeams, int nbodies, const int2* __restrict__ range, int nranges) {
-    extern __shared__ float4 s_nd[];
+                                               Body* __restrict__ bodies, int nbeams, int nbodies) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < nbodies) {
         Body& B = bodies[t];
@@ -344,22 +341,9 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
     const int2 e0 = h0 ? ab[j0] : make_int2(0, 0), e1 = h1 ? ab[j1] : make_int2(0, 0);
     const float4 s0 = h0 ? bst[j0] : make_float4(0, 0, 0, 0), s1 = h1 ? bst[j1] : make_float4(0, 0, 0, 0);
     const float2 c0 = h0 ? kd[j0] : make_float2(0, 0), c1 = h1 ? kd[j1] : make_float2(0, 0);
-    const int2 rg = (int)blockIdx.x < nranges ? range[blockIdx.x] : make_int2(0, -1);
-    const bool staged = rg.y >= 0;
-    if (staged)
-        for (int q = threadIdx.x; q < 2 * (rg.y - rg.x); q += blockDim.x) s_nd[q] = nd[2 * rg.x + q];
-    __syncthreads();
-    const float4* src = staged ? s_nd : nd;
-    const int base = staged ? rg.x : 0;
     float4 pa0 = make_float4(0, 0, 0, 0), va0 = pa0, pb0 = pa0, vb0 = pa0, pa1 = pa0, va1 = pa0, pb1 = pa0, vb1 = pa0;
-    if (h0) {
-        const int a = e0.x - base, b = e0.y - base;
-        pa0 = src[2 * a], va0 = src[2 * a + 1], pb0 = src[2 * b], vb0 = src[2 * b + 1];
-    }
-    if (h1) {
-        const int a = e1.x - base, b = e1.y - base;
-        pa1 = src[2 * a], va1 = src[2 * a + 1], pb1 = src[2 * b], vb1 = src[2 * b + 1];
-    }
+    if (h0) pa0 = nd[2 * e0.x], va0 = nd[2 * e0.x + 1], pb0 = nd[2 * e0.y], vb0 = nd[2 * e0.y + 1];
+    if (h1) pa1 = nd[2 * e1.x], va1 = nd[2 * e1.x + 1], pb1 = nd[2 * e1.y], vb1 = nd[2 * e1.y + 1];
     if (h0) beam_step(j0, m0, s0, c0, pa0, va0, pb0, vb0, bst, bmeta, bcold, stress, bbody, fsc, bodies);
     if (h1) beam_step(j1, m1, s1, c1, pa1, va1, pb1, vb1, bst, bmeta, bcold, stress, bbody, fsc, bodies);
 }
@@ -419,21 +403,9 @@ __device__ __forceinline__ void accumulate_bounds(Body* __restrict__ bodies, int
 // for World::collide_static and the integration (k_integrate) - the contacts between bodies add to it first.
 // Frame bodies (Body::is_fem): the triangles' forces and torques are gathered onto the frame nodes in the reference's
 // order (gather_forces, frame_fem.cpp:2080-2105) and the force is kept in nforce for the frame's implicit step.
-// The positions and beam scalars the block's nodes reach (range[block] = nodes [x, y), beams [z, w); y < 0: too
-// many) are first copied into shared memory with coalesced loads (positions: ncap float4, then the scalars).
 __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ inc_ptr,
                                                const int2* __restrict__ inc2, const float* __restrict__ fsc, Body* __restrict__ bodies, float gx,
-                                               float gy, float gz, int nnodes, int first, NodeFem nf, float4* __restrict__ fnode,
-                                               const int4* __restrict__ range, int ncap) {
-    extern __shared__ float4 s_pos[];
-    float* s_sc = reinterpret_cast<float*>(s_pos + ncap);
-    const int4 rg = range[blockIdx.x];
-    const bool staged = rg.y >= 0;
-    if (staged) {
-        for (int q = threadIdx.x; q < rg.y - rg.x; q += blockDim.x) s_pos[q] = nd[2 * (rg.x + q)];
-        for (int q = threadIdx.x; q < rg.w - rg.z; q += blockDim.x) s_sc[q] = fsc[rg.z + q];
-    }
-    __syncthreads();
+                                               float gy, float gz, int nnodes, int first, NodeFem nf, float4* __restrict__ fnode) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int body = -1;
     float v2 = 0.0f;
@@ -468,20 +440,14 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, co
                 float4 Po[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) e[u] = inc2[q + u];
-                if (staged) {
 #pragma unroll
-                    for (int u = 0; u < 4; u++) sc[u] = s_sc[(e[u].x & 0x7fffffff) - rg.z], Po[u] = s_pos[e[u].y - rg.x];
-                } else {
-#pragma unroll
-                    for (int u = 0; u < 4; u++) sc[u] = fsc[e[u].x & 0x7fffffff], Po[u] = nd[2 * e[u].y];
-                }
+                for (int u = 0; u < 4; u++) sc[u] = fsc[e[u].x & 0x7fffffff], Po[u] = nd[2 * e[u].y];
 #pragma unroll
                 for (int u = 0; u < 4; u++) add(e[u], sc[u], Po[u]);
             }
             for (; q < q1; q++) {
                 const int2 e = inc2[q];
-                if (staged) add(e, s_sc[(e.x & 0x7fffffff) - rg.z], s_pos[e.y - rg.x]);
-                else add(e, fsc[e.x & 0x7fffffff], nd[2 * e.y]);
+                add(e, fsc[e.x & 0x7fffffff], nd[2 * e.y]);
             }
             if (B.is_fem) {
                 live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)

@@ -89,10 +89,6 @@ struct bl_gpu_ctx {
     DevBuf<float4> nd, bst, bcold, nodef;
     DevBuf<float> fsc;
     DevBuf<int2> inc2;
-    // per block of k_beams / k_force: the node (and beam) ranges its threads reach, staged in shared memory
-    DevBuf<int2> brange;
-    DevBuf<int4> frange;
-    int bsmem = 0, fsmem = 0, fncap = 0;
     DevBuf<int4> info;
     DevBuf<int> inc_ptr, inc, bbody;
     DevBuf<int2> ab;
@@ -213,7 +209,7 @@ static void free_contacts(bl_gpu_ctx* c) {
 static void free_device(bl_gpu_ctx* c) {
     free_fem(c);
     free_contacts(c);
-    c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->brange.free_(), c->frange.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
+    c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
 }
@@ -743,40 +739,6 @@ static int commit_bodies(bl_gpu_ctx* c) {
                 inc2[q] = make_int2(e, e < 0 ? e2.x : e2.y); // (the other end)
             }
         if ((rc = upload_vec(c, c->inc2, inc2))) return rc;
-        // k_beams: 512 beams a block; the nodes they reach, as a range (staged when it holds at most kBeamNodes)
-        const int kBeamNodes = 1024, kForceNodes = 1536, kForceBeams = 6144;
-        const int nbb = std::max(1, (M + 511) / 512);
-        std::vector<int2> br(nbb);
-        int bmax = 0;
-        for (int b = 0; b < nbb; b++) {
-            int lo = INT32_MAX, hi = -1;
-            for (int j = 512 * b; j < std::min(M, 512 * b + 512); j++) lo = std::min(lo, std::min(ab[j].x, ab[j].y)), hi = std::max(hi, std::max(ab[j].x, ab[j].y));
-            const bool ok = hi >= 0 && hi + 1 - lo <= kBeamNodes;
-            br[b] = ok ? make_int2(lo, hi + 1) : make_int2(0, -1);
-            if (ok) bmax = std::max(bmax, hi + 1 - lo);
-        }
-        // k_force: 256 nodes a block; the nodes and beams their incidences reach
-        const int nfb = std::max(1, (N + 255) / 256);
-        std::vector<int4> fr(nfb);
-        int fnmax = 0, fbmax = 0;
-        for (int b = 0; b < nfb; b++) {
-            int nlo = INT32_MAX, nhi = -1, blo = INT32_MAX, bhi = -1;
-            for (int i = 256 * b; i < std::min(N, 256 * b + 256); i++) {
-                nlo = std::min(nlo, i), nhi = std::max(nhi, i);
-                for (int q = inc_ptr[i]; q < inc_ptr[i + 1]; q++) {
-                    const int j = inc2[q].x & 0x7fffffff;
-                    nlo = std::min(nlo, inc2[q].y), nhi = std::max(nhi, inc2[q].y), blo = std::min(blo, j), bhi = std::max(bhi, j);
-                }
-            }
-            if (bhi < 0) blo = 0, bhi = -1;
-            const bool ok = nhi >= 0 && nhi + 1 - nlo <= kForceNodes && bhi + 1 - blo <= kForceBeams;
-            fr[b] = ok ? make_int4(nlo, nhi + 1, blo, bhi + 1) : make_int4(0, -1, 0, 0);
-            if (ok) fnmax = std::max(fnmax, nhi + 1 - nlo), fbmax = std::max(fbmax, bhi + 1 - blo);
-        }
-        c->bsmem = 2 * (int)sizeof(float4) * bmax;
-        c->fncap = fnmax;
-        c->fsmem = (int)sizeof(float4) * fnmax + (int)sizeof(float) * fbmax;
-        if ((rc = upload_vec(c, c->brange, br)) || (rc = upload_vec(c, c->frange, fr))) return rc;
     }
     int P = 1;
     while (P < maxn) P <<= 1;
@@ -939,12 +901,12 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             });
         }
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
-        k_beams<<<std::max(gb, 1), tb, c->bsmem, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
-                                                      c->dbodies.p, c->M, c->B, c->brange.p, (int)c->brange.n);
+        k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p,
+                                               c->M, c->B);
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
-        k_force<<<std::max(gn, 1), tb, c->fsmem, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0],
-                                                      c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p, c->frange.p, c->fncap);
+        k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0], c->cfg.gravity[1],
+                                               c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
         mark();
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
