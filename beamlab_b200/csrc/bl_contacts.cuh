@@ -33,16 +33,6 @@ constexpr float kTornStretch2 = 2.5f * 2.5f; // softbody.h:154
 enum : uint32_t { TF_TWO_SIDED = 1, TF_TORN = 2 };
 enum : uint32_t { DEVERR_PAIRS = 4, DEVERR_ISLAND = 8, DEVERR_CONTACT_UNSUPPORTED = 32 };
 
-// The conditions of a frame's graph that guard its substeps' contact kernels: k_islands sets them all to 1 when some
-// island has pairs this frame, else to 0 (the kernels do not run; `skipped` counts the launches so saved)
-constexpr int kMaxCond = 128;
-struct CondSet {
-    cudaGraphConditionalHandle h[kMaxCond];
-    int n;
-    int launches;            // contact kernels of the frame (counted as skipped when the conditions are 0)
-    long long* skipped;
-};
-
 struct Contacts {
     int4* tri;                 // a, b, c, flags | body << 8
     const float* tri_rest2;
@@ -205,7 +195,7 @@ __device__ void uf_union(int* parent, int a, int b) {
 // collision volumes). One block. Bodies with FEM frames take no contacts here: one that would is flagged
 // (DEVERR_CONTACT_UNSUPPORTED) and stays in an island of its own.
 __global__ void __launch_bounds__(1024) k_islands(Body* __restrict__ bodies, int nb, float frame_time, int world_sleeping, Contacts C,
-                                                  uint32_t* __restrict__ deverr, CondSet cs) {
+                                                  uint32_t* __restrict__ deverr) {
     __shared__ int s_warp[32];
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
         Body& B = bodies[i];
@@ -264,11 +254,6 @@ __global__ void __launch_bounds__(1024) k_islands(Body* __restrict__ bodies, int
         const int oi = block_scan_excl(pr ? 1 : 0, ti, s_warp);
         if (pr) C.isl_noff[i] = carry_n + on, C.isl_idx[i] = carry_i + oi;
         carry_n += tn, carry_i += ti;
-    }
-    if (threadIdx.x == 0) {
-        const unsigned v = carry_i > 0 ? 1u : 0u;
-        for (int q = 0; q < cs.n; q++) cudaGraphSetConditional(cs.h[q], v);
-        if (cs.n > 0 && !v) *cs.skipped += cs.launches;
     }
 }
 

@@ -147,7 +147,6 @@ struct bl_gpu_ctx {
     DevBuf<int> pt_node, pt_body, bk_start, bk_fill, bk_items, run_end, g_start, g_fill, g_items, counters;
     DevBuf<int2> pairs;
     DevBuf<float4> hit_a, hit_b;
-    DevBuf<long long> skipped;                 // contact kernel launches the frames' conditions skipped
     Contacts ct{};
     // frames captured as graphs, by substep count
     std::map<int, cudaGraphExec_t> graphs;
@@ -202,7 +201,7 @@ static void free_contacts(bl_gpu_ctx* c) {
     c->isl_cnt.free_(), c->isl_nodes.free_(), c->isl_idx.free_(), c->isl_noff.free_(), c->isl_poff.free_(), c->isl_pcnt.free_();
     c->isl_contacts.free_(), c->pair_total.free_(), c->pt_node.free_(), c->pt_body.free_(), c->bk_start.free_(), c->bk_fill.free_();
     c->bk_items.free_(), c->run_end.free_(), c->g_start.free_(), c->g_fill.free_(), c->g_items.free_(), c->counters.free_();
-    c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_(), c->skipped.free_();
+    c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_();
     c->contacts_on = false;
 }
 
@@ -620,8 +619,6 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
         BL_CUDA(c, d->alloc(B));
     BL_CUDA(c, c->pair_total.alloc(1));
     BL_CUDA(c, c->counters.alloc(4));
-    BL_CUDA(c, c->skipped.alloc(1));
-    BL_CUDA(c, cudaMemsetAsync(c->skipped.p, 0, sizeof(long long), c->stream));
     BL_CUDA(c, c->pairs.alloc(c->cfg.max_pairs));
     BL_CUDA(c, c->hit_a.alloc(c->cfg.max_pairs));
     BL_CUDA(c, c->hit_b.alloc(c->cfg.max_pairs));
@@ -874,17 +871,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     const int tb = 256;
     const int gb = std::max((c->M + 2 * tb - 1) / (2 * tb), (c->B + tb - 1) / tb), gn = (c->N + tb - 1) / tb, gbody = (c->B + tb - 1) / tb;
     const Contacts& CT = c->ct;
-    // the substeps' contact kernels under conditions k_islands sets: skipped on frames without an island with pairs
-    CondSet cs{};
-    cs.skipped = c->skipped.p;
-    if (c->contacts_on && 2 * n <= kMaxCond) {
-        bool ok = true;
-        for (int q = 0; q < 2 * n && ok; q++) ok = make_condition(c, s, &cs.h[q]);
-        cs.n = ok ? 2 * n : 0;
-        for (int k = 0; k < n; k++) cs.launches += 3 + (rebuild_at(c, k) ? 1 : 0);
-    }
-    const bool cond = cs.n > 0;
-    if (c->contacts_on) k_islands<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, frame_time, c->cfg.sleeping, CT, c->deverr.p, cs);
+    if (c->contacts_on) k_islands<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, frame_time, c->cfg.sleeping, CT, c->deverr.p);
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
     mark();
     NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p};
@@ -892,13 +879,11 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     for (int k = 0; k < n; k++) {
         if (c->contacts_on) {
             // wake requests, then the pair search on its substeps (on the positions and velocities the substep starts from)
-            enqueue_if(c, s, cs.h[cond ? 2 * k : 0], cond, [&](cudaStream_t cs2) {
-                k_wake<<<c->B, 256, 0, cs2>>>(c->dbodies.p, c->bmeta.p);
-                if (rebuild_at(c, k)) {
-                    cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), cs2);
-                    k_rebuild<<<c->B, 1024, sizeof(RebuildShared), cs2>>>(c->dbodies.p, c->B, c->nd.p, c->info.p, CT, k == 0 ? 1 : 0, c->deverr.p);
-                }
-            });
+            k_wake<<<c->B, 256, 0, s>>>(c->dbodies.p, c->bmeta.p);
+            if (rebuild_at(c, k)) {
+                cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), s);
+                k_rebuild<<<c->B, 1024, sizeof(RebuildShared), s>>>(c->dbodies.p, c->B, c->nd.p, c->info.p, CT, k == 0 ? 1 : 0, c->deverr.p);
+            }
         }
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
         k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p,
@@ -910,10 +895,8 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         mark();
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
-            enqueue_if(c, s, cs.h[cond ? 2 * k + 1 : 0], cond, [&](cudaStream_t cs2) {
-                k_detect<<<148 * 4, 256, 0, cs2>>>(c->nd.p, c->info.p, c->dbodies.p, CT);
-                k_collide<<<(c->B + 127) / 128, 128, 0, cs2>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
-            });
+            k_detect<<<148 * 4, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, CT);
+            k_collide<<<(c->B + 127) / 128, 128, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
         }
         mark();
         k_integrate<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p);
@@ -1396,9 +1379,6 @@ int bl_gpu_stats(bl_gpu_ctx* c, bl_world_stats* out) {
         int total = 0;
         BL_CUDA(c, cudaMemcpy(&total, c->pair_total.p, sizeof(int), cudaMemcpyDeviceToHost));
         out->pair_searches = cnt[0], out->contacts = cnt[1], out->pairs = total;
-        long long sk = 0;
-        BL_CUDA(c, cudaMemcpy(&sk, c->skipped.p, sizeof(sk), cudaMemcpyDeviceToHost));
-        out->kernel_launches -= sk;
         for (int i = 0; i < (int)recs.size(); i++) out->islands += (recs[i].pairs && recs[i].island == i) ? 1 : 0;
     }
     return BL_GPU_OK;
