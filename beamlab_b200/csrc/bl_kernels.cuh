@@ -399,12 +399,12 @@ __device__ __forceinline__ void accumulate_bounds(Body* __restrict__ bodies, int
 
 // A node's force: clear_forces' gravity (and any constant node force), then its beams in beam order
 // (softbody.cpp:376, 466-467); each beam's force made again from the beam's scalar and the two positions, as k_beams
-// made it. inc2: the node's incidences (beam | bit 31 when the node is the beam's b end, the other end). Into fnode
+// made it. ell: the nodes' incidences (beam | bit 31 when the node is the beam's b end, the other end). Into fnode
 // for World::collide_static and the integration (k_integrate) - the contacts between bodies add to it first.
 // Frame bodies (Body::is_fem): the triangles' forces and torques are gathered onto the frame nodes in the reference's
 // order (gather_forces, frame_fem.cpp:2080-2105) and the force is kept in nforce for the frame's implicit step.
-__global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ inc_ptr,
-                                               const int2* __restrict__ inc2, const float* __restrict__ fsc, Body* __restrict__ bodies, float gx,
+__global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
+                                               const int2* __restrict__ ell, const float* __restrict__ fsc, Body* __restrict__ bodies, float gx,
                                                float gy, float gz, int nnodes, int first, NodeFem nf, float4* __restrict__ fnode) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int body = -1;
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, co
             }
             // (four incidences' loads issued together, then added in order: the gathers overlap)
             auto add = [&](int2 e, float sc, float4 Po) {
-                if (__float_as_uint(sc) == __float_as_uint(kNoPush)) return;
+                if (__float_as_uint(sc) == __float_as_uint(kNoPush) || e.y == i) return; // (e.y == i: padding)
                 if (e.x < 0) { // (this node is the beam's b: dis = p_a - p_b, the force subtracted)
                     const v3 dis = V(Po.x - P.x, Po.y - P.y, Po.z - P.z);
                     f = V(f.x - dis.x * sc, f.y - dis.y * sc, f.z - dis.z * sc);
@@ -432,22 +432,20 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, co
                     f = V(f.x + dis.x * sc, f.y + dis.y * sc, f.z + dis.z * sc);
                 }
             };
-            const int q1 = inc_ptr[i + 1];
-            int q = inc_ptr[i];
-            for (; q + 4 <= q1; q += 4) {
+            // the warp's incidences, interleaved: entry q of lane l at ell[ell_ptr[w] + 32 q + l] (a warp's load reads 32
+            // neighbours), each node's in beam order, padded to the warp's widest node (a multiple of 4) with (0, i)
+            const int w = i >> 5, lane = i & 31;
+            const int q0 = ell_ptr[w], width = (ell_ptr[w + 1] - q0) >> 5;
+            for (int q = 0; q < width; q += 4) {
                 int2 e[4];
                 float sc[4];
                 float4 Po[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) e[u] = inc2[q + u];
+                for (int u = 0; u < 4; u++) e[u] = ell[q0 + 32 * (q + u) + lane];
 #pragma unroll
                 for (int u = 0; u < 4; u++) sc[u] = fsc[e[u].x & 0x7fffffff], Po[u] = nd[2 * e[u].y];
 #pragma unroll
                 for (int u = 0; u < 4; u++) add(e[u], sc[u], Po[u]);
-            }
-            for (; q < q1; q++) {
-                const int2 e = inc2[q];
-                add(e, fsc[e.x & 0x7fffffff], nd[2 * e.y]);
             }
             if (B.is_fem) {
                 live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)

@@ -88,7 +88,8 @@ struct bl_gpu_ctx {
     // device
     DevBuf<float4> nd, bst, bcold, nodef;
     DevBuf<float> fsc;
-    DevBuf<int2> inc2;
+    DevBuf<int2> inc2;                         // per node's incidences, warp-interleaved (k_force)
+    DevBuf<int> ell_ptr;
     DevBuf<int4> info;
     DevBuf<int> inc_ptr, inc, bbody;
     DevBuf<int2> ab;
@@ -208,7 +209,7 @@ static void free_contacts(bl_gpu_ctx* c) {
 static void free_device(bl_gpu_ctx* c) {
     free_fem(c);
     free_contacts(c);
-    c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
+    c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->ell_ptr.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
 }
@@ -727,15 +728,33 @@ static int commit_bodies(bl_gpu_ctx* c) {
         return rc;
     BL_CUDA(c, c->fsc.alloc(M));
     BL_CUDA(c, c->nodef.alloc(N));
-    {
-        std::vector<int2> inc2(inc.size());
-        for (int i = 0; i < N; i++)
-            for (int q = inc_ptr[i]; q < inc_ptr[i + 1]; q++) {
-                const int e = inc[q];
-                const int2 e2 = ab[e & 0x7fffffff];
-                inc2[q] = make_int2(e, e < 0 ? e2.x : e2.y); // (the other end)
+    {   // the incidences with their other ends, per warp of 32 nodes interleaved (entry q of lane l at 32 q + l), each
+        // warp's width its widest node's count rounded up to 4, padded with (0, the node itself)
+        const int nw = (N + 31) / 32;
+        std::vector<int> eptr(nw + 1, 0);
+        for (int w = 0; w < nw; w++) {
+            int width = 0;
+            for (int l = 0; l < 32 && 32 * w + l < N; l++) width = std::max(width, inc_ptr[32 * w + l + 1] - inc_ptr[32 * w + l]);
+            width = (width + 3) / 4 * 4;
+            eptr[w + 1] = eptr[w] + 32 * width;
+        }
+        std::vector<int2> ell(eptr[nw]);
+        for (int w = 0; w < nw; w++) {
+            const int width = (eptr[w + 1] - eptr[w]) / 32;
+            for (int l = 0; l < 32; l++) {
+                const int i = 32 * w + l;
+                for (int q = 0; q < width; q++) {
+                    int2 v = make_int2(0, i < N ? i : 0);
+                    if (i < N && q < inc_ptr[i + 1] - inc_ptr[i]) {
+                        const int e = inc[inc_ptr[i] + q];
+                        const int2 e2 = ab[e & 0x7fffffff];
+                        v = make_int2(e, e < 0 ? e2.x : e2.y); // (the other end)
+                    }
+                    ell[eptr[w] + 32 * q + l] = v;
+                }
             }
-        if ((rc = upload_vec(c, c->inc2, inc2))) return rc;
+        }
+        if ((rc = upload_vec(c, c->inc2, ell)) || (rc = upload_vec(c, c->ell_ptr, eptr))) return rc;
     }
     int P = 1;
     while (P < maxn) P <<= 1;
@@ -890,7 +909,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                                                c->M, c->B);
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
-        k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->inc_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0], c->cfg.gravity[1],
+        k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0], c->cfg.gravity[1],
                                                c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
         mark();
         if (c->contacts_on) {
