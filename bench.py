@@ -314,15 +314,21 @@ def run_gpu(args):
         e2e = total_nodes * FRAME * K / (ms_e2e * 1e-3)
         peak, pk_kind = peaks()
         per = {k: prof[f"{k}_ms"] / FRAME for k in ("beams", "force", "contacts", "integrate", "fem")}
-        # the dominant kernel's algorithmic bytes: k_beams 40 B a beam; the node pass (k_force + k_integrate, one kernel
-        # in the fused ideal where the force never leaves the chip) 52 B a node
-        kern = {"k_beams": (BYTES_PER_BEAM * m, per["beams"], m, "beam", ("k_beams",)),
-                "k_force+k_integrate": (BYTES_PER_NODE * n, per["force"] + per["integrate"], n, "node", ("k_force", "k_integrate"))}
+        # algorithmic bytes a launch (each array touched once): k_beams 40 B a beam; k_force reads a node's position
+        # and mass and writes its force (32 B a node; the beams' scalars and the neighbours' positions it gathers are
+        # the scratch and the L2-resident gathers of the substep); k_integrate reads p, v, 1/m, the force (44 B) and
+        # writes p, v (24 B); the substep as a whole: 40 B a beam + 52 B a node (the force never leaving the chip)
+        kern = {"k_beams": (BYTES_PER_BEAM * m, per["beams"], m, "beam"), "k_force": (32 * n, per["force"], n, "node"),
+                "k_integrate": (68 * n, per["integrate"], n, "node")}
         dom = max(kern, key=lambda k: kern[k][1])
-        alg_bytes, kms, units_, unit_name, parts = kern[dom]
+        alg_bytes, kms, units_, unit_name = kern[dom]
         achieved = alg_bytes / (kms * 1e-3) / 1e9
-        tr = traffic_per_unit()
-        traffic = (sum(tr[p_][f"dram_bytes_per_{unit_name}"] for p_ in parts) * units_) if all(p_ in tr for p_ in parts) else None
+        tr = traffic_per_unit().get(dom)
+        traffic = tr[f"dram_bytes_per_{unit_name}"] * units_ if tr else None
+        sub_ms = per["beams"] + per["force"] + per["integrate"]
+        substep = {"algorithmic_bytes": BYTES_PER_BEAM * m + BYTES_PER_NODE * n, "ms": sub_ms,
+                   "achieved_gbs": (BYTES_PER_BEAM * m + BYTES_PER_NODE * n) / (sub_ms * 1e-3) / 1e9}
+        substep["frac"] = substep["achieved_gbs"] / peak
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -341,7 +347,7 @@ def run_gpu(args):
                          "device_errors": int(st1["device_errors"])},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{pk_kind} hbm_gbs",
-                         "algorithmic_bytes_per_launch": alg_bytes, "traffic": traffic},
+                         "algorithmic_bytes_per_launch": alg_bytes, "traffic": traffic, "substep_kernels": substep},
             "clocks": clk,
         }
         if ws == 1 and args.workload == "plate64":
