@@ -403,7 +403,7 @@ __device__ __forceinline__ void accumulate_bounds(Body* __restrict__ bodies, int
 // for World::collide_static and the integration (k_integrate) - the contacts between bodies add to it first.
 // Frame bodies (Body::is_fem): the triangles' forces and torques are gathered onto the frame nodes in the reference's
 // order (gather_forces, frame_fem.cpp:2080-2105) and the force is kept in nforce for the frame's implicit step.
-__global__ void __launch_bounds__(256) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
+__global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
                                                const int2* __restrict__ ell, const float* __restrict__ fsc, Body* __restrict__ bodies, float gx,
                                                float gy, float gz, int nnodes, int first, NodeFem nf, float4* __restrict__ fnode) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
