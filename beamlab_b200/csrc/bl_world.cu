@@ -121,8 +121,6 @@ struct bl_gpu_ctx {
     DevBuf<long long> piters;
     DevBuf<float> guess, gscale;               // the learned per-frame-node dv guess (3) and preconditioner scale (9)
     int pcg_grid = 1;
-    int solve_grid = 1;                        // k_fem_solve_all's blocks
-    DevBuf<int> d_lvl_col_ptr, d_lvl_grp_ptr;
     cudaStream_t aux = nullptr;                // (captures the bodies of conditional graph nodes)
     // the learned warm start (bl_mlp.cuh): parameters, the step's features, recorded samples, training scratch
     DevBuf<float> mlp_w, mlp_m, mlp_v, feat, prev_dv, smp_x, smp_t, smp_w, gpart, lpart, gsum;
@@ -193,7 +191,6 @@ static void free_fem(bl_gpu_ctx* c) {
     c->fcol_ptr.free_(), c->frow.free_(), c->gdiag_ptr.free_(), c->goff_ptr.free_(), c->fem_fail.free_(), c->fem_clamp.free_();
     c->px.free_(), c->pr.free_(), c->pz.free_(), c->pp.free_(), c->ppf.free_(), c->ppdi.free_(), c->pred.free_(), c->a0d.free_(), c->pxprev.free_();
     c->a0o.free_(), c->b0.free_(), c->res.free_(), c->plast.free_(), c->pstat.free_(), c->piters.free_(), c->guess.free_(), c->gscale.free_();
-    c->d_lvl_col_ptr.free_(), c->d_lvl_grp_ptr.free_();
     c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
     c->xd.free_(), c->diag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
@@ -483,7 +480,8 @@ static int commit_fem(bl_gpu_ctx* c) {
         c->lvl_col_ptr.push_back((int)lvl_col.size());
     }
     // begin, triangles, assembly, per level a factor (and an update) kernel and two substitutions, velocities, integration
-    c->chol_launches = 1; // (k_fem_solve_all: the factorization and substitutions, level by level, in one launch)
+    c->chol_launches = 3 * (int64_t)nlev;
+    for (int L = 0; L < nlev; L++) c->chol_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
     c->fem_launches = 5 + c->chol_launches;
     {   // each row's blocks in the order of their columns
         std::vector<std::vector<int2>> rows(NF);
@@ -533,15 +531,6 @@ static int commit_fem(bl_gpu_ctx* c) {
     F.col_comp = c->col_comp.p, F.comp_fail = c->comp_fail.p, F.rb_ptr = c->rb_ptr.p;
     F.rb = c->rb.p, F.lvl_col = c->lvl_col.p, F.ch2 = c->ch2.p, F.chd = c->chd.p, F.body_failures = c->fem_fail.p, F.body_clamps = c->fem_clamp.p;
     F.h = c->cfg.dt, F.step = c->cfg.dt;
-    if ((rc = upload_vec(c, c->d_lvl_col_ptr, c->lvl_col_ptr)) || (rc = upload_vec(c, c->d_lvl_grp_ptr, c->lvl_grp_ptr))) return rc;
-    {
-        int per = 0, nsm = 0, widest = 1;
-        BL_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fem_solve_all, 128, 0));
-        BL_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->cfg.device));
-        for (size_t L = 0; L + 1 < c->lvl_col_ptr.size(); L++)
-            widest = std::max(widest, std::max(c->lvl_col_ptr[L + 1] - c->lvl_col_ptr[L], c->lvl_grp_ptr[L + 1] - c->lvl_grp_ptr[L]));
-        c->solve_grid = std::max(1, std::min(per * nsm, (widest + 3) / 4));
-    }
     // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
     for (DevBuf<double>* d : {&c->px, &c->pr, &c->pz, &c->pp, &c->ppdi}) BL_CUDA(c, d->alloc(6 * (size_t)NF));
     BL_CUDA(c, c->ppf.alloc(36 * (size_t)NF));
@@ -945,15 +934,20 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             if (rec) k_mlp_record_pre<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
             if (learned) k_mlp_infer<<<(c->NF + kLanes - 1) / kLanes, kLanes, 0, s>>>(F, MD, c->guess.p, c->gscale.p);
             auto cholesky = [c, &F](cudaStream_t cs) {
-                // the factorization and substitutions, level by level, one cooperative launch (k_fem_solve_all)
                 const int nlev = (int)c->lvl_col_ptr.size() - 1;
-                cudaLaunchConfig_t lc{};
-                lc.gridDim = dim3(c->solve_grid), lc.blockDim = dim3(128), lc.dynamicSmemBytes = 0, lc.stream = cs;
-                cudaLaunchAttribute at[1];
-                at[0].id = cudaLaunchAttributeCooperative;
-                at[0].val.cooperative = 1;
-                lc.attrs = at, lc.numAttrs = 1;
-                cudaLaunchKernelEx(&lc, k_fem_solve_all, F, (const int*)c->d_lvl_col_ptr.p, (const int*)c->d_lvl_grp_ptr.p, nlev);
+                for (int L = 0; L < nlev; L++) {
+                    const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1], g0 = c->lvl_grp_ptr[L], g1 = c->lvl_grp_ptr[L + 1];
+                    k_fem_chol_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
+                    if (g1 > g0) k_fem_update_level<<<(g1 - g0 + 3) / 4, 128, 0, cs>>>(F, g0, g1);
+                }
+                for (int L = 0; L < nlev; L++) {
+                    const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
+                    k_fem_forward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
+                }
+                for (int L = nlev - 1; L >= 0; L--) {
+                    const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
+                    k_fem_backward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
+                }
             };
             if (c->cfg.fem_solver == BL_GPU_FEM_CHOLESKY) {
                 cholesky(s);
