@@ -393,10 +393,7 @@ __device__ bool chol6_dev(double* A, double* dinv) {
 
 // The level's columns, one warp each: chol6 of the diagonal block (lane 0), then every row of the column's
 // off-diagonal blocks against it, X := X L^-T (right_solve_lt, frame_fem.cpp:2211-2220), rows over the lanes
-__global__ void __launch_bounds__(128) k_fem_chol_level(FemDev F, int c0, int c1) {
-    const int lane = threadIdx.x & 31;
-    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (ci >= c1) return;
+__device__ __forceinline__ void chol_column(const FemDev& F, int ci, int lane) {
     const int k = F.lvl_col[ci];
     double* Lkk = F.diag + 36 * (size_t)k;
     double* dk = F.dinv + 6 * (size_t)k;
@@ -428,17 +425,18 @@ __global__ void __launch_bounds__(128) k_fem_chol_level(FemDev F, int c0, int c1
     }
 }
 
+__global__ void __launch_bounds__(128) k_fem_chol_level(FemDev F, int c0, int c1) {
+    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (ci >= c1) return;
+    chol_column(F, ci, threadIdx.x & 31);
+}
+
 // The level's columns' updates (the right-looking step of frame_fem.cpp:2910-2914), one warp per target block: the
 // updates this level's columns make to it, in the order of those columns, T -= P Q^T each (sub_abt's sums,
 // frame_fem.cpp:2276-2288). A target meets every level's updates in the order of the levels.
-__global__ void __launch_bounds__(128) k_fem_update_level(FemDev F, int g0, int g1) {
-    __shared__ double sPQ[4][72];
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gi = g0 + blockIdx.x * 4 + wib;
-    if (gi >= g1) return;
+__device__ __forceinline__ void update_group(const FemDev& F, int gi, int lane, double* pq) {
     const int tgt = F.grp_tgt[gi];
     double* T = tgt < F.nf ? F.diag + 36 * (size_t)tgt : F.off + 36 * (size_t)(tgt - F.nf);
-    double* pq = sPQ[wib];
     const int e0 = lane, e1 = lane + 32; // (lane e, and e + 32 for e < 4, own entry e = 6 r + c)
     double acc0 = T[e0], acc1 = lane < 4 ? T[e1] : 0.0;
     for (int u = F.grp_ptr[gi]; u < F.grp_ptr[gi + 1]; u++) {
@@ -465,6 +463,14 @@ __global__ void __launch_bounds__(128) k_fem_update_level(FemDev F, int g0, int 
     if (lane < 4) T[e1] = acc1;
 }
 
+__global__ void __launch_bounds__(128) k_fem_update_level(FemDev F, int g0, int g1) {
+    __shared__ double sPQ[4][72];
+    const int wib = threadIdx.x >> 5;
+    const int gi = g0 + blockIdx.x * 4 + wib;
+    if (gi >= g1) return;
+    update_group(F, gi, threadIdx.x & 31, sPQ[wib]);
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
@@ -472,10 +478,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // L y = r for the level's columns, one warp a column: the blocks in its row (from the columns before it) spread over
 // the lanes and summed, then forward6 (frame_fem.cpp:2304-2310, 2944-2948)
-__global__ void __launch_bounds__(128) k_fem_forward_level(FemDev F, int c0, int c1) {
-    const int lane = threadIdx.x & 31;
-    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (ci >= c1) return;
+__device__ __forceinline__ void forward_column(const FemDev& F, int ci, int lane) {
     const int k = F.lvl_col[ci];
     double s[6] = {0, 0, 0, 0, 0, 0};
     for (int q = F.rb_ptr[k] + lane; q < F.rb_ptr[k + 1]; q += 32) {
@@ -502,12 +505,15 @@ __global__ void __launch_bounds__(128) k_fem_forward_level(FemDev F, int c0, int
     for (int j = 0; j < 6; j++) F.rhs[6 * (size_t)k + j] = y[j];
 }
 
-// L^T x = y for the level's columns (the levels from the top down), one warp a column: its blocks' L^T x_row over
-// the lanes, summed, then backward6 (frame_fem.cpp:2296-2303, 2311-2317, 2949-2954)
-__global__ void __launch_bounds__(128) k_fem_backward_level(FemDev F, int c0, int c1) {
-    const int lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(128) k_fem_forward_level(FemDev F, int c0, int c1) {
     const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
     if (ci >= c1) return;
+    forward_column(F, ci, threadIdx.x & 31);
+}
+
+// L^T x = y for the level's columns (the levels from the top down), one warp a column: its blocks' L^T x_row over
+// the lanes, summed, then backward6 (frame_fem.cpp:2296-2303, 2311-2317, 2949-2954)
+__device__ __forceinline__ void backward_column(const FemDev& F, int ci, int lane) {
     const int k = F.lvl_col[ci];
     double s[6] = {0, 0, 0, 0, 0, 0};
     for (int pb = F.col_ptr[k] + lane; pb < F.col_ptr[k + 1]; pb += 32) {
@@ -531,6 +537,43 @@ __global__ void __launch_bounds__(128) k_fem_backward_level(FemDev F, int c0, in
         x[j] = t * dk[j];
     }
     for (int j = 0; j < 6; j++) F.rhs[6 * (size_t)k + j] = x[j];
+}
+
+__global__ void __launch_bounds__(128) k_fem_backward_level(FemDev F, int c0, int c1) {
+    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (ci >= c1) return;
+    backward_column(F, ci, threadIdx.x & 31);
+}
+
+// The narrow top of the elimination tree (levels [L0, L1): at most a few dozen columns and update targets each, down
+// to chains of single columns) in one block: the same per-column and per-target work as the level kernels, a
+// __syncthreads where a launch boundary was - the results are the level kernels' bit for bit.
+__global__ void __launch_bounds__(1024) k_fem_factor_tail(FemDev F, const int* __restrict__ lvl_col_ptr, const int* __restrict__ lvl_grp_ptr, int L0,
+                                                          int L1) {
+    __shared__ double sPQ[32][72];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int L = L0; L < L1; L++) {
+        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += 32) chol_column(F, ci, lane);
+        __syncthreads();
+        for (int gi = lvl_grp_ptr[L] + w; gi < lvl_grp_ptr[L + 1]; gi += 32) update_group(F, gi, lane, sPQ[w]);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_fem_forward_tail(FemDev F, const int* __restrict__ lvl_col_ptr, int L0, int L1) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int L = L0; L < L1; L++) {
+        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += 32) forward_column(F, ci, lane);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_fem_backward_tail(FemDev F, const int* __restrict__ lvl_col_ptr, int L0, int L1) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int L = L1 - 1; L >= L0; L--) {
+        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += 32) backward_column(F, ci, lane);
+        __syncthreads();
+    }
 }
 
 // ------------------------------------------------------------------------------------------ after the solve

@@ -121,6 +121,8 @@ struct bl_gpu_ctx {
     DevBuf<long long> piters;
     DevBuf<float> guess, gscale;               // the learned per-frame-node dv guess (3) and preconditioner scale (9)
     int pcg_grid = 1;
+    int tail_level = 0;                        // from this level up the tree is narrow: one block takes it
+    DevBuf<int> d_lvl_col_ptr, d_lvl_grp_ptr;
     cudaStream_t aux = nullptr;                // (captures the bodies of conditional graph nodes)
     // the learned warm start (bl_mlp.cuh): parameters, the step's features, recorded samples, training scratch
     DevBuf<float> mlp_w, mlp_m, mlp_v, feat, prev_dv, smp_x, smp_t, smp_w, gpart, lpart, gsum;
@@ -191,6 +193,7 @@ static void free_fem(bl_gpu_ctx* c) {
     c->fcol_ptr.free_(), c->frow.free_(), c->gdiag_ptr.free_(), c->goff_ptr.free_(), c->fem_fail.free_(), c->fem_clamp.free_();
     c->px.free_(), c->pr.free_(), c->pz.free_(), c->pp.free_(), c->ppf.free_(), c->ppdi.free_(), c->pred.free_(), c->a0d.free_(), c->pxprev.free_();
     c->a0o.free_(), c->b0.free_(), c->res.free_(), c->plast.free_(), c->pstat.free_(), c->piters.free_(), c->guess.free_(), c->gscale.free_();
+    c->d_lvl_col_ptr.free_(), c->d_lvl_grp_ptr.free_();
     c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
     c->xd.free_(), c->diag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
@@ -480,8 +483,13 @@ static int commit_fem(bl_gpu_ctx* c) {
         c->lvl_col_ptr.push_back((int)lvl_col.size());
     }
     // begin, triangles, assembly, per level a factor (and an update) kernel and two substitutions, velocities, integration
-    c->chol_launches = 3 * (int64_t)nlev;
-    for (int L = 0; L < nlev; L++) c->chol_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
+    // the narrow top of the tree (every level from it on at most kTail columns and update targets) goes to one block
+    const int kTail = 96;
+    int tail = nlev;
+    while (tail > 0 && c->lvl_col_ptr[tail] - c->lvl_col_ptr[tail - 1] <= kTail && c->lvl_grp_ptr[tail] - c->lvl_grp_ptr[tail - 1] <= kTail) tail--;
+    c->tail_level = tail;
+    c->chol_launches = 3 * (int64_t)tail + (tail < nlev ? 3 : 0);
+    for (int L = 0; L < tail; L++) c->chol_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
     c->fem_launches = 5 + c->chol_launches;
     {   // each row's blocks in the order of their columns
         std::vector<std::vector<int2>> rows(NF);
@@ -531,6 +539,7 @@ static int commit_fem(bl_gpu_ctx* c) {
     F.col_comp = c->col_comp.p, F.comp_fail = c->comp_fail.p, F.rb_ptr = c->rb_ptr.p;
     F.rb = c->rb.p, F.lvl_col = c->lvl_col.p, F.ch2 = c->ch2.p, F.chd = c->chd.p, F.body_failures = c->fem_fail.p, F.body_clamps = c->fem_clamp.p;
     F.h = c->cfg.dt, F.step = c->cfg.dt;
+    if ((rc = upload_vec(c, c->d_lvl_col_ptr, c->lvl_col_ptr)) || (rc = upload_vec(c, c->d_lvl_grp_ptr, c->lvl_grp_ptr))) return rc;
     // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
     for (DevBuf<double>* d : {&c->px, &c->pr, &c->pz, &c->pp, &c->ppdi}) BL_CUDA(c, d->alloc(6 * (size_t)NF));
     BL_CUDA(c, c->ppf.alloc(36 * (size_t)NF));
@@ -934,17 +943,23 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             if (rec) k_mlp_record_pre<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
             if (learned) k_mlp_infer<<<(c->NF + kLanes - 1) / kLanes, kLanes, 0, s>>>(F, MD, c->guess.p, c->gscale.p);
             auto cholesky = [c, &F](cudaStream_t cs) {
-                const int nlev = (int)c->lvl_col_ptr.size() - 1;
-                for (int L = 0; L < nlev; L++) {
+                // the wide levels a launch each (factor, update); the narrow top of the tree in one block
+                const int nlev = (int)c->lvl_col_ptr.size() - 1, tail = c->tail_level;
+                for (int L = 0; L < tail; L++) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1], g0 = c->lvl_grp_ptr[L], g1 = c->lvl_grp_ptr[L + 1];
                     k_fem_chol_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
                     if (g1 > g0) k_fem_update_level<<<(g1 - g0 + 3) / 4, 128, 0, cs>>>(F, g0, g1);
                 }
-                for (int L = 0; L < nlev; L++) {
+                if (tail < nlev) k_fem_factor_tail<<<1, 1024, 0, cs>>>(F, c->d_lvl_col_ptr.p, c->d_lvl_grp_ptr.p, tail, nlev);
+                for (int L = 0; L < tail; L++) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
                     k_fem_forward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
                 }
-                for (int L = nlev - 1; L >= 0; L--) {
+                if (tail < nlev) {
+                    k_fem_forward_tail<<<1, 1024, 0, cs>>>(F, c->d_lvl_col_ptr.p, tail, nlev);
+                    k_fem_backward_tail<<<1, 1024, 0, cs>>>(F, c->d_lvl_col_ptr.p, tail, nlev);
+                }
+                for (int L = tail - 1; L >= 0; L--) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
                     k_fem_backward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
                 }
