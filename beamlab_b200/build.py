@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libbeamlab_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "bl_world.cu"), os.path.join(HERE, "csrc", "bl_noalloc.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("bl_device.cuh", "bl_kernels.cuh", "bl_math.cuh")] + [
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in sorted(os.listdir(os.path.join(HERE, "csrc"))) if f.endswith(".cuh")] + [
     os.path.join(HERE, "..", "include", "beamlab_gpu.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-shared"]

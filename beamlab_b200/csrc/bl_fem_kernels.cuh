@@ -21,9 +21,13 @@
 // within a tolerance, not bitwise.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "bl_device.cuh"
 
 namespace blg {
+
+namespace cg = cooperative_groups;
 
 struct FemSecDev {
     float E, nu, rho, t, damping, drill;
@@ -545,34 +549,38 @@ __global__ void __launch_bounds__(128) k_fem_backward_level(FemDev F, int c0, in
     backward_column(F, ci, threadIdx.x & 31);
 }
 
-// The narrow top of the elimination tree (levels [L0, L1): at most a few dozen columns and update targets each, down
-// to chains of single columns) in one block: the same per-column and per-target work as the level kernels, a
-// __syncthreads where a launch boundary was - the results are the level kernels' bit for bit.
-__global__ void __launch_bounds__(1024) k_fem_factor_tail(FemDev F, const int* __restrict__ lvl_col_ptr, const int* __restrict__ lvl_grp_ptr, int L0,
-                                                          int L1) {
+// The top of the elimination tree (levels [L0, L1), where the levels are narrow: down to chains of single columns)
+// in one launch of a thread-block cluster (cluster_n CTAs of 1024 threads, co-scheduled on cluster_n SMs): each
+// level's columns and update targets spread over all the cluster's warps, and a cluster barrier where a launch
+// boundary was. The barrier's arrive has release and its wait acquire semantics at cluster scope, so a level's
+// writes to global memory are seen by every CTA of the cluster in the next. The per-column and per-target work is
+// the level kernels', in the same order: the results are theirs bit for bit.
+__global__ void __launch_bounds__(1024, 1) k_fem_factor_top(FemDev F, const int* __restrict__ lvl_col_ptr, const int* __restrict__ lvl_grp_ptr, int L0,
+                                                            int L1) {
     __shared__ double sPQ[32][72];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    cg::cluster_group cl = cg::this_cluster();
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int w = (int)cl.block_rank() * 32 + wl, nw = 32 * (int)cl.num_blocks();
     for (int L = L0; L < L1; L++) {
-        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += 32) chol_column(F, ci, lane);
-        __syncthreads();
-        for (int gi = lvl_grp_ptr[L] + w; gi < lvl_grp_ptr[L + 1]; gi += 32) update_group(F, gi, lane, sPQ[w]);
-        __syncthreads();
+        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += nw) chol_column(F, ci, lane);
+        cl.sync();
+        for (int gi = lvl_grp_ptr[L] + w; gi < lvl_grp_ptr[L + 1]; gi += nw) update_group(F, gi, lane, sPQ[wl]);
+        cl.sync();
     }
 }
 
-__global__ void __launch_bounds__(1024) k_fem_forward_tail(FemDev F, const int* __restrict__ lvl_col_ptr, int L0, int L1) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+// Both substitutions over the top levels [L0, L1), as k_fem_factor_top: forward up the levels, then backward down.
+__global__ void __launch_bounds__(1024, 1) k_fem_subst_top(FemDev F, const int* __restrict__ lvl_col_ptr, int L0, int L1) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int lane = threadIdx.x & 31;
+    const int w = (int)cl.block_rank() * 32 + (threadIdx.x >> 5), nw = 32 * (int)cl.num_blocks();
     for (int L = L0; L < L1; L++) {
-        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += 32) forward_column(F, ci, lane);
-        __syncthreads();
+        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += nw) forward_column(F, ci, lane);
+        cl.sync();
     }
-}
-
-__global__ void __launch_bounds__(1024) k_fem_backward_tail(FemDev F, const int* __restrict__ lvl_col_ptr, int L0, int L1) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int L = L1 - 1; L >= L0; L--) {
-        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += 32) backward_column(F, ci, lane);
-        __syncthreads();
+        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += nw) backward_column(F, ci, lane);
+        cl.sync();
     }
 }
 

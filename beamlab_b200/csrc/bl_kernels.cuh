@@ -251,13 +251,21 @@ __global__ void k_frame_begin(Body* __restrict__ bodies, int nbodies, Statics st
 
 // ------------------------------------------------------------------------------------------ per substep
 // SoftBody::compute_beam_forces, one beam (softbody.cpp:412-470), from its loaded state: meta, s0 = (L, max_pos,
-// max_neg, strength), c = (k, d), its ends' states. The beam's force on its end a is dis * fsc[j] (dis = p_a - p_b), on
-// b its negative; fsc[j] = kNoPush when the beam does not push this substep.
-__device__ __forceinline__ void beam_step(int j, uint32_t meta, float4 s0, float2 c, float4 pa, float4 va, float4 pb, float4 vb, float4* __restrict__ bst,
-                                          uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
-                                          const int* __restrict__ bbody, float* __restrict__ fsc, Body* __restrict__ bodies) {
-    if (meta & kBeamAsleep) return;
-    float out = kNoPush;
+// max_neg, strength), c = (k, d), its ends' states. Nothing is written: the caller stores what BeamOut says. The
+// beam's force on its end a is dis * sc (dis = p_a - p_b), on b its negative; sc = kNoPush when the beam does not push.
+struct BeamOut {
+    float sc;          // force scalar (kNoPush: none)
+    float slen;        // Beam::stress (stored when wr_stress)
+    float4 s;          // L, max_pos, max_neg, strength after the substep (stored when changed)
+    uint32_t meta;     // the meta word after the substep (stored when broke)
+    bool wr_stress, changed, broke;
+};
+
+__device__ __forceinline__ BeamOut beam_eval(int j, uint32_t meta, float4 s0, float2 c, float4 pa, float4 va, float4 pb, float4 vb,
+                                             const float4* __restrict__ bcold) {
+    BeamOut o;
+    o.sc = kNoPush, o.slen = 0.0f, o.s = s0, o.meta = meta, o.wr_stress = false, o.changed = false, o.broke = false;
+    if (meta & kBeamAsleep) return o;
     const uint32_t type = meta & 0xffu;
     uint32_t flags = (meta >> 8) & 0xffu;
     if (!(flags & (BF_BROKEN | BF_SHOCK))) {
@@ -305,22 +313,37 @@ __device__ __forceinline__ void beam_step(int j, uint32_t meta, float4 s0, float
                         changed = true;
                     }
                 }
-                if (changed) bst[j] = s;
+                o.s = s, o.changed = changed;
                 if (brk && fabsf(slen) > s.w && !(flags & BF_NO_BREAK)) {
                     broke = true;
                 } else {
-                    stress[j] = slen;
-                    out = slen * inv_len; // (the force on a is dis * out: k_force makes dis again from the same positions)
+                    o.wr_stress = true, o.slen = slen;
+                    o.sc = slen * inv_len; // (the force on a is dis * sc: the node's sum makes dis again from the same positions)
                 }
             }
             if (broke) {
                 flags |= BF_BROKEN;
-                bmeta[j] = (meta & ~(0xffu << 8)) | (flags << 8);
-                atomicAdd(&bodies[bbody[j]].broken_beams, 1);
+                o.meta = (meta & ~(0xffu << 8)) | (flags << 8);
+                o.broke = true;
             }
         }
     }
-    fsc[j] = out;
+    return o;
+}
+
+// beam_eval with its results stored at once (k_beams: the next kernel reads the scalar from fsc)
+__device__ __forceinline__ void beam_step(int j, uint32_t meta, float4 s0, float2 c, float4 pa, float4 va, float4 pb, float4 vb, float4* __restrict__ bst,
+                                          uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
+                                          const int* __restrict__ bbody, float* __restrict__ fsc, Body* __restrict__ bodies) {
+    if (meta & kBeamAsleep) return;
+    const BeamOut o = beam_eval(j, meta, s0, c, pa, va, pb, vb, bcold);
+    if (o.changed) bst[j] = o.s;
+    if (o.wr_stress) stress[j] = o.slen;
+    if (o.broke) {
+        bmeta[j] = o.meta;
+        atomicAdd(&bodies[bbody[j]].broken_beams, 1);
+    }
+    fsc[j] = o.sc;
 }
 
 // Two beams a thread (j and j + blockDim.x of the block's pair of tiles): both beams' loads are issued before either
@@ -397,6 +420,25 @@ __device__ __forceinline__ void accumulate_bounds(Body* __restrict__ bodies, int
     }
 }
 
+// A frame node's force: its triangles' corner forces and torques added in the reference's order (gather_forces,
+// frame_fem.cpp:2080-2105) after gravity and its beams; kept in nforce for the frame's implicit step.
+__device__ __forceinline__ void fem_gather(const NodeFem& nf, int i, v3 f) {
+    const int fs = nf.fslot[i];
+    if (fs >= 0) {
+        const int k = nf.iperm[fs];
+        v3 tq = V(0, 0, 0);
+        for (int g = nf.gdiag_ptr[k]; g < nf.gdiag_ptr[k + 1]; g++) {
+            const int2 e = nf.gdiag[g];
+            if (!nf.ton[e.x]) continue;
+            const float4 tf = nf.tf[3 * e.x + e.y], tt = nf.tt[3 * e.x + e.y];
+            f = V(f.x + tf.x, f.y + tf.y, f.z + tf.z);
+            tq = V(tq.x + tt.x, tq.y + tt.y, tq.z + tt.z);
+        }
+        nf.torque[fs] = make_float4(tq.x, tq.y, tq.z, 0.0f);
+    }
+    nf.nforce[i] = make_float4(f.x, f.y, f.z, 0.0f);
+}
+
 // A node's force: clear_forces' gravity (and any constant node force), then its beams in beam order
 // (softbody.cpp:376, 466-467); each beam's force made again from the beam's scalar and the two positions, as k_beams
 // made it. ell: the nodes' incidences (beam | bit 31 when the node is the beam's b end, the other end). Into fnode
@@ -450,20 +492,7 @@ __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd,
             if (B.is_fem) {
                 live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)
                 if (first) v2 = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
-                const int fs = nf.fslot[i];
-                if (fs >= 0) {
-                    const int k = nf.iperm[fs];
-                    v3 tq = V(0, 0, 0);
-                    for (int g = nf.gdiag_ptr[k]; g < nf.gdiag_ptr[k + 1]; g++) {
-                        const int2 e = nf.gdiag[g];
-                        if (!nf.ton[e.x]) continue;
-                        const float4 tf = nf.tf[3 * e.x + e.y], tt = nf.tt[3 * e.x + e.y];
-                        f = V(f.x + tf.x, f.y + tf.y, f.z + tf.z);
-                        tq = V(tq.x + tt.x, tq.y + tt.y, tq.z + tt.z);
-                    }
-                    nf.torque[fs] = make_float4(tq.x, tq.y, tq.z, 0.0f);
-                }
-                nf.nforce[i] = make_float4(f.x, f.y, f.z, 0.0f);
+                fem_gather(nf, i, f);
             } else {
                 fnode[i] = make_float4(f.x, f.y, f.z, 0.0f);
             }

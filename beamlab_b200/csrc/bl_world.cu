@@ -121,7 +121,8 @@ struct bl_gpu_ctx {
     DevBuf<long long> piters;
     DevBuf<float> guess, gscale;               // the learned per-frame-node dv guess (3) and preconditioner scale (9)
     int pcg_grid = 1;
-    int tail_level = 0;                        // from this level up the tree is narrow: one block takes it
+    int tail_level = 0;                        // from this level up the tree is narrow: one cluster launch takes it
+    int fem_cluster = 0;                       // CTAs of that launch's cluster (0: not chosen yet)
     DevBuf<int> d_lvl_col_ptr, d_lvl_grp_ptr;
     cudaStream_t aux = nullptr;                // (captures the bodies of conditional graph nodes)
     // the learned warm start (bl_mlp.cuh): parameters, the step's features, recorded samples, training scratch
@@ -483,12 +484,42 @@ static int commit_fem(bl_gpu_ctx* c) {
         c->lvl_col_ptr.push_back((int)lvl_col.size());
     }
     // begin, triangles, assembly, per level a factor (and an update) kernel and two substitutions, velocities, integration
-    // the narrow top of the tree (every level from it on at most kTail columns and update targets) goes to one block
-    const int kTail = 96;
+    // the top of the tree (every level from it on at most kTopCols columns and kTopGroups update targets) goes to one
+    // cluster launch for the factorization and one for the substitutions; the levels below, a launch each
+    const int kTopCols = 256, kTopGroups = 4096;
     int tail = nlev;
-    while (tail > 0 && c->lvl_col_ptr[tail] - c->lvl_col_ptr[tail - 1] <= kTail && c->lvl_grp_ptr[tail] - c->lvl_grp_ptr[tail - 1] <= kTail) tail--;
+    if (c->cfg.fem_top_level >= 0) {
+        tail = std::min(nlev, (int)c->cfg.fem_top_level);
+    } else {
+        while (tail > 0 && c->lvl_col_ptr[tail] - c->lvl_col_ptr[tail - 1] <= kTopCols && c->lvl_grp_ptr[tail] - c->lvl_grp_ptr[tail - 1] <= kTopGroups)
+            tail--;
+    }
     c->tail_level = tail;
-    c->chol_launches = 3 * (int64_t)tail + (tail < nlev ? 3 : 0);
+    if (tail < nlev && c->fem_cluster == 0) {
+        // the largest cluster (of 16, 8, 4, 2, 1 CTAs of 1024 threads) the device can run
+        int want = c->cfg.fem_cluster > 0 ? std::min(16, (int)c->cfg.fem_cluster) : 16;
+        for (int cl = want; cl >= 1; cl /= 2) {
+            if (cl > 8) {
+                BL_CUDA(c, cudaFuncSetAttribute(k_fem_factor_top, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+                BL_CUDA(c, cudaFuncSetAttribute(k_fem_subst_top, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            }
+            cudaLaunchConfig_t lc{};
+            lc.gridDim = dim3(cl), lc.blockDim = dim3(1024);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = cl, at[0].val.clusterDim.y = 1, at[0].val.clusterDim.z = 1;
+            lc.attrs = at, lc.numAttrs = 1;
+            int n1 = 0, n2 = 0;
+            if (cudaOccupancyMaxActiveClusters(&n1, k_fem_factor_top, &lc) == cudaSuccess && n1 >= 1 &&
+                cudaOccupancyMaxActiveClusters(&n2, k_fem_subst_top, &lc) == cudaSuccess && n2 >= 1) {
+                c->fem_cluster = cl;
+                break;
+            }
+            cudaGetLastError();
+        }
+        if (c->fem_cluster == 0) return BL_GPU_ECUDA;
+    }
+    c->chol_launches = 3 * (int64_t)tail + (tail < nlev ? 2 : 0);
     for (int L = 0; L < tail; L++) c->chol_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
     c->fem_launches = 5 + c->chol_launches;
     {   // each row's blocks in the order of their columns
@@ -888,6 +919,19 @@ static void launch_pcg(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle
     cudaLaunchKernelEx(&lc, k_fem_pcg, c->fd, P);
 }
 
+// The top of the elimination tree, levels [L0, L1), in one launch of a cluster of fem_cluster CTAs: its factorization
+// (k_fem_factor_top) or both its substitutions (k_fem_subst_top).
+static void launch_top(bl_gpu_ctx* c, cudaStream_t s, bool factor, int L0, int L1) {
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(c->fem_cluster), lc.blockDim = dim3(1024), lc.dynamicSmemBytes = 0, lc.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = c->fem_cluster, at[0].val.clusterDim.y = 1, at[0].val.clusterDim.z = 1;
+    lc.attrs = at, lc.numAttrs = 1;
+    if (factor) cudaLaunchKernelEx(&lc, k_fem_factor_top, c->fd, (const int*)c->d_lvl_col_ptr.p, (const int*)c->d_lvl_grp_ptr.p, L0, L1);
+    else cudaLaunchKernelEx(&lc, k_fem_subst_top, c->fd, (const int*)c->d_lvl_col_ptr.p, L0, L1);
+}
+
 static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev = nullptr) {
     int q = 0;
     auto mark = [&]() {
@@ -914,12 +958,12 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             }
         }
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
-        k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p,
-                                               c->M, c->B);
+        k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
+                                               c->dbodies.p, c->M, c->B);
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
-        k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0], c->cfg.gravity[1],
-                                               c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
+        k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0],
+                                               c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
         mark();
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
@@ -950,15 +994,12 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                     k_fem_chol_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
                     if (g1 > g0) k_fem_update_level<<<(g1 - g0 + 3) / 4, 128, 0, cs>>>(F, g0, g1);
                 }
-                if (tail < nlev) k_fem_factor_tail<<<1, 1024, 0, cs>>>(F, c->d_lvl_col_ptr.p, c->d_lvl_grp_ptr.p, tail, nlev);
+                if (tail < nlev) launch_top(c, cs, true, tail, nlev);
                 for (int L = 0; L < tail; L++) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
                     k_fem_forward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
                 }
-                if (tail < nlev) {
-                    k_fem_forward_tail<<<1, 1024, 0, cs>>>(F, c->d_lvl_col_ptr.p, tail, nlev);
-                    k_fem_backward_tail<<<1, 1024, 0, cs>>>(F, c->d_lvl_col_ptr.p, tail, nlev);
-                }
+                if (tail < nlev) launch_top(c, cs, false, tail, nlev);
                 for (int L = tail - 1; L >= 0; L--) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
                     k_fem_backward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
@@ -1067,6 +1108,9 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->pcg_tol = 1e-6f;
     cfg->fem_check_residual = 0;
     cfg->pcg_learned_scale = 0;
+    cfg->graphs = 1;
+    cfg->fem_top_level = -1;
+    cfg->fem_cluster = 0;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -1092,7 +1136,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
     if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 3 || c0.pcg_max_iters < 0 ||
-        !(c0.pcg_tol > 0))
+        !(c0.pcg_tol > 0) || c0.fem_top_level < -1 || c0.fem_cluster < 0 || c0.fem_cluster > 16 || (c0.fem_cluster & (c0.fem_cluster - 1)) != 0)
         return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
@@ -1280,6 +1324,14 @@ int bl_gpu_step_substeps(bl_gpu_ctx* c, int32_t n, void* stream) {
     c->total_substeps += n;
     if (c->B == 0) return BL_GPU_OK;
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    if (!c->cfg.graphs) {
+        // the plain path: every kernel of the frame launched on s, no capture (a PCG fallback always factors)
+        if ((rc = order_on(c, s))) return rc;
+        enqueue_frame(c, n, s);
+        BL_CUDA(c, cudaGetLastError());
+        c->launches += frame_launches(c, n);
+        return BL_GPU_OK;
+    }
     auto it = c->graphs.find(n);
     if (it == c->graphs.end()) {
         // capture the frame once on the context's stream, replay it from then on

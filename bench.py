@@ -57,12 +57,6 @@ def workload(name: str, rank: int):
         desc = ("plate64: co-rotational FEM shell plate, 64 x 64 nodes (4,096), 7,938 CST/DKT triangles, 1 m x 1 m, "
                 "1.5 mm steel (E 210 GPa, nu 0.3, 7,850 kg/m^3), one edge clamped, a seeded 500 N point load, gravity; "
                 "implicit step every substep: 64,411 off-diagonal 6x6 blocks, 1,359,082 block updates")
-    elif name == "plate64":
-        rig = rigs.shell_plate(63, seed=1 + rank)
-        n, m = rigs.rig_counts(rig)
-        desc = ("plate64: co-rotational FEM shell plate, 64 x 64 nodes (4,096), 7,938 CST/DKT triangles, 1 m x 1 m, "
-                "1.5 mm steel (E 210 GPa, nu 0.3, 7,850 kg/m^3), one edge clamped, a seeded 500 N point load, gravity; "
-                "implicit step every substep: 64,411 off-diagonal 6x6 blocks, 1,359,082 block updates")
     elif name == "truss_car":
         rig = rigs.truss_car(1 + rank)
         n, m = rigs.rig_counts(rig)
@@ -192,6 +186,37 @@ def fem_solvers(device: int, frames: int = 2):
                        "cg_iterations_per_solve": st["pcg_iterations"] / st["pcg_solves"] if st["pcg_solves"] else None,
                        "fallbacks": st["pcg_fallbacks"]}
         w.close()
+    return out
+
+
+def plain_gpu(rig, device: int, stream, sample_every: int = 8, frames: int = 3):
+    """The plain per-instance GPU path the batched one is measured against: every sample_every-th vehicle of the
+    workload in a World of its own (its own context, the same terrain), the worlds stepped one after another on one
+    stream, each frame's kernels launched one by one (graphs off) - and, for reference, the same with each world's
+    frame replayed as a CUDA graph. node-substeps/s of the sample (CUDA events on the stream)."""
+    import torch
+    from beamlab_b200 import world_from_rig
+    sample = rig["bodies"][::sample_every]
+    nodes = sum(len(b["mass"]) for b in sample)
+    out = {"sample": f"{len(sample)} of the {len(rig['bodies'])} vehicles (every {sample_every}th: {nodes:,} nodes), "
+                     f"{frames} frames of {FRAME} substeps each, a World per vehicle"}
+    for key, graphs in (("launches", False), ("graphs", True)):
+        worlds = [world_from_rig({"settings": rig["settings"], "statics": rig["statics"], "bodies": [b]}, device=device,
+                                 graphs=graphs) for b in sample]
+        for w in worlds:  # (warm-up: commits, and captures the graph where on)
+            w.step_substeps(FRAME, stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(frames):
+            for w in worlds:
+                w.step_substeps(FRAME, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[key] = {"value": nodes * FRAME * frames / (ms * 1e-3), "unit": UNIT, "ms_per_frame": ms / frames}
+        for w in worlds:
+            w.close()
     return out
 
 
@@ -352,6 +377,10 @@ def run_gpu(args):
         }
         if ws == 1 and args.workload == "plate64":
             out["fem_solvers"] = fem_solvers(local)
+        if ws == 1 and args.workload == "fleet256" and not args.no_plain:
+            pl = plain_gpu(rig, local, stream)
+            pl["batched_over_plain"] = value / pl["launches"]["value"]
+            out["plain_gpu"] = pl
         if ws == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_reference(rig, n)
         print(json.dumps(out), flush=True)
@@ -368,6 +397,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="fleet256", choices=["fleet256", "plate64", "truss_car"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-instance GPU path's measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")

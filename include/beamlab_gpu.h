@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define BL_GPU_ABI_VERSION 2
+#define BL_GPU_ABI_VERSION 3
 
 enum {
     BL_GPU_OK = 0,
@@ -80,6 +80,14 @@ typedef struct {
                                    step took (bl_gpu_fem_stats); costs a copy of the system a substep */
     int32_t pcg_learned_scale; /* BL_GPU_FEM_PCG_LEARNED: 1 the learned 3x3 scale of the block preconditioner, 0 (default)
                                   none - measured on the plates, the scale as trained costs iterations */
+    int32_t graphs;            /* 1 (default): a frame of n substeps is captured once as a CUDA graph and replayed; 0: its
+                                  kernels are launched one by one every call (the plain path, one launch per kernel) */
+    int32_t fem_top_level;     /* the FEM frames' block Cholesky runs its elimination tree's levels below this one a launch
+                                  each and the levels from it to the top in one cluster launch (and the substitutions
+                                  alike); -1 (default): the first level from which every level is narrow (at most 256
+                                  columns and 4096 updated blocks). Results are the same for every value. */
+    int32_t fem_cluster;       /* CTAs (1024 threads each) of that cluster launch: 1, 2, 4, 8 or 16; 0 (default): the
+                                  largest the device can run */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };

@@ -3,6 +3,7 @@ have the reference's layouts, and the host mirror builds bodies as the reference
 import ctypes as C
 import os
 import subprocess
+import tempfile
 
 import numpy as np
 import pytest
@@ -18,13 +19,14 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 20
     for n in names:
         assert hasattr(L, n), n
-    assert L.bl_gpu_abi_version() == 2
+    assert L.bl_gpu_abi_version() == 3
     assert L.bl_gpu_error_string(-4).decode() == "unsupported feature"
 
 
 def _c_layout():
     """sizeof / offsetof of the header's records, from a C compiler."""
-    src = os.path.join(ROOT, "_work", "abi_layout.c") if os.path.isdir(os.path.join(ROOT, "_work")) else "/tmp/abi_layout.c"
+    tmp = tempfile.mkdtemp(prefix="bl_abi_")
+    src = os.path.join(tmp, "abi_layout.c")
     exe = src[:-2]
     with open(src, "w") as f:
         f.write('#include <stdio.h>\n#include <stddef.h>\n#include "beamlab_gpu.h"\n'
