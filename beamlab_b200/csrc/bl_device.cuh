@@ -25,7 +25,7 @@ enum : uint32_t { BT_NORMAL = 0, BT_ROPE = 1, BT_SUPPORT = 2 };
 enum : uint32_t { BF_BROKEN = 1, BF_NO_DEFORM = 4, BF_NO_BREAK = 8, BF_SHOCK = 64 };
 // body bits kept in each beam's meta word (bits 16-18): the body's allow_deform / allow_break / ductile
 enum : uint32_t { BB_DEFORM = 1u << 16, BB_BREAK = 1u << 17, BB_DUCTILE = 1u << 18 };
-enum : uint32_t { DEVERR_CANDIDATES = 1, DEVERR_NONFINITE = 2 };
+enum : uint32_t { DEVERR_CANDIDATES = 1, DEVERR_NONFINITE = 2, DEVERR_TIMEOUT = 1u << 6 };
 
 // Ground model (GroundModel, static_world.h:18-31): the values of ground_models() (static_world.cpp:85-114)
 struct GroundModel {

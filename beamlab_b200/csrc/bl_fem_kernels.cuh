@@ -6,12 +6,12 @@
 //                      (tri_kinematics + eval_tris, frame_fem.cpp:1584-1621, 1661-1831; elastic sections)
 //   (k_force)          the frame bodies' node forces, their triangles' forces and torques gathered in the reference's
 //                      order (gather_forces, frame_fem.cpp:2080-2105)
-//   k_fem_assemble     columns: the blocks of (M + (theta h^2 + beta h) K + theta h^2 Kg) and the right side
+//   k_fem_assemble_all columns and blocks: the blocks of (M + (theta h^2 + beta h) K + theta h^2 Kg) and the right side
 //                      h f - (theta_d h^2 + beta h) K v (gather_part, frame_fem.cpp:916-1086)
-//   k_fem_chol_level / k_fem_update_level: the right-looking block Cholesky level by level of the elimination tree:
-//                      the level's columns factored (chol6, right_solve_lt), then their updates T -= P Q^T, one warp
-//                      per target block (frame_fem.cpp:2193-2220, 2887-2919)
-//   k_fem_forward_level / k_fem_backward_level: L y = r and L^T x = y by levels (frame_fem.cpp:2944-2954)
+//   k_fem_chol_level / k_fem_update_forward_level: the right-looking block Cholesky level by level of the elimination
+//                      tree: the level's columns factored (chol6, right_solve_lt), then their updates T -= P Q^T, one
+//                      warp per target block (frame_fem.cpp:2193-2220, 2887-2919), with the level's L y = r
+//   k_fem_backward_level: L^T x = y by levels, from the top down (frame_fem.cpp:2944-2954)
 //   k_fem_velocity     columns: the new velocities to forces m dv / step, spins advanced, safety clamps
 //                      (frame_fem.cpp:2998-3025)
 //   k_fem_integrate    the frame bodies' nodes: SoftBody::integrate_nodes, then FemFrame::sync_positions
@@ -21,13 +21,9 @@
 // within a tolerance, not bitwise.
 #pragma once
 
-#include <cooperative_groups.h>
-
 #include "bl_device.cuh"
 
 namespace blg {
-
-namespace cg = cooperative_groups;
 
 struct FemSecDev {
     float E, nu, rho, t, damping, drill;
@@ -58,11 +54,13 @@ struct FemDev {
     const FemSecDev* sec;
     const int* col_ptr;
     const int* row;
+    const int* blk_col;      // block -> its column
     const int* gdiag_ptr;
     const int2* gdiag;       // (triangle, corner)
     const int* goff_ptr;
     const int4* goff;        // (triangle, row corner, column corner)
-    double* diag;            // 36 / column
+    double* diag;            // 36 / column: the assembled diagonal blocks (updated in place as the factor proceeds)
+    double* ldiag;           // 36 / column: the factored diagonal blocks
     double* off;             // 36 / block
     double* rhs;             // 6 / column
     double* dinv;            // 6 / column
@@ -323,10 +321,8 @@ __device__ void tri_block_add(const FemDev& F, int t, int i, int j, double h2, d
         for (int pp = 0; pp < 3; pp++) D[pp * 7] += gg;
 }
 
-// One column's diagonal block, right side and off-diagonal blocks; nforce: the nodes' forces of the substep
-__global__ void k_fem_assemble(FemDev F, const float4* __restrict__ nd, const float4* __restrict__ nforce) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= F.nf) return;
+// One column's diagonal block and right side; nforce: the nodes' forces of the substep
+__device__ __forceinline__ void assemble_column(const FemDev& F, const float4* __restrict__ nd, const float4* __restrict__ nforce, int k) {
     const int i = F.perm[k];
     const int bn = F.fnode[i];
     const float4 P = nd[2 * bn], Vv = nd[2 * bn + 1];
@@ -361,18 +357,31 @@ __global__ void k_fem_assemble(FemDev F, const float4* __restrict__ nd, const fl
     }
     double* Dg = F.diag + 36 * (size_t)k;
     for (int x = 0; x < 36; x++) Dg[x] = D[x];
-    for (int pb = F.col_ptr[k]; pb < F.col_ptr[k + 1]; pb++) {
-        double O[36];
-        for (int x = 0; x < 36; x++) O[x] = 0.0;
-        const int rnode = F.fnode[F.perm[F.row[pb]]];
-        if (!fixed && F.goff_ptr[pb] != F.goff_ptr[pb + 1] && !(nd[2 * rnode].w <= 0))
-            for (int qq = F.goff_ptr[pb]; qq < F.goff_ptr[pb + 1]; qq++) {
-                const int4 g = F.goff[qq];
-                if (F.ton[g.x]) tri_block_add(F, g.x, g.y, g.z, h2, O);
-            }
-        double* Og = F.off + 36 * (size_t)pb;
-        for (int x = 0; x < 36; x++) Og[x] = O[x];
-    }
+}
+
+// The off-diagonal blocks, a thread each (pb: the block; its column from blk_col): zero where a corner is fixed, else
+// the sum of its triangles' blocks in their order
+__device__ __forceinline__ void assemble_off(const FemDev& F, const float4* __restrict__ nd, int pb) {
+    const int k = F.blk_col[pb];
+    const double h2 = F.ch2[k];
+    double O[36];
+    for (int x = 0; x < 36; x++) O[x] = 0.0;
+    const bool fixed = nd[2 * F.fnode[F.perm[k]]].w <= 0;
+    const int rnode = F.fnode[F.perm[F.row[pb]]];
+    if (!fixed && F.goff_ptr[pb] != F.goff_ptr[pb + 1] && !(nd[2 * rnode].w <= 0))
+        for (int qq = F.goff_ptr[pb]; qq < F.goff_ptr[pb + 1]; qq++) {
+            const int4 g = F.goff[qq];
+            if (F.ton[g.x]) tri_block_add(F, g.x, g.y, g.z, h2, O);
+        }
+    double* Og = F.off + 36 * (size_t)pb;
+    for (int x = 0; x < 36; x++) Og[x] = O[x];
+}
+
+// The columns' diagonal blocks and right sides (threads [0, nf)) and the off-diagonal blocks (threads [nf, nf + nblk))
+__global__ void __launch_bounds__(128) k_fem_assemble_all(FemDev F, const float4* __restrict__ nd, const float4* __restrict__ nforce) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < F.nf) assemble_column(F, nd, nforce, t);
+    else if (t < F.nf + F.nblk) assemble_off(F, nd, t - F.nf);
 }
 
 // ------------------------------------------------------------------------------------------ factorization
@@ -395,27 +404,46 @@ __device__ bool chol6_dev(double* A, double* dinv) {
     return true;
 }
 
-// The level's columns, one warp each: chol6 of the diagonal block (lane 0), then every row of the column's
-// off-diagonal blocks against it, X := X L^-T (right_solve_lt, frame_fem.cpp:2211-2220), rows over the lanes
-__device__ __forceinline__ void chol_column(const FemDev& F, int ci, int lane) {
+// The factorization's and substitutions' column work is done by units of 128 threads (4 warps) with a shared buffer
+// sm of 72 doubles and a barrier of their own (bar: a named barrier id, or 0 for a unit that is the whole block). A
+// unit takes one column (one slice of its rows, for the factor); the results do not depend on how units are launched.
+constexpr int kUnit = 128;
+__device__ __forceinline__ void unit_sync(int bar) {
+    if (bar == 0) __syncthreads();
+    else asm volatile("bar.sync %0, 128;" ::"r"(bar) : "memory");
+}
+
+// A column's factor, slice `slice` of `nslice` of its rows: the diagonal block (and its inverse diagonal) staged in
+// sm by the first warp, chol6 there by its first thread - every slice's unit factors it alike, and slice 0's stores
+// the factor in ldiag (the assembled diag stays as it is: another slice may still be reading it) - then the unit's
+// rows of the column's off-diagonal blocks against it, X := X L^-T (right_solve_lt, frame_fem.cpp:2211-2220), a row a
+// thread. The operations and their order are chol6's and right_solve_lt's.
+__device__ __forceinline__ void chol_unit(const FemDev& F, int ci, int slice, int nslice, int ut, int bar, double* sm) {
     const int k = F.lvl_col[ci];
-    double* Lkk = F.diag + 36 * (size_t)k;
-    double* dk = F.dinv + 6 * (size_t)k;
-    int ok = 1;
-    if (lane == 0) ok = chol6_dev(Lkk, dk);
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (!ok) {
-        if (lane == 0) atomicExch(&F.comp_fail[F.col_comp[k]], 1);
-        return;
+    unit_sync(bar); // (sm free)
+    if (ut < 32) {
+        const double* A = F.diag + 36 * (size_t)k;
+        sm[ut] = A[ut];
+        if (ut < 4) sm[32 + ut] = A[32 + ut];
+        if (ut < 6) sm[36 + ut] = F.dinv[6 * (size_t)k + ut];
+        __syncwarp();
+        if (ut == 0) sm[42] = chol6_dev(sm, sm + 36) ? 1.0 : 0.0;
     }
-    __syncwarp();
+    unit_sync(bar);
+    const bool ok = sm[42] != 0.0;
+    if (slice == 0) {
+        if (ut < 36) F.ldiag[36 * (size_t)k + ut] = sm[ut];
+        if (ut < 6) F.dinv[6 * (size_t)k + ut] = sm[36 + ut];
+        if (ut == 0 && !ok) atomicExch(&F.comp_fail[F.col_comp[k]], 1);
+    }
+    if (!ok) return;
     double L[21], di[6];
     for (int j = 0, x = 0; j < 6; j++) {
-        di[j] = dk[j];
-        for (int m = 0; m <= j; m++) L[x++] = Lkk[j * 6 + m];
+        di[j] = sm[36 + j];
+        for (int m = 0; m <= j; m++) L[x++] = sm[j * 6 + m];
     }
     const int nrows = 6 * (F.col_ptr[k + 1] - F.col_ptr[k]);
-    for (int rr = lane; rr < nrows; rr += 32) {
+    for (int rr = slice * kUnit + ut; rr < nrows; rr += nslice * kUnit) {
         double* xrow = F.off + 36 * (size_t)(F.col_ptr[k] + rr / 6) + 6 * (rr % 6);
         double x[6];
         for (int j = 0; j < 6; j++) x[j] = xrow[j];
@@ -429,15 +457,9 @@ __device__ __forceinline__ void chol_column(const FemDev& F, int ci, int lane) {
     }
 }
 
-__global__ void __launch_bounds__(128) k_fem_chol_level(FemDev F, int c0, int c1) {
-    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (ci >= c1) return;
-    chol_column(F, ci, threadIdx.x & 31);
-}
-
 // The level's columns' updates (the right-looking step of frame_fem.cpp:2910-2914), one warp per target block: the
 // updates this level's columns make to it, in the order of those columns, T -= P Q^T each (sub_abt's sums,
-// frame_fem.cpp:2276-2288). A target meets every level's updates in the order of the levels.
+// frame_fem.cpp:2276-2288). A target meets every level's updates in the order of the levels. pq: 72 doubles.
 __device__ __forceinline__ void update_group(const FemDev& F, int gi, int lane, double* pq) {
     const int tgt = F.grp_tgt[gi];
     double* T = tgt < F.nf ? F.diag + 36 * (size_t)tgt : F.off + 36 * (size_t)(tgt - F.nf);
@@ -467,25 +489,32 @@ __device__ __forceinline__ void update_group(const FemDev& F, int gi, int lane, 
     if (lane < 4) T[e1] = acc1;
 }
 
-__global__ void __launch_bounds__(128) k_fem_update_level(FemDev F, int g0, int g1) {
-    __shared__ double sPQ[4][72];
-    const int wib = threadIdx.x >> 5;
-    const int gi = g0 + blockIdx.x * 4 + wib;
-    if (gi >= g1) return;
-    update_group(F, gi, threadIdx.x & 31, sPQ[wib]);
-}
-
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
-// L y = r for the level's columns, one warp a column: the blocks in its row (from the columns before it) spread over
-// the lanes and summed, then forward6 (frame_fem.cpp:2304-2310, 2944-2948)
-__device__ __forceinline__ void forward_column(const FemDev& F, int ci, int lane) {
+// A unit's six partial sums s[] (one set a thread) to their total in thread 0's s[]: each warp's by a butterfly,
+// then the four warps' in order (sm[48..71])
+__device__ __forceinline__ void unit_sum6(double* s, int ut, int bar, double* sm) {
+    for (int j = 0; j < 6; j++) s[j] = warp_sum(s[j]);
+    if ((ut & 31) == 0)
+        for (int j = 0; j < 6; j++) sm[48 + 6 * (ut >> 5) + j] = s[j];
+    unit_sync(bar);
+    if (ut == 0)
+        for (int j = 0; j < 6; j++) s[j] = ((sm[48 + j] + sm[54 + j]) + sm[60 + j]) + sm[66 + j];
+}
+
+// L y = r for a column: the blocks in its row (from the columns before it) spread over the unit and summed, then
+// forward6 (frame_fem.cpp:2304-2310, 2944-2948) by the unit's first thread on the factored diagonal block, its
+// inverse diagonal and r, staged in sm while the row is summed.
+__device__ __forceinline__ void forward_unit(const FemDev& F, int ci, int ut, int bar, double* sm) {
     const int k = F.lvl_col[ci];
+    unit_sync(bar); // (sm free)
+    if (ut < 36) sm[ut] = F.ldiag[36 * (size_t)k + ut];
+    if (ut < 6) sm[36 + ut] = F.dinv[6 * (size_t)k + ut], sm[42 + ut] = F.rhs[6 * (size_t)k + ut];
     double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int q = F.rb_ptr[k] + lane; q < F.rb_ptr[k + 1]; q += 32) {
+    for (int q = F.rb_ptr[k] + ut; q < F.rb_ptr[k + 1]; q += kUnit) {
         const int2 bc = F.rb[q];
         const double* L = F.off + 36 * (size_t)bc.x;
         const double* yk = F.rhs + 6 * (size_t)bc.y;
@@ -495,32 +524,27 @@ __device__ __forceinline__ void forward_column(const FemDev& F, int ci, int lane
             s[ii] += t;
         }
     }
-    for (int j = 0; j < 6; j++) s[j] = warp_sum(s[j]);
-    if (lane != 0) return;
+    unit_sum6(s, ut, bar, sm);
+    if (ut != 0) return;
     double y[6];
-    for (int j = 0; j < 6; j++) y[j] = F.rhs[6 * (size_t)k + j] - s[j];
-    const double* Lkk = F.diag + 36 * (size_t)k;
-    const double* dk = F.dinv + 6 * (size_t)k;
+    for (int j = 0; j < 6; j++) y[j] = sm[42 + j] - s[j];
     for (int j = 0; j < 6; j++) {
         double t = y[j];
-        for (int m = 0; m < j; m++) t -= Lkk[j * 6 + m] * y[m];
-        y[j] = t * dk[j];
+        for (int m = 0; m < j; m++) t -= sm[j * 6 + m] * y[m];
+        y[j] = t * sm[36 + j];
     }
     for (int j = 0; j < 6; j++) F.rhs[6 * (size_t)k + j] = y[j];
 }
 
-__global__ void __launch_bounds__(128) k_fem_forward_level(FemDev F, int c0, int c1) {
-    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (ci >= c1) return;
-    forward_column(F, ci, threadIdx.x & 31);
-}
-
-// L^T x = y for the level's columns (the levels from the top down), one warp a column: its blocks' L^T x_row over
-// the lanes, summed, then backward6 (frame_fem.cpp:2296-2303, 2311-2317, 2949-2954)
-__device__ __forceinline__ void backward_column(const FemDev& F, int ci, int lane) {
+// L^T x = y for a column (the levels from the top down): its blocks' L^T x_row over the unit, summed, then backward6
+// (frame_fem.cpp:2296-2303, 2311-2317, 2949-2954) by the unit's first thread, staged as forward's.
+__device__ __forceinline__ void backward_unit(const FemDev& F, int ci, int ut, int bar, double* sm) {
     const int k = F.lvl_col[ci];
+    unit_sync(bar); // (sm free)
+    if (ut < 36) sm[ut] = F.ldiag[36 * (size_t)k + ut];
+    if (ut < 6) sm[36 + ut] = F.dinv[6 * (size_t)k + ut], sm[42 + ut] = F.rhs[6 * (size_t)k + ut];
     double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int pb = F.col_ptr[k] + lane; pb < F.col_ptr[k + 1]; pb += 32) {
+    for (int pb = F.col_ptr[k] + ut; pb < F.col_ptr[k + 1]; pb += kUnit) {
         const double* L = F.off + 36 * (size_t)pb;
         const double* xr = F.rhs + 6 * (size_t)F.row[pb];
         for (int j = 0; j < 6; j++) {
@@ -529,59 +553,42 @@ __device__ __forceinline__ void backward_column(const FemDev& F, int ci, int lan
             s[j] += t;
         }
     }
-    for (int j = 0; j < 6; j++) s[j] = warp_sum(s[j]);
-    if (lane != 0) return;
+    unit_sum6(s, ut, bar, sm);
+    if (ut != 0) return;
     double x[6];
-    for (int j = 0; j < 6; j++) x[j] = F.rhs[6 * (size_t)k + j] - s[j];
-    const double* Lkk = F.diag + 36 * (size_t)k;
-    const double* dk = F.dinv + 6 * (size_t)k;
+    for (int j = 0; j < 6; j++) x[j] = sm[42 + j] - s[j];
     for (int j = 5; j >= 0; j--) {
         double t = x[j];
-        for (int m = j + 1; m < 6; m++) t -= Lkk[m * 6 + j] * x[m];
-        x[j] = t * dk[j];
+        for (int m = j + 1; m < 6; m++) t -= sm[m * 6 + j] * x[m];
+        x[j] = t * sm[36 + j];
     }
     for (int j = 0; j < 6; j++) F.rhs[6 * (size_t)k + j] = x[j];
 }
 
-__global__ void __launch_bounds__(128) k_fem_backward_level(FemDev F, int c0, int c1) {
-    const int ci = c0 + blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (ci >= c1) return;
-    backward_column(F, ci, threadIdx.x & 31);
+// A level's columns' factors: block (x, y) takes the level's column c0 + x, slice y of gridDim.y of its rows
+__global__ void __launch_bounds__(kUnit) k_fem_chol_level(FemDev F, int c0) {
+    __shared__ double sm[72];
+    chol_unit(F, c0 + blockIdx.x, blockIdx.y, gridDim.y, threadIdx.x, 0, sm);
 }
 
-// The top of the elimination tree (levels [L0, L1), where the levels are narrow: down to chains of single columns)
-// in one launch of a thread-block cluster (cluster_n CTAs of 1024 threads, co-scheduled on cluster_n SMs): each
-// level's columns and update targets spread over all the cluster's warps, and a cluster barrier where a launch
-// boundary was. The barrier's arrive has release and its wait acquire semantics at cluster scope, so a level's
-// writes to global memory are seen by every CTA of the cluster in the next. The per-column and per-target work is
-// the level kernels', in the same order: the results are theirs bit for bit.
-__global__ void __launch_bounds__(1024, 1) k_fem_factor_top(FemDev F, const int* __restrict__ lvl_col_ptr, const int* __restrict__ lvl_grp_ptr, int L0,
-                                                            int L1) {
-    __shared__ double sPQ[32][72];
-    cg::cluster_group cl = cg::this_cluster();
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    const int w = (int)cl.block_rank() * 32 + wl, nw = 32 * (int)cl.num_blocks();
-    for (int L = L0; L < L1; L++) {
-        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += nw) chol_column(F, ci, lane);
-        cl.sync();
-        for (int gi = lvl_grp_ptr[L] + w; gi < lvl_grp_ptr[L + 1]; gi += nw) update_group(F, gi, lane, sPQ[wl]);
-        cl.sync();
+// A level's updates and its forward substitution in one launch (independent: the updates write blocks of later
+// columns, the substitution reads this level's and earlier columns' factors): blocks [0, ceil((g1 - g0) / 4)) take
+// the update targets (a warp each), the rest a column each.
+__global__ void __launch_bounds__(kUnit) k_fem_update_forward_level(FemDev F, int g0, int g1, int c0) {
+    __shared__ double sm[4][72];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nub = (g1 - g0 + 3) / 4;
+    if ((int)blockIdx.x < nub) {
+        const int gi = g0 + blockIdx.x * 4 + wib;
+        if (gi < g1) update_group(F, gi, lane, sm[wib]);
+    } else {
+        forward_unit(F, c0 + blockIdx.x - nub, threadIdx.x, 0, sm[0]);
     }
 }
 
-// Both substitutions over the top levels [L0, L1), as k_fem_factor_top: forward up the levels, then backward down.
-__global__ void __launch_bounds__(1024, 1) k_fem_subst_top(FemDev F, const int* __restrict__ lvl_col_ptr, int L0, int L1) {
-    cg::cluster_group cl = cg::this_cluster();
-    const int lane = threadIdx.x & 31;
-    const int w = (int)cl.block_rank() * 32 + (threadIdx.x >> 5), nw = 32 * (int)cl.num_blocks();
-    for (int L = L0; L < L1; L++) {
-        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += nw) forward_column(F, ci, lane);
-        cl.sync();
-    }
-    for (int L = L1 - 1; L >= L0; L--) {
-        for (int ci = lvl_col_ptr[L] + w; ci < lvl_col_ptr[L + 1]; ci += nw) backward_column(F, ci, lane);
-        cl.sync();
-    }
+__global__ void __launch_bounds__(kUnit) k_fem_backward_level(FemDev F, int c0) {
+    __shared__ double sm[72];
+    backward_unit(F, c0 + blockIdx.x, threadIdx.x, 0, sm);
 }
 
 // ------------------------------------------------------------------------------------------ after the solve

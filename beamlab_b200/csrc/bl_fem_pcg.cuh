@@ -1,6 +1,6 @@
 // The implicit FEM step solved by preconditioned conjugate gradients, and the solve's residual.
 //
-// (A dv = rhs: the system k_fem_assemble leaves in diag / off / rhs - M + (theta h^2 + beta h) K + theta h^2 Kg over
+// (A dv = rhs: the system k_fem_assemble_all leaves in diag / off / rhs - M + (theta h^2 + beta h) K + theta h^2 Kg over
 // the frame's 6-DOF nodes, frame_fem.cpp:916-1086 - in the factor's column order.) The reference solves it by the
 // block Cholesky (frame_fem.cpp:2887-2954), which this library runs as the default and as the judge. k_fem_pcg solves
 // the same system by CG with a block-Jacobi preconditioner (each column's 6 x 6 diagonal block, its translational 3 x 3

@@ -371,6 +371,128 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
     if (h1) beam_step(j1, m1, s1, c1, pa1, va1, pb1, vb1, bst, bmeta, bcold, stress, bbody, fsc, bodies);
 }
 
+// ------------------------------------------------------------------------------------------ bulk copies (TMA)
+// cp.async.bulk global -> shared completing on an mbarrier: the beam arrays stream into shared memory tile after tile
+// while the block computes earlier tiles. Every wait is bounded in time (kWaitNs): a copy that never lands raises
+// DEVERR_TIMEOUT and the block stops instead of waiting for ever.
+constexpr unsigned long long kWaitNs = 1000000000ull; // 1 s
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// bytes and both addresses multiples of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// the generic proxy's reads of a buffer ordered before the async proxy's next writes into it
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// waits for the phase of `parity` to complete; false after kWaitNs
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    uint32_t done = 0;
+    unsigned long long t0 = 0;
+    for (int it = 0;; it++) {
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (done) return true;
+        if (it == 0) t0 = global_ns();
+        else if (global_ns() - t0 > kWaitNs) return false;
+    }
+}
+
+// k_beams with the beam arrays staged by bulk copies: a persistent block takes every gridDim.x-th tile of kBeamTile
+// beams; kBeamStages tiles are in flight while it computes (one thread issues the copies: each tile's a/b ends, k/d,
+// state and meta words, 18 KB). The beam arrays are padded to whole tiles (pads asleep). Per beam the same
+// beam_step as k_beams.
+constexpr int kBeamTile = 512;
+constexpr int kBeamStages = 3;
+constexpr int kBeamThreads = 256;
+struct BeamStage {
+    int2 ab[kBeamTile];
+    float2 kd[kBeamTile];
+    float4 bst[kBeamTile];
+    uint32_t meta[kBeamTile];
+};
+constexpr size_t kBeamSmem = kBeamStages * sizeof(BeamStage) + kBeamStages * sizeof(uint64_t);
+
+__global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
+                                                            uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
+                                                            const int* __restrict__ bbody, float* __restrict__ fsc, const float4* __restrict__ nd,
+                                                            Body* __restrict__ bodies, int nbeams, int nbodies, int ntiles, uint32_t* __restrict__ deverr) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    BeamStage* stg = reinterpret_cast<BeamStage*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kBeamStages * sizeof(BeamStage));
+    const int tid = threadIdx.x;
+    for (int t = blockIdx.x * kBeamThreads + tid; t < nbodies; t += gridDim.x * kBeamThreads) {
+        Body& B = bodies[t]; // (this substep's bounds accumulator, for k_integrate)
+        B.acc_mn[0] = B.acc_mn[1] = B.acc_mn[2] = 1e30f;
+        B.acc_mx[0] = B.acc_mx[1] = B.acc_mx[2] = -1e30f;
+    }
+    const int mine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    if (tid == 0) {
+        for (int s = 0; s < kBeamStages; s++) mbar_init(&full[s], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    auto issue = [&](int i) { // this block's i-th tile into stage i % kBeamStages
+        const int s = i % kBeamStages;
+        const size_t j0 = (size_t)(blockIdx.x + (size_t)i * gridDim.x) * kBeamTile;
+        mbar_expect_tx(&full[s], (uint32_t)(sizeof(BeamStage)));
+        bulk_g2s(stg[s].ab, ab + j0, sizeof(stg[s].ab), &full[s]);
+        bulk_g2s(stg[s].kd, kd + j0, sizeof(stg[s].kd), &full[s]);
+        bulk_g2s(stg[s].bst, bst + j0, sizeof(stg[s].bst), &full[s]);
+        bulk_g2s(stg[s].meta, bmeta + j0, sizeof(stg[s].meta), &full[s]);
+    };
+    if (tid == 0)
+        for (int i = 0; i < kBeamStages && i < mine; i++) issue(i);
+    int issued = min(kBeamStages, mine);
+    for (int i = 0; i < mine; i++) {
+        const int s = i % kBeamStages;
+        const bool late = !mbar_wait(&full[s], (uint32_t)(i / kBeamStages) & 1u);
+        if (__syncthreads_or(late)) {
+            // a copy did not land in time: flag it, let the copies in flight land (bounded), stop
+            if (tid == 0) {
+                atomicOr(deverr, DEVERR_TIMEOUT);
+                for (int k = i; k < issued; k++) mbar_wait(&full[k % kBeamStages], (uint32_t)(k / kBeamStages) & 1u);
+            }
+            __syncthreads();
+            return;
+        }
+        const BeamStage& S = stg[s];
+        const int jt = (blockIdx.x + i * gridDim.x) * kBeamTile;
+        const int q0 = tid, q1 = tid + kBeamThreads;
+        const int j0 = jt + q0, j1 = jt + q1;
+        const bool h0 = j0 < nbeams, h1 = j1 < nbeams;
+        const uint32_t m0 = S.meta[q0], m1 = S.meta[q1];
+        const int2 e0 = S.ab[q0], e1 = S.ab[q1];
+        float4 pa0 = make_float4(0, 0, 0, 0), va0 = pa0, pb0 = pa0, vb0 = pa0, pa1 = pa0, va1 = pa0, pb1 = pa0, vb1 = pa0;
+        const bool g0 = h0 && !(m0 & kBeamAsleep), g1 = h1 && !(m1 & kBeamAsleep);
+        if (g0) pa0 = nd[2 * e0.x], va0 = nd[2 * e0.x + 1], pb0 = nd[2 * e0.y], vb0 = nd[2 * e0.y + 1];
+        if (g1) pa1 = nd[2 * e1.x], va1 = nd[2 * e1.x + 1], pb1 = nd[2 * e1.y], vb1 = nd[2 * e1.y + 1];
+        if (h0) beam_step(j0, m0, S.bst[q0], S.kd[q0], pa0, va0, pb0, vb0, bst, bmeta, bcold, stress, bbody, fsc, bodies);
+        if (h1) beam_step(j1, m1, S.bst[q1], S.kd[q1], pa1, va1, pb1, vb1, bst, bmeta, bcold, stress, bbody, fsc, bodies);
+        __syncthreads(); // (every thread is done with stage s)
+        if (tid == 0 && issued < mine) {
+            fence_proxy_async();
+            issue(issued);
+        }
+        issued = min(issued + 1, mine);
+    }
+}
+
 // The frame bodies' gather (NodeFem): their nodes' forces go to the frame's implicit step
 struct NodeFem {
     const int* fslot;        // node -> frame node (-1: none)

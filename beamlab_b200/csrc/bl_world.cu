@@ -90,6 +90,8 @@ struct bl_gpu_ctx {
     DevBuf<float> fsc;
     DevBuf<int2> inc2;                         // per node's incidences, warp-interleaved (k_force)
     DevBuf<int> ell_ptr;
+    int beam_tiles = 0;                        // k_beams_tma's tiles (the beam arrays hold beam_tiles * kBeamTile)
+    int beam_grid = 0;                         // its persistent grid (0: not sized yet)
     DevBuf<int4> info;
     DevBuf<int> inc_ptr, inc, bbody;
     DevBuf<int2> ab;
@@ -121,9 +123,7 @@ struct bl_gpu_ctx {
     DevBuf<long long> piters;
     DevBuf<float> guess, gscale;               // the learned per-frame-node dv guess (3) and preconditioner scale (9)
     int pcg_grid = 1;
-    int tail_level = 0;                        // from this level up the tree is narrow: one cluster launch takes it
-    int fem_cluster = 0;                       // CTAs of that launch's cluster (0: not chosen yet)
-    DevBuf<int> d_lvl_col_ptr, d_lvl_grp_ptr;
+    std::vector<int> lvl_ns;                   // per level: the slices of kUnit rows its columns' factor is cut in
     cudaStream_t aux = nullptr;                // (captures the bodies of conditional graph nodes)
     // the learned warm start (bl_mlp.cuh): parameters, the step's features, recorded samples, training scratch
     DevBuf<float> mlp_w, mlp_m, mlp_v, feat, prev_dv, smp_x, smp_t, smp_w, gpart, lpart, gsum;
@@ -134,10 +134,10 @@ struct bl_gpu_ctx {
     int adam_t = 0;
     DevBuf<float4> ext, nforce, fq, fw, ftorque, tr0, tf, tt;
     DevBuf<int> fnode, fbody, fperm, fiperm, grp_tgt, grp_ptr, col_comp, comp_fail, rb_ptr, lvl_col, fem_nodes, fslot;
-    DevBuf<int> fcol_ptr, frow, gdiag_ptr, goff_ptr, fem_fail, fem_clamp;
+    DevBuf<int> fcol_ptr, frow, fblk_col, gdiag_ptr, goff_ptr, fem_fail, fem_clamp;
     DevBuf<int2> gdiag, gu, rb;
     DevBuf<int4> goff, tn;
-    DevBuf<double> xd, diag, off, rhs, dinv, tkv, ch2, chd;
+    DevBuf<double> xd, diag, ldiag, off, rhs, dinv, tkv, ch2, chd;
     DevBuf<float> finertia, tX, tk, ttan;
     DevBuf<uint8_t> tbroken, ton, ffixed;
     DevBuf<FemSecDev> fsec;
@@ -191,13 +191,12 @@ static void free_fem(bl_gpu_ctx* c) {
     c->ext.free_(), c->nforce.free_(), c->fq.free_(), c->fw.free_(), c->ftorque.free_(), c->tr0.free_(), c->tf.free_(), c->tt.free_();
     c->fnode.free_(), c->fbody.free_(), c->fperm.free_(), c->fiperm.free_(), c->grp_tgt.free_(), c->grp_ptr.free_();
     c->col_comp.free_(), c->comp_fail.free_(), c->rb_ptr.free_(), c->lvl_col.free_(), c->fem_nodes.free_(), c->fslot.free_();
-    c->fcol_ptr.free_(), c->frow.free_(), c->gdiag_ptr.free_(), c->goff_ptr.free_(), c->fem_fail.free_(), c->fem_clamp.free_();
+    c->fcol_ptr.free_(), c->frow.free_(), c->fblk_col.free_(), c->gdiag_ptr.free_(), c->goff_ptr.free_(), c->fem_fail.free_(), c->fem_clamp.free_();
     c->px.free_(), c->pr.free_(), c->pz.free_(), c->pp.free_(), c->ppf.free_(), c->ppdi.free_(), c->pred.free_(), c->a0d.free_(), c->pxprev.free_();
     c->a0o.free_(), c->b0.free_(), c->res.free_(), c->plast.free_(), c->pstat.free_(), c->piters.free_(), c->guess.free_(), c->gscale.free_();
-    c->d_lvl_col_ptr.free_(), c->d_lvl_grp_ptr.free_();
     c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
-    c->xd.free_(), c->diag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
+    c->xd.free_(), c->diag.free_(), c->ldiag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
 }
 
@@ -483,44 +482,9 @@ static int commit_fem(bl_gpu_ctx* c) {
         c->lvl_grp_ptr.push_back((int)grp_tgt.size());
         c->lvl_col_ptr.push_back((int)lvl_col.size());
     }
-    // begin, triangles, assembly, per level a factor (and an update) kernel and two substitutions, velocities, integration
-    // the top of the tree (every level from it on at most kTopCols columns and kTopGroups update targets) goes to one
-    // cluster launch for the factorization and one for the substitutions; the levels below, a launch each
-    const int kTopCols = 256, kTopGroups = 4096;
-    int tail = nlev;
-    if (c->cfg.fem_top_level >= 0) {
-        tail = std::min(nlev, (int)c->cfg.fem_top_level);
-    } else {
-        while (tail > 0 && c->lvl_col_ptr[tail] - c->lvl_col_ptr[tail - 1] <= kTopCols && c->lvl_grp_ptr[tail] - c->lvl_grp_ptr[tail - 1] <= kTopGroups)
-            tail--;
-    }
-    c->tail_level = tail;
-    if (tail < nlev && c->fem_cluster == 0) {
-        // the largest cluster (of 16, 8, 4, 2, 1 CTAs of 1024 threads) the device can run
-        int want = c->cfg.fem_cluster > 0 ? std::min(16, (int)c->cfg.fem_cluster) : 16;
-        for (int cl = want; cl >= 1; cl /= 2) {
-            if (cl > 8) {
-                BL_CUDA(c, cudaFuncSetAttribute(k_fem_factor_top, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-                BL_CUDA(c, cudaFuncSetAttribute(k_fem_subst_top, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-            }
-            cudaLaunchConfig_t lc{};
-            lc.gridDim = dim3(cl), lc.blockDim = dim3(1024);
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = cl, at[0].val.clusterDim.y = 1, at[0].val.clusterDim.z = 1;
-            lc.attrs = at, lc.numAttrs = 1;
-            int n1 = 0, n2 = 0;
-            if (cudaOccupancyMaxActiveClusters(&n1, k_fem_factor_top, &lc) == cudaSuccess && n1 >= 1 &&
-                cudaOccupancyMaxActiveClusters(&n2, k_fem_subst_top, &lc) == cudaSuccess && n2 >= 1) {
-                c->fem_cluster = cl;
-                break;
-            }
-            cudaGetLastError();
-        }
-        if (c->fem_cluster == 0) return BL_GPU_ECUDA;
-    }
-    c->chol_launches = 3 * (int64_t)tail + (tail < nlev ? 2 : 0);
-    for (int L = 0; L < tail; L++) c->chol_launches += c->lvl_grp_ptr[L + 1] > c->lvl_grp_ptr[L];
+    // begin, triangles, assembly, per level a factor kernel, an update + forward kernel and a backward kernel,
+    // velocities, integration
+    c->chol_launches = 3 * (int64_t)nlev;
     c->fem_launches = 5 + c->chol_launches;
     {   // each row's blocks in the order of their columns
         std::vector<std::vector<int2>> rows(NF);
@@ -548,6 +512,12 @@ static int commit_fem(bl_gpu_ctx* c) {
         (rc = upload_vec(c, c->chd, chd)) || (rc = upload_vec(c, c->fem_fail, zeros_b)) || (rc = upload_vec(c, c->fem_clamp, clamps_b)) ||
         (rc = upload_vec(c, c->fem_nodes, fem_nodes)) || (rc = upload_vec(c, c->fslot, fslot)))
         return rc;
+    {
+        std::vector<int> blk_col(std::max(NB, 1), 0);
+        for (int k = 0; k < NF; k++)
+            for (int pb = col_ptr[k]; pb < col_ptr[k + 1]; pb++) blk_col[pb] = k;
+        if ((rc = upload_vec(c, c->fblk_col, blk_col))) return rc;
+    }
     BL_CUDA(c, c->nforce.alloc(c->N));
     BL_CUDA(c, c->tf.alloc(3 * (size_t)NT));
     BL_CUDA(c, c->tt.alloc(3 * (size_t)NT));
@@ -565,12 +535,20 @@ static int commit_fem(bl_gpu_ctx* c) {
     F.fnode = c->fnode.p, F.fbody = c->fbody.p, F.perm = c->fperm.p, F.iperm = c->fiperm.p, F.xd = c->xd.p, F.q = c->fq.p, F.w = c->fw.p;
     F.inertia = c->finertia.p, F.torque = c->ftorque.p, F.tn = c->tn.p, F.tX = c->tX.p, F.tr0 = c->tr0.p, F.tk = c->tk.p, F.tbroken = c->tbroken.p;
     F.tf = c->tf.p, F.tt = c->tt.p, F.ttan = c->ttan.p, F.tkv = c->tkv.p, F.ton = c->ton.p, F.sec = c->fsec.p, F.col_ptr = c->fcol_ptr.p, F.row = c->frow.p;
+    F.blk_col = c->fblk_col.p;
     F.gdiag_ptr = c->gdiag_ptr.p, F.gdiag = c->gdiag.p, F.goff_ptr = c->goff_ptr.p, F.goff = c->goff.p, F.diag = c->diag.p, F.off = c->off.p;
     F.rhs = c->rhs.p, F.dinv = c->dinv.p, F.fixed = c->ffixed.p, F.grp_tgt = c->grp_tgt.p, F.grp_ptr = c->grp_ptr.p, F.gu = c->gu.p;
     F.col_comp = c->col_comp.p, F.comp_fail = c->comp_fail.p, F.rb_ptr = c->rb_ptr.p;
     F.rb = c->rb.p, F.lvl_col = c->lvl_col.p, F.ch2 = c->ch2.p, F.chd = c->chd.p, F.body_failures = c->fem_fail.p, F.body_clamps = c->fem_clamp.p;
     F.h = c->cfg.dt, F.step = c->cfg.dt;
-    if ((rc = upload_vec(c, c->d_lvl_col_ptr, c->lvl_col_ptr)) || (rc = upload_vec(c, c->d_lvl_grp_ptr, c->lvl_grp_ptr))) return rc;
+    c->lvl_ns.assign(std::max<size_t>(c->lvl_col_ptr.size(), 1) - 1, 1);
+    for (size_t L = 0; L + 1 < c->lvl_col_ptr.size(); L++)
+        for (int ci = c->lvl_col_ptr[L]; ci < c->lvl_col_ptr[L + 1]; ci++) {
+            const int k = lvl_col[ci];
+            c->lvl_ns[L] = std::max(c->lvl_ns[L], (6 * (col_ptr[k + 1] - col_ptr[k]) + kUnit - 1) / kUnit);
+        }
+    BL_CUDA(c, c->ldiag.alloc(36 * (size_t)NF));
+    F.ldiag = c->ldiag.p;
     // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
     for (DevBuf<double>* d : {&c->px, &c->pr, &c->pz, &c->pp, &c->ppdi}) BL_CUDA(c, d->alloc(6 * (size_t)NF));
     BL_CUDA(c, c->ppf.alloc(36 * (size_t)NF));
@@ -758,6 +736,10 @@ static int commit_bodies(bl_gpu_ctx* c) {
             inc[fill[ab[g].y]++] = (int)((uint32_t)g | 0x80000000u);
         }
     }
+    // the arrays k_beams_tma streams padded to whole tiles (the pads asleep: never stepped)
+    const size_t Mpad = (size_t)(M + kBeamTile - 1) / kBeamTile * kBeamTile;
+    ab.resize(Mpad, make_int2(0, 0)), kd.resize(Mpad, make_float2(0, 0)), bst.resize(Mpad, make_float4(0, 0, 0, 0)), meta.resize(Mpad, kBeamAsleep);
+    c->beam_tiles = (int)(Mpad / kBeamTile);
     static_assert(sizeof(bl_node) == 2 * sizeof(float4), "bl_node is two float4");
     BL_CUDA(c, c->nd.alloc(2 * (size_t)N));
     if (N) BL_CUDA(c, cudaMemcpyAsync(c->nd.p, nodes.data(), sizeof(bl_node) * N, cudaMemcpyHostToDevice, c->stream));
@@ -767,6 +749,15 @@ static int commit_bodies(bl_gpu_ctx* c) {
         (rc = upload_vec(c, c->bbody, bbody)) || (rc = upload_vec(c, c->dbodies, recs)))
         return rc;
     BL_CUDA(c, c->fsc.alloc(M));
+    c->beam_grid = 0;
+    if (c->cfg.beam_kernel == 0 && M > 0) {
+        // k_beams_tma: a persistent grid of as many blocks as fit on the device at once (at most one a tile)
+        BL_CUDA(c, cudaFuncSetAttribute(k_beams_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBeamSmem));
+        int per_sm = 0, sms = 0;
+        BL_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_beams_tma, kBeamThreads, kBeamSmem));
+        BL_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+        if (per_sm > 0) c->beam_grid = std::min(c->beam_tiles, per_sm * sms);
+    }
     BL_CUDA(c, c->nodef.alloc(N));
     {   // the incidences with their other ends, per warp of 32 nodes interleaved (entry q of lane l at 32 q + l), each
         // warp's width its widest node's count rounded up to 4, padded with (0, the node itself)
@@ -919,19 +910,6 @@ static void launch_pcg(bl_gpu_ctx* c, cudaStream_t s, cudaGraphConditionalHandle
     cudaLaunchKernelEx(&lc, k_fem_pcg, c->fd, P);
 }
 
-// The top of the elimination tree, levels [L0, L1), in one launch of a cluster of fem_cluster CTAs: its factorization
-// (k_fem_factor_top) or both its substitutions (k_fem_subst_top).
-static void launch_top(bl_gpu_ctx* c, cudaStream_t s, bool factor, int L0, int L1) {
-    cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3(c->fem_cluster), lc.blockDim = dim3(1024), lc.dynamicSmemBytes = 0, lc.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = c->fem_cluster, at[0].val.clusterDim.y = 1, at[0].val.clusterDim.z = 1;
-    lc.attrs = at, lc.numAttrs = 1;
-    if (factor) cudaLaunchKernelEx(&lc, k_fem_factor_top, c->fd, (const int*)c->d_lvl_col_ptr.p, (const int*)c->d_lvl_grp_ptr.p, L0, L1);
-    else cudaLaunchKernelEx(&lc, k_fem_subst_top, c->fd, (const int*)c->d_lvl_col_ptr.p, L0, L1);
-}
-
 static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev = nullptr) {
     int q = 0;
     auto mark = [&]() {
@@ -958,8 +936,13 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             }
         }
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
-        k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
-                                               c->dbodies.p, c->M, c->B);
+        if (c->beam_grid > 0) {
+            k_beams_tma<<<c->beam_grid, kBeamThreads, kBeamSmem, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p,
+                                                                     c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B, c->beam_tiles, c->deverr.p);
+        } else {
+            k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
+                                                   c->dbodies.p, c->M, c->B);
+        }
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
         k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0],
@@ -975,7 +958,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         mark();
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
-            k_fem_assemble<<<(c->NF + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
+            k_fem_assemble_all<<<(c->NF + c->NB + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
             if (c->cfg.fem_check_residual) {
                 cudaMemcpyAsync(c->a0d.p, c->diag.p, sizeof(double) * 36 * c->NF, cudaMemcpyDeviceToDevice, s);
                 cudaMemcpyAsync(c->a0o.p, c->off.p, sizeof(double) * 36 * std::max(c->NB, 1), cudaMemcpyDeviceToDevice, s);
@@ -987,22 +970,17 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             if (rec) k_mlp_record_pre<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
             if (learned) k_mlp_infer<<<(c->NF + kLanes - 1) / kLanes, kLanes, 0, s>>>(F, MD, c->guess.p, c->gscale.p);
             auto cholesky = [c, &F](cudaStream_t cs) {
-                // the wide levels a launch each (factor, update); the narrow top of the tree in one block
-                const int nlev = (int)c->lvl_col_ptr.size() - 1, tail = c->tail_level;
-                for (int L = 0; L < tail; L++) {
+                // the levels of the elimination tree two launches each (factor; updates with the forward substitution),
+                // then the backward substitution a launch a level from the top down
+                const int nlev = (int)c->lvl_col_ptr.size() - 1;
+                for (int L = 0; L < nlev; L++) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1], g0 = c->lvl_grp_ptr[L], g1 = c->lvl_grp_ptr[L + 1];
-                    k_fem_chol_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
-                    if (g1 > g0) k_fem_update_level<<<(g1 - g0 + 3) / 4, 128, 0, cs>>>(F, g0, g1);
+                    k_fem_chol_level<<<dim3(c1 - c0, c->lvl_ns[L]), kUnit, 0, cs>>>(F, c0);
+                    k_fem_update_forward_level<<<(g1 - g0 + 3) / 4 + (c1 - c0), kUnit, 0, cs>>>(F, g0, g1, c0);
                 }
-                if (tail < nlev) launch_top(c, cs, true, tail, nlev);
-                for (int L = 0; L < tail; L++) {
+                for (int L = nlev - 1; L >= 0; L--) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
-                    k_fem_forward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
-                }
-                if (tail < nlev) launch_top(c, cs, false, tail, nlev);
-                for (int L = tail - 1; L >= 0; L--) {
-                    const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
-                    k_fem_backward_level<<<(c1 - c0 + 3) / 4, 128, 0, cs>>>(F, c0, c1);
+                    k_fem_backward_level<<<c1 - c0, kUnit, 0, cs>>>(F, c0);
                 }
             };
             if (c->cfg.fem_solver == BL_GPU_FEM_CHOLESKY) {
@@ -1109,8 +1087,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->fem_check_residual = 0;
     cfg->pcg_learned_scale = 0;
     cfg->graphs = 1;
-    cfg->fem_top_level = -1;
-    cfg->fem_cluster = 0;
+    cfg->beam_kernel = 0;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -1136,7 +1113,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
     if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 3 || c0.pcg_max_iters < 0 ||
-        !(c0.pcg_tol > 0) || c0.fem_top_level < -1 || c0.fem_cluster < 0 || c0.fem_cluster > 16 || (c0.fem_cluster & (c0.fem_cluster - 1)) != 0)
+        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1)
         return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;

@@ -70,10 +70,8 @@ class WorldSettings:
     pcg_learned_scale: bool = False
     # True: each frame captured once as a CUDA graph and replayed; False: its kernels launched one by one (plain path)
     graphs: bool = True
-    # the FEM Cholesky: levels from fem_top_level (-1: automatic) to the tree's top in one launch of a cluster of
-    # fem_cluster CTAs (0: the largest the device runs)
-    fem_top_level: int = -1
-    fem_cluster: int = 0
+    # the beams' kernel: 0 streams the beam arrays by bulk (TMA) copies, 1 plain loads (the same results)
+    beam_kernel: int = 0
 
 
 @dataclass
@@ -317,7 +315,7 @@ class _Config(C.Structure):
                 ("collision_hz", C.c_float), ("inter_body_collisions", C.c_int32), ("max_pairs", C.c_int32),
                 ("fem_solver", C.c_int32), ("pcg_max_iters", C.c_int32), ("pcg_tol", C.c_float),
                 ("fem_check_residual", C.c_int32), ("pcg_learned_scale", C.c_int32), ("graphs", C.c_int32),
-                ("fem_top_level", C.c_int32), ("fem_cluster", C.c_int32)]
+                ("beam_kernel", C.c_int32)]
 
 
 class _FemStats(C.Structure):
@@ -408,8 +406,7 @@ class World:
         cfg.fem_check_residual = int(self.settings.fem_check_residual)
         cfg.pcg_learned_scale = int(self.settings.pcg_learned_scale)
         cfg.graphs = int(self.settings.graphs)
-        cfg.fem_top_level = int(self.settings.fem_top_level)
-        cfg.fem_cluster = int(self.settings.fem_cluster)
+        cfg.beam_kernel = int(self.settings.beam_kernel)
         self._ctx = C.c_void_p()
         _check(self._L.bl_gpu_create(C.byref(cfg), C.byref(self._ctx)), "create")
         self._bodies: list[BodyHandle] = []

@@ -345,6 +345,11 @@ def run_gpu(args):
         # writes p, v (24 B); the substep as a whole: 40 B a beam + 52 B a node (the force never leaving the chip)
         kern = {"k_beams": (BYTES_PER_BEAM * m, per["beams"], m, "beam"), "k_force": (32 * n, per["force"], n, "node"),
                 "k_integrate": (68 * n, per["integrate"], n, "node")}
+        if args.workload == "plate64":
+            # the implicit FEM step: its factor (4,096 diagonal and 64,411 off-diagonal 6x6 blocks of doubles, the
+            # symbolic phase's count for this plate) and right side each read and written once a substep
+            fem_bytes = 2 * 8 * (36 * 4096 + 36 * 64411 + 6 * 4096)
+            kern["fem_step"] = (fem_bytes, per["fem"], 4096, "column")
         dom = max(kern, key=lambda k: kern[k][1])
         alg_bytes, kms, units_, unit_name = kern[dom]
         achieved = alg_bytes / (kms * 1e-3) / 1e9

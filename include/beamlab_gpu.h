@@ -82,12 +82,8 @@ typedef struct {
                                   none - measured on the plates, the scale as trained costs iterations */
     int32_t graphs;            /* 1 (default): a frame of n substeps is captured once as a CUDA graph and replayed; 0: its
                                   kernels are launched one by one every call (the plain path, one launch per kernel) */
-    int32_t fem_top_level;     /* the FEM frames' block Cholesky runs its elimination tree's levels below this one a launch
-                                  each and the levels from it to the top in one cluster launch (and the substitutions
-                                  alike); -1 (default): the first level from which every level is narrow (at most 256
-                                  columns and 4096 updated blocks). Results are the same for every value. */
-    int32_t fem_cluster;       /* CTAs (1024 threads each) of that cluster launch: 1, 2, 4, 8 or 16; 0 (default): the
-                                  largest the device can run */
+    int32_t beam_kernel;       /* 0 (default): the beams' kernel streams the beam arrays through shared memory by bulk
+                                  (TMA) copies; 1: plain loads. Results are the same. */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };
@@ -228,7 +224,9 @@ enum {
     BL_GPU_DEVERR_NONFINITE = 1 << 1,  /* a body needed the repair of non-finite / runaway nodes */
     BL_GPU_DEVERR_PAIRS = 1 << 2,      /* the contact pair list overflowed bl_gpu_config.max_pairs */
     BL_GPU_DEVERR_ISLAND = 1 << 3,     /* an island with contact pairs held more than BL_GPU_MAX_ISLAND_BODIES bodies */
-    BL_GPU_DEVERR_CONTACT_UNSUPPORTED = 1 << 5 /* a body with a FEM frame met another body's triangles (not stepped) */
+    BL_GPU_DEVERR_CONTACT_UNSUPPORTED = 1 << 5, /* a body with a FEM frame met another body's triangles (not stepped) */
+    BL_GPU_DEVERR_TIMEOUT = 1 << 6     /* a kernel's bounded wait on its own bulk copies ran out (1 s): the substep's
+                                          beams were not all stepped */
 };
 #define BL_GPU_MAX_ISLAND_BODIES 256
 #define BL_GPU_MAX_CANDIDATES 64

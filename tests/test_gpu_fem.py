@@ -31,21 +31,3 @@ def test_gpu_plate_matches_reference(name, n):
     st = h.state()
     assert st["fem_failures"] == 0 and st["fem_clamps"] == 0
     w.close()
-
-
-def test_gpu_factorization_schedules_agree():
-    """The block Cholesky's levels launched one by one, the tree's top in one cluster launch (of 1 and of the largest
-    cluster the device runs), or the whole tree in it: the same per-column and per-target work in the same order, so
-    the plate's state is bitwise the same after 60 substeps."""
-    runs = []
-    for top, cl in ((10 ** 6, 0), (-1, 0), (-1, 1), (0, 0), (40, 2)):
-        w = world_from_rig(rigs.shell_plate(20, seed=3), fem_top_level=top, fem_cluster=cl)
-        for _ in range(3):
-            w.step_substeps(20)
-        fem = w.bodies()[0].fem()
-        runs.append((np.ascontiguousarray(w.bodies()[0].nodes()["p"]).copy(), fem["xd"].copy(), fem["w"].copy()))
-        assert w.bodies()[0].state()["fem_failures"] == 0
-        w.close()
-    for r in runs[1:]:
-        for a, b in zip(runs[0], r):
-            assert np.array_equal(a.view(np.uint8), b.view(np.uint8))

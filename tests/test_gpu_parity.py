@@ -102,14 +102,14 @@ def _wall_crash(seed, shuffle=False):
     return rig
 
 
-@pytest.mark.parametrize("shuffle", [False, True])
-def test_gpu_crash_yield_and_break_match_oracle(port_lib, shuffle):
-    """Thousands of beams yield and hundreds break in a 30 m/s crash - with the beams in builder order and shuffled -
-    and the state stays bitwise the oracle's."""
+@pytest.mark.parametrize("shuffle,beam_kernel", [(False, 0), (True, 0), (False, 1)])
+def test_gpu_crash_yield_and_break_match_oracle(port_lib, shuffle, beam_kernel):
+    """Thousands of beams yield and hundreds break in a 30 m/s crash - with the beams in builder order and shuffled,
+    the beam arrays streamed by bulk copies or loaded plainly - and the state stays bitwise the oracle's."""
     from oracle.oracle import PortWorld, build_world
     from beamlab_b200.world import SoftBody
     rig = _wall_crash(5, shuffle)
-    gw, ow = GpuWorld(rig), build_world(PortWorld, rig)
+    gw, ow = GpuWorld(rig, beam_kernel=beam_kernel), build_world(PortWorld, rig)
     for f in range(12):
         gw.step_substeps(25)
         ow.step_substeps(25)
