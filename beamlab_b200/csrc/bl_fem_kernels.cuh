@@ -591,6 +591,203 @@ __global__ void __launch_bounds__(kUnit) k_fem_backward_level(FemDev F, int c0) 
     backward_unit(F, c0 + blockIdx.x, threadIdx.x, 0, sm);
 }
 
+// ------------------------------------------------------------------------------------------ the top chain as one dense front
+// The top of the elimination tree is a chain of single columns (160 of the 64 x 64 plate's 267 levels): every row of a
+// chain column's factor is a later chain column (a column's rows are its ancestors in the tree). After the levels
+// below have made their updates, the chain's blocks form one dense lower triangle D (6 m x 6 m, padded with an
+// identity to whole 32 x 32 tiles), factored by a blocked right-looking Cholesky - per 32-column panel a tile
+// factorization (one warp), the panel's triangular solves and the trailing rank-32 updates - and solved densely; the
+// levels below then run their backward substitutions on the chain's solution. The sums run in another order than the
+// block schedule's (the step is a tolerance match with the reference either way: its element kernels call the GPU's
+// transcendentals).
+constexpr int kFT = 32;       // tile
+constexpr int kFrontMin = 8;  // the shortest chain made a dense front (columns)
+
+struct FrontDev {
+    int m, N, nt;            // chain columns, D's size (6 m rounded up to tiles), tiles a side
+    const int* col;          // chain column c -> its column
+    const int4* blk;         // the chain's off-diagonal blocks: (block, row's chain index, column's chain index, 0)
+    int nblk;
+    const int* chain;        // column -> its chain index, or -1
+    double* D;               // N x N, row-major: the chain's blocks (lower triangle), then the factor
+    double* b;               // N: the chain's right side, then its forward substitution's result
+};
+
+// D's lower triangle from the chain's diagonal and off-diagonal blocks; the padding's diagonal 1 (D zero before)
+__global__ void k_front_scatter(FemDev F, FrontDev X) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nd = 36 * X.m, no = 36 * X.nblk;
+    if (t < nd) {
+        const int c = t / 36, e = t % 36, i = e / 6, j = e % 6;
+        if (j <= i) X.D[(size_t)(6 * c + i) * X.N + 6 * c + j] = F.diag[36 * (size_t)X.col[c] + e];
+    } else if (t < nd + no) {
+        const int q = t - nd, e = q % 36;
+        const int4 bl = X.blk[q / 36];
+        X.D[(size_t)(6 * bl.y + e / 6) * X.N + 6 * bl.z + e % 6] = F.off[36 * (size_t)bl.x + e];
+    } else if (t < nd + no + X.N - 6 * X.m) {
+        const int r = 6 * X.m + (t - nd - no);
+        X.D[(size_t)r * X.N + r] = 1.0;
+    }
+}
+
+// The diagonal tile p: Cholesky in place by one warp, lane i holding row i in registers (column j's entries shared
+// through shared memory each step); a non-positive pivot fails the chain's component
+__global__ void __launch_bounds__(32) k_front_potrf(FemDev F, FrontDev X, int p) {
+    __shared__ double col[kFT];
+    const int lane = threadIdx.x;
+    double* T = X.D + (size_t)(kFT * p) * X.N + kFT * p;
+    double a[kFT];
+#pragma unroll
+    for (int l = 0; l < kFT; l++) a[l] = T[(size_t)lane * X.N + l];
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < kFT; j++) {
+        const double s = __shfl_sync(0xffffffffu, a[j], j);
+        ok = ok && s > 0;
+        const double id = rsqrt(s), d = s * id;
+        a[j] = lane == j ? d : (lane > j ? a[j] * id : a[j]);
+        col[lane] = a[j];
+        __syncwarp();
+#pragma unroll
+        for (int l = j + 1; l < kFT; l++)
+            if (l <= lane) a[l] -= a[j] * col[l];
+        __syncwarp();
+    }
+#pragma unroll
+    for (int l = 0; l < kFT; l++) T[(size_t)lane * X.N + l] = l <= lane ? a[l] : 0.0;
+    if (!ok && lane == 0) atomicExch(&F.comp_fail[F.col_comp[X.col[0]]], 1);
+    // the forward substitution's tile: y_p = L_pp^-1 b_p (b_p already less the earlier panels' parts)
+    double y = X.b[kFT * p + lane];
+#pragma unroll
+    for (int j = 0; j < kFT; j++) {
+        if (lane == j) y /= a[j];
+        const double yj = __shfl_sync(0xffffffffu, y, j);
+        if (lane > j) y -= a[j] * yj;
+    }
+    X.b[kFT * p + lane] = y;
+}
+
+// The panel below tile p: L_ip = A_ip L_pp^-T for the tiles i > p (a block each; thread r: row r of the tile)
+__global__ void __launch_bounds__(kFT) k_front_trsm(FrontDev X, int p) {
+    __shared__ double L[kFT][kFT + 1];
+    __shared__ double id[kFT];
+    const int r = threadIdx.x, i = p + 1 + blockIdx.x;
+    const double* P = X.D + (size_t)(kFT * p) * X.N + kFT * p;
+    for (int q = 0; q < kFT; q++) L[q][r] = P[(size_t)q * X.N + r];
+    __syncwarp();
+    id[r] = 1.0 / L[r][r];
+    __syncwarp();
+    double* row = X.D + (size_t)(kFT * i + r) * X.N + kFT * p;
+    double x[kFT];
+#pragma unroll
+    for (int j = 0; j < kFT; j++) x[j] = row[j];
+#pragma unroll
+    for (int j = 0; j < kFT; j++) {
+        double s = x[j];
+#pragma unroll
+        for (int l = 0; l < j; l++) s -= x[l] * L[j][l];
+        x[j] = s * id[j];
+    }
+#pragma unroll
+    for (int j = 0; j < kFT; j++) row[j] = x[j];
+    // the forward substitution: b_i -= L_ip y_p
+    double sy = 0;
+#pragma unroll
+    for (int j = 0; j < kFT; j++) sy += x[j] * X.b[kFT * p + j];
+    X.b[kFT * i + r] -= sy;
+}
+
+// The trailing update of panel p: A_ij -= L_ip L_jp^T for p < j <= i (a block a tile, 256 threads of 2 x 2 entries)
+__global__ void __launch_bounds__(256) k_front_syrk(FrontDev X, int p) {
+    __shared__ double Li[kFT][kFT + 1], Lj[kFT][kFT + 1];
+    // (blockIdx.x -> (i, j): i = p + 1 + a, j = p + 1 + b, b <= a, row a of the triangle holding a + 1 tiles)
+    const int q = blockIdx.x;
+    int a = (int)((sqrt(8.0 * q + 1.0) - 1.0) * 0.5);
+    while ((a + 1) * (a + 2) / 2 <= q) a++;
+    while (a * (a + 1) / 2 > q) a--;
+    const int bb = q - a * (a + 1) / 2;
+    const int i = p + 1 + a, j = p + 1 + bb;
+    const int t = threadIdx.x;
+    for (int e = t; e < kFT * kFT; e += 256) {
+        const int rr = e / kFT, cc = e % kFT;
+        Li[rr][cc] = X.D[(size_t)(kFT * i + rr) * X.N + kFT * p + cc];
+        Lj[rr][cc] = X.D[(size_t)(kFT * j + rr) * X.N + kFT * p + cc];
+    }
+    __syncthreads();
+    const int r0 = 2 * (t / 16), c0 = 2 * (t % 16);
+    double acc[2][2] = {{0, 0}, {0, 0}};
+#pragma unroll 8
+    for (int k = 0; k < kFT; k++) {
+        const double x0 = Li[r0][k], x1 = Li[r0 + 1][k], y0 = Lj[c0][k], y1 = Lj[c0 + 1][k];
+        acc[0][0] += x0 * y0, acc[0][1] += x0 * y1, acc[1][0] += x1 * y0, acc[1][1] += x1 * y1;
+    }
+    double* T = X.D + (size_t)(kFT * i + r0) * X.N + kFT * j + c0;
+    T[0] -= acc[0][0], T[1] -= acc[0][1], T[X.N] -= acc[1][0], T[X.N + 1] -= acc[1][1];
+}
+
+// The chain's right side: each chain column's r less its row's blocks from the columns below the chain times their y
+// (forward_unit's sum without the chain's own columns), a unit a chain column
+__global__ void __launch_bounds__(kUnit) k_front_rhs(FemDev F, FrontDev X) {
+    __shared__ double sm[72];
+    const int c = blockIdx.x, ut = threadIdx.x, k = X.col[c];
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = F.rb_ptr[k] + ut; q < F.rb_ptr[k + 1]; q += kUnit) {
+        const int2 bc = F.rb[q];
+        if (X.chain[bc.y] >= 0) continue;
+        const double* L = F.off + 36 * (size_t)bc.x;
+        const double* yk = F.rhs + 6 * (size_t)bc.y;
+        for (int ii = 0; ii < 6; ii++) {
+            double t = 0;
+            for (int j = 0; j < 6; j++) t += L[ii * 6 + j] * yk[j];
+            s[ii] += t;
+        }
+    }
+    unit_sum6(s, ut, 0, sm);
+    if (ut == 0)
+        for (int j = 0; j < 6; j++) X.b[6 * c + j] = F.rhs[6 * (size_t)k + j] - s[j];
+    if (c == 0)
+        for (int r = 6 * X.m + ut; r < X.N; r += kUnit) X.b[r] = 0.0; // (the padding's)
+}
+
+// L^T x = y over the dense factor (y: the forward substitution's result, left in b by the factorization's kernels),
+// by one block: per tile from the last, its 32 x 32 diagonal staged in shared memory (with the inverses of its
+// diagonal) and solved by one warp (lane t: row t), then the earlier rows updated by the block; x into the chain
+// columns' rhs
+__global__ void __launch_bounds__(1024) k_front_solve(FemDev F, FrontDev X) {
+    extern __shared__ double v[]; // N
+    __shared__ double Tt[kFT][kFT + 1];
+    __shared__ double inv[kFT];
+    const int t = threadIdx.x, n6 = 6 * X.m, lane = t & 31;
+    for (int r = t; r < X.N; r += blockDim.x) v[r] = X.b[r];
+    for (int p = X.nt - 1; p >= 0; p--) {
+        const int r0 = kFT * p;
+        __syncthreads();
+        Tt[t / kFT][t % kFT] = X.D[(size_t)(r0 + t / kFT) * X.N + r0 + t % kFT]; // (1024 threads: the whole tile)
+        __syncthreads();
+        if (t < kFT) inv[t] = 1.0 / Tt[t][t];
+        __syncthreads();
+        if (t < 32) {
+            double x = v[r0 + lane];
+#pragma unroll
+            for (int j = kFT - 1; j >= 0; j--) {
+                if (lane == j) x *= inv[j];
+                const double xj = __shfl_sync(0xffffffffu, x, j);
+                if (lane < j) x -= Tt[j][lane] * xj;
+            }
+            v[r0 + lane] = x;
+        }
+        __syncthreads();
+        for (int r = t; r < r0; r += blockDim.x) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < kFT; j++) s += X.D[(size_t)(r0 + j) * X.N + r] * v[r0 + j];
+            v[r] -= s;
+        }
+    }
+    __syncthreads();
+    for (int r = t; r < n6; r += blockDim.x) F.rhs[6 * (size_t)X.col[r / 6] + r % 6] = v[r];
+}
+
 // ------------------------------------------------------------------------------------------ after the solve
 __global__ void k_fem_velocity(FemDev F, const float4* __restrict__ nd, float4* __restrict__ nforce) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;

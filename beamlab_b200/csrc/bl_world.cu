@@ -138,6 +138,13 @@ struct bl_gpu_ctx {
     DevBuf<int2> gdiag, gu, rb;
     DevBuf<int4> goff, tn;
     DevBuf<double> xd, diag, ldiag, off, rhs, dinv, tkv, ch2, chd;
+    // the top chain of the elimination tree as one dense front (bl_fem_kernels.cuh: FrontDev); front_level: its first
+    // level (the level count: none)
+    FrontDev front{};
+    int front_level = 0;
+    DevBuf<int> fcol, fchain;
+    DevBuf<int4> fblk;
+    DevBuf<double> fD, fb;
     DevBuf<float> finertia, tX, tk, ttan;
     DevBuf<uint8_t> tbroken, ton, ffixed;
     DevBuf<FemSecDev> fsec;
@@ -196,6 +203,7 @@ static void free_fem(bl_gpu_ctx* c) {
     c->a0o.free_(), c->b0.free_(), c->res.free_(), c->plast.free_(), c->pstat.free_(), c->piters.free_(), c->guess.free_(), c->gscale.free_();
     c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
+    c->fcol.free_(), c->fchain.free_(), c->fblk.free_(), c->fD.free_(), c->fb.free_(), c->front = FrontDev{}, c->front_level = 0;
     c->xd.free_(), c->diag.free_(), c->ldiag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
 }
@@ -484,8 +492,6 @@ static int commit_fem(bl_gpu_ctx* c) {
     }
     // begin, triangles, assembly, per level a factor kernel, an update + forward kernel and a backward kernel,
     // velocities, integration
-    c->chol_launches = 3 * (int64_t)nlev;
-    c->fem_launches = 5 + c->chol_launches;
     {   // each row's blocks in the order of their columns
         std::vector<std::vector<int2>> rows(NF);
         for (int k = 0; k < NF; k++)
@@ -549,6 +555,40 @@ static int commit_fem(bl_gpu_ctx* c) {
         }
     BL_CUDA(c, c->ldiag.alloc(36 * (size_t)NF));
     F.ldiag = c->ldiag.p;
+    {   // the top chain (the levels from front_level up have one column each) as one dense front, when every row of
+        // its columns is a chain column and it is long enough to pay
+        const int nlev = (int)c->lvl_col_ptr.size() - 1;
+        int top = nlev;
+        while (top > 0 && c->lvl_col_ptr[top] - c->lvl_col_ptr[top - 1] == 1) top--;
+        const int m = c->cfg.fem_dense_front ? nlev - top : 0;
+        std::vector<int> chain(NF, -1), fcol;
+        std::vector<int4> fblk;
+        bool closed = m >= kFrontMin && 6 * m <= 8192; // (D at most 512 MB, its solve's vector in shared memory)
+        for (int x = 0; closed && x < m; x++) fcol.push_back(lvl_col[c->lvl_col_ptr[top + x]]), chain[fcol.back()] = x;
+        for (int x = 0; closed && x < m; x++) {
+            const int k = fcol[x];
+            for (int pb = col_ptr[k]; pb < col_ptr[k + 1]; pb++) {
+                if (chain[row[pb]] < 0) closed = false;
+                else fblk.push_back(make_int4(pb, chain[row[pb]], x, 0));
+            }
+        }
+        c->front_level = nlev;
+        c->front = FrontDev{};
+        if (closed) {
+            FrontDev& X = c->front;
+            X.m = m, X.nt = (6 * m + kFT - 1) / kFT, X.N = kFT * X.nt, X.nblk = (int)fblk.size();
+            if ((rc = upload_vec(c, c->fcol, fcol)) || (rc = upload_vec(c, c->fblk, fblk)) || (rc = upload_vec(c, c->fchain, chain))) return rc;
+            BL_CUDA(c, c->fD.alloc((size_t)X.N * X.N));
+            BL_CUDA(c, c->fb.alloc((size_t)X.N));
+            X.col = c->fcol.p, X.blk = c->fblk.p, X.chain = c->fchain.p, X.D = c->fD.p, X.b = c->fb.p;
+            if ((size_t)X.N * sizeof(double) > 48 * 1024)
+                BL_CUDA(c, cudaFuncSetAttribute(k_front_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(X.N * sizeof(double))));
+            c->front_level = top;
+        }
+        c->chol_launches = 3 * (int64_t)c->front_level;
+        if (c->front_level < nlev) c->chol_launches += 1 + c->front.nt + 2 * (c->front.nt - 1) + 2;
+        c->fem_launches = 5 + c->chol_launches;
+    }
     // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
     for (DevBuf<double>* d : {&c->px, &c->pr, &c->pz, &c->pp, &c->ppdi}) BL_CUDA(c, d->alloc(6 * (size_t)NF));
     BL_CUDA(c, c->ppf.alloc(36 * (size_t)NF));
@@ -972,13 +1012,31 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             auto cholesky = [c, &F](cudaStream_t cs) {
                 // the levels of the elimination tree two launches each (factor; updates with the forward substitution),
                 // then the backward substitution a launch a level from the top down
-                const int nlev = (int)c->lvl_col_ptr.size() - 1;
-                for (int L = 0; L < nlev; L++) {
+                const int nlev = (int)c->lvl_col_ptr.size() - 1, top = c->front_level;
+                for (int L = 0; L < top; L++) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1], g0 = c->lvl_grp_ptr[L], g1 = c->lvl_grp_ptr[L + 1];
                     k_fem_chol_level<<<dim3(c1 - c0, c->lvl_ns[L]), kUnit, 0, cs>>>(F, c0);
                     k_fem_update_forward_level<<<(g1 - g0 + 3) / 4 + (c1 - c0), kUnit, 0, cs>>>(F, g0, g1, c0);
                 }
-                for (int L = nlev - 1; L >= 0; L--) {
+                if (top < nlev) {
+                    // the top chain: its dense front scattered, its right side, then panel by panel the factor with
+                    // the forward substitution, then the backward substitution
+                    const FrontDev& X = c->front;
+                    cudaMemsetAsync(X.D, 0, sizeof(double) * X.N * X.N, cs);
+                    const int ns = 36 * (X.m + X.nblk) + X.N - 6 * X.m;
+                    k_front_scatter<<<(ns + 255) / 256, 256, 0, cs>>>(F, X);
+                    k_front_rhs<<<X.m, kUnit, 0, cs>>>(F, X);
+                    for (int p = 0; p < X.nt; p++) {
+                        k_front_potrf<<<1, 32, 0, cs>>>(F, X, p);
+                        const int t = X.nt - p - 1;
+                        if (t > 0) {
+                            k_front_trsm<<<t, kFT, 0, cs>>>(X, p);
+                            k_front_syrk<<<t * (t + 1) / 2, 256, 0, cs>>>(X, p);
+                        }
+                    }
+                    k_front_solve<<<1, 1024, sizeof(double) * X.N, cs>>>(F, X);
+                }
+                for (int L = top - 1; L >= 0; L--) {
                     const int c0 = c->lvl_col_ptr[L], c1 = c->lvl_col_ptr[L + 1];
                     k_fem_backward_level<<<c1 - c0, kUnit, 0, cs>>>(F, c0);
                 }
@@ -1088,6 +1146,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->pcg_learned_scale = 0;
     cfg->graphs = 1;
     cfg->beam_kernel = 0;
+    cfg->fem_dense_front = 1;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -1113,7 +1172,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
     if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 3 || c0.pcg_max_iters < 0 ||
-        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1)
+        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 1)
         return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
@@ -1248,6 +1307,19 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
         if (d->tris[t].a >= (uint32_t)d->n_nodes || d->tris[t].b >= (uint32_t)d->n_nodes || d->tris[t].c >= (uint32_t)d->n_nodes) return BL_GPU_EINVAL;
     if (d->self_collision) return BL_GPU_EUNSUPPORTED;                               // (a body's nodes against its own triangles)
     if (d->n_tris > 0 && d->fem && d->fem->n_tris > 0) return BL_GPU_EUNSUPPORTED; // (contacts of frame nodes)
+    if (d->fem && d->fem->n_tris > 0 && d->fem->tris && d->n_beams > 0) {
+        // a beam on a frame node is a spring of the frame's implicit step in the reference (its links, frame_fem.cpp:
+        // 576-590, 2774-2825): not on this path
+        std::vector<uint8_t> on_frame(d->n_nodes, 0);
+        for (int t = 0; t < d->fem->n_tris; t++) {
+            const bl_fem_tri& ft = d->fem->tris[t];
+            if (ft.a < (uint32_t)d->n_nodes) on_frame[ft.a] = 1;
+            if (ft.b < (uint32_t)d->n_nodes) on_frame[ft.b] = 1;
+            if (ft.c < (uint32_t)d->n_nodes) on_frame[ft.c] = 1;
+        }
+        for (int j = 0; j < d->n_beams; j++)
+            if (on_frame[d->beams[j].a] || on_frame[d->beams[j].b]) return BL_GPU_EUNSUPPORTED;
+    }
     if (c->bodies.size() >= (size_t)(1 << 23)) return BL_GPU_ELIMIT;               // (a triangle keeps its body in 23 bits)
     HostBody hb;
     hb.nodes.assign(d->nodes, d->nodes + d->n_nodes);

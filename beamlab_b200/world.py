@@ -72,6 +72,8 @@ class WorldSettings:
     graphs: bool = True
     # the beams' kernel: 0 streams the beam arrays by bulk (TMA) copies, 1 plain loads (the same results)
     beam_kernel: int = 0
+    # the FEM factorization's top chain as one dense front (True) or block column by block column (False)
+    fem_dense_front: bool = True
 
 
 @dataclass
@@ -315,7 +317,7 @@ class _Config(C.Structure):
                 ("collision_hz", C.c_float), ("inter_body_collisions", C.c_int32), ("max_pairs", C.c_int32),
                 ("fem_solver", C.c_int32), ("pcg_max_iters", C.c_int32), ("pcg_tol", C.c_float),
                 ("fem_check_residual", C.c_int32), ("pcg_learned_scale", C.c_int32), ("graphs", C.c_int32),
-                ("beam_kernel", C.c_int32)]
+                ("beam_kernel", C.c_int32), ("fem_dense_front", C.c_int32)]
 
 
 class _FemStats(C.Structure):
@@ -407,6 +409,7 @@ class World:
         cfg.pcg_learned_scale = int(self.settings.pcg_learned_scale)
         cfg.graphs = int(self.settings.graphs)
         cfg.beam_kernel = int(self.settings.beam_kernel)
+        cfg.fem_dense_front = int(self.settings.fem_dense_front)
         self._ctx = C.c_void_p()
         _check(self._L.bl_gpu_create(C.byref(cfg), C.byref(self._ctx)), "create")
         self._bodies: list[BodyHandle] = []

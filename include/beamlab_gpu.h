@@ -84,6 +84,9 @@ typedef struct {
                                   kernels are launched one by one every call (the plain path, one launch per kernel) */
     int32_t beam_kernel;       /* 0 (default): the beams' kernel streams the beam arrays through shared memory by bulk
                                   (TMA) copies; 1: plain loads. Results are the same. */
+    int32_t fem_dense_front;   /* 1 (default): the FEM factorization takes the top chain of its elimination tree (levels of
+                                  one column each) as one dense front (a blocked dense Cholesky and dense solves); 0: block
+                                  column by block column in the reference's order of sums throughout */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };
