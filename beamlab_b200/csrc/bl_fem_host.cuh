@@ -175,12 +175,25 @@ static void tri_stiffness_host(const float X[3][2], const FemSection& s, float P
         }
 }
 
-// One body's frame of triangle elements, as built and analysed
+struct FrameSectionH { // FrameSection (frame_fem.h:90-112): the elastic member step's fields
+    float E, G, rho, A, Iy, Iz, J, As_y, As_z, damping, axial, joint_k;
+};
+
+// One body's frame of members and triangle elements, as built and analysed
 struct FemModel {
-    // frame nodes (in the order add_tri made them: each triangle's corners a, b, c)
+    // frame nodes (in the order add_element and add_tri made them: each member's a, b, then each triangle's corners)
     std::vector<uint32_t> node;      // body node of each frame node
     std::vector<double> xd;          // 3 per frame node
     std::vector<float> inertia;
+    // members (FemFrame::elems)
+    std::vector<std::array<int, 2>> mn;  // frame nodes a, b
+    std::vector<uint16_t> msec;
+    std::vector<uint8_t> mend;       // 2 per member: the joints at a, b
+    std::vector<float> mL0, mmass;   // rest length; the mass it put on its nodes
+    std::vector<float> mq;           // 8 per member: its rest frame in its end nodes' frames, qa then qb (x y z w)
+    std::vector<uint8_t> mbroken;
+    std::vector<int> mblock;         // its off-diagonal block (-1: its ends share a column)
+    std::vector<uint8_t> mswap;      // the block's row is its a end
     // triangles
     std::vector<std::array<int, 3>> tn;  // frame nodes
     std::vector<uint16_t> tsec;
@@ -197,18 +210,41 @@ struct FemModel {
     std::vector<std::array<int, 3>> upd; // (pi, pj, target)
     std::vector<std::array<int, 3>> tri_block;
     std::vector<std::array<uint8_t, 3>> tri_swap;
-    // gather lists: per column, its triangles' corners (tri, corner); per off-diagonal block, (tri, i, j)
+    // gather lists, members first (gather_lists, frame_fem.cpp:863-901): per column its members' ends (-(member + 1),
+    // end 0 a / 1 b) and its triangles' corners (tri, corner); per off-diagonal block (-(member + 1), 2: block (b, a)
+    // / 3: block (a, b), 0) and (tri, i, j)
     std::vector<int> gdiag_ptr, goff_ptr;
     std::vector<std::array<int, 2>> gdiag;
     std::vector<std::array<int, 3>> goff;
 };
 
-// FemFrame::finalize's triangle part and node inertias (frame_fem.cpp:224-260, 3075-3086): p, mass - the body's node
-// positions and masses
-static void fem_finalize(FemModel& M, const float* px, const float* py, const float* pz, const float* mass) {
+// FemFrame::finalize (frame_fem.cpp:224-260) and the node inertias (node_inertia, frame_fem.cpp:3075-3086): p, mass - the
+// body's node positions and masses; mpm - each member's section's mass per metre (FrameSection::mass_per_m)
+static void fem_finalize(FemModel& M, const float* px, const float* py, const float* pz, const float* mass, const std::vector<float>& mpm) {
     const size_t n = M.node.size();
     M.xd.resize(n * 3);
     for (size_t i = 0; i < n; i++) M.xd[3 * i] = px[M.node[i]], M.xd[3 * i + 1] = py[M.node[i]], M.xd[3 * i + 2] = pz[M.node[i]];
+    const size_t E = M.mn.size();
+    M.mL0.assign(E, 0.0f), M.mq.assign(8 * E, 0.0f), M.mbroken.assign(E, 0);
+    for (size_t e = 0; e < E; e++) {
+        const int a = M.mn[e][0], b = M.mn[e][1];
+        const HF3 xa = h3(px[M.node[a]], py[M.node[a]], pz[M.node[a]]), xb = h3(px[M.node[b]], py[M.node[b]], pz[M.node[b]]);
+        const HF3 d = hsub(xb, xa);
+        const float L0 = hlen(d);
+        M.mL0[e] = L0;
+        if (L0 < 1e-5f || a == b) {
+            M.mbroken[e] = 1;
+            continue;
+        }
+        // the rest frame: x along the member, y towards the world's up (a vertical member: towards x)
+        const HF3 e1 = hmul(d, 1.0f / L0);
+        const HF3 ref = std::fabs(e1.y) < 0.9f ? h3(0, 1, 0) : h3(1, 0, 0);
+        const HF3 e2 = hnormalize(hsub(ref, hmul(e1, hdot(e1, ref)))), e3 = hcross(e1, e2);
+        const HQ E0 = hfrom_mat3(e1, e2, e3);
+        const HQ r = hqnormalize(hqmul(hqconj(HQ{0, 0, 0, 1}), E0)); // (both ends' rest orientation: the identity)
+        for (int h = 0; h < 2; h++) M.mq[8 * e + 4 * h] = r.x, M.mq[8 * e + 4 * h + 1] = r.y, M.mq[8 * e + 4 * h + 2] = r.z, M.mq[8 * e + 4 * h + 3] = r.w;
+        if (M.mmass[e] <= 0) M.mmass[e] = mpm[e] * L0;
+    }
     const size_t T = M.tn.size();
     M.tX.assign(T * 6, 0.0f), M.tr0.assign(T * 12, 0.0f), M.tarea0.assign(T, 0.0f), M.tbroken.assign(T, 0);
     for (size_t t = 0; t < T; t++) {
@@ -236,6 +272,13 @@ static void fem_finalize(FemModel& M, const float* px, const float* py, const fl
     }
     M.inertia.assign(n, 0.0f);
     std::vector<float> I(n, 0.0f);
+    // (the members' halves first, each node's sum in member order: the lumped m L^2 / 78 an end, m = mass_per_m L0)
+    for (size_t e = 0; e < E; e++) {
+        if (M.mbroken[e]) continue;
+        const float add = mpm[e] * M.mL0[e] * M.mL0[e] * M.mL0[e] / 78.0f;
+        I[M.mn[e][0]] += add;
+        if (M.mn[e][1] != M.mn[e][0]) I[M.mn[e][1]] += add;
+    }
     for (size_t t = 0; t < T; t++) {
         if (M.tbroken[t]) continue;
         const int* fn = M.tn[t].data();
@@ -250,7 +293,7 @@ static void fem_finalize(FemModel& M, const float* px, const float* py, const fl
     }
 }
 
-// FemFrame::analyse + gather_lists (frame_fem.cpp:544-901) for triangle elements
+// FemFrame::analyse + gather_lists (frame_fem.cpp:544-901) for members and triangle elements
 static void fem_analyse(FemModel& M) {
     const int n = (int)M.node.size();
     const size_t T = M.tn.size();
@@ -260,9 +303,13 @@ static void fem_analyse(FemModel& M) {
         while (up[x] != x) x = up[x] = up[up[x]];
         return x;
     };
+    const size_t E = M.mn.size();
+    for (size_t e = 0; e < E; e++) up[find(M.mn[e][0])] = find(M.mn[e][1]);
     for (size_t t = 0; t < T; t++)
         if (!M.tbroken[t]) up[find(M.tn[t][0])] = find(M.tn[t][1]), up[find(M.tn[t][1])] = find(M.tn[t][2]);
     std::vector<std::pair<int, int>> edge;
+    for (size_t e = 0; e < E; e++)
+        if (M.mn[e][0] != M.mn[e][1]) edge.push_back({M.mn[e][0], M.mn[e][1]});
     for (size_t t = 0; t < T; t++) {
         if (M.tbroken[t]) continue;
         const int a = M.tn[t][0], b = M.tn[t][1], c = M.tn[t][2];
@@ -381,6 +428,14 @@ static void fem_analyse(FemModel& M) {
         }
         M.upd_ptr[kk + 1] = (int)M.upd.size();
     }
+    M.mblock.assign(E, -1);
+    M.mswap.assign(E, 0);
+    for (size_t e = 0; e < E; e++) {
+        const int ka = M.iperm[M.mn[e][0]], kb = M.iperm[M.mn[e][1]];
+        if (ka == kb) continue;
+        M.mblock[e] = find_block(std::min(ka, kb), std::max(ka, kb));
+        M.mswap[e] = ka > kb;
+    }
     M.tri_block.assign(T, {-1, -1, -1});
     M.tri_swap.assign(T, {0, 0, 0});
     for (size_t t = 0; t < T; t++) {
@@ -395,6 +450,10 @@ static void fem_analyse(FemModel& M) {
     // gather lists in the triangles' order (gather_lists, frame_fem.cpp:863-901)
     M.gdiag_ptr.assign(n + 1, 0);
     M.goff_ptr.assign(M.row.size() + 1, 0);
+    for (size_t e = 0; e < E; e++) {
+        M.gdiag_ptr[M.iperm[M.mn[e][0]] + 1]++, M.gdiag_ptr[M.iperm[M.mn[e][1]] + 1]++;
+        if (M.mblock[e] >= 0) M.goff_ptr[M.mblock[e] + 1]++;
+    }
     for (size_t t = 0; t < T; t++) {
         if (M.tbroken[t]) continue;
         for (int c = 0; c < 3; c++) M.gdiag_ptr[M.iperm[M.tn[t][c]] + 1]++;
@@ -406,6 +465,11 @@ static void fem_analyse(FemModel& M) {
     M.gdiag.assign(M.gdiag_ptr.back(), {0, 0});
     M.goff.assign(M.goff_ptr.back(), {0, 0, 0});
     std::vector<int> fd(M.gdiag_ptr.begin(), M.gdiag_ptr.end() - 1), fo(M.goff_ptr.begin(), M.goff_ptr.end() - 1);
+    for (size_t e = 0; e < E; e++) {
+        M.gdiag[fd[M.iperm[M.mn[e][0]]]++] = {-(int)e - 1, 0};
+        M.gdiag[fd[M.iperm[M.mn[e][1]]]++] = {-(int)e - 1, 1};
+        if (M.mblock[e] >= 0) M.goff[fo[M.mblock[e]]++] = {-(int)e - 1, M.mswap[e] ? 3 : 2, 0}; // (the row node's: b, or a)
+    }
     for (size_t t = 0; t < T; t++) {
         if (M.tbroken[t]) continue;
         for (int c = 0; c < 3; c++) M.gdiag[fd[M.iperm[M.tn[t][c]]]++] = {(int)t, c};

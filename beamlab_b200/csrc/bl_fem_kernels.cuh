@@ -78,6 +78,20 @@ struct FemDev {
     int* body_failures;      // / body
     int* body_clamps;        // / body
     float h, step;
+    // members (k_member_eval)
+    int nmem;
+    const int2* mn;          // frame nodes a, b
+    const int* mmeta;        // section | joint at a << 16 | joint at b << 24; -1: broken at rest
+    const float* mL0;
+    const float4* mq;        // 2 / member: its rest frame in a's and in b's frame
+    const struct FemMemSecDev* msec;
+    float4* mfa;             // force on a (on b: its negative)
+    float4* mta;             // torque on a
+    float4* mtb;             // torque on b
+    uint8_t* mon;            // evaluated this substep (FemFrame::Tangent::on)
+    float4* mtan;            // the tangent's axis e1 and N / L (its geometric stiffness)
+    double* mkw;             // 144 / member: the world blocks aa, bb, ba, ab (FemFrame::mem_kw_)
+    double* mkv;             // 12 / member: K v (FemFrame::mem_kv_)
 };
 
 // ------------------------------------------------------------------------------------------ quaternions (math.h:105-215)
@@ -276,6 +290,214 @@ __global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __rest
     F.ton[ti] = 1;
 }
 
+// ------------------------------------------------------------------------------------------ members (frame beams)
+// FemFrame::eval_forces for elastic members (frame_fem.cpp:1896-2070 with no plastic limits: Np = Mp = Tp = 0, no
+// joint damping, no break force): the co-rotated frame (kinematics, frame_fem.cpp:1384-1406), the joints' end
+// stiffnesses (stiffness, frame_fem.cpp:1408-1476), the axial force, torque and end moments, the nodal forces
+// -B^T g, the tangent and its world blocks with K v (member_world_k / element_matrix, frame_fem.cpp:1834-1850,
+// 2157-2186), a thread a member, float where the reference is float and double where it is double.
+struct FemMemSecDev { // FrameSection (frame_fem.h:90-112)
+    float E, G, rho, A, Iy, Iz, J, As_y, As_z, damping, axial, joint_k;
+};
+enum : int { FJ_RIGID = 0, FJ_BALL = 1, FJ_HINGE_V = 2, FJ_HINGE_H = 3, FJ_SWIVEL = 4, FJ_ELASTIC = 5 };
+
+__device__ __forceinline__ v3 cross3(v3 a, v3 b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+__device__ __forceinline__ v3 qrotate(q4 q, v3 p) { // quat::rotate (math.h:150-154)
+    const v3 u = V(q.x, q.y, q.z);
+    const v3 t = cross3(u, p) * 2.0f;
+    return p + t * q.w + cross3(u, t);
+}
+__device__ __forceinline__ q4 qscale(q4 q, float s) { return {q.x * s, q.y * s, q.z * s, q.w * s}; }
+__device__ __forceinline__ q4 qadd(q4 a, q4 b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
+// quat::axis_angle (math.h:136-140)
+__device__ __forceinline__ q4 qaxis_angle(v3 axis, float angle) {
+    const float h = angle * 0.5f, s = sinf(h);
+    const v3 a = normalize(axis);
+    return {a.x * s, a.y * s, a.z * s, cosf(h)};
+}
+// quat_from_to (math.h:203-212): the minimal rotation taking unit a to unit b
+__device__ __forceinline__ q4 qfrom_to(v3 a, v3 b) {
+    const float d = dot(a, b);
+    if (d < -0.999999f) {
+        const v3 t = fabsf(a.x) < 0.7f ? V(1, 0, 0) : V(0, 1, 0); // (any_perpendicular, math.h:82-85)
+        return qaxis_angle(normalize(cross3(a, t)), 3.14159265358979323846f);
+    }
+    const v3 c = cross3(a, b);
+    return qnormalize(q4{c.x, c.y, c.z, 1.0f + d});
+}
+// slerp (math.h:227-232)
+__device__ __forceinline__ q4 qslerp(q4 a, q4 b, float t) {
+    float d = a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
+    if (d < 0) b = qscale(b, -1.0f), d = -d;
+    if (d > 0.9995f) return qnormalize(qadd(a, qscale(qadd(b, qscale(a, -1.0f)), t)));
+    const float th = acosf(d), s = sinf(th);
+    return qadd(qscale(a, sinf((1 - t) * th) / s), qscale(b, sinf(t * th) / s));
+}
+
+// what a joint frees (twist, about y, about z) and its flexibility (end_flex, frame_fem.cpp:1420-1431)
+struct EndFlexD {
+    bool rel[3];
+    float f;
+};
+__device__ __forceinline__ EndFlexD end_flex_dev(int j, float joint_k) {
+    EndFlexD e{{false, false, false}, 0.0f};
+    if (j == FJ_BALL) e.rel[0] = e.rel[1] = e.rel[2] = true;
+    else if (j == FJ_HINGE_V) e.rel[2] = true;
+    else if (j == FJ_HINGE_H) e.rel[1] = true;
+    else if (j == FJ_SWIVEL) e.rel[0] = true;
+    else if (j == FJ_ELASTIC) e.f = joint_k > 0 ? 1.0f / joint_k : 0.0f;
+    return e;
+}
+// condense / ends2 (frame_fem.cpp:1414-1418, 1435-1454)
+__device__ __forceinline__ void condense_dev(float c[3], bool pin_a, bool pin_b) {
+    if (pin_a && pin_b) c[0] = c[1] = c[2] = 0;
+    else if (pin_a) c[2] = c[0] > 0 ? c[2] - c[1] * c[1] / c[0] : 0, c[0] = c[1] = 0;
+    else if (pin_b) c[0] = c[2] > 0 ? c[0] - c[1] * c[1] / c[2] : 0, c[1] = c[2] = 0;
+}
+__device__ __forceinline__ void ends2_dev(float c[3], bool ra, bool rb, float fa, float fb) {
+    if (ra || rb) {
+        condense_dev(c, ra, rb);
+        if (ra != rb) {
+            float& k = ra ? c[2] : c[0];
+            const float f = ra ? fb : fa;
+            if (f > 0 && k > 0) k = 1.0f / (1.0f / k + f);
+        }
+        return;
+    }
+    if (fa <= 0 && fb <= 0) return;
+    const double det = (double)c[0] * c[2] - (double)c[1] * c[1];
+    if (!(det > 0)) return;
+    const double F00 = c[2] / det + fa, F01 = -c[1] / det, F11 = c[0] / det + fb;
+    const double d2 = F00 * F11 - F01 * F01;
+    c[0] = (float)(F11 / d2), c[1] = (float)(-F01 / d2), c[2] = (float)(F00 / d2);
+}
+
+__global__ void __launch_bounds__(128) k_member_eval(FemDev F, const float4* __restrict__ nd) {
+    const int ei = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ei >= F.nmem) return;
+    F.mon[ei] = 0;
+    const int meta = F.mmeta[ei];
+    if (meta < 0) return; // (broken: no length at rest)
+    const int2 ab = F.mn[ei];
+    const int endA = (meta >> 16) & 0xff, endB = (meta >> 24) & 0x7f;
+    const FemMemSecDev s = F.msec[meta & 0xffff];
+    const float L0 = F.mL0[ei];
+    // ---- kinematics
+    const double* xa = F.xd + 3 * (size_t)ab.x;
+    const double* xb = F.xd + 3 * (size_t)ab.y;
+    const double dx = xb[0] - xa[0], dy = xb[1] - xa[1], dz = xb[2] - xa[2];
+    const double Ld = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(Ld > 1e-6) || !isfinite(Ld)) return;
+    const float L = (float)Ld;
+    const double dL = Ld - (double)L0;
+    const v3 e1 = V((float)(dx / Ld), (float)(dy / Ld), (float)(dz / Ld));
+    const float4 qa4 = F.q[ab.x], qb4 = F.q[ab.y], ra4 = F.mq[2 * ei], rb4 = F.mq[2 * ei + 1];
+    const q4 Ea = qnormalize(qmul(q4{qa4.x, qa4.y, qa4.z, qa4.w}, q4{ra4.x, ra4.y, ra4.z, ra4.w}));
+    const q4 Eb = qnormalize(qmul(q4{qb4.x, qb4.y, qb4.z, qb4.w}, q4{rb4.x, rb4.y, rb4.z, rb4.w}));
+    const bool fta = endA == FJ_BALL || endA == FJ_SWIVEL, ftb = endB == FJ_BALL || endB == FJ_SWIVEL;
+    const float tw8 = fta == ftb ? 0.5f : fta ? 1.0f : 0.0f; // (twist_weight, frame_fem.cpp:1372-1375)
+    const q4 Em = tw8 <= 0.0f ? Ea : tw8 >= 1.0f ? Eb : qslerp(Ea, Eb, tw8);
+    const q4 E = qnormalize(qmul(qfrom_to(normalize(qrotate(Em, V(1, 0, 0))), e1), Em));
+    const q4 Ec = qconj(E);
+    const v3 ra = quat_log(qmul(Ec, Ea)), rb = quat_log(qmul(Ec, Eb));
+    const v3 e2 = qrotate(E, V(0, 1, 0)), e3 = qrotate(E, V(0, 0, 1));
+    // ---- the section's stiffness with the joints
+    const EndFlexD fa = end_flex_dev(endA, s.joint_k), fb = end_flex_dev(endB, s.joint_k);
+    const float ka = s.axial * s.E * s.A / L0;
+    float kt = s.G * s.J / L0;
+    if (fa.rel[0] || fb.rel[0]) kt = 0;
+    else if (fa.f + fb.f > 0) kt = 1.0f / (1.0f / kt + fa.f + fb.f);
+    float cy[3], cz[3];
+    {
+        const float phi = s.As_z > 0 ? 12.0f * s.E * s.Iy / (s.G * s.As_z * L0 * L0) : 0.0f;
+        const float k0 = s.E * s.Iy / (L0 * (1.0f + phi));
+        cy[0] = cy[2] = (4.0f + phi) * k0;
+        cy[1] = (2.0f - phi) * k0;
+        ends2_dev(cy, fa.rel[1], fb.rel[1], fa.f, fb.f);
+    }
+    {
+        const float phi = s.As_y > 0 ? 12.0f * s.E * s.Iz / (s.G * s.As_y * L0 * L0) : 0.0f;
+        const float k0 = s.E * s.Iz / (L0 * (1.0f + phi));
+        cz[0] = cz[2] = (4.0f + phi) * k0;
+        cz[1] = (2.0f - phi) * k0;
+        ends2_dev(cz, fa.rel[2], fb.rel[2], fa.f, fb.f);
+    }
+    // ---- forces: elastic (no plastic parts: up = tp = 0, pa = pb = 0)
+    const float delta = (float)dL;
+    const float N = ka * (delta - 0.0f);
+    const float twist = rb.x - ra.x;
+    const float T = kt * (twist - 0.0f);
+    const float dax = ra.y - 0.0f, day = ra.z - 0.0f, dbx = rb.y - 0.0f, dby = rb.z - 0.0f;
+    const float Max = cy[0] * dax + cy[1] * dbx, May = cz[0] * day + cz[1] * dby;
+    const float Mbx = cy[1] * dax + cy[2] * dbx, Mby = cz[1] * day + cz[2] * dby;
+    const float Sy = Max + Mbx, Sz = May + Mby;
+    const v3 fav = e1 * N + e3 * (Sy / L) - e2 * (Sz / L);
+    const v3 tav = e1 * T - e2 * Max - e3 * May;
+    const v3 tbv = e1 * (-T) - e2 * Mbx - e3 * Mby;
+    F.mfa[ei] = make_float4(fav.x, fav.y, fav.z, 0.0f);
+    F.mta[ei] = make_float4(tav.x, tav.y, tav.z, 0.0f);
+    F.mtb[ei] = make_float4(tbv.x, tbv.y, tbv.z, 0.0f);
+    F.mon[ei] = 1;
+    F.mtan[ei] = make_float4(e1.x, e1.y, e1.z, N > 0 ? N / L : 0.0f);
+    // ---- the tangent's world blocks (element_matrix in 3 x 3 blocks of [ua, pa, ub, pb]) and K v
+    const double iL = 1.0 / L;
+    const double E1[3] = {e1.x, e1.y, e1.z}, E2[3] = {e2.x, e2.y, e2.z}, E3[3] = {e3.x, e3.y, e3.z};
+    const double g[3] = {E3[0] * iL, E3[1] * iL, E3[2] * iL}, h[3] = {E2[0] * iL, E2[1] * iL, E2[2] * iL};
+    const double cy0 = cy[0], cy1 = cy[1], cy2 = cy[2], cz0 = cz[0], cz1 = cz[1], cz2 = cz[2];
+    const double Sy2 = cy0 + 2 * cy1 + cy2, Sz2 = cz0 + 2 * cz1 + cz2, ay = cy0 + cy1, by = cy1 + cy2, az = cz0 + cz1, bz = cz1 + cz2;
+    const double kad = ka, ktd = kt;
+    double K[12][12];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            const double uu = kad * E1[i] * E1[j] + Sy2 * g[i] * g[j] + Sz2 * h[i] * h[j];
+            const double up = -ay * g[i] * E2[j] + az * h[i] * E3[j];
+            const double ub = -by * g[i] * E2[j] + bz * h[i] * E3[j];
+            const double tt = ktd * E1[i] * E1[j];
+            const double pa = tt + cy0 * E2[i] * E2[j] + cz0 * E3[i] * E3[j];
+            const double pb = -tt + cy1 * E2[i] * E2[j] + cz1 * E3[i] * E3[j];
+            const double qb = tt + cy2 * E2[i] * E2[j] + cz2 * E3[i] * E3[j];
+            K[i][j] = uu, K[i][3 + j] = up, K[i][6 + j] = -uu, K[i][9 + j] = ub;
+            K[3 + i][3 + j] = pa, K[3 + i][9 + j] = pb;
+            K[6 + i][6 + j] = uu, K[6 + i][9 + j] = -ub;
+            K[9 + i][9 + j] = qb;
+        }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) K[3 + i][6 + j] = -K[j][3 + i];
+    for (int r = 0; r < 12; r++)
+        for (int c2 = r + 1; c2 < 12; c2++) K[c2][r] = K[r][c2];
+    double* W = F.mkw + 144 * (size_t)ei;
+    for (int r = 0; r < 6; r++)
+        for (int q = 0; q < 6; q++)
+            W[r * 6 + q] = K[r][q], W[36 + r * 6 + q] = K[6 + r][6 + q], W[72 + r * 6 + q] = K[6 + r][q], W[108 + r * 6 + q] = K[r][6 + q];
+    const float4 va = nd[2 * F.fnode[ab.x] + 1], vb = nd[2 * F.fnode[ab.y] + 1], wa = F.w[ab.x], wb = F.w[ab.y];
+    const double u[12] = {va.x, va.y, va.z, wa.x, wa.y, wa.z, vb.x, vb.y, vb.z, wb.x, wb.y, wb.z};
+    double* kv = F.mkv + 12 * (size_t)ei;
+    for (int r = 0; r < 12; r++) {
+        double s2 = 0;
+        for (int q = 0; q < 12; q++) s2 += K[r][q] * u[q];
+        kv[r] = s2;
+    }
+}
+
+// gather_part's member block (frame_fem.cpp:927-941): block blk (0 aa, 1 bb, 2 ba, 3 ab) times c, with the geometric
+// stiffness of its tension (sign gs)
+__device__ __forceinline__ void member_block_add(const FemDev& F, int ei, int blk, double h2, double gs, double* D) {
+    const int meta = F.mmeta[ei];
+    const double c = h2 + (double)F.msec[meta & 0xffff].damping * F.h;
+    const double* B = F.mkw + 144 * (size_t)ei + 36 * blk;
+    for (int x = 0; x < 36; x++) D[x] += c * B[x];
+    const float4 t = F.mtan[ei];
+    const double gg = h2 * t.w;
+    if (gg != 0) {
+        double P[9];
+        const double ee[3] = {t.x, t.y, t.z};
+        for (int r = 0; r < 3; r++)
+            for (int q = 0; q < 3; q++) P[r * 3 + q] = gg * ((r == q ? 1.0 : 0.0) - ee[r] * ee[q]);
+        for (int r = 0; r < 3; r++)
+            for (int q = 0; q < 3; q++) D[r * 6 + q] += gs * P[r * 3 + q];
+    }
+}
+
 // ------------------------------------------------------------------------------------------ assembly
 // A triangle's block of corners (i, j) in the world's axes times c, with its tension's geometric stiffness
 // (gather_part's tri_block, frame_fem.cpp:961-1003)
@@ -341,6 +563,17 @@ __device__ __forceinline__ void assemble_column(const FemDev& F, const float4* _
         double rd[6] = {0, 0, 0, 0, 0, 0};
         for (int qq = F.gdiag_ptr[k]; qq < F.gdiag_ptr[k + 1]; qq++) {
             const int2 g = F.gdiag[qq];
+            if (g.x < 0) { // (a member's end: -(member + 1), end)
+                const int ei = -g.x - 1;
+                if (!F.mon[ei]) continue;
+                member_block_add(F, ei, g.y, h2, 1.0, D);
+                const double cr = hd + (double)F.msec[F.mmeta[ei] & 0xffff].damping * F.h;
+                if (cr != 0) {
+                    const double* kv = F.mkv + 12 * (size_t)ei + 6 * g.y;
+                    for (int j = 0; j < 6; j++) rd[j] -= cr * kv[j];
+                }
+                continue;
+            }
             if (!F.ton[g.x]) continue;
             tri_block_add(F, g.x, g.y, g.y, h2, D);
             const double cr = hd + (double)F.sec[F.tn[g.x].w].damping * F.h;
@@ -371,7 +604,11 @@ __device__ __forceinline__ void assemble_off(const FemDev& F, const float4* __re
     if (!fixed && F.goff_ptr[pb] != F.goff_ptr[pb + 1] && !(nd[2 * rnode].w <= 0))
         for (int qq = F.goff_ptr[pb]; qq < F.goff_ptr[pb + 1]; qq++) {
             const int4 g = F.goff[qq];
-            if (F.ton[g.x]) tri_block_add(F, g.x, g.y, g.z, h2, O);
+            if (g.x < 0) { // (a member's block: -(member + 1), 2 ba / 3 ab)
+                if (F.mon[-g.x - 1]) member_block_add(F, -g.x - 1, g.y, h2, -1.0, O);
+            } else if (F.ton[g.x]) {
+                tri_block_add(F, g.x, g.y, g.z, h2, O);
+            }
         }
     double* Og = F.off + 36 * (size_t)pb;
     for (int x = 0; x < 36; x++) Og[x] = O[x];

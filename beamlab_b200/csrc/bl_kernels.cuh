@@ -505,6 +505,10 @@ struct NodeFem {
     float4* torque;
     float4* nforce;
     const float4* ext;       // constant node forces (bl_gpu_set_node_force)
+    const uint8_t* mon;      // the members' forces of the substep (k_member_eval)
+    const float4* mfa;
+    const float4* mta;
+    const float4* mtb;
 };
 
 // the bounds, top speed and static contacts of a warp's nodes into their bodies' accumulators (a warp of one body
@@ -551,6 +555,15 @@ __device__ __forceinline__ void fem_gather(const NodeFem& nf, int i, v3 f) {
         v3 tq = V(0, 0, 0);
         for (int g = nf.gdiag_ptr[k]; g < nf.gdiag_ptr[k + 1]; g++) {
             const int2 e = nf.gdiag[g];
+            if (e.x < 0) { // (a member's end a (+fa, ta) or b (-fa, tb): gather_forces, frame_fem.cpp:2092-2096)
+                const int ei = -e.x - 1;
+                if (!nf.mon[ei]) continue;
+                const float4 fa = nf.mfa[ei], tq4 = e.y == 0 ? nf.mta[ei] : nf.mtb[ei];
+                if (e.y == 0) f = V(f.x + fa.x, f.y + fa.y, f.z + fa.z);
+                else f = V(f.x - fa.x, f.y - fa.y, f.z - fa.z);
+                tq = V(tq.x + tq4.x, tq.y + tq4.y, tq.z + tq4.z);
+                continue;
+            }
             if (!nf.ton[e.x]) continue;
             const float4 tf = nf.tf[3 * e.x + e.y], tt = nf.tt[3 * e.x + e.y];
             f = V(f.x + tf.x, f.y + tf.y, f.z + tf.z);

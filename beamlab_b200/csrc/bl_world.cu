@@ -44,6 +44,7 @@ struct HostBody {
     std::vector<float4> ext;               // constant node forces (empty: none)
     std::shared_ptr<FemModel> fem;         // its FEM frame (null: none), with its dynamic state q / w between commits
     std::vector<FemSection> sections;
+    std::vector<FrameSectionH> fsections;   // its members' sections
     std::vector<float> fq, fw;             // frame nodes' orientation (4) and angular velocity (3)
     float theta = 0.5f, diss = 0.02f;
     int fem_failures = 0, fem_clamps = 0;
@@ -138,6 +139,15 @@ struct bl_gpu_ctx {
     DevBuf<int2> gdiag, gu, rb;
     DevBuf<int4> goff, tn;
     DevBuf<double> xd, diag, ldiag, off, rhs, dinv, tkv, ch2, chd;
+    // the FEM members (k_member_eval)
+    int NM = 0;
+    DevBuf<int2> mn;
+    DevBuf<int> mmeta;
+    DevBuf<float> mL0;
+    DevBuf<float4> mq, mfa, mta, mtb, mtan;
+    DevBuf<FemMemSecDev> msec;
+    DevBuf<uint8_t> mon;
+    DevBuf<double> mkw, mkv;
     // the top chain of the elimination tree as one dense front (bl_fem_kernels.cuh: FrontDev); front_level: its first
     // level (the level count: none)
     FrontDev front{};
@@ -204,6 +214,8 @@ static void free_fem(bl_gpu_ctx* c) {
     c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
     c->fcol.free_(), c->fchain.free_(), c->fblk.free_(), c->fD.free_(), c->fb.free_(), c->front = FrontDev{}, c->front_level = 0;
+    c->mn.free_(), c->mmeta.free_(), c->mL0.free_(), c->mq.free_(), c->mfa.free_(), c->mta.free_(), c->mtb.free_(), c->mtan.free_();
+    c->msec.free_(), c->mon.free_(), c->mkw.free_(), c->mkv.free_(), c->NM = 0;
     c->xd.free_(), c->diag.free_(), c->ldiag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
 }
@@ -402,7 +414,12 @@ static int commit_fem(bl_gpu_ctx* c) {
     std::vector<FemSecDev> sec;
     std::vector<std::array<int, 3>> gupd; // every update (global): target, pj, pi - in the reference's order
     std::vector<int> upd_col;             // ... and its source column
-    int fo = 0, to = 0, bo = 0, co = 0, so = 0;
+    int fo = 0, to = 0, bo = 0, co = 0, so = 0, mo = 0, mso = 0;
+    std::vector<int2> mnv;                // members: frame nodes, meta, rest length, rest frames; their sections
+    std::vector<int> mmeta;
+    std::vector<float> mL0;
+    std::vector<float4> mqv;
+    std::vector<FemMemSecDev> msecv;
     for (int bi = 0; bi < c->B; bi++) {
         const HostBody& hb = c->bodies[bi];
         if (!hb.fem) continue;
@@ -427,12 +444,21 @@ static int commit_fem(bl_gpu_ctx* c) {
             col_ptr[fo + k + 1] = bo + M.col_ptr[k + 1];
             gdiag_ptr[fo + k + 1] = (int)gdiag.size() + (M.gdiag_ptr[k + 1] - M.gdiag_ptr[0]);
         }
-        for (const auto& g : M.gdiag) gdiag.push_back(make_int2(to + g[0], g[1]));
+        for (const auto& g : M.gdiag) gdiag.push_back(make_int2(g[0] < 0 ? g[0] - mo : to + g[0], g[1])); // (members: -(member + 1))
         for (int pb = 0; pb < nb; pb++) {
             row[bo + pb] = fo + M.row[pb];
             goff_ptr[bo + pb + 1] = (int)goff.size() + (M.goff_ptr[pb + 1] - M.goff_ptr[0]);
         }
-        for (const auto& g : M.goff) goff.push_back(make_int4(to + g[0], g[1], g[2], 0));
+        for (const auto& g : M.goff) goff.push_back(make_int4(g[0] < 0 ? g[0] - mo : to + g[0], g[1], g[2], 0));
+        for (size_t e = 0; e < M.mn.size(); e++) {
+            mnv.push_back(make_int2(fo + M.mn[e][0], fo + M.mn[e][1]));
+            mmeta.push_back(M.mbroken[e] ? -1 : (int)((mso + M.msec[e]) | (M.mend[2 * e] << 16) | (M.mend[2 * e + 1] << 24)));
+            mL0.push_back(M.mL0[e]);
+            mqv.push_back(make_float4(M.mq[8 * e], M.mq[8 * e + 1], M.mq[8 * e + 2], M.mq[8 * e + 3]));
+            mqv.push_back(make_float4(M.mq[8 * e + 4], M.mq[8 * e + 5], M.mq[8 * e + 6], M.mq[8 * e + 7]));
+        }
+        for (const FrameSectionH& fs : hb.fsections)
+            msecv.push_back(FemMemSecDev{fs.E, fs.G, fs.rho, fs.A, fs.Iy, fs.Iz, fs.J, fs.As_y, fs.As_z, fs.damping, fs.axial, fs.joint_k});
         for (int cc = 0; cc < M.ncomp; cc++)
             for (int k = M.comp_first[cc]; k < M.comp_first[cc + 1]; k++) col_comp[fo + k] = co + cc;
         for (int t = 0; t < nt; t++) {
@@ -457,6 +483,7 @@ static int commit_fem(bl_gpu_ctx* c) {
             level[fo + par] = std::max(level[fo + par], level[fo + k] + 1);
         }
         fo += nf, to += nt, bo += nb, co += M.ncomp, so += (int)hb.sections.size();
+        mo += (int)M.mn.size(), mso += (int)hb.fsections.size();
     }
     int nlev = 0;
     for (int k = 0; k < NF; k++) nlev = std::max(nlev, level[k] + 1);
@@ -555,6 +582,23 @@ static int commit_fem(bl_gpu_ctx* c) {
         }
     BL_CUDA(c, c->ldiag.alloc(36 * (size_t)NF));
     F.ldiag = c->ldiag.p;
+    {   // the members
+        const int E = (int)mnv.size();
+        if ((rc = upload_vec(c, c->mn, mnv)) || (rc = upload_vec(c, c->mmeta, mmeta)) || (rc = upload_vec(c, c->mL0, mL0)) ||
+            (rc = upload_vec(c, c->mq, mqv)) || (rc = upload_vec(c, c->msec, msecv)))
+            return rc;
+        BL_CUDA(c, c->mfa.alloc(E));
+        BL_CUDA(c, c->mta.alloc(E));
+        BL_CUDA(c, c->mtb.alloc(E));
+        BL_CUDA(c, c->mtan.alloc(E));
+        BL_CUDA(c, c->mon.alloc(E));
+        BL_CUDA(c, c->mkw.alloc(144 * (size_t)E));
+        BL_CUDA(c, c->mkv.alloc(12 * (size_t)E));
+        BL_CUDA(c, cudaMemsetAsync(c->mon.p, 0, std::max(E, 1), c->stream));
+        F.nmem = E, F.mn = c->mn.p, F.mmeta = c->mmeta.p, F.mL0 = c->mL0.p, F.mq = c->mq.p, F.msec = c->msec.p;
+        F.mfa = c->mfa.p, F.mta = c->mta.p, F.mtb = c->mtb.p, F.mon = c->mon.p, F.mtan = c->mtan.p, F.mkw = c->mkw.p, F.mkv = c->mkv.p;
+        c->NM = E;
+    }
     {   // the top chain (the levels from front_level up have one column each) as one dense front, when every row of
         // its columns is a chain column and it is long enough to pay
         const int nlev = (int)c->lvl_col_ptr.size() - 1;
@@ -587,7 +631,7 @@ static int commit_fem(bl_gpu_ctx* c) {
         }
         c->chol_launches = 3 * (int64_t)c->front_level;
         if (c->front_level < nlev) c->chol_launches += 1 + c->front.nt + 2 * (c->front.nt - 1) + 2;
-        c->fem_launches = 5 + c->chol_launches;
+        c->fem_launches = 4 + (c->NT > 0 ? 1 : 0) + (c->NM > 0 ? 1 : 0) + c->chol_launches; // (begin, triangles, members, assembly, velocity, integration)
     }
     // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
     for (DevBuf<double>* d : {&c->px, &c->pr, &c->pz, &c->pp, &c->ppdi}) BL_CUDA(c, d->alloc(6 * (size_t)NF));
@@ -964,7 +1008,8 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     if (c->contacts_on) k_islands<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, frame_time, c->cfg.sleeping, CT, c->deverr.p);
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
     mark();
-    NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p};
+    NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p,
+                c->mon.p, c->mfa.p, c->mta.p, c->mtb.p};
     const FemDev& F = c->fd;
     for (int k = 0; k < n; k++) {
         if (c->contacts_on) {
@@ -984,6 +1029,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                                                    c->dbodies.p, c->M, c->B);
         }
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
+        if (c->NM > 0) k_member_eval<<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
         k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0],
                                                c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
@@ -1079,14 +1125,22 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
 // A body's FEM frame of triangle elements made ready (bl_fem_host.cuh): frame nodes in the order FemFrame::add_tri
 // makes them, FemFrame::finalize's rest shapes and inertias, analyse's pattern, the elements' stiffnesses.
 static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32_t n_nodes, const bl_fem_desc& fd, std::vector<FemSection>& sections,
-                           std::shared_ptr<FemModel>& out) {
-    if (!fd.tris || !fd.sections || fd.n_sections <= 0 || !nodes || !info) return BL_GPU_EINVAL;
-    sections.clear();
-    for (int k = 0; k < fd.n_sections; k++) {
+                           std::vector<FrameSectionH>& fsections, std::shared_ptr<FemModel>& out) {
+    if (fd.n_tris < 0 || fd.n_members < 0 || (fd.n_tris > 0 && (!fd.tris || !fd.sections || fd.n_sections <= 0)) ||
+        (fd.n_members > 0 && (!fd.members || !fd.frame_sections || fd.n_frame_sections <= 0)) || fd.n_tris + fd.n_members == 0 || !nodes || !info)
+        return BL_GPU_EINVAL;
+    sections.clear(), fsections.clear();
+    for (int k = 0; k < (fd.n_tris > 0 ? fd.n_sections : 0); k++) {
         const bl_shell_section& ss = fd.sections[k];
         if (ss.yield > 0) return BL_GPU_EUNSUPPORTED; // (plastic flow, folds and tears: not on this path)
         if (!(ss.t > 0) || !(ss.E > 0)) return BL_GPU_EINVAL;
         sections.push_back(FemSection{ss.E, ss.nu, ss.rho, ss.t, ss.yield, ss.damping, ss.drill});
+    }
+    for (int k = 0; k < (fd.n_members > 0 ? fd.n_frame_sections : 0); k++) {
+        const bl_frame_section& fs = fd.frame_sections[k];
+        if (fs.Np > 0 || fs.Mp > 0 || fs.Tp > 0) return BL_GPU_EUNSUPPORTED; // (plastic hinges, yield, buckling: not on this path)
+        if (!(fs.E > 0) || !(fs.G > 0) || !(fs.A > 0)) return BL_GPU_EINVAL;
+        fsections.push_back(FrameSectionH{fs.E, fs.G, fs.rho, fs.A, fs.Iy, fs.Iz, fs.J, fs.As_y, fs.As_z, fs.damping, fs.axial, fs.joint_k});
     }
     auto M = std::make_shared<FemModel>();
     std::vector<int> slot(n_nodes, -1);
@@ -1094,23 +1148,42 @@ static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32
         if (slot[bn] < 0) slot[bn] = (int)M->node.size(), M->node.push_back(bn);
         return slot[bn];
     };
-    for (int t = 0; t < fd.n_tris; t++) {
-        const bl_fem_tri& tr = fd.tris[t];
-        if (tr.a >= (uint32_t)n_nodes || tr.b >= (uint32_t)n_nodes || tr.c >= (uint32_t)n_nodes || tr.section >= fd.n_sections) return BL_GPU_EINVAL;
-        const int a = add_node(tr.a), b = add_node(tr.b), cc = add_node(tr.c);
-        M->tn.push_back({a, b, cc});
-        M->tsec.push_back(tr.section);
-        M->tmass.push_back(tr.mass);
+    auto add_tris = [&]() {
+        for (int t = 0; t < fd.n_tris; t++) {
+            const bl_fem_tri& tr = fd.tris[t];
+            if (tr.a >= (uint32_t)n_nodes || tr.b >= (uint32_t)n_nodes || tr.c >= (uint32_t)n_nodes || tr.section >= fd.n_sections) return false;
+            const int a = add_node(tr.a), b = add_node(tr.b), cc = add_node(tr.c);
+            M->tn.push_back({a, b, cc});
+            M->tsec.push_back(tr.section);
+            M->tmass.push_back(tr.mass);
+        }
+        return true;
+    };
+    if (fd.tris_first && !add_tris()) return BL_GPU_EINVAL;
+    std::vector<float> mpm;
+    for (int e = 0; e < fd.n_members; e++) { // (the add_element calls, in the order the caller made them)
+        const bl_fem_member& mb = fd.members[e];
+        if (mb.a >= (uint32_t)n_nodes || mb.b >= (uint32_t)n_nodes || mb.section >= fd.n_frame_sections || mb.end_a > BL_FJ_ELASTIC ||
+            mb.end_b > BL_FJ_ELASTIC)
+            return BL_GPU_EINVAL;
+        const int a = add_node(mb.a), b = add_node(mb.b);
+        M->mn.push_back({a, b});
+        M->msec.push_back(mb.section);
+        M->mend.push_back(mb.end_a), M->mend.push_back(mb.end_b);
+        M->mmass.push_back(mb.mass);
+        const FrameSectionH& fs = fsections[mb.section];
+        mpm.push_back(fs.rho * fs.A); // (FrameSection::mass_per_m)
     }
+    if (!fd.tris_first && !add_tris()) return BL_GPU_EINVAL;
     for (uint32_t bn : M->node)
         if (info[bn].flags & BL_NF_GROUND) return BL_GPU_EUNSUPPORTED; // (a frame's static contacts: not on this path)
     std::vector<float> px(n_nodes), py(n_nodes), pz(n_nodes), ms(n_nodes);
     for (int i = 0; i < n_nodes; i++) px[i] = nodes[i].p[0], py[i] = nodes[i].p[1], pz[i] = nodes[i].p[2], ms[i] = nodes[i].mass;
-    fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data());
+    fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data(), mpm);
     bool again = false;
     for (size_t t = 0; t < M->tn.size(); t++) // (the caller's mass, else its section's over its area: tri_mass, frame_fem.h:373)
         if (!(M->tmass[t] > 0)) M->tmass[t] = sections[M->tsec[t]].rho * sections[M->tsec[t]].t * M->tarea0[t], again = true;
-    if (again) fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data()); // (the inertias from those masses)
+    if (again) fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data(), mpm); // (the inertias from those masses)
     fem_analyse(*M);
     M->tk.assign(162 * M->tn.size(), 0.0f);
     for (size_t t = 0; t < M->tn.size(); t++) {
@@ -1306,16 +1379,22 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
     for (int t = 0; t < d->n_tris; t++)
         if (d->tris[t].a >= (uint32_t)d->n_nodes || d->tris[t].b >= (uint32_t)d->n_nodes || d->tris[t].c >= (uint32_t)d->n_nodes) return BL_GPU_EINVAL;
     if (d->self_collision) return BL_GPU_EUNSUPPORTED;                               // (a body's nodes against its own triangles)
-    if (d->n_tris > 0 && d->fem && d->fem->n_tris > 0) return BL_GPU_EUNSUPPORTED; // (contacts of frame nodes)
-    if (d->fem && d->fem->n_tris > 0 && d->fem->tris && d->n_beams > 0) {
+    const bool has_frame = d->fem && (d->fem->n_tris > 0 || d->fem->n_members > 0);
+    if (d->n_tris > 0 && has_frame) return BL_GPU_EUNSUPPORTED; // (contacts of frame nodes)
+    if (has_frame && d->n_beams > 0) {
         // a beam on a frame node is a spring of the frame's implicit step in the reference (its links, frame_fem.cpp:
         // 576-590, 2774-2825): not on this path
         std::vector<uint8_t> on_frame(d->n_nodes, 0);
-        for (int t = 0; t < d->fem->n_tris; t++) {
+        for (int t = 0; d->fem->tris && t < d->fem->n_tris; t++) {
             const bl_fem_tri& ft = d->fem->tris[t];
             if (ft.a < (uint32_t)d->n_nodes) on_frame[ft.a] = 1;
             if (ft.b < (uint32_t)d->n_nodes) on_frame[ft.b] = 1;
             if (ft.c < (uint32_t)d->n_nodes) on_frame[ft.c] = 1;
+        }
+        for (int e = 0; d->fem->members && e < d->fem->n_members; e++) {
+            const bl_fem_member& mb = d->fem->members[e];
+            if (mb.a < (uint32_t)d->n_nodes) on_frame[mb.a] = 1;
+            if (mb.b < (uint32_t)d->n_nodes) on_frame[mb.b] = 1;
         }
         for (int j = 0; j < d->n_beams; j++)
             if (on_frame[d->beams[j].a] || on_frame[d->beams[j].b]) return BL_GPU_EUNSUPPORTED;
@@ -1345,9 +1424,9 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
         for (int k = 0; k < 3; k++) mn[k] = (n.p[k] < mn[k]) ? n.p[k] : mn[k], mx[k] = (mx[k] < n.p[k]) ? n.p[k] : mx[k];
     for (int k = 0; k < 3; k++) r.aabb_mn[k] = mn[k], r.aabb_mx[k] = mx[k];
     hb.beam_bits = (d->allow_deform ? BB_DEFORM : 0u) | (d->allow_break ? BB_BREAK : 0u) | (d->ductile ? BB_DUCTILE : 0u);
-    if (d->fem && d->fem->n_tris > 0) {
+    if (d->fem && (d->fem->n_tris > 0 || d->fem->n_members > 0)) {
         std::shared_ptr<FemModel> M;
-        const int rc = build_fem_model(d->nodes, d->info, d->n_nodes, *d->fem, hb.sections, M);
+        const int rc = build_fem_model(d->nodes, d->info, d->n_nodes, *d->fem, hb.sections, hb.fsections, M);
         if (rc) return rc;
         hb.fq.assign(4 * M->node.size(), 0.0f);
         for (size_t i = 0; i < M->node.size(); i++) hb.fq[4 * i + 3] = 1.0f;
@@ -1878,8 +1957,9 @@ int bl_fem_pattern(const bl_node* nodes, const bl_node_info* info, int32_t n_nod
                    int32_t* col_ptr, int32_t* row, int32_t* upd, float* rest, float* inertia) {
     if (!fem || !sizes || n_nodes < 0) return BL_GPU_EINVAL;
     std::vector<FemSection> secs;
+    std::vector<FrameSectionH> fsecs;
     std::shared_ptr<FemModel> M;
-    const int rc = build_fem_model(nodes, info, n_nodes, *fem, secs, M);
+    const int rc = build_fem_model(nodes, info, n_nodes, *fem, secs, fsecs, M);
     if (rc) return rc;
     const int nf = (int)M->node.size();
     sizes[0] = nf, sizes[1] = (int32_t)M->row.size(), sizes[2] = (int32_t)M->upd.size(), sizes[3] = M->ncomp;

@@ -425,3 +425,90 @@ def shell_plate(n: int = 63, size: float = 1.0, origin=(0.0, 1.0, 0.0), thicknes
     }
     return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005}, "statics": {}, "bodies": [body],
             "name": f"shell_plate(n={n}, seed={seed})"}
+
+
+def tube_section(outer: float = 0.04, wall: float = 0.003, E: float = 2.1e11, G: float = 8.1e10, rho: float = 7850.0,
+                 damping: float = 2e-5) -> dict:
+    """An elastic round steel tube's FrameSection fields (frame_fem.h:90-112): area, second moments, torsion constant,
+    Timoshenko shear areas (half the area each way)."""
+    ro, ri = outer / 2, outer / 2 - wall
+    A = math.pi * (ro * ro - ri * ri)
+    I = math.pi / 4 * (ro ** 4 - ri ** 4)
+    return {"E": E, "G": G, "rho": rho, "A": A, "Iy": I, "Iz": I, "J": 2 * I, "As_y": A / 2, "As_z": A / 2,
+            "damping": damping, "axial": 1.0, "joint_k": 2.0e4}
+
+
+def frame_ladder(rails: int = 12, spacing: float = 0.25, width: float = 0.6, origin=(0.0, 1.0, 0.0), load: float = 300.0,
+                 joints=None, section: dict | None = None) -> dict:
+    """A ladder frame of members (FemFrame::add_element): two rails of `rails` nodes along x, `spacing` apart, `width`
+    apart in z, rungs between them at every node and a diagonal in each bay; the rails' first nodes clamped (anchored);
+    a constant `load` N down (and a tenth of it across) at the far end of one rail, gravity. Each member's mass is its
+    section's rho A L, half on each end node. joints: per rung, the joints at its ends (FJ_*; default rigid) - a few
+    balls, hinges, swivels and elastic joints exercise the joints' end stiffnesses and the twist's weighting."""
+    s = section or tube_section()
+    ox, oy, oz = (np.float32(v) for v in origin)
+    n = 2 * rails
+    pos = np.zeros((n, 3), np.float32)
+    for i in range(rails):
+        for r in range(2):
+            pos[2 * i + r] = (ox + np.float32(spacing * i), oy, oz + np.float32(width * r))
+    members, ends = [], []
+    for i in range(rails - 1):  # rails
+        for r in range(2):
+            members.append((2 * i + r, 2 * (i + 1) + r)), ends.append((0, 0))
+    for i in range(rails):  # rungs
+        members.append((2 * i, 2 * i + 1))
+        ends.append(joints[i % len(joints)] if joints else (0, 0))
+    for i in range(rails - 1):  # diagonals
+        members.append((2 * i, 2 * (i + 1) + 1)), ends.append((0, 0))
+    mpm = np.float32(np.float32(s["rho"]) * np.float32(s["A"]))
+    mass = np.zeros(n, np.float32)
+    for a, b in members:
+        d = pos[b] - pos[a]
+        m = np.float32(mpm * np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1]) + np.float32(d[2] * d[2])))
+        mass[a] += np.float32(m * np.float32(0.5))
+        mass[b] += np.float32(m * np.float32(0.5))
+    flags = np.zeros(n, np.uint16)
+    flags[0] |= NF_FIXED
+    flags[1] |= NF_FIXED
+    body = {
+        "pos": pos, "vel": np.zeros((n, 3), np.float32), "mass": mass, "node_flags": flags,
+        "friction": np.ones(n, np.float32), "radius": np.zeros(n, np.float32),
+        "ab": np.zeros((0, 2), np.uint32), "k": np.zeros(0, np.float32), "d": np.zeros(0, np.float32),
+        "strength": np.zeros(0, np.float32), "deform": np.zeros(0, np.float32), "beam_type": np.zeros(0, np.uint8),
+        "beam_flags": np.zeros(0, np.uint8),
+        "params": {"ground_friction": 1.0, "bounce": -1.0, "contact_push_max": 2.0, "contact_slop": 0.0,
+                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 1, "ductile": 0, "can_sleep": 0,
+                   "sleep_speed": 0.0},
+        "frame_sections": [s], "fem_members": np.asarray(members, np.uint32),
+        "member_section": np.zeros(len(members), np.uint16), "member_ends": np.asarray(ends, np.uint8),
+        "member_mass": np.zeros(len(members), np.float32),
+        "loads": [(n - 2, (0.0, -float(load), 0.1 * float(load)))],
+    }
+    return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005}, "statics": {}, "bodies": [body],
+            "name": f"frame_ladder(rails={rails})"}
+
+
+def plate_with_rails(n: int = 20, seed: int = 1, section: dict | None = None, tris_first: bool = True) -> dict:
+    """shell_plate(n) stiffened by members: a rail of tubes along each of the two edges that run away from the clamped
+    one, on the plate's own edge nodes (a frame of members and triangles; tris_first: the plate's add_tri calls before
+    the rails' add_element calls). The rails' masses are added to their nodes."""
+    rig = shell_plate(n, seed=seed)
+    b = rig["bodies"][0]
+    s = section or tube_section(0.02, 0.002)
+    members = []
+    for j in range(n):  # (nodes j * (n + 1) + i: the edges i = 0 and i = n, along z)
+        members.append((j * (n + 1), (j + 1) * (n + 1)))
+        members.append((j * (n + 1) + n, (j + 1) * (n + 1) + n))
+    mpm = np.float32(np.float32(s["rho"]) * np.float32(s["A"]))
+    pos, mass = b["pos"], b["mass"]
+    for a, c in members:
+        d = pos[c] - pos[a]
+        m = np.float32(mpm * np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1]) + np.float32(d[2] * d[2])))
+        mass[a] += np.float32(m * np.float32(0.5))
+        mass[c] += np.float32(m * np.float32(0.5))
+    b.update({"frame_sections": [s], "fem_members": np.asarray(members, np.uint32),
+              "member_section": np.zeros(len(members), np.uint16), "member_ends": np.zeros((len(members), 2), np.uint8),
+              "member_mass": np.zeros(len(members), np.float32), "fem_tris_first": tris_first})
+    rig["name"] = f"plate_with_rails(n={n}, seed={seed}, tris_first={tris_first})"
+    return rig

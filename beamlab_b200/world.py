@@ -145,6 +145,9 @@ class SoftBody:
         # FEM frame of triangle elements (FemFrame: add_shell_section / add_tri)
         self.fem_sections: list[dict] = []
         self.fem_tris = np.zeros(0, FEM_TRI_DTYPE)
+        self.frame_sections: list[dict] = []           # FrameSection fields (frame_fem.h:90-112) by name
+        self.fem_members = np.zeros(0, FEM_MEMBER_DTYPE)
+        self.fem_tris_first = False                   # the add_tri calls before the add_element calls
         self.fem_theta = 0.5
         self.fem_dissipation = 0.02
 
@@ -211,6 +214,17 @@ class SoftBody:
             ft["section"] = np.asarray(body.get("fem_tri_section", np.zeros(len(tri))), np.uint16)
             ft["mass"] = np.asarray(body["fem_tri_mass"], np.float32)
             sb.fem_tris = ft
+        if "fem_members" in body:
+            sb.frame_sections = list(body["frame_sections"])
+            mab = np.asarray(body["fem_members"], np.uint32).reshape(-1, 2)
+            fm = np.zeros(len(mab), FEM_MEMBER_DTYPE)
+            fm["a"], fm["b"] = mab[:, 0], mab[:, 1]
+            fm["section"] = np.asarray(body.get("member_section", np.zeros(len(mab))), np.uint16)
+            ends = np.asarray(body.get("member_ends", np.zeros((len(mab), 2))), np.uint8).reshape(-1, 2)
+            fm["end_a"], fm["end_b"] = ends[:, 0], ends[:, 1]
+            fm["mass"] = np.asarray(body.get("member_mass", np.zeros(len(mab))), np.float32)
+            sb.fem_members = fm
+            sb.fem_tris_first = bool(body.get("fem_tris_first", False))
         if "tris" in body and len(body["tris"]):
             tri = np.asarray(body["tris"], np.uint32).reshape(-1, 3)
             tr = np.zeros(len(tri), TRI_DTYPE)
@@ -274,9 +288,21 @@ class _ShellSection(C.Structure):
 FEM_TRI_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("c", "<u4"), ("section", "<u2"), ("pad", "<u2"), ("mass", "<f4")])
 
 
+class _FrameSection(C.Structure):
+    _fields_ = [(k, C.c_float) for k in ("E", "G", "rho", "A", "Iy", "Iz", "J", "As_y", "As_z", "damping", "axial", "joint_k",
+                                         "Np", "Mp", "Tp")]
+
+
+# == bl_fem_member: a member between two body nodes (FemFrame::add_element), its section, the joints at its ends
+FEM_MEMBER_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("section", "<u2"), ("end_a", "u1"), ("end_b", "u1"), ("mass", "<f4")])
+FJ_RIGID, FJ_BALL, FJ_HINGE_V, FJ_HINGE_H, FJ_SWIVEL, FJ_ELASTIC = range(6)
+
+
 class _FemDesc(C.Structure):
     _fields_ = [("n_sections", C.c_int32), ("sections", C.c_void_p), ("n_tris", C.c_int32), ("tris", C.c_void_p),
-                ("theta", C.c_float), ("dissipation", C.c_float)]
+                ("theta", C.c_float), ("dissipation", C.c_float), ("n_frame_sections", C.c_int32),
+                ("frame_sections", C.c_void_p), ("n_members", C.c_int32), ("members", C.c_void_p),
+                ("tris_first", C.c_int32)]
 
 
 class _BodyDesc(C.Structure):
@@ -467,14 +493,23 @@ class World:
         info = np.ascontiguousarray(body.info, NODE_INFO_DTYPE)
         beams = np.ascontiguousarray(body.beams, BEAM_DTYPE)
         fem_ptr = None
-        if len(body.fem_tris):
-            secs = (_ShellSection * len(body.fem_sections))(*[
+        if len(body.fem_tris) or len(body.fem_members):
+            secs = (_ShellSection * max(len(body.fem_sections), 1))(*[
                 _ShellSection(float(x["E"]), float(x["nu"]), float(x["rho"]), float(x["t"]), float(x.get("yield", 0.0)),
                               float(x.get("damping", 3e-4)), float(x.get("drill", 0.05))) for x in body.fem_sections])
             tris = np.ascontiguousarray(body.fem_tris, FEM_TRI_DTYPE)
-            fd = _FemDesc(len(body.fem_sections), C.cast(secs, C.c_void_p), len(tris), tris.ctypes.data,
-                          float(body.fem_theta), float(body.fem_dissipation))
-            self._keep += [secs, tris, fd]
+            fsecs = (_FrameSection * max(len(body.frame_sections), 1))(*[
+                _FrameSection(*(float(x.get(k, d)) for k, d in (("E", 2.1e11), ("G", 8.1e10), ("rho", 7850.0), ("A", 0.0),
+                                                                 ("Iy", 0.0), ("Iz", 0.0), ("J", 0.0), ("As_y", 0.0),
+                                                                 ("As_z", 0.0), ("damping", 2e-5), ("axial", 1.0),
+                                                                 ("joint_k", 2.0e4), ("Np", 0.0), ("Mp", 0.0),
+                                                                 ("Tp", 0.0)))) for x in body.frame_sections])
+            mems = np.ascontiguousarray(body.fem_members, FEM_MEMBER_DTYPE)
+            fd = _FemDesc(len(body.fem_sections), C.cast(secs, C.c_void_p), len(tris), tris.ctypes.data if len(tris) else None,
+                          float(body.fem_theta), float(body.fem_dissipation), len(body.frame_sections),
+                          C.cast(fsecs, C.c_void_p), len(mems), mems.ctypes.data if len(mems) else None,
+                          int(body.fem_tris_first))
+            self._keep += [secs, tris, fsecs, mems, fd]
             fem_ptr = C.pointer(fd)
         d = _BodyDesc(len(nodes), nodes.ctypes.data, info.ctypes.data, len(beams), beams.ctypes.data,
                       body.ground_friction, body.bounce, body.contact_push_max, body.contact_slop,

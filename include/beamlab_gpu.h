@@ -147,9 +147,36 @@ typedef struct {
     float mass;
 } bl_fem_tri;
 
-/* A body's FEM frame of triangle elements (FemFrame, frame_fem.h:330-815: its add_tri calls; no members or mounts).
- * The library does what the reference's FemFrame::finalize and analyse do (rest shapes, inertias, the minimum-degree
- * ordering and the factor's pattern) and steps it implicitly every substep (FemFrame::solve, frame_fem.cpp:2512-3027). */
+/* == the fields of bl::phys::FrameSection (frame_fem.h:90-112) the elastic member step reads */
+typedef struct {
+    float E, G, rho;           /* Young's and shear moduli (Pa), density (kg/m3) */
+    float A, Iy, Iz, J;        /* area (m2), second moments about the local y and z axes, torsion constant (m4) */
+    float As_y, As_z;          /* shear areas along y and z (Timoshenko; 0: none) */
+    float damping;             /* stiffness-proportional damping (s) */
+    float axial;               /* a factor on the axial stiffness (1) */
+    float joint_k;             /* BL_FJ_ELASTIC joints: rotational stiffness (N m/rad) */
+    float Np, Mp, Tp;          /* plastic axial force, moment, torque: 0 only (elastic); a yielding section is
+                                  BL_GPU_EUNSUPPORTED, as are a joint's damping and a mount's break force (no fields) */
+} bl_frame_section;
+
+/* the joints at a member's ends (FrameJoint, frame_fem.h:182-193) */
+enum { BL_FJ_RIGID = 0, BL_FJ_BALL = 1, BL_FJ_HINGE_V = 2, BL_FJ_HINGE_H = 3, BL_FJ_SWIVEL = 4, BL_FJ_ELASTIC = 5 };
+
+/* A member between two body nodes, as FemFrame::add_element makes it (frame_fem.cpp:211-222); mass: the mass it put on
+ * its nodes (already in their masses; <= 0: its section's rho A L0), which sets the nodes' rotational inertia */
+typedef struct {
+    uint32_t a, b;
+    uint16_t section;          /* into bl_fem_desc.frame_sections */
+    uint8_t end_a, end_b;      /* BL_FJ_* */
+    float mass;
+} bl_fem_member;
+
+/* A body's FEM frame (FemFrame, frame_fem.h:330-815): its add_element calls (the members) and its add_tri calls (the
+ * triangles) - the frame nodes are numbered as those calls meet them, the members' first unless tris_first; no mounts
+ * or springs. The
+ * library does what the reference's FemFrame::finalize and analyse do (rest frames and shapes, inertias, the
+ * minimum-degree ordering and the factor's pattern) and steps it implicitly every substep (FemFrame::solve,
+ * frame_fem.cpp:2512-3027). */
 typedef struct {
     int32_t n_sections;
     const bl_shell_section* sections;
@@ -157,6 +184,11 @@ typedef struct {
     const bl_fem_tri* tris;
     float theta;               /* WorldSettings::frame_theta (0.5) */
     float dissipation;         /* SoftBody::fem_dissipation, else WorldSettings::frame_dissipation (0.02) */
+    int32_t n_frame_sections;
+    const bl_frame_section* frame_sections;
+    int32_t n_members;
+    const bl_fem_member* members;
+    int32_t tris_first;        /* 1: the add_tri calls came before the add_element calls */
 } bl_fem_desc;
 
 /* One body: a SoftBody after finalize (softbody.cpp:76-83) - its arrays and the knobs of the explicit path

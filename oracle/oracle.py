@@ -90,6 +90,8 @@ def _load(path: str, prefix: str) -> C.CDLL:
         lib.ref_add_plate.argtypes = [vp, i] + [f] * 9 + [f] * 7 + [i, i]
         lib.ref_add_plate.restype = i
         lib.ref_set_point_load.argtypes = [vp, i, i, f, f, f]
+        lib.ref_add_fem_body.argtypes = [vp, i, fp, fp, fp, u16p, i, fp, i, u32p, u16p, fp, i, fp, i, u32p, u16p, u8p, fp, i]
+        lib.ref_add_fem_body.restype = i
         lib.ref_fem_info.argtypes = [vp, i, C.POINTER(C.c_longlong)]
         lib.ref_fem_pattern.argtypes = [vp, i, vp, vp, vp, vp]
         lib.ref_fem_nodes.argtypes = [vp, i, vp, vp, vp, vp]
@@ -222,6 +224,39 @@ class _FemMixin:
             self._lib.ref_set_point_load(self._w, b, int(node), *map(float, fv))
         return b
 
+    def add_fem_body(self, body: dict) -> int:
+        """A body with a FEM frame of members and triangles from its arrays (FemFrame::add_section /
+        add_shell_section / add_element / add_tri in the body's order), its point loads."""
+        n = len(body["mass"])
+        a = {k: np.ascontiguousarray(body[k], dtype=dt) for k, dt in (("pos", np.float32), ("vel", np.float32),
+                                                                      ("mass", np.float32), ("node_flags", np.uint16))}
+        ss = np.asarray([[float(x["E"]), float(x["nu"]), float(x["rho"]), float(x["t"]), float(x.get("yield", 0.0)),
+                          float(x.get("damping", 3e-4)), float(x.get("drill", 0.05))] for x in body.get("fem_sections", [])],
+                        np.float32).reshape(-1, 7)
+        tri = np.ascontiguousarray(body.get("fem_tris", np.zeros((0, 3))), dtype=np.uint32).reshape(-1, 3)
+        nt = len(tri)
+        tsec = np.ascontiguousarray(body.get("fem_tri_section", np.zeros(nt)), dtype=np.uint16)
+        tmass = np.ascontiguousarray(body.get("fem_tri_mass", np.zeros(nt)), dtype=np.float32)
+        keys = ("E", "G", "rho", "A", "Iy", "Iz", "J", "As_y", "As_z", "damping", "axial", "joint_k", "Np", "Mp", "Tp")
+        dflt = {"E": 2.1e11, "G": 8.1e10, "rho": 7850.0, "damping": 2e-5, "axial": 1.0, "joint_k": 2.0e4}
+        fs = np.asarray([[float(sd.get(k, dflt.get(k, 0.0))) for k in keys] for sd in body.get("frame_sections", [])],
+                        np.float32).reshape(-1, 15)
+        ab = np.ascontiguousarray(body.get("fem_members", np.zeros((0, 2))), dtype=np.uint32).reshape(-1, 2)
+        m = len(ab)
+        msec = np.ascontiguousarray(body.get("member_section", np.zeros(m)), dtype=np.uint16)
+        ends = np.ascontiguousarray(body.get("member_ends", np.zeros((m, 2))), dtype=np.uint8)
+        mm = np.ascontiguousarray(body.get("member_mass", np.zeros(m)), dtype=np.float32)
+        self._keep += list(a.values()) + [ss, tri, tsec, tmass, fs, ab, msec, ends, mm]
+        b = self._lib.ref_add_fem_body(self._w, n, _ptr(a["pos"], C.c_float), _ptr(a["vel"], C.c_float),
+                                       _ptr(a["mass"], C.c_float), _ptr(a["node_flags"], C.c_uint16), len(ss),
+                                       _ptr(ss, C.c_float), nt, _ptr(tri, C.c_uint32), _ptr(tsec, C.c_uint16),
+                                       _ptr(tmass, C.c_float), len(fs), _ptr(fs, C.c_float), m, _ptr(ab, C.c_uint32),
+                                       _ptr(msec, C.c_uint16), _ptr(ends, C.c_uint8), _ptr(mm, C.c_float),
+                                       int(body.get("fem_tris_first", False)))
+        for node, fv in body.get("loads", []):
+            self._lib.ref_set_point_load(self._w, b, int(node), *map(float, fv))
+        return b
+
     def fem_info(self, body: int) -> dict:
         o = (C.c_longlong * 7)()
         self._lib.ref_fem_info(self._w, body, o)
@@ -308,10 +343,14 @@ def build_world(cls, rig: dict, **settings):
     w.settings(**s)
     w.load_statics(rig.get("statics", {}))
     for b in rig["bodies"]:
-        if "plate" in b:
+        if "plate" in b and "fem_members" not in b:
             if not hasattr(w, "add_plate"):
                 raise ValueError("FEM plates step in the reference only (RefWorld)")
             w.add_plate(b)
+        elif "fem_members" in b:
+            if not hasattr(w, "add_fem_body"):
+                raise ValueError("FEM frames step in the reference only (RefWorld)")
+            w.add_fem_body(b)
         else:
             w.add_body(b)
     return w

@@ -186,6 +186,56 @@ int ref_add_plate(RefWorld* r, int n, float ox, float oy, float oz, float dux, f
     return (int)r->bodies.size() - 1;
 }
 
+// A body with a FEM frame of members and triangles (FemFrame::add_section / add_shell_section / add_element /
+// add_tri, frame_fem.cpp:190-222; then finalize as a first step would): its nodes (SoftBody::add_node); the shell
+// sections (7 floats each: E nu rho t yield damping drill, on make_shell_section's defaults with no pattern), the
+// triangles (a, b, c, section; the mass they put on their corners); the frame sections (15 floats each: E G rho A
+// Iy Iz J As_y As_z damping axial joint_k Np Mp Tp), the members (ends, section, joints, mass); tris_first: the
+// add_tri calls before the add_element calls (the frame nodes numbered in the calls' order)
+int ref_add_fem_body(RefWorld* r, int n_nodes, const float* pos, const float* vel, const float* mass, const uint16_t* nflags, int n_ssec,
+                     const float* ssec, int n_tris, const uint32_t* tri, const uint16_t* tsec, const float* tmass, int n_fsec, const float* fsec,
+                     int n_members, const uint32_t* ab, const uint16_t* msec, const uint8_t* ends, const float* mmass, int tris_first) {
+    auto b = std::make_unique<SoftBody>();
+    b->name = "fem" + std::to_string(r->bodies.size());
+    b->can_sleep = false;
+    for (int i = 0; i < n_nodes; i++) {
+        const uint32_t id = b->add_node(vec3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]), mass[i], nflags[i]);
+        b->nodes[id].v = vec3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    }
+    for (int k = 0; k < n_ssec; k++) {
+        const float* f = ssec + 7 * k;
+        ShellSection s = make_shell_section("Steel", f[3]);
+        s.E = f[0], s.nu = f[1], s.rho = f[2], s.t = f[3], s.yield = f[4], s.damping = f[5], s.drill = f[6];
+        s.pattern = ShellPattern::None;
+        s.max_level = 0;
+        b->fem.add_shell_section(s);
+    }
+    for (int k = 0; k < n_fsec; k++) {
+        const float* f = fsec + 15 * k;
+        FrameSection s;
+        s.E = f[0], s.G = f[1], s.rho = f[2], s.A = f[3], s.Iy = f[4], s.Iz = f[5], s.J = f[6], s.As_y = f[7], s.As_z = f[8];
+        s.damping = f[9], s.axial = f[10], s.joint_k = f[11], s.Np = f[12], s.Mp = f[13], s.Tp = f[14];
+        b->fem.add_section(s);
+    }
+    auto add_tris = [&]() {
+        for (int t = 0; t < n_tris; t++) {
+            const uint32_t id = b->fem.add_tri(tri[3 * t], tri[3 * t + 1], tri[3 * t + 2], tsec[t]);
+            b->fem.tris[id].mass = tmass[t];
+        }
+    };
+    if (tris_first) add_tris();
+    for (int e = 0; e < n_members; e++) {
+        const uint32_t id = b->fem.add_element(ab[2 * e], ab[2 * e + 1], msec[e], ends[2 * e], ends[2 * e + 1]);
+        b->fem.elems[id].mass = mmass[e];
+    }
+    if (!tris_first) add_tris();
+    b->finalize();
+    SoftBody* bp = r->w.add_body(std::move(b));
+    bp->fem.finalize(*bp);
+    r->bodies.push_back(bp);
+    return (int)r->bodies.size() - 1;
+}
+
 // A constant force on one node of a body, applied every substep right after gravity (the SoftBody::pre_substep hook,
 // world.cpp:3261)
 void ref_set_point_load(RefWorld* r, int body, int node, float fx, float fy, float fz) {
