@@ -580,9 +580,15 @@ __device__ __forceinline__ void fem_gather(const NodeFem& nf, int i, v3 f) {
 // for World::collide_static and the integration (k_integrate) - the contacts between bodies add to it first.
 // Frame bodies (Body::is_fem): the triangles' forces and torques are gathered onto the frame nodes in the reference's
 // order (gather_forces, frame_fem.cpp:2080-2105) and the force is kept in nforce for the frame's implicit step.
+// kPacked: the incidences as 32-bit words: the beam's index less the warp's base (ell_base, bits 0-14; 0x7fff:
+// padding), bit 15 set where this node is the beam's b end, the other end's index less this node's plus 32768 (bits
+// 16-31) - half the bytes of the (beam | b-end bit, other end) pairs, for rigs whose warps' beams and neighbours lie
+// close enough (bl_world.cu checks every warp)
+template <bool kPacked>
 __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
-                                               const int2* __restrict__ ell, const float* __restrict__ fsc, Body* __restrict__ bodies, float gx,
-                                               float gy, float gz, int nnodes, int first, NodeFem nf, float4* __restrict__ fnode) {
+                                               const void* __restrict__ ell_, const int* __restrict__ ell_base, const float* __restrict__ fsc,
+                                               Body* __restrict__ bodies, float gx, float gy, float gz, int nnodes, int first, NodeFem nf,
+                                               float4* __restrict__ fnode) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int body = -1;
     float v2 = 0.0f;
@@ -599,9 +605,9 @@ __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd,
                 f = V(f.x + e.x, f.y + e.y, f.z + e.z);
             }
             // (four incidences' loads issued together, then added in order: the gathers overlap)
-            auto add = [&](int2 e, float sc, float4 Po) {
-                if (__float_as_uint(sc) == __float_as_uint(kNoPush) || e.y == i) return; // (e.y == i: padding)
-                if (e.x < 0) { // (this node is the beam's b: dis = p_a - p_b, the force subtracted)
+            auto add = [&](bool pad, bool bend, float sc, float4 Po) {
+                if (__float_as_uint(sc) == __float_as_uint(kNoPush) || pad) return;
+                if (bend) { // (this node is the beam's b: dis = p_a - p_b, the force subtracted)
                     const v3 dis = V(Po.x - P.x, Po.y - P.y, Po.z - P.z);
                     f = V(f.x - dis.x * sc, f.y - dis.y * sc, f.z - dis.z * sc);
                 } else {
@@ -610,19 +616,31 @@ __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd,
                 }
             };
             // the warp's incidences, interleaved: entry q of lane l at ell[ell_ptr[w] + 32 q + l] (a warp's load reads 32
-            // neighbours), each node's in beam order, padded to the warp's widest node (a multiple of 4) with (0, i)
+            // neighbours), each node's in beam order, padded to the warp's widest node (a multiple of 4)
             const int w = i >> 5, lane = i & 31;
             const int q0 = ell_ptr[w], width = (ell_ptr[w + 1] - q0) >> 5;
+            const int base = kPacked ? ell_base[w] : 0;
             for (int q = 0; q < width; q += 4) {
-                int2 e[4];
+                int beam[4], other[4];
+                bool pad[4], bend[4];
                 float sc[4];
                 float4 Po[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) e[u] = ell[q0 + 32 * (q + u) + lane];
+                for (int u = 0; u < 4; u++) {
+                    if (kPacked) {
+                        const uint32_t x = static_cast<const uint32_t*>(ell_)[q0 + 32 * (q + u) + lane];
+                        pad[u] = (x & 0x7fffu) == 0x7fffu;
+                        beam[u] = base + (int)(x & 0x7fffu), bend[u] = (x & 0x8000u) != 0, other[u] = i + (int)(x >> 16) - 32768;
+                    } else {
+                        const int2 e = static_cast<const int2*>(ell_)[q0 + 32 * (q + u) + lane];
+                        pad[u] = e.y == i; // (padding: (0, the node itself))
+                        beam[u] = e.x & 0x7fffffff, bend[u] = e.x < 0, other[u] = e.y;
+                    }
+                }
 #pragma unroll
-                for (int u = 0; u < 4; u++) sc[u] = fsc[e[u].x & 0x7fffffff], Po[u] = nd[2 * e[u].y];
+                for (int u = 0; u < 4; u++) sc[u] = pad[u] ? kNoPush : fsc[beam[u]], Po[u] = nd[2 * other[u]];
 #pragma unroll
-                for (int u = 0; u < 4; u++) add(e[u], sc[u], Po[u]);
+                for (int u = 0; u < 4; u++) add(pad[u], bend[u], sc[u], Po[u]);
             }
             if (B.is_fem) {
                 live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)

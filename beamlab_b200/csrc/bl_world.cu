@@ -91,6 +91,9 @@ struct bl_gpu_ctx {
     DevBuf<float> fsc;
     DevBuf<int2> inc2;                         // per node's incidences, warp-interleaved (k_force)
     DevBuf<int> ell_ptr;
+    bool packed_inc = false;                   // the incidences in their 4-byte form (inc4, ell_base) instead
+    DevBuf<uint32_t> inc4;
+    DevBuf<int> ell_base;
     int beam_tiles = 0;                        // k_beams_tma's tiles (the beam arrays hold beam_tiles * kBeamTile)
     int beam_grid = 0;                         // its persistent grid (0: not sized yet)
     DevBuf<int4> info;
@@ -114,6 +117,7 @@ struct bl_gpu_ctx {
     Statics st{};
     // FEM frames of all bodies back to back (see bl_fem_kernels.cuh)
     int NF = 0, NT = 0, NB = 0, n_fem_nodes = 0;
+    int64_t NU = 0;                            // block updates of a factorization
     bool any_ext = false;
     std::vector<int> lvl_grp_ptr, lvl_col_ptr; // per level: its update groups / columns
     int64_t fem_launches = 0;                  // kernels of one substep's frame step (with the Cholesky)
@@ -233,6 +237,7 @@ static void free_device(bl_gpu_ctx* c) {
     free_fem(c);
     free_contacts(c);
     c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->ell_ptr.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
+    c->inc4.free_(), c->ell_base.free_(), c->packed_inc = false;
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
 }
@@ -493,6 +498,7 @@ static int commit_fem(bl_gpu_ctx* c) {
     std::vector<int> rb_ptr(NF + 1, 0);
     std::vector<std::vector<int>> bylev(nlev);
     for (int k = 0; k < NF; k++) bylev[level[k]].push_back(k);
+    c->NU = (int64_t)gupd.size();
     std::vector<std::vector<int>> col_upds(NF);
     for (size_t u = 0; u < gupd.size(); u++) col_upds[upd_col[u]].push_back((int)u);
     c->lvl_grp_ptr.assign(1, 0), c->lvl_col_ptr.assign(1, 0);
@@ -840,6 +846,7 @@ static int commit_bodies(bl_gpu_ctx* c) {
         int per_sm = 0, sms = 0;
         BL_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_beams_tma, kBeamThreads, kBeamSmem));
         BL_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+        if (c->cfg.beams_per_sm > 0) per_sm = std::min(per_sm, (int)c->cfg.beams_per_sm);
         if (per_sm > 0) c->beam_grid = std::min(c->beam_tiles, per_sm * sms);
     }
     BL_CUDA(c, c->nodef.alloc(N));
@@ -869,7 +876,40 @@ static int commit_bodies(bl_gpu_ctx* c) {
                 }
             }
         }
-        if ((rc = upload_vec(c, c->inc2, ell)) || (rc = upload_vec(c, c->ell_ptr, eptr))) return rc;
+        if ((rc = upload_vec(c, c->ell_ptr, eptr))) return rc;
+        // the 4-byte form where every warp's beams lie within 32,767 of its first and every neighbour within 32,767
+        // nodes (k_force<true>): half the bytes of the incidence stream
+        std::vector<int> base(nw, 0);
+        bool packed = c->cfg.beam_kernel == 0;
+        for (int w = 0; w < nw && packed; w++) {
+            int lo = INT32_MAX;
+            for (int q = eptr[w]; q < eptr[w + 1]; q++) {
+                const int i = 32 * w + (q - eptr[w]) % 32;
+                if (!(i >= N || ell[q].y == i)) lo = std::min(lo, ell[q].x & 0x7fffffff); // (not padding)
+            }
+            base[w] = lo == INT32_MAX ? 0 : lo;
+            for (int q = eptr[w]; q < eptr[w + 1] && packed; q++) {
+                const int i = 32 * w + (q - eptr[w]) % 32;
+                if (i >= N || ell[q].y == i) continue;
+                const int g = ell[q].x & 0x7fffffff;
+                if (g - base[w] >= 0x7fff || g < base[w] || std::abs(ell[q].y - i) > 32767) packed = false;
+            }
+        }
+        c->packed_inc = packed;
+        if (packed) {
+            std::vector<uint32_t> pk(ell.size());
+            for (int w = 0; w < nw; w++)
+                for (int q = eptr[w]; q < eptr[w + 1]; q++) {
+                    const int i = 32 * w + (q - eptr[w]) % 32;
+                    const bool pad = i >= N || ell[q].y == i;
+                    pk[q] = pad ? (0x7fffu | (32768u << 16))
+                                : (uint32_t)((ell[q].x & 0x7fffffff) - base[w]) | (ell[q].x < 0 ? 0x8000u : 0u) |
+                                      ((uint32_t)(ell[q].y - i + 32768) << 16);
+                }
+            if ((rc = upload_vec(c, c->inc4, pk)) || (rc = upload_vec(c, c->ell_base, base))) return rc;
+        } else if ((rc = upload_vec(c, c->inc2, ell))) {
+            return rc;
+        }
     }
     int P = 1;
     while (P < maxn) P <<= 1;
@@ -1003,7 +1043,10 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     const float dt = c->cfg.dt;
     const float frame_time = (float)n * dt;
     const int tb = 256;
-    const int gb = std::max((c->M + 2 * tb - 1) / (2 * tb), (c->B + tb - 1) / tb), gn = (c->N + tb - 1) / tb, gbody = (c->B + tb - 1) / tb;
+    const int gb = std::max((c->M + 2 * tb - 1) / (2 * tb), (c->B + tb - 1) / tb), gbody = (c->B + tb - 1) / tb;
+    // (the node kernels' block sizes: bl_gpu_config.force_block / integrate_block, 256 unless tuned)
+    const int fb = c->cfg.force_block > 0 ? c->cfg.force_block : 256, ib = c->cfg.integrate_block > 0 ? c->cfg.integrate_block : 256;
+    const int gfn = (c->N + fb - 1) / fb, gin = (c->N + ib - 1) / ib;
     const Contacts& CT = c->ct;
     if (c->contacts_on) k_islands<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, frame_time, c->cfg.sleeping, CT, c->deverr.p);
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
@@ -1031,8 +1074,12 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         if (c->NM > 0) k_member_eval<<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
-        k_force<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, c->fsc.p, c->dbodies.p, c->cfg.gravity[0],
-                                               c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
+        if (c->packed_inc)
+            k_force<true><<<std::max(gfn, 1), fb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc4.p, c->ell_base.p, c->fsc.p, c->dbodies.p,
+                                                         c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
+        else
+            k_force<false><<<std::max(gfn, 1), fb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, nullptr, c->fsc.p, c->dbodies.p,
+                                                          c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
         mark();
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
@@ -1040,7 +1087,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_collide<<<(c->B + 127) / 128, 128, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
         }
         mark();
-        k_integrate<<<std::max(gn, 1), tb, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p);
+        k_integrate<<<std::max(gin, 1), ib, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p);
         mark();
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
@@ -1220,6 +1267,9 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->graphs = 1;
     cfg->beam_kernel = 0;
     cfg->fem_dense_front = 1;
+    cfg->force_block = 0;
+    cfg->integrate_block = 0;
+    cfg->beams_per_sm = 0;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -1245,7 +1295,10 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
     if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 3 || c0.pcg_max_iters < 0 ||
-        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 1)
+        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 1 ||
+        !(c0.force_block == 0 || c0.force_block == 64 || c0.force_block == 128 || c0.force_block == 256) ||
+        !(c0.integrate_block == 0 || c0.integrate_block == 64 || c0.integrate_block == 128 || c0.integrate_block == 256) ||
+        c0.beams_per_sm < 0 || c0.beams_per_sm > 16)
         return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
@@ -1777,6 +1830,7 @@ int bl_gpu_fem_stats(bl_gpu_ctx* c, bl_fem_stats* out) {
     BL_CUDA(c, cudaMemcpy(&last, c->plast.p, sizeof(last), cudaMemcpyDeviceToHost));
     out->pcg_solves = st[0], out->pcg_fallbacks = st[1], out->last_iterations = st[2], out->pcg_iterations = it;
     out->last_pcg_residual = last, out->max_residual = res[0], out->last_residual = res[3];
+    out->columns = c->NF, out->blocks = c->NB, out->updates = c->NU, out->levels = (int64_t)c->lvl_col_ptr.size() - 1;
     return BL_GPU_OK;
 }
 

@@ -512,3 +512,123 @@ def plate_with_rails(n: int = 20, seed: int = 1, section: dict | None = None, tr
               "member_mass": np.zeros(len(members), np.float32), "fem_tris_first": tris_first})
     rig["name"] = f"plate_with_rails(n={n}, seed={seed}, tris_first={tris_first})"
     return rig
+
+
+def rod_section(d: float = 0.006, E: float = 2.1e11, G: float = 8.1e10, rho: float = 7850.0, damping: float = 2e-5) -> dict:
+    """A solid round steel rod's FrameSection fields (a spot weld's nugget)."""
+    r = d / 2
+    A = math.pi * r * r
+    I = math.pi * r ** 4 / 4
+    return {"E": E, "G": G, "rho": rho, "A": A, "Iy": I, "Iz": I, "J": 2 * I, "As_y": 0.9 * A, "As_z": 0.9 * A,
+            "damping": damping, "axial": 1.0, "joint_k": 2.0e4}
+
+
+def shell_body(target_nodes: int = 50000, size=(4.0, 1.4, 1.8), seed: int = 1, t_range=(0.0008, 0.002), inset: float = 0.01,
+               weld_every: int = 2, pillars: int = 2, load: float = 2000.0) -> dict:
+    """A procedural box-and-pillar shell car body: the six faces of a size = (x, y, z) box, each a separate panel of
+    CST/DKT triangles (a node grid split into two triangles a cell, diagonals alternating) of a seeded thickness in
+    t_range, inset `inset` from the box's edges; spot welds - members of a 6 mm rod section - joining the facing edge
+    nodes of adjacent panels every `weld_every` nodes (every 5 cm at the default spacing); tube pillars (members on the
+    side panels' node columns) at `pillars` stations a side. Node spacing chosen for about target_nodes nodes; steel;
+    floating (no ground, no clamp), gravity, a constant `load` N down on the roof's middle node and its seeded random
+    push on a side panel node. Members are added first (their add_element calls), then the triangles."""
+    Lx, Ly, Lz = size
+    area = 2 * (Lx * Ly + Lx * Lz + Ly * Lz)
+    du = math.sqrt(area / target_nodes)
+    nx, ny, nz = (max(3, int(round((L - 2 * inset) / du)) + 1) for L in (Lx, Ly, Lz))
+    gen = np.random.default_rng(seed)
+    pos, panels = [], []
+
+    def panel(origin, ua, va, nu, nv):
+        # nodes origin + ua * i / (nu - 1) + va * j / (nv - 1): index base + j * nu + i
+        base = len(pos)
+        o, ua, va = np.asarray(origin, np.float64), np.asarray(ua, np.float64), np.asarray(va, np.float64)
+        for j in range(nv):
+            for i in range(nu):
+                pos.append(o + ua * (i / (nu - 1)) + va * (j / (nv - 1)))
+        panels.append((base, nu, nv))
+        return base
+    e, X, Y, Z = inset, Lx - 2 * inset, Ly - 2 * inset, Lz - 2 * inset
+    # floor (y = 0) and roof (y = Ly): x by z; sides (z = 0, z = Lz): x by y; front and back (x = 0, x = Lx): z by y
+    panel((e, 0.0, e), (X, 0, 0), (0, 0, Z), nx, nz)
+    panel((e, Ly, e), (X, 0, 0), (0, 0, Z), nx, nz)
+    panel((e, e, 0.0), (X, 0, 0), (0, Y, 0), nx, ny)
+    panel((e, e, Lz), (X, 0, 0), (0, Y, 0), nx, ny)
+    panel((0.0, e, e), (0, 0, Z), (0, Y, 0), nz, ny)
+    panel((Lx, e, e), (0, 0, Z), (0, Y, 0), nz, ny)
+    pos = np.asarray(pos, np.float32)
+    n = len(pos)
+    tris, tsec, sections = [], [], []
+    for pi, (base, nu, nv) in enumerate(panels):
+        t = float(gen.uniform(*t_range))
+        sections.append({"E": 2.1e11, "nu": 0.3, "rho": 7850.0, "t": t, "yield": 0.0, "damping": 3e-4, "drill": 0.05})
+        for j in range(nv - 1):
+            for i in range(nu - 1):
+                a, b, c, d = base + j * nu + i, base + j * nu + i + 1, base + (j + 1) * nu + i, base + (j + 1) * nu + i + 1
+                if (i + j) & 1:
+                    tris += [(a, b, d), (a, d, c)]
+                else:
+                    tris += [(a, b, c), (b, d, c)]
+                tsec += [pi, pi]
+
+    def edge(pnl, which):
+        base, nu, nv = pnl
+        if which == "j0":
+            return [base + i for i in range(nu)]
+        if which == "j1":
+            return [base + (nv - 1) * nu + i for i in range(nu)]
+        if which == "i0":
+            return [base + j * nu for j in range(nv)]
+        return [base + j * nu + nu - 1 for j in range(nv)]
+    P = {k: panels[i] for i, k in enumerate(("fl", "rf", "s0", "s1", "f0", "f1"))}
+    # spot welds along the twelve seams: (panel A's edge nodes, panel B's), every weld_every-th pair
+    seams = [(("fl", "j0"), ("s0", "j0")), (("fl", "j1"), ("s1", "j0")), (("rf", "j0"), ("s0", "j1")), (("rf", "j1"), ("s1", "j1")),
+             (("fl", "i0"), ("f0", "j0")), (("fl", "i1"), ("f1", "j0")), (("rf", "i0"), ("f0", "j1")), (("rf", "i1"), ("f1", "j1")),
+             (("s0", "i0"), ("f0", "i0")), (("s0", "i1"), ("f1", "i0")), (("s1", "i0"), ("f0", "i1")), (("s1", "i1"), ("f1", "i1"))]
+    members, msec = [], []
+    for (pa, ea), (pb, eb) in seams:
+        A, B = edge(P[pa], ea), edge(P[pb], eb)
+        for q in range(0, min(len(A), len(B)), weld_every):
+            members.append((A[q], B[q]))
+            msec.append(1)
+    # pillars: tube members up node columns of the side panels
+    for side in ("s0", "s1"):
+        base, nu, nv = P[side]
+        for k in range(pillars):
+            i = int(round((k + 1) * (nu - 1) / (pillars + 1)))
+            for j in range(nv - 1):
+                members.append((base + j * nu + i, base + (j + 1) * nu + i))
+                msec.append(0)
+    fsec = [tube_section(0.05, 0.002), rod_section(0.006)]
+    # masses: each triangle a third of rho t area on each corner, each member half of rho A L on each end
+    mass = np.zeros(n, np.float64)
+    tri_a = np.asarray(tris, np.int64)
+    pa_, pb_, pc_ = (pos[tri_a[:, c]].astype(np.float64) for c in range(3))
+    ar = 0.5 * np.linalg.norm(np.cross(pb_ - pa_, pc_ - pa_), axis=1)
+    tth = np.asarray([sections[s]["t"] for s in tsec])
+    tm = (7850.0 * tth * ar).astype(np.float32)
+    for c in range(3):
+        np.add.at(mass, tri_a[:, c], tm.astype(np.float64) / 3)
+    mab = np.asarray(members, np.int64)
+    ml = np.linalg.norm(pos[mab[:, 1]].astype(np.float64) - pos[mab[:, 0]], axis=1)
+    mm = np.asarray([fsec[s]["rho"] * fsec[s]["A"] for s in msec]) * ml
+    np.add.at(mass, mab[:, 0], mm / 2)
+    np.add.at(mass, mab[:, 1], mm / 2)
+    body = {
+        "pos": pos, "vel": np.zeros((n, 3), np.float32), "mass": mass.astype(np.float32), "node_flags": np.zeros(n, np.uint16),
+        "friction": np.ones(n, np.float32), "radius": np.zeros(n, np.float32),
+        "ab": np.zeros((0, 2), np.uint32), "k": np.zeros(0, np.float32), "d": np.zeros(0, np.float32),
+        "strength": np.zeros(0, np.float32), "deform": np.zeros(0, np.float32), "beam_type": np.zeros(0, np.uint8),
+        "beam_flags": np.zeros(0, np.uint8),
+        "params": {"ground_friction": 1.0, "bounce": -1.0, "contact_push_max": 2.0, "contact_slop": 0.0,
+                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 1, "ductile": 0, "can_sleep": 0,
+                   "sleep_speed": 0.0},
+        "fem_sections": sections, "fem_tris": np.asarray(tris, np.uint32), "fem_tri_section": np.asarray(tsec, np.uint16),
+        "fem_tri_mass": tm, "frame_sections": fsec, "fem_members": np.asarray(members, np.uint32),
+        "member_section": np.asarray(msec, np.uint16), "member_ends": np.zeros((len(members), 2), np.uint8),
+        "member_mass": np.zeros(len(members), np.float32),
+        "loads": [(P["rf"][0] + (nz // 2) * nx + nx // 2, (0.0, -float(load), 0.0)),
+                  (P["s0"][0] + int(gen.integers(nx * ny)), tuple(float(v) for v in gen.normal(0.0, 0.5 * load, 3)))],
+    }
+    return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005}, "statics": {}, "bodies": [body],
+            "name": f"shell_body(target={target_nodes}, seed={seed})"}

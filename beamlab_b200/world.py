@@ -74,6 +74,11 @@ class WorldSettings:
     beam_kernel: int = 0
     # the FEM factorization's top chain as one dense front (True) or block column by block column (False)
     fem_dense_front: bool = True
+    # launch shapes (None: the tuned ones of beamlab_b200/tuned.json when present, else the library's defaults);
+    # results do not depend on them
+    force_block: int | None = None
+    integrate_block: int | None = None
+    beams_per_sm: int | None = None
 
 
 @dataclass
@@ -343,16 +348,30 @@ class _Config(C.Structure):
                 ("collision_hz", C.c_float), ("inter_body_collisions", C.c_int32), ("max_pairs", C.c_int32),
                 ("fem_solver", C.c_int32), ("pcg_max_iters", C.c_int32), ("pcg_tol", C.c_float),
                 ("fem_check_residual", C.c_int32), ("pcg_learned_scale", C.c_int32), ("graphs", C.c_int32),
-                ("beam_kernel", C.c_int32), ("fem_dense_front", C.c_int32)]
+                ("beam_kernel", C.c_int32), ("fem_dense_front", C.c_int32), ("force_block", C.c_int32),
+                ("integrate_block", C.c_int32), ("beams_per_sm", C.c_int32)]
 
 
 class _FemStats(C.Structure):
     _fields_ = [("pcg_solves", C.c_int64), ("pcg_fallbacks", C.c_int64), ("pcg_iterations", C.c_int64),
                 ("last_iterations", C.c_int32), ("pad", C.c_int32), ("last_pcg_residual", C.c_double),
-                ("max_residual", C.c_double), ("last_residual", C.c_double)]
+                ("max_residual", C.c_double), ("last_residual", C.c_double), ("columns", C.c_int64),
+                ("blocks", C.c_int64), ("updates", C.c_int64), ("levels", C.c_int64)]
 
 
 FEM_SOLVERS = {"cholesky": 0, "pcg": 1, "pcg_learned": 2, "pcg_previous": 3}
+
+
+def _tuned_shapes() -> dict:
+    """The launch shapes beamlab_b200/autotune.py chose (beamlab_b200/tuned.json), if any."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
+    try:
+        with open(path) as f:
+            return {k: int(v) for k, v in json.load(f).get("shapes", {}).items()}
+    except (OSError, ValueError):
+        return {}
 
 
 class BodyHandle:
@@ -436,6 +455,10 @@ class World:
         cfg.graphs = int(self.settings.graphs)
         cfg.beam_kernel = int(self.settings.beam_kernel)
         cfg.fem_dense_front = int(self.settings.fem_dense_front)
+        tuned = _tuned_shapes()
+        for k in ("force_block", "integrate_block", "beams_per_sm"):
+            v = getattr(self.settings, k)
+            setattr(cfg, k, int(v if v is not None else tuned.get(k, 0)))
         self._ctx = C.c_void_p()
         _check(self._L.bl_gpu_create(C.byref(cfg), C.byref(self._ctx)), "create")
         self._bodies: list[BodyHandle] = []

@@ -57,6 +57,13 @@ def workload(name: str, rank: int):
         desc = ("plate64: co-rotational FEM shell plate, 64 x 64 nodes (4,096), 7,938 CST/DKT triangles, 1 m x 1 m, "
                 "1.5 mm steel (E 210 GPa, nu 0.3, 7,850 kg/m^3), one edge clamped, a seeded 500 N point load, gravity; "
                 "implicit step every substep: 64,411 off-diagonal 6x6 blocks, 1,359,082 block updates")
+    elif name == "shellcar":
+        rig = rigs.shell_body(10000, seed=1 + rank)
+        n, m = rigs.rig_counts(rig)
+        b = rig["bodies"][0]
+        desc = (f"shellcar: a procedural box-and-pillar shell car body ({n:,} nodes, {len(b['fem_tris']):,} CST/DKT "
+                f"triangles of 0.8-2.0 mm steel in six welded panels, {len(b['fem_members']):,} members: spot welds every "
+                f"5 cm and tube pillars), floating under gravity and two point loads; implicit step every substep")
     elif name == "truss_car":
         rig = rigs.truss_car(1 + rank)
         n, m = rigs.rig_counts(rig)
@@ -129,10 +136,10 @@ def traffic_per_unit():
     return json.load(open(path)) if os.path.exists(path) else {}
 
 
-def cpu_reference(rig, n_nodes, budget_s=10.0, max_frames=100, warm=4):
+def cpu_reference(rig, n_nodes, budget_s=10.0, max_frames=100, warm=4, frame=FRAME):
     """The reference's own step (compiled from its sources, Release flags) on all host cores: node-substeps/s of a
-    bounded sample (warm-up substeps, then frames of 33 substeps of the same workload until about budget_s seconds
-    have passed, at least 2 and at most max_frames)."""
+    bounded sample (warm-up substeps, then frames of `frame` substeps of the same workload until about budget_s
+    seconds have passed, at least 2 and at most max_frames)."""
     from oracle.oracle import RefWorld, build_world, ref_available, ref_jobs_init, ref_jobs_shutdown
     if not ref_available("timing"):
         return None
@@ -143,24 +150,26 @@ def cpu_reference(rig, n_nodes, budget_s=10.0, max_frames=100, warm=4):
     t0 = time.perf_counter()
     frames = 0
     while frames < 2 or (frames < max_frames and time.perf_counter() - t0 < budget_s):
-        w.step_substeps(FRAME)
+        w.step_substeps(frame)
         frames += 1
     dt = time.perf_counter() - t0
     w.close()
     ref_jobs_shutdown("timing")
-    return {"value": n_nodes * FRAME * frames / dt, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"the same workload, {frames} frames of {FRAME} substeps after {warm} warm-up substeps "
-                      f"({frames * FRAME} substeps, {dt:.2f} s)"}
+    return {"value": n_nodes * frame * frames / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"the same workload, {frames} frames of {frame} substeps after {warm} warm-up substeps "
+                      f"({frames * frame} substeps, {dt:.2f} s)"}
 
 
-def fem_solvers(device: int, frames: int = 2):
-    """The plate's implicit step by each solver (include/beamlab_gpu.h: fem_solver), on a load the network was not
-    trained on: ms a substep (CUDA events of a profiled frame), CG iterations a solve, fallbacks, the largest relative
-    residual of a solution the step took. The network is trained first on 200 substeps of the Cholesky's solves of
-    another load (seed 1; 12 epochs of Adam)."""
+def fem_solvers(device: int, frames: int = 2, make=None, label: str = "shell_plate(63, seed=2)"):
+    """The implicit step by each solver (include/beamlab_gpu.h: fem_solver), on a load the network was not trained on
+    (make(seed 2); default the 64 x 64 plate): ms a substep (CUDA events of a profiled frame), CG iterations a solve,
+    fallbacks, the largest relative residual of a solution the step took. The network is trained first on 200
+    substeps of the Cholesky's solves of another load (make(seed 1); 12 epochs of Adam)."""
     from beamlab_b200 import rigs, world_from_rig
-    rec = world_from_rig(rigs.shell_plate(63, seed=1), device=device)
-    rec.mlp_record(200 * 4096)
+    make = make or (lambda seed: rigs.shell_plate(63, seed=seed))
+    rec = world_from_rig(make(1), device=device)
+    nf = len(rec.bodies()[0].fem()["node"])
+    rec.mlp_record(200 * nf)
     for _ in range(10):
         rec.step_substeps(20)
     rec.mlp_record(0)
@@ -170,11 +179,9 @@ def fem_solvers(device: int, frames: int = 2):
     train_s = time.perf_counter() - t0
     weights = rec.mlp_weights()
     rec.close()
-    out = {"load": "shell_plate(63, seed=2)", "training": {"samples": 200 * 4096, "epochs": 13, "loss": loss,
-                                                           "seconds": train_s}}
+    out = {"load": label, "training": {"samples": 200 * nf, "epochs": 13, "loss": loss, "seconds": train_s}}
     for solver in ("cholesky", "pcg", "pcg_previous", "pcg_learned"):
-        w = world_from_rig(rigs.shell_plate(63, seed=2), device=device, fem_solver=solver, pcg_max_iters=3000,
-                           fem_check_residual=True)
+        w = world_from_rig(make(2), device=device, fem_solver=solver, pcg_max_iters=3000, fem_check_residual=True)
         if solver == "pcg_learned":
             w.set_mlp_weights(weights)
         w.step_substeps(FRAME)  # (warm-up: the graph is captured)
@@ -243,19 +250,20 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     threads = ref_jobs_init(max(0, cores - 1), "timing")
     w = build_world(RefWorld, rig, flavour="timing", multithreaded=True)
+    frame = 1 if args.workload == "shellcar" else FRAME  # (the shell body's reference step takes seconds)
     for _ in range(args.warmup):
-        w.step_substeps(FRAME)
+        w.step_substeps(frame)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        w.step_substeps(FRAME)
+        w.step_substeps(frame)
     dt = time.perf_counter() - t0
-    v = n * FRAME * args.steps / dt
+    v = n * frame * args.steps / dt
     w.close()
     ref_jobs_shutdown("timing")
     base.update({"value": v, "ms_per_step": dt * 1e3 / args.steps, "scaling": "weak", "vs_baseline": None,
                  "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                  "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                                  "sample": f"the whole workload, {args.steps} frames of {FRAME} substeps"}})
+                                  "sample": f"the whole workload, {args.steps} frames of {frame} substeps"}})
     print(json.dumps(base), flush=True)
 
 
@@ -345,11 +353,16 @@ def run_gpu(args):
         # writes p, v (24 B); the substep as a whole: 40 B a beam + 52 B a node (the force never leaving the chip)
         kern = {"k_beams": (BYTES_PER_BEAM * m, per["beams"], m, "beam"), "k_force": (32 * n, per["force"], n, "node"),
                 "k_integrate": (68 * n, per["integrate"], n, "node")}
-        if args.workload == "plate64":
-            # the implicit FEM step: its factor (4,096 diagonal and 64,411 off-diagonal 6x6 blocks of doubles, the
-            # symbolic phase's count for this plate) and right side each read and written once a substep
-            fem_bytes = 2 * 8 * (36 * 4096 + 36 * 64411 + 6 * 4096)
-            kern["fem_step"] = (fem_bytes, per["fem"], 4096, "column")
+        fem_info = None
+        if args.workload in ("plate64", "shellcar"):
+            # the implicit FEM step: its factor (diagonal and off-diagonal 6x6 blocks of doubles) and right side each
+            # read and written once a substep
+            fs = w.fem_stats()
+            fem_bytes = 2 * 8 * (36 * fs["columns"] + 36 * fs["blocks"] + 6 * fs["columns"])
+            kern["fem_step"] = (fem_bytes, per["fem"], fs["columns"], "column")
+            fem_info = {"columns": fs["columns"], "blocks": fs["blocks"], "block_updates": fs["updates"],
+                        "levels": fs["levels"], "ms_per_substep": per["fem"],
+                        "gflops_fp64": 432 * fs["updates"] / (per["fem"] * 1e-3) / 1e9}
         dom = max(kern, key=lambda k: kern[k][1])
         alg_bytes, kms, units_, unit_name = kern[dom]
         achieved = alg_bytes / (kms * 1e-3) / 1e9
@@ -380,14 +393,22 @@ def run_gpu(args):
                          "algorithmic_bytes_per_launch": alg_bytes, "traffic": traffic, "substep_kernels": substep},
             "clocks": clk,
         }
+        if fem_info is not None:
+            out["fem_step"] = fem_info
         if ws == 1 and args.workload == "plate64":
             out["fem_solvers"] = fem_solvers(local)
+        if ws == 1 and args.workload == "shellcar" and not args.no_solvers:
+            from beamlab_b200 import rigs as _rigs
+            out["fem_solvers"] = fem_solvers(local, make=lambda seed: _rigs.shell_body(10000, seed=seed),
+                                             label="shell_body(10000, seed=2)")
         if ws == 1 and args.workload == "fleet256" and not args.no_plain:
             pl = plain_gpu(rig, local, stream)
             pl["batched_over_plain"] = value / pl["launches"]["value"]
             out["plain_gpu"] = pl
         if ws == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_reference(rig, n)
+            # (the shell body's reference step takes seconds: a sample of single substeps)
+            out["cpu_baseline"] = (cpu_reference(rig, n, warm=1, frame=1) if args.workload == "shellcar"
+                                   else cpu_reference(rig, n))
         print(json.dumps(out), flush=True)
     if ws > 1:
         dist.destroy_process_group()
@@ -400,7 +421,8 @@ def main():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fleet256", choices=["fleet256", "plate64", "truss_car"])
+    ap.add_argument("--workload", default="fleet256", choices=["fleet256", "plate64", "shellcar", "truss_car"])
+    ap.add_argument("--no-solvers", action="store_true", help="skip the shell car's comparison of FEM solvers")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-instance GPU path's measurement")
     args = ap.parse_args()

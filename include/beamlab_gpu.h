@@ -83,10 +83,15 @@ typedef struct {
     int32_t graphs;            /* 1 (default): a frame of n substeps is captured once as a CUDA graph and replayed; 0: its
                                   kernels are launched one by one every call (the plain path, one launch per kernel) */
     int32_t beam_kernel;       /* 0 (default): the beams' kernel streams the beam arrays through shared memory by bulk
-                                  (TMA) copies; 1: plain loads. Results are the same. */
+                                  (TMA) copies and the nodes' kernel reads 4-byte incidences where the rig allows; 1:
+                                  plain loads and 8-byte incidences. Results are the same. */
     int32_t fem_dense_front;   /* 1 (default): the FEM factorization takes the top chain of its elimination tree (levels of
                                   one column each) as one dense front (a blocked dense Cholesky and dense solves); 0: block
                                   column by block column in the reference's order of sums throughout */
+    /* launch shapes (results do not depend on them; beamlab_b200/autotune.py measures them for a device and workload): */
+    int32_t force_block;       /* the nodes' force kernel's block size: 64, 128 or 256; 0 (default): 256 */
+    int32_t integrate_block;   /* the integration kernel's block size: 64, 128 or 256; 0 (default): 256 */
+    int32_t beams_per_sm;      /* the beams' persistent kernel's blocks an SM (at most what fits); 0 (default): what fits */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };
@@ -334,6 +339,10 @@ typedef struct {
     double last_pcg_residual;  /* relative residual the last PCG solve reached */
     double max_residual;       /* fem_check_residual: the largest relative residual of a solution the step took */
     double last_residual;      /* fem_check_residual: that of the last substep */
+    int64_t columns;           /* the factor of all frames: block columns (frame nodes), */
+    int64_t blocks;            /* off-diagonal 6 x 6 blocks, */
+    int64_t updates;           /* block updates of a factorization (432 flops each), */
+    int64_t levels;            /* elimination-tree levels */
 } bl_fem_stats;
 int bl_gpu_fem_stats(bl_gpu_ctx* ctx, bl_fem_stats* out);
 

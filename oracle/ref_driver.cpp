@@ -38,6 +38,7 @@ using namespace bl::phys;
 struct RefWorld {
     World w;
     std::vector<SoftBody*> bodies;
+    std::map<int, std::vector<std::pair<uint32_t, vec3>>> loads; // the constant node loads of each body
 };
 
 // per-body knobs of SoftBody that the GPU path supports (softbody.h:650-700)
@@ -240,10 +241,13 @@ int ref_add_fem_body(RefWorld* r, int n_nodes, const float* pos, const float* ve
 // world.cpp:3261)
 void ref_set_point_load(RefWorld* r, int body, int node, float fx, float fy, float fz) {
     SoftBody* b = r->bodies[body];
-    const vec3 f(fx, fy, fz);
-    const uint32_t nd = (uint32_t)node;
-    b->pre_substep = [nd, f](SoftBody& sb, float) {
-        if (nd < sb.force.size()) sb.force[nd] += f;
+    // (every load of the body in one callback: a body has one pre_substep)
+    auto& loads = r->loads[body];
+    loads.push_back({(uint32_t)node, vec3(fx, fy, fz)});
+    const std::vector<std::pair<uint32_t, vec3>> all = loads;
+    b->pre_substep = [all](SoftBody& sb, float) {
+        for (const auto& [nd, f] : all)
+            if (nd < sb.force.size()) sb.force[nd] += f;
     };
 }
 

@@ -91,7 +91,8 @@ def frame_pattern(rig):
 @pytest.mark.parametrize("make", [
     lambda: rigs.frame_ladder(12, joints=[(0, 0), (1, 0), (2, 3), (4, 4), (5, 5), (0, 1)]),
     lambda: rigs.plate_with_rails(12, tris_first=True),
-    lambda: rigs.plate_with_rails(12, tris_first=False)])
+    lambda: rigs.plate_with_rails(12, tris_first=False),
+    lambda: rigs.shell_body(1500)])
 def test_frame_members_pattern_matches_reference(ref_lib, make):
     """Frames with members (FemFrame::add_element): the same frame node numbering, ordering, factor pattern and update
     list as the reference's, bit for bit - members alone with every kind of joint, and members with triangles added in

@@ -79,3 +79,27 @@ def test_contacts_off_keeps_bodies_apart_from_pairs():
     st = w.stats()
     assert len(w.pairs()) == 0 and st["contacts"] == 0 and st["pair_searches"] == 0
     w.close()
+
+
+def test_sleeping_body_woken_by_contact_matches_reference(ref_lib):
+    """A truss resting on the ground falls asleep (its sleep speed raised to 0.5 m/s), another dropped from 20 m lands
+    on it and wakes it (SoftBody::wake_request through the contact between them): the sleeping flags frame by frame
+    and the final states bitwise the reference's."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.drop_pair(1, height=20.0, dims=(6, 2, 3))
+    rig["bodies"][0]["params"]["sleep_speed"] = 0.5
+    w = world_from_rig(rig)
+    ref = build_world(RefWorld, rig, multithreaded=False)
+    got, want = [], []
+    for f in range(130):
+        w.step_substeps(33)
+        ref.step_substeps(33)
+        got.append(bool(w.bodies()[0].state()["sleeping"]))
+        want.append(bool(ref.body(0)["sleeping"]))
+    assert got == want
+    assert any(want) and not want[-1]  # (it slept, and was woken)
+    for b in range(2):
+        nd = w.bodies()[b].nodes()
+        r = ref.nodes(b)
+        assert np.array_equal(bits(nd["p"]), bits(r["pos"])) and np.array_equal(bits(nd["v"]), bits(r["vel"])), f"body {b}"
+    w.close()
