@@ -101,6 +101,13 @@ struct alignas(64) Body {
     int pairs;               // this frame: its island has contact pairs (its nodes finish after the contacts)
     int wake_request;        // SoftBody::wake_request
     int body_contacts;       // SoftBody::body_contacts (this frame)
+    // air drag (SoftBody::clear_forces with air_drag / aero_cda, softbody.cpp:334-378)
+    int drag;                // air_drag > 0 or aero_cda > 0
+    float air_drag, aero_cda;
+    int part_count;          // its parts (SoftBody::part_labels; 0: not labelled yet)
+    int part_age;            // SoftBody::part_age_
+    int part_key;            // the broken-beam count the labels were made at (the part key's only changing input here)
+    int has_wheels;          // SoftBody::wheels (node tyres): their tyre patches share grip (k_tyres)
 };
 
 // ------------------------------------------------------------------------------------------ math in the reference's order

@@ -71,10 +71,12 @@ static inline HQ hfrom_mat3(HF3 c0, HF3 c1, HF3 c2) {
     return hqnormalize(q);
 }
 
-constexpr int kMemDof[3] = {0, 1, 5}, kPlateDof[3] = {2, 3, 4};
+// The element's stiffness (below) is built on the host once per triangle and on the GPU again where a triangle's
+// membrane flows (k_tri_eval): one source for both, compiled for each, so that both give the same bits.
+#define BL_HD __host__ __device__
 
 // The DKT bending's curvature-displacement matrix at area coordinates (xi, eta) (frame_fem.cpp:1482-1509)
-static void dkt_b_host(const double x[3], const double y[3], double xi, double eta, double B[3][9]) {
+BL_HD inline void dkt_b(const double x[3], const double y[3], double xi, double eta, double B[3][9]) {
     const double x23 = x[1] - x[2], x31 = x[2] - x[0], x12 = x[0] - x[1];
     const double y23 = y[1] - y[2], y31 = y[2] - y[0], y12 = y[0] - y[1];
     double P[7], q[7], r[7], t[7];
@@ -105,7 +107,7 @@ static void dkt_b_host(const double x[3], const double y[3], double xi, double e
 }
 
 // the membrane's shape gradients (frame_fem.cpp:1513-1520)
-static void tri_grad_host(const float X[3][2], double b[3], double c[3], double& A2) {
+BL_HD inline void tri_grad(const float X[3][2], double b[3], double c[3], double& A2) {
     for (int i = 0; i < 3; i++) {
         const int j = (i + 1) % 3, k = (i + 2) % 3;
         b[i] = (double)X[j][1] - X[k][1];
@@ -116,14 +118,20 @@ static void tri_grad_host(const float X[3][2], double b[3], double c[3], double&
 
 // The element's stiffness in its own axes, 18 dofs [u v w theta_x theta_y theta_z] per corner: CST membrane, DKT
 // bending at three points, the drilling spring (frame_fem.cpp:1524-1574); packed as the reference's tri_k_: the
-// membrane's 9 x 9 then the plate's (frame_fem.cpp:1628-1636)
-static void tri_stiffness_host(const float X[3][2], const FemSection& s, float P[162]) {
-    static const double kGauss[3][2] = {{1.0 / 6, 1.0 / 6}, {2.0 / 3, 1.0 / 6}, {1.0 / 6, 2.0 / 3}};
+// membrane's 9 x 9 then the plate's; and the bending's curvatures at the three points from the corners' rotations
+// alone, tri_b_ (tri_build_k, frame_fem.cpp:1625-1647). s: the section's E, nu, t, drill and its D() (float).
+struct TriSec {
+    float E, nu, t, drill;
+    BL_HD float D() const { return E * t * t * t / (12.0f * (1.0f - nu * nu)); }
+};
+BL_HD inline void tri_local_k(const float X[3][2], const TriSec& s, float P[162], float Bc[54]) {
+    const double kGauss[3][2] = {{1.0 / 6, 1.0 / 6}, {2.0 / 3, 1.0 / 6}, {1.0 / 6, 2.0 / 3}};
+    const int kMem[3] = {0, 1, 5}, kPlate[3] = {2, 3, 4};
     double K[18][18];
     for (int i = 0; i < 18; i++)
         for (int j = 0; j < 18; j++) K[i][j] = 0;
     double b[3], c[3], A2;
-    tri_grad_host(X, b, c, A2);
+    tri_grad(X, b, c, A2);
     if (A2 > 0) {
         const double A = 0.5 * A2, nu = s.nu;
         const double Dm = (double)s.E * s.t / (1 - nu * nu);
@@ -144,7 +152,7 @@ static void tri_stiffness_host(const float X[3][2], const FemSection& s, float P
         const double Db = s.D();
         for (const auto& g : kGauss) {
             double B[3][9];
-            dkt_b_host(x, y, g[0], g[1], B);
+            dkt_b(x, y, g[0], g[1], B);
             for (int p = 0; p < 9; p++)
                 for (int q = 0; q < 9; q++) {
                     double v = 0;
@@ -168,11 +176,18 @@ static void tri_stiffness_host(const float X[3][2], const FemSection& s, float P
     }
     for (int a = 0; a < 9; a++)
         for (int cc = 0; cc < 9; cc++) {
-            const int im = 6 * (a / 3) + kMemDof[a % 3], jm = 6 * (cc / 3) + kMemDof[cc % 3];
-            const int ip = 6 * (a / 3) + kPlateDof[a % 3], jp = 6 * (cc / 3) + kPlateDof[cc % 3];
-            P[a * 9 + cc] = (float)K[std::min(im, jm)][std::max(im, jm)];
-            P[81 + a * 9 + cc] = (float)K[std::min(ip, jp)][std::max(ip, jp)];
+            const int im = 6 * (a / 3) + kMem[a % 3], jm = 6 * (cc / 3) + kMem[cc % 3];
+            const int ip = 6 * (a / 3) + kPlate[a % 3], jp = 6 * (cc / 3) + kPlate[cc % 3];
+            P[a * 9 + cc] = (float)K[im < jm ? im : jm][im < jm ? jm : im];
+            P[81 + a * 9 + cc] = (float)K[ip < jp ? ip : jp][ip < jp ? jp : ip];
         }
+    const double x[3] = {X[0][0], X[1][0], X[2][0]}, y[3] = {X[0][1], X[1][1], X[2][1]};
+    for (int g = 0; g < 3; g++) {
+        double B[3][9];
+        dkt_b(x, y, kGauss[g][0], kGauss[g][1], B);
+        for (int r = 0; r < 3; r++)
+            for (int i = 0; i < 3; i++) Bc[g * 18 + r * 6 + 2 * i] = (float)B[r][3 * i + 1], Bc[g * 18 + r * 6 + 2 * i + 1] = (float)B[r][3 * i + 2];
+    }
 }
 
 struct FrameSectionH { // FrameSection (frame_fem.h:90-112): the elastic member step's fields
@@ -202,6 +217,10 @@ struct FemModel {
     std::vector<float> tmass, tarea0;
     std::vector<uint8_t> tbroken;
     std::vector<float> tk;           // 162 per triangle
+    std::vector<float> tb;           // 54 per triangle: the bending's curvatures from the corners' rotations (tri_b_)
+    std::vector<float> tX0;          // 6 per triangle: the authored rest shape (the plastic stretch is against it)
+    std::vector<float> th0;          // 9 per triangle: the corners' plastic rest rotations not yet baked into tr0
+    std::vector<float> tdmg;         // per triangle: the plastic stretch reached (FrameTri::dmg)
     // the pattern
     int ncomp = 0;
     std::vector<int> comp_first;     // per component: its first column (and a last entry: n)
@@ -270,6 +289,7 @@ static void fem_finalize(FemModel& M, const float* px, const float* py, const fl
             M.tr0[12 * t + 4 * i] = r.x, M.tr0[12 * t + 4 * i + 1] = r.y, M.tr0[12 * t + 4 * i + 2] = r.z, M.tr0[12 * t + 4 * i + 3] = r.w;
         }
     }
+    M.tX0 = M.tX, M.th0.assign(T * 9, 0.0f), M.tdmg.assign(T, 0.0f);
     M.inertia.assign(n, 0.0f);
     std::vector<float> I(n, 0.0f);
     // (the members' halves first, each node's sum in member order: the lumped m L^2 / 78 an end, m = mass_per_m L0)

@@ -27,6 +27,8 @@ namespace blg {
 
 struct FemSecDev {
     float E, nu, rho, t, damping, drill;
+    float yield;             // ShellSection::yield (Pa)
+    int plastic;             // yield > 0 on a body that deforms (SoftBody::allow_deform): the triangle flows
 };
 
 // All frames of the context, back to back (frame nodes, triangles, columns, blocks in one index space each)
@@ -42,9 +44,13 @@ struct FemDev {
     const float* inertia;
     float4* torque;
     const int4* tn;          // triangle: frame nodes, section
-    const float* tX;         // 6 / triangle
-    const float4* tr0;       // 3 / triangle
-    const float* tk;         // 162 / triangle
+    float* tX;               // 6 / triangle: the rest shape (flows with a yielding membrane)
+    float4* tr0;             // 3 / triangle: the rest frames (the bending's plastic rotations baked in)
+    float* tk;               // 162 / triangle (built again where the membrane flowed)
+    float* tb;               // 54 / triangle: the bending's curvatures from the corners' rotations (tri_b_)
+    const float* tX0;        // 6 / triangle: the authored rest shape
+    float* th0;              // 9 / triangle: the corners' plastic rest rotations (FrameTri::th0)
+    float* tdmg;             // per triangle: the plastic stretch reached (FrameTri::dmg)
     const uint8_t* tbroken;
     float4* tf;              // 3 / triangle: corner forces
     float4* tt;              // 3 / triangle: corner torques
@@ -156,6 +162,87 @@ __global__ void k_fem_begin(FemDev F, const float4* __restrict__ nd) {
 }
 
 // ------------------------------------------------------------------------------------------ per triangle
+// the element built again where its membrane flowed (tri_build_k, frame_fem.cpp:1625-1647): out of line, its 18 x 18
+// doubles in local memory only for the triangles that flow
+__device__ __noinline__ void tri_rebuild_k(FemDev F, int ti, const FemSecDev& s, const float X[3][2]) {
+    tri_local_k(X, TriSec{s.E, s.nu, s.t, s.drill}, F.tk + 162 * (size_t)ti, F.tb + 54 * (size_t)ti);
+}
+
+__device__ __forceinline__ double von_mises(const double m[3]) {
+    const double v = m[0] * m[0] - m[0] * m[1] + m[1] * m[1] + 3 * m[2] * m[2];
+    return sqrt((0.0 < v) ? v : 0.0);
+}
+
+// A yielding section's flow (eval_tris, frame_fem.cpp:1690-1741, on a body that does not break): the membrane
+// radially back to the yield stress, the rest shape following the stretch (recentred; the plastic stretch against the
+// authored shape, its largest principal stretch, into dmg; the element built again); the bending's moments at the
+// three points against the plate's plastic moment, the corners' rest rotations following theirs past it; the plastic
+// rotations baked into the rest frames past 0.02 rad. X, th0, d, b3 / c3 / A2 and sig are the caller's, updated.
+template <class Membrane>
+__device__ void tri_plastic_flow(FemDev F, int ti, const FemSecDev& s, float X[3][2], v3 th0[3], double d[18], double b3[3], double c3[3],
+                                 double& A2, const double sig[3], Membrane membrane) {
+    float dmg = F.tdmg[ti];
+    const double seq = von_mises(sig);
+    bool rest_moved = false, frames_moved = false;
+    if (seq > s.yield) {
+        const double r = 1.0 - s.yield / seq;
+        for (int i = 0; i < 3; i++) X[i][0] += (float)(r * d[6 * i]), X[i][1] += (float)(r * d[6 * i + 1]), d[6 * i] *= 1 - r, d[6 * i + 1] *= 1 - r;
+        const float mx = (X[0][0] + X[1][0] + X[2][0]) / 3.0f, my = (X[0][1] + X[1][1] + X[2][1]) / 3.0f;
+        for (int i = 0; i < 3; i++) X[i][0] -= mx, X[i][1] -= my;
+        const float* X0 = F.tX0 + 6 * (size_t)ti;
+        const double a0x = X0[2] - X0[0], a0y = X0[3] - X0[1], b0x = X0[4] - X0[0], b0y = X0[5] - X0[1];
+        const double ax = X[1][0] - X[0][0], ay = X[1][1] - X[0][1], bx = X[2][0] - X[0][0], by = X[2][1] - X[0][1];
+        const double det = a0x * b0y - b0x * a0y;
+        if (fabs(det) > 1e-12) {
+            const double i00 = b0y / det, i01 = -b0x / det, i10 = -a0y / det, i11 = a0x / det;
+            const double F00 = ax * i00 + bx * i10, F01 = ax * i01 + bx * i11, F10 = ay * i00 + by * i10, F11 = ay * i01 + by * i11;
+            const double C00 = F00 * F00 + F10 * F10, C01 = F00 * F01 + F10 * F11, C11 = F01 * F01 + F11 * F11;
+            const double lmax = 0.5 * (C00 + C11) + sqrt(0.25 * (C00 - C11) * (C00 - C11) + C01 * C01);
+            dmg = smax(dmg, (float)(sqrt(lmax) - 1.0));
+        }
+        rest_moved = true;
+        tri_rebuild_k(F, ti, s, X);
+        tri_grad(X, b3, c3, A2);
+        membrane();
+    }
+    const float* Bc = F.tb + 54 * (size_t)ti;
+    const float Df = s.E * s.t * s.t * s.t / (12.0f * (1.0f - s.nu * s.nu));
+    const double D = Df, nu = s.nu, Mp = 0.25 * s.yield * (double)s.t * s.t;
+    double meq = 0;
+    for (int g = 0; g < 3; g++) {
+        double kap[3] = {0, 0, 0};
+        for (int r = 0; r < 3; r++)
+            for (int i = 0; i < 3; i++) kap[r] += Bc[g * 18 + r * 6 + 2 * i] * d[6 * i + 3] + Bc[g * 18 + r * 6 + 2 * i + 1] * d[6 * i + 4];
+        const double m[3] = {D * (kap[0] + nu * kap[1]), D * (nu * kap[0] + kap[1]), D * 0.5 * (1 - nu) * kap[2]};
+        const double vm = von_mises(m);
+        meq = (meq < vm) ? vm : meq;
+    }
+    if (meq > Mp) {
+        const double r = 1.0 - Mp / meq;
+        for (int i = 0; i < 3; i++) {
+            th0[i].x += (float)(r * d[6 * i + 3]), th0[i].y += (float)(r * d[6 * i + 4]);
+            d[6 * i + 3] *= 1 - r, d[6 * i + 4] *= 1 - r;
+        }
+        dmg = smax(dmg, 1e-5f);
+    }
+    for (int i = 0; i < 3; i++)
+        if (dot(th0[i], th0[i]) > 0.02f * 0.02f) {
+            const float4 rf = F.tr0[3 * ti + i];
+            const q4 r0 = qnormalize(qmul(q4{rf.x, rf.y, rf.z, rf.w}, quat_exp(V(-th0[i].x, -th0[i].y, -th0[i].z))));
+            F.tr0[3 * ti + i] = make_float4(r0.x, r0.y, r0.z, r0.w);
+            th0[i] = V(0, 0, 0);
+            frames_moved = true;
+        }
+    if (rest_moved)
+        for (int i = 0; i < 3; i++) F.tX[6 * ti + 2 * i] = X[i][0], F.tX[6 * ti + 2 * i + 1] = X[i][1];
+    (void)frames_moved;
+    for (int i = 0; i < 3; i++) F.th0[9 * ti + 3 * i] = th0[i].x, F.th0[9 * ti + 3 * i + 1] = th0[i].y, F.th0[9 * ti + 3 * i + 2] = th0[i].z;
+    F.tdmg[ti] = dmg;
+}
+
+// kPlastic: the variant for contexts with a yielding section (its flow's registers and the element's rebuild kept out
+// of the elastic one)
+template <bool kPlastic>
 __global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __restrict__ nd) {
     const int ti = blockIdx.x * blockDim.x + threadIdx.x;
     if (ti >= F.ntri) return;
@@ -166,6 +253,8 @@ __global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __rest
     const FemSecDev s = F.sec[tn.w];
     float X[3][2];
     for (int i = 0; i < 3; i++) X[i][0] = F.tX[6 * ti + 2 * i], X[i][1] = F.tX[6 * ti + 2 * i + 1];
+    v3 th0[3];
+    for (int i = 0; i < 3; i++) th0[i] = kPlastic ? V(F.th0[9 * ti + 3 * i], F.th0[9 * ti + 3 * i + 1], F.th0[9 * ti + 3 * i + 2]) : V(0, 0, 0);
     // ---- tri_kinematics (frame_fem.cpp:1584-1621)
     double x[3][3];
     for (int i = 0; i < 3; i++)
@@ -199,26 +288,26 @@ __global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __rest
         d[6 * i + 1] = -sp * p[i][0] + cp * p[i][1] - X[i][1];
         d[6 * i + 2] = 0;
         const float4 qf = F.q[fnv[i]], rf = F.tr0[3 * ti + i];
-        const v3 th = quat_log(qmul(Ec, qnormalize(qmul(q4{qf.x, qf.y, qf.z, qf.w}, q4{rf.x, rf.y, rf.z, rf.w}))));
+        const v3 th = quat_log(qmul(Ec, qnormalize(qmul(q4{qf.x, qf.y, qf.z, qf.w}, q4{rf.x, rf.y, rf.z, rf.w})))) - th0[i];
         d[6 * i + 3] = th.x, d[6 * i + 4] = th.y, d[6 * i + 5] = th.z;
     }
-    // ---- eval_tris (frame_fem.cpp:1661-1831), an elastic section
-    double b3[3], c3[3];
-    for (int i = 0; i < 3; i++) {
-        const int j = (i + 1) % 3, k = (i + 2) % 3;
-        b3[i] = (double)X[j][1] - X[k][1];
-        c3[i] = (double)X[k][0] - X[j][0];
-    }
-    const double A2 = ((double)X[1][0] - X[0][0]) * ((double)X[2][1] - X[0][1]) - ((double)X[2][0] - X[0][0]) * ((double)X[1][1] - X[0][1]);
+    // ---- eval_tris (frame_fem.cpp:1661-1831)
+    double b3[3], c3[3], A2;
+    tri_grad(X, b3, c3, A2);
     if (!(A2 > 0)) return;
     const double nu = s.nu, Dm = (double)s.E / (1 - nu * nu);
-    double eps[3] = {0, 0, 0}, sig[3];
-    for (int i = 0; i < 3; i++) {
-        eps[0] += b3[i] * d[6 * i] / A2;
-        eps[1] += c3[i] * d[6 * i + 1] / A2;
-        eps[2] += (c3[i] * d[6 * i] + b3[i] * d[6 * i + 1]) / A2;
-    }
-    sig[0] = Dm * (eps[0] + nu * eps[1]), sig[1] = Dm * (nu * eps[0] + eps[1]), sig[2] = Dm * 0.5 * (1 - nu) * eps[2];
+    double eps[3], sig[3];
+    auto membrane = [&]() {
+        eps[0] = eps[1] = eps[2] = 0;
+        for (int i = 0; i < 3; i++) {
+            eps[0] += b3[i] * d[6 * i] / A2;
+            eps[1] += c3[i] * d[6 * i + 1] / A2;
+            eps[2] += (c3[i] * d[6 * i] + b3[i] * d[6 * i + 1]) / A2;
+        }
+        sig[0] = Dm * (eps[0] + nu * eps[1]), sig[1] = Dm * (nu * eps[0] + eps[1]), sig[2] = Dm * 0.5 * (1 - nu) * eps[2];
+    };
+    membrane();
+    if (kPlastic && s.plastic) tri_plastic_flow(F, ti, s, X, th0, d, b3, c3, A2, sig, membrane);
     const float* Km = F.tk + 162 * (size_t)ti;
     const float* Kp = Km + 81;
     double vl[18];

@@ -516,7 +516,10 @@ struct NodeFem {
 __device__ __forceinline__ void accumulate_bounds(Body* __restrict__ bodies, int body, bool live, v3 p, v3 pmx, float v2, int contact) {
     const int lane = threadIdx.x & 31;
     const int b0 = __shfl_sync(0xffffffffu, body, 0);
-    const bool uniform = __all_sync(0xffffffffu, body == b0 && live);
+    // (one body's warp: reduced, its lanes that are not live - asleep, a frame's, a tyre node its wheel integrates -
+    // adding nothing)
+    const bool uniform = __all_sync(0xffffffffu, body == b0) && __any_sync(0xffffffffu, live);
+    if (!live) p = V(1e30f, 1e30f, 1e30f), pmx = V(-1e30f, -1e30f, -1e30f), v2 = 0.0f, contact = 0;
     if (uniform) {
         float mnx = p.x, mny = p.y, mnz = p.z, mxx = pmx.x, mxy = pmx.y, mxz = pmx.z, vv = v2;
         int cc = contact;
@@ -580,6 +583,83 @@ __device__ __forceinline__ void fem_gather(const NodeFem& nf, int i, v3 f) {
 // for World::collide_static and the integration (k_integrate) - the contacts between bodies add to it first.
 // Frame bodies (Body::is_fem): the triangles' forces and torques are gathered onto the frame nodes in the reference's
 // order (gather_forces, frame_fem.cpp:2080-2105) and the force is kept in nforce for the frame's implicit step.
+// ------------------------------------------------------------------------------------------ air drag
+// The parts of the bodies with air drag and their mean velocities (SoftBody::part_labels, softbody.cpp:237-259, and
+// clear_forces' sums, softbody.cpp:334-378), one thread a body, serially in node order as the reference sums: every
+// substep the labels age; they are made again (union of the unbroken beams, parts numbered by their first node) at the
+// first call and when beams broke since and they are 8 calls old. Then per part the mass-weighted mean velocity
+// (pmv) and the aerodynamic acceleration (pacc), at node0 + part.
+struct DragDev {
+    int* up;                 // per node: union-find scratch
+    int* pid;                // per node: a root's part number (scratch)
+    int* part;               // per node: its part
+    float4* pmv;             // per part (at node0 + part): mean velocity; w: the part's mass while summing
+    float4* pacc;            // per part: the aerodynamic acceleration
+};
+__global__ void k_drag_parts(Body* __restrict__ bodies, int nbodies, const float4* __restrict__ nd, const int2* __restrict__ ab,
+                             const uint32_t* __restrict__ bmeta, DragDev D) {
+    const int bi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bi >= nbodies) return;
+    Body& B = bodies[bi];
+    if (!B.drag || B.sleeping) return;
+    const int n0 = B.node0, nn = B.nnodes;
+    B.part_age += 1;
+    if (B.part_count == 0 || (B.broken_beams != B.part_key && B.part_age >= 8)) {
+        int* u = D.up + n0;
+        for (int i = 0; i < nn; i++) u[i] = i;
+        auto find = [&](int x) {
+            while (u[x] != x) x = u[x] = u[u[x]];
+            return x;
+        };
+        for (int j = B.beam0; j < B.beam0 + B.nbeams; j++) {
+            if ((bmeta[j] >> 8) & BF_BROKEN) continue;
+            const int2 e = ab[j];
+            const int rc = find(e.y - n0);
+            u[find(e.x - n0)] = rc;
+        }
+        int* id = D.pid + n0;
+        for (int i = 0; i < nn; i++) u[i] = find(i), id[i] = -1;
+        int cnt = 0;
+        for (int i = 0; i < nn; i++) {
+            if (id[u[i]] < 0) id[u[i]] = cnt++;
+            D.part[n0 + i] = id[u[i]];
+        }
+        B.part_count = cnt, B.part_key = B.broken_beams, B.part_age = 0;
+    }
+    const int np = B.part_count;
+    for (int q = 0; q < np; q++) D.pmv[n0 + q] = make_float4(0, 0, 0, 0);
+    float M = 0;
+    for (int i = 0; i < nn; i++) {
+        const float4 v = nd[2 * (n0 + i) + 1];
+        float4& pv = D.pmv[n0 + D.part[n0 + i]];
+        pv.x = pv.x + v.x * v.w, pv.y = pv.y + v.y * v.w, pv.z = pv.z + v.z * v.w;
+        pv.w = pv.w + v.w;
+        M = M + v.w;
+    }
+    for (int q = 0; q < np; q++) {
+        const float4 pv = D.pmv[n0 + q];
+        const v3 mv = pv.w > 0 ? divs(V(pv.x, pv.y, pv.z), pv.w) : V(0, 0, 0);
+        const v3 a = M > 0 ? mv * (-0.5f * 1.225f * B.aero_cda * length(mv) / M) : V(0, 0, 0);
+        D.pmv[n0 + q] = make_float4(mv.x, mv.y, mv.z, 0.0f);
+        D.pacc[n0 + q] = make_float4(a.x, a.y, a.z, 0.0f);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ wheels and tyres
+// The wheels of node tyres (Wheel, softbody.h:468-498), free rolling: per wheel its hub nodes and its tyre nodes in
+// ascending order (the order the tyre patch's sums run in, world.cpp:871-898); per node its wheel and the parity of
+// its place in the wheel's list (the hub it turns about); per node the substep's tyre contact.
+// A tyre node on no wheel is a patch of its own: a wheel of one node with no hubs (axle0 -1), which gives the same bits
+// (its sums are its own need and cap).
+struct WheelDev {
+    const int4* wheel;       // axle0, axle1 (global nodes; -1: a lone tyre node's), first of its nodes in wnodes, count
+    const int* wnodes;       // the wheels' tyre nodes, each wheel's ascending
+    const int2* nwheel;      // per node: (its wheel, the parity of its place in the wheel's list); (-1, 0): none
+    float4* tcon;            // per node: its static contact this substep (normal xyz, depth w), left for k_tyres
+    float4* tfric;           // per node: (friction coefficient, surface, -, 1 while it waits for k_tyres)
+    float tyre_grip;         // WorldSettings::tyre_grip
+};
+
 // kPacked: the incidences as 32-bit words: the beam's index less the warp's base (ell_base, bits 0-14; 0x7fff:
 // padding), bit 15 set where this node is the beam's b end, the other end's index less this node's plus 32768 (bits
 // 16-31) - half the bytes of the (beam | b-end bit, other end) pairs, for rigs whose warps' beams and neighbours lie
@@ -588,18 +668,31 @@ template <bool kPacked>
 __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
                                                const void* __restrict__ ell_, const int* __restrict__ ell_base, const float* __restrict__ fsc,
                                                Body* __restrict__ bodies, float gx, float gy, float gz, int nnodes, int first, NodeFem nf,
-                                               float4* __restrict__ fnode) {
+                                               float4* __restrict__ fnode, DragDev dg, WheelDev wh) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int body = -1;
     float v2 = 0.0f;
     bool live = false;
     if (i < nnodes) {
-        body = info[i].w;
+        const int4 inf = info[i];
+        body = inf.w;
         const Body& B = bodies[body];
         if (!B.sleeping) {
             const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
             const float m = Vv.w;
-            v3 f = V(gx * m, gy * m, gz * m);
+            v3 f;
+            if (!B.drag) {
+                f = V(gx * m, gy * m, gz * m);
+            } else { // (clear_forces with drag: (g + the part's aerodynamic acceleration) m, less RoR's drag on v - its mean)
+                const int q = B.node0 + dg.part[i];
+                const float4 a = dg.pacc[q];
+                f = V((gx + a.x) * m, (gy + a.y) * m, (gz + a.z) * m);
+                if (!((uint32_t)inf.x & (NF_TYRE | NF_RIM))) {
+                    const float4 mv = dg.pmv[q];
+                    const v3 vr = V(Vv.x - mv.x, Vv.y - mv.y, Vv.z - mv.z);
+                    f = f - vr * (B.air_drag * length(vr));
+                }
+            }
             if (B.has_ext) {
                 const float4 e = nf.ext[i];
                 f = V(f.x + e.x, f.y + e.y, f.z + e.z);
@@ -642,6 +735,22 @@ __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd,
 #pragma unroll
                 for (int u = 0; u < 4; u++) add(pad[u], bend[u], sc[u], Po[u]);
             }
+            if (B.has_wheels) { // (compute_wheel_forces, softbody.cpp:691-744: a free wheel's torque is 0, its share 0 / nodes)
+                const int2 nw = wh.nwheel[i];
+                const int4 W = nw.x >= 0 ? wh.wheel[nw.x] : make_int4(-1, -1, 0, 0);
+                if (W.x >= 0) {
+                    const float4 H0 = nd[2 * W.x], H1 = nd[2 * W.y];
+                    const v3 axis = normalize(V(H1.x - H0.x, H1.y - H0.y, H1.z - H0.z));
+                    const float4 hub = nw.y ? H1 : H0;
+                    const v3 rad = V(P.x - hub.x, P.y - hub.y, P.z - hub.z);
+                    const float rl2 = dot(rad, rad);
+                    if (!(rl2 < 1e-8f)) {
+                        const float inv = 1.0f / sqrtf(rl2);
+                        const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
+                        f = f + dir * ((0.0f / (float)W.w) * inv);
+                    }
+                }
+            }
             if (B.is_fem) {
                 live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)
                 if (first) v2 = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
@@ -654,11 +763,68 @@ __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd,
     accumulate_bounds(bodies, body, live, V(1e30f, 1e30f, 1e30f), V(-1e30f, -1e30f, -1e30f), v2, 0);
 }
 
+// tyre_contact (static_world.cpp:53-83)
+struct TyreC {
+    v3 normal_force, need, slide;
+    float cap;
+    bool touching;
+};
+__device__ TyreC tyre_contact(v3 F, v3 vel, float mass, v3 normal, float dt, const GroundModel& gm, float pen, float friction_coef) {
+    TyreC t;
+    t.normal_force = V(0, 0, 0), t.need = V(0, 0, 0), t.slide = V(0, 0, 0), t.cap = 0.0f, t.touching = false;
+    const float Vn = dot(vel, normal);
+    const float Fn = dot(F, normal);
+    const float sgl = gm.soft_depth;
+    if (sgl > 0 && pen >= 0) {
+        t.normal_force = t.normal_force + vel * (-gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f));
+        float Fb = gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f;
+        if (Vn >= 0 && Fn < 0 && Fb > -Fn) Fb = -Fn;
+        t.normal_force = t.normal_force + normal * Fb;
+    }
+    if (pen < sgl) return t;
+    float R = -Fn;
+    if (Vn < 0) R -= (0.8f * Vn - smin(0.2f * (pen - sgl) / dt, 2.0f)) * mass / dt;
+    if (R <= 0) return t;
+    t.touching = true;
+    t.normal_force = t.normal_force + normal * R;
+    const v3 slipF = F - normal * Fn;
+    const v3 slipV = vel - normal * Vn;
+    const float G = R * gm.strength * friction_coef;
+    t.need = V(-slipF.x, -slipF.y, -slipF.z) - slipV * (0.5f * mass / dt);
+    t.cap = gm.ms * G;
+    const float sv = length(slipV);
+    const float mu_slide = smax(gm.mc, 0.85f * gm.ms);
+    const float g = mu_slide + (gm.ms - mu_slide) * bl_expf(-bl_powf(sv / gm.vs, gm.alpha)) + smin(gm.t2 * sv, 5.0f);
+    const float nl = length(t.need);
+    const v3 dir = sv > 0.05f ? slipV * (-1.0f / sv) : (nl > 1e-6f ? t.need * (1.0f / nl) : V(0, 0, 0));
+    t.slide = dir * (g * G);
+    return t;
+}
+
+// SoftBody::integrate_nodes for one node (softbody.cpp:769-795): v += f inv_m dt, the 400 m/s clamp, NaN reset,
+// p += v dt; v2: its squared speed after
+__device__ __forceinline__ void integrate_node(v3& pos, v3& vel, float inv_mass, v3 f, float dt, float& v2) {
+    if (inv_mass > 0) {
+        vel = vel + f * (inv_mass * dt);
+        v2 = dot(vel, vel);
+        if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
+            vel = vel * (kMaxNodeSpeed / sqrtf(v2));
+            v2 = kMaxNodeSpeed * kMaxNodeSpeed;
+        } else if (!(v2 >= 0.0f)) {
+            vel = V(0, 0, 0);
+            v2 = 0;
+        }
+        pos = pos + vel * dt;
+    }
+}
+
 // World::collide_static for the node (world.cpp:781-870), then SoftBody::integrate_nodes (softbody.cpp:769-795), on
 // the force in fnode (gravity, beams, contacts with other bodies). first: the frame's first substep (the top speed
 // starts from the velocities before it, world.cpp:3217-3222). Frame bodies' nodes are integrated after their solve.
+// A tyre node (NF_TYRE) in contact leaves its contact in wh.tcon / wh.tfric and its force in fnode to its wheel's
+// patch (k_tyres), which takes tyre_contact instead of primitive_collision and integrates it.
 __global__ void __launch_bounds__(256) k_integrate(float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Statics st,
-                                                   float dt, int nnodes, int first, const float4* __restrict__ fnode) {
+                                                   float dt, int nnodes, int first, float4* __restrict__ fnode, WheelDev wh) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int body = -1;
     v3 p = V(1e30f, 1e30f, 1e30f), pmx = V(-1e30f, -1e30f, -1e30f);
@@ -723,6 +889,10 @@ __global__ void __launch_bounds__(256) k_integrate(float4* __restrict__ nd, cons
                                 const float fl = length(fcn);
                                 if (fl > c.max_force) fcn = fcn * (c.max_force / fl);
                                 f = f + fcn;
+                            } else if (flags & NF_TYRE) { // (its wheel's patch: k_tyres)
+                                wh.tcon[i] = make_float4(c.normal.x, c.normal.y, c.normal.z, c.depth);
+                                wh.tfric[i] = make_float4(fc * wh.tyre_grip, __int_as_float(c.surface), 0.0f, 1.0f);
+                                live = false;
                             } else {
                                 f = f + primitive_collision(f, vel, m, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, B.bounce);
                             }
@@ -730,28 +900,115 @@ __global__ void __launch_bounds__(256) k_integrate(float4* __restrict__ nd, cons
                     }
                 }
             }
+            if (live) {
             // ---- integration (SoftBody::integrate_nodes)
-            if (inv_mass > 0) {
-                vel = vel + f * (inv_mass * dt);
-                v2 = dot(vel, vel);
-                if (v2 > kMaxNodeSpeed * kMaxNodeSpeed) {
-                    vel = vel * (kMaxNodeSpeed / sqrtf(v2));
-                    v2 = kMaxNodeSpeed * kMaxNodeSpeed;
-                } else if (!(v2 >= 0.0f)) {
-                    vel = V(0, 0, 0);
-                    v2 = 0;
-                }
-                pos = pos + vel * dt;
-            }
+            integrate_node(pos, vel, inv_mass, f, dt, v2);
             nd[2 * i] = make_float4(pos.x, pos.y, pos.z, inv_mass);
             nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, m);
             // the bounds skip a non-finite coordinate as the reference's vmin / vmax do (a NaN never compares less)
             p = V(pos.x == pos.x ? pos.x : 1e30f, pos.y == pos.y ? pos.y : 1e30f, pos.z == pos.z ? pos.z : 1e30f);
             pmx = V(pos.x == pos.x ? pos.x : -1e30f, pos.y == pos.y ? pos.y : -1e30f, pos.z == pos.z ? pos.z : -1e30f);
             v2 = smax(v2, v2start);
+            } else {
+                contact = 0; // (counted with its wheel's patch)
+            }
         }
     }
     accumulate_bounds(bodies, body, live, p, pmx, v2, contact);
+}
+
+// World::collide_static's tyre contacts and patches (world.cpp:856-898) and the integration of their nodes: a warp a
+// wheel, a lane a tyre node (in chunks of 32) - each node in contact gets tyre_contact on its force and its normal
+// force; the touching ones' needs and caps summed in ascending node order (every lane adds the same broadcast values
+// in the same order); each touching node sticks (its need) if the patch as a whole can hold, else slides; then
+// SoftBody::integrate_nodes for them, the warp's bounds, top speed and contacts into the body's accumulators.
+__global__ void __launch_bounds__(256) k_tyres(float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, float dt,
+                                               int nwheels, int first, const float4* __restrict__ fnode, WheelDev wh) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nwheels) return; // (w is the warp's: its lanes leave together)
+    const int4 W = wh.wheel[w];
+    const int body = info[wh.wnodes[W.z]].w;
+    v3 need = V(0, 0, 0), mn = V(1e30f, 1e30f, 1e30f), mx = V(-1e30f, -1e30f, -1e30f);
+    float cap = 0.0f, vv = 0.0f;
+    int cnt = 0;
+    // pass 1: the contacts and the patch's sums (one chunk's nodes kept in registers for pass 2)
+    int i = -1;
+    TyreC t = {};
+    v3 f = V(0, 0, 0);
+    bool pend = false;
+    for (int c = 0; c < W.w; c += 32) {
+        pend = false;
+        if (c + lane < W.w) {
+            i = wh.wnodes[W.z + c + lane];
+            const float4 tf = wh.tfric[i];
+            pend = tf.w != 0.0f;
+            if (pend) {
+                const float4 cn = wh.tcon[i], f4 = fnode[i], Vv = nd[2 * i + 1];
+                const int surf = __float_as_int(tf.y);
+                const GroundModel& gm = c_ground[surf < kSurfCount ? surf : 0];
+                f = V(f4.x, f4.y, f4.z);
+                t = tyre_contact(f, V(Vv.x, Vv.y, Vv.z), Vv.w, V(cn.x, cn.y, cn.z), dt, gm, cn.w, tf.x);
+                f = f + t.normal_force;
+            }
+        }
+        const bool touch = pend && t.touching;
+        for (unsigned m = __ballot_sync(0xffffffffu, touch); m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            need = V(need.x + __shfl_sync(0xffffffffu, t.need.x, l), need.y + __shfl_sync(0xffffffffu, t.need.y, l),
+                     need.z + __shfl_sync(0xffffffffu, t.need.z, l));
+            cap = cap + __shfl_sync(0xffffffffu, t.cap, l);
+        }
+    }
+    const bool stick = length(need) <= cap;
+    // pass 2: the forces applied and the nodes integrated (a wheel of more than 32 nodes: its contacts again)
+    for (int c = 0; c < W.w; c += 32) {
+        if (W.w > 32) {
+            pend = false;
+            if (c + lane < W.w) {
+                i = wh.wnodes[W.z + c + lane];
+                const float4 tf = wh.tfric[i];
+                pend = tf.w != 0.0f;
+                if (pend) {
+                    const float4 cn = wh.tcon[i], f4 = fnode[i], Vv = nd[2 * i + 1];
+                    const int surf = __float_as_int(tf.y);
+                    const GroundModel& gm = c_ground[surf < kSurfCount ? surf : 0];
+                    f = V(f4.x, f4.y, f4.z);
+                    t = tyre_contact(f, V(Vv.x, Vv.y, Vv.z), Vv.w, V(cn.x, cn.y, cn.z), dt, gm, cn.w, tf.x);
+                    f = f + t.normal_force;
+                }
+            }
+        }
+        if (!pend) continue;
+        if (t.touching) f = f + (stick ? t.need : t.slide);
+        wh.tfric[i].w = 0.0f;
+        const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
+        v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
+        float v2 = 0.0f;
+        const float v2start = first ? Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z : 0.0f;
+        integrate_node(pos, vel, P.w, f, dt, v2);
+        nd[2 * i] = make_float4(pos.x, pos.y, pos.z, P.w);
+        nd[2 * i + 1] = make_float4(vel.x, vel.y, vel.z, Vv.w);
+        // (the bounds skip a non-finite coordinate as the reference's vmin / vmax do)
+        mn = V(fminf(mn.x, pos.x == pos.x ? pos.x : 1e30f), fminf(mn.y, pos.y == pos.y ? pos.y : 1e30f), fminf(mn.z, pos.z == pos.z ? pos.z : 1e30f));
+        mx = V(fmaxf(mx.x, pos.x == pos.x ? pos.x : -1e30f), fmaxf(mx.y, pos.y == pos.y ? pos.y : -1e30f), fmaxf(mx.z, pos.z == pos.z ? pos.z : -1e30f));
+        vv = fmaxf(vv, smax(v2, v2start));
+        cnt++;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = V(fminf(mn.x, __shfl_xor_sync(0xffffffffu, mn.x, o)), fminf(mn.y, __shfl_xor_sync(0xffffffffu, mn.y, o)),
+               fminf(mn.z, __shfl_xor_sync(0xffffffffu, mn.z, o)));
+        mx = V(fmaxf(mx.x, __shfl_xor_sync(0xffffffffu, mx.x, o)), fmaxf(mx.y, __shfl_xor_sync(0xffffffffu, mx.y, o)),
+               fmaxf(mx.z, __shfl_xor_sync(0xffffffffu, mx.z, o)));
+        vv = fmaxf(vv, __shfl_xor_sync(0xffffffffu, vv, o));
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    }
+    if (lane == 0 && cnt > 0) {
+        Body& B = bodies[body];
+        atomic_min_f(&B.acc_mn[0], mn.x), atomic_min_f(&B.acc_mn[1], mn.y), atomic_min_f(&B.acc_mn[2], mn.z);
+        atomic_max_f(&B.acc_mx[0], mx.x), atomic_max_f(&B.acc_mx[1], mx.y), atomic_max_f(&B.acc_mx[2], mx.z);
+        atomic_max_f(&B.acc_v2, vv);
+        atomicAdd(&B.acc_contacts, cnt);
+    }
 }
 
 // ------------------------------------------------------------------------------------------ end of frame

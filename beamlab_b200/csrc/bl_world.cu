@@ -48,6 +48,11 @@ struct HostBody {
     std::vector<float> fq, fw;             // frame nodes' orientation (4) and angular velocity (3)
     float theta = 0.5f, diss = 0.02f;
     int fem_failures = 0, fem_clamps = 0;
+    struct Wheel {
+        uint32_t axle0, axle1;
+        std::vector<uint32_t> nodes;      // its tyre nodes in the given order (the parity of a place: the hub it turns about)
+    };
+    std::vector<Wheel> wheels;             // its free-rolling node wheels (empty: none)
 };
 
 template <class T>
@@ -117,8 +122,17 @@ struct bl_gpu_ctx {
     Statics st{};
     // FEM frames of all bodies back to back (see bl_fem_kernels.cuh)
     int NF = 0, NT = 0, NB = 0, n_fem_nodes = 0;
+    bool any_plastic = false;                  // a yielding shell section on a body that deforms (k_tri_eval<true>)
     int64_t NU = 0;                            // block updates of a factorization
     bool any_ext = false;
+    bool any_drag = false;                     // some body has air drag (k_drag_parts)
+    DevBuf<int> dup, dpid, dpart;
+    DevBuf<float4> dpmv, dpacc;
+    int NW = 0;                                // the wheels of all bodies, and lone tyre nodes (k_tyres: a warp a wheel)
+    DevBuf<int4> dwheel;
+    DevBuf<int> dwnodes;
+    DevBuf<int2> dnwheel;
+    DevBuf<float4> dtcon, dtfric;
     std::vector<int> lvl_grp_ptr, lvl_col_ptr; // per level: its update groups / columns
     int64_t fem_launches = 0;                  // kernels of one substep's frame step (with the Cholesky)
     int64_t chol_launches = 0;                 // of those, the factorization's and substitutions'
@@ -159,7 +173,7 @@ struct bl_gpu_ctx {
     DevBuf<int> fcol, fchain;
     DevBuf<int4> fblk;
     DevBuf<double> fD, fb;
-    DevBuf<float> finertia, tX, tk, ttan;
+    DevBuf<float> finertia, tX, tk, ttan, tb, tX0, th0, tdmg;
     DevBuf<uint8_t> tbroken, ton, ffixed;
     DevBuf<FemSecDev> fsec;
     FemDev fd{};
@@ -221,7 +235,7 @@ static void free_fem(bl_gpu_ctx* c) {
     c->mn.free_(), c->mmeta.free_(), c->mL0.free_(), c->mq.free_(), c->mfa.free_(), c->mta.free_(), c->mtb.free_(), c->mtan.free_();
     c->msec.free_(), c->mon.free_(), c->mkw.free_(), c->mkv.free_(), c->NM = 0;
     c->xd.free_(), c->diag.free_(), c->ldiag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
-    c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
+    c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->tb.free_(), c->tX0.free_(), c->th0.free_(), c->tdmg.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
 }
 
 static void free_contacts(bl_gpu_ctx* c) {
@@ -238,6 +252,8 @@ static void free_device(bl_gpu_ctx* c) {
     free_contacts(c);
     c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->ell_ptr.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
     c->inc4.free_(), c->ell_base.free_(), c->packed_inc = false;
+    c->dup.free_(), c->dpid.free_(), c->dpart.free_(), c->dpmv.free_(), c->dpacc.free_();
+    c->dwheel.free_(), c->dwnodes.free_(), c->dnwheel.free_(), c->dtcon.free_(), c->dtfric.free_(), c->NW = 0;
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
 }
@@ -351,6 +367,7 @@ static int pull_state(bl_gpu_ctx* c) {
             b.stress = stress[r.beam0 + j];
         }
         hb.rec = r;
+        hb.rec.part_count = 0; // (the parts' labels live in arrays made again at the commit: made again at the next call)
     }
     if (c->contacts_on && c->NTRI > 0) {
         std::vector<int4> tri(c->NTRI);
@@ -383,6 +400,34 @@ static int pull_state(bl_gpu_ctx* c) {
             }
             fo += nf;
         }
+        if (c->NT > 0) { // (the triangles' plastic state: rest shapes and frames, stiffnesses, their flow)
+            std::vector<float> tX(6 * (size_t)c->NT), tk(162 * (size_t)c->NT), tb(54 * (size_t)c->NT), th0(9 * (size_t)c->NT), tdmg(c->NT);
+            std::vector<float4> tr0(3 * (size_t)c->NT);
+            BL_CUDA(c, cudaMemcpy(tX.data(), c->tX.p, sizeof(float) * tX.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(tk.data(), c->tk.p, sizeof(float) * tk.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(tb.data(), c->tb.p, sizeof(float) * tb.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(th0.data(), c->th0.p, sizeof(float) * th0.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(tdmg.data(), c->tdmg.p, sizeof(float) * tdmg.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(tr0.data(), c->tr0.p, sizeof(float4) * tr0.size(), cudaMemcpyDeviceToHost));
+            int to = 0;
+            for (int bi = 0; bi < c->B; bi++) {
+                HostBody& hb = c->bodies[bi];
+                if (!hb.fem) continue;
+                FemModel& M = *hb.fem;
+                const size_t nt = M.tn.size();
+                std::copy(tX.begin() + 6 * to, tX.begin() + 6 * (to + nt), M.tX.begin());
+                std::copy(tk.begin() + 162 * to, tk.begin() + 162 * (to + nt), M.tk.begin());
+                std::copy(tb.begin() + 54 * to, tb.begin() + 54 * (to + nt), M.tb.begin());
+                std::copy(th0.begin() + 9 * to, th0.begin() + 9 * (to + nt), M.th0.begin());
+                std::copy(tdmg.begin() + to, tdmg.begin() + to + nt, M.tdmg.begin());
+                for (size_t t = 0; t < nt; t++)
+                    for (int i = 0; i < 3; i++) {
+                        const float4 r = tr0[3 * (to + t) + i];
+                        M.tr0[12 * t + 4 * i] = r.x, M.tr0[12 * t + 4 * i + 1] = r.y, M.tr0[12 * t + 4 * i + 2] = r.z, M.tr0[12 * t + 4 * i + 3] = r.w;
+                    }
+                to += (int)nt;
+            }
+        }
     }
     return BL_GPU_OK;
 }
@@ -396,7 +441,7 @@ static int commit_fem(bl_gpu_ctx* c) {
     for (const HostBody& hb : c->bodies)
         if (hb.fem) NF += (int)hb.fem->node.size(), NT += (int)hb.fem->tn.size(), NB += (int)hb.fem->row.size(), NC += hb.fem->ncomp,
                     NS += (int)hb.sections.size(), nfem_nodes += hb.rec.nnodes;
-    c->NF = NF, c->NT = NT, c->NB = NB, c->n_fem_nodes = nfem_nodes;
+    c->NF = NF, c->NT = NT, c->NB = NB, c->n_fem_nodes = nfem_nodes, c->any_plastic = false;
     c->lvl_grp_ptr.clear(), c->lvl_col_ptr.clear();
     std::vector<float4> ext(c->any_ext ? c->N : 0, make_float4(0, 0, 0, 0));
     for (const HostBody& hb : c->bodies)
@@ -412,7 +457,7 @@ static int commit_fem(bl_gpu_ctx* c) {
     std::vector<int> fem_nodes, fslot(c->N, -1), level(NF, 0);
     std::vector<double> xd(3 * (size_t)NF), ch2(NF), chd(NF);
     std::vector<float4> q(NF), w(NF), tr0(3 * (size_t)NT);
-    std::vector<float> inertia(NF), tX(6 * (size_t)NT), tk(162 * (size_t)NT);
+    std::vector<float> inertia(NF), tX(6 * (size_t)NT), tk(162 * (size_t)NT), tb(54 * (size_t)NT), tX0(6 * (size_t)NT), th0(9 * (size_t)NT), tdmg(NT);
     std::vector<int4> tn(NT), goff;
     std::vector<int2> gdiag;
     std::vector<uint8_t> tbroken(NT);
@@ -471,9 +516,17 @@ static int commit_fem(bl_gpu_ctx* c) {
             for (int x = 0; x < 6; x++) tX[6 * (size_t)(to + t) + x] = M.tX[6 * t + x];
             for (int i = 0; i < 3; i++) tr0[3 * (size_t)(to + t) + i] = make_float4(M.tr0[12 * t + 4 * i], M.tr0[12 * t + 4 * i + 1], M.tr0[12 * t + 4 * i + 2], M.tr0[12 * t + 4 * i + 3]);
             for (int x = 0; x < 162; x++) tk[162 * (size_t)(to + t) + x] = M.tk[162 * t + x];
+            for (int x = 0; x < 54; x++) tb[54 * (size_t)(to + t) + x] = M.tb[54 * t + x];
+            for (int x = 0; x < 6; x++) tX0[6 * (size_t)(to + t) + x] = M.tX0[6 * t + x];
+            for (int x = 0; x < 9; x++) th0[9 * (size_t)(to + t) + x] = M.th0[9 * t + x];
+            tdmg[to + t] = M.tdmg[t];
             tbroken[to + t] = M.tbroken[t];
         }
-        for (const FemSection& fs : hb.sections) sec.push_back(FemSecDev{fs.E, fs.nu, fs.rho, fs.t, fs.damping, fs.drill});
+        // (a section yields where the body deforms: eval_tris' s.yield > 0 && b.allow_deform)
+        const int plastic = (hb.beam_bits & BB_DEFORM) ? 1 : 0;
+        for (const FemSection& fs : hb.sections)
+            sec.push_back(FemSecDev{fs.E, fs.nu, fs.rho, fs.t, fs.damping, fs.drill, fs.yield, fs.yield > 0 ? plastic : 0}),
+                c->any_plastic |= fs.yield > 0 && plastic;
         for (int k = 0; k < nf; k++)
             for (int u = M.upd_ptr[k]; u < M.upd_ptr[k + 1]; u++) {
                 const auto& up = M.upd[u];
@@ -542,7 +595,8 @@ static int commit_fem(bl_gpu_ctx* c) {
     if ((rc = upload_vec(c, c->fnode, fnode)) || (rc = upload_vec(c, c->fbody, fbody)) || (rc = upload_vec(c, c->fperm, perm)) ||
         (rc = upload_vec(c, c->fiperm, iperm)) || (rc = upload_vec(c, c->xd, xd)) || (rc = upload_vec(c, c->fq, q)) || (rc = upload_vec(c, c->fw, w)) ||
         (rc = upload_vec(c, c->finertia, inertia)) || (rc = upload_vec(c, c->ftorque, zero4)) || (rc = upload_vec(c, c->tn, tn)) ||
-        (rc = upload_vec(c, c->tX, tX)) || (rc = upload_vec(c, c->tr0, tr0)) || (rc = upload_vec(c, c->tk, tk)) || (rc = upload_vec(c, c->tbroken, tbroken)) ||
+        (rc = upload_vec(c, c->tX, tX)) || (rc = upload_vec(c, c->tr0, tr0)) || (rc = upload_vec(c, c->tk, tk)) || (rc = upload_vec(c, c->tb, tb)) ||
+        (rc = upload_vec(c, c->tX0, tX0)) || (rc = upload_vec(c, c->th0, th0)) || (rc = upload_vec(c, c->tdmg, tdmg)) || (rc = upload_vec(c, c->tbroken, tbroken)) ||
         (rc = upload_vec(c, c->fsec, sec)) || (rc = upload_vec(c, c->fcol_ptr, col_ptr)) || (rc = upload_vec(c, c->frow, row)) ||
         (rc = upload_vec(c, c->gdiag_ptr, gdiag_ptr)) || (rc = upload_vec(c, c->gdiag, gdiag)) || (rc = upload_vec(c, c->goff_ptr, goff_ptr)) ||
         (rc = upload_vec(c, c->goff, goff)) || (rc = upload_vec(c, c->grp_tgt, grp_tgt)) || (rc = upload_vec(c, c->grp_ptr, grp_ptr)) ||
@@ -572,7 +626,8 @@ static int commit_fem(bl_gpu_ctx* c) {
     FemDev& F = c->fd;
     F.nf = NF, F.ntri = NT, F.nblk = NB;
     F.fnode = c->fnode.p, F.fbody = c->fbody.p, F.perm = c->fperm.p, F.iperm = c->fiperm.p, F.xd = c->xd.p, F.q = c->fq.p, F.w = c->fw.p;
-    F.inertia = c->finertia.p, F.torque = c->ftorque.p, F.tn = c->tn.p, F.tX = c->tX.p, F.tr0 = c->tr0.p, F.tk = c->tk.p, F.tbroken = c->tbroken.p;
+    F.inertia = c->finertia.p, F.torque = c->ftorque.p, F.tn = c->tn.p, F.tX = c->tX.p, F.tr0 = c->tr0.p, F.tk = c->tk.p,
+          F.tb = c->tb.p, F.tX0 = c->tX0.p, F.th0 = c->th0.p, F.tdmg = c->tdmg.p, F.tbroken = c->tbroken.p;
     F.tf = c->tf.p, F.tt = c->tt.p, F.ttan = c->ttan.p, F.tkv = c->tkv.p, F.ton = c->ton.p, F.sec = c->fsec.p, F.col_ptr = c->fcol_ptr.p, F.row = c->frow.p;
     F.blk_col = c->fblk_col.p;
     F.gdiag_ptr = c->gdiag_ptr.p, F.gdiag = c->gdiag.p, F.goff_ptr = c->goff_ptr.p, F.goff = c->goff.p, F.diag = c->diag.p, F.off = c->off.p;
@@ -810,10 +865,13 @@ static int commit_bodies(bl_gpu_ctx* c) {
         }
     }
     c->any_ext = false;
+    bool any_drag = false;
     for (int bi = 0; bi < B; bi++) {
         recs[bi].is_fem = c->bodies[bi].fem ? 1 : 0;
         recs[bi].has_ext = c->bodies[bi].ext.empty() ? 0 : 1;
         c->any_ext |= recs[bi].has_ext != 0;
+        any_drag |= recs[bi].drag != 0;
+        recs[bi].has_wheels = c->bodies[bi].wheels.empty() ? 0 : 1;
     }
     free_device(c);
     c->N = N, c->M = M, c->B = B;
@@ -839,6 +897,50 @@ static int commit_bodies(bl_gpu_ctx* c) {
         (rc = upload_vec(c, c->bbody, bbody)) || (rc = upload_vec(c, c->dbodies, recs)))
         return rc;
     BL_CUDA(c, c->fsc.alloc(M));
+    c->any_drag = any_drag;
+    if (any_drag) { // (the parts' scratch and means: k_drag_parts)
+        BL_CUDA(c, c->dup.alloc(N));
+        BL_CUDA(c, c->dpid.alloc(N));
+        BL_CUDA(c, c->dpart.alloc(N));
+        BL_CUDA(c, c->dpmv.alloc(N));
+        BL_CUDA(c, c->dpacc.alloc(N));
+    }
+    {   // the wheels: per wheel its hubs and its tyre nodes (ascending: the patch's sums run in node order), per node its
+        // wheel and the parity of its place in the wheel's list; every other tyre node of a body without a frame a wheel
+        // of its own with no hubs (a patch of one node: the same bits as its own stick test)
+        std::vector<int4> wh;
+        std::vector<int> wn;
+        std::vector<int2> nw;
+        for (int bi = 0; bi < B; bi++) {
+            const HostBody& hb = c->bodies[bi];
+            if (hb.fem) continue;
+            const int n0 = recs[bi].node0;
+            for (const HostBody::Wheel& w : hb.wheels) {
+                if (nw.empty()) nw.assign(N, make_int2(-1, 0));
+                const int first = (int)wn.size();
+                for (size_t j = 0; j < w.nodes.size(); j++) {
+                    wn.push_back(n0 + (int)w.nodes[j]);
+                    nw[n0 + w.nodes[j]] = make_int2((int)wh.size(), (int)(j & 1));
+                }
+                std::sort(wn.begin() + first, wn.end());
+                wh.push_back(make_int4(n0 + (int)w.axle0, n0 + (int)w.axle1, first, (int)w.nodes.size()));
+            }
+            for (int i = 0; i < recs[bi].nnodes; i++)
+                if ((hb.info[i].flags & BL_NF_TYRE) && (nw.empty() || nw[n0 + i].x < 0)) {
+                    if (nw.empty()) nw.assign(N, make_int2(-1, 0));
+                    nw[n0 + i] = make_int2((int)wh.size(), 0);
+                    wh.push_back(make_int4(-1, -1, (int)wn.size(), 1));
+                    wn.push_back(n0 + i);
+                }
+        }
+        c->NW = (int)wh.size();
+        if (c->NW > 0) {
+            if ((rc = upload_vec(c, c->dwheel, wh)) || (rc = upload_vec(c, c->dwnodes, wn)) || (rc = upload_vec(c, c->dnwheel, nw))) return rc;
+            BL_CUDA(c, c->dtcon.alloc(N));
+            BL_CUDA(c, c->dtfric.alloc(N));
+            BL_CUDA(c, cudaMemsetAsync(c->dtfric.p, 0, sizeof(float4) * N, c->stream));
+        }
+    }
     c->beam_grid = 0;
     if (c->cfg.beam_kernel == 0 && M > 0) {
         // k_beams_tma: a persistent grid of as many blocks as fit on the device at once (at most one a tile)
@@ -950,7 +1052,7 @@ static int ensure_committed(bl_gpu_ctx* c) {
 static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0; } // (s == 0 || s >= next_rebuild)
 
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
-    int64_t per = 3;
+    int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0);
     if (c->NF > 0) {
         per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
         if (c->cfg.fem_solver != BL_GPU_FEM_CHOLESKY) per += 1 - c->chol_launches; // (the Cholesky runs on a fallback only)
@@ -1051,6 +1153,8 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     if (c->contacts_on) k_islands<<<1, 1024, 0, s>>>(c->dbodies.p, c->B, frame_time, c->cfg.sleeping, CT, c->deverr.p);
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
     mark();
+    DragDev dg{c->dup.p, c->dpid.p, c->dpart.p, c->dpmv.p, c->dpacc.p};
+    WheelDev wh{c->dwheel.p, c->dwnodes.p, c->dnwheel.p, c->dtcon.p, c->dtfric.p, c->cfg.tyre_grip};
     NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p,
                 c->mon.p, c->mfa.p, c->mta.p, c->mtb.p};
     const FemDev& F = c->fd;
@@ -1063,6 +1167,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                 k_rebuild<<<c->B, 1024, sizeof(RebuildShared), s>>>(c->dbodies.p, c->B, c->nd.p, c->info.p, CT, k == 0 ? 1 : 0, c->deverr.p);
             }
         }
+        if (c->any_drag) k_drag_parts<<<(c->B + 63) / 64, 64, 0, s>>>(c->dbodies.p, c->B, c->nd.p, c->ab.p, c->bmeta.p, dg);
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
         if (c->beam_grid > 0) {
             k_beams_tma<<<c->beam_grid, kBeamThreads, kBeamSmem, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p,
@@ -1071,15 +1176,16 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
                                                    c->dbodies.p, c->M, c->B);
         }
-        if (c->NT > 0) k_tri_eval<<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
+        if (c->NT > 0 && c->any_plastic) k_tri_eval<true><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
+        else if (c->NT > 0) k_tri_eval<false><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         if (c->NM > 0) k_member_eval<<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
         if (c->packed_inc)
             k_force<true><<<std::max(gfn, 1), fb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc4.p, c->ell_base.p, c->fsc.p, c->dbodies.p,
-                                                         c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
+                                                         c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p, dg, wh);
         else
             k_force<false><<<std::max(gfn, 1), fb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, nullptr, c->fsc.p, c->dbodies.p,
-                                                          c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p);
+                                                          c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p, dg, wh);
         mark();
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
@@ -1087,7 +1193,8 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_collide<<<(c->B + 127) / 128, 128, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
         }
         mark();
-        k_integrate<<<std::max(gin, 1), ib, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p);
+        k_integrate<<<std::max(gin, 1), ib, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p, wh);
+        if (c->NW > 0) k_tyres<<<(c->NW + 7) / 8, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, dt, c->NW, k == 0 ? 1 : 0, c->nodef.p, wh);
         mark();
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
@@ -1179,7 +1286,6 @@ static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32
     sections.clear(), fsections.clear();
     for (int k = 0; k < (fd.n_tris > 0 ? fd.n_sections : 0); k++) {
         const bl_shell_section& ss = fd.sections[k];
-        if (ss.yield > 0) return BL_GPU_EUNSUPPORTED; // (plastic flow, folds and tears: not on this path)
         if (!(ss.t > 0) || !(ss.E > 0)) return BL_GPU_EINVAL;
         sections.push_back(FemSection{ss.E, ss.nu, ss.rho, ss.t, ss.yield, ss.damping, ss.drill});
     }
@@ -1232,12 +1338,13 @@ static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32
         if (!(M->tmass[t] > 0)) M->tmass[t] = sections[M->tsec[t]].rho * sections[M->tsec[t]].t * M->tarea0[t], again = true;
     if (again) fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data(), mpm); // (the inertias from those masses)
     fem_analyse(*M);
-    M->tk.assign(162 * M->tn.size(), 0.0f);
+    M->tk.assign(162 * M->tn.size(), 0.0f), M->tb.assign(54 * M->tn.size(), 0.0f);
     for (size_t t = 0; t < M->tn.size(); t++) {
         if (M->tbroken[t]) continue;
         float X[3][2];
         for (int i = 0; i < 3; i++) X[i][0] = M->tX[6 * t + 2 * i], X[i][1] = M->tX[6 * t + 2 * i + 1];
-        tri_stiffness_host(X, sections[M->tsec[t]], &M->tk[162 * t]);
+        const FemSection& fs = sections[M->tsec[t]];
+        tri_local_k(X, TriSec{fs.E, fs.nu, fs.t, fs.drill}, &M->tk[162 * t], &M->tb[54 * t]);
     }
     out = M;
     return BL_GPU_OK;
@@ -1270,6 +1377,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->force_block = 0;
     cfg->integrate_block = 0;
     cfg->beams_per_sm = 0;
+    cfg->tyre_grip = 1.0f;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -1298,7 +1406,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
         !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 1 ||
         !(c0.force_block == 0 || c0.force_block == 64 || c0.force_block == 128 || c0.force_block == 256) ||
         !(c0.integrate_block == 0 || c0.integrate_block == 64 || c0.integrate_block == 128 || c0.integrate_block == 256) ||
-        c0.beams_per_sm < 0 || c0.beams_per_sm > 16)
+        c0.beams_per_sm < 0 || c0.beams_per_sm > 16 || !(c0.tyre_grip >= 0))
         return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
@@ -1452,6 +1560,9 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
         for (int j = 0; j < d->n_beams; j++)
             if (on_frame[d->beams[j].a] || on_frame[d->beams[j].b]) return BL_GPU_EUNSUPPORTED;
     }
+    if (has_frame && d->allow_deform && d->allow_break)
+        for (int k = 0; d->fem->sections && k < d->fem->n_sections; k++)
+            if (d->fem->sections[k].yield > 0) return BL_GPU_EUNSUPPORTED; // (its tears and bisections: topology events)
     if (c->bodies.size() >= (size_t)(1 << 23)) return BL_GPU_ELIMIT;               // (a triangle keeps its body in 23 bits)
     HostBody hb;
     hb.nodes.assign(d->nodes, d->nodes + d->n_nodes);
@@ -1462,6 +1573,28 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
     std::memset(&r, 0, sizeof(r));
     r.crad = d->collision_radius, r.cfric = d->contact_friction, r.hull_depth = d->hull_depth, r.face_skin = d->face_skin;
     r.faces_only = d->faces_only ? 1 : 0, r.group = d->collision_group, r.island = -1;
+    if (!(d->air_drag >= 0) || !(d->aero_cda >= 0)) return BL_GPU_EINVAL;
+    r.air_drag = d->air_drag, r.aero_cda = d->aero_cda, r.drag = (d->air_drag > 0 || d->aero_cda > 0) ? 1 : 0;
+    if (r.drag && d->fem && (d->fem->n_tris > 0 || d->fem->n_members > 0)) return BL_GPU_EUNSUPPORTED; // (a frame's parts)
+    if (d->n_wheels < 0 || (d->n_wheels > 0 && !d->wheels)) return BL_GPU_EINVAL;
+    if (d->n_wheels > 0) {
+        if (has_frame) return BL_GPU_EUNSUPPORTED; // (tyre nodes of a frame body: its implicit step's)
+        std::vector<uint8_t> on_wheel(d->n_nodes, 0);
+        for (int k = 0; k < d->n_wheels; k++) {
+            const bl_wheel& w = d->wheels[k];
+            if (w.axle0 >= (uint32_t)d->n_nodes || w.axle1 >= (uint32_t)d->n_nodes || w.n_nodes < 0 || (w.n_nodes > 0 && !w.nodes)) return BL_GPU_EINVAL;
+            HostBody::Wheel hw{w.axle0, w.axle1, {}};
+            for (int j = 0; j < w.n_nodes; j++) {
+                // (a node on one wheel once: the reference adds a wheel's turn per place and shares a node's patch with its
+                // last wheel only)
+                if (w.nodes[j] >= (uint32_t)d->n_nodes) return BL_GPU_EINVAL;
+                if (on_wheel[w.nodes[j]]++) return BL_GPU_EUNSUPPORTED;
+                hw.nodes.push_back(w.nodes[j]);
+            }
+            if (!hw.nodes.empty()) hb.wheels.push_back(std::move(hw));
+        }
+        if (hb.wheels.size() > 32767) return BL_GPU_ELIMIT; // (SoftBody::node_wheel: 16-bit)
+    }
     for (const bl_tri& t : hb.tris) r.hull |= t.two_sided ? 0 : 1;
     for (int i = 0; i < d->n_nodes; i++) r.contacters |= (d->info[i].flags & BL_NF_CONTACTER) ? 1 : 0;
     r.fric = d->ground_friction;
@@ -1993,6 +2126,24 @@ int bl_gpu_download_fem(bl_gpu_ctx* c, int32_t body, int32_t* n, int32_t* node, 
             for (int i = 0; i < nf; i++) w[3 * i] = tmp[i].x, w[3 * i + 1] = tmp[i].y, w[3 * i + 2] = tmp[i].z;
         }
     }
+    return BL_GPU_OK;
+}
+
+int bl_gpu_download_fem_tris(bl_gpu_ctx* c, int32_t body, int32_t* n, float* rest, float* frames, float* plastic_stretch) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    if ((rc = ensure_committed(c))) return rc;
+    BL_CUDA(c, cudaDeviceSynchronize());
+    const HostBody& hb = c->bodies[body];
+    const int nt = hb.fem ? (int)hb.fem->tn.size() : 0;
+    if (n) *n = nt;
+    if (nt == 0) return BL_GPU_OK;
+    size_t to = 0;
+    for (int bi = 0; bi < body; bi++)
+        if (c->bodies[bi].fem) to += c->bodies[bi].fem->tn.size();
+    if (rest) BL_CUDA(c, cudaMemcpy(rest, c->tX.p + 6 * to, sizeof(float) * 6 * nt, cudaMemcpyDeviceToHost));
+    if (frames) BL_CUDA(c, cudaMemcpy(frames, c->tr0.p + 3 * to, sizeof(float4) * 3 * nt, cudaMemcpyDeviceToHost));
+    if (plastic_stretch) BL_CUDA(c, cudaMemcpy(plastic_stretch, c->tdmg.p + to, sizeof(float) * nt, cudaMemcpyDeviceToHost));
     return BL_GPU_OK;
 }
 

@@ -239,6 +239,141 @@ def truss_car(seed: int = 1, speed: float = 15.0, dims=(20, 4, 5)) -> dict:
     }
 
 
+def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: float = 0.2, gap: float = 0.1,
+               tyre_mass: float = 0.8, hub_mass: float = 5.0, k_tyre: float = 3e5, d_tyre: float = 300.0,
+               k_hub: float = 2e6, d_hub: float = 500.0, strength: float = 1e7) -> dict:
+    """Four free-rolling wheel rings on a lattice body (lattice_body / lattice_body_fast node order): each wheel two hub
+    nodes on an axle along z beside the lattice's bottom layer, a quarter of the length in from each end, `gap` m out
+    from the side, `width` m apart (axle0 the one of the lesser z, as the reference's vehicle builder spawns them), and
+    `rays` spokes of two tyre nodes (even: axle0's ring, odd: axle1's) at `radius` round the hubs - 24 tyre nodes a
+    wheel with the 12 rays. Beams: each tyre node to both hubs, each ray's pair, the two rings, one diagonal a ray;
+    each hub to the lattice's bottom nodes about its axle and the two hubs to each other. Tyre nodes: NF_GROUND |
+    NF_TYRE | NF_CONTACTER; they and the hubs move at the body's starting velocity. Appends the nodes and beams in
+    place, sets body["wheels"], returns the body."""
+    nx, ny, nz = dims
+    pos = body["pos"]
+    n0, m0 = len(pos), len(body["k"])
+    v0 = np.asarray(body["vel"][0], np.float32)
+    new_pos, new_mass, new_flags, ab, ks, ds = [], [], [], [], [], []
+
+    def node(p, m, flags):
+        new_pos.append(p), new_mass.append(m), new_flags.append(flags)
+        return n0 + len(new_pos) - 1
+
+    def beam(a, b, k, d):
+        ab.append((a, b)), ks.append(k), ds.append(d)
+
+    wheels, blocks = [], []
+    xs = sorted({max(0, (nx - 1) // 4), min(nx - 1, nx - 1 - (nx - 1) // 4)})
+    for ix in xs:
+        for side in (0, 1):
+            iz = 0 if side == 0 else nz - 1
+            base = pos[(ix * ny) * nz + iz]
+            zi = float(base[2]) + (-gap if side == 0 else gap)
+            zo = zi + (-width if side == 0 else width)
+            y = float(base[1])
+            x = float(base[0])
+            b_start, v_start, ln_max = len(ab), len(new_pos), 0
+            inner = node((x, y, zi), hub_mass, NF_GROUND | NF_CONTACTER)
+            outer = node((x, y, zo), hub_mass, NF_GROUND | NF_CONTACTER)
+            a0, a1 = (outer, inner) if side == 0 else (inner, outer)
+            beam(a0, a1, k_hub, d_hub)
+            for jx in range(max(0, ix - 1), min(nx, ix + 2)):
+                for jy in range(min(2, ny)):
+                    ln = (jx * ny + jy) * nz + iz
+                    ln_max = max(ln_max, ln)
+                    beam(ln, inner, k_hub, d_hub)
+                    beam(ln, outer, k_hub, d_hub)
+            tyre = []
+            for r in range(rays):
+                ang = 2.0 * math.pi * r / rays
+                dx, dy = radius * math.cos(ang), radius * math.sin(ang)
+                e = node((x + dx, y + dy, float(new_pos[a0 - n0][2])), tyre_mass, NF_GROUND | NF_TYRE | NF_CONTACTER)
+                o = node((x + dx, y + dy, float(new_pos[a1 - n0][2])), tyre_mass, NF_GROUND | NF_TYRE | NF_CONTACTER)
+                tyre += [e, o]
+            for r in range(rays):
+                e, o = tyre[2 * r], tyre[2 * r + 1]
+                e2, o2 = tyre[(2 * r + 2) % (2 * rays)], tyre[(2 * r + 3) % (2 * rays)]
+                for t in (e, o):
+                    beam(t, a0, k_tyre, d_tyre)
+                    beam(t, a1, k_tyre, d_tyre)
+                beam(e, o, k_tyre, d_tyre)
+                beam(e, e2, k_tyre, d_tyre)
+                beam(o, o2, k_tyre, d_tyre)
+                beam(e, o2, k_tyre, d_tyre)
+            wheels.append({"axle0": a0, "axle1": a1, "nodes": np.asarray(tyre, np.uint32), "radius": radius,
+                           "width": width, "mass": float(np.float32(tyre_mass) * np.float32(len(tyre)))})
+            blocks.append((ln_max, v_start, len(new_pos), b_start, len(ab)))
+    k = len(new_pos)
+    body["pos"] = np.concatenate([pos, np.asarray(new_pos, np.float32)]).astype(np.float32)
+    body["vel"] = np.concatenate([body["vel"], np.tile(v0, (k, 1))]).astype(np.float32)
+    body["mass"] = np.concatenate([body["mass"], np.asarray(new_mass, np.float32)])
+    body["node_flags"] = np.concatenate([body["node_flags"], np.asarray(new_flags, np.uint16)])
+    body["friction"] = np.concatenate([body["friction"], np.ones(k, np.float32)])
+    body["radius"] = np.concatenate([body["radius"], np.zeros(k, np.float32)])
+    m = len(ab)
+    body["ab"] = np.concatenate([body["ab"], np.asarray(ab, np.uint32).reshape(m, 2)])
+    body["k"] = np.concatenate([body["k"], np.asarray(ks, np.float32)])
+    body["d"] = np.concatenate([body["d"], np.asarray(ds, np.float32)])
+    body["strength"] = np.concatenate([body["strength"], np.full(m, strength, np.float32)])
+    body["deform"] = np.concatenate([body["deform"], np.full(m, strength, np.float32)])
+    body["beam_type"] = np.concatenate([body["beam_type"], np.zeros(m, np.uint8)])
+    body["beam_flags"] = np.concatenate([body["beam_flags"], np.zeros(m, np.uint8)])
+    body["wheels"] = wheels
+    assert len(body["k"]) == m0 + m
+    if np.all(np.diff(body["ab"][:m0, 0].astype(np.int64)) >= 0):
+        # each wheel's nodes right after the last lattice node its hubs hold, its beams right after that node's beams:
+        # every 32 consecutive nodes' beams and neighbours then lie within a few lattice slices of each other (the
+        # kernels' 4-byte incidences), as a builder numbering the wheels with the axles they hang on would
+        order, border = [], []
+        lat_ab = body["ab"][:m0, 0].astype(np.int64)
+        nxt, bnxt = 0, 0
+        for ln_max, v0_, v1_, b0_, b1_ in sorted(blocks, key=lambda t: t[0]):
+            order += list(range(nxt, ln_max + 1)) + list(range(n0 + v0_, n0 + v1_))
+            nxt = ln_max + 1
+            cut = int(np.searchsorted(lat_ab, ln_max, side="right"))
+            border += list(range(bnxt, cut)) + list(range(m0 + b0_, m0 + b1_))
+            bnxt = cut
+        order += list(range(nxt, n0))
+        border += list(range(bnxt, m0))
+        order, border = np.asarray(order), np.asarray(border)
+        assert len(order) == n0 + k and len(border) == m0 + m
+        perm = np.empty_like(order)
+        perm[order] = np.arange(len(order))
+        for key in ("pos", "vel", "mass", "node_flags", "friction", "radius"):
+            body[key] = np.ascontiguousarray(body[key][order])
+        for key in ("ab", "k", "d", "strength", "deform", "beam_type", "beam_flags"):
+            body[key] = np.ascontiguousarray(body[key][border])
+        body["ab"] = perm[body["ab"]].astype(np.uint32)
+        if "tris" in body:
+            body["tris"] = perm[np.asarray(body["tris"], np.int64)].astype(np.uint32)
+        for w in wheels:
+            w["axle0"], w["axle1"] = int(perm[w["axle0"]]), int(perm[w["axle1"]])
+            w["nodes"] = perm[w["nodes"].astype(np.int64)].astype(np.uint32)
+    return body
+
+
+def wheeled_car(seed: int = 1, speed: float = 12.0, yaw: float = 0.3, dims=(14, 3, 5), wall: bool = True,
+                height: float = 0.45) -> dict:
+    """A lattice truss on four wheel rings (add_wheels), `height` m up over flat grass, rolling at `speed` m/s at
+    `yaw` rad off +x (so its tyres slip sideways as they land) towards a concrete wall; dt = 0.5 ms."""
+    rng = TRng(seed)
+    vel = (speed * math.cos(yaw), 0.0, speed * math.sin(yaw))
+    body = lattice_body(rng, dims=dims, origin=(-6.0, height, -0.5), velocity=vel, ground_friction=0.8 / GRASS_STATIC_FRICTION)
+    add_wheels(body, dims)
+    front = -6.0 + (dims[0] - 1) * 0.25
+    boxes = []
+    if wall:
+        boxes.append({"center": (front + 4.0 + 0.25, 1.0, 0.0), "half": (0.25, 1.0, 3.0), "rot": (0.0, 0.0, 0.0, 1.0),
+                      "surface": SURF_CONCRETE})
+    return {
+        "settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005},
+        "statics": {"terrain": flat_terrain(), "boxes": boxes, "build_grid": True},
+        "bodies": [body],
+        "name": f"wheeled_car(seed={seed}, speed={speed}, yaw={yaw})",
+    }
+
+
 def rig_counts(rig: dict) -> tuple[int, int]:
     """(nodes, beams) over the rig's bodies."""
     return (sum(len(b["mass"]) for b in rig["bodies"]), sum(len(b["k"]) for b in rig["bodies"]))
@@ -313,12 +448,12 @@ def stress_rig(seed: int = 7) -> dict:
 
 def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, sigma: float = 0.6,
           min_nodes: int = 500, max_nodes: int = 20000, terrain_size: float = 1000.0, terrain_samples: int = 2048,
-          amplitude: float = 2.0, skins: bool = True) -> dict:
+          amplitude: float = 2.0, skins: bool = True, wheels: bool = True) -> dict:
     """A batched fleet of lattice trusses with log-normal node counts (median `median_nodes`, clipped to
     [min_nodes, max_nodes]), each driving at a speed uniform in [5, 30] m/s with a random yaw over a square heightfield
     of terrain_samples^2 samples spanning terrain_size metres, `amplitude` m of seeded smooth noise. Vehicles start on
-    a grid 40 m apart; with skins (lattice_tris) those that meet collide. Random draws: numpy's PCG64 seeded with
-    `seed` (the skins draw none)."""
+    a grid 40 m apart; with skins (lattice_tris) those that meet collide; with wheels each stands on four wheel rings
+    of 24 tyre nodes (add_wheels). Random draws: numpy's PCG64 seeded with `seed` (the skins and wheels draw none)."""
     gen = np.random.default_rng(seed)
     cell = terrain_size / (terrain_samples - 1)
     half = terrain_size / 2
@@ -352,6 +487,8 @@ def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, si
                                  velocity=(speed * math.cos(yaw), 0.0, speed * math.sin(yaw)))
         if skins:
             body["tris"] = lattice_tris((nx, ny, nz))
+        if wheels:
+            add_wheels(body, (nx, ny, nz))
         bodies.append(body)
     return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005},
             "statics": {"terrain": terrain, "boxes": [], "build_grid": True}, "bodies": bodies,
@@ -360,12 +497,13 @@ def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, si
 
 def shell_plate(n: int = 63, size: float = 1.0, origin=(0.0, 1.0, 0.0), thickness: float = 0.0015, E: float = 210e9,
                 nu: float = 0.3, rho: float = 7850.0, damping: float = 3e-4, drill: float = 0.05, clamp_edge: bool = True,
-                load: float = 500.0, seed: int = 1, node_flags: int = 0) -> dict:
+                load: float = 500.0, seed: int = 1, node_flags: int = 0, yield_stress: float = 0.0) -> dict:
     """The co-rotational FEM shell plate: (n + 1)^2 nodes on a size x size square in the horizontal plane at `origin`,
     2 n^2 CST/DKT triangles (two a cell, diagonals alternating: ShellMesher::grid, fem_shell.cpp:34-50), an elastic
     steel section (E, nu, rho, thickness), each triangle's mass a third on each corner; the edge z = origin.z clamped
     (anchored nodes); a seeded random point load of `load` N on a uniformly drawn free node; gravity. The default is
-    the 64 x 64-node, 7,938-triangle plate of 1.5 mm steel."""
+    the 64 x 64-node, 7,938-triangle plate of 1.5 mm steel. yield_stress > 0: a yielding section (the plate flows and
+    folds; it does not tear: allow_break off)."""
     ox, oy, oz = (np.float32(v) for v in origin)
     du = np.float32(size / n)
     pos = np.zeros(((n + 1) * (n + 1), 3), np.float32)
@@ -416,9 +554,10 @@ def shell_plate(n: int = 63, size: float = 1.0, origin=(0.0, 1.0, 0.0), thicknes
         "strength": np.zeros(0, np.float32), "deform": np.zeros(0, np.float32), "beam_type": np.zeros(0, np.uint8),
         "beam_flags": np.zeros(0, np.uint8),
         "params": {"ground_friction": 1.0, "bounce": -1.0, "contact_push_max": 2.0, "contact_slop": 0.0,
-                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 1, "ductile": 0, "can_sleep": 0,
-                   "sleep_speed": 0.0},
-        "fem_sections": [{"E": E, "nu": nu, "rho": rho, "t": thickness, "yield": 0.0, "damping": damping, "drill": drill}],
+                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 0 if yield_stress > 0 else 1, "ductile": 0,
+                   "can_sleep": 0, "sleep_speed": 0.0},
+        "fem_sections": [{"E": E, "nu": nu, "rho": rho, "t": thickness, "yield": float(yield_stress), "damping": damping,
+                          "drill": drill}],
         "fem_tris": np.asarray(tris, np.uint32), "fem_tri_mass": np.asarray(tmass, np.float32),
         "loads": [(node, tuple(float(x) for x in f))],
         "plate": {"n": n, "size": size, "origin": tuple(float(v) for v in origin)},

@@ -74,6 +74,7 @@ class WorldSettings:
     beam_kernel: int = 0
     # the FEM factorization's top chain as one dense front (True) or block column by block column (False)
     fem_dense_front: bool = True
+    tyre_grip: float = 1.0                    # WorldSettings::tyre_grip: a factor on the tyres' friction
     # launch shapes (None: the tuned ones of beamlab_b200/tuned.json when present, else the library's defaults);
     # results do not depend on them
     force_block: int | None = None
@@ -142,6 +143,9 @@ class SoftBody:
         self.faces_only = False
         self.collision_group = 0
         self.self_collision = False
+        self.air_drag = 0.0                           # SoftBody::air_drag (RoR's per-node drag, against the part's mean)
+        self.aero_cda = 0.0                           # SoftBody::aero_cda (Cd A on the parts' mean velocities)
+        self.wheels: list[dict] = []                  # Wheel: axle0, axle1, nodes (even: axle0's ring), radius, width, mass
         self._tris: list = []
         self.tris = np.zeros(0, TRI_DTYPE)
         self.nodes = np.zeros(0, NODE_DTYPE)
@@ -230,6 +234,8 @@ class SoftBody:
             fm["mass"] = np.asarray(body.get("member_mass", np.zeros(len(mab))), np.float32)
             sb.fem_members = fm
             sb.fem_tris_first = bool(body.get("fem_tris_first", False))
+        if "wheels" in body:
+            sb.wheels = [dict(w) for w in body["wheels"]]
         if "tris" in body and len(body["tris"]):
             tri = np.asarray(body["tris"], np.uint32).reshape(-1, 3)
             tr = np.zeros(len(tri), TRI_DTYPE)
@@ -319,7 +325,13 @@ class _BodyDesc(C.Structure):
                 ("fem", C.POINTER(_FemDesc)), ("n_tris", C.c_int32), ("tris", C.c_void_p),
                 ("collision_radius", C.c_float), ("contact_friction", C.c_float), ("hull_depth", C.c_float),
                 ("face_skin", C.c_float), ("faces_only", C.c_int32), ("collision_group", C.c_int32),
-                ("self_collision", C.c_int32)]
+                ("self_collision", C.c_int32), ("air_drag", C.c_float), ("aero_cda", C.c_float),
+                ("n_wheels", C.c_int32), ("wheels", C.c_void_p)]
+
+
+class _Wheel(C.Structure):
+    _fields_ = [("axle0", C.c_uint32), ("axle1", C.c_uint32), ("n_nodes", C.c_int32), ("nodes", C.c_void_p),
+                ("radius", C.c_float), ("width", C.c_float), ("mass", C.c_float)]
 
 
 class _BodyState(C.Structure):
@@ -349,7 +361,7 @@ class _Config(C.Structure):
                 ("fem_solver", C.c_int32), ("pcg_max_iters", C.c_int32), ("pcg_tol", C.c_float),
                 ("fem_check_residual", C.c_int32), ("pcg_learned_scale", C.c_int32), ("graphs", C.c_int32),
                 ("beam_kernel", C.c_int32), ("fem_dense_front", C.c_int32), ("force_block", C.c_int32),
-                ("integrate_block", C.c_int32), ("beams_per_sm", C.c_int32)]
+                ("integrate_block", C.c_int32), ("beams_per_sm", C.c_int32), ("tyre_grip", C.c_float)]
 
 
 class _FemStats(C.Structure):
@@ -423,6 +435,20 @@ class BodyHandle:
                                      w.ctypes.data), "download_fem", ctx)
         return {"node": node, "xd": xd, "q": q, "w": w}
 
+    def fem_tris(self) -> dict | None:
+        """The FEM triangles' plastic state: rest shapes (6 each), rest frames (x y z w per corner), plastic stretch."""
+        L, ctx = self.world._L, self.world._ctx
+        n = C.c_int32()
+        _check(L.bl_gpu_download_fem_tris(ctx, self.index, C.byref(n), None, None, None), "download_fem_tris", ctx)
+        if n.value == 0:
+            return None
+        X = np.zeros((n.value, 6), np.float32)
+        r0 = np.zeros((n.value, 12), np.float32)
+        dmg = np.zeros(n.value, np.float32)
+        _check(L.bl_gpu_download_fem_tris(ctx, self.index, C.byref(n), X.ctypes.data, r0.ctypes.data, dmg.ctypes.data),
+               "download_fem_tris", ctx)
+        return {"X": X, "r0": r0, "dmg": dmg}
+
     def set_node_force(self, node: int, force):
         """A constant force on one node, every substep after gravity (a SoftBody::pre_substep push)."""
         f = (C.c_float * 3)(*[float(x) for x in force])
@@ -455,6 +481,7 @@ class World:
         cfg.graphs = int(self.settings.graphs)
         cfg.beam_kernel = int(self.settings.beam_kernel)
         cfg.fem_dense_front = int(self.settings.fem_dense_front)
+        cfg.tyre_grip = float(self.settings.tyre_grip)
         tuned = _tuned_shapes()
         for k in ("force_block", "integrate_block", "beams_per_sm"):
             v = getattr(self.settings, k)
@@ -544,6 +571,17 @@ class World:
         d.collision_radius, d.contact_friction = float(body.collision_radius), float(body.contact_friction)
         d.hull_depth, d.face_skin, d.faces_only = float(body.hull_depth), float(body.face_skin), int(body.faces_only)
         d.collision_group, d.self_collision = int(body.collision_group), int(body.self_collision)
+        d.air_drag, d.aero_cda = float(body.air_drag), float(body.aero_cda)
+        if body.wheels:
+            wl = []
+            for wh in body.wheels:
+                wn = np.ascontiguousarray(wh["nodes"], np.uint32)
+                self._keep.append(wn)
+                wl.append(_Wheel(int(wh["axle0"]), int(wh["axle1"]), len(wn), wn.ctypes.data, float(wh.get("radius", 0.4)),
+                                 float(wh.get("width", 0.2)), float(wh.get("mass", 0.0))))
+            wa = (_Wheel * len(wl))(*wl)
+            self._keep.append(wa)
+            d.n_wheels, d.wheels = len(wl), C.cast(wa, C.c_void_p)
         idx = C.c_int32()
         _check(self._L.bl_gpu_add_body(self._ctx, C.byref(d), C.byref(idx)), "add_body", self._ctx)
         h = BodyHandle(self, idx.value, len(nodes), len(beams), body.name)

@@ -4,8 +4,9 @@
 
 A step is one 60 Hz frame of 33 substeps (World::step_substeps(33)) over the whole workload. The default workload is
 the batched fleet: 256 seeded lattice vehicles of log-normal size (500-20,000 nodes, median 3,000; about 0.9 M nodes
-and 8.5 M beams) with collision skins, driving over a 2048^2-sample, 1 km^2 heightfield with contacts between the
-vehicles that meet - the fleet configuration's shape without its wheel rings. Under torchrun each rank steps its
+and 8.6 M beams) on four free-rolling wheel rings of 24 tyre nodes each, with collision skins, driving over a
+2048^2-sample, 1 km^2 heightfield with contacts between the vehicles that meet - the fleet configuration's shape.
+Under torchrun each rank steps its
 own fleet (weak scaling, no data-path collective: vehicles that do not touch are independent islands).
 
 Rank 0 prints one JSON line: value = node-substeps/s of all ranks with the state resident in HBM (CUDA events on the
@@ -50,7 +51,8 @@ def workload(name: str, rank: int):
         nt = sum(len(b.get("tris", ())) for b in rig["bodies"])
         desc = (f"fleet256: 256 lattice vehicles ({n:,} nodes, {m:,} beams, {nt:,} collision triangles; log-normal "
                 f"500-20,000 nodes, median 3,000), 2048^2-sample 1 km^2 heightfield, 5-30 m/s random yaw, "
-                f"inter-vehicle node-triangle contacts (islands, pair search every 17 substeps); no wheel rings")
+                f"inter-vehicle node-triangle contacts (islands, pair search every 17 substeps); 4 wheel rings of 24 "
+                f"tyre nodes a vehicle (free rolling, tyre patches sharing grip)")
     elif name == "plate64":
         rig = rigs.shell_plate(63, seed=1 + rank)
         n, m = rigs.rig_counts(rig)

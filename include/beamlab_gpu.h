@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define BL_GPU_ABI_VERSION 3
+#define BL_GPU_ABI_VERSION 4
 
 enum {
     BL_GPU_OK = 0,
@@ -92,6 +92,7 @@ typedef struct {
     int32_t force_block;       /* the nodes' force kernel's block size: 64, 128 or 256; 0 (default): 256 */
     int32_t integrate_block;   /* the integration kernel's block size: 64, 128 or 256; 0 (default): 256 */
     int32_t beams_per_sm;      /* the beams' persistent kernel's blocks an SM (at most what fits); 0 (default): what fits */
+    float tyre_grip;           /* WorldSettings::tyre_grip (1): a factor on the tyres' friction (tyre_contact) */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };
@@ -124,10 +125,12 @@ typedef struct {
     uint16_t group;
 } bl_beam;
 
-/* == the fields of bl::phys::ShellSection (frame_fem.h:114-150) the elastic shell step reads */
+/* == the fields of bl::phys::ShellSection (frame_fem.h:114-150) the shell step reads */
 typedef struct {
     float E, nu, rho, t;       /* Young's modulus (Pa), Poisson's ratio, density (kg/m3), thickness (m) */
-    float yield;               /* yield stress (Pa): 0 only (elastic); a yielding section is BL_GPU_EUNSUPPORTED */
+    float yield;               /* yield stress (Pa; 0: elastic): on a body with allow_deform its triangles flow
+                                  (membrane and bending, eval_tris); with allow_break too BL_GPU_EUNSUPPORTED (its
+                                  tears and bisections are topology events this path does not make) */
     float damping;             /* stiffness-proportional damping (s) */
     float drill;               /* the corners' drilling spring, a share of G t A */
 } bl_shell_section;
@@ -196,10 +199,25 @@ typedef struct {
     int32_t tris_first;        /* 1: the add_tri calls came before the add_element calls */
 } bl_fem_desc;
 
+/* A wheel of tyre nodes (Wheel, softbody.h:468-498): its hub (axle0 on the side of the even tyre nodes, axle1) and its
+ * tyre contact nodes (even: the ring on axle0's side, odd: the other), as the reference's vehicle builder makes them;
+ * free rolling (no drive torque, no brake, no arm). A ring tyre (Wheel::ring) is not on this path. A node lies on one
+ * wheel once (else BL_GPU_EUNSUPPORTED). radius, width and mass are the vehicle builder's record: a free wheel's
+ * forces (compute_wheel_forces with no torque, the tyre patch) do not read them. */
+typedef struct bl_wheel {
+    uint32_t axle0, axle1;
+    int32_t n_nodes;
+    const uint32_t* nodes;
+    float radius, width;
+    float mass;                /* its tyre nodes' mass */
+} bl_wheel;
+
 /* One body: a SoftBody after finalize (softbody.cpp:76-83) - its arrays and the knobs of the explicit path
- * (softbody.h:650-700), and optionally its FEM frame of triangle elements. Bodies with shocks, joints, wheels, slide
- * nodes, sheets, FEM members or mounts, air drag or grab are rejected with BL_GPU_EUNSUPPORTED by the caller's shim
- * (this record has no fields for them); so is a FEM frame whose nodes collide with the static world (NF_GROUND). */
+ * (softbody.h:650-700), its free-rolling node wheels, and optionally its FEM frame of members and triangle elements.
+ * Bodies with shocks, joints, ring tyres, driven or braked wheels, slide nodes, sheets, FEM mounts or grab are
+ * rejected by the caller's shim (this record has no fields for them); BL_GPU_EUNSUPPORTED here: a FEM frame whose
+ * nodes collide with the static world (NF_GROUND), beams on frame nodes, yielding sections on a body that breaks, a frame with collision
+ * triangles, air drag or wheels, self collision, a node on two wheels. */
 typedef struct {
     int32_t n_nodes;
     const bl_node* nodes;
@@ -228,6 +246,11 @@ typedef struct {
     int32_t faces_only;        /* SoftBody::faces_only */
     int32_t collision_group;   /* SoftBody::collision_group (0: none) */
     int32_t self_collision;    /* SoftBody::self_collision: not supported (BL_GPU_EUNSUPPORTED when set) */
+    float air_drag;            /* SoftBody::air_drag (0: none): RoR's per-node drag on the velocity against its part's
+                                  mean (softbody.cpp:334-378); a body with a FEM frame takes none */
+    float aero_cda;            /* SoftBody::aero_cda (0: none): Cd A (m2) on each part's mean velocity, shared by mass */
+    int32_t n_wheels;          /* SoftBody::wheels of node tyres (Wheel, softbody.h:468-498), free rolling: no drive */
+    const struct bl_wheel* wheels; /* torque or brake; their tyre nodes (NF_TYRE) share each patch's grip */
 } bl_body_desc;
 
 /* A body's runtime state (SoftBody::aabb, max_speed, sleeping, static_contacts, stats.broken_beams, sleep_timer) */
@@ -303,6 +326,11 @@ int bl_gpu_set_node_force(bl_gpu_ctx* ctx, int32_t body, int32_t node, const flo
 /* A body's FEM frame nodes (FemFrame::node / xd / q / w, frame_fem.h:331-350): body node, double position (3),
  * orientation (x y z w), angular velocity (3); n the frame node count (0: none). Any pointer may be NULL. */
 int bl_gpu_download_fem(bl_gpu_ctx* ctx, int32_t body, int32_t* n, int32_t* node, double* xd, float* q, float* w);
+
+/* A body's FEM triangles' plastic state (FrameTri::X, r0, dmg, frame_fem.h:153-181): the rest shape (6: the corners in
+ * the element's plane, as a yielding membrane flowed it), the rest frames (12: x y z w per corner, the bending's
+ * plastic rotations baked in), the plastic stretch reached; n the triangle count (0: none). Any pointer may be NULL. */
+int bl_gpu_download_fem_tris(bl_gpu_ctx* ctx, int32_t body, int32_t* n, float* rest, float* frames, float* plastic_stretch);
 
 /* World::step_substeps(n) (world.cpp:368-585): one frame of n substeps of every awake body, enqueued on `stream`
  * (a cudaStream_t; NULL: the context's own). Asynchronous. */

@@ -90,6 +90,11 @@ def _load(path: str, prefix: str) -> C.CDLL:
         lib.ref_add_plate.argtypes = [vp, i] + [f] * 9 + [f] * 7 + [i, i]
         lib.ref_add_plate.restype = i
         lib.ref_set_point_load.argtypes = [vp, i, i, f, f, f]
+        lib.ref_set_drag.argtypes = [vp, i, f, f]
+        lib.ref_add_wheel.argtypes = [vp, i, C.c_uint32, C.c_uint32, u32p, i, f, f, f]
+        lib.ref_set_tyre_grip.argtypes = [vp, f]
+        lib.ref_set_body_flags.argtypes = [vp, i, i, i]
+        lib.ref_fem_tri_dmg.argtypes = [vp, i, vp]
         lib.ref_add_fem_body.argtypes = [vp, i, fp, fp, fp, u16p, i, fp, i, u32p, u16p, fp, i, fp, i, u32p, u16p, u8p, fp, i]
         lib.ref_add_fem_body.restype = i
         lib.ref_fem_info.argtypes = [vp, i, C.POINTER(C.c_longlong)]
@@ -126,9 +131,13 @@ class _OracleWorld:
             pass
 
     def settings(self, gravity=(0.0, -9.81, 0.0), dt=0.0005, sleeping=True, multithreaded=True, inter_body=True,
-                 sleep_speed=0.06, sleep_time=1.0):
+                 sleep_speed=0.06, sleep_time=1.0, tyre_grip=1.0):
         self._fn("world_settings")(self._w, *map(float, gravity), float(dt), int(sleeping), int(multithreaded),
                                    int(inter_body), float(sleep_speed), float(sleep_time))
+        if self.prefix == "ref":
+            self._lib.ref_set_tyre_grip(self._w, float(tyre_grip))
+        elif float(tyre_grip) != 1.0:
+            raise ValueError("tyre grip other than 1 steps in the reference only (RefWorld)")
 
     def load_statics(self, statics: dict):
         t = statics.get("terrain")
@@ -166,6 +175,18 @@ class _OracleWorld:
             len(a["k"]), _ptr(a["ab"], C.c_uint32), _ptr(a["k"], C.c_float), _ptr(a["d"], C.c_float),
             _ptr(a["strength"], C.c_float), _ptr(a["deform"], C.c_float), _ptr(a["beam_type"], C.c_uint8),
             _ptr(a["beam_flags"], C.c_uint8), len(tris), _ptr(tris, C.c_uint32), C.byref(prm))
+        p = body.get("params", {})
+        if float(p.get("air_drag", 0.0)) > 0 or float(p.get("aero_cda", 0.0)) > 0:
+            if self.prefix != "ref":
+                raise ValueError("air drag steps in the reference only (RefWorld)")
+            self._lib.ref_set_drag(self._w, idx, float(p.get("air_drag", 0.0)), float(p.get("aero_cda", 0.0)))
+        for wh in body.get("wheels", ()):
+            if self.prefix != "ref":
+                raise ValueError("wheels step in the reference only (RefWorld)")
+            wn = np.ascontiguousarray(wh["nodes"], dtype=np.uint32)
+            self._keep.append(wn)
+            self._lib.ref_add_wheel(self._w, idx, int(wh["axle0"]), int(wh["axle1"]), _ptr(wn, C.c_uint32), len(wn),
+                                    float(wh.get("radius", 0.4)), float(wh.get("width", 0.2)), float(wh.get("mass", 0.0)))
         if self.prefix == "ref" and len(tris) and "tri_two_sided" in body:
             sides = np.ascontiguousarray(body["tri_two_sided"], dtype=np.uint8)
             self._keep.append(sides)
@@ -220,9 +241,14 @@ class _FemMixin:
         b = self._lib.ref_add_plate(self._w, n, *map(float, o), du, 0.0, 0.0, 0.0, 0.0, du, float(sec["E"]), float(sec["nu"]),
                                     float(sec["rho"]), float(sec["t"]), float(sec.get("yield", 0.0)), float(sec.get("damping", 3e-4)),
                                     float(sec.get("drill", 0.05)), 1 if (body["node_flags"][0] & 2) else 0, int(body["node_flags"][-1]))
+        self._body_flags(b, body)
         for node, fv in body.get("loads", []):
             self._lib.ref_set_point_load(self._w, b, int(node), *map(float, fv))
         return b
+
+    def _body_flags(self, b: int, body: dict):
+        p = body.get("params", {})
+        self._lib.ref_set_body_flags(self._w, b, int(p.get("allow_deform", 1)), int(p.get("allow_break", 1)))
 
     def add_fem_body(self, body: dict) -> int:
         """A body with a FEM frame of members and triangles from its arrays (FemFrame::add_section /
@@ -253,6 +279,7 @@ class _FemMixin:
                                        _ptr(tmass, C.c_float), len(fs), _ptr(fs, C.c_float), m, _ptr(ab, C.c_uint32),
                                        _ptr(msec, C.c_uint16), _ptr(ends, C.c_uint8), _ptr(mm, C.c_float),
                                        int(body.get("fem_tris_first", False)))
+        self._body_flags(b, body)
         for node, fv in body.get("loads", []):
             self._lib.ref_set_point_load(self._w, b, int(node), *map(float, fv))
         return b
@@ -282,6 +309,8 @@ class _FemMixin:
         out = {"n": np.zeros((t, 3), np.int32), "X": np.zeros((t, 6), np.float32), "r0": np.zeros((t, 12), np.float32),
                "mass": np.zeros(t, np.float32), "area0": np.zeros(t, np.float32)}
         self._lib.ref_fem_tris(self._w, body, *(out[k].ctypes.data for k in ("n", "X", "r0", "mass", "area0")))
+        out["dmg"] = np.zeros(t, np.float32)
+        self._lib.ref_fem_tri_dmg(self._w, body, out["dmg"].ctypes.data)
         return out
 
 

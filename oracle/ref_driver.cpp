@@ -82,6 +82,9 @@ void ref_world_settings(RefWorld* r, float gx, float gy, float gz, float dt, int
     s.sleep_time = sleep_time;
 }
 
+// WorldSettings::tyre_grip (world.h:55): the factor on the tyres' friction
+void ref_set_tyre_grip(RefWorld* r, float g) { r->w.settings.tyre_grip = g; }
+
 // heights / surfaces: nz rows of nx samples, x fastest
 void ref_set_terrain(RefWorld* r, int nx, int nz, float cell, float ox, float oz, const float* heights, const uint8_t* surfaces) {
     StaticWorld& st = r->w.statics;
@@ -237,6 +240,28 @@ int ref_add_fem_body(RefWorld* r, int n_nodes, const float* pos, const float* ve
     return (int)r->bodies.size() - 1;
 }
 
+// SoftBody::air_drag and aero_cda of a body (RoR's per-node drag against its part's mean velocity, and Cd A)
+void ref_set_drag(RefWorld* r, int body, float air_drag, float aero_cda) {
+    r->bodies[body]->air_drag = air_drag;
+    r->bodies[body]->aero_cda = aero_cda;
+}
+
+// SoftBody::allow_deform and allow_break of a body (softbody.h:711-712)
+void ref_set_body_flags(RefWorld* r, int body, int allow_deform, int allow_break) {
+    r->bodies[body]->allow_deform = allow_deform != 0;
+    r->bodies[body]->allow_break = allow_break != 0;
+}
+
+// A free-rolling wheel of tyre nodes on a body (Wheel, softbody.h:468-498): its hubs, its tyre nodes (even: axle0's
+// side), radius, width and mass, as the vehicle builder fills them; no torque, no brake, no arm
+void ref_add_wheel(RefWorld* r, int body, uint32_t axle0, uint32_t axle1, const uint32_t* nodes, int n, float radius, float width, float mass) {
+    Wheel w;
+    w.axle0 = axle0, w.axle1 = axle1;
+    w.nodes.assign(nodes, nodes + n);
+    w.radius = radius, w.width = width, w.mass = mass;
+    r->bodies[body]->wheels.push_back(w);
+}
+
 // A constant force on one node of a body, applied every substep right after gravity (the SoftBody::pre_substep hook,
 // world.cpp:3261)
 void ref_set_point_load(RefWorld* r, int body, int node, float fx, float fy, float fz) {
@@ -290,6 +315,12 @@ void ref_fem_tris(RefWorld* r, int body, int* n, float* X, float* r0, float* mas
         }
         mass[t] = tr.mass, area0[t] = tr.area0;
     }
+}
+
+// FrameTri::dmg of each triangle (the plastic stretch reached)
+void ref_fem_tri_dmg(RefWorld* r, int body, float* dmg) {
+    const FemFrame& f = r->bodies[body]->fem;
+    for (size_t t = 0; t < f.tris.size(); t++) dmg[t] = f.tris[t].dmg;
 }
 
 int ref_body_nodes(RefWorld* r, int body) { return (int)r->bodies[body]->nodes.size(); }

@@ -97,3 +97,40 @@ def test_gpu_shell_body_matches_reference(ref_lib):
     assert np.abs(p - p0).max() > 1e-3  # (it moves)
     assert h.state()["fem_failures"] == 0 and ref.fem_info(0)["solve_failures"] == 0
     w.close()
+
+
+def test_gpu_yielding_plate_matches_reference(ref_lib):
+    """A plate of a yielding section (250 MPa) under a 3 kN point load, on a body that deforms and does not break:
+    its membrane flows (the rest shapes follow the stretch, the elements built again) and its bending yields (the
+    corners' rest frames turn) in the reference's eval_tris (frame_fem.cpp:1690-1741); on the GPU the same triangles
+    flow, the nodes, rest shapes and plastic stretches within the FEM tolerance after 200 substeps."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.shell_plate(20, yield_stress=2.5e8, load=3000.0, seed=2)
+    w = world_from_rig(rig)
+    ref = build_world(RefWorld, rig, multithreaded=False)
+    h = w.bodies()[0]
+    X0 = h.fem_tris()["X"].copy()
+    for f in range(10):
+        w.step_substeps(20)
+        ref.step_substeps(20)
+        if f in (1, 5, 9):
+            p = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
+            d = np.abs(p - ref.nodes(0)["pos"]).max()
+            assert d <= TOL, f"frame {f}: max |dp| {d:.3g} m"
+    g, r = h.fem_tris(), ref.fem_tris(0)
+    flowed_g, flowed_r = (g["X"] != X0).any(1), (r["X"] != X0).any(1)
+    assert flowed_r.sum() > 100 and abs(int(flowed_g.sum()) - int(flowed_r.sum())) <= 0.02 * flowed_r.sum()
+    assert np.abs(g["X"] - r["X"]).max() <= 1e-5
+    assert np.abs(g["dmg"] - r["dmg"]).max() <= 1e-4 and r["dmg"].max() > 1e-3
+    st = h.state()
+    assert st["fem_failures"] == 0 and st["fem_clamps"] == 0
+    w.close()
+
+
+def test_gpu_yielding_section_on_a_breaking_body_is_refused():
+    """Tears and bisections of a yielding plate are topology events this path does not make: refused at add_body."""
+    from beamlab_b200.world import BeamLabError
+    rig = rigs.shell_plate(8, yield_stress=2.5e8)
+    rig["bodies"][0]["params"]["allow_break"] = 1
+    with pytest.raises(BeamLabError, match="unsupported"):
+        world_from_rig(rig)

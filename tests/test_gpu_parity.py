@@ -36,7 +36,8 @@ def test_gpu_matches_golden(name):
 
 @pytest.mark.parametrize("make", [lambda: rigs.truss_car(2, speed=30.0), lambda: rigs.stress_rig(11),
                                   lambda: rigs.fleet(12, seed=5, median_nodes=800, min_nodes=60, max_nodes=4000,
-                                                     terrain_size=300.0, terrain_samples=257, skins=False)])
+                                                     terrain_size=300.0, terrain_samples=257, skins=False,
+                                                     wheels=False)])
 def test_gpu_matches_oracle_live(port_lib, make):
     from oracle.oracle import PortWorld, build_world
     rig = make()
@@ -118,3 +119,19 @@ def test_gpu_crash_yield_and_break_match_oracle(port_lib, shuffle, beam_kernel):
     rest = SoftBody.from_arrays(rig["bodies"][0]).beams["L"]
     yielded = np.count_nonzero(gw.beams(0)["L"] != rest)
     assert gw.body(0)["broken_beams"] > 100 and yielded > 1000, (gw.body(0)["broken_beams"], yielded)
+
+
+@pytest.mark.parametrize("split", [False, True])
+def test_gpu_air_drag_matches_reference(ref_lib, split):
+    """RoR's per-node air drag against each part's mean velocity and Cd A drag on the parts' means
+    (SoftBody::clear_forces, softbody.cpp:334-378): the truss car - one part - and the 30 m/s crash whose broken
+    beams split it into parts (labelled again when they are 8 substeps old), bitwise the compiled reference's."""
+    from oracle.oracle import RefWorld, build_world
+    rig = _wall_crash(5) if split else rigs.truss_car(1)
+    rig["bodies"][0]["params"].update({"air_drag": 0.05, "aero_cda": 0.8})
+    gw, rw = GpuWorld(rig), build_world(RefWorld, rig, multithreaded=False)
+    for f in range(12):
+        gw.step_substeps(25)
+        rw.step_substeps(25)
+        if f in (2, 7, 11):
+            assert_same(gw, rw, 1, f"frame {f}")

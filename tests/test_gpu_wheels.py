@@ -1,0 +1,65 @@
+"""Free-rolling node wheels on the GPU against the reference compiled from its sources (oracle/_ref, parity build):
+the wheel's turn (SoftBody::compute_wheel_forces with no torque, softbody.cpp:691-744), the tyre contact
+(tyre_contact, static_world.cpp:53-83) and each wheel's patch sharing its grip (World::collide_static,
+world.cpp:871-898) - node and beam states bitwise equal after 1,485 substeps of a wheeled car landing sideways, rolling
+and hitting a wall, and after three frames of a small wheeled fleet with collision skins."""
+import numpy as np
+import pytest
+
+from beamlab_b200 import rigs, world_from_rig
+from beamlab_b200.world import BeamLabError
+from gpu_adapter import GpuWorld
+from test_gpu_parity import assert_same
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("variant", ["plain", "drag", "grip", "launches"])
+def test_gpu_wheeled_car_matches_reference(ref_lib, variant):
+    """plain: the car as built; drag: with air drag (RoR's per-node drag skips the tyre nodes); grip: the world's
+    tyre grip at 0.6; launches: the frames' kernels launched one by one instead of as CUDA graphs."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.wheeled_car()
+    if variant == "drag":
+        rig["bodies"][0]["params"].update({"air_drag": 0.05, "aero_cda": 0.8})
+    if variant == "grip":
+        rig["settings"]["tyre_grip"] = 0.6
+    gw = GpuWorld(rig, graphs=False) if variant == "launches" else GpuWorld(rig)
+    rw = build_world(RefWorld, rig, multithreaded=False)
+    for f in range(45):
+        gw.step_substeps(33)
+        rw.step_substeps(33)
+        if f in (5, 13, 22, 30, 44):
+            assert_same(gw, rw, 1, f"frame {f}")
+    b = rig["bodies"][0]
+    tn = np.concatenate([w["nodes"] for w in b["wheels"]])
+    assert rw.body(0)["static_contacts"] > 0 or rw.nodes(0)["pos"][tn, 1].min() < 0.05  # (the tyres reached the ground)
+
+
+def test_gpu_wheeled_fleet_matches_reference(ref_lib):
+    """Six wheeled lattice vehicles with collision skins on the heightfield, batched in one World: bitwise the
+    reference's after three uneven frames."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.fleet(6, seed=9, median_nodes=600, min_nodes=200, max_nodes=1500, terrain_size=300.0, terrain_samples=257)
+    for b in rig["bodies"]:
+        b["pos"][:, 1] -= 0.28  # (the tyres start a few cm over the ground: they land within the frames)
+    gw = GpuWorld(rig)
+    rw = build_world(RefWorld, rig, multithreaded=False)
+    for n in (33, 20, 33, 33, 33):
+        gw.step_substeps(n)
+        rw.step_substeps(n)
+    assert_same(gw, rw, len(rig["bodies"]), "fleet")
+    assert sum(rw.body(b)["static_contacts"] for b in range(len(rig["bodies"]))) > 0
+
+
+def test_gpu_wheel_rejections():
+    """A node on two wheels, or a wheel's node out of the body, is refused at add_body."""
+    rig = rigs.wheeled_car()
+    w = rig["bodies"][0]["wheels"]
+    w[1]["nodes"] = np.concatenate([w[1]["nodes"], w[0]["nodes"][:1]])
+    with pytest.raises(BeamLabError, match="unsupported"):
+        world_from_rig(rig)
+    rig = rigs.wheeled_car()
+    rig["bodies"][0]["wheels"][0]["axle0"] = len(rig["bodies"][0]["mass"])
+    with pytest.raises(BeamLabError, match="invalid"):
+        world_from_rig(rig)

@@ -57,7 +57,8 @@ def test_golden_fixtures_exercise_every_branch():
 
 @pytest.mark.parametrize("make", [lambda: rigs.truss_car(2, speed=30.0), lambda: rigs.stress_rig(11),
                                   lambda: rigs.fleet(6, seed=5, median_nodes=300, min_nodes=60, max_nodes=900,
-                                                     terrain_size=300.0, terrain_samples=257, skins=False)])
+                                                     terrain_size=300.0, terrain_samples=257, skins=False,
+                                                     wheels=False)])
 def test_port_matches_reference_live(port_lib, ref_lib, make):
     from oracle.oracle import PortWorld, RefWorld, build_world
     rig = make()

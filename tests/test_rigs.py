@@ -58,3 +58,24 @@ def test_lattice_skin_faces_outward():
     a, b, d = p[tris[:, 0]], p[tris[:, 1]], p[tris[:, 2]]
     n = np.cross(b - a, d - a)
     assert np.all(np.einsum("ij,ij->i", n, (a + b + d) / 3 - c) > 0)
+
+
+def test_wheel_rings():
+    """add_wheels: four wheels of 24 tyre nodes (even on axle0's side, odd on axle1's, at the radius round the hubs),
+    axle0 of the lesser z, every tyre node NF_GROUND | NF_TYRE and beamed to both hubs."""
+    rig = rigs.wheeled_car()
+    b = rig["bodies"][0]
+    p = b["pos"].astype(np.float64)
+    pairs = {tuple(sorted(e)) for e in b["ab"].tolist()}
+    assert len(b["wheels"]) == 4
+    for w in b["wheels"]:
+        a0, a1, nodes = w["axle0"], w["axle1"], w["nodes"]
+        assert len(nodes) == 24 and p[a0, 2] < p[a1, 2]
+        ev, od = nodes[0::2], nodes[1::2]
+        assert np.allclose(p[ev, 2], p[a0, 2]) and np.allclose(p[od, 2], p[a1, 2])
+        assert np.allclose(np.linalg.norm(p[ev, :2] - p[a0, :2], axis=1), 0.3, atol=1e-5)
+        assert np.all(b["node_flags"][nodes] & (rigs.NF_GROUND | rigs.NF_TYRE) == rigs.NF_GROUND | rigs.NF_TYRE)
+        for t in nodes.tolist():
+            assert tuple(sorted((t, a0))) in pairs and tuple(sorted((t, a1))) in pairs
+    every = np.concatenate([w["nodes"] for w in b["wheels"]])
+    assert len(np.unique(every)) == len(every)
