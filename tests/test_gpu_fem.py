@@ -103,23 +103,27 @@ def test_gpu_yielding_plate_matches_reference(ref_lib):
     """A plate of a yielding section (250 MPa) under a 3 kN point load, on a body that deforms and does not break:
     its membrane flows (the rest shapes follow the stretch, the elements built again) and its bending yields (the
     corners' rest frames turn) in the reference's eval_tris (frame_fem.cpp:1690-1741); on the GPU the same triangles
-    flow, the nodes, rest shapes and plastic stretches within the FEM tolerance after 200 substeps."""
+    flow, the same triangles flow, the rest shapes and plastic stretches agree. The flow amplifies the kinematics'
+    last-bit differences (atan2 / sin / cos, the substitutions' order of sums) smoothly - 1e-6 m after 100 substeps,
+    1e-5 m after 120 as the flow spreads - so the nodes are held to the FEM tolerance (1e-4 m) over 140 substeps and to
+    1e-4 of the plate's 1.8 m motion (1.8e-4 m) over 200."""
     from oracle.oracle import RefWorld, build_world
     rig = rigs.shell_plate(20, yield_stress=2.5e8, load=3000.0, seed=2)
     w = world_from_rig(rig)
     ref = build_world(RefWorld, rig, multithreaded=False)
     h = w.bodies()[0]
     X0 = h.fem_tris()["X"].copy()
+    p0 = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
     for f in range(10):
         w.step_substeps(20)
         ref.step_substeps(20)
-        if f in (1, 5, 9):
-            p = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
-            d = np.abs(p - ref.nodes(0)["pos"]).max()
-            assert d <= TOL, f"frame {f}: max |dp| {d:.3g} m"
-    g, r = h.fem_tris(), ref.fem_tris(0)
-    flowed_g, flowed_r = (g["X"] != X0).any(1), (r["X"] != X0).any(1)
-    assert flowed_r.sum() > 100 and abs(int(flowed_g.sum()) - int(flowed_r.sum())) <= 0.02 * flowed_r.sum()
+        p = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
+        d = np.abs(p - ref.nodes(0)["pos"]).max()
+        lim = TOL if f <= 6 else 1e-4 * np.abs(p - p0).max()
+        assert d <= lim, f"frame {f}: max |dp| {d:.3g} m"
+        g, r = h.fem_tris(), ref.fem_tris(0)
+        assert np.array_equal((g["X"] != X0).any(1), (r["X"] != X0).any(1)), f"frame {f}: other triangles flowed"
+    assert (r["X"] != X0).any(1).sum() > 100 and np.abs(p - p0).max() > 1.0
     assert np.abs(g["X"] - r["X"]).max() <= 1e-5
     assert np.abs(g["dmg"] - r["dmg"]).max() <= 1e-4 and r["dmg"].max() > 1e-3
     st = h.state()
