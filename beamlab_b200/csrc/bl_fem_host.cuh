@@ -190,8 +190,9 @@ BL_HD inline void tri_local_k(const float X[3][2], const TriSec& s, float P[162]
     }
 }
 
-struct FrameSectionH { // FrameSection (frame_fem.h:90-112): the elastic member step's fields
+struct FrameSectionH { // FrameSection (frame_fem.h:90-112): the member step's fields
     float E, G, rho, A, Iy, Iz, J, As_y, As_z, damping, axial, joint_k;
+    float Np, Mp, Tp, hardening;
 };
 
 // One body's frame of members and triangle elements, as built and analysed
@@ -206,6 +207,8 @@ struct FemModel {
     std::vector<uint8_t> mend;       // 2 per member: the joints at a, b
     std::vector<float> mL0, mmass;   // rest length; the mass it put on its nodes
     std::vector<float> mq;           // 8 per member: its rest frame in its end nodes' frames, qa then qb (x y z w)
+    std::vector<float> mps;          // 16 per member: its plastic state (up tp bt dmg_a, pa pb, ba bb, dmg_b - - -)
+    std::vector<uint32_t> mflag;     // per member: its tangent's yield and unload bits and its elastic hold
     std::vector<uint8_t> mbroken;
     std::vector<int> mblock;         // its off-diagonal block (-1: its ends share a column)
     std::vector<uint8_t> mswap;      // the block's row is its a end

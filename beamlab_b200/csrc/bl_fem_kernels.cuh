@@ -89,7 +89,7 @@ struct FemDev {
     const int2* mn;          // frame nodes a, b
     const int* mmeta;        // section | joint at a << 16 | joint at b << 24; -1: broken at rest
     const float* mL0;
-    const float4* mq;        // 2 / member: its rest frame in a's and in b's frame
+    float4* mq;              // 2 / member: its rest frame in a's and in b's frame (the plastic rotations baked in)
     const struct FemMemSecDev* msec;
     float4* mfa;             // force on a (on b: its negative)
     float4* mta;             // torque on a
@@ -98,6 +98,19 @@ struct FemDev {
     float4* mtan;            // the tangent's axis e1 and N / L (its geometric stiffness)
     double* mkw;             // 144 / member: the world blocks aa, bb, ba, ab (FemFrame::mem_kw_)
     double* mkv;             // 12 / member: K v (FemFrame::mem_kv_)
+    // the members' plasticity (FrameElement's plastic state, FemFrame::Tangent) and the unload re-pass
+    float4* mps;             // 4 / member: (up, tp, bt, dmg_a), (pa, pb), (ba, bb), (dmg_b, -, -, -)
+    float4* mtg;             // 6 / member: the tangent - (e1, L), (e2, ka), (e3, kt), (cy0 cy1 cy2 cz0), (cz1 cz2 N T),
+                             // (ma, mb)
+    uint32_t* mflag;         // / member: yield (bits 0-3), unload (8-11), elastic_hold (16-23)
+    float* credit;           // / body: FemFrame::repass_credit_
+    int* elastic;            // / body: FemFrame::elastic_step_
+    int* comp_again;         // / component: bit p - pass p's check found a hinge the step unloads
+    const int* comp_size;    // / component: its columns
+    const int* body_comp;    // / body + 1: its components' range
+    int* rp;                 // [0], [1]: a re-pass after pass 0, pass 1
+    long long* repc;         // the re-passes run
+    int nbody;
 };
 
 // ------------------------------------------------------------------------------------------ quaternions (math.h:105-215)
@@ -385,8 +398,12 @@ __global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __rest
 // stiffnesses (stiffness, frame_fem.cpp:1408-1476), the axial force, torque and end moments, the nodal forces
 // -B^T g, the tangent and its world blocks with K v (member_world_k / element_matrix, frame_fem.cpp:1834-1850,
 // 2157-2186), a thread a member, float where the reference is float and double where it is double.
+constexpr float kPi = 3.14159265358979323846f;
+
 struct FemMemSecDev { // FrameSection (frame_fem.h:90-112)
     float E, G, rho, A, Iy, Iz, J, As_y, As_z, damping, axial, joint_k;
+    float Np, Mp, Tp, hardening;
+    int plastic;             // Np > 0 on a body that deforms: the member yields (eval_forces' plastic)
 };
 enum : int { FJ_RIGID = 0, FJ_BALL = 1, FJ_HINGE_V = 2, FJ_HINGE_H = 3, FJ_SWIVEL = 4, FJ_ELASTIC = 5 };
 
@@ -461,6 +478,62 @@ __device__ __forceinline__ void ends2_dev(float c[3], bool ra, bool rb, float fa
     c[0] = (float)(F11 / d2), c[1] = (float)(-F01 / d2), c[2] = (float)(F00 / d2);
 }
 
+// FemFrame::condense (frame_fem.cpp:1414-1418): a flowing hinge's end turns like a pin
+__device__ __forceinline__ void condense(float c[3], bool pin_a, bool pin_b) {
+    if (pin_a && pin_b) c[0] = c[1] = c[2] = 0;
+    else if (pin_a) c[2] = c[0] > 0 ? c[2] - c[1] * c[1] / c[0] : 0, c[0] = c[1] = 0;
+    else if (pin_b) c[0] = c[2] > 0 ? c[0] - c[1] * c[1] / c[2] : 0, c[1] = c[2] = 0;
+}
+
+// member_world_k (frame_fem.cpp:1834-1850) of the effective tangent (FemFrame::effective, frame_fem.cpp:2147-2155:
+// the flowing parts its yield bits less its unload bits name - hinges condensed, axial and twist at 1 %): the world
+// blocks of element_matrix (frame_fem.cpp:2157-2186) and K v at the ends' velocities
+__device__ void member_world_k(const FemDev& F, const float4* __restrict__ nd, int ei, int2 ab, v3 e1, v3 e2, v3 e3, float L, float ka, float kt,
+                               const float cy_in[3], const float cz_in[3], uint32_t y) {
+    float cy[3] = {cy_in[0], cy_in[1], cy_in[2]}, cz[3] = {cz_in[0], cz_in[1], cz_in[2]};
+    if (y & 3) condense(cy, y & 1, y & 2), condense(cz, y & 1, y & 2);
+    if (y & 4) ka *= 0.01f;
+    if (y & 8) kt *= 0.01f;
+    const double iL = 1.0 / L;
+    const double E1[3] = {e1.x, e1.y, e1.z}, E2[3] = {e2.x, e2.y, e2.z}, E3[3] = {e3.x, e3.y, e3.z};
+    const double g[3] = {E3[0] * iL, E3[1] * iL, E3[2] * iL}, h[3] = {E2[0] * iL, E2[1] * iL, E2[2] * iL};
+    const double cy0 = cy[0], cy1 = cy[1], cy2 = cy[2], cz0 = cz[0], cz1 = cz[1], cz2 = cz[2];
+    const double Sy2 = cy0 + 2 * cy1 + cy2, Sz2 = cz0 + 2 * cz1 + cz2, ay = cy0 + cy1, by = cy1 + cy2, az = cz0 + cz1, bz = cz1 + cz2;
+    const double kad = ka, ktd = kt;
+    double K[12][12];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            const double uu = kad * E1[i] * E1[j] + Sy2 * g[i] * g[j] + Sz2 * h[i] * h[j];
+            const double up = -ay * g[i] * E2[j] + az * h[i] * E3[j];
+            const double ub = -by * g[i] * E2[j] + bz * h[i] * E3[j];
+            const double tt = ktd * E1[i] * E1[j];
+            const double pa = tt + cy0 * E2[i] * E2[j] + cz0 * E3[i] * E3[j];
+            const double pb = -tt + cy1 * E2[i] * E2[j] + cz1 * E3[i] * E3[j];
+            const double qb = tt + cy2 * E2[i] * E2[j] + cz2 * E3[i] * E3[j];
+            K[i][j] = uu, K[i][3 + j] = up, K[i][6 + j] = -uu, K[i][9 + j] = ub;
+            K[3 + i][3 + j] = pa, K[3 + i][9 + j] = pb;
+            K[6 + i][6 + j] = uu, K[6 + i][9 + j] = -ub;
+            K[9 + i][9 + j] = qb;
+        }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) K[3 + i][6 + j] = -K[j][3 + i];
+    for (int r = 0; r < 12; r++)
+        for (int c2 = r + 1; c2 < 12; c2++) K[c2][r] = K[r][c2];
+    double* W = F.mkw + 144 * (size_t)ei;
+    for (int r = 0; r < 6; r++)
+        for (int q = 0; q < 6; q++)
+            W[r * 6 + q] = K[r][q], W[36 + r * 6 + q] = K[6 + r][6 + q], W[72 + r * 6 + q] = K[6 + r][q], W[108 + r * 6 + q] = K[r][6 + q];
+    const float4 va = nd[2 * F.fnode[ab.x] + 1], vb = nd[2 * F.fnode[ab.y] + 1], wa = F.w[ab.x], wb = F.w[ab.y];
+    const double u[12] = {va.x, va.y, va.z, wa.x, wa.y, wa.z, vb.x, vb.y, vb.z, wb.x, wb.y, wb.z};
+    double* kv = F.mkv + 12 * (size_t)ei;
+    for (int r = 0; r < 12; r++) {
+        double s2 = 0;
+        for (int q = 0; q < 12; q++) s2 += K[r][q] * u[q];
+        kv[r] = s2;
+    }
+}
+
+template <bool kPlastic>
 __global__ void __launch_bounds__(128) k_member_eval(FemDev F, const float4* __restrict__ nd) {
     const int ei = blockIdx.x * blockDim.x + threadIdx.x;
     if (ei >= F.nmem) return;
@@ -511,14 +584,66 @@ __global__ void __launch_bounds__(128) k_member_eval(FemDev F, const float4* __r
         cz[1] = (2.0f - phi) * k0;
         ends2_dev(cz, fa.rel[2], fb.rel[2], fa.f, fb.f);
     }
-    // ---- forces: elastic (no plastic parts: up = tp = 0, pa = pb = 0)
+    // ---- the section's forces: axial yield at Np (compression at the lower of Np and the Euler load of 0.7 L), the
+    // twist's at Tp, radial-return hinges at the ends against the hardened plastic moment, twice (eval_forces,
+    // frame_fem.cpp:1915-1982); an elastic section's plastic parts stay 0
+    const bool plastic = kPlastic && s.plastic;
+    float up = 0, tp = 0, bt = 0, dmga = 0, dmgb = 0, pax = 0, pay = 0, pbx = 0, pby = 0, bax = 0, bay = 0, bbx = 0, bby = 0;
+    uint32_t fl = 0;
+    if (kPlastic) {
+        const float4 s0 = F.mps[4 * ei], s1 = F.mps[4 * ei + 1], s2 = F.mps[4 * ei + 2], s3 = F.mps[4 * ei + 3];
+        up = s0.x, tp = s0.y, bt = s0.z, dmga = s0.w, pax = s1.x, pay = s1.y, pbx = s1.z, pby = s1.w;
+        bax = s2.x, bay = s2.y, bbx = s2.z, bby = s2.w, dmgb = s3.x;
+        fl = F.mflag[ei];
+    }
     const float delta = (float)dL;
-    const float N = ka * (delta - 0.0f);
+    float N = ka * (delta - up);
+    float flow_ax = 0, flow_t = 0, flow_a = 0, flow_b = 0;
+    if (plastic) {
+        const float Nt = s.Np, Le = 0.7f * L0;
+        const float Nc = smin(s.Np, kPi * kPi * s.E * smin(s.Iy, s.Iz) / (Le * Le));
+        if (N > Nt || N < -Nc) {
+            const float lim = N > 0 ? Nt : -Nc;
+            const float dup = (N - lim) / ka;
+            up += dup;
+            flow_ax = fabsf(dup) / L0;
+            N = lim;
+        }
+    }
     const float twist = rb.x - ra.x;
-    const float T = kt * (twist - 0.0f);
-    const float dax = ra.y - 0.0f, day = ra.z - 0.0f, dbx = rb.y - 0.0f, dby = rb.z - 0.0f;
-    const float Max = cy[0] * dax + cy[1] * dbx, May = cz[0] * day + cz[1] * dby;
-    const float Mbx = cy[1] * dax + cy[2] * dbx, Mby = cz[1] * day + cz[2] * dby;
+    float T = kt * (twist - tp);
+    if (plastic && s.Tp > 0 && kt > 0 && fabsf(T) > s.Tp) {
+        const float lim = T > 0 ? s.Tp : -s.Tp;
+        const float dtp = (T - lim) / kt;
+        tp += dtp;
+        flow_t = fabsf(dtp);
+        T = lim;
+    }
+    float Max, May, Mbx, Mby;
+    auto moments = [&]() {
+        const float dax = ra.y - pax, day = ra.z - pay, dbx = rb.y - pbx, dby = rb.z - pby;
+        Max = cy[0] * dax + cy[1] * dbx, May = cz[0] * day + cz[1] * dby;
+        Mbx = cy[1] * dax + cy[2] * dbx, Mby = cz[1] * day + cz[2] * dby;
+    };
+    moments();
+    if (plastic && s.Mp > 0) {
+        auto yield_end = [&](float Mx, float My, float cyy, float czz, float& px, float& py, float bx, float by, float& dmg, float& flow) {
+            const float Mp = s.Mp * (1.0f + s.hardening * smin(1.0f, dmg));
+            const float l = sqrtf(Mx * Mx + My * My);
+            if (l <= Mp) return false;
+            const float r = 1.0f - Mp / l;
+            const float dpx = cyy > 0 ? Mx * r / cyy : 0.0f, dpy = czz > 0 ? My * r / czz : 0.0f;
+            px = px + dpx, py = py + dpy;
+            flow += sqrtf(dpx * dpx + dpy * dpy);
+            const float qx = px + bx, qy = py + by;
+            dmg = smax(dmg, sqrtf(qx * qx + qy * qy));
+            return true;
+        };
+        for (int it = 0; it < 2; it++) {
+            if (yield_end(Max, May, cy[0], cz[0], pax, pay, bax, bay, dmga, flow_a)) moments();
+            if (yield_end(Mbx, Mby, cy[2], cz[2], pbx, pby, bbx, bby, dmgb, flow_b)) moments();
+        }
+    }
     const float Sy = Max + Mbx, Sz = May + Mby;
     const v3 fav = e1 * N + e3 * (Sy / L) - e2 * (Sz / L);
     const v3 tav = e1 * T - e2 * Max - e3 * May;
@@ -526,46 +651,120 @@ __global__ void __launch_bounds__(128) k_member_eval(FemDev F, const float4* __r
     F.mfa[ei] = make_float4(fav.x, fav.y, fav.z, 0.0f);
     F.mta[ei] = make_float4(tav.x, tav.y, tav.z, 0.0f);
     F.mtb[ei] = make_float4(tbv.x, tbv.y, tbv.z, 0.0f);
+    uint32_t y = 0;
+    if (kPlastic) {
+        // the plastic rotations into the rest frames past 0.02 rad, the twist half into each end (frame_fem.cpp:
+        // 2045-2054)
+        const float kBake = 0.02f;
+        if (pax * pax + pay * pay > kBake * kBake) {
+            const float4 q = F.mq[2 * ei];
+            const q4 n = qnormalize(qmul(q4{q.x, q.y, q.z, q.w}, quat_exp(V(0, -pax, -pay))));
+            F.mq[2 * ei] = make_float4(n.x, n.y, n.z, n.w);
+            bax = bax + pax, bay = bay + pay, pax = pay = 0;
+        }
+        if (pbx * pbx + pby * pby > kBake * kBake) {
+            const float4 q = F.mq[2 * ei + 1];
+            const q4 n = qnormalize(qmul(q4{q.x, q.y, q.z, q.w}, quat_exp(V(0, -pbx, -pby))));
+            F.mq[2 * ei + 1] = make_float4(n.x, n.y, n.z, n.w);
+            bbx = bbx + pbx, bby = bby + pby, pbx = pby = 0;
+        }
+        if (fabsf(tp) > kBake) {
+            const float4 qa = F.mq[2 * ei], qb = F.mq[2 * ei + 1];
+            const q4 na = qnormalize(qmul(q4{qa.x, qa.y, qa.z, qa.w}, quat_exp(V(0.5f * tp, 0, 0))));
+            const q4 nb = qnormalize(qmul(q4{qb.x, qb.y, qb.z, qb.w}, quat_exp(V(-0.5f * tp, 0, 0))));
+            F.mq[2 * ei] = make_float4(na.x, na.y, na.z, na.w), F.mq[2 * ei + 1] = make_float4(nb.x, nb.y, nb.z, nb.w);
+            bt += tp, tp = 0;
+        }
+        F.mps[4 * ei] = make_float4(up, tp, bt, dmga);
+        F.mps[4 * ei + 1] = make_float4(pax, pay, pbx, pby);
+        F.mps[4 * ei + 2] = make_float4(bax, bay, bbx, bby);
+        F.mps[4 * ei + 3] = make_float4(dmgb, 0.0f, 0.0f, 0.0f);
+        // the tangent: elastic, the parts flowing this step plastic unless the step unloads them (frame_fem.cpp:
+        // 2056-2069): held elastic 16 steps after an unload, and while the re-passes' budget is spent
+        const float kFlow = 1e-4f;
+        const uint32_t yl = (flow_a > kFlow ? 1u : 0u) | (flow_b > kFlow ? 2u : 0u) | (flow_ax > 0.1f * kFlow ? 4u : 0u) | (flow_t > kFlow ? 8u : 0u);
+        uint32_t hold = (fl >> 16) & 0xff, unload = 0;
+        if (hold > 0) hold--, unload = yl;
+        if (F.elastic[F.fbody[ab.x]]) unload = yl;
+        F.mflag[ei] = yl | (unload << 8) | (hold << 16);
+        F.mtg[6 * ei] = make_float4(e1.x, e1.y, e1.z, L);
+        F.mtg[6 * ei + 1] = make_float4(e2.x, e2.y, e2.z, ka);
+        F.mtg[6 * ei + 2] = make_float4(e3.x, e3.y, e3.z, kt);
+        F.mtg[6 * ei + 3] = make_float4(cy[0], cy[1], cy[2], cz[0]);
+        F.mtg[6 * ei + 4] = make_float4(cz[1], cz[2], N, T);
+        F.mtg[6 * ei + 5] = make_float4(Max, May, Mbx, Mby);
+        y = yl & ~unload;
+    }
     F.mon[ei] = 1;
     F.mtan[ei] = make_float4(e1.x, e1.y, e1.z, N > 0 ? N / L : 0.0f);
-    // ---- the tangent's world blocks (element_matrix in 3 x 3 blocks of [ua, pa, ub, pb]) and K v
-    const double iL = 1.0 / L;
-    const double E1[3] = {e1.x, e1.y, e1.z}, E2[3] = {e2.x, e2.y, e2.z}, E3[3] = {e3.x, e3.y, e3.z};
-    const double g[3] = {E3[0] * iL, E3[1] * iL, E3[2] * iL}, h[3] = {E2[0] * iL, E2[1] * iL, E2[2] * iL};
-    const double cy0 = cy[0], cy1 = cy[1], cy2 = cy[2], cz0 = cz[0], cz1 = cz[1], cz2 = cz[2];
-    const double Sy2 = cy0 + 2 * cy1 + cy2, Sz2 = cz0 + 2 * cz1 + cz2, ay = cy0 + cy1, by = cy1 + cy2, az = cz0 + cz1, bz = cz1 + cz2;
-    const double kad = ka, ktd = kt;
-    double K[12][12];
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) {
-            const double uu = kad * E1[i] * E1[j] + Sy2 * g[i] * g[j] + Sz2 * h[i] * h[j];
-            const double up = -ay * g[i] * E2[j] + az * h[i] * E3[j];
-            const double ub = -by * g[i] * E2[j] + bz * h[i] * E3[j];
-            const double tt = ktd * E1[i] * E1[j];
-            const double pa = tt + cy0 * E2[i] * E2[j] + cz0 * E3[i] * E3[j];
-            const double pb = -tt + cy1 * E2[i] * E2[j] + cz1 * E3[i] * E3[j];
-            const double qb = tt + cy2 * E2[i] * E2[j] + cz2 * E3[i] * E3[j];
-            K[i][j] = uu, K[i][3 + j] = up, K[i][6 + j] = -uu, K[i][9 + j] = ub;
-            K[3 + i][3 + j] = pa, K[3 + i][9 + j] = pb;
-            K[6 + i][6 + j] = uu, K[6 + i][9 + j] = -ub;
-            K[9 + i][9 + j] = qb;
+    member_world_k(F, nd, ei, ab, e1, e2, e3, L, ka, kt, cy, cz, y);
+}
+
+// The unload check after pass `pass`'s solve (frame_fem.cpp:2959-2989): a flowing part of a member whose end rates
+// from the solution run against its moment (force, torque) gets its elastic tangent (held 16 steps), its world blocks
+// again; its component is marked for another pass. Pass 1's check runs only where pass 1 ran.
+__global__ void k_member_unload(FemDev F, const float4* __restrict__ nd, int pass) {
+    const int ei = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ei >= F.nmem || (pass > 0 && F.rp[pass - 1] == 0) || !F.mon[ei]) return;
+    const uint32_t fl = F.mflag[ei];
+    const uint32_t yl = fl & 0xf, unload = (fl >> 8) & 0xf, y = yl & ~unload;
+    if (!y) return;
+    const int2 ab = F.mn[ei];
+    auto vel = [&](int fn, v3& v, v3& om) {
+        const int col = F.iperm[fn];
+        if (F.fixed[col]) {
+            v = om = V(0, 0, 0);
+            return;
         }
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) K[3 + i][6 + j] = -K[j][3 + i];
-    for (int r = 0; r < 12; r++)
-        for (int c2 = r + 1; c2 < 12; c2++) K[c2][r] = K[r][c2];
-    double* W = F.mkw + 144 * (size_t)ei;
-    for (int r = 0; r < 6; r++)
-        for (int q = 0; q < 6; q++)
-            W[r * 6 + q] = K[r][q], W[36 + r * 6 + q] = K[6 + r][6 + q], W[72 + r * 6 + q] = K[6 + r][q], W[108 + r * 6 + q] = K[r][6 + q];
-    const float4 va = nd[2 * F.fnode[ab.x] + 1], vb = nd[2 * F.fnode[ab.y] + 1], wa = F.w[ab.x], wb = F.w[ab.y];
-    const double u[12] = {va.x, va.y, va.z, wa.x, wa.y, wa.z, vb.x, vb.y, vb.z, wb.x, wb.y, wb.z};
-    double* kv = F.mkv + 12 * (size_t)ei;
-    for (int r = 0; r < 12; r++) {
-        double s2 = 0;
-        for (int q = 0; q < 12; q++) s2 += K[r][q] * u[q];
-        kv[r] = s2;
+        const double* x = F.rhs + 6 * (size_t)col;
+        const float4 nv = nd[2 * F.fnode[fn] + 1], w = F.w[fn];
+        v = V(nv.x + (float)x[0], nv.y + (float)x[1], nv.z + (float)x[2]);
+        om = V(w.x + (float)x[3], w.y + (float)x[4], w.z + (float)x[5]);
+    };
+    v3 va, wa, vb, wb;
+    vel(ab.x, va, wa), vel(ab.y, vb, wb);
+    const float4 t0 = F.mtg[6 * ei], t1 = F.mtg[6 * ei + 1], t2 = F.mtg[6 * ei + 2], t4 = F.mtg[6 * ei + 4], t5 = F.mtg[6 * ei + 5];
+    const v3 e1 = V(t0.x, t0.y, t0.z), e2 = V(t1.x, t1.y, t1.z), e3 = V(t2.x, t2.y, t2.z);
+    const float iL = 1.0f / t0.w;
+    const v3 dv = vb - va;
+    const float rax = dot(e3, dv) * iL + dot(e2, wa), ray = -dot(e2, dv) * iL + dot(e3, wa);
+    const float rbx = dot(e3, dv) * iL + dot(e2, wb), rby = -dot(e2, dv) * iL + dot(e3, wb);
+    uint32_t u = 0;
+    if ((y & 1) && rax * t5.x + ray * t5.y < 0) u |= 1;
+    if ((y & 2) && rbx * t5.z + rby * t5.w < 0) u |= 2;
+    if ((y & 4) && dot(e1, dv) * t4.z < 0) u |= 4;
+    if ((y & 8) && dot(e1, wb - wa) * t4.w < 0) u |= 8;
+    if (!u) return;
+    const uint32_t un = unload | u;
+    F.mflag[ei] = yl | (un << 8) | (16u << 16);
+    const float4 t3 = F.mtg[6 * ei + 3];
+    const float cy[3] = {t3.x, t3.y, t3.z}, cz[3] = {t3.w, t4.x, t4.y};
+    member_world_k(F, nd, ei, ab, e1, e2, e3, t0.w, t1.w, t2.w, cy, cz, yl & ~un);
+    atomicOr(&F.comp_again[F.col_comp[F.iperm[ab.x]]], 1 << pass);
+    F.rp[pass] = 1;
+}
+
+// the condition of the IF node of pass + 1's re-pass: set where pass `pass`'s check found an unload
+__global__ void k_repass_cond(const int* __restrict__ rp, int pass, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, rp[pass] ? 1u : 0u);
+}
+
+// The re-passes' budget (FemFrame::begin_forces, frame_fem.cpp:1863-1864, and solve's accounting, frame_fem.cpp:2591,
+// 2990): a body's re-passes of components of 60 columns or more spent from its credit, then its credit for the next
+// step refilled by a quarter (at most 8); with less than one left its next step's tangents stay elastic.
+__global__ void k_repass_account(FemDev F) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b == 0) *F.repc += F.rp[0] + F.rp[1], F.rp[0] = F.rp[1] = 0;
+    if (b >= F.nbody) return;
+    float cr = F.credit[b];
+    for (int cc = F.body_comp[b]; cc < F.body_comp[b + 1]; cc++) {
+        const int bits = F.comp_again[cc];
+        if (bits && F.comp_size[cc] >= 60) cr -= (float)__popc(bits);
+        F.comp_again[cc] = 0;
     }
+    cr = smin(8.0f, cr + 0.25f);
+    F.credit[b] = cr;
+    F.elastic[b] = cr < 1.0f ? 1 : 0;
 }
 
 // gather_part's member block (frame_fem.cpp:927-941): block blk (0 aa, 1 bb, 2 ba, 3 ab) times c, with the geometric

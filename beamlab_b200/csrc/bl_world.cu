@@ -48,6 +48,8 @@ struct HostBody {
     std::vector<float> fq, fw;             // frame nodes' orientation (4) and angular velocity (3)
     float theta = 0.5f, diss = 0.02f;
     int fem_failures = 0, fem_clamps = 0;
+    float repass_credit = 8.0f;            // FemFrame::repass_credit_ (refilled for its next step)
+    int elastic_step = 0;                  // FemFrame::elastic_step_ of its next step
     struct Wheel {
         uint32_t axle0, axle1;
         std::vector<uint32_t> nodes;      // its tyre nodes in the given order (the parity of a place: the hub it turns about)
@@ -123,6 +125,8 @@ struct bl_gpu_ctx {
     // FEM frames of all bodies back to back (see bl_fem_kernels.cuh)
     int NF = 0, NT = 0, NB = 0, n_fem_nodes = 0;
     bool any_plastic = false;                  // a yielding shell section on a body that deforms (k_tri_eval<true>)
+    bool any_plastic_members = false;          // a yielding member section on a body that deforms (k_member_eval<true>,
+                                               // the unload re-pass)
     int64_t NU = 0;                            // block updates of a factorization
     bool any_ext = false;
     bool any_drag = false;                     // some body has air drag (k_drag_parts)
@@ -162,7 +166,11 @@ struct bl_gpu_ctx {
     DevBuf<int2> mn;
     DevBuf<int> mmeta;
     DevBuf<float> mL0;
-    DevBuf<float4> mq, mfa, mta, mtb, mtan;
+    DevBuf<float4> mq, mfa, mta, mtb, mtan, mps, mtg;
+    DevBuf<uint32_t> mflag;
+    DevBuf<float> credit;
+    DevBuf<int> elastic, comp_again, comp_size, body_comp, rp;
+    DevBuf<long long> repc;
     DevBuf<FemMemSecDev> msec;
     DevBuf<uint8_t> mon;
     DevBuf<double> mkw, mkv;
@@ -234,6 +242,8 @@ static void free_fem(bl_gpu_ctx* c) {
     c->fcol.free_(), c->fchain.free_(), c->fblk.free_(), c->fD.free_(), c->fb.free_(), c->front = FrontDev{}, c->front_level = 0;
     c->mn.free_(), c->mmeta.free_(), c->mL0.free_(), c->mq.free_(), c->mfa.free_(), c->mta.free_(), c->mtb.free_(), c->mtan.free_();
     c->msec.free_(), c->mon.free_(), c->mkw.free_(), c->mkv.free_(), c->NM = 0;
+    c->mps.free_(), c->mtg.free_(), c->mflag.free_(), c->credit.free_(), c->elastic.free_(), c->comp_again.free_(), c->comp_size.free_();
+    c->body_comp.free_(), c->rp.free_(), c->repc.free_();
     c->xd.free_(), c->diag.free_(), c->ldiag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->tb.free_(), c->tX0.free_(), c->th0.free_(), c->tdmg.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
 }
@@ -428,6 +438,37 @@ static int pull_state(bl_gpu_ctx* c) {
                 to += (int)nt;
             }
         }
+        if (c->NM > 0 && c->any_plastic_members) { // (the members' plastic state and rest frames, the re-passes' budget)
+            std::vector<float4> mq(2 * (size_t)c->NM), mps(4 * (size_t)c->NM);
+            std::vector<uint32_t> mflag(c->NM);
+            std::vector<float> credit(c->B);
+            std::vector<int> elastic(c->B);
+            BL_CUDA(c, cudaMemcpy(mq.data(), c->mq.p, sizeof(float4) * mq.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(mps.data(), c->mps.p, sizeof(float4) * mps.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(mflag.data(), c->mflag.p, sizeof(uint32_t) * mflag.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(credit.data(), c->credit.p, sizeof(float) * credit.size(), cudaMemcpyDeviceToHost));
+            BL_CUDA(c, cudaMemcpy(elastic.data(), c->elastic.p, sizeof(int) * elastic.size(), cudaMemcpyDeviceToHost));
+            size_t mo = 0;
+            for (int bi = 0; bi < c->B; bi++) {
+                HostBody& hb = c->bodies[bi];
+                hb.repass_credit = credit[bi], hb.elastic_step = elastic[bi];
+                if (!hb.fem) continue;
+                FemModel& M = *hb.fem;
+                const size_t E = M.mn.size();
+                M.mps.resize(16 * E), M.mflag.resize(E);
+                for (size_t e = 0; e < E; e++) {
+                    const float4 qa = mq[2 * (mo + e)], qb = mq[2 * (mo + e) + 1];
+                    const float q8[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
+                    for (int k = 0; k < 8; k++) M.mq[8 * e + k] = q8[k];
+                    for (int k = 0; k < 4; k++) {
+                        const float4 v = mps[4 * (mo + e) + k];
+                        M.mps[16 * e + 4 * k] = v.x, M.mps[16 * e + 4 * k + 1] = v.y, M.mps[16 * e + 4 * k + 2] = v.z, M.mps[16 * e + 4 * k + 3] = v.w;
+                    }
+                    M.mflag[e] = mflag[mo + e];
+                }
+                mo += E;
+            }
+        }
     }
     return BL_GPU_OK;
 }
@@ -441,7 +482,7 @@ static int commit_fem(bl_gpu_ctx* c) {
     for (const HostBody& hb : c->bodies)
         if (hb.fem) NF += (int)hb.fem->node.size(), NT += (int)hb.fem->tn.size(), NB += (int)hb.fem->row.size(), NC += hb.fem->ncomp,
                     NS += (int)hb.sections.size(), nfem_nodes += hb.rec.nnodes;
-    c->NF = NF, c->NT = NT, c->NB = NB, c->n_fem_nodes = nfem_nodes, c->any_plastic = false;
+    c->NF = NF, c->NT = NT, c->NB = NB, c->n_fem_nodes = nfem_nodes, c->any_plastic = false, c->any_plastic_members = false;
     c->lvl_grp_ptr.clear(), c->lvl_col_ptr.clear();
     std::vector<float4> ext(c->any_ext ? c->N : 0, make_float4(0, 0, 0, 0));
     for (const HostBody& hb : c->bodies)
@@ -468,13 +509,19 @@ static int commit_fem(bl_gpu_ctx* c) {
     std::vector<int2> mnv;                // members: frame nodes, meta, rest length, rest frames; their sections
     std::vector<int> mmeta;
     std::vector<float> mL0;
-    std::vector<float4> mqv;
+    std::vector<float4> mqv, mpsv;
+    std::vector<uint32_t> mflagv;
     std::vector<FemMemSecDev> msecv;
+    std::vector<int> comp_size, body_comp(c->B + 1, 0);
+    std::vector<float> credit(c->B, 8.0f);
+    std::vector<int> elastic(c->B, 0);
     for (int bi = 0; bi < c->B; bi++) {
         const HostBody& hb = c->bodies[bi];
         if (!hb.fem) continue;
         const FemModel& M = *hb.fem;
         const int nf = (int)M.node.size(), nt = (int)M.tn.size(), nb = (int)M.row.size();
+        // (a section yields where the body deforms: eval_tris' s.yield > 0 and eval_forces' s.Np > 0, with allow_deform)
+        const int plastic = (hb.beam_bits & BB_DEFORM) ? 1 : 0;
         for (int i = 0; i < hb.rec.nnodes; i++) fem_nodes.push_back(hb.rec.node0 + i);
         const float dt = c->cfg.dt;
         const double h2 = (double)hb.theta * dt * dt, hd = (double)hb.diss * dt * dt;
@@ -506,11 +553,21 @@ static int commit_fem(bl_gpu_ctx* c) {
             mL0.push_back(M.mL0[e]);
             mqv.push_back(make_float4(M.mq[8 * e], M.mq[8 * e + 1], M.mq[8 * e + 2], M.mq[8 * e + 3]));
             mqv.push_back(make_float4(M.mq[8 * e + 4], M.mq[8 * e + 5], M.mq[8 * e + 6], M.mq[8 * e + 7]));
+            const bool st = M.mps.size() == 16 * M.mn.size();
+            for (int k = 0; k < 4; k++)
+                mpsv.push_back(st ? make_float4(M.mps[16 * e + 4 * k], M.mps[16 * e + 4 * k + 1], M.mps[16 * e + 4 * k + 2], M.mps[16 * e + 4 * k + 3])
+                                  : make_float4(0, 0, 0, 0));
+            mflagv.push_back(M.mflag.size() == M.mn.size() ? M.mflag[e] : 0u);
         }
-        for (const FrameSectionH& fs : hb.fsections)
-            msecv.push_back(FemMemSecDev{fs.E, fs.G, fs.rho, fs.A, fs.Iy, fs.Iz, fs.J, fs.As_y, fs.As_z, fs.damping, fs.axial, fs.joint_k});
-        for (int cc = 0; cc < M.ncomp; cc++)
+        credit[bi] = hb.repass_credit, elastic[bi] = hb.elastic_step;
+        for (const FrameSectionH& fs : hb.fsections) // (it yields on a body that deforms: eval_forces' s.Np > 0 && allow_deform)
+            msecv.push_back(FemMemSecDev{fs.E, fs.G, fs.rho, fs.A, fs.Iy, fs.Iz, fs.J, fs.As_y, fs.As_z, fs.damping, fs.axial, fs.joint_k,
+                                         fs.Np, fs.Mp, fs.Tp, fs.hardening, fs.Np > 0 ? plastic : 0}),
+                c->any_plastic_members |= fs.Np > 0 && plastic;
+        for (int cc = 0; cc < M.ncomp; cc++) {
             for (int k = M.comp_first[cc]; k < M.comp_first[cc + 1]; k++) col_comp[fo + k] = co + cc;
+            comp_size.push_back(M.comp_first[cc + 1] - M.comp_first[cc]);
+        }
         for (int t = 0; t < nt; t++) {
             tn[to + t] = make_int4(fo + M.tn[t][0], fo + M.tn[t][1], fo + M.tn[t][2], so + M.tsec[t]);
             for (int x = 0; x < 6; x++) tX[6 * (size_t)(to + t) + x] = M.tX[6 * t + x];
@@ -522,8 +579,6 @@ static int commit_fem(bl_gpu_ctx* c) {
             tdmg[to + t] = M.tdmg[t];
             tbroken[to + t] = M.tbroken[t];
         }
-        // (a section yields where the body deforms: eval_tris' s.yield > 0 && b.allow_deform)
-        const int plastic = (hb.beam_bits & BB_DEFORM) ? 1 : 0;
         for (const FemSection& fs : hb.sections)
             sec.push_back(FemSecDev{fs.E, fs.nu, fs.rho, fs.t, fs.damping, fs.drill, fs.yield, fs.yield > 0 ? plastic : 0}),
                 c->any_plastic |= fs.yield > 0 && plastic;
@@ -541,8 +596,10 @@ static int commit_fem(bl_gpu_ctx* c) {
             level[fo + par] = std::max(level[fo + par], level[fo + k] + 1);
         }
         fo += nf, to += nt, bo += nb, co += M.ncomp, so += (int)hb.sections.size();
+        body_comp[bi + 1] = co;
         mo += (int)M.mn.size(), mso += (int)hb.fsections.size();
     }
+    for (int bi = 0; bi < c->B; bi++) body_comp[bi + 1] = std::max(body_comp[bi + 1], body_comp[bi]);
     int nlev = 0;
     for (int k = 0; k < NF; k++) nlev = std::max(nlev, level[k] + 1);
     // per level: its columns, and the updates they make grouped by target (each group in the order of its columns)
@@ -659,6 +716,18 @@ static int commit_fem(bl_gpu_ctx* c) {
         F.nmem = E, F.mn = c->mn.p, F.mmeta = c->mmeta.p, F.mL0 = c->mL0.p, F.mq = c->mq.p, F.msec = c->msec.p;
         F.mfa = c->mfa.p, F.mta = c->mta.p, F.mtb = c->mtb.p, F.mon = c->mon.p, F.mtan = c->mtan.p, F.mkw = c->mkw.p, F.mkv = c->mkv.p;
         c->NM = E;
+        if (c->any_plastic_members) { // (the members' plastic state, their tangents, the re-passes' budget)
+            std::vector<int> rp(2, 0);
+            if ((rc = upload_vec(c, c->mps, mpsv)) || (rc = upload_vec(c, c->mflag, mflagv)) || (rc = upload_vec(c, c->credit, credit)) ||
+                (rc = upload_vec(c, c->elastic, elastic)) || (rc = upload_vec(c, c->comp_again, zeros_c)) ||
+                (rc = upload_vec(c, c->comp_size, comp_size)) || (rc = upload_vec(c, c->body_comp, body_comp)) || (rc = upload_vec(c, c->rp, rp)) ||
+                (rc = upload_vec(c, c->repc, std::vector<long long>(1, 0))))
+                return rc;
+            BL_CUDA(c, c->mtg.alloc(6 * (size_t)E));
+            F.mps = c->mps.p, F.mtg = c->mtg.p, F.mflag = c->mflag.p, F.credit = c->credit.p, F.elastic = c->elastic.p;
+            F.comp_again = c->comp_again.p, F.comp_size = c->comp_size.p, F.body_comp = c->body_comp.p, F.rp = c->rp.p, F.nbody = c->B;
+            F.repc = c->repc.p;
+        }
     }
     {   // the top chain (the levels from front_level up have one column each) as one dense front, when every row of
         // its columns is a chain column and it is long enough to pay
@@ -1055,6 +1124,9 @@ static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
     int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0);
     if (c->NF > 0) {
         per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
+        // (the unload re-pass: its checks, conditions and account; its passes' kernels, which run only where a check
+        // finds an unload, are not counted - launched without a graph they always run)
+        if (c->any_plastic_members) per += c->cfg.graphs ? 5 : 3 + 2 * (1 + c->chol_launches);
         if (c->cfg.fem_solver != BL_GPU_FEM_CHOLESKY) per += 1 - c->chol_launches; // (the Cholesky runs on a fallback only)
         const bool learned = c->cfg.fem_solver == BL_GPU_FEM_PCG_LEARNED, rec = c->rec_on;
         per += (learned || rec ? 2 : 0) + (learned ? 1 : 0) + (rec ? 3 : 0);
@@ -1178,7 +1250,8 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         }
         if (c->NT > 0 && c->any_plastic) k_tri_eval<true><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         else if (c->NT > 0) k_tri_eval<false><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
-        if (c->NM > 0) k_member_eval<<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p);
+        if (c->NM > 0 && c->any_plastic_members) k_member_eval<true><<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p);
+        else if (c->NM > 0) k_member_eval<false><<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         mark();
         if (c->packed_inc)
             k_force<true><<<std::max(gfn, 1), fb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc4.p, c->ell_base.p, c->fsc.p, c->dbodies.p,
@@ -1252,6 +1325,28 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                 // (the solution, PCG's or the fallback's, is the next solve's guess)
                 cudaMemcpyAsync(c->pxprev.p, c->rhs.p, sizeof(double) * 6 * c->NF, cudaMemcpyDeviceToDevice, s);
             }
+            if (c->any_plastic_members) {
+                // the unload re-pass (frame_fem.cpp:2959-2995): where the step unloads a flowing hinge (bar, twist), its
+                // elastic tangent and the step again - assembled and factored again, at most twice; each pass under an
+                // IF node its check sets (launched without a graph, the passes run and solve the same system again)
+                auto repass = [c, &F, cholesky](cudaStream_t cs) {
+                    k_fem_assemble_all<<<(c->NF + c->NB + 127) / 128, 128, 0, cs>>>(F, c->nd.p, c->nforce.p);
+                    if (c->cfg.fem_check_residual) {
+                        cudaMemcpyAsync(c->a0d.p, c->diag.p, sizeof(double) * 36 * c->NF, cudaMemcpyDeviceToDevice, cs);
+                        cudaMemcpyAsync(c->a0o.p, c->off.p, sizeof(double) * 36 * std::max(c->NB, 1), cudaMemcpyDeviceToDevice, cs);
+                        cudaMemcpyAsync(c->b0.p, c->rhs.p, sizeof(double) * 6 * c->NF, cudaMemcpyDeviceToDevice, cs);
+                    }
+                    cholesky(cs);
+                };
+                for (int pass = 0; pass < 2; pass++) {
+                    k_member_unload<<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p, pass);
+                    cudaGraphConditionalHandle h{};
+                    const bool have = make_condition(c, s, &h);
+                    if (have) k_repass_cond<<<1, 1, 0, s>>>(c->rp.p, pass, h);
+                    enqueue_if(c, s, h, have, repass);
+                }
+                k_repass_account<<<(c->B + 127) / 128, 128, 0, s>>>(F);
+            }
             if (c->cfg.fem_check_residual) {
                 k_fem_residual<<<(c->NF + 3) / 4, 128, 0, s>>>(F, c->a0d.p, c->a0o.p, c->b0.p, c->res.p);
                 k_fem_residual_done<<<1, 1, 0, s>>>(c->res.p);
@@ -1291,9 +1386,9 @@ static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32
     }
     for (int k = 0; k < (fd.n_members > 0 ? fd.n_frame_sections : 0); k++) {
         const bl_frame_section& fs = fd.frame_sections[k];
-        if (fs.Np > 0 || fs.Mp > 0 || fs.Tp > 0) return BL_GPU_EUNSUPPORTED; // (plastic hinges, yield, buckling: not on this path)
-        if (!(fs.E > 0) || !(fs.G > 0) || !(fs.A > 0)) return BL_GPU_EINVAL;
-        fsections.push_back(FrameSectionH{fs.E, fs.G, fs.rho, fs.A, fs.Iy, fs.Iz, fs.J, fs.As_y, fs.As_z, fs.damping, fs.axial, fs.joint_k});
+        if (!(fs.E > 0) || !(fs.G > 0) || !(fs.A > 0) || fs.Np < 0 || fs.Mp < 0 || fs.Tp < 0) return BL_GPU_EINVAL;
+        fsections.push_back(FrameSectionH{fs.E, fs.G, fs.rho, fs.A, fs.Iy, fs.Iz, fs.J, fs.As_y, fs.As_z, fs.damping, fs.axial, fs.joint_k,
+                                          fs.Np, fs.Mp, fs.Tp, fs.hardening});
     }
     auto M = std::make_shared<FemModel>();
     std::vector<int> slot(n_nodes, -1);
@@ -1560,9 +1655,12 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
         for (int j = 0; j < d->n_beams; j++)
             if (on_frame[d->beams[j].a] || on_frame[d->beams[j].b]) return BL_GPU_EUNSUPPORTED;
     }
-    if (has_frame && d->allow_deform && d->allow_break)
-        for (int k = 0; d->fem->sections && k < d->fem->n_sections; k++)
-            if (d->fem->sections[k].yield > 0) return BL_GPU_EUNSUPPORTED; // (its tears and bisections: topology events)
+    if (has_frame && d->allow_deform && d->allow_break) { // (yielding: its tears, bisections and splits are topology events)
+        for (int k = 0; d->fem->n_tris > 0 && d->fem->sections && k < d->fem->n_sections; k++)
+            if (d->fem->sections[k].yield > 0) return BL_GPU_EUNSUPPORTED;
+        for (int k = 0; d->fem->n_members > 0 && d->fem->frame_sections && k < d->fem->n_frame_sections; k++)
+            if (d->fem->frame_sections[k].Np > 0) return BL_GPU_EUNSUPPORTED;
+    }
     if (c->bodies.size() >= (size_t)(1 << 23)) return BL_GPU_ELIMIT;               // (a triangle keeps its body in 23 bits)
     HostBody hb;
     hb.nodes.assign(d->nodes, d->nodes + d->n_nodes);
@@ -1964,6 +2062,11 @@ int bl_gpu_fem_stats(bl_gpu_ctx* c, bl_fem_stats* out) {
     out->pcg_solves = st[0], out->pcg_fallbacks = st[1], out->last_iterations = st[2], out->pcg_iterations = it;
     out->last_pcg_residual = last, out->max_residual = res[0], out->last_residual = res[3];
     out->columns = c->NF, out->blocks = c->NB, out->updates = c->NU, out->levels = (int64_t)c->lvl_col_ptr.size() - 1;
+    if (c->any_plastic_members) {
+        long long rp = 0;
+        BL_CUDA(c, cudaMemcpy(&rp, c->repc.p, sizeof(rp), cudaMemcpyDeviceToHost));
+        out->repasses = rp;
+    }
     return BL_GPU_OK;
 }
 

@@ -567,14 +567,21 @@ def shell_plate(n: int = 63, size: float = 1.0, origin=(0.0, 1.0, 0.0), thicknes
 
 
 def tube_section(outer: float = 0.04, wall: float = 0.003, E: float = 2.1e11, G: float = 8.1e10, rho: float = 7850.0,
-                 damping: float = 2e-5) -> dict:
-    """An elastic round steel tube's FrameSection fields (frame_fem.h:90-112): area, second moments, torsion constant,
-    Timoshenko shear areas (half the area each way)."""
+                 damping: float = 2e-5, yield_stress: float = 0.0, hardening: float = 0.25) -> dict:
+    """A round steel tube's FrameSection fields (frame_fem.h:90-112): area, second moments, torsion constant,
+    Timoshenko shear areas (half the area each way); yield_stress > 0: its plastic limits from the textbook formulas
+    for a thin tube - Np = fy A, Mp = fy Zp with the plastic modulus Zp = (D^3 - d^3) / 6, Tp = (2 pi / 3) (fy /
+    sqrt 3) (R^3 - r^3) - and the hinges' hardening."""
     ro, ri = outer / 2, outer / 2 - wall
     A = math.pi * (ro * ro - ri * ri)
     I = math.pi / 4 * (ro ** 4 - ri ** 4)
-    return {"E": E, "G": G, "rho": rho, "A": A, "Iy": I, "Iz": I, "J": 2 * I, "As_y": A / 2, "As_z": A / 2,
-            "damping": damping, "axial": 1.0, "joint_k": 2.0e4}
+    s = {"E": E, "G": G, "rho": rho, "A": A, "Iy": I, "Iz": I, "J": 2 * I, "As_y": A / 2, "As_z": A / 2,
+         "damping": damping, "axial": 1.0, "joint_k": 2.0e4}
+    if yield_stress > 0:
+        D, d = 2 * ro, 2 * ri
+        s.update({"Np": yield_stress * A, "Mp": yield_stress * (D ** 3 - d ** 3) / 6,
+                  "Tp": 2 * math.pi / 3 * (yield_stress / math.sqrt(3)) * (ro ** 3 - ri ** 3), "hardening": hardening})
+    return s
 
 
 def frame_ladder(rails: int = 12, spacing: float = 0.25, width: float = 0.6, origin=(0.0, 1.0, 0.0), load: float = 300.0,
@@ -617,8 +624,8 @@ def frame_ladder(rails: int = 12, spacing: float = 0.25, width: float = 0.6, ori
         "strength": np.zeros(0, np.float32), "deform": np.zeros(0, np.float32), "beam_type": np.zeros(0, np.uint8),
         "beam_flags": np.zeros(0, np.uint8),
         "params": {"ground_friction": 1.0, "bounce": -1.0, "contact_push_max": 2.0, "contact_slop": 0.0,
-                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 1, "ductile": 0, "can_sleep": 0,
-                   "sleep_speed": 0.0},
+                   "collision_radius": 0.05, "allow_deform": 1, "allow_break": 0 if s.get("Np", 0.0) > 0 else 1,
+                   "ductile": 0, "can_sleep": 0, "sleep_speed": 0.0},
         "frame_sections": [s], "fem_members": np.asarray(members, np.uint32),
         "member_section": np.zeros(len(members), np.uint16), "member_ends": np.asarray(ends, np.uint8),
         "member_mass": np.zeros(len(members), np.float32),

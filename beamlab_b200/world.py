@@ -301,7 +301,7 @@ FEM_TRI_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("c", "<u4"), ("section", 
 
 class _FrameSection(C.Structure):
     _fields_ = [(k, C.c_float) for k in ("E", "G", "rho", "A", "Iy", "Iz", "J", "As_y", "As_z", "damping", "axial", "joint_k",
-                                         "Np", "Mp", "Tp")]
+                                         "Np", "Mp", "Tp", "hardening")]
 
 
 # == bl_fem_member: a member between two body nodes (FemFrame::add_element), its section, the joints at its ends
@@ -368,7 +368,7 @@ class _FemStats(C.Structure):
     _fields_ = [("pcg_solves", C.c_int64), ("pcg_fallbacks", C.c_int64), ("pcg_iterations", C.c_int64),
                 ("last_iterations", C.c_int32), ("pad", C.c_int32), ("last_pcg_residual", C.c_double),
                 ("max_residual", C.c_double), ("last_residual", C.c_double), ("columns", C.c_int64),
-                ("blocks", C.c_int64), ("updates", C.c_int64), ("levels", C.c_int64)]
+                ("blocks", C.c_int64), ("updates", C.c_int64), ("levels", C.c_int64), ("repasses", C.c_int64)]
 
 
 FEM_SOLVERS = {"cholesky": 0, "pcg": 1, "pcg_learned": 2, "pcg_previous": 3}
@@ -553,7 +553,7 @@ class World:
                                                                  ("Iy", 0.0), ("Iz", 0.0), ("J", 0.0), ("As_y", 0.0),
                                                                  ("As_z", 0.0), ("damping", 2e-5), ("axial", 1.0),
                                                                  ("joint_k", 2.0e4), ("Np", 0.0), ("Mp", 0.0),
-                                                                 ("Tp", 0.0)))) for x in body.frame_sections])
+                                                                 ("Tp", 0.0), ("hardening", 0.25)))) for x in body.frame_sections])
             mems = np.ascontiguousarray(body.fem_members, FEM_MEMBER_DTYPE)
             fd = _FemDesc(len(body.fem_sections), C.cast(secs, C.c_void_p), len(tris), tris.ctypes.data if len(tris) else None,
                           float(body.fem_theta), float(body.fem_dissipation), len(body.frame_sections),

@@ -155,7 +155,7 @@ typedef struct {
     float mass;
 } bl_fem_tri;
 
-/* == the fields of bl::phys::FrameSection (frame_fem.h:90-112) the elastic member step reads */
+/* == the fields of bl::phys::FrameSection (frame_fem.h:90-112) the member step reads */
 typedef struct {
     float E, G, rho;           /* Young's and shear moduli (Pa), density (kg/m3) */
     float A, Iy, Iz, J;        /* area (m2), second moments about the local y and z axes, torsion constant (m4) */
@@ -163,8 +163,12 @@ typedef struct {
     float damping;             /* stiffness-proportional damping (s) */
     float axial;               /* a factor on the axial stiffness (1) */
     float joint_k;             /* BL_FJ_ELASTIC joints: rotational stiffness (N m/rad) */
-    float Np, Mp, Tp;          /* plastic axial force, moment, torque: 0 only (elastic); a yielding section is
-                                  BL_GPU_EUNSUPPORTED, as are a joint's damping and a mount's break force (no fields) */
+    float Np, Mp, Tp;          /* plastic axial force (N), moment and torque (N m); Np 0: elastic. On a body with
+                                  allow_deform the member yields (axial and Euler buckling, twist, radial-return hinges
+                                  at its ends, the unload re-pass); with allow_break too BL_GPU_EUNSUPPORTED (its splits
+                                  and tears are topology events this path does not make). A joint's damping and a
+                                  mount's break force have no fields. */
+    float hardening;           /* the plastic moment's growth over a hinge's first radian (0.25) */
 } bl_frame_section;
 
 /* the joints at a member's ends (FrameJoint, frame_fem.h:182-193) */
@@ -371,6 +375,8 @@ typedef struct {
     int64_t blocks;            /* off-diagonal 6 x 6 blocks, */
     int64_t updates;           /* block updates of a factorization (432 flops each), */
     int64_t levels;            /* elimination-tree levels */
+    int64_t repasses;          /* unload re-passes: the steps' systems assembled and factored again where the step
+                                  unloaded a flowing hinge, bar or twist of a yielding member */
 } bl_fem_stats;
 int bl_gpu_fem_stats(bl_gpu_ctx* ctx, bl_fem_stats* out);
 

@@ -263,10 +263,11 @@ class _FemMixin:
         nt = len(tri)
         tsec = np.ascontiguousarray(body.get("fem_tri_section", np.zeros(nt)), dtype=np.uint16)
         tmass = np.ascontiguousarray(body.get("fem_tri_mass", np.zeros(nt)), dtype=np.float32)
-        keys = ("E", "G", "rho", "A", "Iy", "Iz", "J", "As_y", "As_z", "damping", "axial", "joint_k", "Np", "Mp", "Tp")
-        dflt = {"E": 2.1e11, "G": 8.1e10, "rho": 7850.0, "damping": 2e-5, "axial": 1.0, "joint_k": 2.0e4}
+        keys = ("E", "G", "rho", "A", "Iy", "Iz", "J", "As_y", "As_z", "damping", "axial", "joint_k", "Np", "Mp", "Tp",
+                "hardening")
+        dflt = {"E": 2.1e11, "G": 8.1e10, "rho": 7850.0, "damping": 2e-5, "axial": 1.0, "joint_k": 2.0e4, "hardening": 0.25}
         fs = np.asarray([[float(sd.get(k, dflt.get(k, 0.0))) for k in keys] for sd in body.get("frame_sections", [])],
-                        np.float32).reshape(-1, 15)
+                        np.float32).reshape(-1, 16)
         ab = np.ascontiguousarray(body.get("fem_members", np.zeros((0, 2))), dtype=np.uint32).reshape(-1, 2)
         m = len(ab)
         msec = np.ascontiguousarray(body.get("member_section", np.zeros(m)), dtype=np.uint16)
@@ -285,9 +286,10 @@ class _FemMixin:
         return b
 
     def fem_info(self, body: int) -> dict:
-        o = (C.c_longlong * 7)()
+        o = (C.c_longlong * 8)()
         self._lib.ref_fem_info(self._w, body, o)
-        return dict(zip(("frame_nodes", "tris", "components", "blocks", "updates", "solve_failures", "clamps"), list(o)))
+        return dict(zip(("frame_nodes", "tris", "components", "blocks", "updates", "solve_failures", "clamps", "passes"),
+                        list(o)))
 
     def fem_pattern(self, body: int) -> dict:
         info = self.fem_info(body)

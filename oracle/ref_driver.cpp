@@ -193,8 +193,8 @@ int ref_add_plate(RefWorld* r, int n, float ox, float oy, float oz, float dux, f
 // A body with a FEM frame of members and triangles (FemFrame::add_section / add_shell_section / add_element /
 // add_tri, frame_fem.cpp:190-222; then finalize as a first step would): its nodes (SoftBody::add_node); the shell
 // sections (7 floats each: E nu rho t yield damping drill, on make_shell_section's defaults with no pattern), the
-// triangles (a, b, c, section; the mass they put on their corners); the frame sections (15 floats each: E G rho A
-// Iy Iz J As_y As_z damping axial joint_k Np Mp Tp), the members (ends, section, joints, mass); tris_first: the
+// triangles (a, b, c, section; the mass they put on their corners); the frame sections (16 floats each: E G rho A
+// Iy Iz J As_y As_z damping axial joint_k Np Mp Tp hardening), the members (ends, section, joints, mass); tris_first: the
 // add_tri calls before the add_element calls (the frame nodes numbered in the calls' order)
 int ref_add_fem_body(RefWorld* r, int n_nodes, const float* pos, const float* vel, const float* mass, const uint16_t* nflags, int n_ssec,
                      const float* ssec, int n_tris, const uint32_t* tri, const uint16_t* tsec, const float* tmass, int n_fsec, const float* fsec,
@@ -215,10 +215,10 @@ int ref_add_fem_body(RefWorld* r, int n_nodes, const float* pos, const float* ve
         b->fem.add_shell_section(s);
     }
     for (int k = 0; k < n_fsec; k++) {
-        const float* f = fsec + 15 * k;
+        const float* f = fsec + 16 * k;
         FrameSection s;
         s.E = f[0], s.G = f[1], s.rho = f[2], s.A = f[3], s.Iy = f[4], s.Iz = f[5], s.J = f[6], s.As_y = f[7], s.As_z = f[8];
-        s.damping = f[9], s.axial = f[10], s.joint_k = f[11], s.Np = f[12], s.Mp = f[13], s.Tp = f[14];
+        s.damping = f[9], s.axial = f[10], s.joint_k = f[11], s.Np = f[12], s.Mp = f[13], s.Tp = f[14], s.hardening = f[15];
         b->fem.add_section(s);
     }
     auto add_tris = [&]() {
@@ -281,6 +281,7 @@ void ref_fem_info(RefWorld* r, int body, long long* out) {
     const FemFrame& f = r->bodies[body]->fem;
     out[0] = (long long)f.node.size(), out[1] = (long long)f.tris.size(), out[2] = f.components(), out[3] = (long long)f.row_.size();
     out[4] = (long long)f.upd_.size(), out[5] = f.solve_failures, out[6] = f.clamps;
+    out[7] = f.passes_; // (the systems assembled and factored: more than one a step where a re-pass ran)
 }
 
 // the pattern itself: perm (n), col_ptr (n + 1), row (blocks), upd as (pi, pj, target) triples

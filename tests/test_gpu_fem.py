@@ -138,3 +138,46 @@ def test_gpu_yielding_section_on_a_breaking_body_is_refused():
     rig["bodies"][0]["params"]["allow_break"] = 1
     with pytest.raises(BeamLabError, match="unsupported"):
         world_from_rig(rig)
+
+
+@pytest.mark.parametrize("load,joints", [(1500.0, None), (3000.0, None), (3000.0, [(0, 0), (1, 0), (2, 3), (4, 4), (5, 5), (0, 1)])])
+def test_gpu_yielding_frame_matches_reference(ref_lib, load, joints):
+    """A ladder of yielding steel tubes (250 MPa: axial yield and Euler buckling, twist, hardening radial-return hinges
+    at the ends, the plastic rotations baked into the rest frames - eval_forces, frame_fem.cpp:1915-2054) on a body
+    that deforms and does not break, loaded past its plastic moment: the tangent of the parts that flow, and where the
+    step unloads one, its elastic tangent and the step again (frame_fem.cpp:2959-2995). 400 substeps on the GPU and by
+    the reference: the nodes within the FEM tolerance as the ladder folds metres; re-passes ran on both sides."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.frame_ladder(12, load=load, joints=joints, section=rigs.tube_section(yield_stress=2.5e8))
+    w = world_from_rig(rig)
+    ref = build_world(RefWorld, rig, multithreaded=False)
+    h = w.bodies()[0]
+    p0 = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
+    for f in range(20):
+        w.step_substeps(20)
+        ref.step_substeps(20)
+        if f in (4, 9, 19):
+            p = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
+            d = np.abs(p - ref.nodes(0)["pos"]).max()
+            assert d <= TOL, f"frame {f}: max |dp| {d:.3g} m"
+    assert np.abs(p - p0).max() > 1.0
+    ref_repasses = ref.fem_info(0)["passes"] - 400
+    assert ref_repasses > 0 and w.fem_stats()["repasses"] == ref_repasses
+    st = h.state()
+    assert st["fem_failures"] == 0 and st["fem_clamps"] == 0
+    w.close()
+
+
+def test_gpu_yielding_frame_graphs_equal_launches():
+    """The re-passes under IF nodes of the frame's graph and, launched one by one, always run (solving the same system
+    again where no hinge unloaded): the same bits."""
+    rig = rigs.frame_ladder(12, load=3000.0, section=rigs.tube_section(yield_stress=2.5e8))
+    ws = [world_from_rig(rig), world_from_rig(rig, graphs=False)]
+    for _ in range(12):
+        for w in ws:
+            w.step_substeps(20)
+    a, b = (np.ascontiguousarray(w.bodies()[0].nodes()["p"]) for w in ws)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert ws[0].fem_stats()["repasses"] > 0
+    for w in ws:
+        w.close()
