@@ -665,7 +665,7 @@ struct WheelDev {
 // 16-31) - half the bytes of the (beam | b-end bit, other end) pairs, for rigs whose warps' beams and neighbours lie
 // close enough (bl_world.cu checks every warp)
 template <bool kPacked>
-__global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
+__global__ void __launch_bounds__(256, 6) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
                                                const void* __restrict__ ell_, const int* __restrict__ ell_base, const float* __restrict__ fsc,
                                                Body* __restrict__ bodies, float gx, float gy, float gz, int nnodes, int first, NodeFem nf,
                                                float4* __restrict__ fnode, DragDev dg, WheelDev wh) {
@@ -674,11 +674,15 @@ __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd,
     float v2 = 0.0f;
     bool live = false;
     if (i < nnodes) {
+        // (the node's own loads and its warp's incidence range issued before its body's state arrives)
         const int4 inf = info[i];
+        const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
+        const int w = i >> 5, lane = i & 31;
+        const int q0 = ell_ptr[w], width = (ell_ptr[w + 1] - q0) >> 5;
+        const int base = kPacked ? ell_base[w] : 0;
         body = inf.w;
         const Body& B = bodies[body];
         if (!B.sleeping) {
-            const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
             const float m = Vv.w;
             v3 f;
             if (!B.drag) {
@@ -710,9 +714,6 @@ __global__ void __launch_bounds__(256, 5) k_force(const float4* __restrict__ nd,
             };
             // the warp's incidences, interleaved: entry q of lane l at ell[ell_ptr[w] + 32 q + l] (a warp's load reads 32
             // neighbours), each node's in beam order, padded to the warp's widest node (a multiple of 4)
-            const int w = i >> 5, lane = i & 31;
-            const int q0 = ell_ptr[w], width = (ell_ptr[w + 1] - q0) >> 5;
-            const int base = kPacked ? ell_base[w] : 0;
             for (int q = 0; q < width; q += 4) {
                 int beam[4], other[4];
                 bool pad[4], bend[4];
@@ -832,14 +833,14 @@ __global__ void __launch_bounds__(256) k_integrate(float4* __restrict__ nd, cons
     int contact = 0;
     bool live = false;
     if (i < nnodes) {
+        // (the node's own loads issued before its body's state arrives)
         const int4 inf = info[i];
+        const float4 P = nd[2 * i], Vv = nd[2 * i + 1], f4 = fnode[i];
         body = inf.w;
         const Body& B = bodies[body];
         if (!B.sleeping && !B.is_fem) {
             live = true;
-            const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
             const float m = Vv.w;
-            const float4 f4 = fnode[i];
             v3 f = V(f4.x, f4.y, f4.z);
             if (first) v2start = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
             v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
@@ -935,6 +936,7 @@ __global__ void __launch_bounds__(256) k_tyres(float4* __restrict__ nd, const in
     int i = -1;
     TyreC t = {};
     v3 f = V(0, 0, 0);
+    float4 P = make_float4(0, 0, 0, 0), Vv = P;
     bool pend = false;
     for (int c = 0; c < W.w; c += 32) {
         pend = false;
@@ -943,7 +945,8 @@ __global__ void __launch_bounds__(256) k_tyres(float4* __restrict__ nd, const in
             const float4 tf = wh.tfric[i];
             pend = tf.w != 0.0f;
             if (pend) {
-                const float4 cn = wh.tcon[i], f4 = fnode[i], Vv = nd[2 * i + 1];
+                const float4 cn = wh.tcon[i], f4 = fnode[i];
+                P = nd[2 * i], Vv = nd[2 * i + 1];
                 const int surf = __float_as_int(tf.y);
                 const GroundModel& gm = c_ground[surf < kSurfCount ? surf : 0];
                 f = V(f4.x, f4.y, f4.z);
@@ -969,7 +972,8 @@ __global__ void __launch_bounds__(256) k_tyres(float4* __restrict__ nd, const in
                 const float4 tf = wh.tfric[i];
                 pend = tf.w != 0.0f;
                 if (pend) {
-                    const float4 cn = wh.tcon[i], f4 = fnode[i], Vv = nd[2 * i + 1];
+                    const float4 cn = wh.tcon[i], f4 = fnode[i];
+                P = nd[2 * i], Vv = nd[2 * i + 1];
                     const int surf = __float_as_int(tf.y);
                     const GroundModel& gm = c_ground[surf < kSurfCount ? surf : 0];
                     f = V(f4.x, f4.y, f4.z);
@@ -981,7 +985,6 @@ __global__ void __launch_bounds__(256) k_tyres(float4* __restrict__ nd, const in
         if (!pend) continue;
         if (t.touching) f = f + (stick ? t.need : t.slide);
         wh.tfric[i].w = 0.0f;
-        const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
         v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
         float v2 = 0.0f;
         const float v2start = first ? Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z : 0.0f;
