@@ -16,6 +16,8 @@
 
 #include "bl_device.cuh"
 
+#include <type_traits>
+
 namespace blg {
 
 // ------------------------------------------------------------------------------------------ statics queries
@@ -416,25 +418,40 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // k_beams with the beam arrays staged by bulk copies: a persistent block takes every gridDim.x-th tile of kBeamTile
 // beams; kBeamStages tiles are in flight while it computes (one thread issues the copies: each tile's a/b ends, k/d,
 // state and meta words, 18 KB). The beam arrays are padded to whole tiles (pads asleep). Per beam the same
-// beam_step as k_beams.
+// beam_step as k_beams. kEnds16: each beam's ends as two 16-bit offsets from its tile's base node (tbase) in one
+// 32-bit word - 4 of the 40 bytes a beam reads - for rigs whose every tile spans fewer than 65,536 nodes (16 KB a tile).
 constexpr int kBeamTile = 512;
 constexpr int kBeamStages = 3;
 constexpr int kBeamThreads = 256;
+template <bool kEnds16>
 struct BeamStage {
     int2 ab[kBeamTile];
     float2 kd[kBeamTile];
     float4 bst[kBeamTile];
     uint32_t meta[kBeamTile];
 };
-constexpr size_t kBeamSmem = kBeamStages * sizeof(BeamStage) + kBeamStages * sizeof(uint64_t);
+template <>
+struct BeamStage<true> {
+    uint32_t ab[kBeamTile];
+    float2 kd[kBeamTile];
+    float4 bst[kBeamTile];
+    uint32_t meta[kBeamTile];
+};
+template <bool kEnds16>
+constexpr size_t beam_smem() { return kBeamStages * sizeof(BeamStage<kEnds16>) + kBeamStages * sizeof(uint64_t); }
 
-__global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
-                                                            uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold, float* __restrict__ stress,
-                                                            const int* __restrict__ bbody, float* __restrict__ fsc, const float4* __restrict__ nd,
-                                                            Body* __restrict__ bodies, int nbeams, int nbodies, int ntiles, uint32_t* __restrict__ deverr) {
+template <bool kEnds16>
+__global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const void* __restrict__ ab_, const int* __restrict__ tbase, const float2* __restrict__ kd,
+                                                            float4* __restrict__ bst, uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold,
+                                                            float* __restrict__ stress, const int* __restrict__ bbody, float* __restrict__ fsc,
+                                                            const float4* __restrict__ nd, Body* __restrict__ bodies, int nbeams, int nbodies, int ntiles,
+                                                            uint32_t* __restrict__ deverr) {
+    using Stage = BeamStage<kEnds16>;
+    using AbT = typename std::remove_reference<decltype(Stage::ab[0])>::type;
+    const AbT* ab = static_cast<const AbT*>(ab_);
     extern __shared__ __align__(128) unsigned char smem[];
-    BeamStage* stg = reinterpret_cast<BeamStage*>(smem);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kBeamStages * sizeof(BeamStage));
+    Stage* stg = reinterpret_cast<Stage*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kBeamStages * sizeof(Stage));
     const int tid = threadIdx.x;
     for (int t = blockIdx.x * kBeamThreads + tid; t < nbodies; t += gridDim.x * kBeamThreads) {
         Body& B = bodies[t]; // (this substep's bounds accumulator, for k_integrate)
@@ -450,7 +467,7 @@ __global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const int2* __restri
     auto issue = [&](int i) { // this block's i-th tile into stage i % kBeamStages
         const int s = i % kBeamStages;
         const size_t j0 = (size_t)(blockIdx.x + (size_t)i * gridDim.x) * kBeamTile;
-        mbar_expect_tx(&full[s], (uint32_t)(sizeof(BeamStage)));
+        mbar_expect_tx(&full[s], (uint32_t)(sizeof(Stage)));
         bulk_g2s(stg[s].ab, ab + j0, sizeof(stg[s].ab), &full[s]);
         bulk_g2s(stg[s].kd, kd + j0, sizeof(stg[s].kd), &full[s]);
         bulk_g2s(stg[s].bst, bst + j0, sizeof(stg[s].bst), &full[s]);
@@ -459,8 +476,11 @@ __global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const int2* __restri
     if (tid == 0)
         for (int i = 0; i < kBeamStages && i < mine; i++) issue(i);
     int issued = min(kBeamStages, mine);
+    int base_next = kEnds16 && mine > 0 ? tbase[blockIdx.x] : 0; // (each tile's base node loaded a tile ahead)
     for (int i = 0; i < mine; i++) {
         const int s = i % kBeamStages;
+        const int base = base_next;
+        if (kEnds16 && i + 1 < mine) base_next = tbase[blockIdx.x + (i + 1) * gridDim.x];
         const bool late = !mbar_wait(&full[s], (uint32_t)(i / kBeamStages) & 1u);
         if (__syncthreads_or(late)) {
             // a copy did not land in time: flag it, let the copies in flight land (bounded), stop
@@ -471,13 +491,19 @@ __global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const int2* __restri
             __syncthreads();
             return;
         }
-        const BeamStage& S = stg[s];
+        const Stage& S = stg[s];
         const int jt = (blockIdx.x + i * gridDim.x) * kBeamTile;
         const int q0 = tid, q1 = tid + kBeamThreads;
         const int j0 = jt + q0, j1 = jt + q1;
         const bool h0 = j0 < nbeams, h1 = j1 < nbeams;
         const uint32_t m0 = S.meta[q0], m1 = S.meta[q1];
-        const int2 e0 = S.ab[q0], e1 = S.ab[q1];
+        int2 e0, e1;
+        if constexpr (kEnds16) {
+            const uint32_t w0 = S.ab[q0], w1 = S.ab[q1];
+            e0 = make_int2(base + (int)(w0 & 0xffffu), base + (int)(w0 >> 16)), e1 = make_int2(base + (int)(w1 & 0xffffu), base + (int)(w1 >> 16));
+        } else {
+            e0 = S.ab[q0], e1 = S.ab[q1];
+        }
         float4 pa0 = make_float4(0, 0, 0, 0), va0 = pa0, pb0 = pa0, vb0 = pa0, pa1 = pa0, va1 = pa0, pb1 = pa0, vb1 = pa0;
         const bool g0 = h0 && !(m0 & kBeamAsleep), g1 = h1 && !(m1 & kBeamAsleep);
         if (g0) pa0 = nd[2 * e0.x], va0 = nd[2 * e0.x + 1], pb0 = nd[2 * e0.y], vb0 = nd[2 * e0.y + 1];

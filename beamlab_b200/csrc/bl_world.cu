@@ -103,6 +103,9 @@ struct bl_gpu_ctx {
     DevBuf<int> ell_base;
     int beam_tiles = 0;                        // k_beams_tma's tiles (the beam arrays hold beam_tiles * kBeamTile)
     int beam_grid = 0;                         // its persistent grid (0: not sized yet)
+    bool ends16 = false;                       // its beams' ends as 16-bit offsets from their tile's base node
+    DevBuf<uint32_t> ab16;
+    DevBuf<int> tbase;
     DevBuf<int4> info;
     DevBuf<int> inc_ptr, inc, bbody;
     DevBuf<int2> ab;
@@ -262,6 +265,7 @@ static void free_device(bl_gpu_ctx* c) {
     free_contacts(c);
     c->nd.free_(), c->bst.free_(), c->bcold.free_(), c->nodef.free_(), c->fsc.free_(), c->inc2.free_(), c->ell_ptr.free_(), c->info.free_(), c->inc_ptr.free_(), c->inc.free_();
     c->inc4.free_(), c->ell_base.free_(), c->packed_inc = false;
+    c->ab16.free_(), c->tbase.free_(), c->ends16 = false;
     c->dup.free_(), c->dpid.free_(), c->dpart.free_(), c->dpmv.free_(), c->dpacc.free_();
     c->dwheel.free_(), c->dwnodes.free_(), c->dnwheel.free_(), c->dtcon.free_(), c->dtfric.free_(), c->NW = 0;
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
@@ -1010,12 +1014,31 @@ static int commit_bodies(bl_gpu_ctx* c) {
             BL_CUDA(c, cudaMemsetAsync(c->dtfric.p, 0, sizeof(float4) * N, c->stream));
         }
     }
-    c->beam_grid = 0;
+    c->beam_grid = 0, c->ends16 = false;
     if (c->cfg.beam_kernel == 0 && M > 0) {
+        // each tile's beams' ends as 16-bit offsets from its lowest node, where every tile spans fewer than 65,536 nodes
+        std::vector<int> tbase(c->beam_tiles, 0);
+        std::vector<uint32_t> ab16(Mpad, 0u);
+        bool fits = true;
+        for (int t = 0; t < c->beam_tiles && fits; t++) {
+            const int j0 = t * kBeamTile, j1 = std::min(M, j0 + kBeamTile);
+            int lo = INT32_MAX, hi = -1;
+            for (int j = j0; j < j1; j++) lo = std::min(lo, std::min(ab[j].x, ab[j].y)), hi = std::max(hi, std::max(ab[j].x, ab[j].y));
+            if (j1 <= j0) continue;
+            fits = hi - lo < 65536;
+            tbase[t] = lo;
+            for (int j = j0; j < j1 && fits; j++) ab16[j] = (uint32_t)(ab[j].x - lo) | ((uint32_t)(ab[j].y - lo) << 16);
+        }
+        if (fits) {
+            if ((rc = upload_vec(c, c->ab16, ab16)) || (rc = upload_vec(c, c->tbase, tbase))) return rc;
+            c->ends16 = true;
+        }
         // k_beams_tma: a persistent grid of as many blocks as fit on the device at once (at most one a tile)
-        BL_CUDA(c, cudaFuncSetAttribute(k_beams_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBeamSmem));
+        const size_t smem = c->ends16 ? beam_smem<true>() : beam_smem<false>();
+        const void* fn = c->ends16 ? (const void*)k_beams_tma<true> : (const void*)k_beams_tma<false>;
+        BL_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0, sms = 0;
-        BL_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_beams_tma, kBeamThreads, kBeamSmem));
+        BL_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBeamThreads, smem));
         BL_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
         if (c->cfg.beams_per_sm > 0) per_sm = std::min(per_sm, (int)c->cfg.beams_per_sm);
         if (per_sm > 0) c->beam_grid = std::min(c->beam_tiles, per_sm * sms);
@@ -1242,8 +1265,14 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         if (c->any_drag) k_drag_parts<<<(c->B + 63) / 64, 64, 0, s>>>(c->dbodies.p, c->B, c->nd.p, c->ab.p, c->bmeta.p, dg);
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
         if (c->beam_grid > 0) {
-            k_beams_tma<<<c->beam_grid, kBeamThreads, kBeamSmem, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p,
-                                                                     c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B, c->beam_tiles, c->deverr.p);
+            if (c->ends16)
+                k_beams_tma<true><<<c->beam_grid, kBeamThreads, beam_smem<true>(), s>>>(c->ab16.p, c->tbase.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p,
+                                                                                       c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B,
+                                                                                       c->beam_tiles, c->deverr.p);
+            else
+                k_beams_tma<false><<<c->beam_grid, kBeamThreads, beam_smem<false>(), s>>>(c->ab.p, nullptr, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p,
+                                                                                         c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B,
+                                                                                         c->beam_tiles, c->deverr.p);
         } else {
             k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
                                                    c->dbodies.p, c->M, c->B);
