@@ -108,6 +108,7 @@ struct alignas(64) Body {
     int part_age;            // SoftBody::part_age_
     int part_key;            // the broken-beam count the labels were made at (the part key's only changing input here)
     int has_wheels;          // SoftBody::wheels (node tyres): their tyre patches share grip (k_tyres)
+    int has_shocks;          // SoftBody::shocks: added after its beams (k_shocks, k_force)
 };
 
 // ------------------------------------------------------------------------------------------ math in the reference's order

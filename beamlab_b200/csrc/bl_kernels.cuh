@@ -348,6 +348,116 @@ __device__ __forceinline__ void beam_step(int j, uint32_t meta, float4 s0, float
     fsc[j] = o.sc;
 }
 
+// ------------------------------------------------------------------------------------------ shocks
+// SoftBody::compute_shock_forces (softbody.cpp:472-566), a thread a shock: its model's rates for the beam's length and
+// rate (type 1 bounded, 2 progressive with soft bump stops, 3 split damping), the break test, the beam's stress, and
+// the scalar its ends add after their beams' (k_force: ssc, in the order of the shocks)
+struct ShockDev {
+    const bl_shock* sh;      // the shocks, each body's in its order (beam: the global beam)
+    const int* ptr;          // per node + 1: its shocks in sinc
+    const int2* inc;         // (shock | bit 31 where the node is the beam's b end, the other end)
+    float* ssc;              // per shock: its scalar (kNoPush: none this substep)
+};
+__global__ void k_shocks(ShockDev S, int nshocks, const int2* __restrict__ ab, const float4* __restrict__ bst, uint32_t* __restrict__ bmeta,
+                         float* __restrict__ stress, const int* __restrict__ bbody, const float4* __restrict__ nd, Body* __restrict__ bodies) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nshocks) return;
+    S.ssc[q] = kNoPush;
+    const bl_shock s = S.sh[q];
+    const int j = (int)s.beam;
+    const uint32_t meta = bmeta[j];
+    if ((meta & kBeamAsleep) || (((meta >> 8) & 0xffu) & BF_BROKEN)) return;
+    const int2 e = ab[j];
+    const float4 pa = nd[2 * e.x], va = nd[2 * e.x + 1], pb = nd[2 * e.y], vb = nd[2 * e.y + 1];
+    const v3 dis = V(pa.x - pb.x, pa.y - pb.y, pa.z - pb.z);
+    const float len2 = dot(dis, dis);
+    if (len2 < 1e-12f) return;
+    const float inv_len = 1.0f / sqrtf(len2);
+    const float len = len2 * inv_len;
+    const float4 b4 = bst[j];
+    const float L = b4.x;
+    const float diff = len - L;
+    const float v = dot(V(va.x - vb.x, va.y - vb.y, va.z - vb.z), dis) * inv_len;
+    float k, d;
+    const float lb = s.long_bound * L, sb = s.short_bound * L;
+    auto sqr = [](float x) { return x * x; };
+    if (s.type == 1) {
+        k = s.spring, d = s.damp;
+        float r = 0;
+        if (diff > lb) r = diff - lb;
+        else if (diff < -sb) r = -diff - sb;
+        if (r != 0) {
+            r = smin(r, 1.0f);
+            k += (s.bound_spring - k) * r;
+            d += (s.bound_damp - d) * r;
+        }
+    } else if (s.type == 2) {
+        auto prog = [&](bool out, float& kk, float& dd) {
+            if (out) {
+                kk = s.spring_out, dd = s.damp_out;
+                const float fr = s.long_bound != 0 ? smin(sqr(diff / (s.long_bound * L)), 1.0f) : 1.0f;
+                kk += s.prog_spring_out * kk * fr;
+                dd += s.prog_damp_out * dd * fr;
+            } else {
+                kk = s.spring_in, dd = s.damp_in;
+                const float fr = s.short_bound != 0 ? smin(sqr(diff / (s.short_bound * L)), 1.0f) : 1.0f;
+                kk += s.prog_spring_in * kk * fr;
+                dd += s.prog_damp_in * dd * fr;
+            }
+        };
+        prog(v > 0, k, d);
+        if (s.soft_bump) {
+            const float Lp = 0.8f * L, lpre = s.long_bound * Lp, spre = -s.short_bound * Lp;
+            if (diff > lpre) {
+                prog(true, k, d);
+                const float f2 = s.long_bound != 0 ? smin(sqr((diff - lpre) * 5.0f / (s.long_bound * L)), 1.0f) : 1.0f;
+                k += (k + 100) * s.prog_spring_out * f2;
+                d += (d + 100) * s.prog_damp_out * f2;
+                if (v < 0) k = s.spring_in, d = s.damp_in;
+            } else if (diff < spre) {
+                prog(false, k, d);
+                const float f2 = s.short_bound != 0 ? smin(sqr((diff - spre) * 5.0f / (s.short_bound * L)), 1.0f) : 1.0f;
+                k += (k + 100) * s.prog_spring_out * f2;
+                d += (d + 100) * s.prog_damp_out * f2;
+                if (v > 0) k = s.spring_out, d = s.damp_out;
+            }
+            if (diff > lb || diff < -sb) {
+                k = smax(k, s.bound_spring);
+                d = smax(d, s.bound_damp);
+            }
+        } else if (diff > lb || diff < -sb) {
+            k = s.bound_spring, d = s.bound_damp;
+        }
+    } else {
+        k = s.spring_in, d = s.damp_in;
+        if (diff > lb) {
+            const float r = smin(diff - lb, 1.0f);
+            k += (s.bound_spring - k) * r;
+            d += (s.bound_damp - d) * r;
+        } else if (diff < -sb) {
+            const float r = smin(-diff - sb, 1.0f);
+            k += (s.bound_spring - k) * r;
+            d += (s.bound_damp - d) * r;
+        } else if (v > 0) {
+            const float w = clampf(fabsf(v), 0.15f, 20.0f);
+            k = s.spring_out;
+            d = (s.damp_out * s.damp_out_slow * smin(w, s.split_out) + s.damp_out * s.damp_out_fast * smax(0.0f, w - s.split_out)) / w;
+        } else if (v < 0) {
+            const float w = clampf(fabsf(v), 0.15f, 20.0f);
+            k = s.spring_in;
+            d = (s.damp_in * s.damp_in_slow * smin(w, s.split_in) + s.damp_in * s.damp_in_fast * smax(0.0f, w - s.split_in)) / w;
+        }
+    }
+    const float slen = -k * diff - d * v;
+    if ((meta & BB_BREAK) && fabsf(slen) > b4.w && !(((meta >> 8) & 0xffu) & BF_NO_BREAK)) {
+        bmeta[j] = meta | ((uint32_t)BF_BROKEN << 8);
+        atomicAdd(&bodies[bbody[j]].broken_beams, 1);
+        return;
+    }
+    stress[j] = slen;
+    S.ssc[q] = slen * inv_len;
+}
+
 // Two beams a thread (j and j + blockDim.x of the block's pair of tiles): both beams' loads are issued before either
 // computes. Thread t < nbodies of the grid also resets body t's bounds accumulator for this substep's k_integrate.
 __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, const float2* __restrict__ kd, float4* __restrict__ bst,
@@ -694,7 +804,7 @@ template <bool kPacked>
 __global__ void __launch_bounds__(256, 6) k_force(const float4* __restrict__ nd, const int4* __restrict__ info, const int* __restrict__ ell_ptr,
                                                const void* __restrict__ ell_, const int* __restrict__ ell_base, const float* __restrict__ fsc,
                                                Body* __restrict__ bodies, float gx, float gy, float gz, int nnodes, int first, NodeFem nf,
-                                               float4* __restrict__ fnode, DragDev dg, WheelDev wh) {
+                                               float4* __restrict__ fnode, DragDev dg, WheelDev wh, ShockDev sk) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int body = -1;
     float v2 = 0.0f;
@@ -762,6 +872,11 @@ __global__ void __launch_bounds__(256, 6) k_force(const float4* __restrict__ nd,
 #pragma unroll
                 for (int u = 0; u < 4; u++) add(pad[u], bend[u], sc[u], Po[u]);
             }
+            if (B.has_shocks) // (compute_shock_forces after the beams: the node's shocks in their order)
+                for (int q = sk.ptr[i]; q < sk.ptr[i + 1]; q++) {
+                    const int2 e = sk.inc[q];
+                    add(false, e.x < 0, sk.ssc[e.x & 0x7fffffff], nd[2 * e.y]);
+                }
             if (B.has_wheels) { // (compute_wheel_forces, softbody.cpp:691-744: a free wheel's torque is 0, its share 0 / nodes)
                 const int2 nw = wh.nwheel[i];
                 const int4 W = nw.x >= 0 ? wh.wheel[nw.x] : make_int4(-1, -1, 0, 0);

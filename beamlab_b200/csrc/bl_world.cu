@@ -55,6 +55,7 @@ struct HostBody {
         std::vector<uint32_t> nodes;      // its tyre nodes in the given order (the parity of a place: the hub it turns about)
     };
     std::vector<Wheel> wheels;             // its free-rolling node wheels (empty: none)
+    std::vector<bl_shock> shocks;          // its shocks in their order (beam: the body's)
 };
 
 template <class T>
@@ -136,6 +137,11 @@ struct bl_gpu_ctx {
     DevBuf<int> dup, dpid, dpart;
     DevBuf<float4> dpmv, dpacc;
     int NW = 0;                                // the wheels of all bodies, and lone tyre nodes (k_tyres: a warp a wheel)
+    int NSH = 0;                               // the shocks of all bodies (k_shocks)
+    DevBuf<bl_shock> dshock;
+    DevBuf<int> sh_ptr;
+    DevBuf<int2> sh_inc;
+    DevBuf<float> ssc;
     DevBuf<int4> dwheel;
     DevBuf<int> dwnodes;
     DevBuf<int2> dnwheel;
@@ -268,6 +274,7 @@ static void free_device(bl_gpu_ctx* c) {
     c->ab16.free_(), c->tbase.free_(), c->ends16 = false;
     c->dup.free_(), c->dpid.free_(), c->dpart.free_(), c->dpmv.free_(), c->dpacc.free_();
     c->dwheel.free_(), c->dwnodes.free_(), c->dnwheel.free_(), c->dtcon.free_(), c->dtfric.free_(), c->NW = 0;
+    c->dshock.free_(), c->sh_ptr.free_(), c->sh_inc.free_(), c->ssc.free_(), c->NSH = 0;
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
 }
@@ -945,6 +952,7 @@ static int commit_bodies(bl_gpu_ctx* c) {
         c->any_ext |= recs[bi].has_ext != 0;
         any_drag |= recs[bi].drag != 0;
         recs[bi].has_wheels = c->bodies[bi].wheels.empty() ? 0 : 1;
+        recs[bi].has_shocks = c->bodies[bi].shocks.empty() ? 0 : 1;
     }
     free_device(c);
     c->N = N, c->M = M, c->B = B;
@@ -1012,6 +1020,30 @@ static int commit_bodies(bl_gpu_ctx* c) {
             BL_CUDA(c, c->dtcon.alloc(N));
             BL_CUDA(c, c->dtfric.alloc(N));
             BL_CUDA(c, cudaMemsetAsync(c->dtfric.p, 0, sizeof(float4) * N, c->stream));
+        }
+    }
+    {   // the shocks of all bodies in their order (each's beam global), and per node its shocks' incidences in that order
+        std::vector<bl_shock> sh;
+        std::vector<std::vector<int2>> per;
+        for (int bi = 0; bi < B; bi++)
+            for (const bl_shock& x : c->bodies[bi].shocks) {
+                bl_shock g = x;
+                g.beam = (uint32_t)(recs[bi].beam0 + (int)x.beam);
+                if (per.empty()) per.resize(N);
+                const int2 e = ab[g.beam], q = make_int2((int)sh.size(), 0);
+                per[e.x].push_back(make_int2(q.x, e.y)), per[e.y].push_back(make_int2((int)((uint32_t)q.x | 0x80000000u), e.x));
+                sh.push_back(g);
+            }
+        c->NSH = (int)sh.size();
+        if (c->NSH > 0) {
+            std::vector<int> ptr(N + 1, 0);
+            std::vector<int2> inc;
+            for (int i = 0; i < N; i++) {
+                inc.insert(inc.end(), per[i].begin(), per[i].end());
+                ptr[i + 1] = (int)inc.size();
+            }
+            if ((rc = upload_vec(c, c->dshock, sh)) || (rc = upload_vec(c, c->sh_ptr, ptr)) || (rc = upload_vec(c, c->sh_inc, inc))) return rc;
+            BL_CUDA(c, c->ssc.alloc(c->NSH));
         }
     }
     c->beam_grid = 0, c->ends16 = false;
@@ -1144,7 +1176,7 @@ static int ensure_committed(bl_gpu_ctx* c) {
 static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0; } // (s == 0 || s >= next_rebuild)
 
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
-    int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0);
+    int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0) + (c->NSH > 0 ? 1 : 0);
     if (c->NF > 0) {
         per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
         // (the unload re-pass: its checks, conditions and account; its passes' kernels, which run only where a check
@@ -1250,6 +1282,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     mark();
     DragDev dg{c->dup.p, c->dpid.p, c->dpart.p, c->dpmv.p, c->dpacc.p};
     WheelDev wh{c->dwheel.p, c->dwnodes.p, c->dnwheel.p, c->dtcon.p, c->dtfric.p, c->cfg.tyre_grip};
+    ShockDev sk{c->dshock.p, c->sh_ptr.p, c->sh_inc.p, c->ssc.p};
     NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p,
                 c->mon.p, c->mfa.p, c->mta.p, c->mtb.p};
     const FemDev& F = c->fd;
@@ -1277,6 +1310,8 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
                                                    c->dbodies.p, c->M, c->B);
         }
+        if (c->NSH > 0)
+            k_shocks<<<(c->NSH + 127) / 128, 128, 0, s>>>(sk, c->NSH, c->ab.p, c->bst.p, c->bmeta.p, c->stress.p, c->bbody.p, c->nd.p, c->dbodies.p);
         if (c->NT > 0 && c->any_plastic) k_tri_eval<true><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         else if (c->NT > 0) k_tri_eval<false><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
         if (c->NM > 0 && c->any_plastic_members) k_member_eval<true><<<(c->NM + 127) / 128, 128, 0, s>>>(F, c->nd.p);
@@ -1284,10 +1319,10 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         mark();
         if (c->packed_inc)
             k_force<true><<<std::max(gfn, 1), fb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc4.p, c->ell_base.p, c->fsc.p, c->dbodies.p,
-                                                         c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p, dg, wh);
+                                                         c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p, dg, wh, sk);
         else
             k_force<false><<<std::max(gfn, 1), fb, 0, s>>>(c->nd.p, c->info.p, c->ell_ptr.p, c->inc2.p, nullptr, c->fsc.p, c->dbodies.p,
-                                                          c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p, dg, wh);
+                                                          c->cfg.gravity[0], c->cfg.gravity[1], c->cfg.gravity[2], c->N, k == 0 ? 1 : 0, nfm, c->nodef.p, dg, wh, sk);
         mark();
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
@@ -1658,7 +1693,6 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
     for (int j = 0; j < d->n_beams; j++) {
         const bl_beam& b = d->beams[j];
         if (b.a >= (uint32_t)d->n_nodes || b.b >= (uint32_t)d->n_nodes || b.type > BL_BT_SUPPORT) return BL_GPU_EINVAL;
-        if (b.flags & BL_BF_SHOCK) return BL_GPU_EUNSUPPORTED; // shocks have their own force model (softbody.cpp:472-575)
     }
     if (d->n_tris < 0 || (d->n_tris > 0 && !d->tris)) return BL_GPU_EINVAL;
     for (int t = 0; t < d->n_tris; t++)
@@ -1721,6 +1755,18 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
             if (!hw.nodes.empty()) hb.wheels.push_back(std::move(hw));
         }
         if (hb.wheels.size() > 32767) return BL_GPU_ELIMIT; // (SoftBody::node_wheel: 16-bit)
+    }
+    if (d->n_shocks < 0 || (d->n_shocks > 0 && !d->shocks)) return BL_GPU_EINVAL;
+    {   // every BL_BF_SHOCK beam has its one shock, every shock a BL_BF_SHOCK beam
+        std::vector<uint8_t> seen(d->n_beams, 0);
+        for (int q = 0; q < d->n_shocks; q++) {
+            const uint32_t j = d->shocks[q].beam;
+            if (j >= (uint32_t)d->n_beams || !(d->beams[j].flags & BL_BF_SHOCK) || seen[j]++) return BL_GPU_EINVAL;
+        }
+        for (int j = 0; j < d->n_beams; j++)
+            if ((d->beams[j].flags & BL_BF_SHOCK) && !seen[j]) return BL_GPU_EINVAL;
+        if (d->n_shocks > 0 && has_frame) return BL_GPU_EUNSUPPORTED; // (shocks on frame nodes: the implicit step's springs)
+        hb.shocks.assign(d->shocks, d->shocks + d->n_shocks);
     }
     for (const bl_tri& t : hb.tris) r.hull |= t.two_sided ? 0 : 1;
     for (int i = 0; i < d->n_nodes; i++) r.contacters |= (d->info[i].flags & BL_NF_CONTACTER) ? 1 : 0;

@@ -18,6 +18,7 @@ import numpy as np
 # node flags (softbody.h:29-39) and beam types (softbody.h:60)
 NF_GROUND, NF_FIXED, NF_TYRE, NF_RIM, NF_CONTACTER = 1, 2, 4, 8, 16
 BT_NORMAL, BT_ROPE, BT_SUPPORT = 0, 1, 2
+BF_SHOCK = 1 << 6  # beam flags (softbody.h:62-69): a shock's beam
 SURF_GRASS, SURF_CONCRETE = 0, 3
 GRASS_STATIC_FRICTION = 0.80  # ground model "grass", ms (static_world.cpp:97)
 
@@ -241,15 +242,16 @@ def truss_car(seed: int = 1, speed: float = 15.0, dims=(20, 4, 5)) -> dict:
 
 def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: float = 0.2, gap: float = 0.1,
                tyre_mass: float = 0.8, hub_mass: float = 5.0, k_tyre: float = 3e5, d_tyre: float = 300.0,
-               k_hub: float = 2e6, d_hub: float = 500.0, strength: float = 1e7) -> dict:
+               k_hub: float = 2e6, d_hub: float = 500.0, strength: float = 1e7, shocks: dict | None = None) -> dict:
     """Four free-rolling wheel rings on a lattice body (lattice_body / lattice_body_fast node order): each wheel two hub
     nodes on an axle along z beside the lattice's bottom layer, a quarter of the length in from each end, `gap` m out
     from the side, `width` m apart (axle0 the one of the lesser z, as the reference's vehicle builder spawns them), and
     `rays` spokes of two tyre nodes (even: axle0's ring, odd: axle1's) at `radius` round the hubs - 24 tyre nodes a
     wheel with the 12 rays. Beams: each tyre node to both hubs, each ray's pair, the two rings, one diagonal a ray;
     each hub to the lattice's bottom nodes about its axle and the two hubs to each other. Tyre nodes: NF_GROUND |
-    NF_TYRE | NF_CONTACTER; they and the hubs move at the body's starting velocity. Appends the nodes and beams in
-    place, sets body["wheels"], returns the body."""
+    NF_TYRE | NF_CONTACTER; they and the hubs move at the body's starting velocity. shocks: a Shock's type and rates
+    (softbody.h:88-101) - the beams from each inner hub to the lattice's second layer become shocks of them (BF_SHOCK).
+    Appends the nodes and beams in place, sets body["wheels"] (and body["shocks"]), returns the body."""
     nx, ny, nz = dims
     pos = body["pos"]
     n0, m0 = len(pos), len(body["k"])
@@ -260,7 +262,11 @@ def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: flo
         new_pos.append(p), new_mass.append(m), new_flags.append(flags)
         return n0 + len(new_pos) - 1
 
-    def beam(a, b, k, d):
+    shock_beams = []
+
+    def beam(a, b, k, d, shock=False):
+        if shock:
+            shock_beams.append(len(ab))
         ab.append((a, b)), ks.append(k), ds.append(d)
 
     wheels, blocks = [], []
@@ -282,7 +288,7 @@ def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: flo
                 for jy in range(min(2, ny)):
                     ln = (jx * ny + jy) * nz + iz
                     ln_max = max(ln_max, ln)
-                    beam(ln, inner, k_hub, d_hub)
+                    beam(ln, inner, k_hub, d_hub, shock=shocks is not None and jy == 1)
                     beam(ln, outer, k_hub, d_hub)
             tyre = []
             for r in range(rays):
@@ -320,6 +326,8 @@ def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: flo
     body["beam_type"] = np.concatenate([body["beam_type"], np.zeros(m, np.uint8)])
     body["beam_flags"] = np.concatenate([body["beam_flags"], np.zeros(m, np.uint8)])
     body["wheels"] = wheels
+    sb = [m0 + q for q in shock_beams]
+    body["beam_flags"][sb] |= BF_SHOCK
     assert len(body["k"]) == m0 + m
     if np.all(np.diff(body["ab"][:m0, 0].astype(np.int64)) >= 0):
         # each wheel's nodes right after the last lattice node its hubs hold, its beams right after that node's beams:
@@ -350,17 +358,34 @@ def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: flo
         for w in wheels:
             w["axle0"], w["axle1"] = int(perm[w["axle0"]]), int(perm[w["axle1"]])
             w["nodes"] = perm[w["nodes"].astype(np.int64)].astype(np.uint32)
+        bperm = np.empty_like(border)
+        bperm[border] = np.arange(len(border))
+        sb = [int(bperm[j]) for j in sb]
+    if shocks is not None:
+        body["shocks"] = [dict(shocks, beam=j) for j in sorted(sb)]
+        assert np.count_nonzero(body["beam_flags"] & BF_SHOCK) == len(sb)
     return body
 
 
+SHOCK_TYPES = {
+    1: {"type": 1, "spring": 1.5e5, "damp": 3000.0, "short_bound": 0.1, "long_bound": 0.1, "bound_spring": 2e6},
+    2: {"type": 2, "spring_in": 1.5e5, "damp_in": 3000.0, "prog_spring_in": 0.5, "prog_damp_in": 0.5, "spring_out": 1.5e5,
+        "damp_out": 2500.0, "prog_spring_out": 0.5, "prog_damp_out": 0.5, "short_bound": 0.1, "long_bound": 0.1,
+        "bound_spring": 2e6},
+    3: {"type": 3, "spring_in": 1.5e5, "damp_in": 3000.0, "spring_out": 1.5e5, "damp_out": 3000.0, "damp_in_slow": 1.0,
+        "split_in": 0.5, "damp_in_fast": 0.5, "damp_out_slow": 1.2, "split_out": 0.5, "damp_out_fast": 0.6,
+        "short_bound": 0.1, "long_bound": 0.1, "bound_spring": 2e6},
+}
+
+
 def wheeled_car(seed: int = 1, speed: float = 12.0, yaw: float = 0.3, dims=(14, 3, 5), wall: bool = True,
-                height: float = 0.45) -> dict:
+                height: float = 0.45, shocks: dict | None = None) -> dict:
     """A lattice truss on four wheel rings (add_wheels), `height` m up over flat grass, rolling at `speed` m/s at
     `yaw` rad off +x (so its tyres slip sideways as they land) towards a concrete wall; dt = 0.5 ms."""
     rng = TRng(seed)
     vel = (speed * math.cos(yaw), 0.0, speed * math.sin(yaw))
     body = lattice_body(rng, dims=dims, origin=(-6.0, height, -0.5), velocity=vel, ground_friction=0.8 / GRASS_STATIC_FRICTION)
-    add_wheels(body, dims)
+    add_wheels(body, dims, shocks=shocks)
     front = -6.0 + (dims[0] - 1) * 0.25
     boxes = []
     if wall:

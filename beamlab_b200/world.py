@@ -146,6 +146,7 @@ class SoftBody:
         self.air_drag = 0.0                           # SoftBody::air_drag (RoR's per-node drag, against the part's mean)
         self.aero_cda = 0.0                           # SoftBody::aero_cda (Cd A on the parts' mean velocities)
         self.wheels: list[dict] = []                  # Wheel: axle0, axle1, nodes (even: axle0's ring), radius, width, mass
+        self.shocks: list[dict] = []                  # Shock: beam, type, soft_bump and the rates of SHOCK_KEYS
         self._tris: list = []
         self.tris = np.zeros(0, TRI_DTYPE)
         self.nodes = np.zeros(0, NODE_DTYPE)
@@ -236,6 +237,8 @@ class SoftBody:
             sb.fem_tris_first = bool(body.get("fem_tris_first", False))
         if "wheels" in body:
             sb.wheels = [dict(w) for w in body["wheels"]]
+        if "shocks" in body:
+            sb.shocks = [dict(x) for x in body["shocks"]]
         if "tris" in body and len(body["tris"]):
             tri = np.asarray(body["tris"], np.uint32).reshape(-1, 3)
             tr = np.zeros(len(tri), TRI_DTYPE)
@@ -326,7 +329,19 @@ class _BodyDesc(C.Structure):
                 ("collision_radius", C.c_float), ("contact_friction", C.c_float), ("hull_depth", C.c_float),
                 ("face_skin", C.c_float), ("faces_only", C.c_int32), ("collision_group", C.c_int32),
                 ("self_collision", C.c_int32), ("air_drag", C.c_float), ("aero_cda", C.c_float),
-                ("n_wheels", C.c_int32), ("wheels", C.c_void_p)]
+                ("n_wheels", C.c_int32), ("wheels", C.c_void_p), ("n_shocks", C.c_int32), ("shocks", C.c_void_p)]
+
+
+SHOCK_KEYS = ("spring", "damp", "spring_in", "damp_in", "prog_spring_in", "prog_damp_in", "spring_out", "damp_out",
+              "prog_spring_out", "prog_damp_out", "damp_in_slow", "split_in", "damp_in_fast", "damp_out_slow", "split_out",
+              "damp_out_fast", "short_bound", "long_bound", "bound_spring", "bound_damp")
+SHOCK_DEFAULTS = {"damp_in_slow": 1.0, "split_in": 1.0, "damp_in_fast": 1.0, "damp_out_slow": 1.0, "split_out": 1.0,
+                  "damp_out_fast": 1.0, "bound_spring": 9e6, "bound_damp": 12000.0}
+
+
+class _Shock(C.Structure):
+    _fields_ = [("beam", C.c_uint32), ("type", C.c_uint8), ("soft_bump", C.c_uint8), ("pad", C.c_uint16)] + \
+               [(k, C.c_float) for k in SHOCK_KEYS]
 
 
 class _Wheel(C.Structure):
@@ -582,6 +597,12 @@ class World:
             wa = (_Wheel * len(wl))(*wl)
             self._keep.append(wa)
             d.n_wheels, d.wheels = len(wl), C.cast(wa, C.c_void_p)
+        if body.shocks:
+            sa = (_Shock * len(body.shocks))(*[
+                _Shock(int(x["beam"]), int(x.get("type", 1)), int(bool(x.get("soft_bump", False))), 0,
+                       *(float(x.get(k, SHOCK_DEFAULTS.get(k, 0.0))) for k in SHOCK_KEYS)) for x in body.shocks])
+            self._keep.append(sa)
+            d.n_shocks, d.shocks = len(body.shocks), C.cast(sa, C.c_void_p)
         idx = C.c_int32()
         _check(self._L.bl_gpu_add_body(self._ctx, C.byref(d), C.byref(idx)), "add_body", self._ctx)
         h = BodyHandle(self, idx.value, len(nodes), len(beams), body.name)

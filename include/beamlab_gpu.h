@@ -216,12 +216,29 @@ typedef struct bl_wheel {
     float mass;                /* its tyre nodes' mass */
 } bl_wheel;
 
+/* A shock (Shock, softbody.h:88-101) on one of the body's beams, which carries BL_BF_SHOCK: its force model (type 1:
+ * shocks and bounded beams, 2: shocks2 with progressive rates and soft bump stops, 3: shocks3 with split damping) in
+ * place of the beam's, added to the ends after all the beams' forces, in the order of the shocks (softbody.cpp:
+ * 472-566). Every BL_BF_SHOCK beam has exactly one shock. */
+typedef struct bl_shock {
+    uint32_t beam;
+    uint8_t type;
+    uint8_t soft_bump;
+    uint16_t pad;
+    float spring, damp;
+    float spring_in, damp_in, prog_spring_in, prog_damp_in;
+    float spring_out, damp_out, prog_spring_out, prog_damp_out;
+    float damp_in_slow, split_in, damp_in_fast, damp_out_slow, split_out, damp_out_fast;
+    float short_bound, long_bound;   /* fractions of the beam's rest length */
+    float bound_spring, bound_damp;  /* the bump stops' stiffness and damping */
+} bl_shock;
+
 /* One body: a SoftBody after finalize (softbody.cpp:76-83) - its arrays and the knobs of the explicit path
  * (softbody.h:650-700), its free-rolling node wheels, and optionally its FEM frame of members and triangle elements.
- * Bodies with shocks, joints, ring tyres, driven or braked wheels, slide nodes, sheets, FEM mounts or grab are
+ * Bodies with joints, ring tyres, driven or braked wheels, slide nodes, sheets, FEM mounts or grab are
  * rejected by the caller's shim (this record has no fields for them); BL_GPU_EUNSUPPORTED here: a FEM frame whose
  * nodes collide with the static world (NF_GROUND), beams on frame nodes, yielding sections on a body that breaks, a frame with collision
- * triangles, air drag or wheels, self collision, a node on two wheels. */
+ * triangles, air drag, wheels or shocks, self collision, a node on two wheels. */
 typedef struct {
     int32_t n_nodes;
     const bl_node* nodes;
@@ -255,6 +272,8 @@ typedef struct {
     float aero_cda;            /* SoftBody::aero_cda (0: none): Cd A (m2) on each part's mean velocity, shared by mass */
     int32_t n_wheels;          /* SoftBody::wheels of node tyres (Wheel, softbody.h:468-498), free rolling: no drive */
     const struct bl_wheel* wheels; /* torque or brake; their tyre nodes (NF_TYRE) share each patch's grip */
+    int32_t n_shocks;          /* SoftBody::shocks (none on a body with a FEM frame) */
+    const struct bl_shock* shocks;
 } bl_body_desc;
 
 /* A body's runtime state (SoftBody::aabb, max_speed, sleeping, static_contacts, stats.broken_beams, sleep_timer) */

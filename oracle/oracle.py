@@ -95,6 +95,7 @@ def _load(path: str, prefix: str) -> C.CDLL:
         lib.ref_set_tyre_grip.argtypes = [vp, f]
         lib.ref_set_body_flags.argtypes = [vp, i, i, i]
         lib.ref_fem_tri_dmg.argtypes = [vp, i, vp]
+        lib.ref_add_shock.argtypes = [vp, i, C.c_uint32, i, i, fp]
         lib.ref_add_fem_body.argtypes = [vp, i, fp, fp, fp, u16p, i, fp, i, u32p, u16p, fp, i, fp, i, u32p, u16p, u8p, fp, i]
         lib.ref_add_fem_body.restype = i
         lib.ref_fem_info.argtypes = [vp, i, C.POINTER(C.c_longlong)]
@@ -106,6 +107,14 @@ def _load(path: str, prefix: str) -> C.CDLL:
         lib.ref_get_pairs.restype = i
     _loaded[path] = lib
     return lib
+
+
+# Shock's rates in ref_add_shock's order, and Shock's defaults where they are not 0 (softbody.h:88-101)
+_SHOCK_KEYS = ("spring", "damp", "spring_in", "damp_in", "prog_spring_in", "prog_damp_in", "spring_out", "damp_out",
+               "prog_spring_out", "prog_damp_out", "damp_in_slow", "split_in", "damp_in_fast", "damp_out_slow", "split_out",
+               "damp_out_fast", "short_bound", "long_bound", "bound_spring", "bound_damp")
+_SHOCK_DEFAULTS = {"damp_in_slow": 1.0, "split_in": 1.0, "damp_in_fast": 1.0, "damp_out_slow": 1.0, "split_out": 1.0,
+                   "damp_out_fast": 1.0, "bound_spring": 9e6, "bound_damp": 12000.0}
 
 
 class _OracleWorld:
@@ -180,6 +189,13 @@ class _OracleWorld:
             if self.prefix != "ref":
                 raise ValueError("air drag steps in the reference only (RefWorld)")
             self._lib.ref_set_drag(self._w, idx, float(p.get("air_drag", 0.0)), float(p.get("aero_cda", 0.0)))
+        for sh in body.get("shocks", ()):
+            if self.prefix != "ref":
+                raise ValueError("shocks step in the reference only (RefWorld)")
+            prm = np.asarray([float(sh.get(k, _SHOCK_DEFAULTS.get(k, 0.0))) for k in _SHOCK_KEYS], np.float32)
+            self._keep.append(prm)
+            self._lib.ref_add_shock(self._w, idx, int(sh["beam"]), int(sh.get("type", 1)), int(bool(sh.get("soft_bump", False))),
+                                    _ptr(prm, C.c_float))
         for wh in body.get("wheels", ()):
             if self.prefix != "ref":
                 raise ValueError("wheels step in the reference only (RefWorld)")

@@ -246,6 +246,19 @@ void ref_set_drag(RefWorld* r, int body, float air_drag, float aero_cda) {
     r->bodies[body]->aero_cda = aero_cda;
 }
 
+// A shock on one of a body's beams (Shock, softbody.h:88-101; the beam carries BF_SHOCK): type, soft bump, then 20
+// floats: spring damp spring_in damp_in prog_spring_in prog_damp_in spring_out damp_out prog_spring_out prog_damp_out
+// damp_in_slow split_in damp_in_fast damp_out_slow split_out damp_out_fast short_bound long_bound bound_spring bound_damp
+void ref_add_shock(RefWorld* r, int body, uint32_t beam, int type, int soft_bump, const float* f) {
+    Shock s;
+    s.beam = beam, s.type = (uint8_t)type, s.soft_bump = soft_bump != 0;
+    s.spring = f[0], s.damp = f[1], s.spring_in = f[2], s.damp_in = f[3], s.prog_spring_in = f[4], s.prog_damp_in = f[5];
+    s.spring_out = f[6], s.damp_out = f[7], s.prog_spring_out = f[8], s.prog_damp_out = f[9];
+    s.damp_in_slow = f[10], s.split_in = f[11], s.damp_in_fast = f[12], s.damp_out_slow = f[13], s.split_out = f[14], s.damp_out_fast = f[15];
+    s.short_bound = f[16], s.long_bound = f[17], s.bound_spring = f[18], s.bound_damp = f[19];
+    r->bodies[body]->shocks.push_back(s);
+}
+
 // SoftBody::allow_deform and allow_break of a body (softbody.h:711-712)
 void ref_set_body_flags(RefWorld* r, int body, int allow_deform, int allow_break) {
     r->bodies[body]->allow_deform = allow_deform != 0;

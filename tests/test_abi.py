@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from beamlab_b200 import _lib, rigs
-from beamlab_b200.world import BEAM_DTYPE, NODE_DTYPE, NODE_INFO_DTYPE, SoftBody, _BodyDesc, _BodyState, _Config, _Wheel, _WorldStats
+from beamlab_b200.world import BEAM_DTYPE, NODE_DTYPE, NODE_INFO_DTYPE, SoftBody, _BodyDesc, _BodyState, _Config, _Shock, _Wheel, _WorldStats
 from conftest import ROOT
 
 
@@ -30,22 +30,22 @@ def _c_layout():
     exe = src[:-2]
     with open(src, "w") as f:
         f.write('#include <stdio.h>\n#include <stddef.h>\n#include "beamlab_gpu.h"\n'
-                'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(bl_node), sizeof(bl_node_info),'
+                'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(bl_node), sizeof(bl_node_info),'
                 ' sizeof(bl_beam), sizeof(bl_body_desc), sizeof(bl_body_state), sizeof(bl_world_stats),'
                 ' sizeof(bl_gpu_config), offsetof(bl_beam, type), offsetof(bl_body_desc, ground_friction),'
-                ' sizeof(bl_wheel), offsetof(bl_body_desc, wheels));return 0;}\n')
+                ' sizeof(bl_wheel), offsetof(bl_body_desc, wheels), sizeof(bl_shock));return 0;}\n')
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
     return [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
 
 
 def test_record_layouts_match_the_header():
-    node, info, beam, desc, state, stats, cfg, off_type, off_gf, wheel, off_wheels = _c_layout()
+    node, info, beam, desc, state, stats, cfg, off_type, off_gf, wheel, off_wheels, shock = _c_layout()
     assert (node, info, beam) == (32, 20, 52)  # the reference's Node, NodeInfo, Beam
     assert NODE_DTYPE.itemsize == node and NODE_INFO_DTYPE.itemsize == info and BEAM_DTYPE.itemsize == beam
     assert C.sizeof(_BodyDesc) == desc and C.sizeof(_BodyState) == state and C.sizeof(_WorldStats) == stats
     assert C.sizeof(_Config) == cfg and BEAM_DTYPE.fields["type"][1] == off_type
     assert _BodyDesc.ground_friction.offset == off_gf
-    assert C.sizeof(_Wheel) == wheel and _BodyDesc.wheels.offset == off_wheels
+    assert C.sizeof(_Wheel) == wheel and _BodyDesc.wheels.offset == off_wheels and C.sizeof(_Shock) == shock
 
 
 def test_world_needs_a_gpu():

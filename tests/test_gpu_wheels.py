@@ -63,3 +63,33 @@ def test_gpu_wheel_rejections():
     rig["bodies"][0]["wheels"][0]["axle0"] = len(rig["bodies"][0]["mass"])
     with pytest.raises(BeamLabError, match="invalid"):
         world_from_rig(rig)
+
+
+@pytest.mark.parametrize("shock_type,soft_bump", [(1, False), (2, False), (2, True), (3, False)])
+def test_gpu_shocks_match_reference(ref_lib, shock_type, soft_bump):
+    """The wheeled car hung on shocks (three a wheel from its inner hub; SoftBody::compute_shock_forces,
+    softbody.cpp:472-566: bounded, progressive with and without soft bump stops, split damping), landing, rolling
+    and hitting the wall: node and beam states bitwise the reference's after 1,485 substeps."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.wheeled_car(shocks=dict(rigs.SHOCK_TYPES[shock_type], soft_bump=soft_bump))
+    gw = GpuWorld(rig)
+    rw = build_world(RefWorld, rig, multithreaded=False)
+    for f in range(45):
+        gw.step_substeps(33)
+        rw.step_substeps(33)
+        if f in (13, 22, 44):
+            assert_same(gw, rw, 1, f"frame {f}")
+    js = [x["beam"] for x in rig["bodies"][0]["shocks"]]
+    assert np.all(rw.beams(0)["stress"][js] != 0)  # (the shocks carry the car)
+
+
+def test_gpu_shock_rejections():
+    """A BF_SHOCK beam without its shock, or a shock on a plain beam, is refused at add_body."""
+    rig = rigs.wheeled_car(shocks=rigs.SHOCK_TYPES[1])
+    rig["bodies"][0]["shocks"] = rig["bodies"][0]["shocks"][1:]
+    with pytest.raises(BeamLabError, match="invalid"):
+        world_from_rig(rig)
+    rig = rigs.wheeled_car(shocks=rigs.SHOCK_TYPES[1])
+    rig["bodies"][0]["shocks"][0]["beam"] = 0
+    with pytest.raises(BeamLabError, match="invalid"):
+        world_from_rig(rig)
