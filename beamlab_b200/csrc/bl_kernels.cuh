@@ -790,11 +790,74 @@ __global__ void k_drag_parts(Body* __restrict__ bodies, int nbodies, const float
 struct WheelDev {
     const int4* wheel;       // axle0, axle1 (global nodes; -1: a lone tyre node's), first of its nodes in wnodes, count
     const int* wnodes;       // the wheels' tyre nodes, each wheel's ascending
-    const int2* nwheel;      // per node: (its wheel, the parity of its place in the wheel's list); (-1, 0): none
+    const int* wlist;        // ... each wheel's in the builder's order (the turn's parity, the speed's sum)
+    const int* wc_ptr;       // per node + 1: its wheel terms in wc, in wheel order
+    const int2* wc;          // (wheel, kind | parity << 2): kind 0 the wheel's turn, 1 its arm (- the reaction), 2 its
+                             // near axle node (+ the reaction)
     float4* tcon;            // per node: its static contact this substep (normal xyz, depth w), left for k_tyres
     float4* tfric;           // per node: (friction coefficient, surface, -, 1 while it waits for k_tyres)
+    float4* wst;             // per wheel: Wheel::speed, avg_speed, last_torque, last_retorque
+    const float4* wctl;      // per wheel: the controller's torque and brake, radius, mass
+    const int4* warm;        // per wheel: arm, near_attach (global; -1 none), propulsed
+    float4* wcf;             // per wheel: this substep's reaction on the arm (xyz; w 1 where it acts)
+    float* wper;             // per wheel: this substep's torque share a tyre node (torque / nodes)
+    int nreal;               // the builders' wheels (the lone tyre nodes' come after)
     float tyre_grip;         // WorldSettings::tyre_grip
 };
+
+// SoftBody::compute_wheel_forces (softbody.cpp:691-767) a thread a wheel, on the substep's starting state: the
+// controller's torque (every substep: the first short step's), the brake's stop torque against the average speed and
+// the last reaction, the share a tyre node, the tread's speed (summed in the builder's order), the average speed and
+// the reaction of the inertia, and the drive's reaction on the arm; the nodes' terms are k_force's.
+__global__ void k_wheels(const float4* __restrict__ nd, WheelDev wh, float dt) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= wh.nreal) return;
+    const int4 W = wh.wheel[w];
+    if (W.w == 0) return;
+    const float4 ctl = wh.wctl[w], st = wh.wst[w];
+    const int4 A = wh.warm[w];
+    float T = ctl.x;
+    if (ctl.y > 0) {
+        const float stop = -st.y * ctl.z * ctl.w / dt - st.w;
+        T += st.x > 0 ? clampf(stop, -ctl.y, 0.0f) : clampf(stop, 0.0f, ctl.y);
+    }
+    const float4 H0 = nd[2 * W.x], H1 = nd[2 * W.y], U0 = nd[2 * W.x + 1], U1 = nd[2 * W.y + 1];
+    const v3 axis = normalize(V(H1.x - H0.x, H1.y - H0.y, H1.z - H0.z));
+    const float per = T / (float)W.w;
+    float expected = st.x, speed = 0.0f;
+    for (int j = 0; j < W.w; j++) {
+        const int ni = wh.wlist[W.z + j];
+        const float4 hp = (j & 1) ? H1 : H0, hv = (j & 1) ? U1 : U0, P = nd[2 * ni], Vn = nd[2 * ni + 1];
+        v3 rad = V(P.x - hp.x, P.y - hp.y, P.z - hp.z);
+        const float rl2 = dot(rad, rad);
+        if (rl2 < 1e-8f) continue;
+        const float inv = 1.0f / sqrtf(rl2);
+        if (A.z == 2) rad = V(-rad.x, -rad.y, -rad.z);
+        const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
+        speed += dot(V(Vn.x - hv.x, Vn.y - hv.y, Vn.z - hv.z), dir);
+    }
+    wh.wper[w] = per;
+    const float sp = speed / (float)W.w, avg = 0.99f * st.y + 0.1f * sp;
+    float lrt = st.w;
+    if (ctl.w > 0 && ctl.z > 0) {
+        expected += (st.z / ctl.z) / ctl.w * dt;
+        lrt = ctl.w * (sp - expected) / dt;
+    }
+    float4 cf4 = make_float4(0, 0, 0, 0);
+    if (A.x >= 0 && A.y >= 0 && fabsf(T) > 0.01f) {
+        const float4 Pa = nd[2 * A.x], Pn = nd[2 * A.y];
+        const v3 rr = V(Pa.x - Pn.x, Pa.y - Pn.y, Pa.z - Pn.z);
+        v3 r = rr - axis * dot(rr, axis);
+        const float off = length(rr - r), rl = length(r);
+        if (rl > 0.01f && 2 * off < rl) {
+            r = divs(r, rl);
+            const v3 cf = V(axis.y * r.z - axis.z * r.y, axis.z * r.x - axis.x * r.z, axis.x * r.y - axis.y * r.x) * (0.5f * T / rl) * (1.0f - 2.0f * off / rl);
+            cf4 = make_float4(cf.x, cf.y, cf.z, 1.0f);
+        }
+    }
+    wh.wcf[w] = cf4;
+    wh.wst[w] = make_float4(sp, avg, T, lrt);
+}
 
 // kPacked: the incidences as 32-bit words: the beam's index less the warp's base (ell_base, bits 0-14; 0x7fff:
 // padding), bit 15 set where this node is the beam's b end, the other end's index less this node's plus 32768 (bits
@@ -877,22 +940,27 @@ __global__ void __launch_bounds__(256, 6) k_force(const float4* __restrict__ nd,
                     const int2 e = sk.inc[q];
                     add(false, e.x < 0, sk.ssc[e.x & 0x7fffffff], nd[2 * e.y]);
                 }
-            if (B.has_wheels) { // (compute_wheel_forces, softbody.cpp:691-744: a free wheel's torque is 0, its share 0 / nodes)
-                const int2 nw = wh.nwheel[i];
-                const int4 W = nw.x >= 0 ? wh.wheel[nw.x] : make_int4(-1, -1, 0, 0);
-                if (W.x >= 0) {
-                    const float4 H0 = nd[2 * W.x], H1 = nd[2 * W.y];
-                    const v3 axis = normalize(V(H1.x - H0.x, H1.y - H0.y, H1.z - H0.z));
-                    const float4 hub = nw.y ? H1 : H0;
-                    const v3 rad = V(P.x - hub.x, P.y - hub.y, P.z - hub.z);
-                    const float rl2 = dot(rad, rad);
-                    if (!(rl2 < 1e-8f)) {
-                        const float inv = 1.0f / sqrtf(rl2);
-                        const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
-                        f = f + dir * ((0.0f / (float)W.w) * inv);
+            if (B.has_wheels) // (compute_wheel_forces, softbody.cpp:691-767: the wheels' terms on this node in their order)
+                for (int q = wh.wc_ptr[i]; q < wh.wc_ptr[i + 1]; q++) {
+                    const int2 e = wh.wc[q];
+                    if ((e.y & 3) == 0) { // (a tyre node: its share of the torque along its tangent)
+                        const int4 W = wh.wheel[e.x];
+                        const float4 H0 = nd[2 * W.x], H1 = nd[2 * W.y];
+                        const v3 axis = normalize(V(H1.x - H0.x, H1.y - H0.y, H1.z - H0.z));
+                        const float4 hub = (e.y >> 2) ? H1 : H0;
+                        v3 rad = V(P.x - hub.x, P.y - hub.y, P.z - hub.z);
+                        const float rl2 = dot(rad, rad);
+                        if (!(rl2 < 1e-8f)) {
+                            const float inv = 1.0f / sqrtf(rl2);
+                            if (wh.warm[e.x].z == 2) rad = V(-rad.x, -rad.y, -rad.z);
+                            const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
+                            f = f + dir * (wh.wper[e.x] * inv);
+                        }
+                    } else { // (the arm, the near axle node: the drive's reaction)
+                        const float4 cf = wh.wcf[e.x];
+                        if (cf.w != 0.0f) f = (e.y & 3) == 1 ? f - V(cf.x, cf.y, cf.z) : f + V(cf.x, cf.y, cf.z);
                     }
                 }
-            }
             if (B.is_fem) {
                 live = true; // (its bounds and speeds after the frame's step: k_fem_integrate; the start's top speed here)
                 if (first) v2 = Vv.x * Vv.x + Vv.y * Vv.y + Vv.z * Vv.z;
@@ -1069,6 +1137,7 @@ __global__ void __launch_bounds__(256) k_tyres(float4* __restrict__ nd, const in
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= nwheels) return; // (w is the warp's: its lanes leave together)
     const int4 W = wh.wheel[w];
+    if (W.w == 0) return;
     const int body = info[wh.wnodes[W.z]].w;
     v3 need = V(0, 0, 0), mn = V(1e30f, 1e30f, 1e30f), mx = V(-1e30f, -1e30f, -1e30f);
     float cap = 0.0f, vv = 0.0f;

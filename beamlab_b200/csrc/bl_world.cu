@@ -53,8 +53,13 @@ struct HostBody {
     struct Wheel {
         uint32_t axle0, axle1;
         std::vector<uint32_t> nodes;      // its tyre nodes in the given order (the parity of a place: the hub it turns about)
+        float radius, mass;
+        int propulsed, arm, near_attach;  // (arm, near_attach: the body's nodes, -1 none)
+        float torque = 0, brake = 0;      // the controller's, every substep (bl_gpu_set_wheel_drive)
+        float st[4] = {0, 0, 0, 0};       // speed, avg_speed, last_torque, last_retorque between commits
     };
-    std::vector<Wheel> wheels;             // its free-rolling node wheels (empty: none)
+    std::vector<Wheel> wheels;             // its node wheels (empty: none)
+    int wheel0 = 0;                        // its first wheel among the context's (the last commit's)
     std::vector<bl_shock> shocks;          // its shocks in their order (beam: the body's)
 };
 
@@ -144,7 +149,12 @@ struct bl_gpu_ctx {
     DevBuf<float> ssc;
     DevBuf<int4> dwheel;
     DevBuf<int> dwnodes;
-    DevBuf<int2> dnwheel;
+    DevBuf<int> dwlist, dwc_ptr;
+    DevBuf<int2> dwc;
+    DevBuf<float4> dwst, dwctl, dwcf;
+    DevBuf<int4> dwarm;
+    DevBuf<float> dwper;
+    int NWR = 0;                               // of those, the builders' wheels (k_wheels)
     DevBuf<float4> dtcon, dtfric;
     std::vector<int> lvl_grp_ptr, lvl_col_ptr; // per level: its update groups / columns
     int64_t fem_launches = 0;                  // kernels of one substep's frame step (with the Cholesky)
@@ -273,7 +283,8 @@ static void free_device(bl_gpu_ctx* c) {
     c->inc4.free_(), c->ell_base.free_(), c->packed_inc = false;
     c->ab16.free_(), c->tbase.free_(), c->ends16 = false;
     c->dup.free_(), c->dpid.free_(), c->dpart.free_(), c->dpmv.free_(), c->dpacc.free_();
-    c->dwheel.free_(), c->dwnodes.free_(), c->dnwheel.free_(), c->dtcon.free_(), c->dtfric.free_(), c->NW = 0;
+    c->dwheel.free_(), c->dwnodes.free_(), c->dtcon.free_(), c->dtfric.free_(), c->NW = 0;
+    c->dwlist.free_(), c->dwc_ptr.free_(), c->dwc.free_(), c->dwst.free_(), c->dwctl.free_(), c->dwcf.free_(), c->dwarm.free_(), c->dwper.free_(), c->NWR = 0;
     c->dshock.free_(), c->sh_ptr.free_(), c->sh_inc.free_(), c->ssc.free_(), c->NSH = 0;
     c->bbody.free_(), c->ab.free_(), c->kd.free_(), c->bmeta.free_(), c->stress.free_(), c->dbodies.free_();
     c->rs_sort.free_(), c->rs_bad.free_(), c->rs_np.free_(), c->rs_nv.free_();
@@ -397,6 +408,15 @@ static int pull_state(bl_gpu_ctx* c) {
             HostBody& hb = c->bodies[bi];
             for (int t = 0; t < hb.rec.ntris; t++) hb.tris[t].torn = (tri[hb.rec.tri0 + t].w & TF_TORN) ? 1 : 0;
         }
+    }
+    if (c->NWR > 0) { // (the wheels' speeds and their last torques and reactions)
+        std::vector<float4> st(c->NWR);
+        BL_CUDA(c, cudaMemcpy(st.data(), c->dwst.p, sizeof(float4) * c->NWR, cudaMemcpyDeviceToHost));
+        for (HostBody& hb : c->bodies)
+            for (size_t k = 0; k < hb.wheels.size() && !hb.fem; k++) {
+                const float4 v = st[hb.wheel0 + k];
+                hb.wheels[k].st[0] = v.x, hb.wheels[k].st[1] = v.y, hb.wheels[k].st[2] = v.z, hb.wheels[k].st[3] = v.w;
+            }
     }
     // the frames' dynamic state (their positions in double, orientations, spins) and counters
     if (c->NF > 0) {
@@ -989,22 +1009,33 @@ static int commit_bodies(bl_gpu_ctx* c) {
     {   // the wheels: per wheel its hubs and its tyre nodes (ascending: the patch's sums run in node order), per node its
         // wheel and the parity of its place in the wheel's list; every other tyre node of a body without a frame a wheel
         // of its own with no hubs (a patch of one node: the same bits as its own stick test)
-        std::vector<int4> wh;
-        std::vector<int> wn;
+        std::vector<int4> wh, warm;
+        std::vector<int> wn, wl;
         std::vector<int2> nw;
+        std::vector<float4> wst, wctl;
+        std::vector<std::vector<int2>> wterm; // per node: its wheel terms in wheel order
         for (int bi = 0; bi < B; bi++) {
-            const HostBody& hb = c->bodies[bi];
+            HostBody& hb = c->bodies[bi];
+            hb.wheel0 = (int)wh.size();
             if (hb.fem) continue;
             const int n0 = recs[bi].node0;
             for (const HostBody::Wheel& w : hb.wheels) {
-                if (nw.empty()) nw.assign(N, make_int2(-1, 0));
-                const int first = (int)wn.size();
+                if (nw.empty()) nw.assign(N, make_int2(-1, 0)), wterm.resize(N);
+                const int first = (int)wn.size(), k = (int)wh.size();
                 for (size_t j = 0; j < w.nodes.size(); j++) {
-                    wn.push_back(n0 + (int)w.nodes[j]);
-                    nw[n0 + w.nodes[j]] = make_int2((int)wh.size(), (int)(j & 1));
+                    wn.push_back(n0 + (int)w.nodes[j]), wl.push_back(n0 + (int)w.nodes[j]);
+                    nw[n0 + w.nodes[j]] = make_int2(k, (int)(j & 1));
+                    wterm[n0 + w.nodes[j]].push_back(make_int2(k, (int)((j & 1) << 2)));
+                }
+                if (w.arm >= 0 && w.near_attach >= 0) {
+                    wterm[n0 + w.arm].push_back(make_int2(k, 1));
+                    wterm[n0 + w.near_attach].push_back(make_int2(k, 2));
                 }
                 std::sort(wn.begin() + first, wn.end());
                 wh.push_back(make_int4(n0 + (int)w.axle0, n0 + (int)w.axle1, first, (int)w.nodes.size()));
+                warm.push_back(make_int4(w.arm >= 0 ? n0 + w.arm : -1, w.near_attach >= 0 ? n0 + w.near_attach : -1, w.propulsed, 0));
+                wst.push_back(make_float4(w.st[0], w.st[1], w.st[2], w.st[3]));
+                wctl.push_back(make_float4(w.torque, w.brake, w.radius, w.mass));
             }
             for (int i = 0; i < recs[bi].nnodes; i++)
                 if ((hb.info[i].flags & BL_NF_TYRE) && (nw.empty() || nw[n0 + i].x < 0)) {
@@ -1014,9 +1045,22 @@ static int commit_bodies(bl_gpu_ctx* c) {
                     wn.push_back(n0 + i);
                 }
         }
-        c->NW = (int)wh.size();
+        c->NW = (int)wh.size(), c->NWR = (int)warm.size();
         if (c->NW > 0) {
-            if ((rc = upload_vec(c, c->dwheel, wh)) || (rc = upload_vec(c, c->dwnodes, wn)) || (rc = upload_vec(c, c->dnwheel, nw))) return rc;
+            std::vector<int> wc_ptr(N + 1, 0);
+            std::vector<int2> wc;
+            for (int i = 0; i < N && !wterm.empty(); i++) {
+                wc.insert(wc.end(), wterm[i].begin(), wterm[i].end());
+                wc_ptr[i + 1] = (int)wc.size();
+            }
+            if ((rc = upload_vec(c, c->dwheel, wh)) || (rc = upload_vec(c, c->dwnodes, wn)) || (rc = upload_vec(c, c->dwlist, wl)) ||
+                (rc = upload_vec(c, c->dwc_ptr, wc_ptr)) || (rc = upload_vec(c, c->dwc, wc)) || (rc = upload_vec(c, c->dwst, wst)) ||
+                (rc = upload_vec(c, c->dwctl, wctl)) || (rc = upload_vec(c, c->dwarm, warm)))
+                return rc;
+            BL_CUDA(c, c->dwcf.alloc(std::max(c->NWR, 1)));
+            BL_CUDA(c, c->dwper.alloc(std::max(c->NWR, 1)));
+            BL_CUDA(c, cudaMemsetAsync(c->dwcf.p, 0, sizeof(float4) * std::max(c->NWR, 1), c->stream));
+            BL_CUDA(c, cudaMemsetAsync(c->dwper.p, 0, sizeof(float) * std::max(c->NWR, 1), c->stream));
             BL_CUDA(c, c->dtcon.alloc(N));
             BL_CUDA(c, c->dtfric.alloc(N));
             BL_CUDA(c, cudaMemsetAsync(c->dtfric.p, 0, sizeof(float4) * N, c->stream));
@@ -1176,7 +1220,7 @@ static int ensure_committed(bl_gpu_ctx* c) {
 static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0; } // (s == 0 || s >= next_rebuild)
 
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
-    int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0) + (c->NSH > 0 ? 1 : 0);
+    int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0) + (c->NWR > 0 ? 1 : 0) + (c->NSH > 0 ? 1 : 0);
     if (c->NF > 0) {
         per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
         // (the unload re-pass: its checks, conditions and account; its passes' kernels, which run only where a check
@@ -1281,7 +1325,8 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
     k_frame_begin<<<std::max(gbody, 1), tb, 0, s>>>(c->dbodies.p, c->B, c->st, frame_time, c->cfg.sleeping, c->deverr.p);
     mark();
     DragDev dg{c->dup.p, c->dpid.p, c->dpart.p, c->dpmv.p, c->dpacc.p};
-    WheelDev wh{c->dwheel.p, c->dwnodes.p, c->dnwheel.p, c->dtcon.p, c->dtfric.p, c->cfg.tyre_grip};
+    WheelDev wh{c->dwheel.p, c->dwnodes.p, c->dwlist.p, c->dwc_ptr.p, c->dwc.p, c->dtcon.p, c->dtfric.p, c->dwst.p, c->dwctl.p,
+                c->dwarm.p, c->dwcf.p, c->dwper.p, c->NWR, c->cfg.tyre_grip};
     ShockDev sk{c->dshock.p, c->sh_ptr.p, c->sh_inc.p, c->ssc.p};
     NodeFem nfm{c->fslot.p, c->fiperm.p, c->gdiag_ptr.p, c->gdiag.p, c->ton.p, c->tf.p, c->tt.p, c->ftorque.p, c->nforce.p, c->ext.p,
                 c->mon.p, c->mfa.p, c->mta.p, c->mtb.p};
@@ -1310,6 +1355,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
                                                    c->dbodies.p, c->M, c->B);
         }
+        if (c->NWR > 0) k_wheels<<<(c->NWR + 127) / 128, 128, 0, s>>>(c->nd.p, wh, dt);
         if (c->NSH > 0)
             k_shocks<<<(c->NSH + 127) / 128, 128, 0, s>>>(sk, c->NSH, c->ab.p, c->bst.p, c->bmeta.p, c->stress.p, c->bbody.p, c->nd.p, c->dbodies.p);
         if (c->NT > 0 && c->any_plastic) k_tri_eval<true><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
@@ -1743,8 +1789,10 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
         std::vector<uint8_t> on_wheel(d->n_nodes, 0);
         for (int k = 0; k < d->n_wheels; k++) {
             const bl_wheel& w = d->wheels[k];
-            if (w.axle0 >= (uint32_t)d->n_nodes || w.axle1 >= (uint32_t)d->n_nodes || w.n_nodes < 0 || (w.n_nodes > 0 && !w.nodes)) return BL_GPU_EINVAL;
-            HostBody::Wheel hw{w.axle0, w.axle1, {}};
+            if (w.axle0 >= (uint32_t)d->n_nodes || w.axle1 >= (uint32_t)d->n_nodes || w.n_nodes < 0 || (w.n_nodes > 0 && !w.nodes) ||
+                w.propulsed < 0 || w.propulsed > 2 || w.arm < -1 || w.arm >= d->n_nodes || w.near_attach < -1 || w.near_attach >= d->n_nodes)
+                return BL_GPU_EINVAL;
+            HostBody::Wheel hw{w.axle0, w.axle1, {}, w.radius, w.mass, w.propulsed, w.arm, w.near_attach};
             for (int j = 0; j < w.n_nodes; j++) {
                 // (a node on one wheel once: the reference adds a wheel's turn per place and shares a node's patch with its
                 // last wheel only)
@@ -1752,7 +1800,7 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
                 if (on_wheel[w.nodes[j]]++) return BL_GPU_EUNSUPPORTED;
                 hw.nodes.push_back(w.nodes[j]);
             }
-            if (!hw.nodes.empty()) hb.wheels.push_back(std::move(hw));
+            hb.wheels.push_back(std::move(hw));
         }
         if (hb.wheels.size() > 32767) return BL_GPU_ELIMIT; // (SoftBody::node_wheel: 16-bit)
     }
@@ -2303,6 +2351,38 @@ int bl_gpu_download_fem(bl_gpu_ctx* c, int32_t body, int32_t* n, int32_t* node, 
             BL_CUDA(c, cudaMemcpy(tmp.data(), c->fw.p + fo, sizeof(float4) * nf, cudaMemcpyDeviceToHost));
             for (int i = 0; i < nf; i++) w[3 * i] = tmp[i].x, w[3 * i + 1] = tmp[i].y, w[3 * i + 2] = tmp[i].z;
         }
+    }
+    return BL_GPU_OK;
+}
+
+int bl_gpu_set_wheel_drive(bl_gpu_ctx* c, int32_t body, int32_t wheel, float torque, float brake) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    HostBody& hb = c->bodies[body];
+    if (wheel < 0 || wheel >= (int)hb.wheels.size() || !std::isfinite(torque) || !(brake >= 0) || !std::isfinite(brake)) return BL_GPU_EINVAL;
+    hb.wheels[wheel].torque = torque, hb.wheels[wheel].brake = brake;
+    if (c->committed && !c->bodies_dirty && c->NWR > 0) {
+        const float tb[2] = {torque, brake};
+        BL_CUDA(c, cudaSetDevice(c->cfg.device));
+        BL_CUDA(c, cudaMemcpy(c->dwctl.p + hb.wheel0 + wheel, tb, sizeof(tb), cudaMemcpyHostToDevice));
+    }
+    return BL_GPU_OK;
+}
+
+int bl_gpu_download_wheels(bl_gpu_ctx* c, int32_t body, int32_t* n, float* speed, float* avg_speed) {
+    int rc = check_body(c, body);
+    if (rc) return rc;
+    if ((rc = ensure_committed(c))) return rc;
+    const HostBody& hb = c->bodies[body];
+    const int nw = (int)hb.wheels.size();
+    if (n) *n = nw;
+    if (nw == 0 || (!speed && !avg_speed)) return BL_GPU_OK;
+    std::vector<float4> st(nw);
+    BL_CUDA(c, cudaDeviceSynchronize());
+    BL_CUDA(c, cudaMemcpy(st.data(), c->dwst.p + hb.wheel0, sizeof(float4) * nw, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < nw; k++) {
+        if (speed) speed[k] = st[k].x;
+        if (avg_speed) avg_speed[k] = st[k].y;
     }
     return BL_GPU_OK;
 }

@@ -249,7 +249,9 @@ def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: flo
     `rays` spokes of two tyre nodes (even: axle0's ring, odd: axle1's) at `radius` round the hubs - 24 tyre nodes a
     wheel with the 12 rays. Beams: each tyre node to both hubs, each ray's pair, the two rings, one diagonal a ray;
     each hub to the lattice's bottom nodes about its axle and the two hubs to each other. Tyre nodes: NF_GROUND |
-    NF_TYRE | NF_CONTACTER; they and the hubs move at the body's starting velocity. shocks: a Shock's type and rates
+    NF_TYRE | NF_CONTACTER; they and the hubs move at the body's starting velocity. The rear wheels (the lesser x) are
+    the propelled ones; each wheel's reaction arm is the lattice node over its axle, its near axle node the inner hub.
+    shocks: a Shock's type and rates
     (softbody.h:88-101) - the beams from each inner hub to the lattice's second layer become shocks of them (BF_SHOCK).
     Appends the nodes and beams in place, sets body["wheels"] (and body["shocks"]), returns the body."""
     nx, ny, nz = dims
@@ -307,8 +309,10 @@ def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: flo
                 beam(e, e2, k_tyre, d_tyre)
                 beam(o, o2, k_tyre, d_tyre)
                 beam(e, o2, k_tyre, d_tyre)
+            arm = (ix * ny + min(1, ny - 1)) * nz + iz  # (the lattice node over the axle: the drive's reaction arm)
             wheels.append({"axle0": a0, "axle1": a1, "nodes": np.asarray(tyre, np.uint32), "radius": radius,
-                           "width": width, "mass": float(np.float32(tyre_mass) * np.float32(len(tyre)))})
+                           "width": width, "mass": float(np.float32(tyre_mass) * np.float32(len(tyre))),
+                           "propulsed": 1 if ix == xs[0] else 0, "arm": arm, "near_attach": inner})
             blocks.append((ln_max, v_start, len(new_pos), b_start, len(ab)))
     k = len(new_pos)
     body["pos"] = np.concatenate([pos, np.asarray(new_pos, np.float32)]).astype(np.float32)
@@ -357,6 +361,7 @@ def add_wheels(body: dict, dims, radius: float = 0.3, rays: int = 12, width: flo
             body["tris"] = perm[np.asarray(body["tris"], np.int64)].astype(np.uint32)
         for w in wheels:
             w["axle0"], w["axle1"] = int(perm[w["axle0"]]), int(perm[w["axle1"]])
+            w["arm"], w["near_attach"] = int(perm[w["arm"]]), int(perm[w["near_attach"]])
             w["nodes"] = perm[w["nodes"].astype(np.int64)].astype(np.uint32)
         bperm = np.empty_like(border)
         bperm[border] = np.arange(len(border))

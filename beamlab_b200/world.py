@@ -346,7 +346,8 @@ class _Shock(C.Structure):
 
 class _Wheel(C.Structure):
     _fields_ = [("axle0", C.c_uint32), ("axle1", C.c_uint32), ("n_nodes", C.c_int32), ("nodes", C.c_void_p),
-                ("radius", C.c_float), ("width", C.c_float), ("mass", C.c_float)]
+                ("radius", C.c_float), ("width", C.c_float), ("mass", C.c_float), ("propulsed", C.c_int32),
+                ("arm", C.c_int32), ("near_attach", C.c_int32)]
 
 
 class _BodyState(C.Structure):
@@ -463,6 +464,20 @@ class BodyHandle:
         _check(L.bl_gpu_download_fem_tris(ctx, self.index, C.byref(n), X.ctypes.data, r0.ctypes.data, dmg.ctypes.data),
                "download_fem_tris", ctx)
         return {"X": X, "r0": r0, "dmg": dmg}
+
+    def set_wheel_drive(self, wheel: int, torque: float, brake: float = 0.0):
+        """A wheel's drive and brake torque (N m), every substep from the next on."""
+        _check(self.world._L.bl_gpu_set_wheel_drive(self.world._ctx, self.index, int(wheel), float(torque), float(brake)),
+               "set_wheel_drive", self.world._ctx)
+
+    def wheels(self) -> dict:
+        """Its wheels' tread speed (Wheel::speed, m/s) and average speed."""
+        L, ctx = self.world._L, self.world._ctx
+        n = C.c_int32()
+        _check(L.bl_gpu_download_wheels(ctx, self.index, C.byref(n), None, None), "download_wheels", ctx)
+        sp, av = np.zeros(n.value, np.float32), np.zeros(n.value, np.float32)
+        _check(L.bl_gpu_download_wheels(ctx, self.index, C.byref(n), sp.ctypes.data, av.ctypes.data), "download_wheels", ctx)
+        return {"speed": sp, "avg_speed": av}
 
     def set_node_force(self, node: int, force):
         """A constant force on one node, every substep after gravity (a SoftBody::pre_substep push)."""
@@ -593,7 +608,8 @@ class World:
                 wn = np.ascontiguousarray(wh["nodes"], np.uint32)
                 self._keep.append(wn)
                 wl.append(_Wheel(int(wh["axle0"]), int(wh["axle1"]), len(wn), wn.ctypes.data, float(wh.get("radius", 0.4)),
-                                 float(wh.get("width", 0.2)), float(wh.get("mass", 0.0))))
+                                 float(wh.get("width", 0.2)), float(wh.get("mass", 0.0)), int(wh.get("propulsed", 0)),
+                                 int(wh.get("arm", -1)), int(wh.get("near_attach", -1))))
             wa = (_Wheel * len(wl))(*wl)
             self._keep.append(wa)
             d.n_wheels, d.wheels = len(wl), C.cast(wa, C.c_void_p)

@@ -204,16 +204,17 @@ typedef struct {
 } bl_fem_desc;
 
 /* A wheel of tyre nodes (Wheel, softbody.h:468-498): its hub (axle0 on the side of the even tyre nodes, axle1) and its
- * tyre contact nodes (even: the ring on axle0's side, odd: the other), as the reference's vehicle builder makes them;
- * free rolling (no drive torque, no brake, no arm). A ring tyre (Wheel::ring) is not on this path. A node lies on one
- * wheel once (else BL_GPU_EUNSUPPORTED). radius, width and mass are the vehicle builder's record: a free wheel's
- * forces (compute_wheel_forces with no torque, the tyre patch) do not read them. */
+ * tyre contact nodes (even: the ring on axle0's side, odd: the other), as the reference's vehicle builder makes them.
+ * Its drive and brake torques come from bl_gpu_set_wheel_drive (0: free rolling). A ring tyre (Wheel::ring) is not
+ * on this path. A node lies on one wheel once (else BL_GPU_EUNSUPPORTED). */
 typedef struct bl_wheel {
     uint32_t axle0, axle1;
     int32_t n_nodes;
     const uint32_t* nodes;
     float radius, width;
-    float mass;                /* its tyre nodes' mass */
+    float mass;                /* its tyre nodes' mass (the brake's stop torque and the drive's reaction read it) */
+    int32_t propulsed;         /* 0 none, 1 forward, 2 backward (the tangent turned round) */
+    int32_t arm, near_attach;  /* the node the drive's reaction torque acts on and its nearer axle node (-1: none) */
 } bl_wheel;
 
 /* A shock (Shock, softbody.h:88-101) on one of the body's beams, which carries BL_BF_SHOCK: its force model (type 1:
@@ -234,7 +235,7 @@ typedef struct bl_shock {
 } bl_shock;
 
 /* One body: a SoftBody after finalize (softbody.cpp:76-83) - its arrays and the knobs of the explicit path
- * (softbody.h:650-700), its free-rolling node wheels, and optionally its FEM frame of members and triangle elements.
+ * (softbody.h:650-700), its node wheels and shocks, and optionally its FEM frame of members and triangle elements.
  * Bodies with joints, ring tyres, driven or braked wheels, slide nodes, sheets, FEM mounts or grab are
  * rejected by the caller's shim (this record has no fields for them); BL_GPU_EUNSUPPORTED here: a FEM frame whose
  * nodes collide with the static world (NF_GROUND), beams on frame nodes, yielding sections on a body that breaks, a frame with collision
@@ -270,8 +271,8 @@ typedef struct {
     float air_drag;            /* SoftBody::air_drag (0: none): RoR's per-node drag on the velocity against its part's
                                   mean (softbody.cpp:334-378); a body with a FEM frame takes none */
     float aero_cda;            /* SoftBody::aero_cda (0: none): Cd A (m2) on each part's mean velocity, shared by mass */
-    int32_t n_wheels;          /* SoftBody::wheels of node tyres (Wheel, softbody.h:468-498), free rolling: no drive */
-    const struct bl_wheel* wheels; /* torque or brake; their tyre nodes (NF_TYRE) share each patch's grip */
+    int32_t n_wheels;          /* SoftBody::wheels of node tyres (Wheel, softbody.h:468-498); their tyre nodes (NF_TYRE) */
+    const struct bl_wheel* wheels; /* share each patch's grip */
     int32_t n_shocks;          /* SoftBody::shocks (none on a body with a FEM frame) */
     const struct bl_shock* shocks;
 } bl_body_desc;
@@ -345,6 +346,14 @@ int bl_gpu_add_body(bl_gpu_ctx* ctx, const bl_body_desc* desc, int32_t* body_id)
 /* A constant force (N) on one node of a body, added every substep right after gravity - what a SoftBody::pre_substep
  * controller that pushes a node does (world.cpp:3261). Zero removes it. */
 int bl_gpu_set_node_force(bl_gpu_ctx* ctx, int32_t body, int32_t node, const float force[3]);
+
+/* A wheel's drive torque and brake torque (N m) from the next substep on, every substep - what a vehicle controller
+ * that sets Wheel::torque and brake in its pre_substep hook does (compute_wheel_forces, softbody.cpp:691-767: the
+ * torque spread over the tyre nodes along their tangents, the brake's stop torque, the reaction on the arm). */
+int bl_gpu_set_wheel_drive(bl_gpu_ctx* ctx, int32_t body, int32_t wheel, float torque, float brake);
+
+/* A body's wheels' Wheel::speed (the tread's tangential speed, m/s) and avg_speed; n the wheel count. Synchronous. */
+int bl_gpu_download_wheels(bl_gpu_ctx* ctx, int32_t body, int32_t* n, float* speed, float* avg_speed);
 
 /* A body's FEM frame nodes (FemFrame::node / xd / q / w, frame_fem.h:331-350): body node, double position (3),
  * orientation (x y z w), angular velocity (3); n the frame node count (0: none). Any pointer may be NULL. */

@@ -91,7 +91,9 @@ def _load(path: str, prefix: str) -> C.CDLL:
         lib.ref_add_plate.restype = i
         lib.ref_set_point_load.argtypes = [vp, i, i, f, f, f]
         lib.ref_set_drag.argtypes = [vp, i, f, f]
-        lib.ref_add_wheel.argtypes = [vp, i, C.c_uint32, C.c_uint32, u32p, i, f, f, f]
+        lib.ref_add_wheel.argtypes = [vp, i, C.c_uint32, C.c_uint32, u32p, i, f, f, f, i, i, i]
+        lib.ref_set_wheel_drive.argtypes = [vp, i, i, f, f]
+        lib.ref_wheel_state.argtypes = [vp, i, vp, vp]
         lib.ref_set_tyre_grip.argtypes = [vp, f]
         lib.ref_set_body_flags.argtypes = [vp, i, i, i]
         lib.ref_fem_tri_dmg.argtypes = [vp, i, vp]
@@ -202,7 +204,8 @@ class _OracleWorld:
             wn = np.ascontiguousarray(wh["nodes"], dtype=np.uint32)
             self._keep.append(wn)
             self._lib.ref_add_wheel(self._w, idx, int(wh["axle0"]), int(wh["axle1"]), _ptr(wn, C.c_uint32), len(wn),
-                                    float(wh.get("radius", 0.4)), float(wh.get("width", 0.2)), float(wh.get("mass", 0.0)))
+                                    float(wh.get("radius", 0.4)), float(wh.get("width", 0.2)), float(wh.get("mass", 0.0)),
+                                    int(wh.get("propulsed", 0)), int(wh.get("arm", -1)), int(wh.get("near_attach", -1)))
         if self.prefix == "ref" and len(tris) and "tri_two_sided" in body:
             sides = np.ascontiguousarray(body["tri_two_sided"], dtype=np.uint8)
             self._keep.append(sides)
@@ -211,6 +214,16 @@ class _OracleWorld:
 
     def step_substeps(self, n: int):
         self._fn("step_substeps")(self._w, int(n))
+
+    def set_wheel_drive(self, body: int, wheel: int, torque: float, brake: float):
+        """A wheel's drive and brake torque (N m), set every substep from now on (RefWorld only)."""
+        self._lib.ref_set_wheel_drive(self._w, body, wheel, float(torque), float(brake))
+
+    def wheels(self, body: int, n: int) -> dict:
+        """The first n wheels' speed and average speed (RefWorld only)."""
+        sp, av = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self._lib.ref_wheel_state(self._w, body, sp.ctypes.data, av.ctypes.data)
+        return {"speed": sp, "avg_speed": av}
 
     def nodes(self, body: int):
         n = self._fn("body_nodes")(self._w, body)

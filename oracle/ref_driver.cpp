@@ -39,7 +39,20 @@ struct RefWorld {
     World w;
     std::vector<SoftBody*> bodies;
     std::map<int, std::vector<std::pair<uint32_t, vec3>>> loads; // the constant node loads of each body
+    std::map<int, std::map<int, std::pair<float, float>>> drives; // each body's wheels' torque and brake (N m)
 };
+
+// a body's one pre_substep (the controller hook, world.cpp:3261): its wheels' torque and brake set, its loads added
+static void install_pre_substep(RefWorld* r, int body) {
+    const std::vector<std::pair<uint32_t, vec3>> all = r->loads[body];
+    const std::map<int, std::pair<float, float>> drv = r->drives[body];
+    r->bodies[body]->pre_substep = [all, drv](SoftBody& sb, float) {
+        for (const auto& [k, tb] : drv)
+            if (k < (int)sb.wheels.size()) sb.wheels[k].torque = tb.first, sb.wheels[k].brake = tb.second;
+        for (const auto& [nd, f] : all)
+            if (nd < sb.force.size()) sb.force[nd] += f;
+    };
+}
 
 // per-body knobs of SoftBody that the GPU path supports (softbody.h:650-700)
 struct RefBodyParams {
@@ -265,28 +278,32 @@ void ref_set_body_flags(RefWorld* r, int body, int allow_deform, int allow_break
     r->bodies[body]->allow_break = allow_break != 0;
 }
 
-// A free-rolling wheel of tyre nodes on a body (Wheel, softbody.h:468-498): its hubs, its tyre nodes (even: axle0's
-// side), radius, width and mass, as the vehicle builder fills them; no torque, no brake, no arm
-void ref_add_wheel(RefWorld* r, int body, uint32_t axle0, uint32_t axle1, const uint32_t* nodes, int n, float radius, float width, float mass) {
+// A wheel of tyre nodes on a body (Wheel, softbody.h:468-498): its hubs, its tyre nodes (even: axle0's side), radius,
+// width, mass, propulsion (0 none, 1 forward, 2 backward) and arm (the reaction torque's arm node and its nearer axle
+// node; -1: none), as the vehicle builder fills them
+void ref_add_wheel(RefWorld* r, int body, uint32_t axle0, uint32_t axle1, const uint32_t* nodes, int n, float radius, float width, float mass,
+                   int propulsed, int arm, int near_attach) {
     Wheel w;
     w.axle0 = axle0, w.axle1 = axle1;
     w.nodes.assign(nodes, nodes + n);
     w.radius = radius, w.width = width, w.mass = mass;
+    w.propulsed = propulsed, w.arm = arm, w.near_attach = near_attach;
     r->bodies[body]->wheels.push_back(w);
 }
 
 // A constant force on one node of a body, applied every substep right after gravity (the SoftBody::pre_substep hook,
 // world.cpp:3261)
 void ref_set_point_load(RefWorld* r, int body, int node, float fx, float fy, float fz) {
-    SoftBody* b = r->bodies[body];
     // (every load of the body in one callback: a body has one pre_substep)
-    auto& loads = r->loads[body];
-    loads.push_back({(uint32_t)node, vec3(fx, fy, fz)});
-    const std::vector<std::pair<uint32_t, vec3>> all = loads;
-    b->pre_substep = [all](SoftBody& sb, float) {
-        for (const auto& [nd, f] : all)
-            if (nd < sb.force.size()) sb.force[nd] += f;
-    };
+    r->loads[body].push_back({(uint32_t)node, vec3(fx, fy, fz)});
+    install_pre_substep(r, body);
+}
+
+// A wheel's drive torque and brake torque (N m), set by the controller hook every substep from now on (a vehicle
+// controller's differential output and brake, as the truck controller sets Wheel::torque and brake)
+void ref_set_wheel_drive(RefWorld* r, int body, int wheel, float torque, float brake) {
+    r->drives[body][wheel] = {torque, brake};
+    install_pre_substep(r, body);
 }
 
 // the frame's pattern sizes: [frame nodes, tris, components, off-diagonal blocks, block updates, solve failures, clamps]
@@ -329,6 +346,12 @@ void ref_fem_tris(RefWorld* r, int body, int* n, float* X, float* r0, float* mas
         }
         mass[t] = tr.mass, area0[t] = tr.area0;
     }
+}
+
+// each wheel's Wheel::speed and avg_speed
+void ref_wheel_state(RefWorld* r, int body, float* speed, float* avg_speed) {
+    const SoftBody* b = r->bodies[body];
+    for (size_t k = 0; k < b->wheels.size(); k++) speed[k] = b->wheels[k].speed, avg_speed[k] = b->wheels[k].avg_speed;
 }
 
 // FrameTri::dmg of each triangle (the plastic stretch reached)

@@ -93,3 +93,33 @@ def test_gpu_shock_rejections():
     rig["bodies"][0]["shocks"][0]["beam"] = 0
     with pytest.raises(BeamLabError, match="invalid"):
         world_from_rig(rig)
+
+
+@pytest.mark.parametrize("torque,brake", [(400.0, 1500.0), (-300.0, 600.0)])
+def test_gpu_driven_wheels_match_reference(ref_lib, torque, brake):
+    """The wheeled car (no wall) driven: its rear wheels' torque spread over their tyre nodes along their tangents with
+    the reaction on their arms, then every wheel braked (the stop torque against the average speed and the last
+    reaction) - SoftBody::compute_wheel_forces, softbody.cpp:691-767, with the controller setting torque and brake every
+    substep. Node and beam states and the wheels' speeds bitwise the reference's."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.wheeled_car(speed=4.0, yaw=0.0, wall=False)
+    gw = GpuWorld(rig)
+    rw = build_world(RefWorld, rig, multithreaded=False)
+    h = gw.h[0]
+    wheels = rig["bodies"][0]["wheels"]
+    top = 0.0
+    for f in range(50):
+        if f in (0, 30):
+            for k, w in enumerate(wheels):
+                t, b = (torque if w["propulsed"] else 0.0, 0.0) if f == 0 else (0.0, brake)
+                h.set_wheel_drive(k, t, b)
+                rw.set_wheel_drive(0, k, t, b)
+        gw.step_substeps(33)
+        rw.step_substeps(33)
+        if f in (12, 29, 49):
+            assert_same(gw, rw, 1, f"frame {f}")
+            gs, rs = h.wheels(), rw.wheels(0, len(wheels))
+            assert np.array_equal(gs["speed"].view(np.uint32), rs["speed"].view(np.uint32)), f"frame {f}: wheel speeds"
+            assert np.array_equal(gs["avg_speed"].view(np.uint32), rs["avg_speed"].view(np.uint32))
+            top = max(top, float(np.abs(rs["speed"]).max()))
+    assert top > 5.0  # (the driven wheels spun up before the brakes held them)
