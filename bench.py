@@ -236,6 +236,20 @@ def dist_setup():
     return ws, rank, local
 
 
+def aggregate(ms: float, ms_e2e: float, n_nodes: int, ws: int, device="cuda"):
+    """The whole job's figures over the ranks: the slowest rank's timed regions (resident, end to end) and the nodes
+    every rank stepped (each rank its own fleet: weak scaling, no data-path collective)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=device)
+    units = torch.tensor([float(n_nodes)], dtype=torch.float64, device=device)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(units, op=dist.ReduceOp.SUM)
+        dist.barrier()
+    return float(t[0]), float(t[1]), float(units[0])
+
+
 def run_reference(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
@@ -336,14 +350,7 @@ def run_gpu(args):
     ms_e2e = f0.elapsed_time(f1)
     clk = clocks.stop()
 
-    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
-    units = torch.tensor([float(n)], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(units, op=dist.ReduceOp.SUM)
-        dist.barrier()
-    ms, ms_e2e = float(t[0]), float(t[1])
-    total_nodes = float(units[0])
+    ms, ms_e2e, total_nodes = aggregate(ms, ms_e2e, n, ws, "cuda")
     if rank == 0:
         value = total_nodes * FRAME * K / (ms * 1e-3)
         e2e = total_nodes * FRAME * K / (ms_e2e * 1e-3)
