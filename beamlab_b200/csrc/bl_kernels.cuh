@@ -805,15 +805,16 @@ struct WheelDev {
     float tyre_grip;         // WorldSettings::tyre_grip
 };
 
-// SoftBody::compute_wheel_forces (softbody.cpp:691-767) a thread a wheel, on the substep's starting state: the
+// SoftBody::compute_wheel_forces (softbody.cpp:691-767) a warp a wheel, on the substep's starting state: the
 // controller's torque (every substep: the first short step's), the brake's stop torque against the average speed and
 // the last reaction, the share a tyre node, the tread's speed (summed in the builder's order), the average speed and
 // the reaction of the inertia, and the drive's reaction on the arm; the nodes' terms are k_force's.
-__global__ void k_wheels(const float4* __restrict__ nd, WheelDev wh, float dt) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= wh.nreal) return;
+__global__ void __launch_bounds__(256) k_wheels(const float4* __restrict__ nd, const int4* __restrict__ info, const Body* __restrict__ bodies,
+                                                WheelDev wh, float dt) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= wh.nreal) return; // (w is the warp's: its lanes leave together)
     const int4 W = wh.wheel[w];
-    if (W.w == 0) return;
+    if (W.w == 0 || bodies[info[W.x].w].sleeping) return; // (an asleep body's forces are not made)
     const float4 ctl = wh.wctl[w], st = wh.wst[w];
     const int4 A = wh.warm[w];
     float T = ctl.x;
@@ -825,17 +826,26 @@ __global__ void k_wheels(const float4* __restrict__ nd, WheelDev wh, float dt) {
     const v3 axis = normalize(V(H1.x - H0.x, H1.y - H0.y, H1.z - H0.z));
     const float per = T / (float)W.w;
     float expected = st.x, speed = 0.0f;
-    for (int j = 0; j < W.w; j++) {
-        const int ni = wh.wlist[W.z + j];
-        const float4 hp = (j & 1) ? H1 : H0, hv = (j & 1) ? U1 : U0, P = nd[2 * ni], Vn = nd[2 * ni + 1];
-        v3 rad = V(P.x - hp.x, P.y - hp.y, P.z - hp.z);
-        const float rl2 = dot(rad, rad);
-        if (rl2 < 1e-8f) continue;
-        const float inv = 1.0f / sqrtf(rl2);
-        if (A.z == 2) rad = V(-rad.x, -rad.y, -rad.z);
-        const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
-        speed += dot(V(Vn.x - hv.x, Vn.y - hv.y, Vn.z - hv.z), dir);
+    // (a lane a node: each node's term, then the sum in the builder's order by broadcasts)
+    for (int c = 0; c < W.w; c += 32) {
+        const int j = c + lane;
+        float term = 0.0f;
+        bool has = false;
+        if (j < W.w) {
+            const int ni = wh.wlist[W.z + j];
+            const float4 hp = (j & 1) ? H1 : H0, hv = (j & 1) ? U1 : U0, P = nd[2 * ni], Vn = nd[2 * ni + 1];
+            v3 rad = V(P.x - hp.x, P.y - hp.y, P.z - hp.z);
+            const float rl2 = dot(rad, rad);
+            if (!(rl2 < 1e-8f)) {
+                const float inv = 1.0f / sqrtf(rl2);
+                if (A.z == 2) rad = V(-rad.x, -rad.y, -rad.z);
+                const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
+                term = dot(V(Vn.x - hv.x, Vn.y - hv.y, Vn.z - hv.z), dir), has = true;
+            }
+        }
+        for (unsigned m = __ballot_sync(0xffffffffu, has); m; m &= m - 1) speed += __shfl_sync(0xffffffffu, term, __ffs(m) - 1);
     }
+    if (lane != 0) return;
     wh.wper[w] = per;
     const float sp = speed / (float)W.w, avg = 0.99f * st.y + 0.1f * sp;
     float lrt = st.w;

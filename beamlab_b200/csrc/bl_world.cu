@@ -1355,7 +1355,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
                                                    c->dbodies.p, c->M, c->B);
         }
-        if (c->NWR > 0) k_wheels<<<(c->NWR + 127) / 128, 128, 0, s>>>(c->nd.p, wh, dt);
+        if (c->NWR > 0) k_wheels<<<(c->NWR + 7) / 8, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, wh, dt);
         if (c->NSH > 0)
             k_shocks<<<(c->NSH + 127) / 128, 128, 0, s>>>(sk, c->NSH, c->ab.p, c->bst.p, c->bmeta.p, c->stress.p, c->bbody.p, c->nd.p, c->dbodies.p);
         if (c->NT > 0 && c->any_plastic) k_tri_eval<true><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
