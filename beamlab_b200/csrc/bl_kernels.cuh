@@ -525,6 +525,93 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     }
 }
 
+// A tyre node on no wheel is a patch of its own: a wheel of one node with no hubs (axle0 -1), which gives the same bits
+// (its sums are its own need and cap).
+struct WheelDev {
+    const int4* wheel;       // axle0, axle1 (global nodes; -1: a lone tyre node's), first of its nodes in wnodes, count
+    const int* wnodes;       // the wheels' tyre nodes, each wheel's ascending
+    const int* wlist;        // ... each wheel's in the builder's order (the turn's parity, the speed's sum)
+    const int* wc_ptr;       // per node + 1: its wheel terms in wc, in wheel order
+    const int2* wc;          // (wheel, kind | parity << 2): kind 0 the wheel's turn, 1 its arm (- the reaction), 2 its
+                             // near axle node (+ the reaction)
+    float4* tcon;            // per node: its static contact this substep (normal xyz, depth w), left for k_tyres
+    float4* tfric;           // per node: (friction coefficient, surface, -, 1 while it waits for k_tyres)
+    float4* wst;             // per wheel: Wheel::speed, avg_speed, last_torque, last_retorque
+    const float4* wctl;      // per wheel: the controller's torque and brake, radius, mass
+    const int4* warm;        // per wheel: arm, near_attach (global; -1 none), propulsed
+    float4* wcf;             // per wheel: this substep's reaction on the arm (xyz; w 1 where it acts)
+    float* wper;             // per wheel: this substep's torque share a tyre node (torque / nodes)
+    int nreal;               // the builders' wheels (the lone tyre nodes' come after)
+    float tyre_grip;         // WorldSettings::tyre_grip
+};
+
+// SoftBody::compute_wheel_forces (softbody.cpp:691-767) a warp a wheel, on the substep's starting state: the
+// controller's torque (every substep: the first short step's), the brake's stop torque against the average speed and
+// the last reaction, the share a tyre node, the tread's speed (summed in the builder's order), the average speed and
+// the reaction of the inertia, and the drive's reaction on the arm; the nodes' terms are k_force's.
+__device__ void wheel_step(int w, int lane, const float4* __restrict__ nd, const int4* __restrict__ info, const Body* __restrict__ bodies,
+                           const WheelDev& wh, float dt) {
+    const int4 W = wh.wheel[w];
+    if (W.w == 0 || bodies[info[W.x].w].sleeping) return; // (an asleep body's forces are not made)
+    const float4 ctl = wh.wctl[w], st = wh.wst[w];
+    const int4 A = wh.warm[w];
+    float T = ctl.x;
+    if (ctl.y > 0) {
+        const float stop = -st.y * ctl.z * ctl.w / dt - st.w;
+        T += st.x > 0 ? clampf(stop, -ctl.y, 0.0f) : clampf(stop, 0.0f, ctl.y);
+    }
+    const float4 H0 = nd[2 * W.x], H1 = nd[2 * W.y], U0 = nd[2 * W.x + 1], U1 = nd[2 * W.y + 1];
+    const v3 axis = normalize(V(H1.x - H0.x, H1.y - H0.y, H1.z - H0.z));
+    const float per = T / (float)W.w;
+    float expected = st.x, speed = 0.0f;
+    // (a lane a node: each node's term, then the sum in the builder's order by broadcasts)
+    for (int c = 0; c < W.w; c += 32) {
+        const int j = c + lane;
+        float term = 0.0f;
+        bool has = false;
+        if (j < W.w) {
+            const int ni = wh.wlist[W.z + j];
+            const float4 hp = (j & 1) ? H1 : H0, hv = (j & 1) ? U1 : U0, P = nd[2 * ni], Vn = nd[2 * ni + 1];
+            v3 rad = V(P.x - hp.x, P.y - hp.y, P.z - hp.z);
+            const float rl2 = dot(rad, rad);
+            if (!(rl2 < 1e-8f)) {
+                const float inv = 1.0f / sqrtf(rl2);
+                if (A.z == 2) rad = V(-rad.x, -rad.y, -rad.z);
+                const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
+                term = dot(V(Vn.x - hv.x, Vn.y - hv.y, Vn.z - hv.z), dir), has = true;
+            }
+        }
+        for (unsigned m = __ballot_sync(0xffffffffu, has); m; m &= m - 1) speed += __shfl_sync(0xffffffffu, term, __ffs(m) - 1);
+    }
+    if (lane != 0) return;
+    wh.wper[w] = per;
+    const float sp = speed / (float)W.w, avg = 0.99f * st.y + 0.1f * sp;
+    float lrt = st.w;
+    if (ctl.w > 0 && ctl.z > 0) {
+        expected += (st.z / ctl.z) / ctl.w * dt;
+        lrt = ctl.w * (sp - expected) / dt;
+    }
+    float4 cf4 = make_float4(0, 0, 0, 0);
+    if (A.x >= 0 && A.y >= 0 && fabsf(T) > 0.01f) {
+        const float4 Pa = nd[2 * A.x], Pn = nd[2 * A.y];
+        const v3 rr = V(Pa.x - Pn.x, Pa.y - Pn.y, Pa.z - Pn.z);
+        v3 r = rr - axis * dot(rr, axis);
+        const float off = length(rr - r), rl = length(r);
+        if (rl > 0.01f && 2 * off < rl) {
+            r = divs(r, rl);
+            const v3 cf = V(axis.y * r.z - axis.z * r.y, axis.z * r.x - axis.x * r.z, axis.x * r.y - axis.y * r.x) * (0.5f * T / rl) * (1.0f - 2.0f * off / rl);
+            cf4 = make_float4(cf.x, cf.y, cf.z, 1.0f);
+        }
+    }
+    wh.wcf[w] = cf4;
+    wh.wst[w] = make_float4(sp, avg, T, lrt);
+}
+__global__ void __launch_bounds__(256) k_wheels(const float4* __restrict__ nd, const int4* __restrict__ info, const Body* __restrict__ bodies,
+                                                WheelDev wh, float dt) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w < wh.nreal) wheel_step(w, threadIdx.x & 31, nd, info, bodies, wh, dt); // (w is the warp's: its lanes go together)
+}
+
 // k_beams with the beam arrays staged by bulk copies: a persistent block takes every gridDim.x-th tile of kBeamTile
 // beams; kBeamStages tiles are in flight while it computes (one thread issues the copies: each tile's a/b ends, k/d,
 // state and meta words, 18 KB). The beam arrays are padded to whole tiles (pads asleep). Per beam the same
@@ -555,7 +642,7 @@ __global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const void* __restri
                                                             float4* __restrict__ bst, uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold,
                                                             float* __restrict__ stress, const int* __restrict__ bbody, float* __restrict__ fsc,
                                                             const float4* __restrict__ nd, Body* __restrict__ bodies, int nbeams, int nbodies, int ntiles,
-                                                            uint32_t* __restrict__ deverr) {
+                                                            uint32_t* __restrict__ deverr, const int4* __restrict__ info, WheelDev wh, float dt) {
     using Stage = BeamStage<kEnds16>;
     using AbT = typename std::remove_reference<decltype(Stage::ab[0])>::type;
     const AbT* ab = static_cast<const AbT*>(ab_);
@@ -627,6 +714,10 @@ __global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const void* __restri
         }
         issued = min(issued + 1, mine);
     }
+    // then the wheels (k_wheels' work, a warp a wheel: it reads the substep's starting state as the beams do, and only
+    // k_force reads what it writes)
+    for (int w = blockIdx.x * (kBeamThreads / 32) + (tid >> 5); w < wh.nreal; w += gridDim.x * (kBeamThreads / 32))
+        wheel_step(w, tid & 31, nd, info, bodies, wh, dt);
 }
 
 // The frame bodies' gather (NodeFem): their nodes' forces go to the frame's implicit step
@@ -785,90 +876,6 @@ __global__ void k_drag_parts(Body* __restrict__ bodies, int nbodies, const float
 // The wheels of node tyres (Wheel, softbody.h:468-498), free rolling: per wheel its hub nodes and its tyre nodes in
 // ascending order (the order the tyre patch's sums run in, world.cpp:871-898); per node its wheel and the parity of
 // its place in the wheel's list (the hub it turns about); per node the substep's tyre contact.
-// A tyre node on no wheel is a patch of its own: a wheel of one node with no hubs (axle0 -1), which gives the same bits
-// (its sums are its own need and cap).
-struct WheelDev {
-    const int4* wheel;       // axle0, axle1 (global nodes; -1: a lone tyre node's), first of its nodes in wnodes, count
-    const int* wnodes;       // the wheels' tyre nodes, each wheel's ascending
-    const int* wlist;        // ... each wheel's in the builder's order (the turn's parity, the speed's sum)
-    const int* wc_ptr;       // per node + 1: its wheel terms in wc, in wheel order
-    const int2* wc;          // (wheel, kind | parity << 2): kind 0 the wheel's turn, 1 its arm (- the reaction), 2 its
-                             // near axle node (+ the reaction)
-    float4* tcon;            // per node: its static contact this substep (normal xyz, depth w), left for k_tyres
-    float4* tfric;           // per node: (friction coefficient, surface, -, 1 while it waits for k_tyres)
-    float4* wst;             // per wheel: Wheel::speed, avg_speed, last_torque, last_retorque
-    const float4* wctl;      // per wheel: the controller's torque and brake, radius, mass
-    const int4* warm;        // per wheel: arm, near_attach (global; -1 none), propulsed
-    float4* wcf;             // per wheel: this substep's reaction on the arm (xyz; w 1 where it acts)
-    float* wper;             // per wheel: this substep's torque share a tyre node (torque / nodes)
-    int nreal;               // the builders' wheels (the lone tyre nodes' come after)
-    float tyre_grip;         // WorldSettings::tyre_grip
-};
-
-// SoftBody::compute_wheel_forces (softbody.cpp:691-767) a warp a wheel, on the substep's starting state: the
-// controller's torque (every substep: the first short step's), the brake's stop torque against the average speed and
-// the last reaction, the share a tyre node, the tread's speed (summed in the builder's order), the average speed and
-// the reaction of the inertia, and the drive's reaction on the arm; the nodes' terms are k_force's.
-__global__ void __launch_bounds__(256) k_wheels(const float4* __restrict__ nd, const int4* __restrict__ info, const Body* __restrict__ bodies,
-                                                WheelDev wh, float dt) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= wh.nreal) return; // (w is the warp's: its lanes leave together)
-    const int4 W = wh.wheel[w];
-    if (W.w == 0 || bodies[info[W.x].w].sleeping) return; // (an asleep body's forces are not made)
-    const float4 ctl = wh.wctl[w], st = wh.wst[w];
-    const int4 A = wh.warm[w];
-    float T = ctl.x;
-    if (ctl.y > 0) {
-        const float stop = -st.y * ctl.z * ctl.w / dt - st.w;
-        T += st.x > 0 ? clampf(stop, -ctl.y, 0.0f) : clampf(stop, 0.0f, ctl.y);
-    }
-    const float4 H0 = nd[2 * W.x], H1 = nd[2 * W.y], U0 = nd[2 * W.x + 1], U1 = nd[2 * W.y + 1];
-    const v3 axis = normalize(V(H1.x - H0.x, H1.y - H0.y, H1.z - H0.z));
-    const float per = T / (float)W.w;
-    float expected = st.x, speed = 0.0f;
-    // (a lane a node: each node's term, then the sum in the builder's order by broadcasts)
-    for (int c = 0; c < W.w; c += 32) {
-        const int j = c + lane;
-        float term = 0.0f;
-        bool has = false;
-        if (j < W.w) {
-            const int ni = wh.wlist[W.z + j];
-            const float4 hp = (j & 1) ? H1 : H0, hv = (j & 1) ? U1 : U0, P = nd[2 * ni], Vn = nd[2 * ni + 1];
-            v3 rad = V(P.x - hp.x, P.y - hp.y, P.z - hp.z);
-            const float rl2 = dot(rad, rad);
-            if (!(rl2 < 1e-8f)) {
-                const float inv = 1.0f / sqrtf(rl2);
-                if (A.z == 2) rad = V(-rad.x, -rad.y, -rad.z);
-                const v3 dir = V(axis.y * rad.z - axis.z * rad.y, axis.z * rad.x - axis.x * rad.z, axis.x * rad.y - axis.y * rad.x) * inv;
-                term = dot(V(Vn.x - hv.x, Vn.y - hv.y, Vn.z - hv.z), dir), has = true;
-            }
-        }
-        for (unsigned m = __ballot_sync(0xffffffffu, has); m; m &= m - 1) speed += __shfl_sync(0xffffffffu, term, __ffs(m) - 1);
-    }
-    if (lane != 0) return;
-    wh.wper[w] = per;
-    const float sp = speed / (float)W.w, avg = 0.99f * st.y + 0.1f * sp;
-    float lrt = st.w;
-    if (ctl.w > 0 && ctl.z > 0) {
-        expected += (st.z / ctl.z) / ctl.w * dt;
-        lrt = ctl.w * (sp - expected) / dt;
-    }
-    float4 cf4 = make_float4(0, 0, 0, 0);
-    if (A.x >= 0 && A.y >= 0 && fabsf(T) > 0.01f) {
-        const float4 Pa = nd[2 * A.x], Pn = nd[2 * A.y];
-        const v3 rr = V(Pa.x - Pn.x, Pa.y - Pn.y, Pa.z - Pn.z);
-        v3 r = rr - axis * dot(rr, axis);
-        const float off = length(rr - r), rl = length(r);
-        if (rl > 0.01f && 2 * off < rl) {
-            r = divs(r, rl);
-            const v3 cf = V(axis.y * r.z - axis.z * r.y, axis.z * r.x - axis.x * r.z, axis.x * r.y - axis.y * r.x) * (0.5f * T / rl) * (1.0f - 2.0f * off / rl);
-            cf4 = make_float4(cf.x, cf.y, cf.z, 1.0f);
-        }
-    }
-    wh.wcf[w] = cf4;
-    wh.wst[w] = make_float4(sp, avg, T, lrt);
-}
-
 // kPacked: the incidences as 32-bit words: the beam's index less the warp's base (ell_base, bits 0-14; 0x7fff:
 // padding), bit 15 set where this node is the beam's b end, the other end's index less this node's plus 32768 (bits
 // 16-31) - half the bytes of the (beam | b-end bit, other end) pairs, for rigs whose warps' beams and neighbours lie

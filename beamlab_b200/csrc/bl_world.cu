@@ -1220,7 +1220,7 @@ static int ensure_committed(bl_gpu_ctx* c) {
 static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0; } // (s == 0 || s >= next_rebuild)
 
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
-    int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0) + (c->NWR > 0 ? 1 : 0) + (c->NSH > 0 ? 1 : 0);
+    int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0) + (c->NWR > 0 && c->beam_grid == 0 ? 1 : 0) + (c->NSH > 0 ? 1 : 0);
     if (c->NF > 0) {
         per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
         // (the unload re-pass: its checks, conditions and account; its passes' kernels, which run only where a check
@@ -1343,19 +1343,20 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         if (c->any_drag) k_drag_parts<<<(c->B + 63) / 64, 64, 0, s>>>(c->dbodies.p, c->B, c->nd.p, c->ab.p, c->bmeta.p, dg);
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
         if (c->beam_grid > 0) {
+            // (the wheels' step in the same launch, after each block's tiles)
             if (c->ends16)
                 k_beams_tma<true><<<c->beam_grid, kBeamThreads, beam_smem<true>(), s>>>(c->ab16.p, c->tbase.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p,
                                                                                        c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B,
-                                                                                       c->beam_tiles, c->deverr.p);
+                                                                                       c->beam_tiles, c->deverr.p, c->info.p, wh, dt);
             else
                 k_beams_tma<false><<<c->beam_grid, kBeamThreads, beam_smem<false>(), s>>>(c->ab.p, nullptr, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p,
                                                                                          c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B,
-                                                                                         c->beam_tiles, c->deverr.p);
+                                                                                         c->beam_tiles, c->deverr.p, c->info.p, wh, dt);
         } else {
             k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
                                                    c->dbodies.p, c->M, c->B);
+            if (c->NWR > 0) k_wheels<<<(c->NWR + 7) / 8, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, wh, dt);
         }
-        if (c->NWR > 0) k_wheels<<<(c->NWR + 7) / 8, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, wh, dt);
         if (c->NSH > 0)
             k_shocks<<<(c->NSH + 127) / 128, 128, 0, s>>>(sk, c->NSH, c->ab.p, c->bst.p, c->bmeta.p, c->stress.p, c->bbody.p, c->nd.p, c->dbodies.p);
         if (c->NT > 0 && c->any_plastic) k_tri_eval<true><<<(c->NT + 127) / 128, 128, 0, s>>>(F, c->nd.p);
