@@ -84,6 +84,7 @@ struct FemDev {
     int* body_failures;      // / body
     int* body_clamps;        // / body
     float h, step;
+    const float4* contact_n; // per frame node: its ground contact's normal this step, doubled where it sticks (null: none)
     // members (k_member_eval)
     int nmem;
     const int2* mn;          // frame nodes a, b
@@ -874,6 +875,32 @@ __device__ __forceinline__ void assemble_column(const FemDev& F, const float4* _
         const double h = F.h;
         R[0] = h * (double)f.x, R[1] = h * (double)f.y, R[2] = h * (double)f.z;
         R[3] = h * (double)m.x, R[4] = h * (double)m.y, R[5] = h * (double)m.z;
+        if (F.contact_n) {
+            // a ground contact: kappa n n^T towards the normal velocity change it asked for, kappa = 200 m; sticking,
+            // along the ground too towards stopping its sliding (gather_part, frame_fem.cpp:1043-1064)
+            const float4 c4 = F.contact_n[i];
+            v3 cn = V(c4.x, c4.y, c4.z);
+            const float l2 = dot(cn, cn);
+            if (l2 > 0) {
+                const bool stick = l2 > 2.0f;
+                if (stick) cn = cn * 0.5f;
+                const double kap = 200.0 * Vv.w, want = F.step * (double)dot(V(f.x, f.y, f.z), cn) / Vv.w;
+                const double nn[3] = {cn.x, cn.y, cn.z};
+                for (int p = 0; p < 3; p++) {
+                    for (int q2 = 0; q2 < 3; q2++) D[p * 6 + q2] += kap * nn[p] * nn[q2];
+                    R[p] += kap * want * nn[p];
+                }
+                if (stick) {
+                    const v3 vel = V(Vv.x, Vv.y, Vv.z);
+                    const v3 vt = vel - cn * dot(vel, cn);
+                    const double wt[3] = {-vt.x, -vt.y, -vt.z};
+                    for (int p = 0; p < 3; p++) {
+                        for (int q2 = 0; q2 < 3; q2++) D[p * 6 + q2] += kap * ((p == q2 ? 1.0 : 0.0) - nn[p] * nn[q2]);
+                        R[p] += kap * wt[p];
+                    }
+                }
+            }
+        }
         for (int j = 0; j < 6; j++) R[j] += rd[j];
     }
     double* Dg = F.diag + 36 * (size_t)k;

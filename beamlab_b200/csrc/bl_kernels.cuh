@@ -1045,6 +1045,38 @@ __device__ __forceinline__ void integrate_node(v3& pos, v3& vel, float inv_mass,
     }
 }
 
+// World::collide_static's query for one node (world.cpp:804-832): the terrain if the node is within its reach, the
+// body's candidate boxes and cylinders within reach of the node (all of them past 16 of either), StaticWorld::
+// collide_point's deepest contact
+__device__ __forceinline__ bool static_query(const Statics& st, const Body& B, v3 pos, float r, Contact& c) {
+    const bool near_terrain = st.has_terrain && pos.y - r <= B.terrain_max + 0.05f;
+    const int nbox = B.nbox, ncyl = B.ncyl;
+    if (!near_terrain && nbox == 0 && ncyl == 0) return false;
+    int bids[16], cids[16];
+    const int* bp = B.box_ids;
+    const int* cp = B.cyl_ids;
+    int nb = nbox, nc = ncyl;
+    if (nbox <= 16 && ncyl <= 16) {
+        nb = nc = 0;
+        const float rr = r + 0.01f;
+        for (int k = 0; k < nbox; k++) {
+            const Box& a = st.boxes[B.box_ids[k]];
+            if (pos.x >= a.mnx - rr && pos.x <= a.mxx + rr && pos.y >= a.mny - rr && pos.y <= a.mxy + rr && pos.z >= a.mnz - rr && pos.z <= a.mxz + rr)
+                bids[nb++] = B.box_ids[k];
+        }
+        for (int k = 0; k < ncyl; k++) {
+            const Cyl& cy = st.cyls[B.cyl_ids[k]];
+            const float cr = cy.radius + rr;
+            if (fabsf(pos.x - cy.bx) <= cr && fabsf(pos.z - cy.bz) <= cr && pos.y >= cy.by - rr && pos.y <= cy.by + cy.height + rr)
+                cids[nc++] = B.cyl_ids[k];
+        }
+        bp = bids;
+        cp = cids;
+        if (!near_terrain && nb == 0 && nc == 0) return false;
+    }
+    return collide_point(st, pos, r, bp, nb, cp, nc, near_terrain, c);
+}
+
 // World::collide_static for the node (world.cpp:781-870), then SoftBody::integrate_nodes (softbody.cpp:769-795), on
 // the force in fnode (gravity, beams, contacts with other bodies). first: the frame's first substep (the top speed
 // starts from the velocities before it, world.cpp:3217-3222). Frame bodies' nodes are integrated after their solve.
@@ -1078,36 +1110,9 @@ __global__ void __launch_bounds__(256) k_integrate(float4* __restrict__ nd, cons
                     vel = V(0, 0, 0);
                     inv_mass = 0;
                 } else {
-                    const float r = __int_as_float(inf.z);
-                    const bool near_terrain = st.has_terrain && pos.y - r <= B.terrain_max + 0.05f;
-                    const int nbox = B.nbox, ncyl = B.ncyl;
-                    if (near_terrain || nbox != 0 || ncyl != 0) {
-                        int bids[16], cids[16];
-                        const int* bp = B.box_ids;
-                        const int* cp = B.cyl_ids;
-                        int nb = nbox, nc = ncyl;
-                        bool go = true;
-                        if (nbox <= 16 && ncyl <= 16) {
-                            nb = nc = 0;
-                            const float rr = r + 0.01f;
-                            for (int k = 0; k < nbox; k++) {
-                                const Box& a = st.boxes[B.box_ids[k]];
-                                if (pos.x >= a.mnx - rr && pos.x <= a.mxx + rr && pos.y >= a.mny - rr && pos.y <= a.mxy + rr && pos.z >= a.mnz - rr &&
-                                    pos.z <= a.mxz + rr)
-                                    bids[nb++] = B.box_ids[k];
-                            }
-                            for (int k = 0; k < ncyl; k++) {
-                                const Cyl& cy = st.cyls[B.cyl_ids[k]];
-                                const float cr = cy.radius + rr;
-                                if (fabsf(pos.x - cy.bx) <= cr && fabsf(pos.z - cy.bz) <= cr && pos.y >= cy.by - rr && pos.y <= cy.by + cy.height + rr)
-                                    cids[nc++] = B.cyl_ids[k];
-                            }
-                            bp = bids;
-                            cp = cids;
-                            go = near_terrain || nb != 0 || nc != 0;
-                        }
+                    {
                         Contact c;
-                        if (go && collide_point(st, pos, r, bp, nb, cp, nc, near_terrain, c)) {
+                        if (static_query(st, B, pos, __int_as_float(inf.z), c)) {
                             contact = 1;
                             const GroundModel& gm = c_ground[c.surface < kSurfCount ? c.surface : 0];
                             const float fc = __int_as_float(inf.y) * B.fric;
@@ -1239,6 +1244,54 @@ __global__ void __launch_bounds__(256) k_tyres(float4* __restrict__ nd, const in
         atomic_max_f(&B.acc_v2, vv);
         atomicAdd(&B.acc_contacts, cnt);
     }
+}
+
+// World::collide_static for the frame bodies' nodes (world.cpp:781-870 on a body with a frame of members), before the
+// frame's implicit step: a node's contact force into its force (nforce, the step's right side); a frame node pressed on
+// records its ground contact's normal for the step (FemFrame::contact_n: doubled where it sticks - slower than 5 cm/s
+// along the ground and its friction holding what pushes it along), which the assembly holds with kappa = 200 m
+__global__ void k_fem_static(float4* __restrict__ nd, float4* __restrict__ nforce, const int* __restrict__ fem_nodes, int n_fem_nodes,
+                             const int* __restrict__ fslot, const int4* __restrict__ info, Body* __restrict__ bodies, Statics st, float dt,
+                             float4* __restrict__ contact_n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_fem_nodes) return;
+    const int i = fem_nodes[t];
+    const int4 inf = info[i];
+    Body& B = bodies[inf.w];
+    const float4 P = nd[2 * i], Vv = nd[2 * i + 1];
+    if (B.sleeping || !((uint32_t)inf.x & NF_GROUND) || P.w <= 0) return;
+    const v3 pos = V(P.x, P.y, P.z), vel = V(Vv.x, Vv.y, Vv.z);
+    if (pos.y < st.kill_y) { // (fell off the world)
+        nd[2 * i] = make_float4(P.x, P.y, P.z, 0.0f);
+        nd[2 * i + 1] = make_float4(0.0f, 0.0f, 0.0f, Vv.w);
+        return;
+    }
+    Contact c;
+    if (!static_query(st, B, pos, __int_as_float(inf.z), c)) return;
+    atomicAdd(&B.acc_contacts, 1);
+    const GroundModel& gm = c_ground[c.surface < kSurfCount ? c.surface : 0];
+    const float fc = __int_as_float(inf.y) * B.fric;
+    const float4 f4 = nforce[i];
+    v3 F = V(f4.x, f4.y, f4.z);
+    if (c.max_force > 0) {
+        v3 fcn = primitive_collision(F, vel, Vv.w, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, -1.0f);
+        const float fl = length(fcn);
+        if (fl > c.max_force) fcn = fcn * (c.max_force / fl);
+        F = F + fcn;
+    } else {
+        const v3 fo = primitive_collision(F, vel, Vv.w, c.normal, dt, gm, c.depth, fc, B.push_max, B.slop, B.bounce);
+        F = F + fo;
+        const int sl = fslot[i];
+        if (sl >= 0) {
+            const float fn = dot(fo, c.normal);
+            const v3 ft = F - c.normal * dot(F, c.normal), vt = vel - c.normal * dot(vel, c.normal);
+            if (fn > 0) {
+                const v3 cn = c.normal * (dot(vt, vt) < 0.05f * 0.05f && length(ft) < 0.3f * fn ? 2.0f : 1.0f);
+                contact_n[sl] = make_float4(cn.x, cn.y, cn.z, 0.0f);
+            }
+        }
+    }
+    nforce[i] = make_float4(F.x, F.y, F.z, f4.w);
 }
 
 // ------------------------------------------------------------------------------------------ end of frame

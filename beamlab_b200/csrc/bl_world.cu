@@ -134,6 +134,8 @@ struct bl_gpu_ctx {
     // FEM frames of all bodies back to back (see bl_fem_kernels.cuh)
     int NF = 0, NT = 0, NB = 0, n_fem_nodes = 0;
     bool any_plastic = false;                  // a yielding shell section on a body that deforms (k_tri_eval<true>)
+    bool fem_ground = false;                   // a frame body's node collides with the static world (k_fem_static)
+    DevBuf<float4> contact_n;                  // per frame node: its ground contact's normal this step
     bool any_plastic_members = false;          // a yielding member section on a body that deforms (k_member_eval<true>,
                                                // the unload re-pass)
     int64_t NU = 0;                            // block updates of a factorization
@@ -263,6 +265,7 @@ static void free_fem(bl_gpu_ctx* c) {
     c->msec.free_(), c->mon.free_(), c->mkw.free_(), c->mkv.free_(), c->NM = 0;
     c->mps.free_(), c->mtg.free_(), c->mflag.free_(), c->credit.free_(), c->elastic.free_(), c->comp_again.free_(), c->comp_size.free_();
     c->body_comp.free_(), c->rp.free_(), c->repc.free_();
+    c->contact_n.free_(), c->fem_ground = false;
     c->xd.free_(), c->diag.free_(), c->ldiag.free_(), c->off.free_(), c->rhs.free_(), c->dinv.free_(), c->tkv.free_(), c->ch2.free_(), c->chd.free_();
     c->finertia.free_(), c->tX.free_(), c->tk.free_(), c->tb.free_(), c->tX0.free_(), c->th0.free_(), c->tdmg.free_(), c->ttan.free_(), c->tbroken.free_(), c->ton.free_(), c->ffixed.free_(), c->fsec.free_();
 }
@@ -514,6 +517,7 @@ static int commit_fem(bl_gpu_ctx* c) {
         if (hb.fem) NF += (int)hb.fem->node.size(), NT += (int)hb.fem->tn.size(), NB += (int)hb.fem->row.size(), NC += hb.fem->ncomp,
                     NS += (int)hb.sections.size(), nfem_nodes += hb.rec.nnodes;
     c->NF = NF, c->NT = NT, c->NB = NB, c->n_fem_nodes = nfem_nodes, c->any_plastic = false, c->any_plastic_members = false;
+    c->fem_ground = false;
     c->lvl_grp_ptr.clear(), c->lvl_col_ptr.clear();
     std::vector<float4> ext(c->any_ext ? c->N : 0, make_float4(0, 0, 0, 0));
     for (const HostBody& hb : c->bodies)
@@ -553,7 +557,7 @@ static int commit_fem(bl_gpu_ctx* c) {
         const int nf = (int)M.node.size(), nt = (int)M.tn.size(), nb = (int)M.row.size();
         // (a section yields where the body deforms: eval_tris' s.yield > 0 and eval_forces' s.Np > 0, with allow_deform)
         const int plastic = (hb.beam_bits & BB_DEFORM) ? 1 : 0;
-        for (int i = 0; i < hb.rec.nnodes; i++) fem_nodes.push_back(hb.rec.node0 + i);
+        for (int i = 0; i < hb.rec.nnodes; i++) fem_nodes.push_back(hb.rec.node0 + i), c->fem_ground |= (hb.info[i].flags & BL_NF_GROUND) != 0;
         const float dt = c->cfg.dt;
         const double h2 = (double)hb.theta * dt * dt, hd = (double)hb.diss * dt * dt;
         for (int i = 0; i < nf; i++) {
@@ -731,6 +735,11 @@ static int commit_fem(bl_gpu_ctx* c) {
         }
     BL_CUDA(c, c->ldiag.alloc(36 * (size_t)NF));
     F.ldiag = c->ldiag.p;
+    F.contact_n = nullptr;
+    if (c->fem_ground) {
+        BL_CUDA(c, c->contact_n.alloc(NF));
+        F.contact_n = c->contact_n.p;
+    }
     {   // the members
         const int E = (int)mnv.size();
         if ((rc = upload_vec(c, c->mn, mnv)) || (rc = upload_vec(c, c->mmeta, mmeta)) || (rc = upload_vec(c, c->mL0, mL0)) ||
@@ -1222,7 +1231,7 @@ static bool rebuild_at(const bl_gpu_ctx* c, int k) { return k % c->interval == 0
 static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
     int64_t per = 3 + (c->any_drag ? 1 : 0) + (c->NW > 0 ? 1 : 0) + (c->NWR > 0 && c->beam_grid == 0 ? 1 : 0) + (c->NSH > 0 ? 1 : 0);
     if (c->NF > 0) {
-        per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0);
+        per += c->fem_launches + (c->cfg.fem_check_residual ? 2 : 0) + (c->fem_ground ? 1 : 0);
         // (the unload re-pass: its checks, conditions and account; its passes' kernels, which run only where a check
         // finds an unload, are not counted - launched without a graph they always run)
         if (c->any_plastic_members) per += c->cfg.graphs ? 5 : 3 + 2 * (1 + c->chol_launches);
@@ -1382,6 +1391,11 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         mark();
         if (c->NF > 0) {
             // the frames' implicit step: assembly, factorization and substitutions level by level, velocities, integration
+            if (c->fem_ground) { // (the frame nodes' static contacts: their forces, the ground's hold in the step)
+                cudaMemsetAsync(c->contact_n.p, 0, sizeof(float4) * c->NF, s);
+                k_fem_static<<<(c->n_fem_nodes + 127) / 128, 128, 0, s>>>(c->nd.p, c->nforce.p, c->fem_nodes.p, c->n_fem_nodes, c->fslot.p, c->info.p,
+                                                                        c->dbodies.p, c->st, dt, c->contact_n.p);
+            }
             k_fem_assemble_all<<<(c->NF + c->NB + 127) / 128, 128, 0, s>>>(F, c->nd.p, c->nforce.p);
             if (c->cfg.fem_check_residual) {
                 cudaMemcpyAsync(c->a0d.p, c->diag.p, sizeof(double) * 36 * c->NF, cudaMemcpyDeviceToDevice, s);
@@ -1534,8 +1548,12 @@ static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32
         mpm.push_back(fs.rho * fs.A); // (FrameSection::mass_per_m)
     }
     if (!fd.tris_first && !add_tris()) return BL_GPU_EINVAL;
+    // (a frame of triangles on the ground: its plates' mid points take contacts too - collide_static_mids - not on this
+    // path; a frame of members takes its nodes' static contacts)
     for (uint32_t bn : M->node)
-        if (info[bn].flags & BL_NF_GROUND) return BL_GPU_EUNSUPPORTED; // (a frame's static contacts: not on this path)
+        if ((info[bn].flags & BL_NF_GROUND) && !M->tn.empty()) return BL_GPU_EUNSUPPORTED;
+    for (int i = 0; i < n_nodes; i++)
+        if (info[i].flags & BL_NF_TYRE) return BL_GPU_EUNSUPPORTED; // (tyre nodes on a frame body)
     std::vector<float> px(n_nodes), py(n_nodes), pz(n_nodes), ms(n_nodes);
     for (int i = 0; i < n_nodes; i++) px[i] = nodes[i].p[0], py[i] = nodes[i].p[1], pz[i] = nodes[i].p[2], ms[i] = nodes[i].mass;
     fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data(), mpm);

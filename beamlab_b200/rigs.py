@@ -615,12 +615,13 @@ def tube_section(outer: float = 0.04, wall: float = 0.003, E: float = 2.1e11, G:
 
 
 def frame_ladder(rails: int = 12, spacing: float = 0.25, width: float = 0.6, origin=(0.0, 1.0, 0.0), load: float = 300.0,
-                 joints=None, section: dict | None = None) -> dict:
+                 joints=None, section: dict | None = None, ground: bool = False) -> dict:
     """A ladder frame of members (FemFrame::add_element): two rails of `rails` nodes along x, `spacing` apart, `width`
     apart in z, rungs between them at every node and a diagonal in each bay; the rails' first nodes clamped (anchored);
     a constant `load` N down (and a tenth of it across) at the far end of one rail, gravity. Each member's mass is its
     section's rho A L, half on each end node. joints: per rung, the joints at its ends (FJ_*; default rigid) - a few
-    balls, hinges, swivels and elastic joints exercise the joints' end stiffnesses and the twist's weighting."""
+    balls, hinges, swivels and elastic joints exercise the joints' end stiffnesses and the twist's weighting. ground:
+    no anchors, every node NF_GROUND over flat grass (the ladder dropped onto the ground from `origin`)."""
     s = section or tube_section()
     ox, oy, oz = (np.float32(v) for v in origin)
     n = 2 * rails
@@ -645,8 +646,11 @@ def frame_ladder(rails: int = 12, spacing: float = 0.25, width: float = 0.6, ori
         mass[a] += np.float32(m * np.float32(0.5))
         mass[b] += np.float32(m * np.float32(0.5))
     flags = np.zeros(n, np.uint16)
-    flags[0] |= NF_FIXED
-    flags[1] |= NF_FIXED
+    if ground:
+        flags |= NF_GROUND
+    else:
+        flags[0] |= NF_FIXED
+        flags[1] |= NF_FIXED
     body = {
         "pos": pos, "vel": np.zeros((n, 3), np.float32), "mass": mass, "node_flags": flags,
         "friction": np.ones(n, np.float32), "radius": np.zeros(n, np.float32),
@@ -661,7 +665,8 @@ def frame_ladder(rails: int = 12, spacing: float = 0.25, width: float = 0.6, ori
         "member_mass": np.zeros(len(members), np.float32),
         "loads": [(n - 2, (0.0, -float(load), 0.1 * float(load)))],
     }
-    return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005}, "statics": {}, "bodies": [body],
+    statics = {"terrain": flat_terrain(), "boxes": [], "build_grid": True} if ground else {}
+    return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005}, "statics": statics, "bodies": [body],
             "name": f"frame_ladder(rails={rails})"}
 
 

@@ -237,8 +237,9 @@ typedef struct bl_shock {
 /* One body: a SoftBody after finalize (softbody.cpp:76-83) - its arrays and the knobs of the explicit path
  * (softbody.h:650-700), its node wheels and shocks, and optionally its FEM frame of members and triangle elements.
  * Bodies with joints, ring tyres, driven or braked wheels, slide nodes, sheets, FEM mounts or grab are
- * rejected by the caller's shim (this record has no fields for them); BL_GPU_EUNSUPPORTED here: a FEM frame whose
- * nodes collide with the static world (NF_GROUND), beams on frame nodes, yielding sections on a body that breaks, a frame with collision
+ * rejected by the caller's shim (this record has no fields for them); BL_GPU_EUNSUPPORTED here: a FEM frame of
+ * triangles whose nodes collide with the static world (NF_GROUND; a frame of members takes its nodes' static
+ * contacts), tyre nodes on a body with a frame, beams on frame nodes, yielding sections on a body that breaks, a frame with collision
  * triangles, air drag, wheels or shocks, self collision, a node on two wheels. */
 typedef struct {
     int32_t n_nodes;

@@ -181,3 +181,28 @@ def test_gpu_yielding_frame_graphs_equal_launches():
     assert ws[0].fem_stats()["repasses"] > 0
     for w in ws:
         w.close()
+
+
+def test_gpu_frame_on_ground_matches_reference(ref_lib):
+    """A ladder frame of members dropped onto flat grass: its nodes' static contacts (World::collide_static's
+    primitive_collision into the node forces) and the frame step's hold on the pressed nodes (FemFrame::contact_n:
+    kappa = 200 m along the normal, and along the ground where a node sticks - gather_part, frame_fem.cpp:1043-1064),
+    the landing, the bounce and the settling: the nodes within the FEM tolerance of the reference over 600 substeps."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.frame_ladder(12, origin=(0.0, 0.3, 0.0), load=300.0, ground=True)
+    w = world_from_rig(rig)
+    ref = build_world(RefWorld, rig, multithreaded=False)
+    h = w.bodies()[0]
+    touched = 0
+    for f in range(30):
+        w.step_substeps(20)
+        ref.step_substeps(20)
+        touched = max(touched, ref.body(0)["static_contacts"])
+        if f in (9, 14, 19, 29):
+            p = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
+            d = np.abs(p - ref.nodes(0)["pos"]).max()
+            assert d <= TOL, f"frame {f}: max |dp| {d:.3g} m"
+    assert touched > 0 and np.abs(p[:, 1]).max() < 0.2  # (it landed)
+    st = h.state()
+    assert st["fem_failures"] == 0 and st["fem_clamps"] == 0
+    w.close()
