@@ -206,3 +206,28 @@ def test_gpu_frame_on_ground_matches_reference(ref_lib):
     st = h.state()
     assert st["fem_failures"] == 0 and st["fem_clamps"] == 0
     w.close()
+
+
+def test_gpu_plastic_state_survives_a_recommit():
+    """A body added while a yielding ladder folds and a yielding plate flows (the context commits again, pulling the
+    members' plastic state and rest frames, the re-passes' budget, the triangles' rest shapes, frames, stiffnesses and
+    plastic rotations back from the device): both frames go on bitwise as in a world that never committed again."""
+    from beamlab_b200.world import SoftBody
+    lad = rigs.frame_ladder(12, load=3000.0, section=rigs.tube_section(yield_stress=2.5e8))
+    pl = rigs.shell_plate(12, yield_stress=2.5e8, load=3000.0, seed=2, origin=(0.0, 1.0, 5.0))
+    rig = {"settings": lad["settings"], "statics": {}, "bodies": lad["bodies"] + pl["bodies"]}
+    ws = [world_from_rig(rig), world_from_rig(rig)]
+    for f in range(14):
+        if f == 6:
+            extra = rigs.truss_car(4, speed=0.0, dims=(4, 2, 2))["bodies"][0]
+            extra["pos"][:, 2] += 30.0
+            ws[1].add_body(SoftBody.from_arrays(extra, name="extra"))
+        for w in ws:
+            w.step_substeps(20)
+    for b in (0, 1):
+        x, y = (np.ascontiguousarray(w.bodies()[b].nodes()["p"]) for w in ws)
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f"body {b}"
+    assert ws[1].fem_stats()["repasses"] > 0
+    assert (ws[1].bodies()[1].fem_tris()["dmg"] > 0).any()
+    for w in ws:
+        w.close()

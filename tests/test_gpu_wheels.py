@@ -123,3 +123,35 @@ def test_gpu_driven_wheels_match_reference(ref_lib, torque, brake):
             assert np.array_equal(gs["avg_speed"].view(np.uint32), rs["avg_speed"].view(np.uint32))
             top = max(top, float(np.abs(rs["speed"]).max()))
     assert top > 5.0  # (the driven wheels spun up before the brakes held them)
+
+
+def test_gpu_wheel_state_survives_a_recommit(ref_lib):
+    """A body added while a driven, braked wheeled car rolls (the context commits its bodies again, pulling every
+    state back from the device - the wheels' speeds, last torques and reactions with them): both bodies and the wheels'
+    speeds stay bitwise the reference's, which takes the new body into its running world the same way."""
+    from beamlab_b200.world import SoftBody
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.wheeled_car(speed=4.0, yaw=0.0, wall=False)
+    gw = GpuWorld(rig)
+    rw = build_world(RefWorld, rig, multithreaded=False)
+    h = gw.h[0]
+    wheels = rig["bodies"][0]["wheels"]
+    for k, w in enumerate(wheels):
+        t, b = (300.0 if w["propulsed"] else 0.0), (0.0 if w["propulsed"] else 200.0)
+        h.set_wheel_drive(k, t, b)
+        rw.set_wheel_drive(0, k, t, b)
+    for _ in range(10):
+        gw.step_substeps(33)
+        rw.step_substeps(33)
+    extra = rigs.truss_car(4, speed=3.0, dims=(6, 3, 3))["bodies"][0]
+    extra["pos"][:, 2] += 20.0
+    gw.w.add_body(SoftBody.from_arrays(extra, name="extra"))
+    gw.h = gw.w.bodies()
+    rw.add_body(extra)
+    for _ in range(10):
+        gw.step_substeps(33)
+        rw.step_substeps(33)
+    assert_same(gw, rw, 2, "after the recommit")
+    gs, rs = gw.h[0].wheels(), rw.wheels(0, len(wheels))
+    assert np.array_equal(gs["speed"].view(np.uint32), rs["speed"].view(np.uint32))
+    assert np.array_equal(gs["avg_speed"].view(np.uint32), rs["avg_speed"].view(np.uint32))
