@@ -42,6 +42,7 @@ _SIGNATURES = {
     "bl_gpu_set_node_force": ([_vp, _i32, _i32, _vp], C.c_int),
     "bl_gpu_set_wheel_drive": ([_vp, _i32, _i32, _f, _f], C.c_int),
     "bl_gpu_download_wheels": ([_vp, _i32, _vp, _vp, _vp], C.c_int),
+    "bl_gpu_wheel_speed": ([_vp, _i32, _vp, _vp], C.c_int),
     "bl_gpu_download_fem": ([_vp, _i32, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "bl_gpu_download_fem_tris": ([_vp, _i32, _vp, _vp, _vp, _vp], C.c_int),
     "bl_gpu_download_pairs": ([_vp, _vp, _i32, _vp], C.c_int),

@@ -2406,6 +2406,25 @@ int bl_gpu_download_wheels(bl_gpu_ctx* c, int32_t body, int32_t* n, float* speed
     return BL_GPU_OK;
 }
 
+int bl_gpu_wheel_speed(bl_gpu_ctx* c, int32_t body, float* wheel_speed, float* wheel_spin) {
+    if (!wheel_speed || !wheel_spin) return BL_GPU_EINVAL;
+    int32_t n = 0;
+    int rc = bl_gpu_download_wheels(c, body, &n, nullptr, nullptr);
+    if (rc) return rc;
+    std::vector<float> sp(n), av(n);
+    if (n > 0 && (rc = bl_gpu_download_wheels(c, body, &n, sp.data(), av.data()))) return rc;
+    // (compute_wheel_forces' sums over the forward-propelled wheels in their order)
+    const HostBody& hb = c->bodies[body];
+    float speed_sum = 0, spin_sum = 0;
+    int nprop = 0;
+    for (int k = 0; k < n; k++)
+        if (hb.wheels[k].propulsed == 1 && !hb.wheels[k].nodes.empty())
+            speed_sum += sp[k], spin_sum += sp[k] / std::max(0.05f, hb.wheels[k].radius), nprop++;
+    *wheel_speed = nprop > 0 ? speed_sum / nprop : 0.0f;
+    *wheel_spin = nprop > 0 ? spin_sum / nprop : 0.0f;
+    return BL_GPU_OK;
+}
+
 int bl_gpu_download_fem_tris(bl_gpu_ctx* c, int32_t body, int32_t* n, float* rest, float* frames, float* plastic_stretch) {
     int rc = check_body(c, body);
     if (rc) return rc;

@@ -479,6 +479,13 @@ class BodyHandle:
         _check(L.bl_gpu_download_wheels(ctx, self.index, C.byref(n), sp.ctypes.data, av.ctypes.data), "download_wheels", ctx)
         return {"speed": sp, "avg_speed": av}
 
+    def wheel_speed(self) -> tuple[float, float]:
+        """SoftBody::wheel_speed and wheel_spin: the forward-propelled wheels' mean tread speed and spin."""
+        sp, spin = C.c_float(), C.c_float()
+        _check(self.world._L.bl_gpu_wheel_speed(self.world._ctx, self.index, C.byref(sp), C.byref(spin)), "wheel_speed",
+               self.world._ctx)
+        return sp.value, spin.value
+
     def set_node_force(self, node: int, force):
         """A constant force on one node, every substep after gravity (a SoftBody::pre_substep push)."""
         f = (C.c_float * 3)(*[float(x) for x in force])

@@ -356,6 +356,10 @@ int bl_gpu_set_wheel_drive(bl_gpu_ctx* ctx, int32_t body, int32_t wheel, float t
 /* A body's wheels' Wheel::speed (the tread's tangential speed, m/s) and avg_speed; n the wheel count. Synchronous. */
 int bl_gpu_download_wheels(bl_gpu_ctx* ctx, int32_t body, int32_t* n, float* speed, float* avg_speed);
 
+/* SoftBody::wheel_speed and wheel_spin (softbody.cpp:723-766): the mean tread speed (m/s) and spin (rad/s) of the
+ * body's forward-propelled wheels, for its drivetrain; 0 while it has none. Synchronous. */
+int bl_gpu_wheel_speed(bl_gpu_ctx* ctx, int32_t body, float* wheel_speed, float* wheel_spin);
+
 /* A body's FEM frame nodes (FemFrame::node / xd / q / w, frame_fem.h:331-350): body node, double position (3),
  * orientation (x y z w), angular velocity (3); n the frame node count (0: none). Any pointer may be NULL. */
 int bl_gpu_download_fem(bl_gpu_ctx* ctx, int32_t body, int32_t* n, int32_t* node, double* xd, float* q, float* w);

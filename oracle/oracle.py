@@ -94,6 +94,7 @@ def _load(path: str, prefix: str) -> C.CDLL:
         lib.ref_add_wheel.argtypes = [vp, i, C.c_uint32, C.c_uint32, u32p, i, f, f, f, i, i, i]
         lib.ref_set_wheel_drive.argtypes = [vp, i, i, f, f]
         lib.ref_wheel_state.argtypes = [vp, i, vp, vp]
+        lib.ref_body_wheel_speed.argtypes = [vp, i, vp]
         lib.ref_set_tyre_grip.argtypes = [vp, f]
         lib.ref_set_body_flags.argtypes = [vp, i, i, i]
         lib.ref_fem_tri_dmg.argtypes = [vp, i, vp]
@@ -223,7 +224,9 @@ class _OracleWorld:
         """The first n wheels' speed and average speed (RefWorld only)."""
         sp, av = np.zeros(n, np.float32), np.zeros(n, np.float32)
         self._lib.ref_wheel_state(self._w, body, sp.ctypes.data, av.ctypes.data)
-        return {"speed": sp, "avg_speed": av}
+        ws = np.zeros(2, np.float32)
+        self._lib.ref_body_wheel_speed(self._w, body, ws.ctypes.data)
+        return {"speed": sp, "avg_speed": av, "wheel_speed": ws[0], "wheel_spin": ws[1]}
 
     def nodes(self, body: int):
         n = self._fn("body_nodes")(self._w, body)

@@ -354,6 +354,9 @@ void ref_wheel_state(RefWorld* r, int body, float* speed, float* avg_speed) {
     for (size_t k = 0; k < b->wheels.size(); k++) speed[k] = b->wheels[k].speed, avg_speed[k] = b->wheels[k].avg_speed;
 }
 
+// SoftBody::wheel_speed, wheel_spin
+void ref_body_wheel_speed(RefWorld* r, int body, float* out) { out[0] = r->bodies[body]->wheel_speed, out[1] = r->bodies[body]->wheel_spin; }
+
 // FrameTri::dmg of each triangle (the plastic stretch reached)
 void ref_fem_tri_dmg(RefWorld* r, int body, float* dmg) {
     const FemFrame& f = r->bodies[body]->fem;

@@ -121,6 +121,8 @@ def test_gpu_driven_wheels_match_reference(ref_lib, torque, brake):
             gs, rs = h.wheels(), rw.wheels(0, len(wheels))
             assert np.array_equal(gs["speed"].view(np.uint32), rs["speed"].view(np.uint32)), f"frame {f}: wheel speeds"
             assert np.array_equal(gs["avg_speed"].view(np.uint32), rs["avg_speed"].view(np.uint32))
+            gsp, gspin = h.wheel_speed()
+            assert np.float32(gsp) == rs["wheel_speed"] and np.float32(gspin) == rs["wheel_spin"]
             top = max(top, float(np.abs(rs["speed"]).max()))
     assert top > 5.0  # (the driven wheels spun up before the brakes held them)
 
