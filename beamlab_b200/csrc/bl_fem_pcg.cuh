@@ -2,8 +2,8 @@
 //
 // (A dv = rhs: the system k_fem_assemble_all leaves in diag / off / rhs - M + (theta h^2 + beta h) K + theta h^2 Kg over
 // the frame's 6-DOF nodes, frame_fem.cpp:916-1086 - in the factor's column order.) The reference solves it by the
-// block Cholesky (frame_fem.cpp:2887-2954), which this library runs as the default and as the judge. k_fem_pcg solves
-// the same system by CG with a block-Jacobi preconditioner (each column's 6 x 6 diagonal block, its translational 3 x 3
+// block Cholesky (frame_fem.cpp:2887-2954), which this library runs as the default and as the arbiter of its error.
+// k_fem_pcg solves the same system by CG with a block-Jacobi preconditioner (each column's 6 x 6 diagonal block, its translational 3 x 3
 // part optionally scaled by a learned S: z = T D^-1 T^T r with T = diag(S, I), symmetric positive definite for any
 // invertible S) from an initial guess: zero, or the best combination (in the energy norm: the Galerkin projection onto
 // their span) of the last substep's solution and, with the learned warm start, the network's per-node dv. The
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256) k_fem_pcg(FemDev F, PcgArgs P) {
     const double bb = s_tot[0];
     double rz = s_tot[1], rr = s_tot[2];
     const double lim = P.tol * P.tol * bb;
-    const bool bad = s_tot[3] > 0 || !(rr == rr); // (a diagonal block not positive definite, a NaN: the Cholesky judges)
+    const bool bad = s_tot[3] > 0 || !(rr == rr); // (a diagonal block not positive definite, a NaN: the Cholesky decides)
     int it = 0;
     bool ok = !bad && rr <= lim;
     while (!ok && !bad && it < P.max_iters) {
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256) k_fem_pcg(FemDev F, PcgArgs P) {
         grid.sync();
         grid_totals(P, 1, nw, 2, s_tot);
         rr = s_tot[1];
-        if (!(rr == rr)) break; // (NaN: the Cholesky judges)
+        if (!(rr == rr)) break; // (NaN: the Cholesky decides)
         if (rr <= lim) {
             ok = true;
             break;
