@@ -8,10 +8,12 @@
 //
 // The scratch: g_noalloc_fv, BL_GPU_NOALLOC_MAX_BEAMS float4 (16 MiB), a file-scope __device__ array that every GPU
 // which loads the library holds until the process exits. In host code its name stands for a host-side shadow, not a
-// device address, so the kernel gets the address that cudaGetSymbolAddress returns for the current device, looked up
-// once per device on its first call (that first call should come before any stream capture begins). Every call shares
-// the array; a call writes each slot before it reads it, so nothing needs clearing, but two calls whose kernels overlap
-// on the GPU race on it.
+// device address, so the kernel gets the address that cudaGetSymbolAddress returns in the calling thread's current
+// CUDA context. The address belongs to the context (a caller's own cuCtxCreate context, or a primary context made
+// again after cudaDeviceReset, has its own copy of the array), so it is looked up again on every call whose stream is
+// not being captured and kept per context for the calls made during a capture; the first call in a context should
+// come before any stream capture begins. Every call shares the array; a call writes each slot before it reads it, so
+// nothing needs clearing, but two calls whose kernels overlap on the GPU race on it.
 #include "../../include/beamlab_gpu.h"
 #include "bl_math.cuh"
 
@@ -131,8 +133,53 @@ __global__ void k_noalloc_nodes(bl_node* __restrict__ nodes, int n_nodes, const 
     }
 }
 
+// The scratch's address per CUDA context, for the calls made while their stream is being captured (a capture forbids
+// nothing here, but a context's first lookup may load the library's module). cuCtxGetCurrent is reached through the
+// runtime's driver entry point, so the library does not link libcuda itself.
+typedef int (*ctx_get_current_fn)(void** ctx);
+struct ScratchSlot {
+    void* ctx;
+    float4* fv;
+};
 std::mutex g_setup_mutex;
-float4* g_fv_ptr[128] = {};
+ScratchSlot g_slots[64] = {};
+int g_next_slot = 0;
+ctx_get_current_fn g_ctx_get_current = nullptr;
+
+int current_context(void** ctx) {
+    if (!g_ctx_get_current) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return BL_GPU_ECUDA;
+        g_ctx_get_current = (ctx_get_current_fn)fn;
+    }
+    *ctx = nullptr;
+    return (g_ctx_get_current(ctx) == 0 && *ctx) ? BL_GPU_OK : BL_GPU_ECUDA;
+}
+
+// The scratch's address in the current context: looked up afresh unless the stream is capturing, then remembered.
+int scratch_address(cudaStream_t s, float4** out) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    // a runtime call first, so that the thread has a current context (the device's primary one if it had none)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const bool capturing = cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+    void* ctx = nullptr;
+    if (current_context(&ctx) != BL_GPU_OK) return BL_GPU_ECUDA;
+    int slot = -1;
+    for (int i = 0; i < 64; i++)
+        if (g_slots[i].ctx == ctx) slot = i;
+    if (capturing && slot >= 0) {
+        *out = g_slots[slot].fv;
+        return BL_GPU_OK;
+    }
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_fv) != cudaSuccess || !p) return BL_GPU_ECUDA;
+    if (slot < 0) slot = g_next_slot, g_next_slot = (g_next_slot + 1) % 64;
+    g_slots[slot] = {ctx, (float4*)p};
+    *out = (float4*)p;
+    return BL_GPU_OK;
+}
 
 } // namespace
 
@@ -141,21 +188,19 @@ extern "C" int bl_gpu_substep_noalloc(bl_node* nodes, int32_t n_nodes, bl_beam* 
     if (n_nodes < 0 || n_beams < 0 || !gravity || !(dt > 0) || (n_nodes > 0 && (!nodes || !inc_ptr)) || (n_beams > 0 && (!beams || !inc)))
         return BL_GPU_EINVAL;
     if (n_beams > BL_GPU_NOALLOC_MAX_BEAMS) return BL_GPU_ELIMIT;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return BL_GPU_ECUDA;
-    float4* fv = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_fv_ptr[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_fv) != cudaSuccess || !p) return BL_GPU_ECUDA;
-            g_fv_ptr[dev] = (float4*)p;
-        }
-        fv = g_fv_ptr[dev];
-    }
-    if (n_nodes == 0) return BL_GPU_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    if (n_beams > 0) k_noalloc_beams<<<(n_beams + 255) / 256, 256, 0, s>>>(nodes, beams, n_beams, allow_deform, allow_break, ductile, fv);
-    k_noalloc_nodes<<<(n_nodes + 255) / 256, 256, 0, s>>>(nodes, n_nodes, inc_ptr, inc, fv, gravity[0], gravity[1], gravity[2], dt);
-    return cudaGetLastError() == cudaSuccess ? BL_GPU_OK : BL_GPU_ECUDA;
+    float4* fv = nullptr;
+    if (scratch_address(s, &fv) != BL_GPU_OK) return BL_GPU_ECUDA;
+    if (n_nodes == 0) return BL_GPU_OK;
+    // each launch's own status (cudaLaunchKernel returns it), not an earlier error left pending by other code
+    if (n_beams > 0) {
+        const bl_node* cn = nodes;
+        void* args[] = {(void*)&cn, (void*)&beams, (void*)&n_beams, (void*)&allow_deform, (void*)&allow_break, (void*)&ductile, (void*)&fv};
+        if (cudaLaunchKernel((const void*)k_noalloc_beams, dim3((n_beams + 255) / 256), dim3(256), args, 0, s) != cudaSuccess) return BL_GPU_ECUDA;
+    }
+    const float4* cfv = fv;
+    float gx = gravity[0], gy = gravity[1], gz = gravity[2];
+    void* args[] = {(void*)&nodes, (void*)&n_nodes, (void*)&inc_ptr, (void*)&inc, (void*)&cfv, (void*)&gx, (void*)&gy, (void*)&gz, (void*)&dt};
+    if (cudaLaunchKernel((const void*)k_noalloc_nodes, dim3((n_nodes + 255) / 256), dim3(256), args, 0, s) != cudaSuccess) return BL_GPU_ECUDA;
+    return BL_GPU_OK;
 }

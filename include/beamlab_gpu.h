@@ -357,7 +357,10 @@ int bl_gpu_set_wheel_drive(bl_gpu_ctx* ctx, int32_t body, int32_t wheel, float t
 int bl_gpu_download_wheels(bl_gpu_ctx* ctx, int32_t body, int32_t* n, float* speed, float* avg_speed);
 
 /* SoftBody::wheel_speed and wheel_spin (softbody.cpp:723-766): the mean tread speed (m/s) and spin (rad/s) of the
- * body's forward-propelled wheels, for its drivetrain; 0 while it has none. Synchronous. */
+ * body's forward-propelled wheels, for its drivetrain. A body with none reads 0: the reference starts both at 0
+ * (softbody.h:1112-1113) and keeps the last value while no forward-propelled wheel steps, and this path's set of such
+ * wheels never changes (detached wheels, which the reference skips, are not modelled: a shim keeps a body that detaches
+ * a wheel on the reference's CPU path), so the two agree. Synchronous. */
 int bl_gpu_wheel_speed(bl_gpu_ctx* ctx, int32_t body, float* wheel_speed, float* wheel_spin);
 
 /* A body's FEM frame nodes (FemFrame::node / xd / q / w, frame_fem.h:331-350): body node, double position (3),
@@ -473,13 +476,19 @@ int bl_fem_pattern(const bl_node* nodes, const bl_node_info* info, int32_t n_nod
  * device buffers the caller owns, for callers that cannot let the library allocate GPU memory: their memory belongs to
  * another allocator (an engine's or a framework's pool), or they step where allocation is forbidden (a real-time frame
  * loop, a CUDA stream capture). No counterpart in the reference: it is the body part of bl_gpu_step_substeps without
- * a context, without statics and without the frame's bookkeeping, and gives the same node and beam states.
+ * a context, without statics and without the frame's bookkeeping. Only a plain beam body gets the node and beam states
+ * bl_gpu_step_substeps gives it: gravity and beams (normal, rope, support) alone - no shocks (a BL_BF_SHOCK beam is
+ * stepped as a beam with no force), no wheels or tyres, no air drag, no FEM frame, no contacts.
  * nodes / beams: device arrays of bl_node / bl_beam (in and out); inc_ptr (n_nodes + 1) / inc (2 n_beams): device
  * arrays listing each node's beams in beam order, a beam's index with bit 31 set where the node is its b end.
+ * The caller guarantees every index: each beam's ends below n_nodes, each inc entry's beam below n_beams, inc_ptr
+ * ascending within [0, 2 n_beams]; nothing on the GPU checks them.
  * Allocates nothing: its per-beam scratch is a fixed device array of BL_GPU_NOALLOC_MAX_BEAMS entries (16 MiB, held by
- * every GPU that loads the library until exit), so more beams return BL_GPU_ELIMIT. The first call on a device looks
- * up that array's address and should come before any stream capture. Calls whose kernels overlap on the GPU share the
- * scratch and race; order them on one stream. Asynchronous on `stream` (NULL: the legacy default stream). */
+ * every GPU that loads the library until exit), so more beams return BL_GPU_ELIMIT. That array's address belongs to a
+ * CUDA context: it is looked up on every call whose stream is not capturing and kept per context for calls made during
+ * a capture, so the first call in a context should come before any stream capture. Calls whose kernels overlap on the
+ * GPU share the scratch and race; order them on one stream. Asynchronous on `stream` (NULL: the legacy default
+ * stream). */
 #define BL_GPU_NOALLOC_MAX_BEAMS (1 << 20)
 int bl_gpu_substep_noalloc(bl_node* nodes, int32_t n_nodes, bl_beam* beams, int32_t n_beams, const int32_t* inc_ptr, const int32_t* inc,
                            const float gravity[3], float dt, int32_t allow_deform, int32_t allow_break, int32_t ductile, void* stream);

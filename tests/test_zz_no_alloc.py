@@ -3,9 +3,13 @@ belongs to another allocator, or they step where allocation is forbidden): it mu
 
 The test allocates the body's device buffers itself (as such a caller does, here through torch), calls the entry
 point twice in a row through the C ABI, and after each call compares the nodes and beams with the context API's
-(bl_gpu_step_substeps, one-substep frames) on the same rig - bitwise, the tolerance of every parity test here. It
-runs alone in a fresh process as well as after the other tests."""
+(bl_gpu_step_substeps, one-substep frames) on the same rig - bitwise, the tolerance of every parity test here. The
+file sorts last, so it runs after the other tests; test_noalloc_in_a_fresh_process runs the comparison again in a
+python process of its own, where the entry point's first call is the process's first use of the GPU."""
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -85,3 +89,12 @@ def test_noalloc_rejects_too_many_beams():
     n = L.bl_gpu_substep_noalloc(C.c_void_p(16), 1, C.c_void_p(16), (1 << 20) + 1, C.c_void_p(16), C.c_void_p(16),
                                  (C.c_float * 3)(0, -9.81, 0), 0.0005, 1, 1, 0, None)
     assert n == -5 and L.bl_gpu_error_string(n).decode() == "capacity exceeded"
+
+
+def test_noalloc_in_a_fresh_process():
+    here = os.path.dirname(os.path.abspath(__file__))
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-p", "no:cacheprovider", "-m", "gpu",
+                        f"{os.path.join(here, 'test_zz_no_alloc.py')}::test_noalloc_substep_matches_the_context_api"],
+                       cwd=os.path.dirname(here), capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert "1 passed" in r.stdout
