@@ -13,6 +13,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 namespace blg {
@@ -316,148 +317,221 @@ static void fem_finalize(FemModel& M, const float* px, const float* py, const fl
     }
 }
 
-// FemFrame::analyse + gather_lists (frame_fem.cpp:544-901) for members and triangle elements
-static void fem_analyse(FemModel& M) {
+// ------------------------------------------------------------------------------------------ the symbolic phase
+// What FemFrame::analyse + gather_lists (frame_fem.cpp:544-901) compute for members and triangle elements, by a
+// design of this file's own. The results that must match the reference bit for bit are fixed by rules, not by the
+// reference's data structures:
+//  * components: frame nodes joined by members and unbroken triangles, numbered in order of their lowest node;
+//  * the elimination order, component after component: exact minimum degree on the elimination graph (a node's degree
+//    counts its neighbours once the nodes before it are eliminated, each elimination joining its neighbours into a
+//    clique), the ties going to the lowest frame node;
+//  * the factor's pattern: column k's rows are its node's neighbours at its elimination, in elimination positions,
+//    ascending;
+//  * the update list: for each column k, each pair of its rows (i <= j, by position) in order - the product of blocks
+//    i and j of column k subtracts from block (row j, column row i), or from that column's diagonal when i == j.
+// Here the elimination graph is never formed: the ordering runs on the quotient graph, in which every eliminated
+// node becomes an element standing for the clique of its neighbours and absorbs the elements next to it, so that a
+// node's neighbourhood is its remaining node neighbours plus the nodes of its elements, and every degree is counted
+// exactly (no approximate degrees, no supervariables: either could change a tie). The least (degree, node) is kept
+// in a binary heap whose stale entries are skipped when they surface.
+
+struct FemComponents {
+    int count = 0;
+    std::vector<int> of;                 // per frame node
+    std::vector<std::vector<int>> nodes; // per component, its nodes ascending
+};
+
+// each frame node's distinct neighbours (CSR, ascending) from the members and the unbroken triangles' edges
+static void fem_graph(const FemModel& M, std::vector<int>& ptr, std::vector<int>& nbr) {
     const int n = (int)M.node.size();
-    const size_t T = M.tn.size();
-    std::vector<int> up(n);
-    for (int i = 0; i < n; i++) up[i] = i;
-    auto find = [&](int x) {
-        while (up[x] != x) x = up[x] = up[up[x]];
-        return x;
-    };
-    const size_t E = M.mn.size();
-    for (size_t e = 0; e < E; e++) up[find(M.mn[e][0])] = find(M.mn[e][1]);
-    for (size_t t = 0; t < T; t++)
-        if (!M.tbroken[t]) up[find(M.tn[t][0])] = find(M.tn[t][1]), up[find(M.tn[t][1])] = find(M.tn[t][2]);
-    std::vector<std::pair<int, int>> edge;
-    for (size_t e = 0; e < E; e++)
-        if (M.mn[e][0] != M.mn[e][1]) edge.push_back({M.mn[e][0], M.mn[e][1]});
-    for (size_t t = 0; t < T; t++) {
-        if (M.tbroken[t]) continue;
-        const int a = M.tn[t][0], b = M.tn[t][1], c = M.tn[t][2];
-        if (a != b) edge.push_back({a, b});
-        if (b != c) edge.push_back({b, c});
-        if (c != a) edge.push_back({c, a});
-    }
-    std::vector<int> comp_of(n, -1), roots;
-    for (int i = 0; i < n; i++) {
-        const int r = find(i);
-        if (comp_of[r] < 0) comp_of[r] = (int)roots.size(), roots.push_back(r);
-        comp_of[i] = comp_of[r];
-    }
-    const int nc = (int)roots.size();
-    // each node's neighbours once
     std::vector<std::vector<int>> adj(n);
-    for (const auto& e : edge) adj[e.first].push_back(e.second), adj[e.second].push_back(e.first);
-    std::vector<std::vector<int>> comp_nodes(nc);
-    for (int i = 0; i < n; i++) comp_nodes[comp_of[i]].push_back(i);
-    M.ncomp = nc;
-    M.perm.assign(n, 0), M.iperm.assign(n, 0);
-    M.comp_first.assign(nc + 1, 0);
-    // exact minimum degree over the elimination graph as bit rows: the node taken is the first of least degree in the
-    // component's order; its elimination joins its neighbours to each other
-    std::vector<int> cols_ptr(n + 1, 0), cols_buf, loc(n, -1), deg;
-    std::vector<uint64_t> bits, bucket;
-    int k = 0;
-    for (int c = 0; c < nc; c++) {
-        M.comp_first[c] = k;
-        const std::vector<int>& cn = comp_nodes[c];
-        const int m = (int)cn.size(), W = (m + 63) / 64;
-        for (int x = 0; x < m; x++) loc[cn[x]] = x;
-        bits.assign((size_t)m * W, 0ull);
-        bucket.assign((size_t)(m + 1) * W, 0ull);
-        deg.assign(m, 0);
-        int mind = m;
-        for (int x = 0; x < m; x++) {
-            uint64_t* rx = &bits[(size_t)x * W];
-            for (int y0 : adj[cn[x]]) {
-                const int y = loc[y0];
-                rx[y >> 6] |= 1ull << (y & 63);
-            }
-            int d = 0;
-            for (int q = 0; q < W; q++) d += __builtin_popcountll(rx[q]);
-            deg[x] = d;
-            bucket[(size_t)d * W + (x >> 6)] |= 1ull << (x & 63);
-            mind = std::min(mind, d);
-        }
-        for (int step = 0; step < m; step++, k++) {
-            int v = -1;
-            while (v < 0) {
-                const uint64_t* bd = &bucket[(size_t)mind * W];
-                for (int w = 0; w < W; w++)
-                    if (bd[w]) {
-                        v = (w << 6) + __builtin_ctzll(bd[w]);
-                        break;
-                    }
-                if (v < 0) mind++;
-            }
-            bucket[(size_t)deg[v] * W + (v >> 6)] &= ~(1ull << (v & 63));
-            M.perm[k] = cn[v];
-            M.iperm[cn[v]] = k;
-            uint64_t* rv = &bits[(size_t)v * W];
-            for (int w = 0; w < W; w++)
-                for (uint64_t bb = rv[w]; bb; bb &= bb - 1) {
-                    const int y = (w << 6) + __builtin_ctzll(bb);
-                    cols_buf.push_back(cn[y]);
-                    uint64_t* ry = &bits[(size_t)y * W];
-                    for (int q = 0; q < W; q++) ry[q] |= rv[q];
-                    ry[y >> 6] &= ~(1ull << (y & 63));
-                    ry[v >> 6] &= ~(1ull << (v & 63));
-                    int d = 0;
-                    for (int q = 0; q < W; q++) d += __builtin_popcountll(ry[q]);
-                    bucket[(size_t)deg[y] * W + (y >> 6)] &= ~(1ull << (y & 63));
-                    bucket[(size_t)d * W + (y >> 6)] |= 1ull << (y & 63);
-                    deg[y] = d;
-                    mind = std::min(mind, d);
-                }
-            for (int w = 0; w < W; w++) rv[w] = 0;
-            cols_ptr[k + 1] = (int)cols_buf.size();
-        }
-    }
-    M.comp_first[nc] = k;
-    // the columns' rows (sorted) and the right-looking update list with its targets
-    M.col_ptr.assign(n + 1, 0);
-    M.row.resize(cols_buf.size());
-    for (int kk = 0; kk < n; kk++) {
-        const int a0 = cols_ptr[kk], a1 = cols_ptr[kk + 1];
-        for (int q = a0; q < a1; q++) M.row[q] = M.iperm[cols_buf[q]];
-        std::sort(M.row.begin() + a0, M.row.begin() + a1);
-        M.col_ptr[kk + 1] = a1;
-    }
-    auto find_block = [&](int col, int r) {
-        const int* a = M.row.data() + M.col_ptr[col];
-        const int* e = M.row.data() + M.col_ptr[col + 1];
-        const int* it = std::lower_bound(a, e, r);
-        return it != e && *it == r ? (int)(it - M.row.data()) : -1;
+    auto join = [&](int a, int b) {
+        if (a == b) return;
+        adj[a].push_back(b), adj[b].push_back(a);
     };
-    M.upd_ptr.assign(n + 1, 0);
-    M.upd.clear();
-    for (int kk = 0; kk < n; kk++) {
-        for (int pi = M.col_ptr[kk]; pi < M.col_ptr[kk + 1]; pi++) {
-            const int c = M.row[pi], qe = M.col_ptr[c + 1];
-            int q = M.col_ptr[c];
-            for (int pj = pi; pj < M.col_ptr[kk + 1]; pj++) {
-                int target;
-                if (pi == pj) {
-                    target = -(c + 1);
-                } else {
-                    const int rr = M.row[pj];
-                    while (q < qe && M.row[q] < rr) q++;
-                    target = q < qe && M.row[q] == rr ? q : -1;
-                }
-                M.upd.push_back({pi, pj, target});
-            }
-        }
-        M.upd_ptr[kk + 1] = (int)M.upd.size();
+    for (const auto& m : M.mn) join(m[0], m[1]);
+    for (size_t t = 0; t < M.tn.size(); t++)
+        if (!M.tbroken[t])
+            for (int e = 0; e < 3; e++) join(M.tn[t][e], M.tn[t][(e + 1) % 3]);
+    ptr.assign(n + 1, 0);
+    nbr.clear();
+    for (int i = 0; i < n; i++) {
+        std::sort(adj[i].begin(), adj[i].end());
+        adj[i].erase(std::unique(adj[i].begin(), adj[i].end()), adj[i].end());
+        nbr.insert(nbr.end(), adj[i].begin(), adj[i].end());
+        ptr[i + 1] = (int)nbr.size();
     }
-    M.mblock.assign(E, -1);
-    M.mswap.assign(E, 0);
+}
+
+// connected components by breadth-first search from each not yet labelled node in ascending order: component c is
+// the one whose lowest node is the c-th lowest such node
+static FemComponents fem_components(int n, const std::vector<int>& ptr, const std::vector<int>& nbr) {
+    FemComponents C;
+    C.of.assign(n, -1);
+    std::vector<int> queue;
+    for (int s = 0; s < n; s++) {
+        if (C.of[s] >= 0) continue;
+        const int c = C.count++;
+        queue.assign(1, s);
+        C.of[s] = c;
+        for (size_t h = 0; h < queue.size(); h++)
+            for (int q = ptr[queue[h]]; q < ptr[queue[h] + 1]; q++)
+                if (C.of[nbr[q]] < 0) C.of[nbr[q]] = c, queue.push_back(nbr[q]);
+        std::sort(queue.begin(), queue.end());
+        C.nodes.push_back(queue);
+    }
+    return C;
+}
+
+// Exact minimum degree on the quotient graph of one component. Appends the component's nodes to order (in elimination
+// order) and, per eliminated node, its neighbours at elimination (frame node ids) to reach / reach_ptr.
+struct QuotientGraph {
+    std::vector<std::vector<int>> var_adj;  // per node: node neighbours not yet covered by an element
+    std::vector<std::vector<int>> elem_adj; // per node: adjacent elements (an element is named by its eliminated node)
+    std::vector<std::vector<int>> members;  // per element: the nodes of its clique
+    std::vector<uint8_t> eliminated, absorbed;
+    std::vector<int> degree, mark;
+    int stamp = 0;
+
+    explicit QuotientGraph(int n) : var_adj(n), elem_adj(n), members(n), eliminated(n, 0), absorbed(n, 0), degree(n, 0), mark(n, 0) {}
+
+    int next_stamp() {
+        if (++stamp == 0x7fffffff) std::fill(mark.begin(), mark.end(), 0), stamp = 1;
+        return stamp;
+    }
+    // |neighbourhood of y| - |fresh| where the nodes of element `fresh` (marked with `inside`) are counted by the caller
+    int outside_count(int y, int fresh, int inside) {
+        const int seen = next_stamp();
+        int d = 0;
+        for (int z : var_adj[y])
+            if (mark[z] != inside && mark[z] != seen) mark[z] = seen, d++;
+        for (int e : elem_adj[y]) {
+            if (e == fresh) continue;
+            for (int z : members[e])
+                if (z != y && mark[z] != inside && mark[z] != seen) mark[z] = seen, d++;
+        }
+        return d;
+    }
+};
+
+static void fem_min_degree(const std::vector<int>& comp, const std::vector<int>& ptr, const std::vector<int>& nbr, QuotientGraph& G,
+                           std::vector<int>& order, std::vector<int>& reach, std::vector<int>& reach_ptr) {
+    typedef std::pair<int, int> Key; // (degree, node): the heap's least is the next pivot
+    std::vector<Key> heap;
+    auto push = [&](int d, int y) {
+        heap.push_back({d, y});
+        std::push_heap(heap.begin(), heap.end(), std::greater<Key>());
+    };
+    for (int x : comp) {
+        G.var_adj[x].assign(nbr.begin() + ptr[x], nbr.begin() + ptr[x + 1]);
+        G.degree[x] = ptr[x + 1] - ptr[x];
+        push(G.degree[x], x);
+    }
+    std::vector<int> clique;
+    for (size_t step = 0; step < comp.size(); step++) {
+        int p = -1;
+        while (p < 0) {
+            std::pop_heap(heap.begin(), heap.end(), std::greater<Key>());
+            const Key k = heap.back();
+            heap.pop_back();
+            if (!G.eliminated[k.second] && G.degree[k.second] == k.first) p = k.second;
+        }
+        G.eliminated[p] = 1;
+        order.push_back(p);
+        // p's neighbourhood: its node neighbours and the nodes of its elements, which p's element absorbs
+        const int in = G.next_stamp();
+        G.mark[p] = in;
+        clique.clear();
+        for (int z : G.var_adj[p])
+            if (G.mark[z] != in) G.mark[z] = in, clique.push_back(z);
+        for (int e : G.elem_adj[p]) {
+            for (int z : G.members[e])
+                if (G.mark[z] != in) G.mark[z] = in, clique.push_back(z);
+            G.absorbed[e] = 1;
+            std::vector<int>().swap(G.members[e]);
+        }
+        std::vector<int>().swap(G.var_adj[p]);
+        std::vector<int>().swap(G.elem_adj[p]);
+        reach.insert(reach.end(), clique.begin(), clique.end());
+        reach_ptr.push_back((int)reach.size());
+        G.members[p] = clique;
+        // each neighbour: its node neighbours inside the clique are now covered by p's element (p itself goes too),
+        // its absorbed elements are replaced by p's; then its exact degree
+        for (int y : clique) {
+            std::vector<int>& va = G.var_adj[y];
+            size_t w = 0;
+            for (int z : va)
+                if (G.mark[z] != in) va[w++] = z;
+            va.resize(w);
+            std::vector<int>& ea = G.elem_adj[y];
+            w = 0;
+            for (int e : ea)
+                if (!G.absorbed[e]) ea[w++] = e;
+            ea.resize(w);
+            ea.push_back(p);
+        }
+        const int base = (int)clique.size() - 1; // (each neighbour sees the rest of the clique)
+        for (int y : clique) {
+            const int d = base + G.outside_count(y, p, in);
+            if (d != G.degree[y]) G.degree[y] = d, push(d, y);
+        }
+    }
+}
+
+// FemModel's ordering, pattern, block maps and gather lists; the update list too where want_updates
+static void fem_analyse(FemModel& M, bool want_updates = true) {
+    const int n = (int)M.node.size();
+    const size_t T = M.tn.size(), E = M.mn.size();
+    std::vector<int> gptr, gnbr;
+    fem_graph(M, gptr, gnbr);
+    const FemComponents C = fem_components(n, gptr, gnbr);
+    M.ncomp = C.count;
+    M.comp_first.assign(C.count + 1, 0);
+    std::vector<int> order, reach, reach_ptr(1, 0);
+    order.reserve(n);
+    QuotientGraph G(n);
+    for (int c = 0; c < C.count; c++) {
+        M.comp_first[c] = (int)order.size();
+        fem_min_degree(C.nodes[c], gptr, gnbr, G, order, reach, reach_ptr);
+    }
+    M.comp_first[C.count] = n;
+    M.perm = order;
+    M.iperm.assign(n, 0);
+    for (int k = 0; k < n; k++) M.iperm[order[k]] = k;
+    // the pattern: column k's rows are the elimination positions of its node's neighbours at elimination, ascending
+    M.col_ptr.assign(reach_ptr.begin(), reach_ptr.end());
+    M.row.resize(reach.size());
+    for (size_t q = 0; q < reach.size(); q++) M.row[q] = M.iperm[reach[q]];
+    for (int k = 0; k < n; k++) std::sort(M.row.begin() + M.col_ptr[k], M.row.begin() + M.col_ptr[k + 1]);
+    // the off-diagonal block (row r, column k < r): its index in row, or -1 where the pattern has none
+    auto block_at = [&](int k, int r) {
+        const auto first = M.row.begin() + M.col_ptr[k], last = M.row.begin() + M.col_ptr[k + 1];
+        const auto range = std::equal_range(first, last, r);
+        return range.first == range.second ? -1 : (int)(range.first - M.row.begin());
+    };
+    M.upd.clear();
+    M.upd_ptr.assign(n + 1, 0);
+    if (want_updates) {
+        // each source column k: the rows of column c = row[i] scattered into a position table once, then every later
+        // row j of column k looked up in it
+        std::vector<int> pos(n, -1);
+        for (int k = 0; k < n; k++) {
+            const int a0 = M.col_ptr[k], a1 = M.col_ptr[k + 1];
+            for (int i = a0; i < a1; i++) {
+                const int c = M.row[i];
+                for (int q = M.col_ptr[c]; q < M.col_ptr[c + 1]; q++) pos[M.row[q]] = q;
+                M.upd.push_back({i, i, -(c + 1)});
+                for (int j = i + 1; j < a1; j++) M.upd.push_back({i, j, pos[M.row[j]]});
+                for (int q = M.col_ptr[c]; q < M.col_ptr[c + 1]; q++) pos[M.row[q]] = -1;
+            }
+            M.upd_ptr[k + 1] = (int)M.upd.size();
+        }
+    }
+    // each member's and each triangle edge's block (the block's row is the end eliminated later)
+    M.mblock.assign(E, -1), M.mswap.assign(E, 0);
     for (size_t e = 0; e < E; e++) {
         const int ka = M.iperm[M.mn[e][0]], kb = M.iperm[M.mn[e][1]];
-        if (ka == kb) continue;
-        M.mblock[e] = find_block(std::min(ka, kb), std::max(ka, kb));
-        M.mswap[e] = ka > kb;
+        if (ka != kb) M.mblock[e] = block_at(std::min(ka, kb), std::max(ka, kb)), M.mswap[e] = ka > kb;
     }
     M.tri_block.assign(T, {-1, -1, -1});
     M.tri_swap.assign(T, {0, 0, 0});
@@ -465,43 +539,32 @@ static void fem_analyse(FemModel& M) {
         if (M.tbroken[t]) continue;
         for (int e = 0; e < 3; e++) {
             const int ki = M.iperm[M.tn[t][e]], kj = M.iperm[M.tn[t][(e + 1) % 3]];
-            if (ki == kj) continue;
-            M.tri_block[t][e] = find_block(std::min(ki, kj), std::max(ki, kj));
-            M.tri_swap[t][e] = ki > kj;
+            if (ki != kj) M.tri_block[t][e] = block_at(std::min(ki, kj), std::max(ki, kj)), M.tri_swap[t][e] = ki > kj;
         }
     }
-    // gather lists in the triangles' order (gather_lists, frame_fem.cpp:863-901)
-    M.gdiag_ptr.assign(n + 1, 0);
-    M.goff_ptr.assign(M.row.size() + 1, 0);
+    // gather lists: each column's entries (members' ends, then triangles' corners) and each block's (members, then
+    // triangle edges), each in element order - built as lists and flattened
+    std::vector<std::vector<std::array<int, 2>>> dl(n);
+    std::vector<std::vector<std::array<int, 3>>> ol(M.row.size());
     for (size_t e = 0; e < E; e++) {
-        M.gdiag_ptr[M.iperm[M.mn[e][0]] + 1]++, M.gdiag_ptr[M.iperm[M.mn[e][1]] + 1]++;
-        if (M.mblock[e] >= 0) M.goff_ptr[M.mblock[e] + 1]++;
+        const int tag = -(int)e - 1;
+        dl[M.iperm[M.mn[e][0]]].push_back({tag, 0});
+        dl[M.iperm[M.mn[e][1]]].push_back({tag, 1});
+        if (M.mblock[e] >= 0) ol[M.mblock[e]].push_back({tag, M.mswap[e] ? 3 : 2, 0}); // (3: the row node is the a end)
     }
     for (size_t t = 0; t < T; t++) {
         if (M.tbroken[t]) continue;
-        for (int c = 0; c < 3; c++) M.gdiag_ptr[M.iperm[M.tn[t][c]] + 1]++;
-        for (int e = 0; e < 3; e++)
-            if (M.tri_block[t][e] >= 0) M.goff_ptr[M.tri_block[t][e] + 1]++;
+        for (int c = 0; c < 3; c++) dl[M.iperm[M.tn[t][c]]].push_back({(int)t, c});
+        for (int e = 0; e < 3; e++) {
+            if (M.tri_block[t][e] < 0) continue;
+            const int i = e, j = (e + 1) % 3; // (the entry: the block's row corner, then its column corner)
+            ol[M.tri_block[t][e]].push_back(M.tri_swap[t][e] ? std::array<int, 3>{(int)t, i, j} : std::array<int, 3>{(int)t, j, i});
+        }
     }
-    for (size_t q = 1; q < M.gdiag_ptr.size(); q++) M.gdiag_ptr[q] += M.gdiag_ptr[q - 1];
-    for (size_t q = 1; q < M.goff_ptr.size(); q++) M.goff_ptr[q] += M.goff_ptr[q - 1];
-    M.gdiag.assign(M.gdiag_ptr.back(), {0, 0});
-    M.goff.assign(M.goff_ptr.back(), {0, 0, 0});
-    std::vector<int> fd(M.gdiag_ptr.begin(), M.gdiag_ptr.end() - 1), fo(M.goff_ptr.begin(), M.goff_ptr.end() - 1);
-    for (size_t e = 0; e < E; e++) {
-        M.gdiag[fd[M.iperm[M.mn[e][0]]]++] = {-(int)e - 1, 0};
-        M.gdiag[fd[M.iperm[M.mn[e][1]]]++] = {-(int)e - 1, 1};
-        if (M.mblock[e] >= 0) M.goff[fo[M.mblock[e]]++] = {-(int)e - 1, M.mswap[e] ? 3 : 2, 0}; // (the row node's: b, or a)
-    }
-    for (size_t t = 0; t < T; t++) {
-        if (M.tbroken[t]) continue;
-        for (int c = 0; c < 3; c++) M.gdiag[fd[M.iperm[M.tn[t][c]]]++] = {(int)t, c};
-        for (int e = 0; e < 3; e++)
-            if (M.tri_block[t][e] >= 0) { // (the block's row is the later corner in the order)
-                const int i = e, j = (e + 1) % 3;
-                M.goff[fo[M.tri_block[t][e]]++] = {(int)t, M.tri_swap[t][e] ? i : j, M.tri_swap[t][e] ? j : i};
-            }
-    }
+    M.gdiag_ptr.assign(1, 0), M.goff_ptr.assign(1, 0);
+    M.gdiag.clear(), M.goff.clear();
+    for (const auto& l : dl) M.gdiag.insert(M.gdiag.end(), l.begin(), l.end()), M.gdiag_ptr.push_back((int)M.gdiag.size());
+    for (const auto& l : ol) M.goff.insert(M.goff.end(), l.begin(), l.end()), M.goff_ptr.push_back((int)M.goff.size());
 }
 
 } // namespace blg
