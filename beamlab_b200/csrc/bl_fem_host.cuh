@@ -76,118 +76,139 @@ static inline HQ hfrom_mat3(HF3 c0, HF3 c1, HF3 c2) {
 // membrane flows (k_tri_eval): one source for both, compiled for each, so that both give the same bits.
 #define BL_HD __host__ __device__
 
-// The DKT bending's curvature-displacement matrix at area coordinates (xi, eta) (frame_fem.cpp:1482-1509)
-BL_HD inline void dkt_b(const double x[3], const double y[3], double xi, double eta, double B[3][9]) {
-    const double x23 = x[1] - x[2], x31 = x[2] - x[0], x12 = x[0] - x[1];
-    const double y23 = y[1] - y[2], y31 = y[2] - y[0], y12 = y[0] - y[1];
-    double P[7], q[7], r[7], t[7];
-    const double xs[3] = {x23, x31, x12}, ys[3] = {y23, y31, y12};
-    for (int k = 4; k <= 6; k++) {
-        const double xij = xs[k - 4], yij = ys[k - 4], l2 = xij * xij + yij * yij;
-        P[k] = -6 * xij / l2, q[k] = 3 * xij * yij / l2, t[k] = -6 * yij / l2, r[k] = 3 * yij * yij / l2;
-    }
-    const double a = 1 - 2 * xi, bb = 1 - 2 * eta;
-    const double Hx_xi[9] = {P[6] * a + (P[5] - P[6]) * eta, q[6] * a - (q[5] + q[6]) * eta, -4 + 6 * (xi + eta) + r[6] * a - eta * (r[5] + r[6]),
-                             -P[6] * a + eta * (P[4] + P[6]), q[6] * a - eta * (q[6] - q[4]), -2 + 6 * xi + r[6] * a + eta * (r[4] - r[6]),
-                             -eta * (P[5] + P[4]), eta * (q[4] - q[5]), -eta * (r[5] - r[4])};
-    const double Hy_xi[9] = {t[6] * a + eta * (t[5] - t[6]), 1 + r[6] * a - eta * (r[5] + r[6]), -q[6] * a + eta * (q[5] + q[6]),
-                             -t[6] * a + eta * (t[4] + t[6]), -1 + r[6] * a + eta * (r[4] - r[6]), -q[6] * a - eta * (q[4] - q[6]),
-                             -eta * (t[4] + t[5]), eta * (r[4] - r[5]), -eta * (q[4] - q[5])};
-    const double Hx_eta[9] = {-P[5] * bb - xi * (P[6] - P[5]), q[5] * bb - xi * (q[5] + q[6]), -4 + 6 * (xi + eta) + r[5] * bb - xi * (r[5] + r[6]),
-                              xi * (P[4] + P[6]), xi * (q[4] - q[6]), -xi * (r[6] - r[4]),
-                              P[5] * bb - xi * (P[4] + P[5]), q[5] * bb + xi * (q[4] - q[5]), -2 + 6 * eta + r[5] * bb + xi * (r[4] - r[5])};
-    const double Hy_eta[9] = {-t[5] * bb - xi * (t[6] - t[5]), 1 + r[5] * bb - xi * (r[5] + r[6]), -q[5] * bb + xi * (q[5] + q[6]),
-                              xi * (t[4] + t[6]), xi * (r[4] - r[6]), -xi * (q[4] - q[6]),
-                              t[5] * bb - xi * (t[4] + t[5]), -1 + r[5] * bb + xi * (r[4] - r[5]), -q[5] * bb - xi * (q[4] - q[5])};
-    const double A2 = x31 * y12 - x12 * y31, iA = 1.0 / A2;
-    for (int j = 0; j < 9; j++) {
-        B[0][j] = (y31 * Hx_xi[j] + y12 * Hx_eta[j]) * iA;
-        B[1][j] = (-x31 * Hy_xi[j] - x12 * Hy_eta[j]) * iA;
-        B[2][j] = (-x31 * Hx_xi[j] - x12 * Hx_eta[j] + y31 * Hy_xi[j] + y12 * Hy_eta[j]) * iA;
-    }
-}
+// ------------------------------------------------------------------------------------------ the shell element
+// A flat triangle in its own axes (x, y in its plane): corners X[i], 6 dofs each (u, v, w, theta_x, theta_y,
+// theta_z). Membrane: the constant-strain triangle. Bending: the discrete Kirchhoff triangle (DKT; Batoz, Bathe & Ho,
+// Int. J. Numer. Meth. Eng. 15, 1980), sampled at three points. Drilling: a penalty tying each corner's theta_z to the
+// element's in-plane rotation. Restated here from those definitions (the reference's tri_local_k,
+// frame_fem.cpp:1524-1574, builds the same element).
 
-// the membrane's shape gradients (frame_fem.cpp:1513-1520)
-BL_HD inline void tri_grad(const float X[3][2], double b[3], double c[3], double& A2) {
+// The triangle's linear geometry: twice its signed area and the area coordinates' gradients, dL_i/dx = b_i / A2,
+// dL_i/dy = c_i / A2, where (b_i, c_i) is the edge opposite corner i (from corner i+1 to corner i+2) turned by -90
+// degrees.
+struct TriGeom {
+    double b[3], c[3], A2;
+};
+template <class XY>
+BL_HD inline TriGeom tri_geom(const XY& X) {
+    TriGeom g;
     for (int i = 0; i < 3; i++) {
-        const int j = (i + 1) % 3, k = (i + 2) % 3;
-        b[i] = (double)X[j][1] - X[k][1];
-        c[i] = (double)X[k][0] - X[j][0];
+        const int j = i == 2 ? 0 : i + 1, k = j == 2 ? 0 : j + 1;
+        const double ex = (double)X[k][0] - X[j][0], ey = (double)X[k][1] - X[j][1];
+        g.b[i] = -ey, g.c[i] = ex;
     }
-    A2 = ((double)X[1][0] - X[0][0]) * ((double)X[2][1] - X[0][1]) - ((double)X[2][0] - X[0][0]) * ((double)X[1][1] - X[0][1]);
+    g.A2 = ((double)X[1][0] - X[0][0]) * ((double)X[2][1] - X[0][1]) - ((double)X[2][0] - X[0][0]) * ((double)X[1][1] - X[0][1]);
+    return g;
+}
+// (the form the element kernels use)
+BL_HD inline void tri_grad(const float X[3][2], double b[3], double c[3], double& A2) {
+    const TriGeom g = tri_geom(X);
+    for (int i = 0; i < 3; i++) b[i] = g.b[i], c[i] = g.c[i];
+    A2 = g.A2;
 }
 
-// The element's stiffness in its own axes, 18 dofs [u v w theta_x theta_y theta_z] per corner: CST membrane, DKT
-// bending at three points, the drilling spring (frame_fem.cpp:1524-1574); packed as the reference's tri_k_: the
-// membrane's 9 x 9 then the plate's; and the bending's curvatures at the three points from the corners' rotations
-// alone, tri_b_ (tri_build_k, frame_fem.cpp:1625-1647). s: the section's E, nu, t, drill and its D() (float).
+// The DKT curvatures (kappa_x, kappa_y, 2 kappa_xy) at area coordinates (L1, L2) = (xi, eta) from the 9 bending dofs
+// (w, theta_x, theta_y per corner). The normal's rotation beta = (theta_y, -theta_x) is interpolated quadratically
+// over the six-node triangle; at each edge's midpoint its tangential part is what a cubic w along the edge gives
+// (beta_s = -dw/ds: -3 (w_j - w_i) / (2 l) - (beta_s,i + beta_s,j) / 4) and its normal part the corners' mean; the
+// curvatures are beta's derivatives: kappa_x = dbeta_x/dx, kappa_y = dbeta_y/dy, 2 kappa_xy = dbeta_x/dy + dbeta_y/dx.
+BL_HD inline void dkt_b(const double x[3], const double y[3], double xi, double eta, double B[3][9]) {
+    const double xy[3][2] = {{x[0], y[0]}, {x[1], y[1]}, {x[2], y[2]}};
+    const TriGeom g = tri_geom(xy);
+    const double L[3] = {1 - xi - eta, xi, eta};
+    // beta at the six nodes (corners 0-2, then the midpoints of edges 01, 12, 20) as rows over the 9 dofs
+    double bx[6][9], by[6][9];
+    for (int a = 0; a < 6; a++)
+        for (int d = 0; d < 9; d++) bx[a][d] = by[a][d] = 0;
+    for (int i = 0; i < 3; i++) bx[i][3 * i + 2] = 1, by[i][3 * i + 1] = -1;
+    for (int e = 0; e < 3; e++) {
+        const int i = e, j = e == 2 ? 0 : e + 1;
+        const double ex = x[j] - x[i], ey = y[j] - y[i], l = sqrt(ex * ex + ey * ey);
+        const double sx = ex / l, sy = ey / l, nx = sy, ny = -sx;
+        for (int d = 0; d < 9; d++) {
+            double bs = -0.25 * ((bx[i][d] + bx[j][d]) * sx + (by[i][d] + by[j][d]) * sy);
+            const double bn = 0.5 * ((bx[i][d] + bx[j][d]) * nx + (by[i][d] + by[j][d]) * ny);
+            if (d == 3 * i) bs += 1.5 / l;
+            if (d == 3 * j) bs -= 1.5 / l;
+            bx[3 + e][d] = bs * sx + bn * nx, by[3 + e][d] = bs * sy + bn * ny;
+        }
+    }
+    // the quadratic shape functions' gradients: corner L(2L - 1), midpoint 4 L_i L_j
+    double nxd[6], nyd[6];
+    for (int i = 0; i < 3; i++) nxd[i] = (4 * L[i] - 1) * g.b[i] / g.A2, nyd[i] = (4 * L[i] - 1) * g.c[i] / g.A2;
+    for (int e = 0; e < 3; e++) {
+        const int i = e, j = e == 2 ? 0 : e + 1;
+        nxd[3 + e] = 4 * (L[i] * g.b[j] + L[j] * g.b[i]) / g.A2, nyd[3 + e] = 4 * (L[i] * g.c[j] + L[j] * g.c[i]) / g.A2;
+    }
+    for (int d = 0; d < 9; d++) {
+        double kx = 0, ky = 0, kxy = 0;
+        for (int a = 0; a < 6; a++) kx += nxd[a] * bx[a][d], ky += nyd[a] * by[a][d], kxy += nyd[a] * bx[a][d] + nxd[a] * by[a][d];
+        B[0][d] = kx, B[1][d] = ky, B[2][d] = kxy;
+    }
+}
+
+// The element's stiffness in its own axes, stored as the membrane's 9 x 9 (dofs u, v, theta_z per corner) then the
+// plate's 9 x 9 (w, theta_x, theta_y per corner) - P[162] - and the bending's curvatures from the corners' rotations
+// alone at the three sample points (kappa rows x (theta_x, theta_y) per corner) - Bc[54]. s: the section's E, nu, t,
+// drill and its plate rigidity D() (float, as the section's).
 struct TriSec {
     float E, nu, t, drill;
     BL_HD float D() const { return E * t * t * t / (12.0f * (1.0f - nu * nu)); }
 };
 BL_HD inline void tri_local_k(const float X[3][2], const TriSec& s, float P[162], float Bc[54]) {
-    const double kGauss[3][2] = {{1.0 / 6, 1.0 / 6}, {2.0 / 3, 1.0 / 6}, {1.0 / 6, 2.0 / 3}};
-    const int kMem[3] = {0, 1, 5}, kPlate[3] = {2, 3, 4};
-    double K[18][18];
-    for (int i = 0; i < 18; i++)
-        for (int j = 0; j < 18; j++) K[i][j] = 0;
-    double b[3], c[3], A2;
-    tri_grad(X, b, c, A2);
-    if (A2 > 0) {
-        const double A = 0.5 * A2, nu = s.nu;
-        const double Dm = (double)s.E * s.t / (1 - nu * nu);
-        double Bm[3][6];
-        for (int i = 0; i < 3; i++) {
-            Bm[0][2 * i] = b[i] / A2, Bm[1][2 * i] = 0, Bm[2][2 * i] = c[i] / A2;
-            Bm[0][2 * i + 1] = 0, Bm[1][2 * i + 1] = c[i] / A2, Bm[2][2 * i + 1] = b[i] / A2;
-        }
-        const double D3[3][3] = {{1, nu, 0}, {nu, 1, 0}, {0, 0, 0.5 * (1 - nu)}};
-        for (int p = 0; p < 6; p++)
-            for (int q = 0; q < 6; q++) {
-                double v = 0;
-                for (int r = 0; r < 3; r++)
-                    for (int t = 0; t < 3; t++) v += Bm[r][p] * D3[r][t] * Bm[t][q];
-                K[6 * (p / 2) + p % 2][6 * (q / 2) + q % 2] += A * Dm * v;
-            }
-        const double x[3] = {X[0][0], X[1][0], X[2][0]}, y[3] = {X[0][1], X[1][1], X[2][1]};
-        const double Db = s.D();
-        for (const auto& g : kGauss) {
-            double B[3][9];
-            dkt_b(x, y, g[0], g[1], B);
-            for (int p = 0; p < 9; p++)
-                for (int q = 0; q < 9; q++) {
-                    double v = 0;
-                    for (int r = 0; r < 3; r++)
-                        for (int t = 0; t < 3; t++) v += B[r][p] * D3[r][t] * B[t][q];
-                    K[6 * (p / 3) + 2 + p % 3][6 * (q / 3) + 2 + q % 3] += A2 / 6.0 * Db * v;
-                }
-        }
-        const double G = (double)s.E / (2 * (1 + nu)), kd = (double)s.drill * G * s.t * A;
-        double gu[3], gv[3];
-        for (int i = 0; i < 3; i++) gu[i] = -c[i] / (2 * A2), gv[i] = b[i] / (2 * A2);
-        for (int i = 0; i < 3; i++) {
-            K[6 * i + 5][6 * i + 5] += kd;
+    // the three sample points (area coordinates L1, L2) of the bending, each weighted by a third of the area
+    const double pts[3][2] = {{1.0 / 6, 1.0 / 6}, {2.0 / 3, 1.0 / 6}, {1.0 / 6, 2.0 / 3}};
+    double Km[9][9], Kp[9][9]; // membrane (u, v, theta_z) and plate (w, theta_x, theta_y), corner-major
+    for (int r = 0; r < 9; r++)
+        for (int q = 0; q < 9; q++) Km[r][q] = Kp[r][q] = 0;
+    const TriGeom g = tri_geom(X);
+    const double x[3] = {X[0][0], X[1][0], X[2][0]}, y[3] = {X[0][1], X[1][1], X[2][1]};
+    if (g.A2 > 0) {
+        const double nu = s.nu, A = 0.5 * g.A2, half = 0.5 * (1 - nu);
+        // membrane: A t Bm^T Dm Bm pair by pair, Bm of corner i = [b_i 0; 0 c_i; c_i b_i] / A2
+        const double km = A * ((double)s.E * s.t / (1 - nu * nu)) / (g.A2 * g.A2);
+        for (int i = 0; i < 3; i++)
             for (int j = 0; j < 3; j++) {
-                K[6 * i + 5][6 * j] -= kd * gu[j], K[6 * j][6 * i + 5] -= kd * gu[j];
-                K[6 * i + 5][6 * j + 1] -= kd * gv[j], K[6 * j + 1][6 * i + 5] -= kd * gv[j];
-                K[6 * i][6 * j] += 3 * kd * gu[i] * gu[j], K[6 * i][6 * j + 1] += 3 * kd * gu[i] * gv[j];
-                K[6 * i + 1][6 * j] += 3 * kd * gv[i] * gu[j], K[6 * i + 1][6 * j + 1] += 3 * kd * gv[i] * gv[j];
+                const double bi = g.b[i], ci = g.c[i], bj = g.b[j], cj = g.c[j];
+                Km[3 * i][3 * j] += km * (bi * bj + half * ci * cj);
+                Km[3 * i][3 * j + 1] += km * (nu * bi * cj + half * ci * bj);
+                Km[3 * i + 1][3 * j] += km * (nu * ci * bj + half * bi * cj);
+                Km[3 * i + 1][3 * j + 1] += km * (ci * cj + half * bi * bj);
             }
+        // bending: sum over the points of (A / 3) D B^T [1 nu 0; nu 1 0; 0 0 (1 - nu) / 2] B
+        const double kb = A / 3.0 * (double)s.D();
+        for (const auto& pt : pts) {
+            double B[3][9];
+            dkt_b(x, y, pt[0], pt[1], B);
+            for (int q = 0; q < 9; q++) {
+                const double m0 = B[0][q] + nu * B[1][q], m1 = nu * B[0][q] + B[1][q], m2 = half * B[2][q]; // (D B)_q / D
+                for (int r = 0; r < 9; r++) Kp[r][q] += kb * (B[0][r] * m0 + B[1][r] * m1 + B[2][r] * m2);
+            }
+        }
+        // drilling: (kd / 2) sum_i (theta_z,i - omega)^2, omega = (dv/dx - du/dy) / 2 the element's in-plane rotation;
+        // with go omega's gradient over u / v, each corner adds kd r r^T, r = e(theta_z,i) - go
+        const double kd = (double)s.drill * ((double)s.E / (2 * (1 + nu))) * s.t * A;
+        double go[9];
+        for (int j = 0; j < 3; j++) go[3 * j] = -g.c[j] / (2 * g.A2), go[3 * j + 1] = g.b[j] / (2 * g.A2), go[3 * j + 2] = 0;
+        for (int i = 0; i < 3; i++) {
+            double r[9];
+            for (int q = 0; q < 9; q++) r[q] = -go[q];
+            r[3 * i + 2] += 1;
+            for (int a = 0; a < 9; a++)
+                for (int q = 0; q < 9; q++) Km[a][q] += kd * r[a] * r[q];
         }
     }
-    for (int a = 0; a < 9; a++)
-        for (int cc = 0; cc < 9; cc++) {
-            const int im = 6 * (a / 3) + kMem[a % 3], jm = 6 * (cc / 3) + kMem[cc % 3];
-            const int ip = 6 * (a / 3) + kPlate[a % 3], jp = 6 * (cc / 3) + kPlate[cc % 3];
-            P[a * 9 + cc] = (float)K[im < jm ? im : jm][im < jm ? jm : im];
-            P[81 + a * 9 + cc] = (float)K[ip < jp ? ip : jp][ip < jp ? jp : ip];
+    // (both stored exactly symmetric: each pair from the upper triangle)
+    for (int r = 0; r < 9; r++)
+        for (int q = 0; q < 9; q++) {
+            const int lo = r < q ? r : q, hi = r < q ? q : r;
+            P[r * 9 + q] = (float)Km[lo][hi], P[81 + r * 9 + q] = (float)Kp[lo][hi];
         }
-    const double x[3] = {X[0][0], X[1][0], X[2][0]}, y[3] = {X[0][1], X[1][1], X[2][1]};
-    for (int g = 0; g < 3; g++) {
+    for (int p = 0; p < 3; p++) {
         double B[3][9];
-        dkt_b(x, y, kGauss[g][0], kGauss[g][1], B);
-        for (int r = 0; r < 3; r++)
-            for (int i = 0; i < 3; i++) Bc[g * 18 + r * 6 + 2 * i] = (float)B[r][3 * i + 1], Bc[g * 18 + r * 6 + 2 * i + 1] = (float)B[r][3 * i + 2];
+        dkt_b(x, y, pts[p][0], pts[p][1], B);
+        for (int k = 0; k < 3; k++)
+            for (int i = 0; i < 3; i++) Bc[18 * p + 6 * k + 2 * i] = (float)B[k][3 * i + 1], Bc[18 * p + 6 * k + 2 * i + 1] = (float)B[k][3 * i + 2];
     }
 }
 

@@ -187,69 +187,93 @@ __device__ __forceinline__ double von_mises(const double m[3]) {
     return sqrt((0.0 < v) ? v : 0.0);
 }
 
-// A yielding section's flow (eval_tris, frame_fem.cpp:1690-1741, on a body that does not break): the membrane
-// radially back to the yield stress, the rest shape following the stretch (recentred; the plastic stretch against the
-// authored shape, its largest principal stretch, into dmg; the element built again); the bending's moments at the
-// three points against the plate's plastic moment, the corners' rest rotations following theirs past it; the plastic
-// rotations baked into the rest frames past 0.02 rad. X, th0, d, b3 / c3 / A2 and sig are the caller's, updated.
+// A yielding shell section (the flow eval_tris applies on a body that does not break, frame_fem.cpp:1690-1741), in
+// three steps of this file's own:
+//  membrane_return: where the membrane's von Mises stress exceeds the yield stress, the stress is returned radially to
+//    the yield surface: the fraction r = 1 - yield / sigma_eq of the in-plane displacements becomes permanent - the rest
+//    shape moves by it (then recentred on its centroid) and the element is built again - and the plastic stretch
+//    reached (the largest principal stretch of the rest shape against the authored one) is kept in dmg;
+//  bending_return: the same on the largest von Mises moment of the three sample points against the plate's plastic
+//    moment yield t^2 / 4: the corners' plastic rotations take the fraction r of their bending rotations;
+//  bake_rotations: a corner's plastic rotation past 0.02 rad goes into its rest frame.
+// X, th0, d, b3 / c3 / A2 and sig are the caller's and are updated.
+__device__ __forceinline__ float principal_stretch(const float* X0, const float X[3][2]) {
+    // F maps the authored edges (from corner 0) to the current rest edges; the stretch is sqrt of C = F^T F's larger
+    // eigenvalue, less one (0 where the authored shape is degenerate)
+    const double e0[2][2] = {{(double)X0[2] - X0[0], (double)X0[4] - X0[0]}, {(double)X0[3] - X0[1], (double)X0[5] - X0[1]}};
+    const double e[2][2] = {{(double)X[1][0] - X[0][0], (double)X[2][0] - X[0][0]}, {(double)X[1][1] - X[0][1], (double)X[2][1] - X[0][1]}};
+    const double det = e0[0][0] * e0[1][1] - e0[0][1] * e0[1][0];
+    if (!(fabs(det) > 1e-12)) return 0.0f;
+    const double inv[2][2] = {{e0[1][1] / det, -e0[0][1] / det}, {-e0[1][0] / det, e0[0][0] / det}};
+    double Fm[2][2];
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) Fm[i][j] = e[i][0] * inv[0][j] + e[i][1] * inv[1][j];
+    const double c00 = Fm[0][0] * Fm[0][0] + Fm[1][0] * Fm[1][0], c11 = Fm[0][1] * Fm[0][1] + Fm[1][1] * Fm[1][1];
+    const double c01 = Fm[0][0] * Fm[0][1] + Fm[1][0] * Fm[1][1];
+    const double lmax = 0.5 * (c00 + c11 + sqrt((c00 - c11) * (c00 - c11) + 4 * c01 * c01));
+    return (float)(sqrt(lmax) - 1.0);
+}
+
+template <class Membrane>
+__device__ __forceinline__ bool membrane_return(FemDev F, int ti, const FemSecDev& s, float X[3][2], double d[18], double b3[3], double c3[3],
+                                                double& A2, const double sig[3], float& dmg, Membrane membrane) {
+    const double seq = von_mises(sig);
+    if (!(seq > s.yield)) return false;
+    const double r = 1.0 - s.yield / seq;
+    for (int i = 0; i < 3; i++)
+        for (int a = 0; a < 2; a++) X[i][a] += (float)(r * d[6 * i + a]), d[6 * i + a] *= 1 - r;
+    const float mx = (X[0][0] + X[1][0] + X[2][0]) / 3.0f, my = (X[0][1] + X[1][1] + X[2][1]) / 3.0f;
+    for (int i = 0; i < 3; i++) X[i][0] -= mx, X[i][1] -= my;
+    dmg = smax(dmg, principal_stretch(F.tX0 + 6 * (size_t)ti, X));
+    tri_rebuild_k(F, ti, s, X);
+    tri_grad(X, b3, c3, A2);
+    membrane();
+    return true;
+}
+
+__device__ __forceinline__ void bending_return(FemDev F, int ti, const FemSecDev& s, v3 th0[3], double d[18], float& dmg) {
+    const float* Bc = F.tb + 54 * (size_t)ti;
+    const double D = s.E * s.t * s.t * s.t / (12.0f * (1.0f - s.nu * s.nu)), nu = s.nu, Mp = 0.25 * s.yield * (double)s.t * s.t;
+    double worst = 0;
+    for (int pt = 0; pt < 3; pt++) {
+        const float* Bp = Bc + 18 * pt;
+        double k[3];
+        for (int row = 0; row < 3; row++) {
+            k[row] = 0;
+            for (int i = 0; i < 3; i++) k[row] += Bp[6 * row + 2 * i] * d[6 * i + 3] + Bp[6 * row + 2 * i + 1] * d[6 * i + 4];
+        }
+        const double m[3] = {D * (k[0] + nu * k[1]), D * (nu * k[0] + k[1]), D * 0.5 * (1 - nu) * k[2]};
+        const double vm = von_mises(m);
+        worst = (worst < vm) ? vm : worst;
+    }
+    if (!(worst > Mp)) return;
+    const double r = 1.0 - Mp / worst;
+    for (int i = 0; i < 3; i++) {
+        th0[i].x += (float)(r * d[6 * i + 3]), th0[i].y += (float)(r * d[6 * i + 4]);
+        d[6 * i + 3] *= 1 - r, d[6 * i + 4] *= 1 - r;
+    }
+    dmg = smax(dmg, 1e-5f);
+}
+
+__device__ __forceinline__ void bake_rotations(FemDev F, int ti, v3 th0[3]) {
+    for (int i = 0; i < 3; i++) {
+        if (!(dot(th0[i], th0[i]) > 0.02f * 0.02f)) continue;
+        const float4 rf = F.tr0[3 * ti + i];
+        const q4 r0 = qnormalize(qmul(q4{rf.x, rf.y, rf.z, rf.w}, quat_exp(V(-th0[i].x, -th0[i].y, -th0[i].z))));
+        F.tr0[3 * ti + i] = make_float4(r0.x, r0.y, r0.z, r0.w);
+        th0[i] = V(0, 0, 0);
+    }
+}
+
 template <class Membrane>
 __device__ void tri_plastic_flow(FemDev F, int ti, const FemSecDev& s, float X[3][2], v3 th0[3], double d[18], double b3[3], double c3[3],
                                  double& A2, const double sig[3], Membrane membrane) {
     float dmg = F.tdmg[ti];
-    const double seq = von_mises(sig);
-    bool rest_moved = false, frames_moved = false;
-    if (seq > s.yield) {
-        const double r = 1.0 - s.yield / seq;
-        for (int i = 0; i < 3; i++) X[i][0] += (float)(r * d[6 * i]), X[i][1] += (float)(r * d[6 * i + 1]), d[6 * i] *= 1 - r, d[6 * i + 1] *= 1 - r;
-        const float mx = (X[0][0] + X[1][0] + X[2][0]) / 3.0f, my = (X[0][1] + X[1][1] + X[2][1]) / 3.0f;
-        for (int i = 0; i < 3; i++) X[i][0] -= mx, X[i][1] -= my;
-        const float* X0 = F.tX0 + 6 * (size_t)ti;
-        const double a0x = X0[2] - X0[0], a0y = X0[3] - X0[1], b0x = X0[4] - X0[0], b0y = X0[5] - X0[1];
-        const double ax = X[1][0] - X[0][0], ay = X[1][1] - X[0][1], bx = X[2][0] - X[0][0], by = X[2][1] - X[0][1];
-        const double det = a0x * b0y - b0x * a0y;
-        if (fabs(det) > 1e-12) {
-            const double i00 = b0y / det, i01 = -b0x / det, i10 = -a0y / det, i11 = a0x / det;
-            const double F00 = ax * i00 + bx * i10, F01 = ax * i01 + bx * i11, F10 = ay * i00 + by * i10, F11 = ay * i01 + by * i11;
-            const double C00 = F00 * F00 + F10 * F10, C01 = F00 * F01 + F10 * F11, C11 = F01 * F01 + F11 * F11;
-            const double lmax = 0.5 * (C00 + C11) + sqrt(0.25 * (C00 - C11) * (C00 - C11) + C01 * C01);
-            dmg = smax(dmg, (float)(sqrt(lmax) - 1.0));
-        }
-        rest_moved = true;
-        tri_rebuild_k(F, ti, s, X);
-        tri_grad(X, b3, c3, A2);
-        membrane();
-    }
-    const float* Bc = F.tb + 54 * (size_t)ti;
-    const float Df = s.E * s.t * s.t * s.t / (12.0f * (1.0f - s.nu * s.nu));
-    const double D = Df, nu = s.nu, Mp = 0.25 * s.yield * (double)s.t * s.t;
-    double meq = 0;
-    for (int g = 0; g < 3; g++) {
-        double kap[3] = {0, 0, 0};
-        for (int r = 0; r < 3; r++)
-            for (int i = 0; i < 3; i++) kap[r] += Bc[g * 18 + r * 6 + 2 * i] * d[6 * i + 3] + Bc[g * 18 + r * 6 + 2 * i + 1] * d[6 * i + 4];
-        const double m[3] = {D * (kap[0] + nu * kap[1]), D * (nu * kap[0] + kap[1]), D * 0.5 * (1 - nu) * kap[2]};
-        const double vm = von_mises(m);
-        meq = (meq < vm) ? vm : meq;
-    }
-    if (meq > Mp) {
-        const double r = 1.0 - Mp / meq;
-        for (int i = 0; i < 3; i++) {
-            th0[i].x += (float)(r * d[6 * i + 3]), th0[i].y += (float)(r * d[6 * i + 4]);
-            d[6 * i + 3] *= 1 - r, d[6 * i + 4] *= 1 - r;
-        }
-        dmg = smax(dmg, 1e-5f);
-    }
-    for (int i = 0; i < 3; i++)
-        if (dot(th0[i], th0[i]) > 0.02f * 0.02f) {
-            const float4 rf = F.tr0[3 * ti + i];
-            const q4 r0 = qnormalize(qmul(q4{rf.x, rf.y, rf.z, rf.w}, quat_exp(V(-th0[i].x, -th0[i].y, -th0[i].z))));
-            F.tr0[3 * ti + i] = make_float4(r0.x, r0.y, r0.z, r0.w);
-            th0[i] = V(0, 0, 0);
-            frames_moved = true;
-        }
+    const bool rest_moved = membrane_return(F, ti, s, X, d, b3, c3, A2, sig, dmg, membrane);
+    bending_return(F, ti, s, th0, d, dmg);
+    bake_rotations(F, ti, th0);
     if (rest_moved)
         for (int i = 0; i < 3; i++) F.tX[6 * ti + 2 * i] = X[i][0], F.tX[6 * ti + 2 * i + 1] = X[i][1];
-    (void)frames_moved;
     for (int i = 0; i < 3; i++) F.th0[9 * ti + 3 * i] = th0[i].x, F.th0[9 * ti + 3 * i + 1] = th0[i].y, F.th0[9 * ti + 3 * i + 2] = th0[i].z;
     F.tdmg[ti] = dmg;
 }
@@ -269,40 +293,47 @@ __global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __rest
     for (int i = 0; i < 3; i++) X[i][0] = F.tX[6 * ti + 2 * i], X[i][1] = F.tX[6 * ti + 2 * i + 1];
     v3 th0[3];
     for (int i = 0; i < 3; i++) th0[i] = kPlastic ? V(F.th0[9 * ti + 3 * i], F.th0[9 * ti + 3 * i + 1], F.th0[9 * ti + 3 * i + 2]) : V(0, 0, 0);
-    // ---- tri_kinematics (frame_fem.cpp:1584-1621)
+    // ---- the co-rotated frame (tri_kinematics, frame_fem.cpp:1584-1621, defines the same one): the plane's normal n
+    // from the corners, a first in-plane axis t1 along the edge 0 -> 1, then the in-plane rotation that best aligns the
+    // rest shape with the current corners about their centroid. That rotation is the least-squares one: its cosine and
+    // sine are the normalised sums of the dot and cross products of rest and current corner vectors, so no angle is
+    // formed. The local displacements are the corners' coordinates on the aligned axes less the rest shape; the
+    // corners' rotations are their frames' rotations relative to the element's, as rotation vectors.
     double x[3][3];
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) x[i][j] = F.xd[3 * (size_t)fnv[i] + j];
-    const double a[3] = {x[1][0] - x[0][0], x[1][1] - x[0][1], x[1][2] - x[0][2]}, c[3] = {x[2][0] - x[0][0], x[2][1] - x[0][1], x[2][2] - x[0][2]};
-    double n[3] = {a[1] * c[2] - a[2] * c[1], a[2] * c[0] - a[0] * c[2], a[0] * c[1] - a[1] * c[0]};
-    const double nl = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]), al = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
-    if (!(nl > 1e-12) || !(al > 1e-9) || !isfinite(nl)) return;
-    for (int j = 0; j < 3; j++) n[j] /= nl;
-    const double t1[3] = {a[0] / al, a[1] / al, a[2] / al};
-    const double t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
-    double cen[3];
-    for (int j = 0; j < 3; j++) cen[j] = (x[0][j] + x[1][j] + x[2][j]) / 3.0;
-    double p[3][2];
-    for (int i = 0; i < 3; i++) {
-        const double r[3] = {x[i][0] - cen[0], x[i][1] - cen[1], x[i][2] - cen[2]};
-        p[i][0] = r[0] * t1[0] + r[1] * t1[1] + r[2] * t1[2];
-        p[i][1] = r[0] * t2[0] + r[1] * t2[1] + r[2] * t2[2];
+    double r[3][3], u01[3], u02[3], n[3];
+    for (int j = 0; j < 3; j++) {
+        const double cj = (x[0][j] + x[1][j] + x[2][j]) / 3.0;
+        for (int i = 0; i < 3; i++) r[i][j] = x[i][j] - cj;
+        u01[j] = x[1][j] - x[0][j], u02[j] = x[2][j] - x[0][j];
     }
-    double sn = 0, cs = 0;
-    for (int i = 0; i < 3; i++) sn += X[i][0] * p[i][1] - X[i][1] * p[i][0], cs += X[i][0] * p[i][0] + X[i][1] * p[i][1];
-    const double phi = atan2(sn, cs), cp = cos(phi), sp = sin(phi);
+    n[0] = u01[1] * u02[2] - u01[2] * u02[1], n[1] = u01[2] * u02[0] - u01[0] * u02[2], n[2] = u01[0] * u02[1] - u01[1] * u02[0];
+    const double nl = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]), al = sqrt(u01[0] * u01[0] + u01[1] * u01[1] + u01[2] * u01[2]);
+    if (!(nl > 1e-12) || !(al > 1e-9) || !isfinite(nl)) return;
+    double t1[3], t2[3];
+    for (int j = 0; j < 3; j++) n[j] /= nl, t1[j] = u01[j] / al;
+    t2[0] = n[1] * t1[2] - n[2] * t1[1], t2[1] = n[2] * t1[0] - n[0] * t1[2], t2[2] = n[0] * t1[1] - n[1] * t1[0];
+    double dotsum = 0, crosssum = 0;
+    for (int i = 0; i < 3; i++) {
+        const double px = r[i][0] * t1[0] + r[i][1] * t1[1] + r[i][2] * t1[2], py = r[i][0] * t2[0] + r[i][1] * t2[1] + r[i][2] * t2[2];
+        dotsum += X[i][0] * px + X[i][1] * py, crosssum += X[i][0] * py - X[i][1] * px;
+    }
+    const double rot = sqrt(dotsum * dotsum + crosssum * crosssum);
+    const double cp = rot > 0 ? dotsum / rot : 1.0, sp = rot > 0 ? crosssum / rot : 0.0;
     double e1d[3], e2d[3];
-    for (int j = 0; j < 3; j++) e1d[j] = cp * t1[j] + sp * t2[j], e2d[j] = -sp * t1[j] + cp * t2[j];
+    for (int j = 0; j < 3; j++) e1d[j] = cp * t1[j] + sp * t2[j], e2d[j] = cp * t2[j] - sp * t1[j];
     const v3 e1 = V((float)e1d[0], (float)e1d[1], (float)e1d[2]), e2 = V((float)e2d[0], (float)e2d[1], (float)e2d[2]);
     const v3 e3 = V((float)n[0], (float)n[1], (float)n[2]);
     const q4 Ec = qconj(qfrom_mat3(e1, e2, e3));
     double d[18];
     for (int i = 0; i < 3; i++) {
-        d[6 * i] = cp * p[i][0] + sp * p[i][1] - X[i][0];
-        d[6 * i + 1] = -sp * p[i][0] + cp * p[i][1] - X[i][1];
+        d[6 * i] = r[i][0] * e1d[0] + r[i][1] * e1d[1] + r[i][2] * e1d[2] - X[i][0];
+        d[6 * i + 1] = r[i][0] * e2d[0] + r[i][1] * e2d[1] + r[i][2] * e2d[2] - X[i][1];
         d[6 * i + 2] = 0;
         const float4 qf = F.q[fnv[i]], rf = F.tr0[3 * ti + i];
-        const v3 th = quat_log(qmul(Ec, qnormalize(qmul(q4{qf.x, qf.y, qf.z, qf.w}, q4{rf.x, rf.y, rf.z, rf.w})))) - th0[i];
+        const q4 corner = qnormalize(qmul(q4{qf.x, qf.y, qf.z, qf.w}, q4{rf.x, rf.y, rf.z, rf.w})); // (the corner's frame)
+        const v3 th = quat_log(qmul(Ec, corner)) - th0[i];
         d[6 * i + 3] = th.x, d[6 * i + 4] = th.y, d[6 * i + 5] = th.z;
     }
     // ---- eval_tris (frame_fem.cpp:1661-1831)
@@ -310,15 +341,16 @@ __global__ void __launch_bounds__(128) k_tri_eval(FemDev F, const float4* __rest
     tri_grad(X, b3, c3, A2);
     if (!(A2 > 0)) return;
     const double nu = s.nu, Dm = (double)s.E / (1 - nu * nu);
-    double eps[3], sig[3];
+    double sig[3];
+    // the constant membrane strain (du/dx, dv/dy, du/dy + dv/dx from the area coordinates' gradients) and its
+    // plane-stress stress
     auto membrane = [&]() {
-        eps[0] = eps[1] = eps[2] = 0;
+        double ux = 0, vy = 0, shear = 0;
         for (int i = 0; i < 3; i++) {
-            eps[0] += b3[i] * d[6 * i] / A2;
-            eps[1] += c3[i] * d[6 * i + 1] / A2;
-            eps[2] += (c3[i] * d[6 * i] + b3[i] * d[6 * i + 1]) / A2;
+            const double gx = b3[i] / A2, gy = c3[i] / A2, u = d[6 * i], v = d[6 * i + 1];
+            ux += gx * u, vy += gy * v, shear += gy * u + gx * v;
         }
-        sig[0] = Dm * (eps[0] + nu * eps[1]), sig[1] = Dm * (nu * eps[0] + eps[1]), sig[2] = Dm * 0.5 * (1 - nu) * eps[2];
+        sig[0] = Dm * (ux + nu * vy), sig[1] = Dm * (nu * ux + vy), sig[2] = Dm * 0.5 * (1 - nu) * shear;
     };
     membrane();
     if (kPlastic && s.plastic) tri_plastic_flow(F, ti, s, X, th0, d, b3, c3, A2, sig, membrane);
@@ -441,54 +473,55 @@ __device__ __forceinline__ q4 qslerp(q4 a, q4 b, float t) {
     return qadd(qscale(a, sinf((1 - t) * th) / s), qscale(b, sinf(t * th) / s));
 }
 
-// what a joint frees (twist, about y, about z) and its flexibility (end_flex, frame_fem.cpp:1420-1431)
-struct EndFlexD {
-    bool rel[3];
-    float f;
+// A member end's joint (FemFrame's joint kinds, frame_fem.cpp:1420-1431): what it frees - the twist, the rotation about
+// the member's y, about its z - and, for an elastic joint, its compliance (rad per N m).
+struct JointEnd {
+    bool free_twist, free_y, free_z;
+    double flex;
 };
-__device__ __forceinline__ EndFlexD end_flex_dev(int j, float joint_k) {
-    EndFlexD e{{false, false, false}, 0.0f};
-    if (j == FJ_BALL) e.rel[0] = e.rel[1] = e.rel[2] = true;
-    else if (j == FJ_HINGE_V) e.rel[2] = true;
-    else if (j == FJ_HINGE_H) e.rel[1] = true;
-    else if (j == FJ_SWIVEL) e.rel[0] = true;
-    else if (j == FJ_ELASTIC) e.f = joint_k > 0 ? 1.0f / joint_k : 0.0f;
-    return e;
-}
-// condense / ends2 (frame_fem.cpp:1414-1418, 1435-1454)
-__device__ __forceinline__ void condense_dev(float c[3], bool pin_a, bool pin_b) {
-    if (pin_a && pin_b) c[0] = c[1] = c[2] = 0;
-    else if (pin_a) c[2] = c[0] > 0 ? c[2] - c[1] * c[1] / c[0] : 0, c[0] = c[1] = 0;
-    else if (pin_b) c[0] = c[2] > 0 ? c[0] - c[1] * c[1] / c[2] : 0, c[1] = c[2] = 0;
-}
-__device__ __forceinline__ void ends2_dev(float c[3], bool ra, bool rb, float fa, float fb) {
-    if (ra || rb) {
-        condense_dev(c, ra, rb);
-        if (ra != rb) {
-            float& k = ra ? c[2] : c[0];
-            const float f = ra ? fb : fa;
-            if (f > 0 && k > 0) k = 1.0f / (1.0f / k + f);
-        }
-        return;
-    }
-    if (fa <= 0 && fb <= 0) return;
-    const double det = (double)c[0] * c[2] - (double)c[1] * c[1];
-    if (!(det > 0)) return;
-    const double F00 = c[2] / det + fa, F01 = -c[1] / det, F11 = c[0] / det + fb;
-    const double d2 = F00 * F11 - F01 * F01;
-    c[0] = (float)(F11 / d2), c[1] = (float)(-F01 / d2), c[2] = (float)(F00 / d2);
+__device__ __forceinline__ JointEnd joint_end(int kind, float joint_k) {
+    JointEnd j{kind == FJ_BALL || kind == FJ_SWIVEL, kind == FJ_BALL || kind == FJ_HINGE_H, kind == FJ_BALL || kind == FJ_HINGE_V, 0.0};
+    if (kind == FJ_ELASTIC && joint_k > 0) j.flex = 1.0 / (double)joint_k;
+    return j;
 }
 
-// FemFrame::condense (frame_fem.cpp:1414-1418): a flowing hinge's end turns like a pin
+// One bending plane's end stiffness [aa, ab, bb]: (M_a, M_b) = K (theta_a, theta_b). Built from the Timoshenko member's
+// flexibility, F = L / (6 EI) [2 -1; -1 2] + 1 / (G As L) [1 1; 1 1] (the second term its shear, none without a
+// shear area), with each held end's joint compliance added on its diagonal, then inverted. A released end carries no
+// moment: only the other end's entry is left, the inverse of its own diagonal flexibility (its joint's included);
+// with both released the plane carries nothing. (The same stiffness as stiffness / ends2, frame_fem.cpp:1414-1476.)
+__device__ __forceinline__ void end_pair(float out[3], float E, float I, float G, float As, float L, bool free_a, bool free_b, double flex_a,
+                                         double flex_b) {
+    out[0] = out[1] = out[2] = 0.0f;
+    const double EI = (double)E * I;
+    if (!(EI > 0) || (free_a && free_b)) return;
+    const double bend = L / (6.0 * EI), shear = As > 0 ? 1.0 / ((double)G * As * L) : 0.0;
+    const double faa = 2 * bend + shear + flex_a, fbb = 2 * bend + shear + flex_b, fab = -bend + shear;
+    if (free_a) {
+        out[2] = (float)(1.0 / fbb);
+    } else if (free_b) {
+        out[0] = (float)(1.0 / faa);
+    } else {
+        const double det = faa * fbb - fab * fab;
+        if (!(det > 0)) return;
+        out[0] = (float)(fbb / det), out[1] = (float)(-fab / det), out[2] = (float)(faa / det);
+    }
+}
+
+// FemFrame::condense (frame_fem.cpp:1414-1418), for the tangent of a flowing hinge: the end turns freely, so the
+// plane's pair keeps only the other end's condensed stiffness (its Schur complement)
 __device__ __forceinline__ void condense(float c[3], bool pin_a, bool pin_b) {
     if (pin_a && pin_b) c[0] = c[1] = c[2] = 0;
     else if (pin_a) c[2] = c[0] > 0 ? c[2] - c[1] * c[1] / c[0] : 0, c[0] = c[1] = 0;
     else if (pin_b) c[0] = c[2] > 0 ? c[0] - c[1] * c[1] / c[2] : 0, c[1] = c[2] = 0;
 }
 
-// member_world_k (frame_fem.cpp:1834-1850) of the effective tangent (FemFrame::effective, frame_fem.cpp:2147-2155:
-// the flowing parts its yield bits less its unload bits name - hinges condensed, axial and twist at 1 %): the world
-// blocks of element_matrix (frame_fem.cpp:2157-2186) and K v at the ends' velocities
+// The member's tangent in world axes (member_world_k / element_matrix, frame_fem.cpp:1834-1850, 2157-2186, of the
+// effective tangent FemFrame::effective gives, frame_fem.cpp:2147-2155: the flowing parts its yield bits less its
+// unload bits name - hinges condensed, axial and twist at 1 %), as K = B^T D B: B maps the 12 end dofs
+// [u_a, phi_a, u_b, phi_b] to the six deformations - elongation e1.(u_b - u_a), twist e1.(phi_b - phi_a), each end's
+// rotation about e2 against the chord e2.phi + e3.(u_b - u_a) / L and about e3 e3.phi - e2.(u_b - u_a) / L - and D is
+// ka, kt and the two planes' end pairs. Stored as its four 6 x 6 world blocks with K v at the ends' velocities.
 __device__ void member_world_k(const FemDev& F, const float4* __restrict__ nd, int ei, int2 ab, v3 e1, v3 e2, v3 e3, float L, float ka, float kt,
                                const float cy_in[3], const float cz_in[3], uint32_t y) {
     float cy[3] = {cy_in[0], cy_in[1], cy_in[2]}, cz[3] = {cz_in[0], cz_in[1], cz_in[2]};
@@ -496,30 +529,32 @@ __device__ void member_world_k(const FemDev& F, const float4* __restrict__ nd, i
     if (y & 4) ka *= 0.01f;
     if (y & 8) kt *= 0.01f;
     const double iL = 1.0 / L;
-    const double E1[3] = {e1.x, e1.y, e1.z}, E2[3] = {e2.x, e2.y, e2.z}, E3[3] = {e3.x, e3.y, e3.z};
-    const double g[3] = {E3[0] * iL, E3[1] * iL, E3[2] * iL}, h[3] = {E2[0] * iL, E2[1] * iL, E2[2] * iL};
-    const double cy0 = cy[0], cy1 = cy[1], cy2 = cy[2], cz0 = cz[0], cz1 = cz[1], cz2 = cz[2];
-    const double Sy2 = cy0 + 2 * cy1 + cy2, Sz2 = cz0 + 2 * cz1 + cz2, ay = cy0 + cy1, by = cy1 + cy2, az = cz0 + cz1, bz = cz1 + cz2;
-    const double kad = ka, ktd = kt;
+    const double a1[3] = {e1.x, e1.y, e1.z}, a2[3] = {e2.x, e2.y, e2.z}, a3[3] = {e3.x, e3.y, e3.z};
+    double B[6][12];
+    for (int r = 0; r < 6; r++)
+        for (int q = 0; q < 12; q++) B[r][q] = 0;
+    for (int j = 0; j < 3; j++) {
+        const double g = a3[j] * iL, h = a2[j] * iL;
+        B[0][j] = -a1[j], B[0][6 + j] = a1[j];
+        B[1][3 + j] = -a1[j], B[1][9 + j] = a1[j];
+        B[2][j] = -g, B[2][6 + j] = g, B[2][3 + j] = a2[j];
+        B[3][j] = -g, B[3][6 + j] = g, B[3][9 + j] = a2[j];
+        B[4][j] = h, B[4][6 + j] = -h, B[4][3 + j] = a3[j];
+        B[5][j] = h, B[5][6 + j] = -h, B[5][9 + j] = a3[j];
+    }
+    double DB[6][12];
+    for (int q = 0; q < 12; q++) {
+        DB[0][q] = (double)ka * B[0][q], DB[1][q] = (double)kt * B[1][q];
+        DB[2][q] = (double)cy[0] * B[2][q] + (double)cy[1] * B[3][q], DB[3][q] = (double)cy[1] * B[2][q] + (double)cy[2] * B[3][q];
+        DB[4][q] = (double)cz[0] * B[4][q] + (double)cz[1] * B[5][q], DB[5][q] = (double)cz[1] * B[4][q] + (double)cz[2] * B[5][q];
+    }
     double K[12][12];
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) {
-            const double uu = kad * E1[i] * E1[j] + Sy2 * g[i] * g[j] + Sz2 * h[i] * h[j];
-            const double up = -ay * g[i] * E2[j] + az * h[i] * E3[j];
-            const double ub = -by * g[i] * E2[j] + bz * h[i] * E3[j];
-            const double tt = ktd * E1[i] * E1[j];
-            const double pa = tt + cy0 * E2[i] * E2[j] + cz0 * E3[i] * E3[j];
-            const double pb = -tt + cy1 * E2[i] * E2[j] + cz1 * E3[i] * E3[j];
-            const double qb = tt + cy2 * E2[i] * E2[j] + cz2 * E3[i] * E3[j];
-            K[i][j] = uu, K[i][3 + j] = up, K[i][6 + j] = -uu, K[i][9 + j] = ub;
-            K[3 + i][3 + j] = pa, K[3 + i][9 + j] = pb;
-            K[6 + i][6 + j] = uu, K[6 + i][9 + j] = -ub;
-            K[9 + i][9 + j] = qb;
-        }
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) K[3 + i][6 + j] = -K[j][3 + i];
     for (int r = 0; r < 12; r++)
-        for (int c2 = r + 1; c2 < 12; c2++) K[c2][r] = K[r][c2];
+        for (int q = r; q < 12; q++) {
+            double v = 0;
+            for (int k = 0; k < 6; k++) v += B[k][r] * DB[k][q];
+            K[r][q] = K[q][r] = v;
+        }
     double* W = F.mkw + 144 * (size_t)ei;
     for (int r = 0; r < 6; r++)
         for (int q = 0; q < 6; q++)
@@ -564,27 +599,14 @@ __global__ void __launch_bounds__(128) k_member_eval(FemDev F, const float4* __r
     const q4 Ec = qconj(E);
     const v3 ra = quat_log(qmul(Ec, Ea)), rb = quat_log(qmul(Ec, Eb));
     const v3 e2 = qrotate(E, V(0, 1, 0)), e3 = qrotate(E, V(0, 0, 1));
-    // ---- the section's stiffness with the joints
-    const EndFlexD fa = end_flex_dev(endA, s.joint_k), fb = end_flex_dev(endB, s.joint_k);
+    // ---- the section's stiffness with the joints: axial, twist (a freed twist carries none; elastic joints add their
+    // compliances in series) and the two bending planes' end pairs
+    const JointEnd ja = joint_end(endA, s.joint_k), jb = joint_end(endB, s.joint_k);
     const float ka = s.axial * s.E * s.A / L0;
-    float kt = s.G * s.J / L0;
-    if (fa.rel[0] || fb.rel[0]) kt = 0;
-    else if (fa.f + fb.f > 0) kt = 1.0f / (1.0f / kt + fa.f + fb.f);
+    const float kt = (ja.free_twist || jb.free_twist) ? 0.0f : (float)(1.0 / ((double)L0 / ((double)s.G * s.J) + ja.flex + jb.flex));
     float cy[3], cz[3];
-    {
-        const float phi = s.As_z > 0 ? 12.0f * s.E * s.Iy / (s.G * s.As_z * L0 * L0) : 0.0f;
-        const float k0 = s.E * s.Iy / (L0 * (1.0f + phi));
-        cy[0] = cy[2] = (4.0f + phi) * k0;
-        cy[1] = (2.0f - phi) * k0;
-        ends2_dev(cy, fa.rel[1], fb.rel[1], fa.f, fb.f);
-    }
-    {
-        const float phi = s.As_y > 0 ? 12.0f * s.E * s.Iz / (s.G * s.As_y * L0 * L0) : 0.0f;
-        const float k0 = s.E * s.Iz / (L0 * (1.0f + phi));
-        cz[0] = cz[2] = (4.0f + phi) * k0;
-        cz[1] = (2.0f - phi) * k0;
-        ends2_dev(cz, fa.rel[2], fb.rel[2], fa.f, fb.f);
-    }
+    end_pair(cy, s.E, s.Iy, s.G, s.As_z, L0, ja.free_y, jb.free_y, ja.flex, jb.flex);
+    end_pair(cz, s.E, s.Iz, s.G, s.As_y, L0, ja.free_z, jb.free_z, ja.flex, jb.flex);
     // ---- the section's forces: axial yield at Np (compression at the lower of Np and the Euler load of 0.7 L), the
     // twist's at Tp, radial-return hinges at the ends against the hardened plastic moment, twice (eval_forces,
     // frame_fem.cpp:1915-1982); an elastic section's plastic parts stay 0
@@ -937,21 +959,19 @@ __global__ void __launch_bounds__(128) k_fem_assemble_all(FemDev F, const float4
 }
 
 // ------------------------------------------------------------------------------------------ factorization
-// chol6 (frame_fem.cpp:2193-2209) by one thread
+// The Cholesky factor of one 6 x 6 block (what chol6, frame_fem.cpp:2193-2209, computes), by one thread, right-looking:
+// each pivot's square root, its column scaled by the pivot's inverse, then the trailing lower triangle less that
+// column's outer product. A (row-major) gets L in its lower triangle and zeros above; dinv the pivots' inverses. False
+// at a pivot that is not positive (the block is not positive definite).
 __device__ bool chol6_dev(double* A, double* dinv) {
-    for (int j = 0; j < 6; j++) {
-        double s = A[j * 6 + j];
-        for (int k = 0; k < j; k++) s -= A[j * 6 + k] * A[j * 6 + k];
-        if (!(s > 0)) return false;
-        const double d = sqrt(s), id = 1.0 / d;
-        A[j * 6 + j] = d;
-        dinv[j] = id;
-        for (int i = j + 1; i < 6; i++) {
-            double t = A[i * 6 + j];
-            for (int k = 0; k < j; k++) t -= A[i * 6 + k] * A[j * 6 + k];
-            A[i * 6 + j] = t * id;
-        }
-        for (int i = 0; i < j; i++) A[i * 6 + j] = 0;
+    for (int k = 0; k < 6; k++) {
+        const double piv = A[7 * k];
+        if (!(piv > 0)) return false;
+        const double d = sqrt(piv), id = 1.0 / d;
+        A[7 * k] = d, dinv[k] = id;
+        for (int i = k + 1; i < 6; i++) A[6 * i + k] *= id, A[6 * k + i] = 0;
+        for (int j = k + 1; j < 6; j++)
+            for (int i = j; i < 6; i++) A[6 * i + j] -= A[6 * i + k] * A[6 * j + k];
     }
     return true;
 }
