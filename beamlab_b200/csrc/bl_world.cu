@@ -17,6 +17,8 @@
 #include "bl_fem_host.cuh"
 #include "bl_fem_kernels.cuh"
 #include "bl_fem_pcg.cuh"
+#include "bl_mf_plan.cuh"
+#include "bl_multifrontal.cuh"
 #include "bl_mlp.cuh"
 #include "bl_kernels.cuh"
 
@@ -202,6 +204,19 @@ struct bl_gpu_ctx {
     DevBuf<int> fcol, fchain;
     DevBuf<int4> fblk;
     DevBuf<double> fD, fb;
+    // the multifrontal factorization (bl_multifrontal.cuh), fem_dense_front == 2: fronts, their maps, the pool, and per
+    // level its task ranges (assembly; per panel, panel and update tasks)
+    MfDev mf{};
+    DevBuf<MfFrontDev> mf_fr;
+    DevBuf<int> mf_idx, mf_cmap, mf_child;
+    DevBuf<double> mf_pool, mf_u, mf_dt;
+    DevBuf<int2> mf_tcol, mf_tpan;
+    DevBuf<int4> mf_tupd;
+    std::vector<int> mf_level_ptr;             // fronts of each level (execution order)
+    std::vector<int> mf_tcol_ptr;              // per level: its assembly tasks
+    std::vector<std::vector<int>> mf_tpan_ptr, mf_tupd_ptr; // per level, per panel: its tasks
+    size_t mf_smem = 0;                        // the solves' dynamic shared memory (the largest front)
+    double mf_flops = 0;
     DevBuf<float> finertia, tX, tk, ttan, tb, tX0, th0, tdmg;
     DevBuf<uint8_t> tbroken, ton, ffixed;
     DevBuf<FemSecDev> fsec;
@@ -261,6 +276,8 @@ static void free_fem(bl_gpu_ctx* c) {
     c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
     c->fcol.free_(), c->fchain.free_(), c->fblk.free_(), c->fD.free_(), c->fb.free_(), c->front = FrontDev{}, c->front_level = 0;
+    c->mf_fr.free_(), c->mf_idx.free_(), c->mf_cmap.free_(), c->mf_child.free_(), c->mf_pool.free_(), c->mf_u.free_(), c->mf_dt.free_();
+    c->mf_tcol.free_(), c->mf_tpan.free_(), c->mf_tupd.free_(), c->mf = MfDev{}, c->mf_level_ptr.clear(), c->mf_flops = 0;
     c->mn.free_(), c->mmeta.free_(), c->mL0.free_(), c->mq.free_(), c->mfa.free_(), c->mta.free_(), c->mtb.free_(), c->mtan.free_();
     c->msec.free_(), c->mon.free_(), c->mkw.free_(), c->mkv.free_(), c->NM = 0;
     c->mps.free_(), c->mtg.free_(), c->mflag.free_(), c->credit.free_(), c->elastic.free_(), c->comp_again.free_(), c->comp_size.free_();
@@ -511,6 +528,75 @@ static int pull_state(bl_gpu_ctx* c) {
 // elimination-tree level (a column's level is one more than its deepest child's), each level's target blocks (a
 // column's diagonal block then its off-diagonal ones) with each target's updates in the order of their source columns,
 // each row's blocks in the order of their columns for the forward substitution.
+// The multifrontal plan over every frame's columns (global pattern col_ptr / row, components col_comp): the fronts,
+// their maps and the pool on the device, and each level's task lists (bl_multifrontal.cuh)
+static int commit_multifrontal(bl_gpu_ctx* c, const std::vector<int>& col_ptr, const std::vector<int>& row, const std::vector<int>& col_comp) {
+    const int NF = (int)col_ptr.size() - 1;
+    std::vector<std::vector<int>> fr_cols;
+    std::vector<int> fr_top, fr_comp;
+    mf_plan_columns(NF, col_ptr, row, col_comp, fr_cols, fr_top, fr_comp);
+    const MfPlan P = mf_finish(NF, col_ptr, row, fr_cols, fr_top, fr_comp);
+    const int nfr = (int)P.npiv.size(), nlev = (int)P.level_ptr.size() - 1;
+    std::vector<MfFrontDev> fr(nfr);
+    long long pool = 0;
+    int u = 0, dtn = 0, maxn = 0;
+    for (int f = 0; f < nfr; f++) {
+        MfFrontDev& d = fr[f];
+        d.n = 6 * (P.npiv[f] + P.nrow[f]), d.p = 6 * P.npiv[f];
+        d.off = pool, d.idx0 = P.idx_ptr[f], d.child0 = P.child_ptr[f], d.child1 = P.child_ptr[f + 1], d.comp = P.comp[f];
+        d.u0 = u, d.dt0 = dtn;
+        pool += (long long)d.n * d.n;
+        u += d.n - d.p;
+        dtn += kMfT * kMfT * ((d.p + kMfT - 1) / kMfT);
+        maxn = std::max(maxn, d.n);
+    }
+    std::vector<int2> tcol, tpan;
+    std::vector<int4> tupd;
+    c->mf_tcol_ptr.assign(1, 0), c->mf_tpan_ptr.assign(nlev, {}), c->mf_tupd_ptr.assign(nlev, {});
+    int64_t launches = 0;
+    for (int L = 0; L < nlev; L++) {
+        int np = 0;
+        for (int f = P.level_ptr[L]; f < P.level_ptr[L + 1]; f++) {
+            const int nt = (fr[f].n + kMfT - 1) / kMfT;
+            for (int jt = 0; jt < nt; jt++) tcol.push_back(make_int2(f, jt));
+            np = std::max(np, (fr[f].p + kMfT - 1) / kMfT);
+        }
+        c->mf_tcol_ptr.push_back((int)tcol.size());
+        c->mf_tpan_ptr[L].push_back((int)tpan.size()), c->mf_tupd_ptr[L].push_back((int)tupd.size());
+        for (int sp = 0; sp < np; sp++) {
+            for (int f = P.level_ptr[L]; f < P.level_ptr[L + 1]; f++) {
+                if (fr[f].p <= kMfT * sp) continue;
+                const int nt = (fr[f].n + kMfT - 1) / kMfT;
+                for (int r = sp; r < nt; r++) tpan.push_back(make_int2(f, r));
+                tupd.push_back(make_int4(f, -1, -1, 0));
+                for (int j = sp + 1; j < nt; j++)
+                    for (int i = j; i < nt; i++) tupd.push_back(make_int4(f, i, j, 0));
+            }
+            c->mf_tpan_ptr[L].push_back((int)tpan.size()), c->mf_tupd_ptr[L].push_back((int)tupd.size());
+        }
+        launches += 1 + 2 * np + 2;
+    }
+    int rc;
+    if ((rc = upload_vec(c, c->mf_fr, fr)) || (rc = upload_vec(c, c->mf_idx, P.idx)) || (rc = upload_vec(c, c->mf_cmap, P.cmap)) ||
+        (rc = upload_vec(c, c->mf_child, P.child.empty() ? std::vector<int>(1, 0) : P.child)) || (rc = upload_vec(c, c->mf_tcol, tcol)) ||
+        (rc = upload_vec(c, c->mf_tpan, tpan.empty() ? std::vector<int2>(1) : tpan)) || (rc = upload_vec(c, c->mf_tupd, tupd.empty() ? std::vector<int4>(1) : tupd)))
+        return rc;
+    BL_CUDA(c, c->mf_pool.alloc((size_t)std::max(pool, 1LL)));
+    BL_CUDA(c, c->mf_u.alloc((size_t)std::max(u, 1)));
+    BL_CUDA(c, c->mf_dt.alloc((size_t)std::max(dtn, 1)));
+    c->mf_smem = sizeof(double) * (size_t)maxn;
+    if (c->mf_smem > 227 * 1024 - 2 * sizeof(double) * kMfT * (kMfT + 1)) return BL_GPU_ELIMIT; // (a front of more than ~3,500 nodes)
+    if (c->mf_smem > 40 * 1024) {
+        BL_CUDA(c, cudaFuncSetAttribute(k_mf_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->mf_smem));
+        BL_CUDA(c, cudaFuncSetAttribute(k_mf_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->mf_smem));
+    }
+    c->mf = MfDev{c->mf_fr.p, c->mf_idx.p, c->mf_cmap.p, c->mf_child.p, c->mf_pool.p, c->mf_u.p, c->mf_dt.p, c->mf_tcol.p, c->mf_tpan.p, c->mf_tupd.p};
+    c->mf_level_ptr = P.level_ptr;
+    c->mf_flops = P.flops;
+    c->chol_launches = launches;
+    return BL_GPU_OK;
+}
+
 static int commit_fem(bl_gpu_ctx* c) {
     int NF = 0, NT = 0, NB = 0, NC = 0, NS = 0, nfem_nodes = 0;
     for (const HostBody& hb : c->bodies)
@@ -643,7 +729,8 @@ static int commit_fem(bl_gpu_ctx* c) {
     std::vector<int> rb_ptr(NF + 1, 0);
     std::vector<std::vector<int>> bylev(nlev);
     for (int k = 0; k < NF; k++) bylev[level[k]].push_back(k);
-    c->NU = (int64_t)gupd.size();
+    c->NU = 0; // (the pattern's block updates, whether or not their list was built: sum over columns of d (d + 1) / 2)
+    for (int k = 0; k < NF; k++) c->NU += (int64_t)(col_ptr[k + 1] - col_ptr[k]) * (col_ptr[k + 1] - col_ptr[k] + 1) / 2;
     std::vector<std::vector<int>> col_upds(NF);
     for (size_t u = 0; u < gupd.size(); u++) col_upds[upd_col[u]].push_back((int)u);
     c->lvl_grp_ptr.assign(1, 0), c->lvl_col_ptr.assign(1, 0);
@@ -774,7 +861,7 @@ static int commit_fem(bl_gpu_ctx* c) {
         const int nlev = (int)c->lvl_col_ptr.size() - 1;
         int top = nlev;
         while (top > 0 && c->lvl_col_ptr[top] - c->lvl_col_ptr[top - 1] == 1) top--;
-        const int m = c->cfg.fem_dense_front ? nlev - top : 0;
+        const int m = c->cfg.fem_dense_front == 1 ? nlev - top : 0;
         std::vector<int> chain(NF, -1), fcol;
         std::vector<int4> fblk;
         bool closed = m >= kFrontMin && 6 * m <= 8192; // (D at most 512 MB, its solve's vector in shared memory)
@@ -801,6 +888,7 @@ static int commit_fem(bl_gpu_ctx* c) {
         }
         c->chol_launches = 3 * (int64_t)c->front_level;
         if (c->front_level < nlev) c->chol_launches += 1 + c->front.nt + 2 * (c->front.nt - 1) + 2;
+        if (c->cfg.fem_dense_front == 2 && (rc = commit_multifrontal(c, col_ptr, row, col_comp))) return rc;
         c->fem_launches = 4 + (c->NT > 0 ? 1 : 0) + (c->NM > 0 ? 1 : 0) + c->chol_launches; // (begin, triangles, members, assembly, velocity, integration)
     }
     // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
@@ -1408,6 +1496,26 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             if (rec) k_mlp_record_pre<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
             if (learned) k_mlp_infer<<<(c->NF + kLanes - 1) / kLanes, kLanes, 0, s>>>(F, MD, c->guess.p, c->gscale.p);
             auto cholesky = [c, &F](cudaStream_t cs) {
+                if (c->cfg.fem_dense_front == 2) {
+                    // multifrontal: per level of the front tree its fronts assembled, then panel by panel factored and
+                    // updated; the forward substitution level by level, the backward from the root down
+                    const MfDev& M = c->mf;
+                    const int nlev = (int)c->mf_level_ptr.size() - 1;
+                    for (int L = 0; L < nlev; L++) {
+                        k_mf_assemble<<<c->mf_tcol_ptr[L + 1] - c->mf_tcol_ptr[L], 256, 0, cs>>>(F, M, c->mf_tcol_ptr[L]);
+                        const std::vector<int>& tp = c->mf_tpan_ptr[L];
+                        const std::vector<int>& tu = c->mf_tupd_ptr[L];
+                        for (size_t sp = 0; sp + 1 < tp.size(); sp++) {
+                            k_mf_panel<<<tp[sp + 1] - tp[sp], 32, 0, cs>>>(M, tp[sp], (int)sp, F.comp_fail);
+                            k_mf_update<<<tu[sp + 1] - tu[sp], 256, 0, cs>>>(M, tu[sp], (int)sp);
+                        }
+                    }
+                    for (int L = 0; L < nlev; L++)
+                        k_mf_forward<<<c->mf_level_ptr[L + 1] - c->mf_level_ptr[L], 256, c->mf_smem, cs>>>(F, M, c->mf_level_ptr[L]);
+                    for (int L = nlev - 1; L >= 0; L--)
+                        k_mf_backward<<<c->mf_level_ptr[L + 1] - c->mf_level_ptr[L], 256, c->mf_smem, cs>>>(F, M, c->mf_level_ptr[L]);
+                    return;
+                }
                 // the levels of the elimination tree two launches each (factor; updates with the forward substitution),
                 // then the backward substitution a launch a level from the top down
                 const int nlev = (int)c->lvl_col_ptr.size() - 1, top = c->front_level;
@@ -1499,7 +1607,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
 // A body's FEM frame of triangle elements made ready (bl_fem_host.cuh): frame nodes in the order FemFrame::add_tri
 // makes them, FemFrame::finalize's rest shapes and inertias, analyse's pattern, the elements' stiffnesses.
 static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32_t n_nodes, const bl_fem_desc& fd, std::vector<FemSection>& sections,
-                           std::vector<FrameSectionH>& fsections, std::shared_ptr<FemModel>& out) {
+                           std::vector<FrameSectionH>& fsections, std::shared_ptr<FemModel>& out, bool want_updates = true) {
     if (fd.n_tris < 0 || fd.n_members < 0 || (fd.n_tris > 0 && (!fd.tris || !fd.sections || fd.n_sections <= 0)) ||
         (fd.n_members > 0 && (!fd.members || !fd.frame_sections || fd.n_frame_sections <= 0)) || fd.n_tris + fd.n_members == 0 || !nodes || !info)
         return BL_GPU_EINVAL;
@@ -1561,7 +1669,7 @@ static int build_fem_model(const bl_node* nodes, const bl_node_info* info, int32
     for (size_t t = 0; t < M->tn.size(); t++) // (the caller's mass, else its section's over its area: tri_mass, frame_fem.h:373)
         if (!(M->tmass[t] > 0)) M->tmass[t] = sections[M->tsec[t]].rho * sections[M->tsec[t]].t * M->tarea0[t], again = true;
     if (again) fem_finalize(*M, px.data(), py.data(), pz.data(), ms.data(), mpm); // (the inertias from those masses)
-    fem_analyse(*M);
+    fem_analyse(*M, want_updates);
     M->tk.assign(162 * M->tn.size(), 0.0f), M->tb.assign(54 * M->tn.size(), 0.0f);
     for (size_t t = 0; t < M->tn.size(); t++) {
         if (M->tbroken[t]) continue;
@@ -1597,7 +1705,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->pcg_learned_scale = 0;
     cfg->graphs = 1;
     cfg->beam_kernel = 0;
-    cfg->fem_dense_front = 1;
+    cfg->fem_dense_front = 2;
     cfg->force_block = 0;
     cfg->integrate_block = 0;
     cfg->beams_per_sm = 0;
@@ -1627,7 +1735,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
     if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 3 || c0.pcg_max_iters < 0 ||
-        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 1 ||
+        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 2 ||
         !(c0.force_block == 0 || c0.force_block == 64 || c0.force_block == 128 || c0.force_block == 256) ||
         !(c0.integrate_block == 0 || c0.integrate_block == 64 || c0.integrate_block == 128 || c0.integrate_block == 256) ||
         c0.beams_per_sm < 0 || c0.beams_per_sm > 16 || !(c0.tyre_grip >= 0))
@@ -1852,7 +1960,7 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
     hb.beam_bits = (d->allow_deform ? BB_DEFORM : 0u) | (d->allow_break ? BB_BREAK : 0u) | (d->ductile ? BB_DUCTILE : 0u);
     if (d->fem && (d->fem->n_tris > 0 || d->fem->n_members > 0)) {
         std::shared_ptr<FemModel> M;
-        const int rc = build_fem_model(d->nodes, d->info, d->n_nodes, *d->fem, hb.sections, hb.fsections, M);
+        const int rc = build_fem_model(d->nodes, d->info, d->n_nodes, *d->fem, hb.sections, hb.fsections, M, c->cfg.fem_dense_front != 2);
         if (rc) return rc;
         hb.fq.assign(4 * M->node.size(), 0.0f);
         for (size_t i = 0; i < M->node.size(); i++) hb.fq[4 * i + 3] = 1.0f;
@@ -2204,6 +2312,9 @@ int bl_gpu_fem_stats(bl_gpu_ctx* c, bl_fem_stats* out) {
     out->pcg_solves = st[0], out->pcg_fallbacks = st[1], out->last_iterations = st[2], out->pcg_iterations = it;
     out->last_pcg_residual = last, out->max_residual = res[0], out->last_residual = res[3];
     out->columns = c->NF, out->blocks = c->NB, out->updates = c->NU, out->levels = (int64_t)c->lvl_col_ptr.size() - 1;
+    out->fronts = c->cfg.fem_dense_front == 2 ? (int64_t)c->mf_fr.n : 0;
+    out->factor_flops = c->cfg.fem_dense_front == 2 ? c->mf_flops : 432.0 * (double)c->NU;
+    if (c->cfg.fem_dense_front == 2) out->levels = (int64_t)c->mf_level_ptr.size() - 1;
     if (c->any_plastic_members) {
         long long rp = 0;
         BL_CUDA(c, cudaMemcpy(&rp, c->repc.p, sizeof(rp), cudaMemcpyDeviceToHost));

@@ -72,8 +72,9 @@ class WorldSettings:
     graphs: bool = True
     # the beams' kernel: 0 streams the beam arrays by bulk (TMA) copies, 1 plain loads (the same results)
     beam_kernel: int = 0
-    # the FEM factorization's top chain as one dense front (True) or block column by block column (False)
-    fem_dense_front: bool = True
+    # the FEM factorization: 2 multifrontal (dense fronts, level by level of the front tree), 1 block columns with the
+    # top chain as one dense front, 0 block columns in the reference's order of sums
+    fem_dense_front: int = 2
     tyre_grip: float = 1.0                    # WorldSettings::tyre_grip: a factor on the tyres' friction
     # launch shapes (None: the tuned ones of beamlab_b200/tuned.json when present, else the library's defaults);
     # results do not depend on them
@@ -384,7 +385,8 @@ class _FemStats(C.Structure):
     _fields_ = [("pcg_solves", C.c_int64), ("pcg_fallbacks", C.c_int64), ("pcg_iterations", C.c_int64),
                 ("last_iterations", C.c_int32), ("pad", C.c_int32), ("last_pcg_residual", C.c_double),
                 ("max_residual", C.c_double), ("last_residual", C.c_double), ("columns", C.c_int64),
-                ("blocks", C.c_int64), ("updates", C.c_int64), ("levels", C.c_int64), ("repasses", C.c_int64)]
+                ("blocks", C.c_int64), ("updates", C.c_int64), ("levels", C.c_int64), ("repasses", C.c_int64),
+                ("fronts", C.c_int64), ("factor_flops", C.c_double)]
 
 
 FEM_SOLVERS = {"cholesky": 0, "pcg": 1, "pcg_learned": 2, "pcg_previous": 3}

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define BL_GPU_ABI_VERSION 4
+#define BL_GPU_ABI_VERSION 5
 
 enum {
     BL_GPU_OK = 0,
@@ -85,9 +85,13 @@ typedef struct {
     int32_t beam_kernel;       /* 0 (default): the beams' kernel streams the beam arrays through shared memory by bulk
                                   (TMA) copies and the nodes' kernel reads 4-byte incidences where the rig allows; 1:
                                   plain loads and 8-byte incidences. Results are the same. */
-    int32_t fem_dense_front;   /* 1 (default): the FEM factorization takes the top chain of its elimination tree (levels of
-                                  one column each) as one dense front (a blocked dense Cholesky and dense solves); 0: block
-                                  column by block column in the reference's order of sums throughout */
+    int32_t fem_dense_front;   /* how the FEM step factors its system (the same pattern and fill as the reference's):
+                                  2 (default): multifrontal - the columns grouped into dense fronts (supernodes of the
+                                  elimination tree, small ones amalgamated), each factored by dense tiled kernels, level by
+                                  level of the front tree; 1: block column by block column, with the top chain of the
+                                  elimination tree (levels of one column each) as one dense front; 0: block column by block
+                                  column in the reference's order of sums throughout. 2 and 1 differ from 0 in the order of
+                                  the floating-point sums only. */
     /* launch shapes (results do not depend on them; beamlab_b200/autotune.py measures them for a device and workload): */
     int32_t force_block;       /* the nodes' force kernel's block size: 64, 128 or 256; 0 (default): 256 */
     int32_t integrate_block;   /* the integration kernel's block size: 64, 128 or 256; 0 (default): 256 */
@@ -413,6 +417,9 @@ typedef struct {
     int64_t levels;            /* elimination-tree levels */
     int64_t repasses;          /* unload re-passes: the steps' systems assembled and factored again where the step
                                   unloaded a flowing hinge, bar or twist of a yielding member */
+    int64_t fronts;            /* fem_dense_front == 2: the multifrontal factorization's dense fronts (0 otherwise); */
+    double factor_flops;       /* the flops of one factorization as this path runs it (multiplies and adds counted
+                                  apart; the multifrontal's dense fronts include their explicit zeros) */
 } bl_fem_stats;
 int bl_gpu_fem_stats(bl_gpu_ctx* ctx, bl_fem_stats* out);
 
