@@ -493,6 +493,16 @@ __device__ __forceinline__ JointEnd joint_end(int kind, float joint_k) {
 __device__ __forceinline__ void end_pair(float out[3], float E, float I, float G, float As, float L, bool free_a, bool free_b, double flex_a,
                                          double flex_b) {
     out[0] = out[1] = out[2] = 0.0f;
+    if (!free_a && !free_b && flex_a == 0 && flex_b == 0) {
+        // both ends held rigidly: the inverse in closed form, the Timoshenko element's end-moment stiffness
+        // EI / (L (1 + phi)) [4 + phi, 2 - phi; 2 - phi, 4 + phi] with phi = 12 EI / (G As L^2), in float as the
+        // section's stiffness is stored
+        const float phi = As > 0 ? 12.0f * E * I / (G * As * L * L) : 0.0f;
+        const float k0 = E * I / (L * (1.0f + phi));
+        out[0] = out[2] = (4.0f + phi) * k0;
+        out[1] = (2.0f - phi) * k0;
+        return;
+    }
     const double EI = (double)E * I;
     if (!(EI > 0) || (free_a && free_b)) return;
     const double bend = L / (6.0 * EI), shear = As > 0 ? 1.0 / ((double)G * As * L) : 0.0;
@@ -603,7 +613,9 @@ __global__ void __launch_bounds__(128) k_member_eval(FemDev F, const float4* __r
     // compliances in series) and the two bending planes' end pairs
     const JointEnd ja = joint_end(endA, s.joint_k), jb = joint_end(endB, s.joint_k);
     const float ka = s.axial * s.E * s.A / L0;
-    const float kt = (ja.free_twist || jb.free_twist) ? 0.0f : (float)(1.0 / ((double)L0 / ((double)s.G * s.J) + ja.flex + jb.flex));
+    const float kt = (ja.free_twist || jb.free_twist) ? 0.0f
+                     : (ja.flex + jb.flex > 0) ? (float)(1.0 / ((double)L0 / ((double)s.G * s.J) + ja.flex + jb.flex))
+                                               : s.G * s.J / L0;
     float cy[3], cz[3];
     end_pair(cy, s.E, s.Iy, s.G, s.As_z, L0, ja.free_y, jb.free_y, ja.flex, jb.flex);
     end_pair(cz, s.E, s.Iz, s.G, s.As_y, L0, ja.free_z, jb.free_z, ja.flex, jb.flex);
