@@ -208,12 +208,12 @@ struct bl_gpu_ctx {
     // level its task ranges (assembly; per panel, panel and update tasks)
     MfDev mf{};
     DevBuf<MfFrontDev> mf_fr;
-    DevBuf<int> mf_idx, mf_cmap, mf_child;
-    DevBuf<double> mf_pool, mf_u, mf_dt;
-    DevBuf<int2> mf_tcol, mf_tpan;
-    DevBuf<int4> mf_tupd;
+    DevBuf<int> mf_idx, mf_cmap, mf_child, mf_brow;
+    DevBuf<double> mf_pool, mf_dt;
+    DevBuf<int2> mf_tpan;
+    DevBuf<int4> mf_tasm, mf_tupd;
     std::vector<int> mf_level_ptr;             // fronts of each level (execution order)
-    std::vector<int> mf_tcol_ptr;              // per level: its assembly tasks
+    std::vector<int> mf_tasm_ptr;              // per level: its assembly tasks
     std::vector<std::vector<int>> mf_tpan_ptr, mf_tupd_ptr; // per level, per panel: its tasks
     size_t mf_smem = 0;                        // the solves' dynamic shared memory (the largest front)
     double mf_flops = 0;
@@ -276,8 +276,8 @@ static void free_fem(bl_gpu_ctx* c) {
     c->feat.free_(), c->prev_dv.free_(), c->adj_ptr.free_(), c->adj.free_();
     c->gdiag.free_(), c->gu.free_(), c->rb.free_(), c->goff.free_(), c->tn.free_();
     c->fcol.free_(), c->fchain.free_(), c->fblk.free_(), c->fD.free_(), c->fb.free_(), c->front = FrontDev{}, c->front_level = 0;
-    c->mf_fr.free_(), c->mf_idx.free_(), c->mf_cmap.free_(), c->mf_child.free_(), c->mf_pool.free_(), c->mf_u.free_(), c->mf_dt.free_();
-    c->mf_tcol.free_(), c->mf_tpan.free_(), c->mf_tupd.free_(), c->mf = MfDev{}, c->mf_level_ptr.clear(), c->mf_flops = 0;
+    c->mf_fr.free_(), c->mf_idx.free_(), c->mf_cmap.free_(), c->mf_child.free_(), c->mf_brow.free_(), c->mf_pool.free_(), c->mf_dt.free_();
+    c->mf_tasm.free_(), c->mf_tpan.free_(), c->mf_tupd.free_(), c->mf = MfDev{}, c->mf_level_ptr.clear(), c->mf_flops = 0;
     c->mn.free_(), c->mmeta.free_(), c->mL0.free_(), c->mq.free_(), c->mfa.free_(), c->mta.free_(), c->mtb.free_(), c->mtan.free_();
     c->msec.free_(), c->mon.free_(), c->mkw.free_(), c->mkv.free_(), c->NM = 0;
     c->mps.free_(), c->mtg.free_(), c->mflag.free_(), c->credit.free_(), c->elastic.free_(), c->comp_again.free_(), c->comp_size.free_();
@@ -539,58 +539,68 @@ static int commit_multifrontal(bl_gpu_ctx* c, const std::vector<int>& col_ptr, c
     const int nfr = (int)P.npiv.size(), nlev = (int)P.level_ptr.size() - 1;
     std::vector<MfFrontDev> fr(nfr);
     long long pool = 0;
-    int u = 0, dtn = 0, maxn = 0;
+    int dtn = 0, maxn = 0;
     for (int f = 0; f < nfr; f++) {
         MfFrontDev& d = fr[f];
         d.n = 6 * (P.npiv[f] + P.nrow[f]), d.p = 6 * P.npiv[f];
         d.off = pool, d.idx0 = P.idx_ptr[f], d.child0 = P.child_ptr[f], d.child1 = P.child_ptr[f + 1], d.comp = P.comp[f];
-        d.u0 = u, d.dt0 = dtn;
-        pool += (long long)d.n * d.n;
-        u += d.n - d.p;
-        dtn += kMfT * kMfT * ((d.p + kMfT - 1) / kMfT);
+        d.dt0 = dtn;
+        pool += (long long)d.n * (d.n + 1);
+        dtn += 2 * kMfT * kMfT * ((d.p + kMfT - 1) / kMfT);
         maxn = std::max(maxn, d.n);
     }
-    std::vector<int2> tcol, tpan;
-    std::vector<int4> tupd;
-    c->mf_tcol_ptr.assign(1, 0), c->mf_tpan_ptr.assign(nlev, {}), c->mf_tupd_ptr.assign(nlev, {});
+    // each off-diagonal block's row: its node's place in the front of its column
+    std::vector<int> brow(std::max<size_t>(row.size(), 1), 0);
+    for (int f = 0; f < nfr; f++) {
+        const int* first = P.idx.data() + P.idx_ptr[f];
+        const int* last = P.idx.data() + P.idx_ptr[f + 1];
+        for (int l = 0; l < P.npiv[f]; l++) {
+            const int k = first[l];
+            for (int pb = col_ptr[k]; pb < col_ptr[k + 1]; pb++) brow[pb] = (int)(std::lower_bound(first, last, row[pb]) - first);
+        }
+    }
+    std::vector<int4> tasm, tupd;
+    std::vector<int2> tpan;
+    c->mf_tasm_ptr.assign(1, 0), c->mf_tpan_ptr.assign(nlev, {}), c->mf_tupd_ptr.assign(nlev, {});
     int64_t launches = 0;
     for (int L = 0; L < nlev; L++) {
         int np = 0;
         for (int f = P.level_ptr[L]; f < P.level_ptr[L + 1]; f++) {
             const int nt = (fr[f].n + kMfT - 1) / kMfT;
-            for (int jt = 0; jt < nt; jt++) tcol.push_back(make_int2(f, jt));
+            for (int it = 0; it < nt; it++) {
+                for (int jt = 0; jt <= it; jt++) tasm.push_back(make_int4(f, it, jt, 0));
+                tasm.push_back(make_int4(f, it, -1, 0));
+            }
             np = std::max(np, (fr[f].p + kMfT - 1) / kMfT);
         }
-        c->mf_tcol_ptr.push_back((int)tcol.size());
+        c->mf_tasm_ptr.push_back((int)tasm.size());
         c->mf_tpan_ptr[L].push_back((int)tpan.size()), c->mf_tupd_ptr[L].push_back((int)tupd.size());
         for (int sp = 0; sp < np; sp++) {
             for (int f = P.level_ptr[L]; f < P.level_ptr[L + 1]; f++) {
                 if (fr[f].p <= kMfT * sp) continue;
                 const int nt = (fr[f].n + kMfT - 1) / kMfT;
                 for (int r = sp; r < nt; r++) tpan.push_back(make_int2(f, r));
-                tupd.push_back(make_int4(f, -1, -1, 0));
+                tupd.push_back(make_int4(f, 0, -1, 0));
+                for (int i = sp + 1; i < nt; i++) tupd.push_back(make_int4(f, i, -2, 0));
                 for (int j = sp + 1; j < nt; j++)
                     for (int i = j; i < nt; i++) tupd.push_back(make_int4(f, i, j, 0));
             }
             c->mf_tpan_ptr[L].push_back((int)tpan.size()), c->mf_tupd_ptr[L].push_back((int)tupd.size());
         }
-        launches += 1 + 2 * np + 2;
+        launches += 1 + 2 * np + 1;
     }
     int rc;
     if ((rc = upload_vec(c, c->mf_fr, fr)) || (rc = upload_vec(c, c->mf_idx, P.idx)) || (rc = upload_vec(c, c->mf_cmap, P.cmap)) ||
-        (rc = upload_vec(c, c->mf_child, P.child.empty() ? std::vector<int>(1, 0) : P.child)) || (rc = upload_vec(c, c->mf_tcol, tcol)) ||
-        (rc = upload_vec(c, c->mf_tpan, tpan.empty() ? std::vector<int2>(1) : tpan)) || (rc = upload_vec(c, c->mf_tupd, tupd.empty() ? std::vector<int4>(1) : tupd)))
+        (rc = upload_vec(c, c->mf_child, P.child.empty() ? std::vector<int>(1, 0) : P.child)) || (rc = upload_vec(c, c->mf_brow, brow)) ||
+        (rc = upload_vec(c, c->mf_tasm, tasm)) || (rc = upload_vec(c, c->mf_tpan, tpan.empty() ? std::vector<int2>(1) : tpan)) ||
+        (rc = upload_vec(c, c->mf_tupd, tupd.empty() ? std::vector<int4>(1) : tupd)))
         return rc;
     BL_CUDA(c, c->mf_pool.alloc((size_t)std::max(pool, 1LL)));
-    BL_CUDA(c, c->mf_u.alloc((size_t)std::max(u, 1)));
     BL_CUDA(c, c->mf_dt.alloc((size_t)std::max(dtn, 1)));
     c->mf_smem = sizeof(double) * (size_t)maxn;
-    if (c->mf_smem > 227 * 1024 - 2 * sizeof(double) * kMfT * (kMfT + 1)) return BL_GPU_ELIMIT; // (a front of more than ~3,500 nodes)
-    if (c->mf_smem > 40 * 1024) {
-        BL_CUDA(c, cudaFuncSetAttribute(k_mf_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->mf_smem));
-        BL_CUDA(c, cudaFuncSetAttribute(k_mf_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->mf_smem));
-    }
-    c->mf = MfDev{c->mf_fr.p, c->mf_idx.p, c->mf_cmap.p, c->mf_child.p, c->mf_pool.p, c->mf_u.p, c->mf_dt.p, c->mf_tcol.p, c->mf_tpan.p, c->mf_tupd.p};
+    if (c->mf_smem > 200 * 1024) return BL_GPU_ELIMIT; // (a front of more than ~4,200 nodes: its backward solve's vector)
+    if (c->mf_smem > 40 * 1024) BL_CUDA(c, cudaFuncSetAttribute(k_mf_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->mf_smem));
+    c->mf = MfDev{c->mf_fr.p, c->mf_idx.p, c->mf_cmap.p, c->mf_child.p, c->mf_brow.p, c->mf_pool.p, c->mf_dt.p, c->mf_tasm.p, c->mf_tpan.p, c->mf_tupd.p};
     c->mf_level_ptr = P.level_ptr;
     c->mf_flops = P.flops;
     c->chol_launches = launches;
@@ -1498,20 +1508,18 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             auto cholesky = [c, &F](cudaStream_t cs) {
                 if (c->cfg.fem_dense_front == 2) {
                     // multifrontal: per level of the front tree its fronts assembled, then panel by panel factored and
-                    // updated; the forward substitution level by level, the backward from the root down
+                    // updated with the right side carried along (the forward substitution); the backward from the root down
                     const MfDev& M = c->mf;
                     const int nlev = (int)c->mf_level_ptr.size() - 1;
                     for (int L = 0; L < nlev; L++) {
-                        k_mf_assemble<<<c->mf_tcol_ptr[L + 1] - c->mf_tcol_ptr[L], 256, 0, cs>>>(F, M, c->mf_tcol_ptr[L]);
+                        k_mf_assemble<<<c->mf_tasm_ptr[L + 1] - c->mf_tasm_ptr[L], 256, 0, cs>>>(F, M, c->mf_tasm_ptr[L]);
                         const std::vector<int>& tp = c->mf_tpan_ptr[L];
                         const std::vector<int>& tu = c->mf_tupd_ptr[L];
                         for (size_t sp = 0; sp + 1 < tp.size(); sp++) {
-                            k_mf_panel<<<tp[sp + 1] - tp[sp], 32, 0, cs>>>(M, tp[sp], (int)sp, F.comp_fail);
+                            k_mf_panel<<<tp[sp + 1] - tp[sp], 256, 0, cs>>>(M, tp[sp], (int)sp, F.comp_fail);
                             k_mf_update<<<tu[sp + 1] - tu[sp], 256, 0, cs>>>(M, tu[sp], (int)sp);
                         }
                     }
-                    for (int L = 0; L < nlev; L++)
-                        k_mf_forward<<<c->mf_level_ptr[L + 1] - c->mf_level_ptr[L], 256, c->mf_smem, cs>>>(F, M, c->mf_level_ptr[L]);
                     for (int L = nlev - 1; L >= 0; L--)
                         k_mf_backward<<<c->mf_level_ptr[L + 1] - c->mf_level_ptr[L], 256, c->mf_smem, cs>>>(F, M, c->mf_level_ptr[L]);
                     return;
