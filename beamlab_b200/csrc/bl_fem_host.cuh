@@ -499,6 +499,33 @@ static void fem_min_degree(const std::vector<int>& comp, const std::vector<int>&
     }
 }
 
+// The pattern's block updates, whether or not their list is built: sum over the columns of d (d + 1) / 2
+static int64_t fem_update_count(const FemModel& M) {
+    int64_t u = 0;
+    for (size_t k = 0; k + 1 < M.col_ptr.size(); k++) u += (int64_t)(M.col_ptr[k + 1] - M.col_ptr[k]) * (M.col_ptr[k + 1] - M.col_ptr[k] + 1) / 2;
+    return u;
+}
+
+// The update list of the column-by-column factorization: each source column k: the rows of column c = row[i]
+// scattered into a position table once, then every later row j of column k looked up in it
+static void fem_update_list(FemModel& M) {
+    const int n = (int)M.node.size();
+    M.upd.clear();
+    M.upd_ptr.assign(n + 1, 0);
+    std::vector<int> pos(n, -1);
+    for (int k = 0; k < n; k++) {
+        const int a0 = M.col_ptr[k], a1 = M.col_ptr[k + 1];
+        for (int i = a0; i < a1; i++) {
+            const int c = M.row[i];
+            for (int q = M.col_ptr[c]; q < M.col_ptr[c + 1]; q++) pos[M.row[q]] = q;
+            M.upd.push_back({i, i, -(c + 1)});
+            for (int j = i + 1; j < a1; j++) M.upd.push_back({i, j, pos[M.row[j]]});
+            for (int q = M.col_ptr[c]; q < M.col_ptr[c + 1]; q++) pos[M.row[q]] = -1;
+        }
+        M.upd_ptr[k + 1] = (int)M.upd.size();
+    }
+}
+
 // FemModel's ordering, pattern, block maps and gather lists; the update list too where want_updates
 static void fem_analyse(FemModel& M, bool want_updates = true) {
     const int n = (int)M.node.size();
@@ -532,22 +559,7 @@ static void fem_analyse(FemModel& M, bool want_updates = true) {
     };
     M.upd.clear();
     M.upd_ptr.assign(n + 1, 0);
-    if (want_updates) {
-        // each source column k: the rows of column c = row[i] scattered into a position table once, then every later
-        // row j of column k looked up in it
-        std::vector<int> pos(n, -1);
-        for (int k = 0; k < n; k++) {
-            const int a0 = M.col_ptr[k], a1 = M.col_ptr[k + 1];
-            for (int i = a0; i < a1; i++) {
-                const int c = M.row[i];
-                for (int q = M.col_ptr[c]; q < M.col_ptr[c + 1]; q++) pos[M.row[q]] = q;
-                M.upd.push_back({i, i, -(c + 1)});
-                for (int j = i + 1; j < a1; j++) M.upd.push_back({i, j, pos[M.row[j]]});
-                for (int q = M.col_ptr[c]; q < M.col_ptr[c + 1]; q++) pos[M.row[q]] = -1;
-            }
-            M.upd_ptr[k + 1] = (int)M.upd.size();
-        }
-    }
+    if (want_updates) fem_update_list(M);
     // each member's and each triangle edge's block (the block's row is the end eliminated later)
     M.mblock.assign(E, -1), M.mswap.assign(E, 0);
     for (size_t e = 0; e < E; e++) {

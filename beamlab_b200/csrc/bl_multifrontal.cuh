@@ -12,7 +12,7 @@
 //                  extend-add; a CTA owns its tile, so nothing races and the sums' order is fixed;
 //   per 32-wide panel s of the pivots, two launches:
 //   k_mf_panel     a CTA per (front, row tile r >= s): the panel's diagonal tile factored and its triangle inverted in
-//                  shared memory by one warp (every CTA alike); the CTA of r == s keeps both in the side buffer dt,
+//                  shared memory by the whole block (every CTA alike); the CTA of r == s keeps both in the side buffer dt,
 //                  writes the tile's trailing Schur complement where the panel ends inside the tile, and solves the
 //                  panel's part of b (y_s = L_ss^-1 b_s); a row tile's CTA forms X = A_rs L_ss^-T by all its warps and,
 //                  past a partial panel, updates the rest of its tile;
@@ -132,43 +132,49 @@ __global__ void __launch_bounds__(256) k_mf_assemble(FemDev F, MfDev M, int t0) 
     }
 }
 
-// The panel's diagonal tile (rows/columns past n as zeros) in D, factored over its first w columns by warp 0
-// (right-looking; lane = row); full: also the tile's trailing part (the Schur complement of the columns past w). Then
-// the inverse of its w x w triangle into Li (lane = column: each column of the inverse by forward substitution).
-// Returns false at a pivot that is not positive.
-__device__ __forceinline__ bool mf_factor_tile(double (*D)[kMfT + 1], double (*Li)[kMfT + 1], int w, int ncols, bool full) {
-    const int lane = threadIdx.x & 31;
-    bool ok = true;
+// The panel's diagonal tile (rows/columns past n as zeros) in D, factored over its first w columns by the whole block,
+// right-looking, with the inverse of its w x w triangle built in the same sweep (Y starts as the identity; at column k
+// its row k is scaled by the pivot's inverse and the rows below lose D_rk times it). full: also the tile's trailing
+// part (the Schur complement of the columns past w). Two barriers a column; a thread a few entries of each update.
+// (Measured against one warp owning a column each: that took 40 % longer, its lanes' loops uneven.) Returns false at a
+// pivot that is not positive.
+__device__ __forceinline__ bool mf_factor_tile(double (*D)[kMfT + 1], double (*Y)[kMfT + 1], int w, int ncols, bool full, int* bad) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    for (int e = tid; e < kMfT * kMfT; e += nth) {
+        const int i = e & (kMfT - 1), j = e / kMfT;
+        Y[i][j] = (i == j && i < w) ? 1.0 : 0.0;
+    }
+    if (tid == 0) *bad = 0;
+    __syncthreads();
     const int jend = full ? ncols : w;
     for (int k = 0; k < w; k++) {
-        __syncwarp();
         double dk = D[k][k];
-        if (!(dk > 0)) ok = false, dk = 1.0;
-        const double d = sqrt(dk), id = 1.0 / d;
-        __syncwarp();
-        if (lane == k) D[k][k] = d;
-        if (lane > k) D[lane][k] *= id;
-        __syncwarp();
-        if (lane > k)
-            for (int j = k + 1; j <= lane && j < jend; j++) D[lane][j] -= D[lane][k] * D[j][k];
-    }
-    __syncwarp();
-    // column `lane` of L^-1: L x = e_lane, rows from lane on
-    for (int i = 0; i < kMfT; i++) Li[i][lane] = 0.0;
-    if (lane < w) {
-        for (int i = lane; i < w; i++) {
-            double t = i == lane ? 1.0 : 0.0;
-            for (int m = lane; m < i; m++) t -= D[i][m] * Li[m][lane];
-            Li[i][lane] = t / D[i][i];
+        if (!(dk > 0)) dk = 1.0;
+        const double id = 1.0 / sqrt(dk);
+        // the trailing lower triangle and the inverse's rows below k, from column k and row k of Y scaled on the fly
+        for (int e = tid; e < kMfT * kMfT; e += nth) {
+            const int i = e & (kMfT - 1), j = e / kMfT;
+            if (j > k && j <= i && j < jend) D[i][j] -= (D[i][k] * id) * (D[j][k] * id);
+            if (i > k && i < w && j <= k) Y[i][j] -= (D[i][k] * id) * (Y[k][j] * id);
         }
+        __syncthreads();
+        if (tid < kMfT) {
+            if (tid > k) D[tid][k] *= id;
+            else if (tid == k) {
+                if (!(D[k][k] > 0)) *bad = 1;
+                D[k][k] = 1.0 / id;
+            }
+        } else if (tid < 2 * kMfT && tid - kMfT <= k) {
+            Y[k][tid - kMfT] *= id;
+        }
+        __syncthreads();
     }
-    __syncwarp();
-    return ok;
+    return *bad == 0;
 }
 
 __global__ void __launch_bounds__(256) k_mf_panel(MfDev M, int t0, int s, int* comp_fail) {
     __shared__ double D[kMfT][kMfT + 1], Li[kMfT][kMfT + 1], R[kMfT][kMfT + 1];
-    __shared__ int okf;
+    __shared__ int bad;
     const int2 task = M.tpan[t0 + blockIdx.x];
     const MfFrontDev fr = M.fr[task.x];
     const int n = fr.n, c0 = kMfT * s, w = min(kMfT, fr.p - c0), ncols = min(kMfT, n - c0), tid = threadIdx.x;
@@ -180,11 +186,7 @@ __global__ void __launch_bounds__(256) k_mf_panel(MfDev M, int t0, int s, int* c
         D[i][j] = (j < jload && i < ncols) ? A[(size_t)(c0 + j) * n + c0 + i] : 0.0;
     }
     __syncthreads();
-    if (tid < 32) {
-        const bool ok = mf_factor_tile(D, Li, w, ncols, diag);
-        if (tid == 0) okf = ok;
-    }
-    __syncthreads();
+    const bool ok = mf_factor_tile(D, Li, w, ncols, diag, &bad);
     if (diag) {
         double* T = M.dt + fr.dt0 + (size_t)s * 2 * kMfT * kMfT; // (L then L^-1, column-major)
         for (int e = tid; e < kMfT * kMfT; e += blockDim.x) {
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(256) k_mf_panel(MfDev M, int t0, int s, int* c
             for (int m = 0; m < w; m++) t -= D[tid][m] * y[m];
             b[tid] = t;
         }
-        if (!okf && tid == 0) atomicExch(&comp_fail[fr.comp], 1);
+        if (!ok && tid == 0) atomicExch(&comp_fail[fr.comp], 1);
         return;
     }
     const int r0 = kMfT * task.y, nr = min(kMfT, n - r0);

@@ -216,6 +216,7 @@ struct bl_gpu_ctx {
     std::vector<int> mf_tasm_ptr;              // per level: its assembly tasks
     std::vector<std::vector<int>> mf_tpan_ptr, mf_tupd_ptr; // per level, per panel: its tasks
     size_t mf_smem = 0;                        // the solves' dynamic shared memory (the largest front)
+    int fem_mode = 0;                          // the factorization in use: fem_dense_front, 3 resolved to 1 or 2
     double mf_flops = 0;
     DevBuf<float> finertia, tX, tk, ttan, tb, tX0, th0, tdmg;
     DevBuf<uint8_t> tbroken, ton, ffixed;
@@ -607,6 +608,12 @@ static int commit_multifrontal(bl_gpu_ctx* c, const std::vector<int>& col_ptr, c
     return BL_GPU_OK;
 }
 
+// fem_dense_front 3 (automatic): the block-column path with its dense top chain while the frames' factorization makes
+// at most this many block updates, the multifrontal one above (measured on B200: the 64 x 64 plate's 1.4 M updates
+// factor in 2.3 ms a substep by block columns against 3.9 ms multifrontal; the 10k-node shell body's 12.6 M in 7.8 ms
+// against 8.0 ms; beyond, the block columns' update lists and levels grow as fast as the fill)
+constexpr int64_t kAutoMultifrontal = 8000000;
+
 static int commit_fem(bl_gpu_ctx* c) {
     int NF = 0, NT = 0, NB = 0, NC = 0, NS = 0, nfem_nodes = 0;
     for (const HostBody& hb : c->bodies)
@@ -741,6 +748,14 @@ static int commit_fem(bl_gpu_ctx* c) {
     for (int k = 0; k < NF; k++) bylev[level[k]].push_back(k);
     c->NU = 0; // (the pattern's block updates, whether or not their list was built: sum over columns of d (d + 1) / 2)
     for (int k = 0; k < NF; k++) c->NU += (int64_t)(col_ptr[k + 1] - col_ptr[k]) * (col_ptr[k + 1] - col_ptr[k] + 1) / 2;
+    if (c->cfg.fem_dense_front == 3) {
+        bool lists = c->NU <= kAutoMultifrontal;
+        for (const HostBody& hb : c->bodies)
+            if (hb.fem && fem_update_count(*hb.fem) > 0 && hb.fem->upd.empty()) lists = false;
+        c->fem_mode = lists ? 1 : 2;
+    } else {
+        c->fem_mode = c->cfg.fem_dense_front;
+    }
     std::vector<std::vector<int>> col_upds(NF);
     for (size_t u = 0; u < gupd.size(); u++) col_upds[upd_col[u]].push_back((int)u);
     c->lvl_grp_ptr.assign(1, 0), c->lvl_col_ptr.assign(1, 0);
@@ -871,7 +886,7 @@ static int commit_fem(bl_gpu_ctx* c) {
         const int nlev = (int)c->lvl_col_ptr.size() - 1;
         int top = nlev;
         while (top > 0 && c->lvl_col_ptr[top] - c->lvl_col_ptr[top - 1] == 1) top--;
-        const int m = c->cfg.fem_dense_front == 1 ? nlev - top : 0;
+        const int m = c->fem_mode == 1 ? nlev - top : 0;
         std::vector<int> chain(NF, -1), fcol;
         std::vector<int4> fblk;
         bool closed = m >= kFrontMin && 6 * m <= 8192; // (D at most 512 MB, its solve's vector in shared memory)
@@ -898,7 +913,7 @@ static int commit_fem(bl_gpu_ctx* c) {
         }
         c->chol_launches = 3 * (int64_t)c->front_level;
         if (c->front_level < nlev) c->chol_launches += 1 + c->front.nt + 2 * (c->front.nt - 1) + 2;
-        if (c->cfg.fem_dense_front == 2 && (rc = commit_multifrontal(c, col_ptr, row, col_comp))) return rc;
+        if (c->fem_mode == 2 && (rc = commit_multifrontal(c, col_ptr, row, col_comp))) return rc;
         c->fem_launches = 4 + (c->NT > 0 ? 1 : 0) + (c->NM > 0 ? 1 : 0) + c->chol_launches; // (begin, triangles, members, assembly, velocity, integration)
     }
     // PCG: vectors, block-Jacobi factors, the grid's partial sums (one cooperative launch: as many blocks as fit)
@@ -1506,7 +1521,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             if (rec) k_mlp_record_pre<<<(c->NF + 127) / 128, 128, 0, s>>>(F, MD);
             if (learned) k_mlp_infer<<<(c->NF + kLanes - 1) / kLanes, kLanes, 0, s>>>(F, MD, c->guess.p, c->gscale.p);
             auto cholesky = [c, &F](cudaStream_t cs) {
-                if (c->cfg.fem_dense_front == 2) {
+                if (c->fem_mode == 2) {
                     // multifrontal: per level of the front tree its fronts assembled, then panel by panel factored and
                     // updated with the right side carried along (the forward substitution); the backward from the root down
                     const MfDev& M = c->mf;
@@ -1713,7 +1728,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->pcg_learned_scale = 0;
     cfg->graphs = 1;
     cfg->beam_kernel = 0;
-    cfg->fem_dense_front = 2;
+    cfg->fem_dense_front = 3;
     cfg->force_block = 0;
     cfg->integrate_block = 0;
     cfg->beams_per_sm = 0;
@@ -1743,7 +1758,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_default_config(&c0);
     if (cfg) c0 = *cfg;
     if (!(c0.dt > 0) || c0.deterministic != 1 || c0.max_pairs < 1 || c0.fem_solver < 0 || c0.fem_solver > 3 || c0.pcg_max_iters < 0 ||
-        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 2 ||
+        !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 3 ||
         !(c0.force_block == 0 || c0.force_block == 64 || c0.force_block == 128 || c0.force_block == 256) ||
         !(c0.integrate_block == 0 || c0.integrate_block == 64 || c0.integrate_block == 128 || c0.integrate_block == 256) ||
         c0.beams_per_sm < 0 || c0.beams_per_sm > 16 || !(c0.tyre_grip >= 0))
@@ -1968,7 +1983,9 @@ int bl_gpu_add_body(bl_gpu_ctx* c, const bl_body_desc* d, int32_t* body_id) {
     hb.beam_bits = (d->allow_deform ? BB_DEFORM : 0u) | (d->allow_break ? BB_BREAK : 0u) | (d->ductile ? BB_DUCTILE : 0u);
     if (d->fem && (d->fem->n_tris > 0 || d->fem->n_members > 0)) {
         std::shared_ptr<FemModel> M;
-        const int rc = build_fem_model(d->nodes, d->info, d->n_nodes, *d->fem, hb.sections, hb.fsections, M, c->cfg.fem_dense_front != 2);
+        const int mode = c->cfg.fem_dense_front;
+        const int rc = build_fem_model(d->nodes, d->info, d->n_nodes, *d->fem, hb.sections, hb.fsections, M, mode == 0 || mode == 1);
+        if (!rc && mode == 3 && fem_update_count(*M) <= kAutoMultifrontal) fem_update_list(*M); // (the block-column path may be chosen)
         if (rc) return rc;
         hb.fq.assign(4 * M->node.size(), 0.0f);
         for (size_t i = 0; i < M->node.size(); i++) hb.fq[4 * i + 3] = 1.0f;
@@ -2320,9 +2337,9 @@ int bl_gpu_fem_stats(bl_gpu_ctx* c, bl_fem_stats* out) {
     out->pcg_solves = st[0], out->pcg_fallbacks = st[1], out->last_iterations = st[2], out->pcg_iterations = it;
     out->last_pcg_residual = last, out->max_residual = res[0], out->last_residual = res[3];
     out->columns = c->NF, out->blocks = c->NB, out->updates = c->NU, out->levels = (int64_t)c->lvl_col_ptr.size() - 1;
-    out->fronts = c->cfg.fem_dense_front == 2 ? (int64_t)c->mf_fr.n : 0;
-    out->factor_flops = c->cfg.fem_dense_front == 2 ? c->mf_flops : 432.0 * (double)c->NU;
-    if (c->cfg.fem_dense_front == 2) out->levels = (int64_t)c->mf_level_ptr.size() - 1;
+    out->fronts = c->fem_mode == 2 ? (int64_t)c->mf_fr.n : 0;
+    out->factor_flops = c->fem_mode == 2 ? c->mf_flops : 432.0 * (double)c->NU;
+    if (c->fem_mode == 2) out->levels = (int64_t)c->mf_level_ptr.size() - 1;
     if (c->any_plastic_members) {
         long long rp = 0;
         BL_CUDA(c, cudaMemcpy(&rp, c->repc.p, sizeof(rp), cudaMemcpyDeviceToHost));

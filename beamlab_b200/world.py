@@ -72,9 +72,9 @@ class WorldSettings:
     graphs: bool = True
     # the beams' kernel: 0 streams the beam arrays by bulk (TMA) copies, 1 plain loads (the same results)
     beam_kernel: int = 0
-    # the FEM factorization: 2 multifrontal (dense fronts, level by level of the front tree), 1 block columns with the
-    # top chain as one dense front, 0 block columns in the reference's order of sums
-    fem_dense_front: int = 2
+    # the FEM factorization: 3 by size (1 up to 8 M block updates, else 2), 2 multifrontal (dense fronts, level by level
+    # of the front tree), 1 block columns with the top chain as one dense front, 0 block columns in the reference's order
+    fem_dense_front: int = 3
     tyre_grip: float = 1.0                    # WorldSettings::tyre_grip: a factor on the tyres' friction
     # launch shapes (None: the tuned ones of beamlab_b200/tuned.json when present, else the library's defaults);
     # results do not depend on them

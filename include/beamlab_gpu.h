@@ -86,12 +86,13 @@ typedef struct {
                                   (TMA) copies and the nodes' kernel reads 4-byte incidences where the rig allows; 1:
                                   plain loads and 8-byte incidences. Results are the same. */
     int32_t fem_dense_front;   /* how the FEM step factors its system (the same pattern and fill as the reference's):
-                                  2 (default): multifrontal - the columns grouped into dense fronts (supernodes of the
-                                  elimination tree, small ones amalgamated), each factored by dense tiled kernels, level by
-                                  level of the front tree; 1: block column by block column, with the top chain of the
-                                  elimination tree (levels of one column each) as one dense front; 0: block column by block
-                                  column in the reference's order of sums throughout. 2 and 1 differ from 0 in the order of
-                                  the floating-point sums only. */
+                                  3 (default): 1 while the frames' factorization makes at most 8 M block updates, 2 above;
+                                  2: multifrontal - the columns grouped into dense fronts (supernodes of the elimination
+                                  tree, small ones amalgamated), each factored by dense tiled kernels, level by level of the
+                                  front tree; 1: block column by block column, with the top chain of the elimination tree
+                                  (levels of one column each) as one dense front; 0: block column by block column in the
+                                  reference's order of sums throughout. 2 and 1 differ from 0 in the order of the
+                                  floating-point sums only. */
     /* launch shapes (results do not depend on them; beamlab_b200/autotune.py measures them for a device and workload): */
     int32_t force_block;       /* the nodes' force kernel's block size: 64, 128 or 256; 0 (default): 256 */
     int32_t integrate_block;   /* the integration kernel's block size: 64, 128 or 256; 0 (default): 256 */
