@@ -478,12 +478,16 @@ def stress_rig(seed: int = 7) -> dict:
 
 def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, sigma: float = 0.6,
           min_nodes: int = 500, max_nodes: int = 20000, terrain_size: float = 1000.0, terrain_samples: int = 2048,
-          amplitude: float = 2.0, skins: bool = True, wheels: bool = True) -> dict:
+          amplitude: float = 2.0, skins: bool = True, wheels: bool = True, layout: str = "grid") -> dict:
     """A batched fleet of lattice trusses with log-normal node counts (median `median_nodes`, clipped to
     [min_nodes, max_nodes]), each driving at a speed uniform in [5, 30] m/s with a random yaw over a square heightfield
-    of terrain_samples^2 samples spanning terrain_size metres, `amplitude` m of seeded smooth noise. Vehicles start on
-    a grid 40 m apart; with skins (lattice_tris) those that meet collide; with wheels each stands on four wheel rings
-    of 24 tyre nodes (add_wheels). Random draws: numpy's PCG64 seeded with `seed` (the skins and wheels draw none)."""
+    of terrain_samples^2 samples spanning terrain_size metres, `amplitude` m of seeded smooth noise (two octaves of
+    bilinear value noise). layout "grid": vehicles start on a grid 40 m apart, each on its own heading (few meet);
+    "pairs": vehicles two by two on a grid 40 m apart, each pair head-on along a random axis, each vehicle its reach,
+    0.15 m and its speed times the pair's meeting time (uniform in [0.02, 0.12] s) from the pair's centre - every pair
+    crashes within its first few frames and stays in contact. With skins (lattice_tris) vehicles that meet collide; with wheels each stands on
+    four wheel rings of 24 tyre nodes (add_wheels). Random draws: numpy's PCG64 seeded with `seed` (the skins and
+    wheels draw none)."""
     gen = np.random.default_rng(seed)
     cell = terrain_size / (terrain_samples - 1)
     half = terrain_size / 2
@@ -498,23 +502,45 @@ def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, si
     h = (octave(33, amplitude) + octave(129, amplitude * 0.25)).astype(np.float32)
     terrain = {"nx": terrain_samples, "nz": terrain_samples, "cell": cell, "origin": (-half, -half), "heights": h,
                "surfaces": np.zeros((terrain_samples, terrain_samples), np.uint8)}
-    side = int(math.ceil(math.sqrt(n_vehicles)))
-    bodies = []
-    for v in range(n_vehicles):
-        nn = int(np.clip(median_nodes * math.exp(sigma * gen.standard_normal()), min_nodes, max_nodes))
-        # lattice dims in a car's proportions: length 4, width 1.25, height 1
+    if layout not in ("grid", "pairs"):
+        raise ValueError(f"unknown layout {layout}")
+    slots = n_vehicles if layout == "grid" else (n_vehicles + 1) // 2
+    side = int(math.ceil(math.sqrt(slots)))
+    sp = 0.25  # (lattice_body_fast's spacing)
+
+    def dims_of(nn):  # lattice dims in a car's proportions: length 4, width 1.25, height 1
         unit = (nn / 5.0) ** (1.0 / 3.0)
         nx = max(2, int(round(4 * unit / 1.7)))
         nz = max(2, int(round(1.25 * unit / 1.7 * 1.2)))
         ny = max(2, int(round(nn / (nx * nz))))
-        gx, gz = v % side, v // side
-        x0, z0 = -half + 60 + gx * 40.0, -half + 60 + gz * 40.0
-        ix, iz = int((x0 + half) / cell), int((z0 + half) / cell)
-        ground = float(h[min(iz, terrain_samples - 1), min(ix, terrain_samples - 1)])
+        return nx, ny, nz
+
+    bodies = []
+    pair = None  # (the pair's centre, axis, the first vehicle's reach and speed) while its second is drawn
+    for v in range(n_vehicles):
+        nn = int(np.clip(median_nodes * math.exp(sigma * gen.standard_normal()), min_nodes, max_nodes))
+        nx, ny, nz = dims_of(nn)
+        reach = 0.5 * sp * math.hypot(nx - 1, nz - 1)  # (the lattice's horizontal half-diagonal)
         speed = float(gen.uniform(5.0, 30.0))
         yaw = float(gen.uniform(0.0, 2 * math.pi))
-        body = lattice_body_fast(gen, dims=(nx, ny, nz), origin=(x0, ground + 0.6, z0),
-                                 velocity=(speed * math.cos(yaw), 0.0, speed * math.sin(yaw)))
+        if layout == "grid":
+            gx, gz = v % side, v // side
+            x0, z0 = -half + 60 + gx * 40.0, -half + 60 + gz * 40.0
+            vel = (speed * math.cos(yaw), 0.0, speed * math.sin(yaw))
+        else:
+            if v % 2 == 0:
+                gx, gz = (v // 2) % side, (v // 2) // side
+                pair = ((-half + 60 + gx * 40.0, -half + 60 + gz * 40.0), (math.cos(yaw), math.sin(yaw)), reach, speed,
+                        float(gen.uniform(0.02, 0.12)))
+            (cx, cz), (ux, uz), _, _, t_meet = pair
+            away = reach + 0.15 + speed * t_meet  # (its reach and its run to the meeting point)
+            sgn = -1.0 if v % 2 == 0 else 1.0  # (the first on the axis' near side driving along it, the second facing it)
+            ccx, ccz = cx + sgn * away * ux, cz + sgn * away * uz
+            x0, z0 = ccx - 0.5 * sp * (nx - 1), ccz - 0.5 * sp * (nz - 1)
+            vel = (-sgn * speed * ux, 0.0, -sgn * speed * uz)
+        ix, iz = int((x0 + half) / cell), int((z0 + half) / cell)
+        ground = float(h[min(max(iz, 0), terrain_samples - 1), min(max(ix, 0), terrain_samples - 1)])
+        body = lattice_body_fast(gen, dims=(nx, ny, nz), origin=(x0, ground + 0.6, z0), velocity=vel)
         if skins:
             body["tris"] = lattice_tris((nx, ny, nz))
         if wheels:
@@ -522,7 +548,7 @@ def fleet(n_vehicles: int = 256, seed: int = 3, median_nodes: float = 3000.0, si
         bodies.append(body)
     return {"settings": {"gravity": (0.0, -9.81, 0.0), "dt": 0.0005},
             "statics": {"terrain": terrain, "boxes": [], "build_grid": True}, "bodies": bodies,
-            "name": f"fleet(n={n_vehicles}, seed={seed})"}
+            "name": f"fleet(n={n_vehicles}, seed={seed}, layout={layout})"}
 
 
 def shell_plate(n: int = 63, size: float = 1.0, origin=(0.0, 1.0, 0.0), thickness: float = 0.0015, E: float = 210e9,

@@ -46,11 +46,12 @@ BYTES_PER_NODE = 52
 def workload(name: str, rank: int):
     from beamlab_b200 import rigs
     if name == "fleet256":
-        rig = rigs.fleet(256, seed=3 + rank)
+        rig = rigs.fleet(256, seed=3 + rank, layout="pairs")
         n, m = rigs.rig_counts(rig)
         nt = sum(len(b.get("tris", ())) for b in rig["bodies"])
         desc = (f"fleet256: 256 lattice vehicles ({n:,} nodes, {m:,} beams, {nt:,} collision triangles; log-normal "
-                f"500-20,000 nodes, median 3,000), 2048^2-sample 1 km^2 heightfield, 5-30 m/s random yaw, "
+                f"500-20,000 nodes, median 3,000), 2048^2-sample 1 km^2 heightfield (two octaves of value noise, 2 m), "
+                f"5-30 m/s, laid out in 128 head-on pairs on random axes that crash within their first 0.12 s, "
                 f"inter-vehicle node-triangle contacts (islands, pair search every 17 substeps); 4 wheel rings of 24 "
                 f"tyre nodes a vehicle (free rolling, tyre patches sharing grip)")
     elif name == "plate64":

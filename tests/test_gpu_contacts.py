@@ -103,3 +103,32 @@ def test_sleeping_body_woken_by_contact_matches_reference(ref_lib):
         r = ref.nodes(b)
         assert np.array_equal(bits(nd["p"]), bits(r["pos"])) and np.array_equal(bits(nd["v"]), bits(r["vel"])), f"body {b}"
     w.close()
+
+
+def test_fleet_pairs_crashing_at_once_equal_reference(ref_lib):
+    """Eight islands in contact at once: a fleet of 16 lattice vehicles with skins and wheels laid out in head-on pairs
+    (rigs.fleet(layout="pairs")) over a heightfield, 8 frames of 33 substeps on the GPU and by the compiled reference:
+    after every frame the pair lists equal the reference's element for element (the islands' lists in the reference's
+    order) and every node's position and velocity is bitwise the reference's."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.fleet(16, seed=5, median_nodes=900, min_nodes=300, max_nodes=3000, terrain_size=400.0, terrain_samples=513,
+                     layout="pairs")
+    w = world_from_rig(rig)
+    r = build_world(RefWorld, rig, multithreaded=False)
+    total = 0
+    for f in range(8):
+        w.step_substeps(33)
+        r.step_substeps(33)
+        got, want = w.pairs(), r.pairs()
+        assert got.shape == want.shape and np.array_equal(got, want), f"frame {f}: pair lists differ ({len(got)} vs {len(want)})"
+        total += len(want)
+        for b in range(len(rig["bodies"])):
+            g, ref = w.bodies()[b].nodes(), r.nodes(b)
+            assert np.array_equal(bits(g["p"]), bits(ref["pos"])), f"frame {f} vehicle {b}: positions differ"
+            assert np.array_equal(bits(g["v"]), bits(ref["vel"])), f"frame {f} vehicle {b}: velocities differ"
+    st = w.stats()
+    assert total > 0 and st["contacts"] > 1000 and st["pair_searches"] > 0 and st["device_errors"] == 0
+    touched = sum(1 for b in range(16) if w.bodies()[b].state()["body_contacts"] > 0)
+    assert touched >= 14, f"only {touched} of 16 vehicles in contact"  # (all eight pairs crash)
+    w.close()
+    r.close()

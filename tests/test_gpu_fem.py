@@ -100,6 +100,31 @@ def test_gpu_shell_body_matches_reference(ref_lib):
     w.close()
 
 
+def test_gpu_large_shell_body_multifrontal_matches_reference(ref_lib):
+    """The shell body at 5,384 nodes (10,024 triangles, 344 members; 4.9 M block updates a factorization by the
+    reference's column-by-column Cholesky) factored by the multifrontal path: 60 substeps under gravity and two point
+    loads within the FEM tolerance (1e-4 m) of the compiled reference, every solution's relative residual at most 1e-6
+    (measured against the assembled system kept aside), no failed factorization on either side."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.shell_body(5000)
+    w = world_from_rig(rig, fem_dense_front=2, fem_check_residual=True)
+    ref = build_world(RefWorld, rig, multithreaded=False)
+    h = w.bodies()[0]
+    p0 = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
+    for f in range(3):
+        w.step_substeps(20)
+        ref.step_substeps(20)
+    p = np.ascontiguousarray(h.nodes()["p"]).astype(np.float64)
+    d = np.abs(p - ref.nodes(0)["pos"]).max()
+    fs = w.fem_stats()
+    assert fs["fronts"] > 0 and fs["columns"] > 5000
+    assert d <= TOL, f"max |dp| {d:.3g} m"
+    assert fs["max_residual"] <= 1e-6, fs["max_residual"]
+    assert np.abs(p - p0).max() > 1e-4  # (it moves)
+    assert h.state()["fem_failures"] == 0 and ref.fem_info(0)["solve_failures"] == 0
+    w.close()
+
+
 def test_gpu_yielding_plate_matches_reference(ref_lib):
     """A plate of a yielding section (250 MPa) under a 3 kN point load, on a body that deforms and does not break:
     its membrane flows (the rest shapes follow the stretch, the elements built again) and its bending yields (the
