@@ -485,8 +485,9 @@ __global__ void __launch_bounds__(256) k_beams(const int2* __restrict__ ab, cons
 
 // ------------------------------------------------------------------------------------------ bulk copies (TMA)
 // cp.async.bulk global -> shared completing on an mbarrier: the beam arrays stream into shared memory tile after tile
-// while the block computes earlier tiles. Every wait is bounded in time (kWaitNs): a copy that never lands raises
-// DEVERR_TIMEOUT and the block stops instead of waiting for ever.
+// while the block computes earlier tiles. Every wait is bounded in time (the context's bulk_wait_s, 1 s by default): a
+// copy that never lands raises DEVERR_TIMEOUT and the block lets the copies still in flight land (bounded by kWaitNs)
+// and stops instead of waiting for ever.
 constexpr unsigned long long kWaitNs = 1000000000ull; // 1 s
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -509,11 +510,18 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 // the generic proxy's reads of a buffer ordered before the async proxy's next writes into it
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// waits for the phase of `parity` to complete; false after kWaitNs
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// waits for the phase of `parity` to complete; false after limit_ns (limit 0: one non-blocking test)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long limit_ns = kWaitNs) {
     const uint32_t a = smem_u32(bar);
     uint32_t done = 0;
     unsigned long long t0 = 0;
+    if (limit_ns == 0) {
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        return done != 0;
+    }
     for (int it = 0;; it++) {
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
                      : "=r"(done)
@@ -521,7 +529,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
                      : "memory");
         if (done) return true;
         if (it == 0) t0 = global_ns();
-        else if (global_ns() - t0 > kWaitNs) return false;
+        else if (global_ns() - t0 > limit_ns) return false;
     }
 }
 
@@ -642,7 +650,8 @@ __global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const void* __restri
                                                             float4* __restrict__ bst, uint32_t* __restrict__ bmeta, const float4* __restrict__ bcold,
                                                             float* __restrict__ stress, const int* __restrict__ bbody, float* __restrict__ fsc,
                                                             const float4* __restrict__ nd, Body* __restrict__ bodies, int nbeams, int nbodies, int ntiles,
-                                                            uint32_t* __restrict__ deverr, const int4* __restrict__ info, WheelDev wh, float dt) {
+                                                            uint32_t* __restrict__ deverr, const int4* __restrict__ info, WheelDev wh, float dt,
+                                                            unsigned long long wait_ns) {
     using Stage = BeamStage<kEnds16>;
     using AbT = typename std::remove_reference<decltype(Stage::ab[0])>::type;
     const AbT* ab = static_cast<const AbT*>(ab_);
@@ -678,7 +687,7 @@ __global__ void __launch_bounds__(kBeamThreads) k_beams_tma(const void* __restri
         const int s = i % kBeamStages;
         const int base = base_next;
         if (kEnds16 && i + 1 < mine) base_next = tbase[blockIdx.x + (i + 1) * gridDim.x];
-        const bool late = !mbar_wait(&full[s], (uint32_t)(i / kBeamStages) & 1u);
+        const bool late = !mbar_wait(&full[s], (uint32_t)(i / kBeamStages) & 1u, wait_ns);
         if (__syncthreads_or(late)) {
             // a copy did not land in time: flag it, let the copies in flight land (bounded), stop
             if (tid == 0) {

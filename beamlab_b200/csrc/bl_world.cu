@@ -217,6 +217,7 @@ struct bl_gpu_ctx {
     std::vector<std::vector<int>> mf_tpan_ptr, mf_tupd_ptr; // per level, per panel: its tasks
     size_t mf_smem = 0;                        // the solves' dynamic shared memory (the largest front)
     int fem_mode = 0;                          // the factorization in use: fem_dense_front, 3 resolved to 1 or 2
+    unsigned long long wait_ns = 1000000000ull; // the beams kernel's bound on a wait for its bulk copies (bulk_wait_s)
     double mf_flops = 0;
     DevBuf<float> finertia, tX, tk, ttan, tb, tX0, th0, tdmg;
     DevBuf<uint8_t> tbroken, ton, ffixed;
@@ -1469,11 +1470,11 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             if (c->ends16)
                 k_beams_tma<true><<<c->beam_grid, kBeamThreads, beam_smem<true>(), s>>>(c->ab16.p, c->tbase.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p,
                                                                                        c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B,
-                                                                                       c->beam_tiles, c->deverr.p, c->info.p, wh, dt);
+                                                                                       c->beam_tiles, c->deverr.p, c->info.p, wh, dt, c->wait_ns);
             else
                 k_beams_tma<false><<<c->beam_grid, kBeamThreads, beam_smem<false>(), s>>>(c->ab.p, nullptr, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p,
                                                                                          c->stress.p, c->bbody.p, c->fsc.p, c->nd.p, c->dbodies.p, c->M, c->B,
-                                                                                         c->beam_tiles, c->deverr.p, c->info.p, wh, dt);
+                                                                                         c->beam_tiles, c->deverr.p, c->info.p, wh, dt, c->wait_ns);
         } else {
             k_beams<<<std::max(gb, 1), tb, 0, s>>>(c->ab.p, c->kd.p, c->bst.p, c->bmeta.p, c->bcold.p, c->stress.p, c->bbody.p, c->fsc.p, c->nd.p,
                                                    c->dbodies.p, c->M, c->B);
@@ -1733,6 +1734,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->integrate_block = 0;
     cfg->beams_per_sm = 0;
     cfg->tyre_grip = 1.0f;
+    cfg->bulk_wait_s = 1.0f;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -1761,7 +1763,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
         !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 3 ||
         !(c0.force_block == 0 || c0.force_block == 64 || c0.force_block == 128 || c0.force_block == 256) ||
         !(c0.integrate_block == 0 || c0.integrate_block == 64 || c0.integrate_block == 128 || c0.integrate_block == 256) ||
-        c0.beams_per_sm < 0 || c0.beams_per_sm > 16 || !(c0.tyre_grip >= 0))
+        c0.beams_per_sm < 0 || c0.beams_per_sm > 16 || !(c0.tyre_grip >= 0) || !(c0.bulk_wait_s >= 0 && c0.bulk_wait_s <= 10))
         return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;
@@ -1770,6 +1772,7 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
     bl_gpu_ctx* c = new (std::nothrow) bl_gpu_ctx();
     if (!c) return BL_GPU_ENOMEM;
     c->cfg = c0;
+    c->wait_ns = (unsigned long long)((double)c0.bulk_wait_s * 1e9);
     auto fail = [&](cudaError_t e) {
         c->last_cuda = (int)e;
         delete c;

@@ -61,6 +61,7 @@ class WorldSettings:
     sleep_time: float = 1.0
     collision_hz: float = 120.0
     inter_body_collisions: bool = True
+    max_pairs: int = 0                        # the contact pair list's capacity (0: the library's default, 2^21)
     # the FEM frames' implicit step (no counterpart in the reference, which always factors): "cholesky", "pcg",
     # "pcg_learned", "pcg_previous"; a PCG solve that misses pcg_tol within pcg_max_iters falls back to the Cholesky
     fem_solver: str = "cholesky"
@@ -76,6 +77,7 @@ class WorldSettings:
     # of the front tree), 1 block columns with the top chain as one dense front, 0 block columns in the reference's order
     fem_dense_front: int = 3
     tyre_grip: float = 1.0                    # WorldSettings::tyre_grip: a factor on the tyres' friction
+    bulk_wait_s: float = 1.0                  # the beams kernel's bound on a wait for its bulk copies (0: test once)
     # launch shapes (None: the tuned ones of beamlab_b200/tuned.json when present, else the library's defaults);
     # results do not depend on them
     force_block: int | None = None
@@ -378,7 +380,8 @@ class _Config(C.Structure):
                 ("fem_solver", C.c_int32), ("pcg_max_iters", C.c_int32), ("pcg_tol", C.c_float),
                 ("fem_check_residual", C.c_int32), ("pcg_learned_scale", C.c_int32), ("graphs", C.c_int32),
                 ("beam_kernel", C.c_int32), ("fem_dense_front", C.c_int32), ("force_block", C.c_int32),
-                ("integrate_block", C.c_int32), ("beams_per_sm", C.c_int32), ("tyre_grip", C.c_float)]
+                ("integrate_block", C.c_int32), ("beams_per_sm", C.c_int32), ("tyre_grip", C.c_float),
+                ("bulk_wait_s", C.c_float)]
 
 
 class _FemStats(C.Structure):
@@ -512,6 +515,8 @@ class World:
         cfg.device = device
         cfg.collision_hz = self.settings.collision_hz
         cfg.inter_body_collisions = int(self.settings.inter_body_collisions)
+        if self.settings.max_pairs > 0:
+            cfg.max_pairs = int(self.settings.max_pairs)
         cfg.fem_solver = FEM_SOLVERS[self.settings.fem_solver]
         cfg.pcg_max_iters = int(self.settings.pcg_max_iters)
         cfg.pcg_tol = float(self.settings.pcg_tol)
@@ -521,6 +526,7 @@ class World:
         cfg.beam_kernel = int(self.settings.beam_kernel)
         cfg.fem_dense_front = int(self.settings.fem_dense_front)
         cfg.tyre_grip = float(self.settings.tyre_grip)
+        cfg.bulk_wait_s = float(self.settings.bulk_wait_s)
         tuned = _tuned_shapes()
         for k in ("force_block", "integrate_block", "beams_per_sm"):
             v = getattr(self.settings, k)

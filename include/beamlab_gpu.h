@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define BL_GPU_ABI_VERSION 5
+#define BL_GPU_ABI_VERSION 6
 
 enum {
     BL_GPU_OK = 0,
@@ -98,6 +98,10 @@ typedef struct {
     int32_t integrate_block;   /* the integration kernel's block size: 64, 128 or 256; 0 (default): 256 */
     int32_t beams_per_sm;      /* the beams' persistent kernel's blocks an SM (at most what fits); 0 (default): what fits */
     float tyre_grip;           /* WorldSettings::tyre_grip (1): a factor on the tyres' friction (tyre_contact) */
+    float bulk_wait_s;         /* (no counterpart in the reference) the beams kernel's bound on a wait for its own bulk
+                                  copies, in seconds (default 1, at most 10): one that runs out raises
+                                  BL_GPU_DEVERR_TIMEOUT, lets the copies in flight land and ends the block's work for that
+                                  substep; 0 tests each copy once without waiting (for tests of that path) */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };
@@ -318,8 +322,8 @@ enum {
     BL_GPU_DEVERR_PAIRS = 1 << 2,      /* the contact pair list overflowed bl_gpu_config.max_pairs */
     BL_GPU_DEVERR_ISLAND = 1 << 3,     /* an island with contact pairs held more than BL_GPU_MAX_ISLAND_BODIES bodies */
     BL_GPU_DEVERR_CONTACT_UNSUPPORTED = 1 << 5, /* a body with a FEM frame met another body's triangles (not stepped) */
-    BL_GPU_DEVERR_TIMEOUT = 1 << 6     /* a kernel's bounded wait on its own bulk copies ran out (1 s): the substep's
-                                          beams were not all stepped */
+    BL_GPU_DEVERR_TIMEOUT = 1 << 6     /* a kernel's bounded wait on its own bulk copies ran out (bulk_wait_s): the
+                                          substep's beams were not all stepped */
 };
 #define BL_GPU_MAX_ISLAND_BODIES 256
 #define BL_GPU_MAX_CANDIDATES 64
