@@ -981,8 +981,10 @@ __global__ void k_collide(const float4* __restrict__ nd, const int4* __restrict_
                     for (int q = 0; q < 3; q++) FB[q] = FB[q] - f * wb[q];
             }
         } else {
-            // contact_force<1, 3> (world.cpp:59-92), the node's weight 1
-            const float fric = 0.8f * smin(bn.cfric, bt.cfric);
+            // contact_force<1, 3> (world.cpp:59-92), the node's weight 1; a tyre node grips with its own friction
+            // (world.cpp:3013)
+            const int4 ina = info[ia];
+            const float fric = ((uint32_t)ina.x & NF_TYRE) ? __int_as_float(ina.y) : 0.8f * smin(bn.cfric, bt.cfric);
             float W = 0;
             if (ma) W += 1.0f * 1.0f * Aim;
             if (mb)

@@ -510,18 +510,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 // the generic proxy's reads of a buffer ordered before the async proxy's next writes into it
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// waits for the phase of `parity` to complete; false after limit_ns (limit 0: one non-blocking test)
+// waits for the phase of `parity` to complete; false after limit_ns (limit 0: false at once, the run-out path's test)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long limit_ns = kWaitNs) {
     const uint32_t a = smem_u32(bar);
     uint32_t done = 0;
     unsigned long long t0 = 0;
-    if (limit_ns == 0) {
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(done)
-                     : "r"(a), "r"(parity)
-                     : "memory");
-        return done != 0;
-    }
+    if (limit_ns == 0) return false;
     for (int it = 0;; it++) {
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
                      : "=r"(done)

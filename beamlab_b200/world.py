@@ -77,7 +77,7 @@ class WorldSettings:
     # of the front tree), 1 block columns with the top chain as one dense front, 0 block columns in the reference's order
     fem_dense_front: int = 3
     tyre_grip: float = 1.0                    # WorldSettings::tyre_grip: a factor on the tyres' friction
-    bulk_wait_s: float = 1.0                  # the beams kernel's bound on a wait for its bulk copies (0: test once)
+    bulk_wait_s: float = 1.0                  # the beams kernel's bound on a wait for its bulk copies (0: runs out)
     # launch shapes (None: the tuned ones of beamlab_b200/tuned.json when present, else the library's defaults);
     # results do not depend on them
     force_block: int | None = None

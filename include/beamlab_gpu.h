@@ -101,7 +101,7 @@ typedef struct {
     float bulk_wait_s;         /* (no counterpart in the reference) the beams kernel's bound on a wait for its own bulk
                                   copies, in seconds (default 1, at most 10): one that runs out raises
                                   BL_GPU_DEVERR_TIMEOUT, lets the copies in flight land and ends the block's work for that
-                                  substep; 0 tests each copy once without waiting (for tests of that path) */
+                                  substep; 0 makes every such wait report as run out (for tests of that path) */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };

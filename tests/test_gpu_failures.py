@@ -1,6 +1,6 @@
 """The failure paths, made to happen without faulting the GPU:
 
-* the beams kernel's bounded wait on its own bulk copies, set to test each copy once (bulk_wait_s = 0), runs out:
+* the beams kernel's bounded wait on its own bulk copies, set to run out at once (bulk_wait_s = 0):
   BL_GPU_DEVERR_TIMEOUT is raised, the copies in flight land, and the device stays usable (a world stepped next on it
   is bitwise the oracle's);
 * a contact pair list too small for an island's pairs (max_pairs): BL_GPU_DEVERR_PAIRS, and the island's contacts are
