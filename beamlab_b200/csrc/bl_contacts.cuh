@@ -909,16 +909,286 @@ __global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, c
 }
 
 // ------------------------------------------------------------------------------------------ response (each substep)
-// World::collide_pairs for node-triangle pairs (world.cpp:2975-3023): one thread an island, its pairs in order;
-// contact_force<1, 3> and hull_push_out<3> (world.cpp:59-120) on the nodes' forces so far (Fs); the concrete ground
-// model.
-__global__ void k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, int nbodies, Contacts C,
-                          float4* __restrict__ Fs) {
-    const int root = blockIdx.x * blockDim.x + threadIdx.x;
+// World::collide_pairs for node-triangle pairs (world.cpp:2975-3023): each contact cancels the forces accumulated so far
+// on its node and its triangle's corners (earlier contacts' included), so an island's contacts run one after another
+// in pair order, as the reference's loop (world.cpp:2999). A CTA an island:
+//  1. its contacts' nodes hashed into shared-memory slots and their forces loaded there (all threads);
+//  2. in chunks of the island's contacts (its pairs with a hit, in pair order, gathered by a block scan), each
+//     contact's record - its slots, the accumulation weights, relative velocity and normal, and every
+//     term of the contact law that does not depend on the forces (the slip direction and speed, the Stribeck
+//     exponentials, the restitution term) - formed in parallel;
+//  3. one thread runs the chain: per contact only the force-dependent arithmetic, on shared memory, with the
+//     reference's operations in its order (contact_force<1, 3> / hull_push_out<3> and primitive_collision,
+//     world.cpp:59-120, static_world.cpp:8-51, split at their force-independent parts);
+//  4. the forces written back. An island with more distinct contact nodes than the slots hold runs the loop on global
+//     memory (collide_island_global). Results are the same bits either way.
+__device__ void collide_island_global(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Contacts C,
+                                      float4* __restrict__ Fs, int root, int off, int cnt);
+
+constexpr int kCollideThreads = 256;
+constexpr int kSlotBits = 13, kSlots = 1 << kSlotBits; // force slots (distinct contact nodes an island)
+constexpr int kRecChunk = 512;                          // contact records formed at a time
+
+struct ContactRec {
+    int sa, sb[3];        // force slots of the node and the triangle's corners
+    float ca, cb[3];      // acc = FA ca - sum FB_q cb_q (the terms the movable sides have)
+    float wb[3], m;       // barycentric weights; effective mass
+    float nx, ny, nz;     // the normal passed to the law (negated where the node's side is immovable)
+    float vx, vy, vz;     // the relative velocity passed to the law
+    float pen, fric;
+    float Vn, rsub;       // vel . normal; the restitution / push term of R where Vn < 0 (else 0); hull: (target - vr) m / dt
+    float sx, sy, sz;     // the slip direction (0 where the slip speed is below 1e-9)
+    float sv, stop;       // the slip speed; mass sv / dt
+    float e1, gsum;       // 1 - exp(-sv / va); the dynamic friction's g + min(t2 sv, 5)
+    int kind;             // 0 none, 1 contact (node movable), 2 contact (node immovable), 3 hull push-out; | ma << 4 | mb << 5
+};
+
+__device__ __forceinline__ int slot_hash(int key) { return (int)(((uint32_t)key * 2654435761u) >> (32 - kSlotBits)); }
+__device__ __forceinline__ int slot_find(const int* keys, int key) {
+    int h = slot_hash(key);
+    while (keys[h] != key) h = (h + 1) & (kSlots - 1);
+    return h;
+}
+
+__global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies,
+                                                            int nbodies, Contacts C, float4* __restrict__ Fs) {
+    extern __shared__ __align__(16) unsigned char csm[];
+    int* keys = reinterpret_cast<int*>(csm);
+    float* fx = reinterpret_cast<float*>(keys + kSlots);
+    float* fy = fx + kSlots;
+    float* fz = fy + kSlots;
+    ContactRec* rec = reinterpret_cast<ContactRec*>(fz + kSlots);
+    __shared__ int used, overflow, ncontacts;
+    const int root = blockIdx.x, tid = threadIdx.x;
     if (root >= nbodies) return;
     const int cnt = C.isl_pcnt[root];
     if (cnt <= 0 || bodies[root].island != root || !bodies[root].pairs) return;
     const int off = C.isl_poff[root];
+    const float dt = C.dt;
+    const GroundModel& gm = c_ground[3]; // SURF_CONCRETE
+    for (int h = tid; h < kSlots; h += kCollideThreads) keys[h] = -1;
+    if (tid == 0) used = 0, overflow = 0, ncontacts = 0;
+    __syncthreads();
+    // 1. the contacts' nodes into slots
+    for (int i = off + tid; i < off + cnt; i += kCollideThreads) {
+        if (C.hit_b[i].w == 0.0f) continue;
+        const int2 pr = C.pairs[i];
+        const int4 tr = C.tri[pr.y];
+        const int nodes[4] = {pr.x, tr.x, tr.y, tr.z};
+        for (int q = 0; q < 4; q++) {
+            int h = slot_hash(nodes[q]);
+            for (int probe = 0;; probe++) {
+                if (probe >= kSlots / 2 || overflow) {
+                    overflow = 1;
+                    break;
+                }
+                const int prev = atomicCAS(&keys[h], -1, nodes[q]);
+                if (prev == -1) {
+                    if (atomicAdd(&used, 1) >= kSlots / 2) overflow = 1; // (kept at most half full: short probes)
+                    break;
+                }
+                if (prev == nodes[q]) break;
+                h = (h + 1) & (kSlots - 1);
+            }
+        }
+    }
+    __syncthreads();
+    if (overflow) {
+        if (tid == 0) collide_island_global(nd, info, bodies, C, Fs, root, off, cnt);
+        return;
+    }
+    for (int h = tid; h < kSlots; h += kCollideThreads)
+        if (keys[h] >= 0) {
+            const float4 f = Fs[keys[h]];
+            fx[h] = f.x, fy[h] = f.y, fz[h] = f.z;
+        }
+    // the island's contacts (pairs with a hit), in pair order, kRecChunk at a time: a block scan places each
+    __shared__ int hl[kRecChunk], wsum[kCollideThreads / 32], nhl;
+    int next = off;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) nhl = 0;
+        __syncthreads();
+        while (next < off + cnt && nhl + kCollideThreads <= kRecChunk) {
+            const int i = next + tid;
+            const bool hit = i < off + cnt && C.hit_b[i].w != 0.0f;
+            const unsigned bal = __ballot_sync(0xffffffffu, hit);
+            if ((tid & 31) == 0) wsum[tid >> 5] = __popc(bal);
+            __syncthreads();
+            int before = nhl;
+            for (int wq = 0; wq < (tid >> 5); wq++) before += wsum[wq];
+            if (hit) hl[before + __popc(bal & ((1u << (tid & 31)) - 1u))] = i;
+            __syncthreads();
+            if (tid == 0)
+                for (int wq = 0; wq < kCollideThreads / 32; wq++) nhl += wsum[wq];
+            next += kCollideThreads;
+            __syncthreads();
+        }
+        const int nh = nhl;
+        if (nh == 0) break;
+        // 2. the records of these contacts
+        for (int r = tid; r < nh; r += kCollideThreads) {
+            const int i = hl[r];
+            ContactRec& R = rec[r];
+            R.kind = 0;
+            const float4 hb4 = C.hit_b[i];
+            const float4 ha = C.hit_a[i];
+            const int2 pr = C.pairs[i];
+            const int4 tr = C.tri[pr.y];
+            Body& bn = bodies[info[pr.x].w];
+            Body& bt = bodies[tr.w >> 8];
+            // movable (world.cpp:2983-2993): a sleeping side is immovable and asks to wake when the other moves
+            bool ma = true, mb = true;
+            if (bn.sleeping) {
+                if (sqrtf(bt.acc_v2) > smax(C.wake_speed, bt.sleep_speed) * 1.0f) bn.wake_request = 1;
+                ma = false;
+            }
+            if (bt.sleeping) {
+                if (sqrtf(bn.acc_v2) > smax(C.wake_speed, bn.sleep_speed) * 1.0f) bt.wake_request = 1;
+                mb = false;
+            }
+            const int ia = pr.x, ib[3] = {tr.x, tr.y, tr.z};
+            const float wb[3] = {ha.x, ha.y, ha.z};
+            const v3 n = V(hb4.x, hb4.y, hb4.z);
+            const float pen = ha.w;
+            const float4 pa = nd[2 * ia], va4 = nd[2 * ia + 1];
+            const v3 Av = V(va4.x, va4.y, va4.z);
+            const float Aim = pa.w;
+            v3 Bv[3];
+            float Bim[3];
+            for (int q = 0; q < 3; q++) {
+                const float4 pq = nd[2 * ib[q]], vq = nd[2 * ib[q] + 1];
+                Bv[q] = V(vq.x, vq.y, vq.z), Bim[q] = pq.w;
+            }
+            R.sa = slot_find(keys, ia);
+            for (int q = 0; q < 3; q++) R.sb[q] = slot_find(keys, ib[q]), R.wb[q] = wb[q], R.cb[q] = wb[q] * Bim[q];
+            const int mv = (ma ? 16 : 0) | (mb ? 32 : 0);
+            if (!(tr.w & TF_TWO_SIDED) && pen > bn.crad) {
+                // hull_push_out<3> (world.cpp:97-118): behind a hull's face
+                float W = ma ? Aim : 0.0f;
+                if (mb)
+                    for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
+                if (W <= 1e-12f) continue;
+                v3 vb = V(0, 0, 0);
+                for (int q = 0; q < 3; q++) vb = vb + Bv[q] * wb[q];
+                const float m = 1.0f / W, vr = dot(Av - vb, n), target = smin(0.2f * pen / dt, 2.0f);
+                R.ca = Aim, R.m = m, R.nx = n.x, R.ny = n.y, R.nz = n.z;
+                R.rsub = (target - vr) * m / dt;
+                R.kind = 3 | mv;
+            } else {
+                // contact_force<1, 3> (world.cpp:59-92), the node's weight 1; a tyre node grips with its own friction
+                // (world.cpp:3013)
+                const int4 ina = info[ia];
+                const float fric = ((uint32_t)ina.x & NF_TYRE) ? __int_as_float(ina.y) : 0.8f * smin(bn.cfric, bt.cfric);
+                float W = 0;
+                if (ma) W += 1.0f * 1.0f * Aim;
+                if (mb)
+                    for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
+                if (W <= 1e-12f) continue;
+                const float m = 1.0f / W;
+                v3 va = V(0, 0, 0), vb = V(0, 0, 0);
+                va = va + Av * 1.0f;
+                for (int q = 0; q < 3; q++) vb = vb + Bv[q] * wb[q];
+                const v3 vel = ma ? va - vb : vb - va, nrm = ma ? n : neg(n);
+                R.ca = 1.0f * Aim, R.m = m, R.fric = fric, R.pen = pen;
+                R.nx = nrm.x, R.ny = nrm.y, R.nz = nrm.z, R.vx = vel.x, R.vy = vel.y, R.vz = vel.z;
+                // primitive_collision's force-independent terms (static_world.cpp:8-51; push_max 2, slop 0, no
+                // restitution)
+                const float Vn = dot(vel, nrm), sgl = gm.soft_depth;
+                R.Vn = Vn;
+                R.rsub = Vn < 0 ? (0.8f * Vn - smin(0.2f * smax(0.0f, pen - sgl - 0.0f) / dt, 2.0f)) * m / dt : 0.0f;
+                v3 slip = vel - nrm * Vn;
+                const float sv = length(slip);
+                if (sv > 1e-9f) slip = divs(slip, sv);
+                else slip = V(0, 0, 0);
+                R.sx = slip.x, R.sy = slip.y, R.sz = slip.z, R.sv = sv, R.stop = m * sv / dt;
+                R.e1 = 1.0f - bl_expf(-sv / gm.va);
+                const float g = gm.mc + (gm.ms - gm.mc) * bl_expf(-bl_powf(sv / gm.vs, gm.alpha));
+                R.gsum = g + smin(gm.t2 * sv, 5.0f);
+                R.kind = (ma ? 1 : 2) | mv;
+            }
+            atomicAdd(&ncontacts, 1);
+            atomicAdd(&bn.body_contacts, 1);
+            atomicAdd(&bt.body_contacts, 1);
+        }
+        __syncthreads();
+        // 3. the chain
+        if (tid == 0) {
+            for (int r = 0; r < nh; r++) {
+                const ContactRec& R = rec[r];
+                const int kind = R.kind & 15;
+                if (kind == 0) continue;
+                const bool ma = R.kind & 16, mb = R.kind & 32;
+                v3 FA = V(fx[R.sa], fy[R.sa], fz[R.sa]);
+                v3 FB[3];
+                for (int q = 0; q < 3; q++) FB[q] = V(fx[R.sb[q]], fy[R.sb[q]], fz[R.sb[q]]);
+                v3 acc = V(0, 0, 0);
+                if (ma) acc = acc + FA * R.ca;
+                for (int q = 0; q < 3; q++)
+                    if (mb) acc = acc - FB[q] * R.cb[q];
+                const v3 nrm = V(R.nx, R.ny, R.nz);
+                if (kind == 3) {
+                    const float fn = R.rsub - dot(acc, nrm) * R.m;
+                    if (fn > 0) {
+                        const v3 f = nrm * fn;
+                        if (ma) FA = FA + f;
+                        if (mb)
+                            for (int q = 0; q < 3; q++) FB[q] = FB[q] - f * R.wb[q];
+                    }
+                } else {
+                    const v3 f_rel = acc * R.m;
+                    const v3 F = kind == 1 ? f_rel : neg(f_rel);
+                    const v3 vel = V(R.vx, R.vy, R.vz);
+                    // primitive_collision (static_world.cpp:8-51) with its force-independent terms from the record
+                    v3 out = V(0, 0, 0);
+                    const float Vn = R.Vn, Fn = dot(F, nrm), sgl = gm.soft_depth, pen = R.pen;
+                    if (sgl > 0 && pen >= 0) {
+                        out = out + vel * (-gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f));
+                        float Fb = gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f;
+                        if (Vn >= 0 && Fn < 0 && Fb > -Fn) Fb = -Fn;
+                        out = out + nrm * Fb;
+                    }
+                    if (pen >= sgl) {
+                        float Rn = -Fn;
+                        if (Vn < 0) Rn -= R.rsub;
+                        if (Rn > 0) {
+                            const v3 slipF = F - nrm * Fn;
+                            const v3 slip = V(R.sx, R.sy, R.sz);
+                            const float G = Rn * gm.strength * R.fric;
+                            if (R.sv < gm.va && G > 0 && length(slipF) <= gm.ms * G)
+                                out = out + (nrm * Rn - slip * smin(gm.ms * G * R.e1, R.stop) - slipF);
+                            else
+                                out = out + (nrm * Rn - slip * smin(R.gsum * G, smax(0.0f, R.stop + dot(slipF, slip))));
+                        }
+                    }
+                    if (kind == 2) {
+                        for (int q = 0; q < 3; q++) FB[q] = FB[q] + out * R.wb[q];
+                    } else {
+                        FA = FA + out * 1.0f;
+                        if (mb)
+                            for (int q = 0; q < 3; q++) FB[q] = FB[q] - out * R.wb[q];
+                    }
+                }
+                fx[R.sa] = FA.x, fy[R.sa] = FA.y, fz[R.sa] = FA.z;
+                for (int q = 0; q < 3; q++) fx[R.sb[q]] = FB[q].x, fy[R.sb[q]] = FB[q].y, fz[R.sb[q]] = FB[q].z;
+            }
+        }
+    }
+    __syncthreads();
+    // 4. the forces back
+    for (int h = tid; h < kSlots; h += kCollideThreads)
+        if (keys[h] >= 0) Fs[keys[h]] = make_float4(fx[h], fy[h], fz[h], 0.0f);
+    if (tid == 0) {
+        C.isl_contacts[root] += ncontacts;
+        if (ncontacts) atomicAdd(&C.counters[1], ncontacts);
+    }
+}
+
+constexpr size_t kCollideSmem = sizeof(int) * kSlots + 3 * sizeof(float) * kSlots + sizeof(ContactRec) * kRecChunk;
+
+// The serial loop on global memory (the path of an island with more distinct contact nodes than the slots hold)
+__device__ void collide_island_global(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Contacts C,
+                                      float4* __restrict__ Fs, int root, int off, int cnt) {
     const float dt = C.dt;
     const GroundModel& gm = c_ground[3]; // SURF_CONCRETE
     int contacts = 0;

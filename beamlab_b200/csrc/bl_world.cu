@@ -1006,6 +1006,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
         BL_CUDA(c, d->alloc(B));
     BL_CUDA(c, c->pair_total.alloc(1));
     BL_CUDA(c, c->counters.alloc(4));
+    BL_CUDA(c, cudaFuncSetAttribute(k_collide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCollideSmem));
     BL_CUDA(c, c->pairs.alloc(c->cfg.max_pairs));
     BL_CUDA(c, c->hit_a.alloc(c->cfg.max_pairs));
     BL_CUDA(c, c->hit_b.alloc(c->cfg.max_pairs));
@@ -1497,7 +1498,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
         if (c->contacts_on) {
             // contacts between bodies on the forces so far (World::collide_pairs, before the static contacts)
             k_detect<<<148 * 4, 256, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, CT);
-            k_collide<<<(c->B + 127) / 128, 128, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
+            k_collide<<<c->B, kCollideThreads, kCollideSmem, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->B, CT, c->nodef.p);
         }
         mark();
         k_integrate<<<std::max(gin, 1), ib, 0, s>>>(c->nd.p, c->info.p, c->dbodies.p, c->st, dt, c->N, k == 0 ? 1 : 0, c->nodef.p, wh);
