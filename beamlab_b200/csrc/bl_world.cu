@@ -1464,6 +1464,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
                 k_rebuild<<<c->B, 1024, sizeof(RebuildShared), s>>>(c->dbodies.p, c->B, c->nd.p, c->info.p, CT, k == 0 ? 1 : 0, c->deverr.p);
             }
         }
+        mark();
         if (c->any_drag) k_drag_parts<<<(c->B + 63) / 64, 64, 0, s>>>(c->dbodies.p, c->B, c->nd.p, c->ab.p, c->bmeta.p, dg);
         if (c->NF > 0) k_fem_begin<<<(c->NF + tb - 1) / tb, tb, 0, s>>>(F, c->nd.p);
         if (c->beam_grid > 0) {
@@ -2428,7 +2429,7 @@ int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profil
     auto it = c->pgraphs.find(n);
     if (it == c->pgraphs.end()) {
         ProfGraph pg;
-        pg.events.resize(5 * (size_t)n + 4);
+        pg.events.resize(6 * (size_t)n + 4);
         for (cudaEvent_t& e : pg.events) BL_CUDA(c, cudaEventCreate(&e));
         cudaGraph_t g = nullptr;
         BL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -2455,13 +2456,14 @@ int bl_gpu_profile_frame(bl_gpu_ctx* c, int32_t n, void* stream, bl_frame_profil
     };
     out->begin_ms = el(0, 1);
     for (int k = 0; k < n; k++) {
-        const int b = 1 + 5 * k;
-        out->beams_ms += el(b, b + 1), out->force_ms += el(b + 1, b + 2), out->contacts_ms += el(b + 2, b + 3);
-        out->integrate_ms += el(b + 3, b + 4), out->fem_ms += el(b + 4, b + 5);
+        const int b = 1 + 6 * k;
+        out->search_ms += el(b, b + 1);
+        out->beams_ms += el(b + 1, b + 2), out->force_ms += el(b + 2, b + 3), out->contacts_ms += el(b + 3, b + 4);
+        out->integrate_ms += el(b + 4, b + 5), out->fem_ms += el(b + 5, b + 6);
     }
     out->nodes_ms = out->force_ms + out->contacts_ms + out->integrate_ms + out->fem_ms;
-    out->finish_ms = el(1 + 5 * n, 3 + 5 * n);
-    out->frame_ms = el(0, 3 + 5 * n);
+    out->finish_ms = el(1 + 6 * n, 3 + 6 * n);
+    out->frame_ms = el(0, 3 + 6 * n);
     BL_CUDA(c, terr);
     return BL_GPU_OK;
 }

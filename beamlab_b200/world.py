@@ -370,7 +370,7 @@ class _WorldStats(C.Structure):
 class _FrameProfile(C.Structure):
     _fields_ = [("substeps", C.c_int32), ("frame_ms", C.c_float), ("begin_ms", C.c_float), ("beams_ms", C.c_float),
                 ("nodes_ms", C.c_float), ("finish_ms", C.c_float), ("force_ms", C.c_float), ("contacts_ms", C.c_float),
-                ("integrate_ms", C.c_float), ("fem_ms", C.c_float)]
+                ("integrate_ms", C.c_float), ("fem_ms", C.c_float), ("search_ms", C.c_float)]
 
 
 class _Config(C.Structure):

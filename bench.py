@@ -311,14 +311,20 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     from beamlab_b200 import NODE_DTYPE, world_from_rig
     rig, n, m, desc = workload(args.workload, rank)
+    # two worlds of the same rig: `w` for the resident measurement, `we` for the end-to-end one; both are warmed up by
+    # the same W frames, so the two measurements time the same K frames of the same simulation (in a crash the work
+    # changes from frame to frame)
     w = world_from_rig(rig, device=local)
+    we = world_from_rig(rig, device=local)
     stream = torch.cuda.Stream()
     K, W = args.steps, args.warmup
 
     # warm-up: every graph used below is captured here (plain frames, the profiled frame)
     for _ in range(max(W - 1, 0)):
         w.step_substeps(FRAME, stream)
+        we.step_substeps(FRAME, stream)
     w.profile_frame(FRAME, stream)
+    we.step_substeps(FRAME, stream)
     torch.cuda.synchronize()
     st0 = w.stats()
 
@@ -348,21 +354,17 @@ def run_gpu(args):
     # ---- end to end through the C ABI: the node state in from pinned host memory and out again every frame
     host = torch.empty(n * NODE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
     hbuf = np.frombuffer(host.numpy(), dtype=NODE_DTYPE)
-    w.download_all_nodes(hbuf, stream)
+    we.download_all_nodes(hbuf, stream)
     stream.synchronize()
-    for _ in range(2):
-        w.upload_all_nodes(hbuf, stream)
-        w.step_substeps(FRAME, stream)
-        w.download_all_nodes(hbuf, stream)
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(K):
-        w.upload_all_nodes(hbuf, stream)
-        w.step_substeps(FRAME, stream)
-        w.download_all_nodes(hbuf, stream)
+        we.upload_all_nodes(hbuf, stream)
+        we.step_substeps(FRAME, stream)
+        we.download_all_nodes(hbuf, stream)
     f1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = f0.elapsed_time(f1)
@@ -373,7 +375,7 @@ def run_gpu(args):
         value = total_nodes * FRAME * K / (ms * 1e-3)
         e2e = total_nodes * FRAME * K / (ms_e2e * 1e-3)
         peak, pk_kind = peaks()
-        per = {k: prof[f"{k}_ms"] / FRAME for k in ("beams", "force", "contacts", "integrate", "fem")}
+        per = {k: prof[f"{k}_ms"] / FRAME for k in ("search", "beams", "force", "contacts", "integrate", "fem")}
         # algorithmic bytes a launch (each array touched once): k_beams 40 B a beam; k_force reads a node's position
         # and mass and writes its force (32 B a node; the beams' scalars and the neighbours' positions it gathers are
         # the scratch and the L2-resident gathers of the substep); k_integrate reads p, v, 1/m, the force (44 B) and
@@ -411,7 +413,7 @@ def run_gpu(args):
             "config": {"workload": desc, "frame_substeps": FRAME, "step": f"one frame of {FRAME} substeps",
                        "l2": "inputs larger than L2 (the fleet's device state is about 0.8 GB)",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "kernel_ms_per_substep": {"k_beams": per["beams"], "k_force": per["force"],
+                       "kernel_ms_per_substep": {"pair_search": per["search"], "k_beams": per["beams"], "k_force": per["force"],
                                                  "contacts": per["contacts"], "k_integrate": per["integrate"],
                                                  "fem": per["fem"],
                                                  "frame_begin_finish": (prof["begin_ms"] + prof["finish_ms"]) / FRAME}},
@@ -427,6 +429,18 @@ def run_gpu(args):
         }
         if fem_info is not None:
             out["fem_step"] = fem_info
+        if st1["contacts"] > st0["contacts"]:
+            # the contacts between bodies: the narrow phase reads a node and its triangle's three nodes a pair (about
+            # 64 B a pair a substep); the response runs each island's contacts in the reference's order (a serial
+            # chain an island), so it is latency-bound rather than HBM-bound
+            pairs = len(w.pairs())
+            frames_timed = K
+            out["contacts_step"] = {
+                "pairs_last_search": pairs, "contacts_per_substep": (st1["contacts"] - st0["contacts"]) / (frames_timed * FRAME),
+                "ms_per_substep": per["contacts"], "pair_search_ms_per_substep": per["search"],
+                "narrow_phase_bytes_per_substep": 64 * pairs,
+                "achieved_gbs": 64 * pairs / (per["contacts"] * 1e-3) / 1e9 if per["contacts"] > 0 else None,
+                "bound": "latency (serial response per island, pair order)"}
         if ws == 1 and args.workload == "plate64":
             out["fem_solvers"] = fem_solvers(local)
         if ws == 1 and args.workload == "shellcar" and not args.no_solvers:
@@ -445,6 +459,7 @@ def run_gpu(args):
     if ws > 1:
         dist.destroy_process_group()
     w.close()
+    we.close()
 
 
 def main():

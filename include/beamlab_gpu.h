@@ -466,12 +466,13 @@ typedef struct {
     float frame_ms;            /* the whole frame */
     float begin_ms;            /* the frame's start (static candidates per body) */
     float beams_ms;            /* the beams' forces, all substeps */
-    float nodes_ms;            /* force_ms + contacts_ms + integrate_ms + fem_ms */
+    float nodes_ms;            /* force_ms + contacts_ms + integrate_ms + fem_ms (search_ms apart) */
     float finish_ms;           /* the frame's end (bounds, repair, sleep) */
     float force_ms;            /* the nodes' forces (gravity, beams; the FEM frames' gather), all substeps */
     float contacts_ms;         /* the contacts between bodies (narrow phase, response) */
     float integrate_ms;        /* static contacts and integration */
     float fem_ms;              /* the FEM frames' implicit step */
+    float search_ms;           /* the contacts' wake requests and pair searches (World::rebuild_pairs), all substeps */
 } bl_frame_profile;
 int bl_gpu_profile_frame(bl_gpu_ctx* ctx, int32_t n, void* stream, bl_frame_profile* out);
 
