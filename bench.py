@@ -441,7 +441,7 @@ def run_gpu(args):
                 "narrow_phase_bytes_per_substep": 64 * pairs,
                 "achieved_gbs": 64 * pairs / (per["contacts"] * 1e-3) / 1e9 if per["contacts"] > 0 else None,
                 "bound": "latency (serial response per island, pair order)"}
-        if ws == 1 and args.workload == "plate64":
+        if ws == 1 and args.workload == "plate64" and not args.no_solvers:
             out["fem_solvers"] = fem_solvers(local)
         if ws == 1 and args.workload == "shellcar" and not args.no_solvers:
             from beamlab_b200 import rigs as _rigs
