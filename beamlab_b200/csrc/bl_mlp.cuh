@@ -17,6 +17,9 @@
 // zero for its off-diagonal entries (weight 0.01).
 //
 // Parameters, one float vector: W1 (64 x 36, row = output), b1 (64), W2 (64 x 64), b2, W3 (64 x 64), b3, W4 (12 x 64), b4.
+// The forward's four layers run on the tensor cores (mma.sync m16n8k16, BF16 inputs and weights, FP32 accumulation,
+// FP32 bias and ReLU; each layer's input rounded to BF16); the backward (data and weight gradients) runs in FP32 on the
+// BF16-rounded activations the forward used.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -54,32 +57,107 @@ __device__ __forceinline__ float slog(float x) { return x < 0 ? -log1pf(-x / kS0
 __device__ __forceinline__ float islog(float y) { return y < 0 ? -kS0 * expm1f(-y) : kS0 * expm1f(y); }
 
 // ------------------------------------------------------------------------------------------ the network (one sample a lane)
-// activations in shared memory, [feature][kLd]: lane s holds its sample in column s
+constexpr int kKIn = 48;         // the first layer's inputs padded to whole k-steps of 16 (36 features + 12 zeros)
+constexpr int kPadIn = 64 + 8;   // the staged activations' row stride in BF16 (144 B: rows fall in distinct banks)
+constexpr int kOutPad = 16;      // the last layer's outputs padded to two n-tiles of 8
+
+struct MlpTc {
+    __nv_bfloat16 act[kLanes * kPadIn];   // the current layer's input
+    __nv_bfloat16 w[kHid * kPadIn];       // the current layer's weights, nout x nin
+};
+
+// activations in shared memory, [feature][kLd]: lane s holds its sample in column s; the backward's deltas share
+// their storage with the forward's tensor-core staging (live one after the other)
 struct MlpSmem {
     float a0[kIn * kLd];
     float a1[kHid * kLd];
     float a2[kHid * kLd];
     float a3[kHid * kLd];
     float y[kOut * kLd];
-    float d0[kHid * kLd];
-    float d1[kHid * kLd];
+    union {
+        struct {
+            float d0[kHid * kLd];
+            float d1[kHid * kLd];
+        };
+        MlpTc tc;
+    };
 };
 
-__device__ __forceinline__ void dense(const __nv_bfloat16* __restrict__ W, const __nv_bfloat16* __restrict__ b, int nin, int nout, const float* in,
-                                      float* out, int s, bool relu) {
-    for (int o = 0; o < nout; o++) {
-        float acc = __bfloat162float(b[o]);
-        const __nv_bfloat16* wr = W + (size_t)o * nin;
-        for (int i = 0; i < nin; i++) acc += __bfloat162float(wr[i]) * in[i * kLd + s];
-        out[o * kLd + s] = relu ? fmaxf(acc, 0.0f) : acc;
+// ------------------------------------------------------------------------------------------ the layers on the tensor cores
+// One warp runs a layer's 32 samples x nout outputs as mma.sync m16n8k16 tiles (BF16 operands, FP32 accumulation):
+// A = the layer's input, 32 samples x nin, BF16, row-major in shared memory (row stride kPadIn); B = the weights,
+// nout x nin row-major (the "col" operand as it is), BF16 in shared memory. The inputs are rounded to BF16 as they are
+// staged (the activations the next layer reads are the BF16 values); the accumulators, bias and ReLU stay FP32.
+__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ uint32_t lds32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+// out[o * kLd + s] = (relu)(b_o + sum_i W[o][i] act[s][i]) for the 32 samples; the layer's weights (nout x nin from
+// global, zero rows past nout) staged first. nin: a multiple of 16; nout_t: n-tiles of 8.
+__device__ __forceinline__ void dense_tc(const __nv_bfloat16* __restrict__ W, const __nv_bfloat16* __restrict__ b, int nin, int nin_real, int nout,
+                                         int nout_t, MlpTc& T, float* out, bool relu) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    for (int e = lane; e < nout_t * 8 * nin; e += 32) {
+        const int o = e / nin, i = e % nin;
+        T.w[o * kPadIn + i] = (o < nout && i < nin_real) ? W[(size_t)o * nin_real + i] : __float2bfloat16(0.0f);
     }
+    __syncwarp();
+    for (int mt = 0; mt < 2; mt++) {
+        for (int nt = 0; nt < nout_t; nt++) {
+            float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            for (int k0 = 0; k0 < nin; k0 += 16) {
+                const __nv_bfloat16* a_lo = T.act + (16 * mt + g) * kPadIn + k0 + 2 * t;
+                const __nv_bfloat16* a_hi = a_lo + 8 * kPadIn;
+                const uint32_t a[4] = {lds32(a_lo), lds32(a_hi), lds32(a_lo + 8), lds32(a_hi + 8)};
+                const __nv_bfloat16* wp = T.w + (8 * nt + g) * kPadIn + k0 + 2 * t;
+                const uint32_t bb[2] = {lds32(wp), lds32(wp + 8)};
+                mma_bf16(c, a, bb);
+            }
+            // c0, c1: sample 16 mt + g, outputs 8 nt + 2 t, + 1; c2, c3: sample + 8
+            for (int q = 0; q < 4; q++) {
+                const int smp = 16 * mt + g + (q >= 2 ? 8 : 0), o = 8 * nt + 2 * t + (q & 1);
+                if (o < nout) {
+                    const float v = c[q] + __bfloat162float(b[o]);
+                    out[o * kLd + smp] = relu ? fmaxf(v, 0.0f) : v;
+                }
+            }
+        }
+    }
+    __syncwarp();
 }
 
-__device__ void mlp_forward(const MlpDev& M, MlpSmem& S, int s) {
-    dense(M.wb + kOffW1, M.wb + kOffB1, kIn, kHid, S.a0, S.a1, s, true);
-    dense(M.wb + kOffW2, M.wb + kOffB2, kHid, kHid, S.a1, S.a2, s, true);
-    dense(M.wb + kOffW3, M.wb + kOffB3, kHid, kHid, S.a2, S.a3, s, true);
-    dense(M.wb + kOffW4, M.wb + kOffB4, kHid, kOut, S.a3, S.y, s, false);
+// the next layer's input: `in` ([feature][kLd], FP32) as BF16 rows, padded with zeros to nin_pad
+__device__ __forceinline__ void stage_act(const float* in, int nin, int nin_pad, MlpTc& T) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    for (int e = lane; e < kLanes * nin_pad; e += 32) {
+        const int smp = e / nin_pad, i = e % nin_pad;
+        T.act[smp * kPadIn + i] = __float2bfloat16(i < nin ? in[i * kLd + smp] : 0.0f);
+    }
+    __syncwarp();
+}
+
+// The forward of the warp's 32 samples (S.a0 holds their features): a1..a3 and y in S, the BF16-rounded inputs of
+// each layer written back into a0..a3 (what the backward's weight gradients multiply)
+__device__ void mlp_forward(const MlpDev& M, MlpSmem& S, MlpTc& T) {
+    const int lane = threadIdx.x & 31;
+    float* acts[4] = {S.a0, S.a1, S.a2, S.a3};
+    const int nins[4] = {kIn, kHid, kHid, kHid};
+    for (int l = 0; l < 4; l++) {
+        const int nin = nins[l], nin_pad = l == 0 ? kKIn : kHid;
+        stage_act(acts[l], nin, nin_pad, T);
+        for (int e = lane; e < kLanes * nin; e += 32) { // (the layer's input as the tensor cores read it)
+            const int smp = e / nin, i = e % nin;
+            acts[l][i * kLd + smp] = __bfloat162float(T.act[smp * kPadIn + i]);
+        }
+        const int offw[4] = {kOffW1, kOffW2, kOffW3, kOffW4}, offb[4] = {kOffB1, kOffB2, kOffB3, kOffB4};
+        const int nout = l == 3 ? kOut : kHid;
+        dense_tc(M.wb + offw[l], M.wb + offb[l], nin_pad, nin, nout, l == 3 ? kOutPad / 8 : kHid / 8, T, l == 3 ? S.y : acts[l + 1], l < 3);
+    }
+    __syncwarp();
 }
 
 // ------------------------------------------------------------------------------------------ the step's side
@@ -133,12 +211,13 @@ __global__ void k_mlp_features(FemDev F, MlpDev M, const float4* __restrict__ nd
 
 // The network on every frame node's features: the PCG's guess and scale
 __global__ void __launch_bounds__(kLanes) k_mlp_infer(FemDev F, MlpDev M, float* __restrict__ guess, float* __restrict__ gscale) {
-    __shared__ MlpSmem S;
+    __shared__ __align__(16) MlpSmem S;
+    MlpTc& T = S.tc;
     const int s = threadIdx.x;
     const int i = blockIdx.x * kLanes + s;
     const bool on = i < F.nf;
     for (int f = 0; f < kIn; f++) S.a0[f * kLd + s] = on ? M.feat[(size_t)kIn * i + f] : 0.0f;
-    mlp_forward(M, S, s);
+    mlp_forward(M, S, T);
     if (!on) return;
     for (int a = 0; a < 3; a++) guess[3 * i + a] = islog(S.y[a * kLd + s]);
     for (int q = 0; q < 9; q++) gscale[9 * i + q] = ((q % 4) == 0 ? 1.0f : 0.0f) + 0.25f * tanhf(S.y[(3 + q) * kLd + s]);
@@ -218,13 +297,14 @@ __global__ void k_mlp_store_dv(FemDev F, MlpDev M) {
 // over its samples in order (gpart: kParams a block; lpart: the block's loss). Deterministic.
 __global__ void __launch_bounds__(kLanes) k_mlp_grad(MlpDev M, const float* __restrict__ x, const float* __restrict__ t, const float* __restrict__ w,
                                                      const int* __restrict__ idx, int n, float* __restrict__ gpart, float* __restrict__ lpart) {
-    __shared__ MlpSmem S;
+    __shared__ __align__(16) MlpSmem S;
+    MlpTc& T = S.tc;
     const int s = threadIdx.x;
     const int q = blockIdx.x * kLanes + s;
     const bool on = q < n;
     const size_t smp = on ? (size_t)(idx ? idx[q] : q) : 0;
     for (int f = 0; f < kIn; f++) S.a0[f * kLd + s] = on ? x[kIn * smp + f] : 0.0f;
-    mlp_forward(M, S, s);
+    mlp_forward(M, S, T);
     // d4 = w (y - t) / n into y's place; the sample's loss
     float loss = 0.0f;
     const float inv_n = 1.0f / (float)n;
@@ -311,12 +391,13 @@ __global__ void k_mlp_sync_bf16(MlpDev M) {
 
 // The network's outputs for n samples (tests)
 __global__ void __launch_bounds__(kLanes) k_mlp_forward_batch(MlpDev M, const float* __restrict__ x, int n, float* __restrict__ y) {
-    __shared__ MlpSmem S;
+    __shared__ __align__(16) MlpSmem S;
+    MlpTc& T = S.tc;
     const int s = threadIdx.x;
     const int q = blockIdx.x * kLanes + s;
     const bool on = q < n;
     for (int f = 0; f < kIn; f++) S.a0[f * kLd + s] = on ? x[(size_t)kIn * q + f] : 0.0f;
-    mlp_forward(M, S, s);
+    mlp_forward(M, S, T);
     if (on)
         for (int o = 0; o < kOut; o++) y[(size_t)kOut * q + o] = S.y[o * kLd + s];
 }

@@ -2,7 +2,8 @@
 which has no counterpart in the reference) - the checker of the GPU's forward and gradient kernels.
 
 36 -> 64 -> 64 -> 64 -> 12, ReLU, the parameters in one vector (W1 64x36 row = output, b1, W2 64x64, b2, W3 64x64,
-b3, W4 12x64, b4), the forward on the BF16-rounded parameters (as the GPU reads them), accumulation in float64 here.
+b3, W4 12x64, b4), the forward on the BF16-rounded parameters and BF16-rounded layer inputs (as the GPU's tensor cores
+take them), accumulation in float64 here.
 Loss over n samples: sum_s sum_o w_so (y_so - t_so)^2 / (2 n).
 """
 from __future__ import annotations
@@ -32,15 +33,17 @@ def unpack(p: np.ndarray) -> dict:
 
 
 def forward(p: np.ndarray, x: np.ndarray, round_bf16: bool = True):
-    """Outputs and activations of the network on samples x (n x 36), in float64."""
+    """Outputs and activations of the network on samples x (n x 36), in float64. round_bf16: the parameters and each
+    layer's input rounded to BF16, as the GPU's tensor cores take them (the activations returned are those inputs)."""
     q = unpack((bf16(p) if round_bf16 else p).astype(np.float64))
-    a0 = np.asarray(x, np.float64)
+    rnd = (lambda a: bf16(np.asarray(a, np.float32)).astype(np.float64)) if round_bf16 else (lambda a: np.asarray(a, np.float64))
+    a0 = rnd(x)
     z1 = a0 @ q["W1"].T + q["b1"]
-    a1 = np.maximum(z1, 0)
+    a1 = rnd(np.maximum(z1, 0))
     z2 = a1 @ q["W2"].T + q["b2"]
-    a2 = np.maximum(z2, 0)
+    a2 = rnd(np.maximum(z2, 0))
     z3 = a2 @ q["W3"].T + q["b3"]
-    a3 = np.maximum(z3, 0)
+    a3 = rnd(np.maximum(z3, 0))
     y = a3 @ q["W4"].T + q["b4"]
     return y, (a0, a1, a2, a3)
 

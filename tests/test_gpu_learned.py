@@ -21,8 +21,12 @@ def test_mlp_forward_matches_oracle():
     p = w.mlp_weights()
     x = np.random.default_rng(1).normal(0, 1, (257, 36)).astype(np.float32)
     y = w.mlp_forward(x)
-    yo, _ = mo.forward(p, x)  # (the BF16 weights, accumulated in float64)
-    assert np.max(np.abs(y - yo)) <= 1e-5 + 1e-4 * np.max(np.abs(yo))
+    yo, _ = mo.forward(p, x)  # (the BF16 weights and layer inputs, accumulated in float64)
+    err, scale = np.abs(y - yo), np.max(np.abs(yo))
+    # FP32 tensor-core sums against float64 ones: now and then an activation lands on the other side of a BF16
+    # rounding boundary (one BF16 ulp, 2^-8), so the worst entry is held loosely and almost all tightly
+    assert np.max(err) <= 1e-5 + 3e-3 * scale
+    assert np.quantile(err, 0.99) <= 1e-5 + 1e-4 * scale
     w.close()
 
 
@@ -38,8 +42,10 @@ def test_mlp_gradient_matches_oracle_on_two_calls():
     g2, l2 = w.mlp_gradient(x, t, wt)
     assert np.array_equal(g1, g2) and l1 == l2  # (deterministic: sums in a fixed order)
     lo, go = mo.loss_and_grad(p, x, t, wt)
-    assert np.max(np.abs(g1 - go)) <= 1e-4 * np.max(np.abs(go))
-    assert abs(l1 - lo) <= 1e-5 * lo
+    err, scale = np.abs(g1 - go), np.max(np.abs(go))
+    assert np.max(err) <= 3e-3 * scale  # (as the forward: a rare BF16 rounding-boundary flip of an activation)
+    assert np.quantile(err, 0.99) <= 1e-4 * scale
+    assert abs(l1 - lo) <= 1e-3 * lo
     w.close()
 
 
@@ -85,8 +91,10 @@ def test_pcg_fallback_is_the_cholesky():
 
 def test_learned_warm_start_gain():
     """Train the network on the Cholesky's solves of one plate load (200 substeps, 88,200 node samples), then solve
-    200 substeps of another load: the learned start takes fewer CG iterations than the start from zero. (The same
-    measurement, also with the last solution alone as the start, is in the bench line of the plate workload.)"""
+    200 substeps of another load three ways: from zero, from the last solution (the warm start without the network),
+    and from the learned guess (the energy-norm best combination of the network's dv and the last solution). The
+    learned start must beat the start from zero and be no worse than the last solution alone; what it gains over the
+    latter is printed (measured: about nothing - the network adds little beyond the warm start it is given)."""
     rec = plate(seed=1)
     rec.mlp_record(200 * 441)
     for _ in range(10):
@@ -99,7 +107,7 @@ def test_learned_warm_start_gain():
     weights = rec.mlp_weights()
     rec.close()
     iters = {}
-    for solver in ("pcg", "pcg_learned"):
+    for solver in ("pcg", "pcg_previous", "pcg_learned"):
         w = plate(seed=2, fem_solver=solver, pcg_max_iters=3000, fem_check_residual=True)
         if solver == "pcg_learned":
             w.set_mlp_weights(weights)
@@ -109,5 +117,6 @@ def test_learned_warm_start_gain():
         assert st["pcg_fallbacks"] == 0 and st["max_residual"] <= 1.0001e-6
         iters[solver] = st["pcg_iterations"] / st["pcg_solves"]
         w.close()
-    print("mean CG iterations:", iters)
+    print("mean CG iterations:", iters, "learned over previous:", iters["pcg_learned"] / iters["pcg_previous"])
     assert iters["pcg_learned"] < iters["pcg"]
+    assert iters["pcg_learned"] <= 1.02 * iters["pcg_previous"]
