@@ -14,12 +14,12 @@
 // and beams, k_force) before k_integrate takes the static contacts and integrates.
 //
 // The pair search runs on the substeps the reference rebuilds on (the frame's first and every rebuild interval after):
-// one CTA per island (k_rebuild) makes the island's margins and cell size, the partners, the spatial hash of the slow
-// bodies' contacter nodes (cell_hash & mask buckets, each bucket in node order), the triangles' queries, the fast
-// bodies' dense grids and their partners' queries, and keeps the pairs near_pairs keeps - in the reference's order: a
-// count pass, one global range for the island, a write pass. Every substep k_detect finds the contacts of all pairs
-// in parallel and k_collide applies them one island per thread, pair after pair: contact_force cancels the force
-// accumulated so far on both sides, so the order within an island is the reference's.
+// one CTA per island (k_rebuild) sets up the island's search - margins, cell size, partners, the slow bodies' spatial
+// hash, the fast bodies' dense grids - and lists its queries (a triangle against a hash or a grid); the queries of all
+// islands are counted, placed and written by the whole GPU (bl_pair_search.cuh), the pairs near_pairs keeps in the
+// reference's order. Every substep k_detect finds the contacts of all pairs in parallel and k_collide applies them one
+// island per CTA, pair after pair: contact_force cancels the force accumulated so far on both sides, so the order
+// within an island is the reference's.
 #pragma once
 
 #include "bl_kernels.cuh"
@@ -32,6 +32,8 @@ constexpr float kFastSpeed = 8.0f;     // world.cpp:1881
 constexpr float kTornStretch2 = 2.5f * 2.5f; // softbody.h:154
 enum : uint32_t { TF_TWO_SIDED = 1, TF_TORN = 2 };
 enum : uint32_t { DEVERR_PAIRS = 4, DEVERR_ISLAND = 8, DEVERR_CONTACT_UNSUPPORTED = 32 };
+
+struct IslSearch;
 
 struct Contacts {
     int4* tri;                 // a, b, c, flags | body << 8
@@ -59,9 +61,19 @@ struct Contacts {
     int* bk_fill;
     int* bk_items;             // hashed nodes by bucket
     int* run_end;
-    int* g_start;              // fast grids (kGridCells + 1 per island)
+    int* g_start;              // fast grids: each fast body's cells' starts (a pool of cell_cap)
     int* g_fill;
     int* g_items;              // fast grids' nodes, each listed once, in the lowest cell of its travel
+    float4* g_rec;             // ... in the same order: position, reach of its travel (|v| x travel)
+    int* g_hi;                 // ... the highest cell of its travel (x | y << 8 | z << 16)
+    int4* sb_cell;             // slow hash items in bucket order: cell, body
+    float4* sb_pos;            // ... position, node (bits)
+    IslSearch* isl;            // per island with pairs (isl_idx): what its queries read
+    int4* q_group;             // query groups: island (isl_idx), kind | k << 1 | ko << 9, triangles, first query
+    int2* q_chunk;             // chunks of kQueryChunk queries of one group: group, first triangle of the chunk
+    int* q_count;              // per query (a triangle of a group): its pairs, then their running sum over the island
+    int* sc;                   // search counters: [0] queries [1] groups [2] chunks [3] grid cells
+    int q_cap, grp_cap, chunk_cap, cell_cap;
     int* counters;             // [0] pair searches [1] contacts [2] pairs of the searches
     int interval;              // rebuild interval in substeps (world.cpp:1887)
     float dt;
@@ -171,6 +183,19 @@ __device__ int block_scan_excl(int v, int& total, int* s_warp) {
     return before;
 }
 
+// a[0..n) := its inclusive prefix sums, in place, by the whole block: each thread sums a contiguous run, one block scan
+// of the runs' sums, each thread rewrites its run (two block scans' barriers however long the array; the same integers
+// as scanning it 1,024 entries at a time)
+__device__ void block_scan_incl_inplace(int* a, int n, int* s_warp) {
+    const int nt = blockDim.x, per = (n + nt - 1) / nt;
+    const int lo = min(n, (int)threadIdx.x * per), hi = min(n, lo + per);
+    int sum = 0;
+    for (int i = lo; i < hi; i++) sum += a[i];
+    int tot;
+    int run = block_scan_excl(sum, tot, s_warp);
+    for (int i = lo; i < hi; i++) run += a[i], a[i] = run;
+}
+
 // ------------------------------------------------------------------------------------------ islands (once a frame)
 __device__ __forceinline__ int uf_find(volatile int* parent, int x) {
     while (true) {
@@ -269,585 +294,9 @@ __global__ void k_wake(Body* __restrict__ bodies, uint32_t* __restrict__ bmeta) 
 }
 
 // ------------------------------------------------------------------------------------------ the pair search
-struct IslBody {
-    int id;               // global body index
-    float sp;             // max_speed now (the frame's running maximum)
-    float extra;          // extra pair margin of a fast body
-    float bulk;           // bulk speed of a fast body
-    float mn[3], mx[3];   // its bounds now
-    float bmn[3], bmx[3]; // its box grown by the reach (Island::boxes)
-};
-
-struct RebuildShared {
-    IslBody b[kIslMaxBodies];
-    uint32_t partner[kIslMaxBodies][kIslMaxBodies / 32];
-    double term0[1024];
-    double term1[1024];
-    int warp[32];
-    int nb;
-    float rmax, margin, inv_cell, slow_speed, slow_reach, travel;
-    int npts, mask;
-    int count;
-    // the fast grid of the current fast body
-    float g_org[3], g_inv;
-    int g_dim[3];
-    int g_span[3];        // the most cells a node's travel spans along each axis, less one
-};
-
-__device__ __forceinline__ bool same_group(const Body& a, const Body& b) { return a.group != 0 && a.group == b.group; }
-
-__device__ __forceinline__ bool box_hits(const float* mn, const float* mx, v3 qmn, v3 qmx) {
-    return qmn.x <= mx[0] && qmx.x >= mn[0] && qmn.y <= mx[1] && qmx.y >= mn[1] && qmn.z <= mx[2] && qmx.z >= mn[2];
-}
-// near_partner (world.cpp:1955-1962)
-__device__ bool near_partner(const RebuildShared& S, int k, v3 mn, v3 mx) {
-    for (int w = 0; w < kIslMaxBodies / 32; w++) {
-        uint32_t bits = S.partner[k][w];
-        while (bits) {
-            const int o = w * 32 + __ffs(bits) - 1;
-            bits &= bits - 1;
-            if (box_hits(S.b[o].bmn, S.b[o].bmx, mn, mx)) return true;
-        }
-    }
-    return false;
-}
-__device__ __forceinline__ bool has_partner(const RebuildShared& S, int k) {
-    for (int w = 0; w < kIslMaxBodies / 32; w++)
-        if (S.partner[k][w]) return true;
-    return false;
-}
-
-// near_pairs' test of one candidate (world.cpp:2536-2583); T: the reach's time
-__device__ bool near_keep(const float4* __restrict__ nd, const Body& bn, const Body& bt, int node, int4 t, float T) {
-    if (t.w & TF_TORN) return false;
-    const bool two_sided = (t.w & TF_TWO_SIDED) != 0;
-    const v3 xp = nd_p(nd, node), xv = nd_v(nd, node);
-    const v3 ap = nd_p(nd, t.x), bp = nd_p(nd, t.y), cp = nd_p(nd, t.z);
-    const v3 av = nd_v(nd, t.x), bv = nd_v(nd, t.y), cv = nd_v(nd, t.z);
-    v3 bary;
-    const v3 q = closest_on_triangle(xp, ap, bp, cp, bary);
-    const float r0 = bn.crad + (two_sided ? 0.0f : bt.hull_depth);
-    const v3 da = xv - av, db = xv - bv, dc = xv - cv;
-    const float vrel = sqrtf(smax(length2(da), smax(length2(db), length2(dc))));
-    const float reach = r0 + 1.25f * vrel * T + 0.02f;
-    if (length2(xp - q) >= reach * reach) return false;
-    const v3 nn = cross(bp - ap, cp - ap);
-    const float nl = length(nn);
-    if (nl > 1e-12f) {
-        const v3 n0 = divs(nn, nl);
-        const float s0 = dot(n0, xp - ap);
-        if (two_sided || s0 > bn.crad) {
-            const float sg = s0 >= 0 ? 1.0f : -1.0f;
-            const float close = smax(0.0f, smax(-sg * dot(n0, da), smax(-sg * dot(n0, db), -sg * dot(n0, dc))));
-            if (fabsf(s0) - 1.25f * close * T - 0.02f >= bn.crad) return false;
-        }
-    }
-    return true;
-}
-
-__device__ __forceinline__ int cell_of(float v, float inv_cell) { return (int)floorf(v * inv_cell); }
-
-// One triangle of body bt (island slot kt) against the slow bodies' hash (world.cpp:2037-2083), near_pairs' filter
-// applied: counts the pairs, and writes them from `out` when it is given.
-__device__ int slow_query(const RebuildShared& S, const Contacts& C, const Body* __restrict__ bodies, const float4* __restrict__ nd, int kt, int tg,
-                          int bk0, int pt0, float T, int2* out) {
-    const Body& o = bodies[S.b[kt].id];
-    const int4 tr = C.tri[tg];
-    if (tr.w & TF_TORN) return 0;
-    const bool two_sided = (tr.w & TF_TWO_SIDED) != 0;
-    const float depth = two_sided ? 0.0f : o.hull_depth;
-    const float rq = S.rmax + S.margin + S.b[kt].extra + depth;
-    const v3 a = nd_p(nd, tr.x), bb = nd_p(nd, tr.y), c = nd_p(nd, tr.z);
-    const v3 tmn = vmin3(a, vmin3(bb, c)), tmx = vmax3(a, vmax3(bb, c));
-    const v3 vr = V(rq, rq, rq);
-    if (!near_partner(S, kt, tmn - vr, tmx + vr)) return 0;
-    const v3 tn = cross(bb - a, c - a);
-    const float tn2 = dot(tn, tn);
-    const v3 tu = tn2 > 1e-20f ? tn * (1.0f / sqrtf(tn2)) : V(0, 0, 0);
-    const float ic = S.inv_cell;
-    const int x0 = cell_of(tmn.x - rq, ic), x1 = cell_of(tmx.x + rq, ic);
-    const int y0 = cell_of(tmn.y - rq, ic), y1 = cell_of(tmx.y + rq, ic);
-    const int z0 = cell_of(tmn.z - rq, ic), z1 = cell_of(tmx.z + rq, ic);
-    if ((long long)(x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1) > 512) return 0; // degenerate/exploded
-    const int bt = S.b[kt].id;
-    int n = 0;
-    for (int z = z0; z <= z1; z++)
-        for (int y = y0; y <= y1; y++)
-            for (int x = x0; x <= x1; x++) {
-                const int bk = (int)(cell_hash(x, y, z) & (uint32_t)S.mask);
-                const int k1 = C.bk_start[bk0 + bk + 1];
-                for (int k = C.bk_start[bk0 + bk]; k < k1; k++) {
-                    const int pi = C.bk_items[pt0 + k];
-                    const int pb = C.pt_body[pt0 + pi];
-                    if (pb == bt) { // own nodes: skip the whole run
-                        k = C.run_end[pt0 + k] - 1;
-                        continue;
-                    }
-                    const int4 pc = C.pt_cell[pt0 + pi];
-                    if (pc.x != x || pc.y != y || pc.z != z) continue; // hash collision
-                    const int node = C.pt_node[pt0 + pi];
-                    const v3 p = nd_p(nd, node);
-                    if (p.x < tmn.x - rq || p.y < tmn.y - rq || p.z < tmn.z - rq || p.x > tmx.x + rq || p.y > tmx.y + rq || p.z > tmx.z + rq) continue;
-                    const Body& b = bodies[pb];
-                    if (same_group(b, o)) continue;
-                    if (b.sleeping && o.sleeping) continue;
-                    const float r = b.crad + S.margin + S.b[kt].extra;
-                    const float rb = r + depth;
-                    if (p.x < tmn.x - rb || p.y < tmn.y - rb || p.z < tmn.z - rb || p.x > tmx.x + rb || p.y > tmx.y + rb || p.z > tmx.z + rb) continue;
-                    if (!near_triangle(p, a, bb, c, tu, r, two_sided, depth)) continue;
-                    if (!near_keep(nd, b, o, node, tr, T)) continue;
-                    if (out) out[n] = make_int2(node, tg);
-                    n++;
-                }
-            }
-    return n;
-}
-
-// The fast body's grid cell of p (World::fast_pairs' cell_index, world.cpp:2341-2346), per axis
-__device__ __forceinline__ int3 grid_cell(const RebuildShared& S, v3 p) {
-    const int x = min(max((int)((p.x - S.g_org[0]) * S.g_inv), 0), S.g_dim[0] - 1);
-    const int y = min(max((int)((p.y - S.g_org[1]) * S.g_inv), 0), S.g_dim[1] - 1);
-    const int z = min(max((int)((p.z - S.g_org[2]) * S.g_inv), 0), S.g_dim[2] - 1);
-    return make_int3(x, y, z);
-}
-// the cells a node of the fast body is listed in: those within its own travel (world.cpp:2350-2362), as a box of cells
-__device__ __forceinline__ void node_cells(const RebuildShared& S, const float4* __restrict__ nd, int node, int3& lo, int3& hi) {
-    const v3 p = nd_p(nd, node);
-    const float m = length(nd_v(nd, node)) * S.travel;
-    const v3 vm = V(m, m, m);
-    lo = grid_cell(S, p - vm);
-    hi = grid_cell(S, p + vm);
-}
-
-// One triangle of partner body `ko` against fast body `kf`'s grid (world.cpp:2394-2475), near_pairs' filter applied;
-// the pairs come out in node order (the reference sorts and deduplicates the cells' lists; here a node listed in
-// several cells of the scan is taken in the first of them, and the triangle's pairs are sorted after).
-__device__ int fast_query(const RebuildShared& S, const Contacts& C, const Body* __restrict__ bodies, const float4* __restrict__ nd, int kf, int ko,
-                          int tg, int gs0, int gi0, float fast_extra_o, float T, int2* out) {
-    const Body& F = bodies[S.b[kf].id];
-    const Body& o = bodies[S.b[ko].id];
-    const int4 tr = C.tri[tg];
-    if (tr.w & TF_TORN) return 0;
-    const bool o_fast = S.b[ko].extra > 0;
-    const float r = F.crad + S.slow_reach + S.travel * (S.b[kf].sp + (o_fast ? S.b[ko].sp : 0.0f)) + fast_extra_o;
-    const v3 fmn = V(S.b[kf].mn[0] - r, S.b[kf].mn[1] - r, S.b[kf].mn[2] - r), fmx = V(S.b[kf].mx[0] + r, S.b[kf].mx[1] + r, S.b[kf].mx[2] + r);
-    const v3 a = nd_p(nd, tr.x), bb = nd_p(nd, tr.y), c = nd_p(nd, tr.z);
-    const v3 tmn = vmin3(a, vmin3(bb, c)), tmx = vmax3(a, vmax3(bb, c));
-    if (tmx.x < fmn.x || tmx.y < fmn.y || tmx.z < fmn.z || tmn.x > fmx.x || tmn.y > fmx.y || tmn.z > fmx.z) return 0;
-    const float r00 = F.crad + (o_fast ? 0.01f : S.slow_reach);
-    const float rt = o_fast ? r00 + S.travel * sqrtf(smax(length2(nd_v(nd, tr.x)), smax(length2(nd_v(nd, tr.y)), length2(nd_v(nd, tr.z))))) : r00;
-    const bool two_sided = (tr.w & TF_TWO_SIDED) != 0;
-    const float depth = two_sided ? 0.0f : o.hull_depth;
-    const v3 tn = cross(bb - a, c - a);
-    const float tn2 = dot(tn, tn);
-    const v3 tu = tn2 > 1e-20f ? tn * (1.0f / sqrtf(tn2)) : V(0, 0, 0);
-    const float rr = rt + depth;
-    const v3 mn = tmn - V(rr, rr, rr), mx = tmx + V(rr, rr, rr);
-    const int x0 = max(0, (int)floorf((mn.x - S.g_org[0]) * S.g_inv)), x1 = min(S.g_dim[0] - 1, (int)((mx.x - S.g_org[0]) * S.g_inv));
-    const int y0 = max(0, (int)floorf((mn.y - S.g_org[1]) * S.g_inv)), y1 = min(S.g_dim[1] - 1, (int)((mx.y - S.g_org[1]) * S.g_inv));
-    const int z0 = max(0, (int)floorf((mn.z - S.g_org[2]) * S.g_inv)), z1 = min(S.g_dim[2] - 1, (int)((mx.z - S.g_org[2]) * S.g_inv));
-    if (x0 > x1 || y0 > y1 || z0 > z1) return 0;
-    // The reference lists a node in every cell of its travel and scans the cells of the box: a node is found when its
-    // cells' box meets the scan's box. Here each node is listed once, in its lowest cell: the scan starts g_span
-    // cells lower and keeps the nodes whose box reaches the scan's box - each found once, as after the reference's
-    // sort and deduplication.
-    int n = 0;
-    for (int z = max(0, z0 - S.g_span[2]); z <= z1; z++)
-        for (int y = max(0, y0 - S.g_span[1]); y <= y1; y++)
-            for (int x = max(0, x0 - S.g_span[0]); x <= x1; x++) {
-                const int cell = (z * S.g_dim[1] + y) * S.g_dim[0] + x;
-                const int k0 = C.g_start[gs0 + cell], k1 = C.g_start[gs0 + cell + 1];
-                for (int k = k0; k < k1; k++) {
-                    const int ni = C.g_items[gi0 + k];
-                    int3 lo, hi;
-                    node_cells(S, nd, ni, lo, hi);
-                    if (hi.x < x0 || hi.y < y0 || hi.z < z0) continue;
-                    const v3 p = nd_p(nd, ni);
-                    const float rn = rt + length(nd_v(nd, ni)) * S.travel, rb = rn + depth;
-                    if (p.x < tmn.x - rb || p.y < tmn.y - rb || p.z < tmn.z - rb || p.x > tmx.x + rb || p.y > tmx.y + rb || p.z > tmx.z + rb) continue;
-                    if (!near_triangle(p, a, bb, c, tu, rn, two_sided, depth)) continue;
-                    if (!near_keep(nd, F, o, ni, tr, T)) continue;
-                    if (out) out[n] = make_int2(ni, tg);
-                    n++;
-                }
-            }
-    if (out)
-        for (int i = 1; i < n; i++) { // (by node: the order of the reference's sorted scan)
-            const int2 v = out[i];
-            int j = i - 1;
-            while (j >= 0 && out[j].x > v.x) out[j + 1] = out[j], j--;
-            out[j + 1] = v;
-        }
-    return n;
-}
-
-// acc += s_t[0] + s_t[1] + ... one after another, as the reference's loop adds them
-__device__ __forceinline__ void serial_add(double& acc, const double* s_t, int n) {
-    for (int i = 0; i < n; i++) acc += s_t[i];
-}
-
-// World::rebuild_pairs + near_pairs for one island with pairs (its first body = blockIdx.x); s0: the frame's first
-// substep (the bodies' bounds are the frame's, their top speeds are measured now: world.cpp:3216-3222).
-__global__ void __launch_bounds__(1024) k_rebuild(Body* __restrict__ bodies, int nbodies, const float4* __restrict__ nd, const int4* __restrict__ info,
-                                                  Contacts C, int s0, uint32_t* __restrict__ deverr) {
-    const int root = blockIdx.x;
-    if (root >= nbodies) return;
-    {
-        const Body& R = bodies[root];
-        if (!R.pairs || R.island != root) return;
-    }
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    RebuildShared& S = *reinterpret_cast<RebuildShared*>(smem_raw);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    if (tid == 0) S.nb = 0;
-    for (int w = tid; w < kIslMaxBodies * (kIslMaxBodies / 32); w += nt) (&S.partner[0][0])[w] = 0u;
-    __syncthreads();
-    // ---- the island's bodies in body order
-    if (tid == 0) {
-        int n = 0;
-        for (int i = root; i < nbodies; i++)
-            if (C.parent[i] == root) {
-                if (n < kIslMaxBodies) S.b[n].id = i;
-                n++;
-            }
-        if (n > kIslMaxBodies) atomicOr(deverr, DEVERR_ISLAND), n = 0;
-        S.nb = n;
-    }
-    __syncthreads();
-    const int nb = S.nb;
-    if (nb == 0) return;
-    // ---- top speeds (measured over the nodes on the frame's first substep, world.cpp:3217-3222), bounds now
-    if (s0)
-        for (int k = 0; k < nb; k++) {
-            Body& B = bodies[S.b[k].id];
-            if (B.sleeping) continue;
-            float m2 = 0.0f;
-            for (int i = tid; i < B.nnodes; i += nt) m2 = smax(m2, length2(nd_v(nd, B.node0 + i)));
-            for (int o = 16; o > 0; o >>= 1) m2 = fmaxf(m2, __shfl_xor_sync(0xffffffffu, m2, o));
-            if ((tid & 31) == 0 && m2 > 0.0f) atomic_max_f(&B.acc_v2, m2);
-        }
-    __syncthreads();
-    for (int k = tid; k < nb; k += nt) {
-        const Body& B = bodies[S.b[k].id];
-        S.b[k].sp = sqrtf(B.acc_v2);
-        const bool acc = !s0 && B.acc_mn[0] <= B.acc_mx[0]; // (stepped in the last substep: its bounds then)
-        for (int c = 0; c < 3; c++) S.b[k].mn[c] = acc ? B.acc_mn[c] : B.aabb_mn[c], S.b[k].mx[c] = acc ? B.acc_mx[c] : B.aabb_mx[c];
-        S.b[k].extra = 0.0f, S.b[k].bulk = 0.0f;
-    }
-    // ---- torn triangles (world.cpp:1870-1878)
-    for (int k = 0; k < nb; k++) {
-        const Body& B = bodies[S.b[k].id];
-        if (B.sleeping) continue;
-        for (int t = tid; t < B.ntris; t += nt) {
-            const int tg = B.tri0 + t;
-            int4 tr = C.tri[tg];
-            const float r2 = C.tri_rest2[tg];
-            if (!(tr.w & TF_TORN) && r2 > 0 && max_edge2(nd_p(nd, tr.x), nd_p(nd, tr.y), nd_p(nd, tr.z)) > kTornStretch2 * r2) {
-                tr.w |= TF_TORN;
-                C.tri[tg] = tr;
-            }
-        }
-    }
-    __syncthreads();
-    const float dt = C.dt;
-    const int interval = C.interval;
-    if (tid == 0) {
-        float rmax = 0.0f, slow = 0.0f;
-        for (int k = 0; k < nb; k++) {
-            const Body& B = bodies[S.b[k].id];
-            rmax = smax(rmax, B.crad);
-            if (S.b[k].sp <= kFastSpeed) slow = smax(slow, S.b[k].sp);
-        }
-        const float speed = slow + 0.5f;
-        S.rmax = rmax;
-        S.slow_speed = speed;
-        S.margin = 2.0f * speed * (float)interval * dt + 0.02f;
-        S.slow_reach = 2.0f * speed * (float)interval * dt + 0.01f;
-        S.travel = 1.25f * (float)interval * dt;
-    }
-    __syncthreads();
-    // ---- bulk speeds of the fast bodies: mass-weighted RMS in node order, in double (world.cpp:1891-1902)
-    for (int k = 0; k < nb; k++) {
-        const Body& B = bodies[S.b[k].id];
-        if (B.sleeping || !(S.b[k].sp > kFastSpeed)) continue;
-        double mv2 = 0.0, m = 0.0;
-        for (int c0 = 0; c0 < B.nnodes; c0 += nt) {
-            const int i = c0 + tid;
-            if (i < B.nnodes) {
-                const float4 v = nd[2 * (B.node0 + i) + 1];
-                S.term0[tid] = (double)v.w * length2(V(v.x, v.y, v.z));
-                S.term1[tid] = (double)v.w;
-            }
-            __syncthreads();
-            if (tid == 0) {
-                const int n = min(nt, B.nnodes - c0);
-                serial_add(mv2, S.term0, n);
-                serial_add(m, S.term1, n);
-            }
-            __syncthreads();
-        }
-        if (tid == 0) {
-            const float bulk = clampf(m > 0 ? 1.25f * (float)sqrt(mv2 / m) : S.b[k].sp, kFastSpeed, 400.0f);
-            S.b[k].bulk = bulk;
-            S.b[k].extra = bulk * (float)interval * dt;
-        }
-        __syncthreads();
-    }
-    // ---- cell size: the mean longest edge of every 7th triangle, in double (world.cpp:1914-1926)
-    {
-        double tri_size = 0.0;
-        int samples = 0;
-        for (int k = 0; k < nb; k++) {
-            const Body& B = bodies[S.b[k].id];
-            const int ns = (B.ntris + 6) / 7;
-            for (int c0 = 0; c0 < ns; c0 += nt) {
-                const int q = c0 + tid;
-                if (q < ns) {
-                    const int4 tr = C.tri[B.tri0 + 7 * q];
-                    S.term0[tid] = (double)sqrtf(max_edge2(nd_p(nd, tr.x), nd_p(nd, tr.y), nd_p(nd, tr.z)));
-                }
-                __syncthreads();
-                if (tid == 0) serial_add(tri_size, S.term0, min(nt, ns - c0));
-                __syncthreads();
-            }
-            samples += ns;
-        }
-        if (tid == 0) {
-            const float mean = samples ? (float)(tri_size / samples) : 1.0f;
-            S.inv_cell = 1.0f / clampf(mean + 2.0f * (S.rmax + S.margin), 0.25f, 1.0f);
-        }
-    }
-    __syncthreads();
-    // ---- partners: bodies whose boxes, grown by the reach, overlap (world.cpp:1933-1954)
-    const float reach = S.rmax + S.margin;
-    for (int k = tid; k < nb; k += nt) {
-        const Body& B = bodies[S.b[k].id];
-        const float g = reach + S.b[k].extra + (B.hull ? B.hull_depth : 0.0f);
-        for (int c = 0; c < 3; c++) S.b[k].bmn[c] = S.b[k].mn[c] - g, S.b[k].bmx[c] = S.b[k].mx[c] + g;
-    }
-    __syncthreads();
-    for (int q = tid; q < nb * nb; q += nt) {
-        const int a = q / nb, b = q % nb;
-        if (b <= a) continue;
-        const Body& A = bodies[S.b[a].id];
-        const Body& Bb = bodies[S.b[b].id];
-        if (same_group(A, Bb) || (A.sleeping && Bb.sleeping)) continue;
-        if (!(S.b[a].bmn[0] <= S.b[b].bmx[0] && S.b[a].bmx[0] >= S.b[b].bmn[0] && S.b[a].bmn[1] <= S.b[b].bmx[1] && S.b[a].bmx[1] >= S.b[b].bmn[1] &&
-              S.b[a].bmn[2] <= S.b[b].bmx[2] && S.b[a].bmx[2] >= S.b[b].bmn[2]))
-            continue;
-        atomicOr(&S.partner[a][b >> 5], 1u << (b & 31));
-        atomicOr(&S.partner[b][a >> 5], 1u << (a & 31));
-    }
-    __syncthreads();
-    // ---- 1) the spatial hash of the slow bodies' contacter nodes (world.cpp:1966-1978), in body and node order
-    const int pt0 = C.isl_noff[root];
-    const int bk0 = 4 * pt0 + 65 * C.isl_idx[root];
-    {
-        int base = 0;
-        for (int k = 0; k < nb; k++) {
-            const Body& B = bodies[S.b[k].id];
-            if (!has_partner(S, k) || S.b[k].extra > 0) continue;
-            for (int c0 = 0; c0 < B.nnodes; c0 += nt) {
-                const int i = c0 + tid;
-                bool take = false;
-                int4 cell = make_int4(0, 0, 0, 0);
-                if (i < B.nnodes && ((uint32_t)info[B.node0 + i].x & NF_CONTACTER)) {
-                    const v3 p = nd_p(nd, B.node0 + i);
-                    if (near_partner(S, k, p, p)) {
-                        take = true;
-                        cell = make_int4(cell_of(p.x, S.inv_cell), cell_of(p.y, S.inv_cell), cell_of(p.z, S.inv_cell), 0);
-                    }
-                }
-                int tot;
-                const int at = block_scan_excl(take ? 1 : 0, tot, S.warp);
-                if (take) {
-                    C.pt_node[pt0 + base + at] = B.node0 + i;
-                    C.pt_body[pt0 + base + at] = S.b[k].id;
-                    C.pt_cell[pt0 + base + at] = cell;
-                }
-                base += tot;
-            }
-        }
-        if (tid == 0) {
-            int nbk = 64;
-            while (nbk < 2 * base) nbk <<= 1;
-            S.npts = base, S.mask = nbk - 1;
-        }
-        __syncthreads();
-    }
-    const int npts = S.npts, nbk = S.mask + 1;
-    int any_tris = 0;
-    for (int k = 0; k < nb; k++) any_tris |= bodies[S.b[k].id].ntris > 0;
-    if (npts > 0 && any_tris) {
-        // buckets: counts, starts, items (each bucket in node order), runs of one body's nodes
-        for (int q = tid; q <= nbk; q += nt) C.bk_start[bk0 + q] = 0;
-        __syncthreads();
-        for (int q = tid; q < npts; q += nt) {
-            const int4 c = C.pt_cell[pt0 + q];
-            atomicAdd(&C.bk_start[bk0 + (int)(cell_hash(c.x, c.y, c.z) & (uint32_t)S.mask) + 1], 1);
-        }
-        __syncthreads();
-        {
-            int carry = 0;
-            for (int c0 = 0; c0 <= nbk; c0 += nt) {
-                const int q = c0 + tid;
-                const int v = q <= nbk ? C.bk_start[bk0 + q] : 0;
-                int tot;
-                const int ex = block_scan_excl(v, tot, S.warp);
-                if (q <= nbk) C.bk_start[bk0 + q] = carry + ex + v;
-                carry += tot;
-            }
-        }
-        __syncthreads();
-        for (int q = tid; q < nbk; q += nt) C.bk_fill[bk0 + q] = C.bk_start[bk0 + q];
-        __syncthreads();
-        for (int q = tid; q < npts; q += nt) {
-            const int4 c = C.pt_cell[pt0 + q];
-            const int at = atomicAdd(&C.bk_fill[bk0 + (int)(cell_hash(c.x, c.y, c.z) & (uint32_t)S.mask)], 1);
-            C.bk_items[pt0 + at] = q;
-        }
-        __syncthreads();
-        for (int q = tid; q < nbk; q += nt) {
-            const int k0 = C.bk_start[bk0 + q], k1 = C.bk_start[bk0 + q + 1];
-            for (int i = k0 + 1; i < k1; i++) {
-                const int v = C.bk_items[pt0 + i];
-                int j = i - 1;
-                while (j >= k0 && C.bk_items[pt0 + j] > v) C.bk_items[pt0 + j + 1] = C.bk_items[pt0 + j], j--;
-                C.bk_items[pt0 + j + 1] = v;
-            }
-            for (int i = k1; i-- > k0;) {
-                const bool same = i + 1 < k1 && C.pt_body[pt0 + C.bk_items[pt0 + i + 1]] == C.pt_body[pt0 + C.bk_items[pt0 + i]];
-                C.run_end[pt0 + i] = same ? C.run_end[pt0 + i + 1] : i + 1;
-            }
-        }
-        __syncthreads();
-    }
-    const float T = (float)max(interval, 1) * dt;
-    const int gs0 = C.isl_idx[root] * (kGridCells + 1);
-    const int gi0 = pt0;
-    // ---- 2) count, then 3) write: the slow queries (bodies with partners, triangles in order), then the fast pairs
-    int total = 0;
-    for (int pass = 0; pass < 2; pass++) {
-        int2* dst = nullptr;
-        int at = 0;
-        if (pass == 1) {
-            if (tid == 0) {
-                int off = atomicAdd(C.pair_total, total);
-                if (off + total > C.max_pairs) {
-                    atomicOr(deverr, DEVERR_PAIRS);
-                    off = -1;
-                }
-                S.count = off;
-                C.isl_poff[root] = off < 0 ? 0 : off;
-                C.isl_pcnt[root] = off < 0 ? 0 : total;
-                if (off >= 0) atomicAdd(&C.counters[2], total);
-            }
-            __syncthreads();
-            if (S.count < 0) return;
-            dst = C.pairs + S.count;
-        }
-        if (npts > 0 && any_tris) {
-            for (int kt = 0; kt < nb; kt++) {
-                const Body& o = bodies[S.b[kt].id];
-                if (!has_partner(S, kt)) continue;
-                for (int c0 = 0; c0 < o.ntris; c0 += nt) {
-                    const int t = c0 + tid;
-                    const int n = t < o.ntris ? slow_query(S, C, bodies, nd, kt, o.tri0 + t, bk0, pt0, T, nullptr) : 0;
-                    int tot;
-                    const int ex = block_scan_excl(n, tot, S.warp);
-                    if (pass == 1 && n > 0) slow_query(S, C, bodies, nd, kt, o.tri0 + t, bk0, pt0, T, dst + at + ex);
-                    at += tot;
-                }
-            }
-        }
-        // fast bodies' nodes against their partners' triangles (world.cpp:2314-2475)
-        for (int kf = 0; kf < nb; kf++) {
-            if (!(S.b[kf].extra > 0) || !has_partner(S, kf)) continue; // (without partners it has no pairs)
-            const Body& F = bodies[S.b[kf].id];
-            if (tid == 0) {
-                float rmx = 0.0f;
-                for (int ko = 0; ko < nb; ko++)
-                    if (S.partner[kf][ko >> 5] & (1u << (ko & 31))) {
-                        const float fe = S.b[ko].extra > 0 ? S.b[ko].bulk * (float)interval * dt : 0.0f;
-                        rmx = smax(rmx, F.crad + S.slow_reach + fe);
-                    }
-                const float ex = S.b[kf].mx[0] - S.b[kf].mn[0] + 2e-3f, ey = S.b[kf].mx[1] - S.b[kf].mn[1] + 2e-3f;
-                const float ez = S.b[kf].mx[2] - S.b[kf].mn[2] + 2e-3f;
-                float cellsz = clampf(2.0f * rmx, 0.15f, 2.0f);
-                cellsz = smax(cellsz, smax(ex, smax(ey, ez)) / 48.0f);
-                S.g_inv = 1.0f / cellsz;
-                S.g_org[0] = S.b[kf].mn[0] - 1e-3f, S.g_org[1] = S.b[kf].mn[1] - 1e-3f, S.g_org[2] = S.b[kf].mn[2] - 1e-3f;
-                S.g_dim[0] = max(1, min(48, (int)(ex * S.g_inv) + 1));
-                S.g_dim[1] = max(1, min(48, (int)(ey * S.g_inv) + 1));
-                S.g_dim[2] = max(1, min(48, (int)(ez * S.g_inv) + 1));
-                S.g_span[0] = S.g_span[1] = S.g_span[2] = 0;
-            }
-            __syncthreads();
-            const int ncell = S.g_dim[0] * S.g_dim[1] * S.g_dim[2];
-            for (int q = tid; q <= ncell; q += nt) C.g_start[gs0 + q] = 0;
-            __syncthreads();
-            // every contacter node in the lowest cell of its travel: counts, starts, items ascending within a cell
-            for (int i = tid; i < F.nnodes; i += nt) {
-                if (!((uint32_t)info[F.node0 + i].x & NF_CONTACTER)) continue;
-                int3 lo, hi;
-                node_cells(S, nd, F.node0 + i, lo, hi);
-                atomicAdd(&C.g_start[gs0 + (lo.z * S.g_dim[1] + lo.y) * S.g_dim[0] + lo.x + 1], 1);
-                if (hi.x - lo.x > S.g_span[0]) atomicMax(&S.g_span[0], hi.x - lo.x);
-                if (hi.y - lo.y > S.g_span[1]) atomicMax(&S.g_span[1], hi.y - lo.y);
-                if (hi.z - lo.z > S.g_span[2]) atomicMax(&S.g_span[2], hi.z - lo.z);
-            }
-            __syncthreads();
-            {
-                int carry = 0;
-                for (int c0 = 0; c0 <= ncell; c0 += nt) {
-                    const int q = c0 + tid;
-                    const int v = q <= ncell ? C.g_start[gs0 + q] : 0;
-                    int tot;
-                    const int ex = block_scan_excl(v, tot, S.warp);
-                    if (q <= ncell) C.g_start[gs0 + q] = carry + ex + v;
-                    carry += tot;
-                }
-            }
-            __syncthreads();
-            for (int q = tid; q < ncell; q += nt) C.g_fill[gs0 + q] = C.g_start[gs0 + q];
-            __syncthreads();
-            for (int i = tid; i < F.nnodes; i += nt) {
-                if (!((uint32_t)info[F.node0 + i].x & NF_CONTACTER)) continue;
-                int3 lo, hi;
-                node_cells(S, nd, F.node0 + i, lo, hi);
-                const int at2 = atomicAdd(&C.g_fill[gs0 + (lo.z * S.g_dim[1] + lo.y) * S.g_dim[0] + lo.x], 1);
-                C.g_items[gi0 + at2] = F.node0 + i;
-            }
-            __syncthreads();
-            for (int q = tid; q < ncell; q += nt) {
-                const int k0 = C.g_start[gs0 + q], k1 = C.g_start[gs0 + q + 1];
-                for (int i = k0 + 1; i < k1; i++) {
-                    const int v = C.g_items[gi0 + i];
-                    int j = i - 1;
-                    while (j >= k0 && C.g_items[gi0 + j] > v) C.g_items[gi0 + j + 1] = C.g_items[gi0 + j], j--;
-                    C.g_items[gi0 + j + 1] = v;
-                }
-            }
-            __syncthreads();
-            for (int ko = 0; ko < nb; ko++) {
-                if (!(S.partner[kf][ko >> 5] & (1u << (ko & 31)))) continue;
-                const Body& o = bodies[S.b[ko].id];
-                const float fe = S.b[ko].extra > 0 ? S.b[ko].bulk * (float)interval * dt : 0.0f;
-                for (int c0 = 0; c0 < o.ntris; c0 += nt) {
-                    const int t = c0 + tid;
-                    const int n = t < o.ntris ? fast_query(S, C, bodies, nd, kf, ko, o.tri0 + t, gs0, gi0, fe, T, nullptr) : 0;
-                    int tot;
-                    const int ex = block_scan_excl(n, tot, S.warp);
-                    if (pass == 1 && n > 0) fast_query(S, C, bodies, nd, kf, ko, o.tri0 + t, gs0, gi0, fe, T, dst + at + ex);
-                    at += tot;
-                }
-            }
-            __syncthreads();
-        }
-        if (pass == 0) total = at;
-    }
-    if (tid == 0) atomicAdd(&C.counters[0], 1);
-}
+} // namespace blg
+#include "bl_pair_search.cuh"
+namespace blg {
 
 // ------------------------------------------------------------------------------------------ narrow phase (each substep)
 // World::pair_detect for node-triangle pairs (world.cpp:2819-2858): hit_a = (bary, pen), hit_b = (normal, 1) when

@@ -232,6 +232,12 @@ struct bl_gpu_ctx {
     DevBuf<int> pt_node, pt_body, bk_start, bk_fill, bk_items, run_end, g_start, g_fill, g_items, counters;
     DevBuf<int2> pairs;
     DevBuf<float4> hit_a, hit_b;
+    // the pair search's records, island states, queries and counters (bl_pair_search.cuh)
+    DevBuf<float4> g_rec, sb_pos;
+    DevBuf<int4> sb_cell, q_group;
+    DevBuf<int> g_hi, q_count, sc;
+    DevBuf<int2> q_chunk;
+    DevBuf<IslSearch> isl;
     Contacts ct{};
     // frames captured as graphs, by substep count
     std::map<int, cudaGraphExec_t> graphs;
@@ -295,6 +301,8 @@ static void free_contacts(bl_gpu_ctx* c) {
     c->isl_contacts.free_(), c->pair_total.free_(), c->pt_node.free_(), c->pt_body.free_(), c->bk_start.free_(), c->bk_fill.free_();
     c->bk_items.free_(), c->run_end.free_(), c->g_start.free_(), c->g_fill.free_(), c->g_items.free_(), c->counters.free_();
     c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_();
+    c->g_rec.free_(), c->sb_pos.free_(), c->sb_cell.free_(), c->q_group.free_(), c->g_hi.free_(), c->q_count.free_(), c->sc.free_();
+    c->q_chunk.free_(), c->isl.free_();
     c->contacts_on = false;
 }
 
@@ -1014,9 +1022,24 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     BL_CUDA(c, c->pt_cell.alloc(N));
     BL_CUDA(c, c->bk_start.alloc(4 * (size_t)N + 65 * (size_t)B + 1));
     BL_CUDA(c, c->bk_fill.alloc(4 * (size_t)N + 65 * (size_t)B + 1));
-    BL_CUDA(c, c->g_start.alloc((size_t)c->max_isl * (kGridCells + 1)));
+    // (fast grids: the starts of every fast body's cells from one pool, the fill counters one grid per island)
+    const int cell_cap = std::min(B, 512) * (kGridCells + 1);
+    BL_CUDA(c, c->g_start.alloc((size_t)cell_cap));
     BL_CUDA(c, c->g_fill.alloc((size_t)c->max_isl * (kGridCells + 1)));
     BL_CUDA(c, c->g_items.alloc(N));
+    BL_CUDA(c, c->g_rec.alloc(N));
+    BL_CUDA(c, c->g_hi.alloc(N));
+    BL_CUDA(c, c->sb_cell.alloc(N));
+    BL_CUDA(c, c->sb_pos.alloc(N));
+    // queries: a triangle against a hash or a grid; a full list flags DEVERR_PAIRS
+    const int q_cap = 8 * std::max(c->NTRI, 1) + 65536, grp_cap = B * std::min(B, kIslMaxBodies) + B, chunk_cap = grp_cap + q_cap / kQueryChunk;
+    BL_CUDA(c, c->isl.alloc(c->max_isl));
+    BL_CUDA(c, c->q_count.alloc(q_cap));
+    BL_CUDA(c, c->q_group.alloc(grp_cap));
+    BL_CUDA(c, c->q_chunk.alloc(chunk_cap));
+    BL_CUDA(c, c->sc.alloc(4));
+    BL_CUDA(c, cudaMemsetAsync(c->sc.p, 0, 4 * sizeof(int), c->stream));
+    BL_CUDA(c, cudaFuncSetAttribute(k_rebuild, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RebuildShared)));
     // (the pair list starts as valid indices: k_detect reads up to the last search's total)
     BL_CUDA(c, cudaMemsetAsync(c->pairs.p, 0, sizeof(int2) * c->cfg.max_pairs, c->stream));
     BL_CUDA(c, cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), c->stream));
@@ -1032,6 +1055,9 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     C.pair_total = c->pair_total.p, C.pairs = c->pairs.p, C.hit_a = c->hit_a.p, C.hit_b = c->hit_b.p, C.max_pairs = c->cfg.max_pairs;
     C.pt_node = c->pt_node.p, C.pt_body = c->pt_body.p, C.pt_cell = c->pt_cell.p, C.bk_start = c->bk_start.p, C.bk_fill = c->bk_fill.p;
     C.bk_items = c->bk_items.p, C.run_end = c->run_end.p, C.g_start = c->g_start.p, C.g_fill = c->g_fill.p, C.g_items = c->g_items.p;
+    C.g_rec = c->g_rec.p, C.g_hi = c->g_hi.p, C.sb_cell = c->sb_cell.p, C.sb_pos = c->sb_pos.p, C.isl = c->isl.p;
+    C.q_group = c->q_group.p, C.q_chunk = c->q_chunk.p, C.q_count = c->q_count.p, C.sc = c->sc.p;
+    C.q_cap = q_cap, C.grp_cap = grp_cap, C.chunk_cap = chunk_cap, C.cell_cap = cell_cap;
     C.counters = c->counters.p, C.interval = c->interval, C.dt = c->cfg.dt, C.wake_speed = c->cfg.sleep_speed;
     return BL_GPU_OK;
 }
@@ -1357,7 +1383,7 @@ static int64_t frame_launches(const bl_gpu_ctx* c, int n) {
     int64_t total = per * n + 3;
     if (c->contacts_on) {
         total += 1 + 3 * (int64_t)n; // k_islands; k_wake, k_detect, k_collide a substep
-        for (int k = 0; k < n; k++) total += rebuild_at(c, k) ? 1 : 0;
+        for (int k = 0; k < n; k++) total += rebuild_at(c, k) ? 4 : 0; // (k_rebuild, k_pair_count, k_pair_place, k_pair_write)
     }
     return total;
 }
@@ -1461,7 +1487,11 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_wake<<<c->B, 256, 0, s>>>(c->dbodies.p, c->bmeta.p);
             if (rebuild_at(c, k)) {
                 cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), s);
+                cudaMemsetAsync(c->sc.p, 0, 4 * sizeof(int), s);
                 k_rebuild<<<c->B, 1024, sizeof(RebuildShared), s>>>(c->dbodies.p, c->B, c->nd.p, c->info.p, CT, k == 0 ? 1 : 0, c->deverr.p);
+                k_pair_count<<<kQueryGrid, kQueryChunk, 0, s>>>(c->dbodies.p, c->nd.p, CT);
+                k_pair_place<<<c->B, 1024, 0, s>>>(c->dbodies.p, c->B, CT, c->deverr.p);
+                k_pair_write<<<kQueryGrid, kQueryChunk, 0, s>>>(c->dbodies.p, c->nd.p, CT);
             }
         }
         mark();
