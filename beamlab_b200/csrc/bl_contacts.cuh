@@ -366,9 +366,9 @@ __global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, c
 //     contact's record - its slots, the accumulation weights, relative velocity and normal, and every
 //     term of the contact law that does not depend on the forces (the slip direction and speed, the Stribeck
 //     exponentials, the restitution term) - formed in parallel;
-//  3. one thread runs the chain: per contact only the force-dependent arithmetic, on shared memory, with the
-//     reference's operations in its order (contact_force<1, 3> / hull_push_out<3> and primitive_collision,
-//     world.cpp:59-120, static_world.cpp:8-51, split at their force-independent parts);
+//  3. the chain: per contact only the force-dependent arithmetic (apply_contact), on shared memory, level by level -
+//     a contact's level is one above its nodes' earlier contacts' levels, so the contacts of one level touch
+//     distinct nodes and each sees the forces the serial loop would give it;
 //  4. the forces written back. An island with more distinct contact nodes than the slots hold runs the loop on global
 //     memory (collide_island_global). Results are the same bits either way.
 __device__ void collide_island_global(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Contacts C,
@@ -377,6 +377,7 @@ __device__ void collide_island_global(const float4* __restrict__ nd, const int4*
 constexpr int kCollideThreads = 256;
 constexpr int kSlotBits = 13, kSlots = 1 << kSlotBits; // force slots (distinct contact nodes an island)
 constexpr int kRecChunk = 512;                          // contact records formed at a time
+constexpr int kLevelCost = 2;                           // a level's barrier costs about this many serial contacts
 
 struct ContactRec {
     int sa, sb[3];        // force slots of the node and the triangle's corners
@@ -390,6 +391,7 @@ struct ContactRec {
     float sv, stop;       // the slip speed; mass sv / dt
     float e1, gsum;       // 1 - exp(-sv / va); the dynamic friction's g + min(t2 sv, 5)
     int kind;             // 0 none, 1 contact (node movable), 2 contact (node immovable), 3 hull push-out; | ma << 4 | mb << 5
+    int lvl;              // its level in the chain (its contacts run together)
 };
 
 __device__ __forceinline__ int slot_hash(int key) { return (int)(((uint32_t)key * 2654435761u) >> (32 - kSlotBits)); }
@@ -397,6 +399,66 @@ __device__ __forceinline__ int slot_find(const int* keys, int key) {
     int h = slot_hash(key);
     while (keys[h] != key) h = (h + 1) & (kSlots - 1);
     return h;
+}
+
+// One contact of the chain on the forces in the slots: only the force-dependent arithmetic, the reference's operations
+// in its order (contact_force<1, 3> / hull_push_out<3> and primitive_collision, world.cpp:59-120,
+// static_world.cpp:8-51, split at their force-independent parts, which the record holds)
+__device__ __forceinline__ void apply_contact(const ContactRec& R, float* fx, float* fy, float* fz, const GroundModel& gm) {
+    const int kind = R.kind & 15;
+    const bool ma = R.kind & 16, mb = R.kind & 32;
+    v3 FA = V(fx[R.sa], fy[R.sa], fz[R.sa]);
+    v3 FB[3];
+    for (int q = 0; q < 3; q++) FB[q] = V(fx[R.sb[q]], fy[R.sb[q]], fz[R.sb[q]]);
+    v3 acc = V(0, 0, 0);
+    if (ma) acc = acc + FA * R.ca;
+    for (int q = 0; q < 3; q++)
+        if (mb) acc = acc - FB[q] * R.cb[q];
+    const v3 nrm = V(R.nx, R.ny, R.nz);
+    if (kind == 3) {
+        const float fn = R.rsub - dot(acc, nrm) * R.m;
+        if (fn > 0) {
+            const v3 f = nrm * fn;
+            if (ma) FA = FA + f;
+            if (mb)
+                for (int q = 0; q < 3; q++) FB[q] = FB[q] - f * R.wb[q];
+        }
+    } else {
+        const v3 f_rel = acc * R.m;
+        const v3 F = kind == 1 ? f_rel : neg(f_rel);
+        const v3 vel = V(R.vx, R.vy, R.vz);
+        // primitive_collision (static_world.cpp:8-51) with its force-independent terms from the record
+        v3 out = V(0, 0, 0);
+        const float Vn = R.Vn, Fn = dot(F, nrm), sgl = gm.soft_depth, pen = R.pen;
+        if (sgl > 0 && pen >= 0) {
+            out = out + vel * (-gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f));
+            float Fb = gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f;
+            if (Vn >= 0 && Fn < 0 && Fb > -Fn) Fb = -Fn;
+            out = out + nrm * Fb;
+        }
+        if (pen >= sgl) {
+            float Rn = -Fn;
+            if (Vn < 0) Rn -= R.rsub;
+            if (Rn > 0) {
+                const v3 slipF = F - nrm * Fn;
+                const v3 slip = V(R.sx, R.sy, R.sz);
+                const float G = Rn * gm.strength * R.fric;
+                if (R.sv < gm.va && G > 0 && length(slipF) <= gm.ms * G)
+                    out = out + (nrm * Rn - slip * smin(gm.ms * G * R.e1, R.stop) - slipF);
+                else
+                    out = out + (nrm * Rn - slip * smin(R.gsum * G, smax(0.0f, R.stop + dot(slipF, slip))));
+            }
+        }
+        if (kind == 2) {
+            for (int q = 0; q < 3; q++) FB[q] = FB[q] + out * R.wb[q];
+        } else {
+            FA = FA + out * 1.0f;
+            if (mb)
+                for (int q = 0; q < 3; q++) FB[q] = FB[q] - out * R.wb[q];
+        }
+    }
+    fx[R.sa] = FA.x, fy[R.sa] = FA.y, fz[R.sa] = FA.z;
+    for (int q = 0; q < 3; q++) fx[R.sb[q]] = FB[q].x, fy[R.sb[q]] = FB[q].y, fz[R.sb[q]] = FB[q].z;
 }
 
 __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies,
@@ -407,7 +469,8 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
     float* fy = fx + kSlots;
     float* fz = fy + kSlots;
     ContactRec* rec = reinterpret_cast<ContactRec*>(fz + kSlots);
-    __shared__ int used, overflow, ncontacts;
+    unsigned short* slot_lvl = reinterpret_cast<unsigned short*>(rec + kRecChunk); // per slot: its latest contact's level
+    __shared__ int used, overflow, ncontacts, s_depth;
     const int root = blockIdx.x, tid = threadIdx.x;
     if (root >= nbodies) return;
     const int cnt = C.isl_pcnt[root];
@@ -415,7 +478,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
     const int off = C.isl_poff[root];
     const float dt = C.dt;
     const GroundModel& gm = c_ground[3]; // SURF_CONCRETE
-    for (int h = tid; h < kSlots; h += kCollideThreads) keys[h] = -1;
+    for (int h = tid; h < kSlots; h += kCollideThreads) keys[h] = -1, slot_lvl[h] = 0;
     if (tid == 0) used = 0, overflow = 0, ncontacts = 0;
     __syncthreads();
     // 1. the contacts' nodes into slots
@@ -561,66 +624,40 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
             atomicAdd(&bt.body_contacts, 1);
         }
         __syncthreads();
-        // 3. the chain
+        // 3. the chain. A contact reads and writes the forces of its four nodes only, so one that shares no node with
+        // the contacts between it and an earlier one commutes with them: each contact's level is one above the
+        // latest level among its nodes' earlier contacts (one thread, in pair order), then the contacts of a level run
+        // together, level after level - every contact sees the forces the serial loop gives it. Where the levels are
+        // too few per contact to pay for their barriers, one thread runs the loop.
         if (tid == 0) {
+            int depth = 0;
             for (int r = 0; r < nh; r++) {
-                const ContactRec& R = rec[r];
-                const int kind = R.kind & 15;
-                if (kind == 0) continue;
-                const bool ma = R.kind & 16, mb = R.kind & 32;
-                v3 FA = V(fx[R.sa], fy[R.sa], fz[R.sa]);
-                v3 FB[3];
-                for (int q = 0; q < 3; q++) FB[q] = V(fx[R.sb[q]], fy[R.sb[q]], fz[R.sb[q]]);
-                v3 acc = V(0, 0, 0);
-                if (ma) acc = acc + FA * R.ca;
-                for (int q = 0; q < 3; q++)
-                    if (mb) acc = acc - FB[q] * R.cb[q];
-                const v3 nrm = V(R.nx, R.ny, R.nz);
-                if (kind == 3) {
-                    const float fn = R.rsub - dot(acc, nrm) * R.m;
-                    if (fn > 0) {
-                        const v3 f = nrm * fn;
-                        if (ma) FA = FA + f;
-                        if (mb)
-                            for (int q = 0; q < 3; q++) FB[q] = FB[q] - f * R.wb[q];
-                    }
-                } else {
-                    const v3 f_rel = acc * R.m;
-                    const v3 F = kind == 1 ? f_rel : neg(f_rel);
-                    const v3 vel = V(R.vx, R.vy, R.vz);
-                    // primitive_collision (static_world.cpp:8-51) with its force-independent terms from the record
-                    v3 out = V(0, 0, 0);
-                    const float Vn = R.Vn, Fn = dot(F, nrm), sgl = gm.soft_depth, pen = R.pen;
-                    if (sgl > 0 && pen >= 0) {
-                        out = out + vel * (-gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f));
-                        float Fb = gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f;
-                        if (Vn >= 0 && Fn < 0 && Fb > -Fn) Fb = -Fn;
-                        out = out + nrm * Fb;
-                    }
-                    if (pen >= sgl) {
-                        float Rn = -Fn;
-                        if (Vn < 0) Rn -= R.rsub;
-                        if (Rn > 0) {
-                            const v3 slipF = F - nrm * Fn;
-                            const v3 slip = V(R.sx, R.sy, R.sz);
-                            const float G = Rn * gm.strength * R.fric;
-                            if (R.sv < gm.va && G > 0 && length(slipF) <= gm.ms * G)
-                                out = out + (nrm * Rn - slip * smin(gm.ms * G * R.e1, R.stop) - slipF);
-                            else
-                                out = out + (nrm * Rn - slip * smin(R.gsum * G, smax(0.0f, R.stop + dot(slipF, slip))));
-                        }
-                    }
-                    if (kind == 2) {
-                        for (int q = 0; q < 3; q++) FB[q] = FB[q] + out * R.wb[q];
-                    } else {
-                        FA = FA + out * 1.0f;
-                        if (mb)
-                            for (int q = 0; q < 3; q++) FB[q] = FB[q] - out * R.wb[q];
-                    }
-                }
-                fx[R.sa] = FA.x, fy[R.sa] = FA.y, fz[R.sa] = FA.z;
-                for (int q = 0; q < 3; q++) fx[R.sb[q]] = FB[q].x, fy[R.sb[q]] = FB[q].y, fz[R.sb[q]] = FB[q].z;
+                ContactRec& R = rec[r];
+                if ((R.kind & 15) == 0) continue;
+                int l = max(max((int)slot_lvl[R.sa], (int)slot_lvl[R.sb[0]]), max((int)slot_lvl[R.sb[1]], (int)slot_lvl[R.sb[2]])) + 1;
+                slot_lvl[R.sa] = slot_lvl[R.sb[0]] = slot_lvl[R.sb[1]] = slot_lvl[R.sb[2]] = (unsigned short)l;
+                R.lvl = l;
+                depth = max(depth, l);
             }
+            s_depth = depth;
+        }
+        __syncthreads();
+        const int depth = s_depth;
+        if (depth * kLevelCost > nh) {
+            if (tid == 0)
+                for (int r = 0; r < nh; r++)
+                    if (rec[r].kind & 15) apply_contact(rec[r], fx, fy, fz, gm);
+        } else {
+            for (int L = 1; L <= depth; L++) {
+                for (int r = tid; r < nh; r += kCollideThreads)
+                    if ((rec[r].kind & 15) && rec[r].lvl == L) apply_contact(rec[r], fx, fy, fz, gm);
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        for (int r = tid; r < nh; r += kCollideThreads) {
+            const ContactRec& R = rec[r];
+            if (R.kind & 15) slot_lvl[R.sa] = slot_lvl[R.sb[0]] = slot_lvl[R.sb[1]] = slot_lvl[R.sb[2]] = 0;
         }
     }
     __syncthreads();
@@ -632,8 +669,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
         if (ncontacts) atomicAdd(&C.counters[1], ncontacts);
     }
 }
-
-constexpr size_t kCollideSmem = sizeof(int) * kSlots + 3 * sizeof(float) * kSlots + sizeof(ContactRec) * kRecChunk;
+constexpr size_t kCollideSmem = sizeof(int) * kSlots + 3 * sizeof(float) * kSlots + sizeof(ContactRec) * kRecChunk + sizeof(unsigned short) * kSlots;
 
 // The serial loop on global memory (the path of an island with more distinct contact nodes than the slots hold)
 __device__ void collide_island_global(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Contacts C,
