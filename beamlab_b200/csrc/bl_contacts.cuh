@@ -52,6 +52,8 @@ struct Contacts {
     int2* pairs;               // (node, triangle), global indices
     float4* hit_a;             // per pair: bary.xyz, pen
     float4* hit_b;             // per pair: normal.xyz, w = 1 when the pair is in contact
+    uint8_t* hflag;            // per pair: 1 when in contact (hit_b.w as a byte)
+    int* hidx;                 // per island's pair range: its contacts' pair indices, in pair order
     int max_pairs;
     // rebuild scratch
     int* pt_node;              // hashed nodes of an island, in order
@@ -354,6 +356,7 @@ __global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, c
         hb.w = hit ? 1.0f : 0.0f;
         C.hit_a[i] = ha;
         C.hit_b[i] = hb;
+        C.hflag[i] = hit ? 1 : 0;
     }
 }
 
@@ -377,9 +380,8 @@ __device__ void collide_island_global(const float4* __restrict__ nd, const int4*
 constexpr int kCollideThreads = 256;
 constexpr int kSlotBits = 13, kSlots = 1 << kSlotBits; // force slots (distinct contact nodes an island)
 constexpr int kRecChunk = 512;                          // contact records formed at a time
-constexpr int kLevelCost = 2;                           // a level's barrier costs about this many serial contacts
 
-struct ContactRec {
+struct alignas(16) ContactRec {
     int sa, sb[3];        // force slots of the node and the triangle's corners
     float ca, cb[3];      // acc = FA ca - sum FB_q cb_q (the terms the movable sides have)
     float wb[3], m;       // barycentric weights; effective mass
@@ -480,11 +482,22 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
     const GroundModel& gm = c_ground[3]; // SURF_CONCRETE
     for (int h = tid; h < kSlots; h += kCollideThreads) keys[h] = -1, slot_lvl[h] = 0;
     if (tid == 0) used = 0, overflow = 0, ncontacts = 0;
+    __shared__ int s_scan[32];
+    // 0. the island's contacts (its pairs with a hit), in pair order, into hidx[off ...): a run of pairs a thread
+    int nh_all;
+    {
+        const int per = (cnt + kCollideThreads - 1) / kCollideThreads;
+        const int lo = min(cnt, tid * per), hi = min(cnt, lo + per);
+        int mine = 0;
+        for (int i = lo; i < hi; i++) mine += C.hflag[off + i];
+        int at = off + block_scan_excl(mine, nh_all, s_scan);
+        for (int i = lo; i < hi; i++)
+            if (C.hflag[off + i]) C.hidx[at++] = off + i;
+    }
     __syncthreads();
     // 1. the contacts' nodes into slots
-    for (int i = off + tid; i < off + cnt; i += kCollideThreads) {
-        if (C.hit_b[i].w == 0.0f) continue;
-        const int2 pr = C.pairs[i];
+    for (int j = tid; j < nh_all; j += kCollideThreads) {
+        const int2 pr = C.pairs[C.hidx[off + j]];
         const int4 tr = C.tri[pr.y];
         const int nodes[4] = {pr.x, tr.x, tr.y, tr.z};
         for (int q = 0; q < 4; q++) {
@@ -514,33 +527,14 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
             const float4 f = Fs[keys[h]];
             fx[h] = f.x, fy[h] = f.y, fz[h] = f.z;
         }
-    // the island's contacts (pairs with a hit), in pair order, kRecChunk at a time: a block scan places each
-    __shared__ int hl[kRecChunk], wsum[kCollideThreads / 32], nhl;
-    int next = off;
-    while (true) {
+    // the island's contacts in pair order, kRecChunk at a time
+    __shared__ int order[kRecChunk], lend[kRecChunk + 2];
+    for (int c0 = 0; c0 < nh_all; c0 += kRecChunk) {
+        const int nh = min(kRecChunk, nh_all - c0);
         __syncthreads();
-        if (tid == 0) nhl = 0;
-        __syncthreads();
-        while (next < off + cnt && nhl + kCollideThreads <= kRecChunk) {
-            const int i = next + tid;
-            const bool hit = i < off + cnt && C.hit_b[i].w != 0.0f;
-            const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if ((tid & 31) == 0) wsum[tid >> 5] = __popc(bal);
-            __syncthreads();
-            int before = nhl;
-            for (int wq = 0; wq < (tid >> 5); wq++) before += wsum[wq];
-            if (hit) hl[before + __popc(bal & ((1u << (tid & 31)) - 1u))] = i;
-            __syncthreads();
-            if (tid == 0)
-                for (int wq = 0; wq < kCollideThreads / 32; wq++) nhl += wsum[wq];
-            next += kCollideThreads;
-            __syncthreads();
-        }
-        const int nh = nhl;
-        if (nh == 0) break;
         // 2. the records of these contacts
         for (int r = tid; r < nh; r += kCollideThreads) {
-            const int i = hl[r];
+            const int i = C.hidx[off + c0 + r];
             ContactRec& R = rec[r];
             R.kind = 0;
             const float4 hb4 = C.hit_b[i];
@@ -626,32 +620,53 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
         __syncthreads();
         // 3. the chain. A contact reads and writes the forces of its four nodes only, so one that shares no node with
         // the contacts between it and an earlier one commutes with them: each contact's level is one above the
-        // latest level among its nodes' earlier contacts (one thread, in pair order), then the contacts of a level run
-        // together, level after level - every contact sees the forces the serial loop gives it. Where the levels are
-        // too few per contact to pay for their barriers, one thread runs the loop.
+        // latest level among its nodes' earlier contacts (one thread, in pair order), the contacts sorted by level,
+        // then one warp runs them level after level, a level's contacts at once - every contact sees the forces the
+        // serial loop gives it. Where the levels are nearly as many as the contacts, one thread runs the loop.
+        for (int l = tid; l < kRecChunk + 2; l += kCollideThreads) lend[l] = 0;
         if (tid == 0) {
-            int depth = 0;
+            int depth = 0, nk = 0;
+            int4 h = *reinterpret_cast<const int4*>(&rec[0].sa);
+            int kd = rec[0].kind;
             for (int r = 0; r < nh; r++) {
-                ContactRec& R = rec[r];
-                if ((R.kind & 15) == 0) continue;
-                int l = max(max((int)slot_lvl[R.sa], (int)slot_lvl[R.sb[0]]), max((int)slot_lvl[R.sb[1]], (int)slot_lvl[R.sb[2]])) + 1;
-                slot_lvl[R.sa] = slot_lvl[R.sb[0]] = slot_lvl[R.sb[1]] = slot_lvl[R.sb[2]] = (unsigned short)l;
-                R.lvl = l;
-                depth = max(depth, l);
+                // (the next record's slots are loaded before this one's levels are stored)
+                int4 hn = h;
+                int kn = 0;
+                if (r + 1 < nh) hn = *reinterpret_cast<const int4*>(&rec[r + 1].sa), kn = rec[r + 1].kind;
+                if (kd & 15) {
+                    const int l = max(max((int)slot_lvl[h.x], (int)slot_lvl[h.y]), max((int)slot_lvl[h.z], (int)slot_lvl[h.w])) + 1;
+                    slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = (unsigned short)l;
+                    rec[r].lvl = l;
+                    depth = max(depth, l), nk++;
+                }
+                h = hn, kd = kn;
             }
-            s_depth = depth;
+            s_depth = 5 * depth > 4 * nk ? -1 : depth;
         }
         __syncthreads();
         const int depth = s_depth;
-        if (depth * kLevelCost > nh) {
+        if (depth < 0) {
             if (tid == 0)
                 for (int r = 0; r < nh; r++)
                     if (rec[r].kind & 15) apply_contact(rec[r], fx, fy, fz, gm);
-        } else {
-            for (int L = 1; L <= depth; L++) {
-                for (int r = tid; r < nh; r += kCollideThreads)
-                    if ((rec[r].kind & 15) && rec[r].lvl == L) apply_contact(rec[r], fx, fy, fz, gm);
-                __syncthreads();
+        } else if (depth > 0) {
+            // by level: counts, ends (a running sum), places (each level's contacts in any order: they share no node)
+            for (int r = tid; r < nh; r += kCollideThreads)
+                if (rec[r].kind & 15) atomicAdd(&lend[rec[r].lvl], 1);
+            __syncthreads();
+            block_scan_incl_inplace(lend, depth + 1, s_scan);
+            __syncthreads();
+            if (tid == 0) lend[depth + 1] = lend[depth];
+            __syncthreads();
+            for (int r = tid; r < nh; r += kCollideThreads)
+                if (rec[r].kind & 15) order[atomicSub(&lend[rec[r].lvl], 1) - 1] = r; // (lend[L] becomes level L's start)
+            __syncthreads();
+            if (tid < 32) {
+                for (int L = 1; L <= depth; L++) {
+                    const int e = lend[L + 1];
+                    for (int k = lend[L] + tid; k < e; k += 32) apply_contact(rec[order[k]], fx, fy, fz, gm);
+                    __syncwarp();
+                }
             }
         }
         __syncthreads();
