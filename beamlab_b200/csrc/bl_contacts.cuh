@@ -52,7 +52,7 @@ struct Contacts {
     int2* pairs;               // (node, triangle), global indices
     float4* hit_a;             // per pair: bary.xyz, pen
     float4* hit_b;             // per pair: normal.xyz, w = 1 when the pair is in contact
-    uint8_t* hflag;            // per pair: 1 when in contact (hit_b.w as a byte)
+    uint32_t* hbits;           // per 32 pairs: bit j set when pair 32 w + j is in contact
     int* hidx;                 // per island's pair range: its contacts' pair indices, in pair order
     int max_pairs;
     // rebuild scratch
@@ -305,58 +305,63 @@ namespace blg {
 // the pair is in contact, hit_b.w = 0 when not
 __global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, const int4* __restrict__ info, const Body* __restrict__ bodies, Contacts C) {
     const int total = min(*C.pair_total, C.max_pairs);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const int2 pr = C.pairs[i];
-        const int4 tr = C.tri[pr.y];
-        const Body& bn = bodies[info[pr.x].w];
-        const Body& bt = bodies[tr.w >> 8];
-        float4 ha = make_float4(0, 0, 0, 0), hb = make_float4(0, 0, 0, 0);
+    // (a warp takes 32 consecutive pairs: its ballot is their word of hit bits)
+    for (int i0 = blockIdx.x * blockDim.x; i0 < total; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + (int)threadIdx.x;
         bool hit = false;
-        do {
-            if (bn.sleeping && bt.sleeping) break;
-            if (tr.w & TF_TORN) break; // (torn since the pairs were found)
-            const bool two_sided = (tr.w & TF_TWO_SIDED) != 0;
-            const v3 np = nd_p(nd, pr.x);
-            const v3 a = nd_p(nd, tr.x), b = nd_p(nd, tr.y), cc = nd_p(nd, tr.z);
-            v3 bary;
-            const float r = bt.faces_only && !two_sided ? bt.face_skin : bn.crad;
-            if (!two_sided) {
-                // a hull triangle: over its face pushed out along the face's normal, from as deep as the hull's depth
-                const v3 fn = normalize(cross(b - a, cc - a));
-                const float s = dot(np - a, fn);
-                if (s >= r || s < -bt.hull_depth) break;
-                const v3 q = np - fn * s;
-                const v3 cq = closest_on_triangle(q, a, b, cc, bary);
-                if (length2(cq - q) <= 1e-6f) {
-                    ha = make_float4(bary.x, bary.y, bary.z, r - s), hb = make_float4(fn.x, fn.y, fn.z, 0.0f);
-                    hit = true;
-                    break;
+        if (i < total) {
+            const int2 pr = C.pairs[i];
+            const int4 tr = C.tri[pr.y];
+            const Body& bn = bodies[info[pr.x].w];
+            const Body& bt = bodies[tr.w >> 8];
+            float4 ha = make_float4(0, 0, 0, 0), hb = make_float4(0, 0, 0, 0);
+            do {
+                if (bn.sleeping && bt.sleeping) break;
+                if (tr.w & TF_TORN) break; // (torn since the pairs were found)
+                const bool two_sided = (tr.w & TF_TWO_SIDED) != 0;
+                const v3 np = nd_p(nd, pr.x);
+                const v3 a = nd_p(nd, tr.x), b = nd_p(nd, tr.y), cc = nd_p(nd, tr.z);
+                v3 bary;
+                const float r = bt.faces_only && !two_sided ? bt.face_skin : bn.crad;
+                if (!two_sided) {
+                    // a hull triangle: over its face pushed out along the face's normal, from as deep as the hull's depth
+                    const v3 fn = normalize(cross(b - a, cc - a));
+                    const float s = dot(np - a, fn);
+                    if (s >= r || s < -bt.hull_depth) break;
+                    const v3 q = np - fn * s;
+                    const v3 cq = closest_on_triangle(q, a, b, cc, bary);
+                    if (length2(cq - q) <= 1e-6f) {
+                        ha = make_float4(bary.x, bary.y, bary.z, r - s), hb = make_float4(fn.x, fn.y, fn.z, 0.0f);
+                        hit = true;
+                        break;
+                    }
+                    if (s < 0 || bt.faces_only) break;
+                } else {
+                    const v3 lo = vmin3(a, vmin3(b, cc)) - V(r, r, r), hi = vmax3(a, vmax3(b, cc)) + V(r, r, r);
+                    if (outside(np, lo, hi)) break;
                 }
-                if (s < 0 || bt.faces_only) break;
-            } else {
-                const v3 lo = vmin3(a, vmin3(b, cc)) - V(r, r, r), hi = vmax3(a, vmax3(b, cc)) + V(r, r, r);
-                if (outside(np, lo, hi)) break;
-            }
-            const v3 cp = closest_on_triangle(np, a, b, cc, bary);
-            const v3 d = np - cp;
-            const float dist2 = dot(d, d);
-            if (dist2 >= r * r) break;
-            const float dist = sqrtf(dist2);
-            v3 nrm;
-            if (dist > 1e-5f) {
-                nrm = divs(d, dist);
-            } else {
-                nrm = normalize(cross(b - a, cc - a));
-                const v3 vt = nd_v(nd, tr.x) * bary.x + nd_v(nd, tr.y) * bary.y + nd_v(nd, tr.z) * bary.z;
-                if (dot(nd_v(nd, pr.x) - vt, nrm) > 0) nrm = neg(nrm);
-            }
-            ha = make_float4(bary.x, bary.y, bary.z, r - dist), hb = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
-            hit = true;
-        } while (false);
-        hb.w = hit ? 1.0f : 0.0f;
-        C.hit_a[i] = ha;
-        C.hit_b[i] = hb;
-        C.hflag[i] = hit ? 1 : 0;
+                const v3 cp = closest_on_triangle(np, a, b, cc, bary);
+                const v3 d = np - cp;
+                const float dist2 = dot(d, d);
+                if (dist2 >= r * r) break;
+                const float dist = sqrtf(dist2);
+                v3 nrm;
+                if (dist > 1e-5f) {
+                    nrm = divs(d, dist);
+                } else {
+                    nrm = normalize(cross(b - a, cc - a));
+                    const v3 vt = nd_v(nd, tr.x) * bary.x + nd_v(nd, tr.y) * bary.y + nd_v(nd, tr.z) * bary.z;
+                    if (dot(nd_v(nd, pr.x) - vt, nrm) > 0) nrm = neg(nrm);
+                }
+                ha = make_float4(bary.x, bary.y, bary.z, r - dist), hb = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+                hit = true;
+            } while (false);
+            hb.w = hit ? 1.0f : 0.0f;
+            C.hit_a[i] = ha;
+            C.hit_b[i] = hb;
+        }
+        const unsigned bits = __ballot_sync(0xffffffffu, hit);
+        if ((threadIdx.x & 31) == 0) C.hbits[i >> 5] = bits;
     }
 }
 
@@ -380,6 +385,7 @@ __device__ void collide_island_global(const float4* __restrict__ nd, const int4*
 constexpr int kCollideThreads = 256;
 constexpr int kSlotBits = 13, kSlots = 1 << kSlotBits; // force slots (distinct contact nodes an island)
 constexpr int kRecChunk = 512;                          // contact records formed at a time
+constexpr int kSlotPad = 8;                             // slot levels past the slots (kSlots: a level that stays 0)
 
 struct alignas(16) ContactRec {
     int sa, sb[3];        // force slots of the node and the triangle's corners
@@ -392,8 +398,9 @@ struct alignas(16) ContactRec {
     float sx, sy, sz;     // the slip direction (0 where the slip speed is below 1e-9)
     float sv, stop;       // the slip speed; mass sv / dt
     float e1, gsum;       // 1 - exp(-sv / va); the dynamic friction's g + min(t2 sv, 5)
+    float dragf, fb0;     // the soft ground's drag factor and buoyancy (where it is soft under the contact)
     int kind;             // 0 none, 1 contact (node movable), 2 contact (node immovable), 3 hull push-out; | ma << 4 | mb << 5
-    int lvl;              // its level in the chain (its contacts run together)
+                          // | soft (drag, buoyancy) << 6 | pen >= soft depth << 7
 };
 
 __device__ __forceinline__ int slot_hash(int key) { return (int)(((uint32_t)key * 2654435761u) >> (32 - kSlotBits)); }
@@ -431,14 +438,14 @@ __device__ __forceinline__ void apply_contact(const ContactRec& R, float* fx, fl
         const v3 vel = V(R.vx, R.vy, R.vz);
         // primitive_collision (static_world.cpp:8-51) with its force-independent terms from the record
         v3 out = V(0, 0, 0);
-        const float Vn = R.Vn, Fn = dot(F, nrm), sgl = gm.soft_depth, pen = R.pen;
-        if (sgl > 0 && pen >= 0) {
-            out = out + vel * (-gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f));
-            float Fb = gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f;
+        const float Vn = R.Vn, Fn = dot(F, nrm);
+        if (R.kind & 64) {
+            out = out + vel * R.dragf;
+            float Fb = R.fb0;
             if (Vn >= 0 && Fn < 0 && Fb > -Fn) Fb = -Fn;
             out = out + nrm * Fb;
         }
-        if (pen >= sgl) {
+        if (R.kind & 128) {
             float Rn = -Fn;
             if (Vn < 0) Rn -= R.rsub;
             if (Rn > 0) {
@@ -481,39 +488,59 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
     const float dt = C.dt;
     const GroundModel& gm = c_ground[3]; // SURF_CONCRETE
     for (int h = tid; h < kSlots; h += kCollideThreads) keys[h] = -1, slot_lvl[h] = 0;
+    if (tid < kSlotPad) slot_lvl[kSlots + tid] = 0;
     if (tid == 0) used = 0, overflow = 0, ncontacts = 0;
     __shared__ int s_scan[32];
     // 0. the island's contacts (its pairs with a hit), in pair order, into hidx[off ...): a run of pairs a thread
     int nh_all;
     {
-        const int per = (cnt + kCollideThreads - 1) / kCollideThreads;
-        const int lo = min(cnt, tid * per), hi = min(cnt, lo + per);
+        // (the range's words of hit bits, a run of words a thread, the bits outside the range masked)
+        const int w0 = off >> 5, nw = ((off + cnt - 1) >> 5) - w0 + 1;
+        const int per = (nw + kCollideThreads - 1) / kCollideThreads;
+        const int lo = min(nw, tid * per), hi = min(nw, lo + per);
+        auto word = [&](int w) {
+            uint32_t m = C.hbits[w0 + w];
+            const int b0 = (w0 + w) << 5;
+            if (b0 < off) m &= ~0u << (off - b0);
+            if (b0 + 32 > off + cnt) m &= (off + cnt - b0 >= 32) ? ~0u : ((1u << (off + cnt - b0)) - 1u);
+            return m;
+        };
         int mine = 0;
-        for (int i = lo; i < hi; i++) mine += C.hflag[off + i];
+        for (int w = lo; w < hi; w++) mine += __popc(word(w));
         int at = off + block_scan_excl(mine, nh_all, s_scan);
-        for (int i = lo; i < hi; i++)
-            if (C.hflag[off + i]) C.hidx[at++] = off + i;
+        for (int w = lo; w < hi; w++)
+            for (uint32_t m = word(w); m; m &= m - 1) C.hidx[at++] = ((w0 + w) << 5) + __ffs(m) - 1;
     }
     __syncthreads();
-    // 1. the contacts' nodes into slots
-    for (int j = tid; j < nh_all; j += kCollideThreads) {
-        const int2 pr = C.pairs[C.hidx[off + j]];
-        const int4 tr = C.tri[pr.y];
-        const int nodes[4] = {pr.x, tr.x, tr.y, tr.z};
-        for (int q = 0; q < 4; q++) {
-            int h = slot_hash(nodes[q]);
-            for (int probe = 0;; probe++) {
-                if (probe >= kSlots / 2 || overflow) {
-                    overflow = 1;
-                    break;
+    // 1. the contacts' nodes into slots (four contacts a thread at a time: their loads overlap)
+    for (int j0 = tid; j0 < nh_all; j0 += 4 * kCollideThreads) {
+        int nodes4[4][4];
+        for (int u = 0; u < 4; u++) {
+            const int j = j0 + u * kCollideThreads;
+            nodes4[u][0] = -1;
+            if (j >= nh_all) continue;
+            const int2 pr = C.pairs[C.hidx[off + j]];
+            const int4 tr = C.tri[pr.y];
+            nodes4[u][0] = pr.x, nodes4[u][1] = tr.x, nodes4[u][2] = tr.y, nodes4[u][3] = tr.z;
+        }
+        for (int u = 0; u < 4; u++) {
+            if (nodes4[u][0] < 0) continue;
+            for (int q = 0; q < 4; q++) {
+                const int node = nodes4[u][q];
+                int h = slot_hash(node);
+                for (int probe = 0;; probe++) {
+                    if (probe >= kSlots / 2 || overflow) {
+                        overflow = 1;
+                        break;
+                    }
+                    const int prev = atomicCAS(&keys[h], -1, node);
+                    if (prev == -1) {
+                        if (atomicAdd(&used, 1) >= kSlots / 2) overflow = 1; // (kept at most half full: short probes)
+                        break;
+                    }
+                    if (prev == node) break;
+                    h = (h + 1) & (kSlots - 1);
                 }
-                const int prev = atomicCAS(&keys[h], -1, nodes[q]);
-                if (prev == -1) {
-                    if (atomicAdd(&used, 1) >= kSlots / 2) overflow = 1; // (kept at most half full: short probes)
-                    break;
-                }
-                if (prev == nodes[q]) break;
-                h = (h + 1) & (kSlots - 1);
             }
         }
     }
@@ -528,7 +555,8 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
             fx[h] = f.x, fy[h] = f.y, fz[h] = f.z;
         }
     // the island's contacts in pair order, kRecChunk at a time
-    __shared__ int order[kRecChunk], lend[kRecChunk + 2];
+    __shared__ int order[kRecChunk], lend[kRecChunk + 3], lv[kRecChunk];
+    __shared__ int4 sl[kRecChunk + 1]; // per record: its slots (kSlots x 4: not a contact)
     for (int c0 = 0; c0 < nh_all; c0 += kRecChunk) {
         const int nh = min(kRecChunk, nh_all - c0);
         __syncthreads();
@@ -537,6 +565,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
             const int i = C.hidx[off + c0 + r];
             ContactRec& R = rec[r];
             R.kind = 0;
+            sl[r] = make_int4(kSlots, kSlots, kSlots, kSlots); // (none: the slot whose level stays 0)
             const float4 hb4 = C.hit_b[i];
             const float4 ha = C.hit_a[i];
             const int2 pr = C.pairs[i];
@@ -611,8 +640,12 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
                 R.e1 = 1.0f - bl_expf(-sv / gm.va);
                 const float g = gm.mc + (gm.ms - gm.mc) * bl_expf(-bl_powf(sv / gm.vs, gm.alpha));
                 R.gsum = g + smin(gm.t2 * sv, 5.0f);
-                R.kind = (ma ? 1 : 2) | mv;
+                const bool soft = sgl > 0 && pen >= 0;
+                R.dragf = soft ? -gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f) : 0.0f;
+                R.fb0 = soft ? gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f : 0.0f;
+                R.kind = (ma ? 1 : 2) | mv | (soft ? 64 : 0) | (pen >= sgl ? 128 : 0);
             }
+            sl[r] = make_int4(R.sa, R.sb[0], R.sb[1], R.sb[2]);
             atomicAdd(&ncontacts, 1);
             atomicAdd(&bn.body_contacts, 1);
             atomicAdd(&bt.body_contacts, 1);
@@ -623,23 +656,18 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
         // latest level among its nodes' earlier contacts (one thread, in pair order), the contacts sorted by level,
         // then one warp runs them level after level, a level's contacts at once - every contact sees the forces the
         // serial loop gives it. Where the levels are nearly as many as the contacts, one thread runs the loop.
-        for (int l = tid; l < kRecChunk + 2; l += kCollideThreads) lend[l] = 0;
+        for (int l = tid; l < kRecChunk + 3; l += kCollideThreads) lend[l] = 0;
         if (tid == 0) {
             int depth = 0, nk = 0;
-            int4 h = *reinterpret_cast<const int4*>(&rec[0].sa);
-            int kd = rec[0].kind;
+            int4 h = sl[0];
             for (int r = 0; r < nh; r++) {
-                // (the next record's slots are loaded before this one's levels are stored)
-                int4 hn = h;
-                int kn = 0;
-                if (r + 1 < nh) hn = *reinterpret_cast<const int4*>(&rec[r + 1].sa), kn = rec[r + 1].kind;
-                if (kd & 15) {
-                    const int l = max(max((int)slot_lvl[h.x], (int)slot_lvl[h.y]), max((int)slot_lvl[h.z], (int)slot_lvl[h.w])) + 1;
-                    slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = (unsigned short)l;
-                    rec[r].lvl = l;
-                    depth = max(depth, l), nk++;
-                }
-                h = hn, kd = kn;
+                const int4 hn = sl[r + 1]; // (loaded before this record's levels are stored; sl[nh] is not used)
+                const int l = max(max((int)slot_lvl[h.x], (int)slot_lvl[h.y]), max((int)slot_lvl[h.z], (int)slot_lvl[h.w])) + 1;
+                const int lk = h.x == kSlots ? 0 : l;
+                slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = (unsigned short)lk;
+                lv[r] = lk;
+                depth = max(depth, lk), nk += lk != 0;
+                h = hn;
             }
             s_depth = 5 * depth > 4 * nk ? -1 : depth;
         }
@@ -648,31 +676,37 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
         if (depth < 0) {
             if (tid == 0)
                 for (int r = 0; r < nh; r++)
-                    if (rec[r].kind & 15) apply_contact(rec[r], fx, fy, fz, gm);
+                    if (lv[r]) apply_contact(rec[r], fx, fy, fz, gm);
         } else if (depth > 0) {
             // by level: counts, ends (a running sum), places (each level's contacts in any order: they share no node)
             for (int r = tid; r < nh; r += kCollideThreads)
-                if (rec[r].kind & 15) atomicAdd(&lend[rec[r].lvl], 1);
+                if (lv[r]) atomicAdd(&lend[lv[r]], 1);
             __syncthreads();
             block_scan_incl_inplace(lend, depth + 1, s_scan);
             __syncthreads();
             if (tid == 0) lend[depth + 1] = lend[depth];
             __syncthreads();
             for (int r = tid; r < nh; r += kCollideThreads)
-                if (rec[r].kind & 15) order[atomicSub(&lend[rec[r].lvl], 1) - 1] = r; // (lend[L] becomes level L's start)
+                if (lv[r]) order[atomicSub(&lend[lv[r]], 1) - 1] = r; // (lend[L] becomes level L's start)
             __syncthreads();
             if (tid < 32) {
+                // a lane a contact of the level; the next level's first contacts are looked up before this level runs
+                int s0 = lend[1], e0 = lend[2];
+                int rr = s0 + tid < e0 ? order[s0 + tid] : -1;
                 for (int L = 1; L <= depth; L++) {
-                    const int e = lend[L + 1];
-                    for (int k = lend[L] + tid; k < e; k += 32) apply_contact(rec[order[k]], fx, fy, fz, gm);
+                    const int s1 = lend[L + 1], e1 = L < depth ? lend[L + 2] : s1;
+                    const int rn = s1 + tid < e1 ? order[s1 + tid] : -1;
+                    if (rr >= 0) apply_contact(rec[rr], fx, fy, fz, gm);
+                    for (int k = s0 + tid + 32; k < e0; k += 32) apply_contact(rec[order[k]], fx, fy, fz, gm);
                     __syncwarp();
+                    s0 = s1, e0 = e1, rr = rn;
                 }
             }
         }
         __syncthreads();
         for (int r = tid; r < nh; r += kCollideThreads) {
-            const ContactRec& R = rec[r];
-            if (R.kind & 15) slot_lvl[R.sa] = slot_lvl[R.sb[0]] = slot_lvl[R.sb[1]] = slot_lvl[R.sb[2]] = 0;
+            const int4 h = sl[r];
+            slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = 0;
         }
     }
     __syncthreads();
@@ -684,7 +718,8 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
         if (ncontacts) atomicAdd(&C.counters[1], ncontacts);
     }
 }
-constexpr size_t kCollideSmem = sizeof(int) * kSlots + 3 * sizeof(float) * kSlots + sizeof(ContactRec) * kRecChunk + sizeof(unsigned short) * kSlots;
+constexpr size_t kCollideSmem = sizeof(int) * kSlots + 3 * sizeof(float) * kSlots + sizeof(ContactRec) * kRecChunk +
+                                sizeof(unsigned short) * (kSlots + kSlotPad);
 
 // The serial loop on global memory (the path of an island with more distinct contact nodes than the slots hold)
 __device__ void collide_island_global(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Contacts C,

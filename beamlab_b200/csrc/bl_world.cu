@@ -238,7 +238,7 @@ struct bl_gpu_ctx {
     DevBuf<int> g_hi, q_count, sc;
     DevBuf<int2> q_chunk;
     DevBuf<IslSearch> isl;
-    DevBuf<uint8_t> hflag;
+    DevBuf<uint32_t> hbits;
     DevBuf<int> hidx;
     Contacts ct{};
     // frames captured as graphs, by substep count
@@ -304,7 +304,7 @@ static void free_contacts(bl_gpu_ctx* c) {
     c->bk_items.free_(), c->run_end.free_(), c->g_start.free_(), c->g_fill.free_(), c->g_items.free_(), c->counters.free_();
     c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_();
     c->g_rec.free_(), c->sb_pos.free_(), c->sb_cell.free_(), c->q_group.free_(), c->g_hi.free_(), c->q_count.free_(), c->sc.free_();
-    c->q_chunk.free_(), c->isl.free_(), c->hflag.free_(), c->hidx.free_();
+    c->q_chunk.free_(), c->isl.free_(), c->hbits.free_(), c->hidx.free_();
     c->contacts_on = false;
 }
 
@@ -1020,7 +1020,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     BL_CUDA(c, c->pairs.alloc(c->cfg.max_pairs));
     BL_CUDA(c, c->hit_a.alloc(c->cfg.max_pairs));
     BL_CUDA(c, c->hit_b.alloc(c->cfg.max_pairs));
-    BL_CUDA(c, c->hflag.alloc(c->cfg.max_pairs));
+    BL_CUDA(c, c->hbits.alloc((size_t)c->cfg.max_pairs / 32 + 1));
     BL_CUDA(c, c->hidx.alloc(c->cfg.max_pairs));
     for (DevBuf<int>* d : {&c->pt_node, &c->pt_body, &c->bk_items, &c->run_end}) BL_CUDA(c, d->alloc(N));
     BL_CUDA(c, c->pt_cell.alloc(N));
@@ -1061,7 +1061,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     C.bk_items = c->bk_items.p, C.run_end = c->run_end.p, C.g_start = c->g_start.p, C.g_fill = c->g_fill.p, C.g_items = c->g_items.p;
     C.g_rec = c->g_rec.p, C.g_hi = c->g_hi.p, C.sb_cell = c->sb_cell.p, C.sb_pos = c->sb_pos.p, C.isl = c->isl.p;
     C.q_group = c->q_group.p, C.q_chunk = c->q_chunk.p, C.q_count = c->q_count.p, C.sc = c->sc.p;
-    C.hflag = c->hflag.p, C.hidx = c->hidx.p;
+    C.hbits = c->hbits.p, C.hidx = c->hidx.p;
     C.q_cap = q_cap, C.grp_cap = grp_cap, C.chunk_cap = chunk_cap, C.cell_cap = cell_cap;
     C.counters = c->counters.p, C.interval = c->interval, C.dt = c->cfg.dt, C.wake_speed = c->cfg.sleep_speed;
     return BL_GPU_OK;
