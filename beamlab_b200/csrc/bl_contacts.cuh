@@ -34,6 +34,7 @@ enum : uint32_t { TF_TWO_SIDED = 1, TF_TORN = 2 };
 enum : uint32_t { DEVERR_PAIRS = 4, DEVERR_ISLAND = 8, DEVERR_CONTACT_UNSUPPORTED = 32 };
 
 struct IslSearch;
+struct ContactRec;
 
 struct Contacts {
     int4* tri;                 // a, b, c, flags | body << 8
@@ -54,6 +55,9 @@ struct Contacts {
     float4* hit_b;             // per pair: normal.xyz, w = 1 when the pair is in contact
     uint32_t* hbits;           // per 32 pairs: bit j set when pair 32 w + j is in contact
     int* hidx;                 // per island's pair range: its contacts' pair indices, in pair order
+    ContactRec* crec;          // the contacts' records of the islands that run whole (a substep's, taken in turn)
+    int* crec_n;               // records taken this substep (reset by k_detect)
+    int crec_cap;
     int max_pairs;
     // rebuild scratch
     int* pt_node;              // hashed nodes of an island, in order
@@ -305,6 +309,7 @@ namespace blg {
 // the pair is in contact, hit_b.w = 0 when not
 __global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, const int4* __restrict__ info, const Body* __restrict__ bodies, Contacts C) {
     const int total = min(*C.pair_total, C.max_pairs);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *C.crec_n = 0; // (k_collide takes its records after this kernel)
     // (a warp takes 32 consecutive pairs: its ballot is their word of hit bits)
     for (int i0 = blockIdx.x * blockDim.x; i0 < total; i0 += gridDim.x * blockDim.x) {
         const int i = i0 + (int)threadIdx.x;
@@ -386,6 +391,7 @@ constexpr int kCollideThreads = 256;
 constexpr int kSlotBits = 13, kSlots = 1 << kSlotBits; // force slots (distinct contact nodes an island)
 constexpr int kRecChunk = 512;                          // contact records formed at a time
 constexpr int kSlotPad = 8;                             // slot levels past the slots (kSlots: a level that stays 0)
+constexpr int kStage = 6144;                            // contacts of an island that runs whole (slots, levels staged)
 
 struct alignas(16) ContactRec {
     int sa, sb[3];        // force slots of the node and the triangle's corners
@@ -470,7 +476,97 @@ __device__ __forceinline__ void apply_contact(const ContactRec& R, float* fx, fl
     for (int q = 0; q < 3; q++) fx[R.sb[q]] = FB[q].x, fy[R.sb[q]] = FB[q].y, fz[R.sb[q]] = FB[q].z;
 }
 
-__global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies,
+// One contact's record (pair i of the island; kind 0 where the law gives it no force): its slots, the accumulation
+// weights and every force-independent term of the law, and the wake requests of its sleeping sides. True when it is a
+// contact (counted).
+__device__ __forceinline__ bool form_record(ContactRec& R, int i, const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies,
+                                            const Contacts& C, const int* keys, const GroundModel& gm, float dt) {
+    R.kind = 0;
+    const float4 hb4 = C.hit_b[i];
+    const float4 ha = C.hit_a[i];
+    const int2 pr = C.pairs[i];
+    const int4 tr = C.tri[pr.y];
+    Body& bn = bodies[info[pr.x].w];
+    Body& bt = bodies[tr.w >> 8];
+    // movable (world.cpp:2983-2993): a sleeping side is immovable and asks to wake when the other moves
+    bool ma = true, mb = true;
+    if (bn.sleeping) {
+        if (sqrtf(bt.acc_v2) > smax(C.wake_speed, bt.sleep_speed) * 1.0f) bn.wake_request = 1;
+        ma = false;
+    }
+    if (bt.sleeping) {
+        if (sqrtf(bn.acc_v2) > smax(C.wake_speed, bn.sleep_speed) * 1.0f) bt.wake_request = 1;
+        mb = false;
+    }
+    const int ia = pr.x, ib[3] = {tr.x, tr.y, tr.z};
+    const float wb[3] = {ha.x, ha.y, ha.z};
+    const v3 n = V(hb4.x, hb4.y, hb4.z);
+    const float pen = ha.w;
+    const float4 pa = nd[2 * ia], va4 = nd[2 * ia + 1];
+    const v3 Av = V(va4.x, va4.y, va4.z);
+    const float Aim = pa.w;
+    v3 Bv[3];
+    float Bim[3];
+    for (int q = 0; q < 3; q++) {
+        const float4 pq = nd[2 * ib[q]], vq = nd[2 * ib[q] + 1];
+        Bv[q] = V(vq.x, vq.y, vq.z), Bim[q] = pq.w;
+    }
+    R.sa = slot_find(keys, ia);
+    for (int q = 0; q < 3; q++) R.sb[q] = slot_find(keys, ib[q]), R.wb[q] = wb[q], R.cb[q] = wb[q] * Bim[q];
+    const int mv = (ma ? 16 : 0) | (mb ? 32 : 0);
+    if (!(tr.w & TF_TWO_SIDED) && pen > bn.crad) {
+        // hull_push_out<3> (world.cpp:97-118): behind a hull's face
+        float W = ma ? Aim : 0.0f;
+        if (mb)
+            for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
+        if (W <= 1e-12f) return false;
+        v3 vb = V(0, 0, 0);
+        for (int q = 0; q < 3; q++) vb = vb + Bv[q] * wb[q];
+        const float m = 1.0f / W, vr = dot(Av - vb, n), target = smin(0.2f * pen / dt, 2.0f);
+        R.ca = Aim, R.m = m, R.nx = n.x, R.ny = n.y, R.nz = n.z;
+        R.rsub = (target - vr) * m / dt;
+        R.kind = 3 | mv;
+    } else {
+        // contact_force<1, 3> (world.cpp:59-92), the node's weight 1; a tyre node grips with its own friction
+        // (world.cpp:3013)
+        const int4 ina = info[ia];
+        const float fric = ((uint32_t)ina.x & NF_TYRE) ? __int_as_float(ina.y) : 0.8f * smin(bn.cfric, bt.cfric);
+        float W = 0;
+        if (ma) W += 1.0f * 1.0f * Aim;
+        if (mb)
+            for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
+        if (W <= 1e-12f) return false;
+        const float m = 1.0f / W;
+        v3 va = V(0, 0, 0), vb = V(0, 0, 0);
+        va = va + Av * 1.0f;
+        for (int q = 0; q < 3; q++) vb = vb + Bv[q] * wb[q];
+        const v3 vel = ma ? va - vb : vb - va, nrm = ma ? n : neg(n);
+        R.ca = 1.0f * Aim, R.m = m, R.fric = fric, R.pen = pen;
+        R.nx = nrm.x, R.ny = nrm.y, R.nz = nrm.z, R.vx = vel.x, R.vy = vel.y, R.vz = vel.z;
+        // primitive_collision's force-independent terms (static_world.cpp:8-51; push_max 2, slop 0, no
+        // restitution)
+        const float Vn = dot(vel, nrm), sgl = gm.soft_depth;
+        R.Vn = Vn;
+        R.rsub = Vn < 0 ? (0.8f * Vn - smin(0.2f * smax(0.0f, pen - sgl - 0.0f) / dt, 2.0f)) * m / dt : 0.0f;
+        v3 slip = vel - nrm * Vn;
+        const float sv = length(slip);
+        if (sv > 1e-9f) slip = divs(slip, sv);
+        else slip = V(0, 0, 0);
+        R.sx = slip.x, R.sy = slip.y, R.sz = slip.z, R.sv = sv, R.stop = m * sv / dt;
+        R.e1 = 1.0f - bl_expf(-sv / gm.va);
+        const float g = gm.mc + (gm.ms - gm.mc) * bl_expf(-bl_powf(sv / gm.vs, gm.alpha));
+        R.gsum = g + smin(gm.t2 * sv, 5.0f);
+        const bool soft = sgl > 0 && pen >= 0;
+        R.dragf = soft ? -gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f) : 0.0f;
+        R.fb0 = soft ? gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f : 0.0f;
+        R.kind = (ma ? 1 : 2) | mv | (soft ? 64 : 0) | (pen >= sgl ? 128 : 0);
+    }
+    atomicAdd(&bn.body_contacts, 1);
+    atomicAdd(&bt.body_contacts, 1);
+    return true;
+}
+
+__global__ void __launch_bounds__(kCollideThreads, 1) k_collide(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies,
                                                             int nbodies, Contacts C, float4* __restrict__ Fs) {
     extern __shared__ __align__(16) unsigned char csm[];
     int* keys = reinterpret_cast<int*>(csm);
@@ -554,159 +650,163 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(const float4* __res
             const float4 f = Fs[keys[h]];
             fx[h] = f.x, fy[h] = f.y, fz[h] = f.z;
         }
-    // the island's contacts in pair order, kRecChunk at a time
-    __shared__ int order[kRecChunk], lend[kRecChunk + 3], lv[kRecChunk];
-    __shared__ int4 sl[kRecChunk + 1]; // per record: its slots (kSlots x 4: not a contact)
-    for (int c0 = 0; c0 < nh_all; c0 += kRecChunk) {
-        const int nh = min(kRecChunk, nh_all - c0);
-        __syncthreads();
-        // 2. the records of these contacts
-        for (int r = tid; r < nh; r += kCollideThreads) {
-            const int i = C.hidx[off + c0 + r];
-            ContactRec& R = rec[r];
-            R.kind = 0;
-            sl[r] = make_int4(kSlots, kSlots, kSlots, kSlots); // (none: the slot whose level stays 0)
-            const float4 hb4 = C.hit_b[i];
-            const float4 ha = C.hit_a[i];
-            const int2 pr = C.pairs[i];
+    // The island's contacts at once where they fit (kStage at most, and the substep's record buffer has room): their
+    // records in global memory, their slots and levels staged in the record chunk's shared memory - levels over the
+    // whole island, with no barrier between chunks. Otherwise kRecChunk at a time, below.
+    __shared__ int s_base;
+    if (tid == 0) {
+        int b = -1;
+        if (nh_all > 0 && nh_all <= kStage) {
+            b = atomicAdd(C.crec_n, nh_all);
+            if (b + nh_all > C.crec_cap) b = -1;
+        }
+        s_base = b;
+    }
+    __syncthreads();
+    if (s_base >= 0) {
+        const int base = s_base;
+        ushort4* sq = reinterpret_cast<ushort4*>(rec);                          // per contact: its slots
+        unsigned short* lv16 = reinterpret_cast<unsigned short*>(sq + kStage); // per contact: its level
+        // 2. each contact's slots
+        for (int j = tid; j < nh_all; j += kCollideThreads) {
+            const int2 pr = C.pairs[C.hidx[off + j]];
             const int4 tr = C.tri[pr.y];
-            Body& bn = bodies[info[pr.x].w];
-            Body& bt = bodies[tr.w >> 8];
-            // movable (world.cpp:2983-2993): a sleeping side is immovable and asks to wake when the other moves
-            bool ma = true, mb = true;
-            if (bn.sleeping) {
-                if (sqrtf(bt.acc_v2) > smax(C.wake_speed, bt.sleep_speed) * 1.0f) bn.wake_request = 1;
-                ma = false;
-            }
-            if (bt.sleeping) {
-                if (sqrtf(bn.acc_v2) > smax(C.wake_speed, bn.sleep_speed) * 1.0f) bt.wake_request = 1;
-                mb = false;
-            }
-            const int ia = pr.x, ib[3] = {tr.x, tr.y, tr.z};
-            const float wb[3] = {ha.x, ha.y, ha.z};
-            const v3 n = V(hb4.x, hb4.y, hb4.z);
-            const float pen = ha.w;
-            const float4 pa = nd[2 * ia], va4 = nd[2 * ia + 1];
-            const v3 Av = V(va4.x, va4.y, va4.z);
-            const float Aim = pa.w;
-            v3 Bv[3];
-            float Bim[3];
-            for (int q = 0; q < 3; q++) {
-                const float4 pq = nd[2 * ib[q]], vq = nd[2 * ib[q] + 1];
-                Bv[q] = V(vq.x, vq.y, vq.z), Bim[q] = pq.w;
-            }
-            R.sa = slot_find(keys, ia);
-            for (int q = 0; q < 3; q++) R.sb[q] = slot_find(keys, ib[q]), R.wb[q] = wb[q], R.cb[q] = wb[q] * Bim[q];
-            const int mv = (ma ? 16 : 0) | (mb ? 32 : 0);
-            if (!(tr.w & TF_TWO_SIDED) && pen > bn.crad) {
-                // hull_push_out<3> (world.cpp:97-118): behind a hull's face
-                float W = ma ? Aim : 0.0f;
-                if (mb)
-                    for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
-                if (W <= 1e-12f) continue;
-                v3 vb = V(0, 0, 0);
-                for (int q = 0; q < 3; q++) vb = vb + Bv[q] * wb[q];
-                const float m = 1.0f / W, vr = dot(Av - vb, n), target = smin(0.2f * pen / dt, 2.0f);
-                R.ca = Aim, R.m = m, R.nx = n.x, R.ny = n.y, R.nz = n.z;
-                R.rsub = (target - vr) * m / dt;
-                R.kind = 3 | mv;
-            } else {
-                // contact_force<1, 3> (world.cpp:59-92), the node's weight 1; a tyre node grips with its own friction
-                // (world.cpp:3013)
-                const int4 ina = info[ia];
-                const float fric = ((uint32_t)ina.x & NF_TYRE) ? __int_as_float(ina.y) : 0.8f * smin(bn.cfric, bt.cfric);
-                float W = 0;
-                if (ma) W += 1.0f * 1.0f * Aim;
-                if (mb)
-                    for (int q = 0; q < 3; q++) W += wb[q] * wb[q] * Bim[q];
-                if (W <= 1e-12f) continue;
-                const float m = 1.0f / W;
-                v3 va = V(0, 0, 0), vb = V(0, 0, 0);
-                va = va + Av * 1.0f;
-                for (int q = 0; q < 3; q++) vb = vb + Bv[q] * wb[q];
-                const v3 vel = ma ? va - vb : vb - va, nrm = ma ? n : neg(n);
-                R.ca = 1.0f * Aim, R.m = m, R.fric = fric, R.pen = pen;
-                R.nx = nrm.x, R.ny = nrm.y, R.nz = nrm.z, R.vx = vel.x, R.vy = vel.y, R.vz = vel.z;
-                // primitive_collision's force-independent terms (static_world.cpp:8-51; push_max 2, slop 0, no
-                // restitution)
-                const float Vn = dot(vel, nrm), sgl = gm.soft_depth;
-                R.Vn = Vn;
-                R.rsub = Vn < 0 ? (0.8f * Vn - smin(0.2f * smax(0.0f, pen - sgl - 0.0f) / dt, 2.0f)) * m / dt : 0.0f;
-                v3 slip = vel - nrm * Vn;
-                const float sv = length(slip);
-                if (sv > 1e-9f) slip = divs(slip, sv);
-                else slip = V(0, 0, 0);
-                R.sx = slip.x, R.sy = slip.y, R.sz = slip.z, R.sv = sv, R.stop = m * sv / dt;
-                R.e1 = 1.0f - bl_expf(-sv / gm.va);
-                const float g = gm.mc + (gm.ms - gm.mc) * bl_expf(-bl_powf(sv / gm.vs, gm.alpha));
-                R.gsum = g + smin(gm.t2 * sv, 5.0f);
-                const bool soft = sgl > 0 && pen >= 0;
-                R.dragf = soft ? -gm.fluid_drag * smin(1.0f, pen / sgl + 0.2f) : 0.0f;
-                R.fb0 = soft ? gm.fluid_density * smin(pen, sgl) * 9.807f * 0.02f : 0.0f;
-                R.kind = (ma ? 1 : 2) | mv | (soft ? 64 : 0) | (pen >= sgl ? 128 : 0);
-            }
-            sl[r] = make_int4(R.sa, R.sb[0], R.sb[1], R.sb[2]);
-            atomicAdd(&ncontacts, 1);
-            atomicAdd(&bn.body_contacts, 1);
-            atomicAdd(&bt.body_contacts, 1);
+            sq[j] = make_ushort4((unsigned short)slot_find(keys, pr.x), (unsigned short)slot_find(keys, tr.x), (unsigned short)slot_find(keys, tr.y),
+                                 (unsigned short)slot_find(keys, tr.z));
         }
         __syncthreads();
-        // 3. the chain. A contact reads and writes the forces of its four nodes only, so one that shares no node with
-        // the contacts between it and an earlier one commutes with them: each contact's level is one above the
-        // latest level among its nodes' earlier contacts (one thread, in pair order), the contacts sorted by level,
-        // then one warp runs them level after level, a level's contacts at once - every contact sees the forces the
-        // serial loop gives it. Where the levels are nearly as many as the contacts, one thread runs the loop.
-        for (int l = tid; l < kRecChunk + 3; l += kCollideThreads) lend[l] = 0;
+        // 3. the levels (one thread, in pair order; a pair the law gives no force keeps its place, which only orders
+        // more) while the other warps form the records
         if (tid == 0) {
-            int depth = 0, nk = 0;
-            int4 h = sl[0];
-            for (int r = 0; r < nh; r++) {
-                const int4 hn = sl[r + 1]; // (loaded before this record's levels are stored; sl[nh] is not used)
+            int depth = 0;
+            ushort4 h = sq[0];
+            for (int j = 0; j < nh_all; j++) {
+                const ushort4 hn = sq[min(j + 1, nh_all - 1)]; // (loaded before this contact's levels are stored)
                 const int l = max(max((int)slot_lvl[h.x], (int)slot_lvl[h.y]), max((int)slot_lvl[h.z], (int)slot_lvl[h.w])) + 1;
-                const int lk = h.x == kSlots ? 0 : l;
-                slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = (unsigned short)lk;
-                lv[r] = lk;
-                depth = max(depth, lk), nk += lk != 0;
+                slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = (unsigned short)l;
+                lv16[j] = (unsigned short)l;
+                depth = max(depth, l);
                 h = hn;
             }
-            s_depth = 5 * depth > 4 * nk ? -1 : depth;
-        }
-        __syncthreads();
-        const int depth = s_depth;
-        if (depth < 0) {
-            if (tid == 0)
-                for (int r = 0; r < nh; r++)
-                    if (lv[r]) apply_contact(rec[r], fx, fy, fz, gm);
-        } else if (depth > 0) {
-            // by level: counts, ends (a running sum), places (each level's contacts in any order: they share no node)
-            for (int r = tid; r < nh; r += kCollideThreads)
-                if (lv[r]) atomicAdd(&lend[lv[r]], 1);
-            __syncthreads();
-            block_scan_incl_inplace(lend, depth + 1, s_scan);
-            __syncthreads();
-            if (tid == 0) lend[depth + 1] = lend[depth];
-            __syncthreads();
-            for (int r = tid; r < nh; r += kCollideThreads)
-                if (lv[r]) order[atomicSub(&lend[lv[r]], 1) - 1] = r; // (lend[L] becomes level L's start)
-            __syncthreads();
-            if (tid < 32) {
-                // a lane a contact of the level; the next level's first contacts are looked up before this level runs
-                int s0 = lend[1], e0 = lend[2];
-                int rr = s0 + tid < e0 ? order[s0 + tid] : -1;
-                for (int L = 1; L <= depth; L++) {
-                    const int s1 = lend[L + 1], e1 = L < depth ? lend[L + 2] : s1;
-                    const int rn = s1 + tid < e1 ? order[s1 + tid] : -1;
-                    if (rr >= 0) apply_contact(rec[rr], fx, fy, fz, gm);
-                    for (int k = s0 + tid + 32; k < e0; k += 32) apply_contact(rec[order[k]], fx, fy, fz, gm);
-                    __syncwarp();
-                    s0 = s1, e0 = e1, rr = rn;
-                }
+            s_depth = depth;
+        } else if (tid >= 32) {
+            for (int j = tid - 32; j < nh_all; j += kCollideThreads - 32) {
+                ContactRec R;
+                if (form_record(R, C.hidx[off + j], nd, info, bodies, C, keys, gm, dt)) atomicAdd(&ncontacts, 1);
+                C.crec[base + j] = R;
             }
         }
         __syncthreads();
-        for (int r = tid; r < nh; r += kCollideThreads) {
-            const int4 h = sl[r];
-            slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = 0;
+        // by level: counts, ends (a running sum), places (a level's contacts in any order: they share no node)
+        const int depth = s_depth;
+        unsigned short* ord = reinterpret_cast<unsigned short*>(rec); // (over the slots, done with)
+        int* le = reinterpret_cast<int*>(ord + kStage);
+        for (int l = tid; l < depth + 3; l += kCollideThreads) le[l] = 0;
+        __syncthreads();
+        for (int j = tid; j < nh_all; j += kCollideThreads) atomicAdd(&le[lv16[j]], 1);
+        __syncthreads();
+        block_scan_incl_inplace(le, depth + 1, s_scan);
+        __syncthreads();
+        if (tid == 0) le[depth + 1] = le[depth];
+        __syncthreads();
+        for (int j = tid; j < nh_all; j += kCollideThreads) ord[atomicSub(&le[lv16[j]], 1) - 1] = (unsigned short)j; // (le[L]: level L's start)
+        __syncthreads();
+        // 4. the chain: one warp, level after level, a lane a contact; the next level's records loaded while one runs
+        if (tid < 32) {
+            const ContactRec* __restrict__ cr = C.crec + base;
+            int s0 = le[1], e0 = le[2];
+            bool has = s0 + tid < e0;
+            ContactRec cur;
+            if (has) cur = cr[ord[s0 + tid]];
+            for (int L = 1; L <= depth; L++) {
+                const int s1 = le[L + 1], e1 = L < depth ? le[L + 2] : s1;
+                const bool hasn = s1 + tid < e1;
+                ContactRec nxt;
+                if (hasn) nxt = cr[ord[s1 + tid]];
+                if (has && (cur.kind & 15)) apply_contact(cur, fx, fy, fz, gm);
+                for (int k = s0 + tid + 32; k < e0; k += 32) {
+                    const ContactRec R = cr[ord[k]];
+                    if (R.kind & 15) apply_contact(R, fx, fy, fz, gm);
+                }
+                __syncwarp();
+                cur = nxt, has = hasn, s0 = s1, e0 = e1;
+            }
+        }
+    } else {
+        // the island's contacts in pair order, kRecChunk at a time
+        __shared__ int order[kRecChunk], lend[kRecChunk + 3], lv[kRecChunk];
+        __shared__ int4 sl[kRecChunk + 1]; // per record: its slots (kSlots x 4: not a contact)
+        for (int c0 = 0; c0 < nh_all; c0 += kRecChunk) {
+            const int nh = min(kRecChunk, nh_all - c0);
+            __syncthreads();
+            // 2. the records of these contacts
+            for (int r = tid; r < nh; r += kCollideThreads) {
+                const int i = C.hidx[off + c0 + r];
+                ContactRec& R = rec[r];
+                sl[r] = make_int4(kSlots, kSlots, kSlots, kSlots); // (none: the slot whose level stays 0)
+                if (form_record(R, i, nd, info, bodies, C, keys, gm, dt)) {
+                    sl[r] = make_int4(R.sa, R.sb[0], R.sb[1], R.sb[2]);
+                    atomicAdd(&ncontacts, 1);
+                }
+            }
+            __syncthreads();
+            // 3. the chain. A contact reads and writes the forces of its four nodes only, so one that shares no node with
+            // the contacts between it and an earlier one commutes with them: each contact's level is one above the
+            // latest level among its nodes' earlier contacts (one thread, in pair order), the contacts sorted by level,
+            // then one warp runs them level after level, a level's contacts at once - every contact sees the forces the
+            // serial loop gives it. Where the levels are nearly as many as the contacts, one thread runs the loop.
+            for (int l = tid; l < kRecChunk + 3; l += kCollideThreads) lend[l] = 0;
+            if (tid == 0) {
+                int depth = 0, nk = 0;
+                int4 h = sl[0];
+                for (int r = 0; r < nh; r++) {
+                    const int4 hn = sl[r + 1]; // (loaded before this record's levels are stored; sl[nh] is not used)
+                    const int l = max(max((int)slot_lvl[h.x], (int)slot_lvl[h.y]), max((int)slot_lvl[h.z], (int)slot_lvl[h.w])) + 1;
+                    const int lk = h.x == kSlots ? 0 : l;
+                    slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = (unsigned short)lk;
+                    lv[r] = lk;
+                    depth = max(depth, lk), nk += lk != 0;
+                    h = hn;
+                }
+                s_depth = 5 * depth > 4 * nk ? -1 : depth;
+            }
+            __syncthreads();
+            const int depth = s_depth;
+            if (depth < 0) {
+                if (tid == 0)
+                    for (int r = 0; r < nh; r++)
+                        if (lv[r]) apply_contact(rec[r], fx, fy, fz, gm);
+            } else if (depth > 0) {
+                // by level: counts, ends (a running sum), places (each level's contacts in any order: they share no node)
+                for (int r = tid; r < nh; r += kCollideThreads)
+                    if (lv[r]) atomicAdd(&lend[lv[r]], 1);
+                __syncthreads();
+                block_scan_incl_inplace(lend, depth + 1, s_scan);
+                __syncthreads();
+                if (tid == 0) lend[depth + 1] = lend[depth];
+                __syncthreads();
+                for (int r = tid; r < nh; r += kCollideThreads)
+                    if (lv[r]) order[atomicSub(&lend[lv[r]], 1) - 1] = r; // (lend[L] becomes level L's start)
+                __syncthreads();
+                if (tid < 32) {
+                    // a lane a contact of the level; the next level's first contacts are looked up before this level runs
+                    int s0 = lend[1], e0 = lend[2];
+                    int rr = s0 + tid < e0 ? order[s0 + tid] : -1;
+                    for (int L = 1; L <= depth; L++) {
+                        const int s1 = lend[L + 1], e1 = L < depth ? lend[L + 2] : s1;
+                        const int rn = s1 + tid < e1 ? order[s1 + tid] : -1;
+                        if (rr >= 0) apply_contact(rec[rr], fx, fy, fz, gm);
+                        for (int k = s0 + tid + 32; k < e0; k += 32) apply_contact(rec[order[k]], fx, fy, fz, gm);
+                        __syncwarp();
+                        s0 = s1, e0 = e1, rr = rn;
+                    }
+                }
+            }
+            __syncthreads();
+            for (int r = tid; r < nh; r += kCollideThreads) {
+                const int4 h = sl[r];
+                slot_lvl[h.x] = slot_lvl[h.y] = slot_lvl[h.z] = slot_lvl[h.w] = 0;
+            }
         }
     }
     __syncthreads();

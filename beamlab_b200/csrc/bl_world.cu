@@ -239,6 +239,8 @@ struct bl_gpu_ctx {
     DevBuf<int2> q_chunk;
     DevBuf<IslSearch> isl;
     DevBuf<uint32_t> hbits;
+    DevBuf<ContactRec> crec;
+    DevBuf<int> crec_n;
     DevBuf<int> hidx;
     Contacts ct{};
     // frames captured as graphs, by substep count
@@ -304,7 +306,7 @@ static void free_contacts(bl_gpu_ctx* c) {
     c->bk_items.free_(), c->run_end.free_(), c->g_start.free_(), c->g_fill.free_(), c->g_items.free_(), c->counters.free_();
     c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_();
     c->g_rec.free_(), c->sb_pos.free_(), c->sb_cell.free_(), c->q_group.free_(), c->g_hi.free_(), c->q_count.free_(), c->sc.free_();
-    c->q_chunk.free_(), c->isl.free_(), c->hbits.free_(), c->hidx.free_();
+    c->q_chunk.free_(), c->isl.free_(), c->hbits.free_(), c->hidx.free_(), c->crec.free_(), c->crec_n.free_();
     c->contacts_on = false;
 }
 
@@ -1022,6 +1024,10 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     BL_CUDA(c, c->hit_b.alloc(c->cfg.max_pairs));
     BL_CUDA(c, c->hbits.alloc((size_t)c->cfg.max_pairs / 32 + 1));
     BL_CUDA(c, c->hidx.alloc(c->cfg.max_pairs));
+    const int crec_cap = std::max(c->cfg.max_pairs / 4, 65536);
+    BL_CUDA(c, c->crec.alloc(crec_cap));
+    BL_CUDA(c, c->crec_n.alloc(1));
+    BL_CUDA(c, cudaMemsetAsync(c->crec_n.p, 0, sizeof(int), c->stream));
     for (DevBuf<int>* d : {&c->pt_node, &c->pt_body, &c->bk_items, &c->run_end}) BL_CUDA(c, d->alloc(N));
     BL_CUDA(c, c->pt_cell.alloc(N));
     BL_CUDA(c, c->bk_start.alloc(4 * (size_t)N + 65 * (size_t)B + 1));
@@ -1061,7 +1067,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     C.bk_items = c->bk_items.p, C.run_end = c->run_end.p, C.g_start = c->g_start.p, C.g_fill = c->g_fill.p, C.g_items = c->g_items.p;
     C.g_rec = c->g_rec.p, C.g_hi = c->g_hi.p, C.sb_cell = c->sb_cell.p, C.sb_pos = c->sb_pos.p, C.isl = c->isl.p;
     C.q_group = c->q_group.p, C.q_chunk = c->q_chunk.p, C.q_count = c->q_count.p, C.sc = c->sc.p;
-    C.hbits = c->hbits.p, C.hidx = c->hidx.p;
+    C.hbits = c->hbits.p, C.hidx = c->hidx.p, C.crec = c->crec.p, C.crec_n = c->crec_n.p, C.crec_cap = crec_cap;
     C.q_cap = q_cap, C.grp_cap = grp_cap, C.chunk_cap = chunk_cap, C.cell_cap = cell_cap;
     C.counters = c->counters.p, C.interval = c->interval, C.dt = c->cfg.dt, C.wake_speed = c->cfg.sleep_speed;
     return BL_GPU_OK;
