@@ -58,6 +58,7 @@ struct Contacts {
     ContactRec* crec;          // the contacts' records of the islands that run whole (a substep's, taken in turn)
     int* crec_n;               // records taken this substep (reset by k_detect)
     int crec_cap;
+    int whole_max;             // contacts an island runs whole at most (bl_gpu_config.contact_whole_max)
     int max_pairs;
     // rebuild scratch
     int* pt_node;              // hashed nodes of an island, in order
@@ -656,7 +657,7 @@ __global__ void __launch_bounds__(kCollideThreads, 1) k_collide(const float4* __
     __shared__ int s_base;
     if (tid == 0) {
         int b = -1;
-        if (nh_all > 0 && nh_all <= kStage) {
+        if (nh_all > 0 && nh_all <= C.whole_max) {
             b = atomicAdd(C.crec_n, nh_all);
             if (b + nh_all > C.crec_cap) b = -1;
         }

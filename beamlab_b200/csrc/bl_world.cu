@@ -1068,6 +1068,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     C.g_rec = c->g_rec.p, C.g_hi = c->g_hi.p, C.sb_cell = c->sb_cell.p, C.sb_pos = c->sb_pos.p, C.isl = c->isl.p;
     C.q_group = c->q_group.p, C.q_chunk = c->q_chunk.p, C.q_count = c->q_count.p, C.sc = c->sc.p;
     C.hbits = c->hbits.p, C.hidx = c->hidx.p, C.crec = c->crec.p, C.crec_n = c->crec_n.p, C.crec_cap = crec_cap;
+    C.whole_max = c->cfg.contact_whole_max;
     C.q_cap = q_cap, C.grp_cap = grp_cap, C.chunk_cap = chunk_cap, C.cell_cap = cell_cap;
     C.counters = c->counters.p, C.interval = c->interval, C.dt = c->cfg.dt, C.wake_speed = c->cfg.sleep_speed;
     return BL_GPU_OK;
@@ -1778,6 +1779,7 @@ void bl_gpu_default_config(bl_gpu_config* cfg) {
     cfg->beams_per_sm = 0;
     cfg->tyre_grip = 1.0f;
     cfg->bulk_wait_s = 1.0f;
+    cfg->contact_whole_max = kStage;
 }
 
 int bl_gpu_abi_version(void) { return BL_GPU_ABI_VERSION; }
@@ -1806,7 +1808,8 @@ int bl_gpu_create(const bl_gpu_config* cfg, bl_gpu_ctx** out) {
         !(c0.pcg_tol > 0) || c0.beam_kernel < 0 || c0.beam_kernel > 1 || c0.fem_dense_front < 0 || c0.fem_dense_front > 3 ||
         !(c0.force_block == 0 || c0.force_block == 64 || c0.force_block == 128 || c0.force_block == 256) ||
         !(c0.integrate_block == 0 || c0.integrate_block == 64 || c0.integrate_block == 128 || c0.integrate_block == 256) ||
-        c0.beams_per_sm < 0 || c0.beams_per_sm > 16 || !(c0.tyre_grip >= 0) || !(c0.bulk_wait_s >= 0 && c0.bulk_wait_s <= 10))
+        c0.beams_per_sm < 0 || c0.beams_per_sm > 16 || !(c0.tyre_grip >= 0) || !(c0.bulk_wait_s >= 0 && c0.bulk_wait_s <= 10) ||
+        c0.contact_whole_max < 0 || c0.contact_whole_max > kStage)
         return BL_GPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || c0.device < 0 || c0.device >= ndev) return BL_GPU_ENODEVICE;

@@ -78,6 +78,7 @@ class WorldSettings:
     fem_dense_front: int = 3
     tyre_grip: float = 1.0                    # WorldSettings::tyre_grip: a factor on the tyres' friction
     bulk_wait_s: float = 1.0                  # the beams kernel's bound on a wait for its bulk copies (0: runs out)
+    contact_whole_max: int = 6144             # an island's contacts run whole up to this many, else 512 at a time
     # launch shapes (None: the tuned ones of beamlab_b200/tuned.json when present, else the library's defaults);
     # results do not depend on them
     force_block: int | None = None
@@ -381,7 +382,7 @@ class _Config(C.Structure):
                 ("fem_check_residual", C.c_int32), ("pcg_learned_scale", C.c_int32), ("graphs", C.c_int32),
                 ("beam_kernel", C.c_int32), ("fem_dense_front", C.c_int32), ("force_block", C.c_int32),
                 ("integrate_block", C.c_int32), ("beams_per_sm", C.c_int32), ("tyre_grip", C.c_float),
-                ("bulk_wait_s", C.c_float)]
+                ("bulk_wait_s", C.c_float), ("contact_whole_max", C.c_int32)]
 
 
 class _FemStats(C.Structure):
@@ -527,6 +528,7 @@ class World:
         cfg.fem_dense_front = int(self.settings.fem_dense_front)
         cfg.tyre_grip = float(self.settings.tyre_grip)
         cfg.bulk_wait_s = float(self.settings.bulk_wait_s)
+        cfg.contact_whole_max = int(self.settings.contact_whole_max)
         tuned = _tuned_shapes()
         for k in ("force_block", "integrate_block", "beams_per_sm"):
             v = getattr(self.settings, k)

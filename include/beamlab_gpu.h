@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define BL_GPU_ABI_VERSION 6
+#define BL_GPU_ABI_VERSION 7
 
 enum {
     BL_GPU_OK = 0,
@@ -102,6 +102,9 @@ typedef struct {
                                   copies, in seconds (default 1, at most 10): one that runs out raises
                                   BL_GPU_DEVERR_TIMEOUT, lets the copies in flight land and ends the block's work for that
                                   substep; 0 makes every such wait report as run out (for tests of that path) */
+    int32_t contact_whole_max; /* (no counterpart in the reference) an island's contacts run whole - their order found
+                                  over the island - up to this many (default and most: 6144); more run 512 at a time. The
+                                  same results either way; 0 runs every island 512 at a time (for tests of that path) */
 } bl_gpu_config;
 
 enum { BL_GPU_FEM_CHOLESKY = 0, BL_GPU_FEM_PCG = 1, BL_GPU_FEM_PCG_LEARNED = 2, BL_GPU_FEM_PCG_PREVIOUS = 3 };

@@ -19,7 +19,7 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 20
     for n in names:
         assert hasattr(L, n), n
-    assert L.bl_gpu_abi_version() == 6
+    assert L.bl_gpu_abi_version() == 7
     assert L.bl_gpu_error_string(-4).decode() == "unsupported feature"
 
 

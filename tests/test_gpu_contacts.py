@@ -27,10 +27,13 @@ def bits(a):
     return a.view(np.uint32)
 
 
+@pytest.mark.parametrize("whole_max", [6144, 0], ids=["whole", "chunks"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_pairs_and_states_equal_reference_fixture(name):
+def test_pairs_and_states_equal_reference_fixture(name, whole_max):
+    """Both ways an island's contacts run - whole (their order over the island) and 512 at a time - give the
+    reference's states."""
     g = golden(name)
-    w = world_from_rig(CASES[name]())
+    w = world_from_rig(CASES[name](), contact_whole_max=whole_max)
     snaps = set(int(x) for x in g["snap_frames"])
     total_pairs = 0
     for f, n in enumerate(g["frames"]):
@@ -132,3 +135,22 @@ def test_fleet_pairs_crashing_at_once_equal_reference(ref_lib):
     assert touched >= 8, f"only {touched} of 16 vehicles in contact in the last substep"  # (the pairs crash; some rebound)
     w.close()
     r.close()
+
+
+def test_fleet_contacts_whole_equal_chunks():
+    """The fleet's islands (many over 512 contacts in a substep) run whole and 512 at a time: the same node states bit
+    for bit, frame after frame."""
+    rig = rigs.fleet(16, seed=5, median_nodes=900, min_nodes=300, max_nodes=3000, terrain_size=400.0, terrain_samples=513,
+                     layout="pairs")
+    a = world_from_rig(rig)
+    b = world_from_rig(rig, contact_whole_max=0)
+    for f in range(8):
+        a.step_substeps(33)
+        b.step_substeps(33)
+        for k in range(len(rig["bodies"])):
+            x, y = a.bodies()[k].nodes(), b.bodies()[k].nodes()
+            assert np.array_equal(bits(x["p"]), bits(y["p"])) and np.array_equal(bits(x["v"]), bits(y["v"])), f"frame {f} vehicle {k}"
+    sa, sb = a.stats(), b.stats()
+    assert sa["contacts"] == sb["contacts"] > 1000 and sa["device_errors"] == sb["device_errors"] == 0
+    a.close()
+    b.close()
