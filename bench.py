@@ -431,8 +431,9 @@ def run_gpu(args):
             out["fem_step"] = fem_info
         if st1["contacts"] > st0["contacts"]:
             # the contacts between bodies: the narrow phase reads a node and its triangle's three nodes a pair (about
-            # 64 B a pair a substep); the response runs each island's contacts in the reference's order (a serial
-            # chain an island), so it is latency-bound rather than HBM-bound
+            # 64 B a pair a substep); the response runs each island's contacts level by level of their order (a level:
+            # contacts that share no node), so its time is the deepest island's levels x one contact's dependent
+            # arithmetic - latency-bound rather than HBM-bound
             pairs = len(w.pairs())
             frames_timed = K
             out["contacts_step"] = {
@@ -440,7 +441,7 @@ def run_gpu(args):
                 "ms_per_substep": per["contacts"], "pair_search_ms_per_substep": per["search"],
                 "narrow_phase_bytes_per_substep": 64 * pairs,
                 "achieved_gbs": 64 * pairs / (per["contacts"] * 1e-3) / 1e9 if per["contacts"] > 0 else None,
-                "bound": "latency (serial response per island, pair order)"}
+                "bound": "latency (the deepest island's levels of dependent contacts)"}
         if ws == 1 and args.workload == "plate64" and not args.no_solvers:
             out["fem_solvers"] = fem_solvers(local)
         if ws == 1 and args.workload == "shellcar" and not args.no_solvers:
