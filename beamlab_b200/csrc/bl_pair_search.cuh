@@ -11,10 +11,11 @@
 //    in the reference's order (slow bodies in body order, then fast bodies in body order and their partners in body
 //    order), each triangle of a group one query, split in chunks of kQueryChunk.
 //  * k_pair_count, over all islands' chunks at once (every SM busy whatever the islands' sizes): one query a thread,
-//    its kept pairs counted into q_count.
+//    its kept pairs counted into q_count and, up to kLocPairs of them, kept in ptmp.
 //  * k_pair_place, one CTA per island: the running sum of its queries' counts (the pairs' places in the island's
 //    range), the island's range taken from the pair list.
-//  * k_pair_write, over the chunks again: the queries that have pairs run again and write them at their places.
+//  * k_pair_write, over the chunks again: the queries' pairs copied to their places (a query with more pairs than the
+//    count pass keeps runs again).
 // The pairs of an island are the reference's, in its order; the islands' ranges lie in the order the islands finish.
 #pragma once
 
@@ -22,6 +23,7 @@ namespace blg {
 
 constexpr int kQueryChunk = 256;       // queries of one chunk (a CTA of k_pair_count / k_pair_write)
 constexpr int kQueryGrid = 148 * 8;    // CTAs of k_pair_count / k_pair_write (they stride over the chunks)
+constexpr int kLocPairs = 16;          // a query's pairs the count pass keeps (more: the write pass runs it again)
 
 struct IslBody {
     int id;               // global body index
@@ -128,10 +130,10 @@ __device__ __forceinline__ void node_cells(const IslBody& G, float travel, v3 p,
 }
 
 // One triangle of island body kt against the slow bodies' hash (world.cpp:2037-2083), near_pairs' filter applied:
-// counts the pairs, and writes them from `out` when it is given. The hash's records sit in bucket order (cell and
+// counts the pairs, and writes the first `cap` of them from `out` when it is given. The hash's records sit in bucket order (cell and
 // body; position and node), a run of one body's records ends at run_end.
 __device__ int slow_query(const IslSearch& S, const Contacts& C, const Body* __restrict__ bodies, const float4* __restrict__ nd, int kt, int tg,
-                          int2* out) {
+                          int2* out, int cap) {
     const Body& o = bodies[S.b[kt].id];
     const int4 tr = C.tri[tg];
     if (tr.w & TF_TORN) return 0;
@@ -178,7 +180,7 @@ __device__ int slow_query(const IslSearch& S, const Contacts& C, const Body* __r
                     if (!near_triangle(p, a, bb, c, tu, r, two_sided, depth)) continue;
                     const int node = __float_as_int(pp.w);
                     if (!near_keep(nd, b, o, node, tr, T)) continue;
-                    if (out) out[n] = make_int2(node, tg);
+                    if (out && n < cap) out[n] = make_int2(node, tg);
                     n++;
                 }
             }
@@ -189,7 +191,7 @@ __device__ int slow_query(const IslSearch& S, const Contacts& C, const Body* __r
 // pairs come out in node order (the reference sorts and deduplicates the cells' lists; here a node listed in several
 // cells of the scan is taken in the first of them, and the triangle's pairs are sorted after).
 __device__ int fast_query(const IslSearch& S, const Contacts& C, const Body* __restrict__ bodies, const float4* __restrict__ nd, int kf, int ko,
-                          int tg, int2* out) {
+                          int tg, int2* out, int cap) {
     const IslBody& G = S.b[kf];
     const Body& F = bodies[G.id];
     const Body& o = bodies[S.b[ko].id];
@@ -237,11 +239,11 @@ __device__ int fast_query(const IslSearch& S, const Contacts& C, const Body* __r
                 if (!near_triangle(p, a, bb, c, tu, rn, two_sided, depth)) continue;
                 const int ni = C.g_items[gi0 + k];
                 if (!near_keep(nd, F, o, ni, tr, T)) continue;
-                if (out) out[n] = make_int2(ni, tg);
+                if (out && n < cap) out[n] = make_int2(ni, tg);
                 n++;
             }
         }
-    if (out)
+    if (out && n <= cap)
         for (int i = 1; i < n; i++) { // (by node: the order of the reference's sorted scan)
             const int2 v = out[i];
             int j = i - 1;
@@ -641,15 +643,16 @@ __global__ void __launch_bounds__(1024) k_rebuild(Body* __restrict__ bodies, int
 }
 
 // one query: triangle t of group g (kind 0: island body k's triangles against the slow hash; kind 1: partner ko's
-// triangles against fast body k's grid); out: where its pairs go, or null to count them
+// triangles against fast body k's grid); out: where its pairs go (the first cap of them), or null to count them
 __device__ __forceinline__ int run_query(const IslSearch& S, const Contacts& C, const Body* __restrict__ bodies, const float4* __restrict__ nd, int4 g,
-                                         int t, int2* out) {
+                                         int t, int2* out, int cap) {
     const int kind = g.y & 1, k = (g.y >> 1) & 255, ko = g.y >> 9;
     const int tg = bodies[S.b[kind ? ko : k].id].tri0 + t;
-    return kind ? fast_query(S, C, bodies, nd, k, ko, tg, out) : slow_query(S, C, bodies, nd, k, tg, out);
+    return kind ? fast_query(S, C, bodies, nd, k, ko, tg, out, cap) : slow_query(S, C, bodies, nd, k, tg, out, cap);
 }
 
-// every island's queries, kQueryChunk to a CTA: their pairs counted
+// every island's queries, kQueryChunk to a CTA: their pairs counted; a query's pairs, up to kLocPairs of them, kept in
+// ptmp (q_tmp: where; -1: the query runs again to write them)
 __global__ void __launch_bounds__(kQueryChunk) k_pair_count(const Body* __restrict__ bodies, const float4* __restrict__ nd, Contacts C) {
     const int nch = min(C.sc[2], C.chunk_cap);
     for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
@@ -658,7 +661,20 @@ __global__ void __launch_bounds__(kQueryChunk) k_pair_count(const Body* __restri
         const int4 g = C.q_group[cg.x];
         const int t = cg.y + (int)threadIdx.x;
         if (t >= g.z) continue;
-        C.q_count[g.w + t] = run_query(C.isl[g.x], C, bodies, nd, g, t, nullptr);
+        int2 loc[kLocPairs];
+        const int n = run_query(C.isl[g.x], C, bodies, nd, g, t, loc, kLocPairs);
+        C.q_count[g.w + t] = n;
+        if (n > 0) {
+            int at = -1;
+            if (n <= kLocPairs) {
+                at = atomicAdd(C.sc + 4, n);
+                if (at + n <= C.ptmp_cap)
+                    for (int k = 0; k < n; k++) C.ptmp[at + k] = loc[k];
+                else
+                    at = -1;
+            }
+            C.q_tmp[g.w + t] = at;
+        }
     }
 }
 
@@ -689,7 +705,7 @@ __global__ void __launch_bounds__(1024) k_pair_place(const Body* __restrict__ bo
     }
 }
 
-// the queries with pairs run again and write them at their places
+// the queries' pairs at their places: copied from ptmp, or the query run again where they were not kept
 __global__ void __launch_bounds__(kQueryChunk) k_pair_write(const Body* __restrict__ bodies, const float4* __restrict__ nd, Contacts C) {
     const int nch = min(C.sc[2], C.chunk_cap);
     for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
@@ -704,7 +720,12 @@ __global__ void __launch_bounds__(kQueryChunk) k_pair_write(const Body* __restri
         if (C.q_count[q] == start) continue;
         const int root = S.root;
         if (C.isl_pcnt[root] == 0) continue; // (the pair list was full)
-        run_query(S, C, bodies, nd, g, t, C.pairs + C.isl_poff[root] + start);
+        int2* dst = C.pairs + C.isl_poff[root] + start;
+        const int at = C.q_tmp[q];
+        if (at >= 0)
+            for (int k = 0, n = C.q_count[q] - start; k < n; k++) dst[k] = C.ptmp[at + k];
+        else
+            run_query(S, C, bodies, nd, g, t, dst, 0x7fffffff);
     }
 }
 

@@ -236,7 +236,8 @@ struct bl_gpu_ctx {
     DevBuf<float4> g_rec, sb_pos;
     DevBuf<int4> sb_cell, q_group;
     DevBuf<int> g_hi, q_count, sc;
-    DevBuf<int2> q_chunk;
+    DevBuf<int2> q_chunk, ptmp;
+    DevBuf<int> q_tmp;
     DevBuf<IslSearch> isl;
     DevBuf<uint32_t> hbits;
     DevBuf<ContactRec> crec;
@@ -306,7 +307,7 @@ static void free_contacts(bl_gpu_ctx* c) {
     c->bk_items.free_(), c->run_end.free_(), c->g_start.free_(), c->g_fill.free_(), c->g_items.free_(), c->counters.free_();
     c->pairs.free_(), c->hit_a.free_(), c->hit_b.free_();
     c->g_rec.free_(), c->sb_pos.free_(), c->sb_cell.free_(), c->q_group.free_(), c->g_hi.free_(), c->q_count.free_(), c->sc.free_();
-    c->q_chunk.free_(), c->isl.free_(), c->hbits.free_(), c->hidx.free_(), c->crec.free_(), c->crec_n.free_();
+    c->q_chunk.free_(), c->ptmp.free_(), c->q_tmp.free_(), c->isl.free_(), c->hbits.free_(), c->hidx.free_(), c->crec.free_(), c->crec_n.free_();
     c->contacts_on = false;
 }
 
@@ -1047,8 +1048,10 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     BL_CUDA(c, c->q_count.alloc(q_cap));
     BL_CUDA(c, c->q_group.alloc(grp_cap));
     BL_CUDA(c, c->q_chunk.alloc(chunk_cap));
-    BL_CUDA(c, c->sc.alloc(4));
-    BL_CUDA(c, cudaMemsetAsync(c->sc.p, 0, 4 * sizeof(int), c->stream));
+    BL_CUDA(c, c->q_tmp.alloc(q_cap));
+    BL_CUDA(c, c->ptmp.alloc(c->cfg.max_pairs));
+    BL_CUDA(c, c->sc.alloc(8));
+    BL_CUDA(c, cudaMemsetAsync(c->sc.p, 0, 8 * sizeof(int), c->stream));
     BL_CUDA(c, cudaFuncSetAttribute(k_rebuild, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RebuildShared)));
     // (the pair list starts as valid indices: k_detect reads up to the last search's total)
     BL_CUDA(c, cudaMemsetAsync(c->pairs.p, 0, sizeof(int2) * c->cfg.max_pairs, c->stream));
@@ -1067,6 +1070,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     C.bk_items = c->bk_items.p, C.run_end = c->run_end.p, C.g_start = c->g_start.p, C.g_fill = c->g_fill.p, C.g_items = c->g_items.p;
     C.g_rec = c->g_rec.p, C.g_hi = c->g_hi.p, C.sb_cell = c->sb_cell.p, C.sb_pos = c->sb_pos.p, C.isl = c->isl.p;
     C.q_group = c->q_group.p, C.q_chunk = c->q_chunk.p, C.q_count = c->q_count.p, C.sc = c->sc.p;
+    C.ptmp = c->ptmp.p, C.q_tmp = c->q_tmp.p, C.ptmp_cap = c->cfg.max_pairs;
     C.hbits = c->hbits.p, C.hidx = c->hidx.p, C.crec = c->crec.p, C.crec_n = c->crec_n.p, C.crec_cap = crec_cap;
     C.whole_max = c->cfg.contact_whole_max;
     C.q_cap = q_cap, C.grp_cap = grp_cap, C.chunk_cap = chunk_cap, C.cell_cap = cell_cap;
@@ -1499,7 +1503,7 @@ static int enqueue_frame(bl_gpu_ctx* c, int n, cudaStream_t s, cudaEvent_t* ev =
             k_wake<<<c->B, 256, 0, s>>>(c->dbodies.p, c->bmeta.p);
             if (rebuild_at(c, k)) {
                 cudaMemsetAsync(c->pair_total.p, 0, sizeof(int), s);
-                cudaMemsetAsync(c->sc.p, 0, 4 * sizeof(int), s);
+                cudaMemsetAsync(c->sc.p, 0, 8 * sizeof(int), s);
                 k_rebuild<<<c->B, 1024, sizeof(RebuildShared), s>>>(c->dbodies.p, c->B, c->nd.p, c->info.p, CT, k == 0 ? 1 : 0, c->deverr.p);
                 k_pair_count<<<kQueryGrid, kQueryChunk, 0, s>>>(c->dbodies.p, c->nd.p, CT);
                 k_pair_place<<<c->B, 1024, 0, s>>>(c->dbodies.p, c->B, CT, c->deverr.p);
