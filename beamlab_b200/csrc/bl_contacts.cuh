@@ -79,7 +79,10 @@ struct Contacts {
     int4* q_group;             // query groups: island (isl_idx), kind | k << 1 | ko << 9, triangles, first query
     int2* q_chunk;             // chunks of kQueryChunk queries of one group: group, first triangle of the chunk
     int* q_count;              // per query (a triangle of a group): its pairs, then their running sum over the island
-    int* sc;                   // search counters: [0] queries [1] groups [2] chunks [3] grid cells
+    int* sc;                   // search counters: [0] queries [1] groups [2] chunks [3] grid cells [4] ptmp
+    int2* ptmp;                // the count pass's pairs, query by query (ptmp_cap)
+    int* q_tmp;                // per query with pairs: its pairs in ptmp (-1: not kept)
+    int ptmp_cap;
     int q_cap, grp_cap, chunk_cap, cell_cap;
     int* counters;             // [0] pair searches [1] contacts [2] pairs of the searches
     int interval;              // rebuild interval in substeps (world.cpp:1887)
