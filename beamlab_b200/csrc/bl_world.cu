@@ -1043,7 +1043,7 @@ static int commit_contacts(bl_gpu_ctx* c, std::vector<Body>& recs) {
     BL_CUDA(c, c->sb_cell.alloc(N));
     BL_CUDA(c, c->sb_pos.alloc(N));
     // queries: a triangle against a hash or a grid; a full list flags DEVERR_PAIRS
-    const int q_cap = 8 * std::max(c->NTRI, 1) + 65536, grp_cap = B * std::min(B, kIslMaxBodies) + B, chunk_cap = grp_cap + q_cap / kQueryChunk;
+    const int q_cap = std::max(8 * std::max(c->NTRI, 1) + 65536, c->cfg.max_pairs), grp_cap = B * std::min(B, kIslMaxBodies) + B, chunk_cap = grp_cap + q_cap / kQueryChunk;
     BL_CUDA(c, c->isl.alloc(c->max_isl));
     BL_CUDA(c, c->q_count.alloc(q_cap));
     BL_CUDA(c, c->q_group.alloc(grp_cap));

@@ -66,7 +66,10 @@ typedef struct {
                                   ceil(1 / (collision_hz dt)) substeps and at each frame's start */
     int32_t inter_body_collisions; /* WorldSettings::inter_body_collisions (1) */
     int32_t max_pairs;         /* capacity of the contact pair list of all islands (default 2^21); more pairs in one
-                                  search raise BL_GPU_DEVERR_PAIRS and that island's contacts are skipped */
+                                  search raise BL_GPU_DEVERR_PAIRS and that island's contacts are skipped. The search's
+                                  triangle queries (a triangle against a hash or a fast body's grid) hold at least as
+                                  many, and 8 x the collision triangles + 65,536: more - a pile-up of many fast bodies
+                                  all in reach of one another - raise BL_GPU_DEVERR_PAIRS the same way */
     /* the FEM frames' implicit step (no counterpart in the reference, which always factors): */
     int32_t fem_solver;        /* BL_GPU_FEM_CHOLESKY (default: the reference's block Cholesky), BL_GPU_FEM_PCG (conjugate
                                   gradients, block-Jacobi, from zero), BL_GPU_FEM_PCG_LEARNED (from the energy-norm best
@@ -322,7 +325,7 @@ typedef struct {
 enum {
     BL_GPU_DEVERR_CANDIDATES = 1 << 0, /* a body's static candidate list overflowed BL_GPU_MAX_CANDIDATES */
     BL_GPU_DEVERR_NONFINITE = 1 << 1,  /* a body needed the repair of non-finite / runaway nodes */
-    BL_GPU_DEVERR_PAIRS = 1 << 2,      /* the contact pair list overflowed bl_gpu_config.max_pairs */
+    BL_GPU_DEVERR_PAIRS = 1 << 2,      /* the contact pair list (or the search's queries) overflowed bl_gpu_config.max_pairs */
     BL_GPU_DEVERR_ISLAND = 1 << 3,     /* an island with contact pairs held more than BL_GPU_MAX_ISLAND_BODIES bodies */
     BL_GPU_DEVERR_CONTACT_UNSUPPORTED = 1 << 5, /* a body with a FEM frame met another body's triangles (not stepped) */
     BL_GPU_DEVERR_TIMEOUT = 1 << 6     /* a kernel's bounded wait on its own bulk copies ran out (bulk_wait_s): the
