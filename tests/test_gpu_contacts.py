@@ -154,3 +154,28 @@ def test_fleet_contacts_whole_equal_chunks():
     assert sa["contacts"] == sb["contacts"] > 1000 and sa["device_errors"] == sb["device_errors"] == 0
     a.close()
     b.close()
+
+
+def test_fleet_pairs_4000_substeps_equal_reference(ref_lib):
+    """The 16-vehicle crashing fleet over the configuration's horizon: 122 frames of 33 substeps (4,026) on the GPU and
+    by the compiled reference - the crashes, the rebounds and the vehicles rolling on after them. Every 11th frame the
+    pair lists equal the reference's; at the end every node's position and velocity is bitwise the reference's."""
+    from oracle.oracle import RefWorld, build_world
+    rig = rigs.fleet(16, seed=5, median_nodes=900, min_nodes=300, max_nodes=3000, terrain_size=400.0, terrain_samples=513,
+                     layout="pairs")
+    w = world_from_rig(rig)
+    r = build_world(RefWorld, rig, multithreaded=False)
+    for f in range(122):
+        w.step_substeps(33)
+        r.step_substeps(33)
+        if f % 11 == 0:
+            got, want = w.pairs(), r.pairs()
+            assert got.shape == want.shape and np.array_equal(got, want), f"frame {f}: pair lists differ ({len(got)} vs {len(want)})"
+    for b in range(len(rig["bodies"])):
+        g, ref = w.bodies()[b].nodes(), r.nodes(b)
+        assert np.array_equal(bits(g["p"]), bits(ref["pos"])), f"vehicle {b}: positions differ"
+        assert np.array_equal(bits(g["v"]), bits(ref["vel"])), f"vehicle {b}: velocities differ"
+    st = w.stats()
+    assert st["contacts"] > 1000 and st["device_errors"] == 0
+    w.close()
+    r.close()
