@@ -377,17 +377,20 @@ __global__ void __launch_bounds__(256) k_detect(const float4* __restrict__ nd, c
 // ------------------------------------------------------------------------------------------ response (each substep)
 // World::collide_pairs for node-triangle pairs (world.cpp:2975-3023): each contact cancels the forces accumulated so far
 // on its node and its triangle's corners (earlier contacts' included), so an island's contacts run one after another
-// in pair order, as the reference's loop (world.cpp:2999). A CTA an island:
-//  1. its contacts' nodes hashed into shared-memory slots and their forces loaded there (all threads);
-//  2. in chunks of the island's contacts (its pairs with a hit, in pair order, gathered by a block scan), each
-//     contact's record - its slots, the accumulation weights, relative velocity and normal, and every
-//     term of the contact law that does not depend on the forces (the slip direction and speed, the Stribeck
-//     exponentials, the restitution term) - formed in parallel;
-//  3. the chain: per contact only the force-dependent arithmetic (apply_contact), on shared memory, level by level -
-//     a contact's level is one above its nodes' earlier contacts' levels, so the contacts of one level touch
-//     distinct nodes and each sees the forces the serial loop would give it;
+// in pair order, as the reference's loop (world.cpp:2999) - but only contacts that share a node depend on each other.
+// A CTA an island:
+//  1. its contacts (its pairs with a hit bit, in pair order) listed by a block scan; their nodes hashed into
+//     shared-memory force slots and the forces loaded there;
+//  2. each contact's record - its slots, the accumulation weights, relative velocity and normal, and every term of the
+//     contact law that does not depend on the forces (the slip direction and speed, the Stribeck exponentials, the
+//     restitution and push terms, the soft ground's drag and buoyancy) - formed in parallel;
+//  3. each contact's level, one above its nodes' earlier contacts' levels (one thread, in pair order), so the contacts
+//     of one level touch distinct nodes; the levels run one after another, a level's contacts at once, each contact
+//     with only its force-dependent arithmetic (apply_contact) - every contact sees the forces the serial loop gives
+//     it. Up to Contacts::whole_max contacts the island runs whole (its records in global memory, its levels over all
+//     of it, formed while the records are); more, 512 at a time (records and levels in shared memory);
 //  4. the forces written back. An island with more distinct contact nodes than the slots hold runs the loop on global
-//     memory (collide_island_global). Results are the same bits either way.
+//     memory (collide_island_global). Results are the same bits every way.
 __device__ void collide_island_global(const float4* __restrict__ nd, const int4* __restrict__ info, Body* __restrict__ bodies, Contacts C,
                                       float4* __restrict__ Fs, int root, int off, int cnt);
 
