@@ -81,3 +81,19 @@ def test_softbody_builder_calls():
     assert sb.nodes["inv_mass"].tolist() == [0.5, 0.0, 0.0]
     assert sb.beams["L"][0] == np.float32(1e-3) and sb.beams["L"][1] == np.float32(3.0)
     assert sb.beams["max_neg"][1] == -3.0 and sb.beams["type"][1] == 1 and sb.beams["strength"][1] == 7.0
+
+
+def test_config_defaults_and_refusals_without_a_gpu():
+    """bl_gpu_default_config's contact_whole_max is the most an island runs whole (6,144); bl_gpu_create refuses a
+    value outside 0..6,144 (and other out-of-range settings) before it touches a device."""
+    L = _lib.lib()
+    cfg = _Config()
+    L.bl_gpu_default_config(C.byref(cfg))
+    assert cfg.contact_whole_max == 6144 and cfg.max_pairs == 1 << 21 and cfg.bulk_wait_s == 1.0
+    ctx = C.c_void_p()
+    for field, bad in (("contact_whole_max", 6145), ("contact_whole_max", -1), ("max_pairs", 0), ("bulk_wait_s", 11.0)):
+        c = _Config()
+        L.bl_gpu_default_config(C.byref(c))
+        setattr(c, field, bad)
+        assert L.bl_gpu_create(C.byref(c), C.byref(ctx)) == -1, field  # (BL_GPU_EINVAL)
+        assert not ctx.value
