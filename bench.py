@@ -43,6 +43,20 @@ BYTES_PER_BEAM = 40
 BYTES_PER_NODE = 52
 
 
+def broadphase_bytes(rig: dict, pairs: int) -> dict:
+    """Algorithmic bytes of one pair search (a contacter node: its position read, its cell key and id written and
+    sorted, 12 + 12 + 4 x 2 x 12 = 120 B; a collision triangle: its 3 indices and 3 positions read, 48 B; a pair
+    written, 12 B) and the searches a substep (the frame's first substep and every ceil(1 / (collision_hz dt)) after)."""
+    import math
+    contacters = sum(int(np.count_nonzero(np.asarray(b["node_flags"]) & 16)) for b in rig["bodies"])
+    tris = sum(len(b.get("tris", ())) for b in rig["bodies"])
+    st = rig.get("settings", {})
+    dt, hz = float(st.get("dt", 0.0005)), float(st.get("collision_hz", 120.0))
+    interval = max(1, math.ceil(1.0 / (max(hz, 1.0) * dt) - 1e-6))
+    return {"bytes_per_search": 120 * contacters + 48 * tris + 12 * pairs, "contacter_nodes": contacters, "triangles": tris,
+            "searches_per_substep": len(range(0, FRAME, interval)) / FRAME}
+
+
 def workload(name: str, rank: int):
     from beamlab_b200 import rigs
     if name == "fleet256":
@@ -436,12 +450,17 @@ def run_gpu(args):
             # arithmetic - latency-bound rather than HBM-bound
             pairs = len(w.pairs())
             frames_timed = K
+            bp = broadphase_bytes(rig, pairs)
+            search_gbs = (bp["bytes_per_search"] * bp["searches_per_substep"] / (per["search"] * 1e-3) / 1e9
+                          if per["search"] > 0 else None)
             out["contacts_step"] = {
                 "pairs_last_search": pairs, "contacts_per_substep": (st1["contacts"] - st0["contacts"]) / (frames_timed * FRAME),
                 "ms_per_substep": per["contacts"], "pair_search_ms_per_substep": per["search"],
                 "narrow_phase_bytes_per_substep": 64 * pairs,
                 "achieved_gbs": 64 * pairs / (per["contacts"] * 1e-3) / 1e9 if per["contacts"] > 0 else None,
-                "bound": "latency (the deepest island's levels of dependent contacts)"}
+                "bound": "latency (the deepest island's levels of dependent contacts)",
+                "pair_search": {**bp, "achieved_gbs": search_gbs,
+                                "bound": "latency (an island's set-up in the reference's order, then every query at once)"}}
         if ws == 1 and args.workload == "plate64" and not args.no_solvers:
             out["fem_solvers"] = fem_solvers(local)
         if ws == 1 and args.workload == "shellcar" and not args.no_solvers:
