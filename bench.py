@@ -48,7 +48,7 @@ def broadphase_bytes(rig: dict, pairs: int) -> dict:
     sorted, 12 + 12 + 4 x 2 x 12 = 120 B; a collision triangle: its 3 indices and 3 positions read, 48 B; a pair
     written, 12 B) and the searches a substep (the frame's first substep and every ceil(1 / (collision_hz dt)) after)."""
     import math
-    contacters = sum(int(np.count_nonzero(np.asarray(b["node_flags"]) & 16)) for b in rig["bodies"])
+    contacters = sum(int(np.count_nonzero(np.asarray(b.get("node_flags", ()), np.int64) & 16)) for b in rig["bodies"])
     tris = sum(len(b.get("tris", ())) for b in rig["bodies"])
     st = rig.get("settings", {})
     dt, hz = float(st.get("dt", 0.0005)), float(st.get("collision_hz", 120.0))
