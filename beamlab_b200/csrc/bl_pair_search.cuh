@@ -56,7 +56,7 @@ struct RebuildShared {
     double term1[1024];
     int warp[32];
     int npts, fail;
-    int g_base, c_base, ngroups, nchunks;
+    int g_base, c_base;   // the island's first group and chunk
 };
 
 __device__ __forceinline__ bool same_group(const Body& a, const Body& b) { return a.group != 0 && a.group == b.group; }
